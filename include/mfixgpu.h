@@ -1,0 +1,158 @@
+/*
+ * mfixgpu.h -- C ABI of the B200 replacement for MFIX's linear-equation hot
+ * path, SOLVE_LIN_EQ -> LEQ_BICGS (MFIX 2016-1).
+ *
+ * A Fortran host binds these through ISO_C_BINDING (fortran/mfixgpu_mod.f90)
+ * or, for mfixgpu_solve_lin_eq_, through gfortran's implicit calling
+ * convention.  Arrays are passed the way the reference passes them: A_M is the
+ * whole A_M(DIMENSION_3,-3:3,0:DIMENSION_M) array in Fortran (column-major)
+ * order and M selects the phase, B_M is B_M(DIMENSION_3,0:DIMENSION_M).
+ * Plain pointers and sizes only; no exceptions cross the boundary.
+ *
+ * Error convention: the reference's IER values (0 converged, -1 not converged
+ * but below 0.2*Rnorm0, -2 breakdown / singular row, model/leq_bicgs.f:189-233,
+ * 485-495) plus the codes below, all <= -10, where the reference would stop
+ * the run through MFIX_EXIT.
+ */
+#ifndef MFIXGPU_H
+#define MFIXGPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define MFIXGPU_ERR_UNSUPPORTED (-10) /* METHOD/PC/SWEEP/geometry not served (the reference: MFIX_EXIT) */
+#define MFIXGPU_ERR_NOMEM (-11)       /* device memory */
+#define MFIXGPU_ERR_DGTSV (-12)       /* DGTSV INFO != 0 in a JK/IJ sweep (model/leqsol_mod.f:991-996) */
+#define MFIXGPU_ERR_CUDA (-13)        /* CUDA runtime error */
+#define MFIXGPU_ERR_ARGS (-14)        /* inconsistent arguments */
+#define MFIXGPU_ERR_INCOMPLETE (-15)  /* solve stopped without a verdict */
+#define MFIXGPU_ERR_NOGEOM (-16)      /* mfixgpu_init_geometry was not called */
+
+/* ---------------------------------------------------------------- drop-in */
+
+/* Registers the box geometry that SOLVE_LIN_EQ reads from modules: IMAX2,
+ * JMAX2, KMAX2 (model/set_max2.f:48-135), DO_K, DIMENSION_3
+ * (model/set_param.f:98) and DIMENSION_M.  Call once after SET_INCREMENTS.
+ * Only the serial, non-cyclic, non-cut-cell box is served: neighbour offsets
+ * clamp at the array edge as in model/set_increments.f:80-109.  Returns 0 or
+ * MFIXGPU_ERR_ARGS. */
+int mfixgpu_init_geometry(const int *imax2, const int *jmax2, const int *kmax2, const int *do_k,
+                          const int64_t *dimension_3, const int *dimension_m);
+
+/* SOLVE_LIN_EQ(VNAME, VNO, VAR, A_M, B_M, M, ITMAX, METHOD, SWEEP, TOL1, PC, IER),
+ * model/solve_lin_eq.f:17-78, in gfortran's convention: every argument by
+ * reference, CHARACTER lengths appended by value.  METHOD 2 (BiCGSTAB,
+ * :137-153) is served; METHOD 4 (:161-171) is served while BiCGSTAB does not
+ * break down, and returns MFIXGPU_ERR_UNSUPPORTED where the reference would
+ * fall back to GMRES; others return MFIXGPU_ERR_UNSUPPORTED.  As in
+ * model/leq_bicgs.f:194-233, A_M(:,:,M) and B_M(:,M) come back unit-scaled
+ * (option "write_back_ab"). */
+void mfixgpu_solve_lin_eq_(const char *vname, const int *vno, double *var, double *a_m, double *b_m,
+                           const int *m, const int *itmax, const int *method, const char *sweep,
+                           const double *tol1, const char *pc, int *ier, size_t vname_len, size_t sweep_len,
+                           size_t pc_len);
+
+/* The same call with values and explicit lengths, for a BIND(C) interface. */
+void mfixgpu_solve_lin_eq(const char *vname, int vname_len, int vno, double *var, double *a_m, double *b_m,
+                          int m, int itmax, int method, const char *sweep, int sweep_len, double tol1,
+                          const char *pc, int pc_len, int *ier);
+
+/* ITER_TOT(VNO) of MODULE leqsol (model/leqsol_mod.f:17), 1-based VNO in
+ * 1..10 (DIM_EQS, model/param_mod.f:97); the accounting of
+ * model/leq_bicgs.f:458,491. */
+int mfixgpu_iter_tot(int vno);
+void mfixgpu_reset_iter_tot(void);
+
+typedef struct {
+    int ier;
+    int iterations;     /* the reference's ITER at exit (mixed form: inner iterations) */
+    int iter_tot_add;
+    int exit_kind;      /* 0 Rnorm test, 1 Snorm<=TOLMIN, 2 rho=0, 3 ITMAX, 4 singular row, 5 error */
+    int line_skips;     /* J-lines left unchanged on DGTSV INFO != 0 (model/leqsol_mod.f:910-914) */
+    int line_fallbacks; /* J-lines solved by the sequential pivoting DGTSV path */
+    int outer_steps;    /* mixed form: FP64 refinement steps */
+    int pad;
+    double rnorm0, rnorm;
+    double seconds;     /* wall time of the call, copies included */
+    double device_ms;   /* device time of the solve (CUDA events), copies excluded */
+    double jline_ms;    /* summed J-line sweep kernel time (option "time_kernels") */
+    int jline_launches; /* J-line sweep launches timed */
+    int pad2;
+    long long kernel_launches; /* kernels of this library launched by the solve */
+} mfixgpu_stats;
+
+int mfixgpu_last_stats(mfixgpu_stats *out);
+const char *mfixgpu_last_error(void);
+
+/* Options (no reference counterpart; defaults reproduce the reference):
+ *   "precision"      0 FP64 drop-in (default), 1 FP32 inner / FP64 refinement
+ *   "write_back_ab"  1 (default) copy the scaled A_M/B_M slices back
+ *   "rtilde_seed"    seed of the Rtilde random stream (replaces RANDOM_NUMBER, model/leq_bicgs.f:298)
+ *   "inner_tol"      mixed form: relative drop asked of each inner solve (default 1e-4)
+ *   "check_every"    iterations between host polls of convergence (default 4)
+ *   "use_graph"      1 (default) replay the iteration body as a CUDA graph
+ *   "time_kernels"   1: time every J-line sweep launch with CUDA events (no graph replay)
+ * Returns 0, or MFIXGPU_ERR_ARGS for an unknown name. */
+int mfixgpu_set_option(const char *name, double value);
+double mfixgpu_get_option(const char *name);
+
+/* Releases device memory and the per-device engine. */
+void mfixgpu_finalize(void);
+
+/* ---------------------------------------------------------------- single routines on device arrays */
+
+typedef struct {
+    int imax2, jmax2, kmax2, do_k;
+    int64_t dimension_3;
+} mfixgpu_geom;
+
+/* LEQ_MATVEC(VNAME, VAR, A_M, AVAR), model/leqsol_mod.f:103-265: avar = A*var. */
+int mfixgpu_leq_matvec(const mfixgpu_geom *g, const double *a_dev, const double *var_dev, double *avar_dev);
+
+/* LEQ_MSOLVE / LEQ_MSOLVE1 / LEQ_MSOLVE0 (model/leqsol_mod.f:286-749) chosen by
+ * PC as in model/leq_bicgs.f:74-87: var = M^{-1} b.  sweep and pc are 4
+ * characters, blank padded. */
+int mfixgpu_leq_msolve(const mfixgpu_geom *g, const double *b_dev, const double *a_dev, double *var_dev,
+                       const char *sweep, const char *pc);
+
+/* DOT_PRODUCT_PAR(R1, R2), model/leqsol_mod.f:1094-1201, serial semantics
+ * (the whole array): *out = sum r1*r2, reduced in a fixed order. */
+int mfixgpu_dot_product_par(const double *r1_dev, const double *r2_dev, int64_t n, double *out);
+
+/* ---------------------------------------------------------------- batches */
+
+typedef struct {
+    int imax2, jmax2, kmax2, do_k;
+    int64_t dimension_3;
+    double *a_m;  /* 7*DIMENSION_3, the phase slice A_M(:,:,M) */
+    double *b_m;  /* DIMENSION_3 */
+    double *var;  /* DIMENSION_3, initial guess in, solution out */
+    double tol;
+    int itmax;
+    /* results */
+    int ier;
+    int iterations;
+    int outer_steps;
+    int exit_kind;
+    int pad;
+    double rnorm0, rnorm;
+} mfixgpu_system;
+
+/* Solves independent systems of uneven sizes together: every kernel launch of
+ * an iteration covers all of them (the SIMPLE loop's back-to-back calls, e.g.
+ * model/solve_vel_star.f:315-331).  Each system follows the drop-in's
+ * algorithm; results are bit-identical to solving it alone.  precision 0/1 as
+ * the "precision" option; on_device 1: the pointers are device memory, solved
+ * in place.  sweep letters R and S only (other letters: single solves). */
+int mfixgpu_batch_solve(mfixgpu_system *systems, int nsys, const char *sweep, const char *pc, int precision,
+                        int on_device);
+/* mfixgpu_last_stats after a batch: seconds, device_ms, jline_*, kernel_launches of the whole batch. */
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MFIXGPU_H */

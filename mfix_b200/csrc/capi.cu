@@ -1,0 +1,445 @@
+// capi.cu -- the extern "C" boundary (include/mfixgpu.h).
+//
+// The Fortran SOLVE_LIN_EQ signature is kept: the drop-in receives the whole
+// A_M / B_M arrays and the phase index M, decodes METHOD / PC / SWEEP the way
+// model/solve_lin_eq.f:131-191 and model/leq_bicgs.f:74-87 do, and hands one
+// system to the engine.  No C++ exception crosses the boundary; every failure
+// is an IER code.
+#include <chrono>
+#include <cstring>
+#include <memory>
+#include <mutex>
+#include <new>
+#include <string>
+
+#include "../../include/mfixgpu.h"
+#include "leq_engine.h"
+
+using namespace mfixgpu;
+
+namespace {
+
+struct Geometry {
+    bool set = false;
+    int imax2 = 0, jmax2 = 0, kmax2 = 0, do_k = 1;
+    int64_t n = 0;
+    int dimension_m = 0;
+};
+
+struct Options {
+    int precision = PREC_FP64;
+    int write_back_ab = 1;
+    uint64_t seed = 0x5EEDULL;
+    double inner_tol = 1e-4;
+    int check_every = 4;
+    int use_graph = 1;
+    int time_kernels = 0;
+};
+
+struct Global {
+    std::mutex mu;
+    std::unique_ptr<Engine> engine;
+    Geometry geom;
+    Options opt;
+    int iter_tot[10] = {0};
+    mfixgpu_stats last{};
+    std::string err;
+};
+
+Global &G()
+{
+    static Global g;
+    return g;
+}
+
+Engine *engine_locked(Global &g)
+{
+    if (!g.engine) {
+        int n = 0;
+        if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+            cudaGetLastError();
+            g.err = "no CUDA device visible";
+            return nullptr;
+        }
+        try {
+            g.engine.reset(new Engine());
+        } catch (...) {
+            g.err = "engine construction failed";
+            return nullptr;
+        }
+    }
+    return g.engine.get();
+}
+
+// Fortran CHARACTER(LEN=4) value of a (pointer, length) pair: truncated or blank padded.
+void fortran_char4(const char *s, size_t len, char out[4])
+{
+    for (int q = 0; q < 4; ++q) out[q] = (s && (size_t)q < len) ? s[q] : ' ';
+}
+
+// model/leq_bicgs.f:74-87 (exact, case-sensitive comparison as in Fortran)
+int decode_pc(const char pc4[4])
+{
+    if (!std::memcmp(pc4, "LINE", 4)) return PC_LINE;
+    if (!std::memcmp(pc4, "DIAG", 4)) return PC_DIAG;
+    if (!std::memcmp(pc4, "NONE", 4)) return PC_NONE;
+    return -1;
+}
+
+double now_s()
+{
+    return std::chrono::duration<double>(std::chrono::steady_clock::now().time_since_epoch()).count();
+}
+
+SolveOptions make_opts(const Options &o, int pc, const char sweep4[4])
+{
+    SolveOptions so;
+    so.pc = pc;
+    std::memcpy(so.sweep, sweep4, 4);
+    so.precision = o.precision;
+    so.write_back_ab = o.write_back_ab != 0;
+    so.seed = o.seed;
+    so.inner_tol = o.inner_tol;
+    so.check_every = o.check_every;
+    so.use_graph = o.use_graph != 0;
+    so.time_kernels = o.time_kernels != 0;
+    return so;
+}
+
+void solve_impl(int vno, double *var, double *a_m, double *b_m, int m, int itmax, int method, const char sweep4[4],
+                double tol, const char pc4[4], int *ier)
+{
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    const double t0 = now_s();
+    g.last = mfixgpu_stats{};
+    auto finish = [&](int code) {
+        if (ier) *ier = code;
+        g.last.ier = code;
+        g.last.seconds = now_s() - t0;
+    };
+    if (!ier) return;
+    if (!g.geom.set) {
+        g.err = "mfixgpu_init_geometry has not been called";
+        return finish(MFIXGPU_ERR_NOGEOM);
+    }
+    if (!var || !a_m || !b_m) {
+        g.err = "null array argument";
+        return finish(MFIXGPU_ERR_ARGS);
+    }
+    if (m < 0 || m > g.geom.dimension_m) {
+        g.err = "phase index M outside 0:DIMENSION_M";
+        return finish(MFIXGPU_ERR_ARGS);
+    }
+    // model/solve_lin_eq.f:131-191
+    if (method != 2 && method != 4) {
+        g.err = "LEQ_METHOD " + std::to_string(method) + " is not served by the GPU path (BiCGSTAB only)";
+        return finish(MFIXGPU_ERR_UNSUPPORTED);
+    }
+    const int pc = decode_pc(pc4);
+    if (pc < 0) {
+        g.err = "preconditioner option not found";  // the reference's message, model/leq_bicgs.f:84-85
+        return finish(MFIXGPU_ERR_UNSUPPORTED);
+    }
+    Engine *e = engine_locked(g);
+    if (!e) return finish(MFIXGPU_ERR_CUDA);
+    const int64_t n = g.geom.n;
+    SystemSpec s;
+    s.imax2 = g.geom.imax2;
+    s.jmax2 = g.geom.jmax2;
+    s.kmax2 = g.geom.kmax2;
+    s.do_k = g.geom.do_k;
+    s.n = n;
+    s.a = a_m + (size_t)m * 7 * (size_t)n;  // A_M(:,:,M)
+    s.b = b_m + (size_t)m * (size_t)n;      // B_M(:,M)
+    s.x = var;
+    s.tol = tol;
+    s.itmax = itmax;
+    std::vector<SolveResult> out;
+    const int rc = e->solve({s}, make_opts(g.opt, pc, sweep4), out);
+    if (rc) {
+        g.err = e->last_error();
+        return finish(rc);
+    }
+    const SolveResult &r = out[0];
+    int code = r.ier;
+    if (method == 4 && code == -2) {  // :166-171 would continue with GMRES
+        g.err = "BiCGSTAB broke down and METHOD=4 asks for GMRES, which the GPU path does not serve";
+        code = MFIXGPU_ERR_UNSUPPORTED;
+    }
+    if (vno >= 1 && vno <= 10) g.iter_tot[vno - 1] += r.iter_tot_add;
+    g.last.iterations = r.iterations;
+    g.last.iter_tot_add = r.iter_tot_add;
+    g.last.exit_kind = r.exit_kind;
+    g.last.line_skips = r.line_skips;
+    g.last.line_fallbacks = r.line_fallbacks;
+    g.last.outer_steps = r.outer_steps;
+    g.last.rnorm0 = r.rnorm0;
+    g.last.rnorm = r.rnorm;
+    g.last.device_ms = e->timing().device_ms;
+    g.last.jline_ms = e->timing().jline_ms;
+    g.last.jline_launches = e->timing().jline_launches;
+    g.last.kernel_launches = e->timing().kernel_launches;
+    finish(code);
+}
+
+}  // namespace
+
+extern "C" {
+
+int mfixgpu_init_geometry(const int *imax2, const int *jmax2, const int *kmax2, const int *do_k,
+                          const int64_t *dimension_3, const int *dimension_m)
+{
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    if (!imax2 || !jmax2 || !kmax2 || !do_k || !dimension_3 || !dimension_m) return MFIXGPU_ERR_ARGS;
+    if (*imax2 < 1 || *jmax2 < 1 || *kmax2 < 1 || *dimension_m < 0) return MFIXGPU_ERR_ARGS;
+    if (!*do_k && *kmax2 != 1) return MFIXGPU_ERR_ARGS;
+    if ((int64_t)*imax2 * *jmax2 * *kmax2 != *dimension_3) return MFIXGPU_ERR_ARGS;
+    g.geom.set = true;
+    g.geom.imax2 = *imax2;
+    g.geom.jmax2 = *jmax2;
+    g.geom.kmax2 = *kmax2;
+    g.geom.do_k = *do_k ? 1 : 0;
+    g.geom.n = *dimension_3;
+    g.geom.dimension_m = *dimension_m;
+    return 0;
+}
+
+void mfixgpu_solve_lin_eq_(const char *vname, const int *vno, double *var, double *a_m, double *b_m, const int *m,
+                           const int *itmax, const int *method, const char *sweep, const double *tol1,
+                           const char *pc, int *ier, size_t vname_len, size_t sweep_len, size_t pc_len)
+{
+    (void)vname;
+    (void)vname_len;
+    if (!vno || !m || !itmax || !method || !tol1) {
+        if (ier) *ier = MFIXGPU_ERR_ARGS;
+        return;
+    }
+    char s4[4], p4[4];
+    fortran_char4(sweep, sweep_len, s4);
+    fortran_char4(pc, pc_len, p4);
+    solve_impl(*vno, var, a_m, b_m, *m, *itmax, *method, s4, *tol1, p4, ier);
+}
+
+void mfixgpu_solve_lin_eq(const char *vname, int vname_len, int vno, double *var, double *a_m, double *b_m, int m,
+                          int itmax, int method, const char *sweep, int sweep_len, double tol1, const char *pc,
+                          int pc_len, int *ier)
+{
+    (void)vname;
+    (void)vname_len;
+    char s4[4], p4[4];
+    fortran_char4(sweep, sweep_len < 0 ? 0 : (size_t)sweep_len, s4);
+    fortran_char4(pc, pc_len < 0 ? 0 : (size_t)pc_len, p4);
+    solve_impl(vno, var, a_m, b_m, m, itmax, method, s4, tol1, p4, ier);
+}
+
+int mfixgpu_iter_tot(int vno)
+{
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    return (vno >= 1 && vno <= 10) ? g.iter_tot[vno - 1] : 0;
+}
+
+void mfixgpu_reset_iter_tot(void)
+{
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    for (int &v : g.iter_tot) v = 0;
+}
+
+int mfixgpu_last_stats(mfixgpu_stats *out)
+{
+    if (!out) return MFIXGPU_ERR_ARGS;
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    *out = g.last;
+    return 0;
+}
+
+const char *mfixgpu_last_error(void)
+{
+    Global &g = G();
+    return g.err.c_str();
+}
+
+int mfixgpu_set_option(const char *name, double value)
+{
+    if (!name) return MFIXGPU_ERR_ARGS;
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    const std::string k(name);
+    if (k == "precision") {
+        if (value != 0 && value != 1) return MFIXGPU_ERR_ARGS;
+        g.opt.precision = (int)value;
+    } else if (k == "write_back_ab") {
+        g.opt.write_back_ab = value != 0;
+    } else if (k == "rtilde_seed") {
+        g.opt.seed = (uint64_t)value;
+    } else if (k == "inner_tol") {
+        if (!(value > 0 && value < 1)) return MFIXGPU_ERR_ARGS;
+        g.opt.inner_tol = value;
+    } else if (k == "check_every") {
+        if (value < 1) return MFIXGPU_ERR_ARGS;
+        g.opt.check_every = (int)value;
+    } else if (k == "use_graph") {
+        g.opt.use_graph = value != 0;
+    } else if (k == "time_kernels") {
+        g.opt.time_kernels = value != 0;
+    } else {
+        return MFIXGPU_ERR_ARGS;
+    }
+    return 0;
+}
+
+double mfixgpu_get_option(const char *name)
+{
+    if (!name) return 0.0;
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    const std::string k(name);
+    if (k == "precision") return g.opt.precision;
+    if (k == "write_back_ab") return g.opt.write_back_ab;
+    if (k == "rtilde_seed") return (double)g.opt.seed;
+    if (k == "inner_tol") return g.opt.inner_tol;
+    if (k == "check_every") return g.opt.check_every;
+    if (k == "use_graph") return g.opt.use_graph;
+    if (k == "time_kernels") return g.opt.time_kernels;
+    return 0.0;
+}
+
+void mfixgpu_finalize(void)
+{
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    g.engine.reset();
+}
+
+int mfixgpu_leq_matvec(const mfixgpu_geom *gm, const double *a_dev, const double *var_dev, double *avar_dev)
+{
+    if (!gm || !a_dev || !var_dev || !avar_dev) return MFIXGPU_ERR_ARGS;
+    if ((int64_t)gm->imax2 * gm->jmax2 * gm->kmax2 != gm->dimension_3 || gm->imax2 < 1 || gm->jmax2 < 1 ||
+        gm->kmax2 < 1)
+        return MFIXGPU_ERR_ARGS;
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    Engine *e = engine_locked(g);
+    if (!e) return MFIXGPU_ERR_CUDA;
+    SystemSpec s;
+    s.imax2 = gm->imax2;
+    s.jmax2 = gm->jmax2;
+    s.kmax2 = gm->kmax2;
+    s.do_k = gm->do_k ? 1 : 0;
+    s.n = gm->dimension_3;
+    const int rc = e->matvec(s, a_dev, var_dev, avar_dev);
+    if (rc) g.err = e->last_error();
+    return rc;
+}
+
+int mfixgpu_leq_msolve(const mfixgpu_geom *gm, const double *b_dev, const double *a_dev, double *var_dev,
+                       const char *sweep, const char *pc)
+{
+    if (!gm || !b_dev || !a_dev || !var_dev || !sweep || !pc) return MFIXGPU_ERR_ARGS;
+    if ((int64_t)gm->imax2 * gm->jmax2 * gm->kmax2 != gm->dimension_3 || gm->imax2 < 1 || gm->jmax2 < 1 ||
+        gm->kmax2 < 1 || (!gm->do_k && gm->kmax2 != 1))
+        return MFIXGPU_ERR_ARGS;
+    char s4[4], p4[4];
+    fortran_char4(sweep, 4, s4);
+    fortran_char4(pc, 4, p4);
+    const int pcode = decode_pc(p4);
+    if (pcode < 0) return MFIXGPU_ERR_UNSUPPORTED;
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    Engine *e = engine_locked(g);
+    if (!e) return MFIXGPU_ERR_CUDA;
+    SystemSpec s;
+    s.imax2 = gm->imax2;
+    s.jmax2 = gm->jmax2;
+    s.kmax2 = gm->kmax2;
+    s.do_k = gm->do_k ? 1 : 0;
+    s.n = gm->dimension_3;
+    const int rc = e->msolve(s, a_dev, b_dev, var_dev, pcode, s4);
+    if (rc) g.err = e->last_error();
+    return rc;
+}
+
+int mfixgpu_dot_product_par(const double *r1_dev, const double *r2_dev, int64_t n, double *out)
+{
+    if (!r1_dev || !r2_dev || !out || n < 0) return MFIXGPU_ERR_ARGS;
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    Engine *e = engine_locked(g);
+    if (!e) return MFIXGPU_ERR_CUDA;
+    if (n == 0) {
+        *out = 0.0;
+        return 0;
+    }
+    const int rc = e->dot(r1_dev, r2_dev, n, out);
+    if (rc) g.err = e->last_error();
+    return rc;
+}
+
+int mfixgpu_batch_solve(mfixgpu_system *systems, int nsys, const char *sweep, const char *pc, int precision,
+                        int on_device)
+{
+    if (!systems || nsys < 0 || !sweep || !pc) return MFIXGPU_ERR_ARGS;
+    if (precision != 0 && precision != 1) return MFIXGPU_ERR_ARGS;
+    char s4[4], p4[4];
+    fortran_char4(sweep, 4, s4);
+    fortran_char4(pc, 4, p4);
+    const int pcode = decode_pc(p4);
+    if (pcode < 0) return MFIXGPU_ERR_UNSUPPORTED;
+    if (pcode == PC_LINE && nsys > 1)
+        for (int q = 0; q < 4; ++q) {
+            const char ch = s4[q];
+            if (ch == 'I' || ch == 'i' || ch == 'K' || ch == 'k' || ch == 'A' || ch == 'a')
+                return MFIXGPU_ERR_UNSUPPORTED;
+        }
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    Engine *e = engine_locked(g);
+    if (!e) return MFIXGPU_ERR_CUDA;
+    std::vector<SystemSpec> specs(nsys);
+    for (int q = 0; q < nsys; ++q) {
+        const mfixgpu_system &m = systems[q];
+        SystemSpec &s = specs[q];
+        s.imax2 = m.imax2;
+        s.jmax2 = m.jmax2;
+        s.kmax2 = m.kmax2;
+        s.do_k = m.do_k ? 1 : 0;
+        s.n = m.dimension_3;
+        s.a = m.a_m;
+        s.b = m.b_m;
+        s.x = m.var;
+        s.tol = m.tol;
+        s.itmax = m.itmax;
+    }
+    Options o = g.opt;
+    o.precision = precision;
+    SolveOptions so = make_opts(o, pcode, s4);
+    so.on_device = on_device != 0;
+    std::vector<SolveResult> out;
+    const double t0 = now_s();
+    const int rc = e->solve(specs, so, out);
+    if (rc) {
+        g.err = e->last_error();
+        return rc;
+    }
+    g.last = mfixgpu_stats{};
+    g.last.seconds = now_s() - t0;
+    g.last.device_ms = e->timing().device_ms;
+    g.last.jline_ms = e->timing().jline_ms;
+    g.last.jline_launches = e->timing().jline_launches;
+    g.last.kernel_launches = e->timing().kernel_launches;
+    for (int q = 0; q < nsys; ++q) {
+        systems[q].ier = out[q].ier;
+        systems[q].iterations = out[q].iterations;
+        systems[q].outer_steps = out[q].outer_steps;
+        systems[q].exit_kind = out[q].exit_kind;
+        systems[q].rnorm0 = out[q].rnorm0;
+        systems[q].rnorm = out[q].rnorm;
+    }
+    return 0;
+}
+
+}  // extern "C"

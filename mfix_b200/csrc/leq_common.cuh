@@ -1,0 +1,152 @@
+// leq_common.cuh -- device-side data structures shared by every kernel of the
+// B200 linear-equation path (SOLVE_LIN_EQ -> LEQ_BICGS of MFIX 2016-1).
+//
+// Everything is batch-shaped: a "system" is one A_M(:,:,M) / B_M(:,M) / VAR
+// triple on one box geometry, and every kernel walks a device-resident table of
+// systems.  The single-system drop-in is a batch of one.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+namespace mfixgpu {
+
+// Work vectors of LEQ_BICGS0 (model/leq_bicgs.f:171-176) plus the solution.
+enum VecId : int {
+    V_X = 0,  // VAR (inner correction d in the mixed form)
+    V_R,      // R
+    V_RT,     // Rtilde
+    V_P,      // P
+    V_PH,     // P_preconditioned
+    V_S,      // Svec
+    V_SH,     // Svec_preconditioned
+    V_T,      // Tvec
+    V_V,      // V
+    NVEC
+};
+
+enum PcKind : int { PC_NONE = 0, PC_DIAG = 1, PC_LINE = 2 };
+
+enum Status : int { ST_RUNNING = 0, ST_DONE = 1 };
+enum Phase : int { PH_INNER = 0, PH_OUTER = 1 };
+
+// exit_kind values reported per solve
+enum ExitKind : int {
+    EX_RNORM = 0,     // Rnorm <= TOL*Rnorm0 (model/leq_bicgs.f:455-460)
+    EX_SNORM = 1,     // Snorm <= TOLMIN (:375-395)
+    EX_RHO0 = 2,      // rho == 0 (:320-332)
+    EX_ITMAX = 3,     // loop exhausted (:485-495)
+    EX_SINGULAR = 4,  // zero row during unit scaling (:217-233)
+    EX_ERROR = 5
+};
+
+// Magic-number unsigned division by a runtime constant (round-up method,
+// Granlund & Montgomery 1994): q = (umulhi(n, m) + n) >> l, valid for n < 2^32.
+struct FastDiv {
+    uint32_t d, m, l;
+};
+
+__host__ __device__ inline FastDiv make_fastdiv(uint32_t d)
+{
+    FastDiv f;
+    f.d = d;
+    uint32_t l = 0;
+    while ((1ull << l) < d) ++l;
+    f.l = l;
+    f.m = (uint32_t)(((((uint64_t)1) << 32) * ((((uint64_t)1) << l) - d)) / d + 1);
+    return f;
+}
+
+__device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv &f)
+{
+    return (uint32_t)(((uint64_t)__umulhi(n, f.m) + n) >> f.l);
+}
+
+// One system of the batch.
+struct SysDev {
+    int imax2, jmax2, kmax2, do_k;
+    int64_t n;           // DIMENSION_3 (cells incl. the wall layer)
+    FastDiv div_j;       // division by jmax2
+    FastDiv div_i;       // division by imax2
+    int pc;              // PcKind
+    int ntiles;          // cell tiles of this system
+    int tile_base;       // first tile's slot in the partial-sum array
+    int lane_group;      // G: lanes that share one J-line (power of two <= 32)
+    int rows_per_lane;   // c: rows each lane eliminates (odd; G*c >= jmax2)
+    int half_lines;      // ceil(imax2/2): parity-wave slots per k row
+    double *a64;         // 7*n diagonals, Fortran A_M(DIMENSION_3,-3:3) order
+    double *b64;         // B_M(:,M)
+    double *x64[2];      // VAR (x64[1] is the ping-pong buffer of the mixed form)
+    float *a32;          // FP32 copy of the scaled diagonals (mixed form)
+    void *vec[NVEC];     // work vectors, double or float by precision
+};
+
+// Per-system solver state, device resident; the scalars of LEQ_BICGS0 plus
+// the bookkeeping the reference keeps in locals and ITER_TOT.
+struct SysState {
+    double rho, rho_prev, alpha, omega, beta;
+    double rnorm0, rnorm, snorm;
+    double tol;           // TOL
+    double outer_rnorm0;  // mixed form: ||b - A x0|| in FP64
+    double outer_rnorm;   // mixed form: latest FP64 true residual
+    double inner_tol;     // mixed form: relative drop asked of each inner solve
+    int itmax;
+    int i;                // reference loop index of the next iteration (1-based)
+    int iter;             // reference ITER counter
+    int status;           // Status
+    int ier;
+    int exit_kind;
+    int iter_tot_add;
+    int snorm_exit;
+    int phase;            // Phase
+    int outer_steps;
+    int inner_total;      // inner iterations summed over outer steps
+    int inner_first;      // first inner iteration after an outer step
+    int xcur;             // mixed form: which x64 buffer holds VAR
+    int line_skips;       // J-lines left unchanged because DGTSV reported INFO != 0
+    int line_fallbacks;   // J-lines solved by the sequential pivoting path
+    int err;
+    unsigned int arrivals;  // tiles that finished the current reduction kernel
+    int pad;
+};
+
+// One cell tile: TILE consecutive cells of one system.
+struct Tile {
+    int sys;
+    int idx;  // tile index within the system
+};
+
+constexpr int TILE_CELLS = 8192;
+constexpr int CELL_THREADS = 256;
+constexpr int LINE_WARPS = 4;  // warps per block of the J-line kernel
+
+// Ordered parameters of one J-line half-sweep (a "wave").
+struct WaveArgs {
+    int kind;        // 0: lines with ((i + k) & 1) == par, 1: lines with i + k == diag, 2: single line list
+    int par;         // parity or diagonal index
+    int rhs, nbr, old, dst;  // VecId of the right-hand side, neighbour source, own-old source, output
+    int write_old;   // lines skipped on INFO != 0 copy their old value into dst
+    int gate;        // which systems take part (see gate_ok)
+    int count;       // kinds 1 and 2 (single system): work items in the wave
+    int nlines;      // kind 2: lines in `list`
+    const int2 *list;  // kind 2: (i, k) of each line, 1-based
+};
+
+enum Gate : int {
+    G_INNER = 0,        // running, inner phase
+    G_INNER_NOSNORM = 1,// running, inner phase, no Snorm exit this iteration
+    G_OUTER = 2,        // running, outer phase
+    G_ANY = 3           // running
+};
+
+__device__ __forceinline__ bool gate_ok(const SysState &s, int gate)
+{
+    if (s.status != ST_RUNNING) return false;
+    switch (gate) {
+    case G_INNER: return s.phase == PH_INNER;
+    case G_INNER_NOSNORM: return s.phase == PH_INNER && !s.snorm_exit;
+    case G_OUTER: return s.phase == PH_OUTER;
+    default: return true;
+    }
+}
+
+}  // namespace mfixgpu

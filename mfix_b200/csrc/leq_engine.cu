@@ -1,0 +1,734 @@
+// leq_engine.cu -- host engine of the B200 LEQ_BICGS path.
+//
+// One Engine per device: an arena of device memory grown on demand and reused
+// across calls (the reference allocates and frees its eight work vectors inside
+// every call, model/leq_bicgs.f:238-245, 499-506), one stream, batch tables.
+// The iteration body is a fixed sequence of kernels that read every scalar from
+// device memory, so it is captured once per solve into a CUDA graph and replayed;
+// the host reads the per-system state back every few iterations, double
+// buffered, to stop once every system is done.
+#include "leq_engine.h"
+
+#include <algorithm>
+#include <cstring>
+#include <map>
+
+namespace mfixgpu {
+
+#define CK(call)                                                                  \
+    do {                                                                          \
+        cudaError_t e_ = (call);                                                  \
+        if (e_ != cudaSuccess) return fail(std::string(#call) + ": " + cudaGetErrorString(e_), -13); \
+    } while (0)
+
+static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+void line_shape(int L, int *G, int *c)
+{
+    int g = 1;
+    while (g * 2 <= 32 && g * 4 <= L) g *= 2;
+    int cc = (L + g - 1) / g;
+    if (cc < 3) cc = 3;
+    if ((cc & 1) == 0) ++cc;
+    *G = g;
+    *c = cc;
+}
+
+void *DeviceArena::take(size_t bytes)
+{
+    const size_t off = align_up(used, 256);
+    if (off + bytes > cap) return nullptr;
+    used = off + bytes;
+    return base + off;
+}
+
+cudaError_t DeviceArena::reserve(size_t bytes)
+{
+    if (bytes <= cap) return cudaSuccess;
+    if (base) cudaFree(base);
+    base = nullptr;
+    cap = 0;
+    const size_t want = align_up(bytes + bytes / 8, 1 << 20);
+    cudaError_t e = cudaMalloc((void **)&base, want);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        e = cudaMalloc((void **)&base, bytes);
+        if (e != cudaSuccess) return e;
+        cap = bytes;
+        return cudaSuccess;
+    }
+    cap = want;
+    return cudaSuccess;
+}
+
+void DeviceArena::release()
+{
+    if (base) cudaFree(base);
+    base = nullptr;
+    cap = used = 0;
+}
+
+Engine::Engine()
+{
+    cudaGetDevice(&dev_);
+    cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev_);
+    cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&ev_a_, cudaEventDisableTiming);
+    cudaEventCreateWithFlags(&ev_b_, cudaEventDisableTiming);
+    cudaEventCreate(&ev_t0_);
+    cudaEventCreate(&ev_t1_);
+    cell_bpsm_ = cell_blocks_per_sm();
+}
+
+Engine::~Engine()
+{
+    if (stream_) cudaStreamSynchronize(stream_);
+    arena_.release();
+    cudaFree(d_sys_);
+    cudaFree(d_st_);
+    cudaFree(d_tiles_);
+    cudaFree(d_prefix_);
+    cudaFree(d_partials_);
+    cudaFree(d_lines_);
+    cudaFree(d_seq_scratch_);
+    cudaFree(d_one_sys_);
+    cudaFree(d_dot_partials_);
+    cudaFree(d_dot_counter_);
+    cudaFree(d_dot_out_);
+    if (h_st_pinned_) cudaFreeHost(h_st_pinned_);
+    if (ev_a_) cudaEventDestroy(ev_a_);
+    if (ev_b_) cudaEventDestroy(ev_b_);
+    if (ev_t0_) cudaEventDestroy(ev_t0_);
+    if (ev_t1_) cudaEventDestroy(ev_t1_);
+    for (auto &e : jt_ev_)
+        if (e) cudaEventDestroy(e);
+    if (stream_) cudaStreamDestroy(stream_);
+}
+
+int Engine::fail(const std::string &msg, int code)
+{
+    err_ = msg;
+    return code;
+}
+
+template <typename T>
+static cudaError_t upload(T **dptr, size_t *cap_elems, const T *src, size_t n, cudaStream_t s)
+{
+    if (n > *cap_elems || *dptr == nullptr) {
+        if (*dptr) cudaFree(*dptr);
+        *dptr = nullptr;
+        const size_t want = std::max<size_t>(n, 16);
+        cudaError_t e = cudaMalloc((void **)dptr, want * sizeof(T));
+        if (e != cudaSuccess) return e;
+        *cap_elems = want;
+    }
+    if (n == 0) return cudaSuccess;
+    return cudaMemcpyAsync(*dptr, src, n * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+// ------------------------------------------------------------------ batch setup
+int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions &opt)
+{
+    nsys_ = (int)specs.size();
+    const bool mixed = opt.precision == PREC_MIXED;
+    const size_t ew = mixed ? sizeof(float) : sizeof(double);
+
+    // memory plan
+    size_t bytes = 0;
+    for (const auto &s : specs) {
+        const size_t n = (size_t)s.n;
+        if (!opt.on_device) bytes += align_up(7 * n * 8, 256) + 2 * align_up(n * 8, 256);
+        if (mixed) bytes += align_up(n * 8, 256) + align_up(7 * n * 4, 256);
+        bytes += NVEC * align_up(n * ew, 256);
+    }
+    bytes += 4096;
+    cudaError_t e = arena_.reserve(bytes);
+    if (e != cudaSuccess) return fail(std::string("device memory for the batch: ") + cudaGetErrorString(e), -11);
+    arena_.reset();
+
+    h_sys_.assign(nsys_, SysDev{});
+    h_st_.assign(nsys_, SysState{});
+    h_tiles_.clear();
+    h_prefix_.assign(nsys_ + 1, 0);
+    int cmax = 3;
+    int tile_base = 0;
+    for (int s = 0; s < nsys_; ++s) {
+        const SystemSpec &sp = specs[s];
+        SysDev &d = h_sys_[s];
+        d.imax2 = sp.imax2;
+        d.jmax2 = sp.jmax2;
+        d.kmax2 = sp.kmax2;
+        d.do_k = sp.do_k;
+        d.n = sp.n;
+        d.div_j = make_fastdiv((uint32_t)sp.jmax2);
+        d.div_i = make_fastdiv((uint32_t)sp.imax2);
+        d.pc = opt.pc;
+        d.ntiles = (int)((sp.n + TILE_CELLS - 1) / TILE_CELLS);
+        d.tile_base = tile_base;
+        tile_base += d.ntiles;
+        line_shape(sp.jmax2, &d.lane_group, &d.rows_per_lane);
+        cmax = std::max(cmax, d.rows_per_lane);
+        d.half_lines = (sp.imax2 + 1) / 2;
+        const size_t n = (size_t)sp.n;
+        if (opt.on_device) {
+            d.a64 = sp.a;
+            d.b64 = sp.b;
+            d.x64[0] = sp.x;
+        } else {
+            d.a64 = (double *)arena_.take(7 * n * 8);
+            d.b64 = (double *)arena_.take(n * 8);
+            d.x64[0] = (double *)arena_.take(n * 8);
+        }
+        if (mixed) {
+            d.x64[1] = (double *)arena_.take(n * 8);
+            d.a32 = (float *)arena_.take(7 * n * 4);
+        }
+        for (int v = 0; v < NVEC; ++v) d.vec[v] = arena_.take(n * ew);
+        if (!mixed) d.vec[V_X] = d.x64[0];
+        for (int t = 0; t < d.ntiles; ++t) h_tiles_.push_back(Tile{s, t});
+        const int lpw = 32 / d.lane_group;
+        const int64_t slots = (int64_t)d.half_lines * sp.kmax2;
+        h_prefix_[s + 1] = h_prefix_[s] + (int)((slots + lpw - 1) / lpw);
+
+        SysState &st = h_st_[s];
+        st.tol = sp.tol;
+        st.itmax = sp.itmax;
+        st.status = ST_RUNNING;
+        st.phase = mixed ? PH_OUTER : PH_INNER;
+        st.inner_tol = opt.inner_tol;
+        st.i = 1;
+        st.iter = 1;
+    }
+
+    // host -> device copies of the systems
+    if (!opt.on_device) {
+        for (int s = 0; s < nsys_; ++s) {
+            const SystemSpec &sp = specs[s];
+            const size_t n = (size_t)sp.n;
+            CK(cudaMemcpyAsync(h_sys_[s].a64, sp.a, 7 * n * 8, cudaMemcpyHostToDevice, stream_));
+            CK(cudaMemcpyAsync(h_sys_[s].b64, sp.b, n * 8, cudaMemcpyHostToDevice, stream_));
+            CK(cudaMemcpyAsync(h_sys_[s].x64[0], sp.x, n * 8, cudaMemcpyHostToDevice, stream_));
+        }
+    }
+
+    // tables are small; their device copies are reallocated only when they grow
+    CK(upload(&d_sys_, &sys_cap_, h_sys_.data(), h_sys_.size(), stream_));
+    CK(upload(&d_st_, &st_cap_, h_st_.data(), h_st_.size(), stream_));
+    CK(upload(&d_tiles_, &tiles_cap_, h_tiles_.data(), h_tiles_.size(), stream_));
+    CK(upload(&d_prefix_, &prefix_cap_, h_prefix_.data(), h_prefix_.size(), stream_));
+    const size_t need_part = 2 * (size_t)std::max(tile_base, 1);
+    if (need_part > part_cap_) {
+        cudaFree(d_partials_);
+        d_partials_ = nullptr;
+        CK(cudaMalloc((void **)&d_partials_, need_part * sizeof(double)));
+        part_cap_ = need_part;
+    }
+    if ((size_t)nsys_ * 2 > h_st_pinned_cap_) {
+        if (h_st_pinned_) cudaFreeHost(h_st_pinned_);
+        h_st_pinned_ = nullptr;
+        CK(cudaMallocHost((void **)&h_st_pinned_, sizeof(SysState) * 2 * (size_t)nsys_));
+        h_st_pinned_cap_ = 2 * (size_t)nsys_;
+    }
+
+    view_.sys = d_sys_;
+    view_.st = d_st_;
+    view_.tiles = d_tiles_;
+    view_.ntiles = (int)h_tiles_.size();
+    view_.nsys = nsys_;
+    view_.line_prefix = d_prefix_;
+    view_.partials = d_partials_;
+
+    cfg_.stream = stream_;
+    cfg_.line_cmax = cmax;
+    cfg_.cell_grid = std::max(1, std::min(view_.ntiles, sms_ * cell_bpsm_));
+    const int bpsm = mixed ? prepare_line_kernel<float>(cmax) : prepare_line_kernel<double>(cmax);
+    if (bpsm <= 0) return fail("J-line kernel does not fit on the device (shared memory)", -11);
+    const int items = h_prefix_[nsys_];
+    cfg_.line_grid = std::max(1, std::min((items + LINE_WARPS - 1) / LINE_WARPS, sms_ * bpsm));
+    return 0;
+}
+
+// ------------------------------------------------------------------ LINE preconditioner plan
+// LEQ_MSOLVE (model/leqsol_mod.f:286-598) as a list of device steps.  Var = B
+// (SETGUESS) is folded into the first red/black pass when the first active
+// letter is 'R': its first wave reads neighbours and old values from B, its
+// second wave reads its own old values from B.
+int Engine::plan_msolve(const SolveOptions &opt, int src, int dst, int gate, int which)
+{
+    plan_[which].clear();
+    if (opt.pc == PC_NONE) return 0;
+    if (opt.pc == PC_DIAG) {
+        Step st{};
+        st.type = 3;
+        st.w.rhs = src;
+        st.w.dst = dst;
+        st.w.gate = gate;
+        plan_[which].push_back(st);
+        return 0;
+    }
+    const SysDev &d0 = h_sys_[0];
+    const bool single = nsys_ == 1;
+    auto letter = [&](char ch) -> int {
+        if (ch == 'R' || ch == 'r') return 'R';
+        if (ch == 'I' || ch == 'i') return 'I';
+        if (ch == 'K' || ch == 'k') return 'K';
+        if (ch == 'A' || ch == 'a') return 'A';
+        return 0;
+    };
+    int first = 0;
+    for (int q = 0; q < 4 && !first; ++q) {
+        const int L = letter(opt.sweep[q]);
+        if (!L) continue;
+        if (!d0.do_k && (L == 'A' || L == 'K')) continue;  // no-ops in the 2-D branch
+        first = L;
+    }
+    if (!first) {
+        Step cp{};
+        cp.type = 1;
+        cp.w.rhs = src;
+        cp.w.dst = dst;
+        cp.w.gate = gate;
+        plan_[which].push_back(cp);
+        return 0;
+    }
+    bool fused_guess = (first == 'R');
+    if (!fused_guess) {
+        Step cp{};
+        cp.type = 1;
+        cp.w.rhs = src;
+        cp.w.dst = dst;
+        cp.w.gate = gate;
+        plan_[which].push_back(cp);
+    }
+    int waves_done = 0;
+    auto wave = [&](int kind, int par, int count, const int2 *list, int nlines) {
+        Step st{};
+        st.type = 0;
+        WaveArgs &w = st.w;
+        w.kind = kind;
+        w.par = par;
+        w.rhs = src;
+        w.dst = dst;
+        w.gate = gate;
+        w.count = count;
+        w.list = list;
+        w.nlines = nlines;
+        if (fused_guess && waves_done == 0) {
+            w.nbr = src;
+            w.old = src;
+            w.write_old = 1;
+        } else if (fused_guess && waves_done == 1) {
+            w.nbr = dst;
+            w.old = src;
+            w.write_old = 1;
+        } else {
+            w.nbr = dst;
+            w.old = dst;
+            w.write_old = 0;
+        }
+        ++waves_done;
+        plan_[which].push_back(st);
+    };
+    std::vector<std::pair<size_t, size_t>> list_refs;  // (plan index, offset into h_lines_) for kind 2 / seq
+    for (int q = 0; q < 4; ++q) {
+        const int L = letter(opt.sweep[q]);
+        if (!L) continue;
+        if (!d0.do_k) {
+            if (L == 'R') {  // :382-391, i odd then i even
+                wave(0, 0, 0, nullptr, 0);
+                wave(0, 1, 0, nullptr, 0);
+            } else if (L == 'I') {  // :374-379, i = 1..imax2 in order
+                if (!single) return fail("sweep letter 'I' is served for single-system solves only", -10);
+                for (int dgl = 2; dgl <= d0.imax2 + 1; ++dgl) wave(1, dgl, 1, nullptr, 0);
+            }
+            continue;
+        }
+        if (L == 'R') {  // :497-522, (i+k) odd first
+            wave(0, 1, 0, nullptr, 0);
+            wave(0, 0, 0, nullptr, 0);
+        } else if (L == 'I' || L == 'K') {
+            // :567-582: lexicographic line Gauss-Seidel; both orders give the same
+            // result, and the lines of one anti-diagonal i+k = const are independent.
+            if (!single) return fail("sweep letters 'I'/'K' are served for single-system solves only", -10);
+            const int lpw = 32 / d0.lane_group;
+            for (int dgl = 2; dgl <= d0.imax2 + d0.kmax2; ++dgl) {
+                const int ilo = std::max(1, dgl - d0.kmax2), ihi = std::min(d0.imax2, dgl - 1);
+                const int cnt = ihi - ilo + 1;
+                wave(1, dgl, (cnt + lpw - 1) / lpw, nullptr, 0);
+            }
+        } else if (L == 'A') {
+            if (!single) return fail("sweep letter 'A' is served for single-system solves only", -10);
+            // :398-470: JK, IJ then IK loops, each sequential in the reference.  Lines are
+            // grouped into levels so that every line sees exactly the neighbour values
+            // it sees in the reference order.
+            const int isize = d0.imax2, jsize = d0.jmax2, ksize = d0.kmax2;
+            for (int part = 0; part < 3; ++part) {
+                // part 0: I-lines at (j,k); part 1: K-lines at (i,j); part 2: J-lines at (i,k)
+                const int n1 = part == 0 ? jsize : isize;   // fast coordinate of the line
+                const int n2 = part == 1 ? jsize : ksize;   // slow coordinate
+                std::vector<int2> order;
+                for (int icase = 1; icase <= 2; ++icase)
+                    for (int m = icase; m <= n1 * n2; m += 2) {
+                        int b2 = (m % n1 != 0) ? m / n1 + 1 : m / n1;
+                        int b1 = (m - 1 - (b2 - 1) * n1) + 1 + (b2 % 2);
+                        if (b1 > n1) b1 = b1 - n1;
+                        order.push_back(make_int2(b1, b2));
+                    }
+                std::vector<int> level((size_t)n1 * n2, 0);
+                int maxlev = 0;
+                std::vector<int> lev_of(order.size());
+                for (size_t t = 0; t < order.size(); ++t) {
+                    const int b1 = order[t].x, b2 = order[t].y;
+                    int lv = 0;
+                    const int nb[4][2] = {{b1 - 1, b2}, {b1 + 1, b2}, {b1, b2 - 1}, {b1, b2 + 1}};
+                    for (auto &p : nb)
+                        if (p[0] >= 1 && p[0] <= n1 && p[1] >= 1 && p[1] <= n2)
+                            lv = std::max(lv, level[(size_t)(p[1] - 1) * n1 + (p[0] - 1)]);
+                    level[(size_t)(b2 - 1) * n1 + (b1 - 1)] = lv + 1;
+                    lev_of[t] = lv + 1;
+                    maxlev = std::max(maxlev, lv + 1);
+                }
+                for (int lv = 1; lv <= maxlev; ++lv) {
+                    const size_t off = h_lines_.size();
+                    for (size_t t = 0; t < order.size(); ++t)
+                        if (lev_of[t] == lv) h_lines_.push_back(order[t]);
+                    const int cnt = (int)(h_lines_.size() - off);
+                    if (part == 2) {
+                        const int lpw = 32 / d0.lane_group;
+                        wave(2, 0, (cnt + lpw - 1) / lpw, nullptr, cnt);
+                    } else {
+                        Step st{};
+                        st.type = 2;
+                        st.s.axis = part == 0 ? 0 : 2;
+                        st.s.count = cnt;
+                        st.s.rhs = src;
+                        st.s.var = dst;
+                        st.s.fatal_on_info = 1;
+                        st.s.lmax = std::max(d0.imax2, d0.kmax2);
+                        if (!fused_guess || waves_done >= 2) {
+                            plan_[which].push_back(st);
+                        } else {
+                            return fail("internal: ASAS after a fused first pass", -13);
+                        }
+                    }
+                    list_refs.push_back({plan_[which].size() - 1, off});
+                }
+            }
+        }
+    }
+    for (auto &r : list_refs) list_refs_.push_back({which, r.first, r.second});
+    return 0;
+}
+
+// Line lists of both plans go to the device in one upload, after both plans exist.
+int Engine::bind_lists()
+{
+    if (list_refs_.empty()) return 0;
+    size_t cap = d_lines_cap_;
+    cudaError_t e = upload(&d_lines_, &cap, h_lines_.data(), h_lines_.size(), stream_);
+    if (e != cudaSuccess) return fail(cudaGetErrorString(e), -13);
+    d_lines_cap_ = cap;
+    size_t scratch_need = 0;
+    for (auto &r : list_refs_) {
+        Step &st = plan_[r.which][r.index];
+        if (st.type == 0) st.w.list = d_lines_ + r.offset;
+        if (st.type == 2) {
+            st.s.lines = d_lines_ + r.offset;
+            scratch_need = std::max(scratch_need, (size_t)4 * st.s.lmax * st.s.count);
+        }
+    }
+    if (scratch_need > d_seq_scratch_cap_) {
+        cudaFree(d_seq_scratch_);
+        d_seq_scratch_ = nullptr;
+        e = cudaMalloc((void **)&d_seq_scratch_, scratch_need * sizeof(double));
+        if (e != cudaSuccess) return fail(cudaGetErrorString(e), -11);
+        d_seq_scratch_cap_ = scratch_need;
+    }
+    for (auto &r : list_refs_) {
+        Step &st = plan_[r.which][r.index];
+        if (st.type == 2) st.s.scratch = d_seq_scratch_;
+    }
+    return 0;
+}
+
+int Engine::run_msolve_plan(int which, int elem)
+{
+    for (const Step &st : plan_[which]) {
+        cudaError_t e = cudaSuccess;
+        if (st.type == 0) {
+            if (jline_timing_) cudaEventRecord(jt_ev_[2 * (jline_count_ % JT_EVENTS)], stream_);
+            e = (elem == 8) ? launch_jline<double>(view_, cfg_, st.w) : launch_jline<float>(view_, cfg_, st.w);
+            if (jline_timing_) {
+                cudaEventRecord(jt_ev_[2 * (jline_count_ % JT_EVENTS) + 1], stream_);
+                ++jline_count_;
+            }
+        } else if (st.type == 1) {
+            e = (elem == 8) ? launch_copy<double>(view_, cfg_, st.w.rhs, st.w.dst, st.w.gate)
+                            : launch_copy<float>(view_, cfg_, st.w.rhs, st.w.dst, st.w.gate);
+        } else if (st.type == 2) {
+            e = (elem == 8) ? launch_seq_lines<double>(view_, st.s, stream_) : launch_seq_lines<float>(view_, st.s, stream_);
+        } else if (st.type == 3) {
+            e = (elem == 8) ? launch_diag<double>(view_, cfg_, st.w.rhs, st.w.dst, st.w.gate)
+                            : launch_diag<float>(view_, cfg_, st.w.rhs, st.w.dst, st.w.gate);
+        }
+        if (e != cudaSuccess) return fail(std::string("sweep launch: ") + cudaGetErrorString(e), -13);
+        ++launches_;
+    }
+    return 0;
+}
+
+// ------------------------------------------------------------------ solve
+int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt, std::vector<SolveResult> &out)
+{
+    err_.clear();
+    out.assign(specs.size(), SolveResult{});
+    if (specs.empty()) return 0;
+    for (const auto &s : specs) {
+        if (s.imax2 < 1 || s.jmax2 < 1 || s.kmax2 < 1) return fail("grid extents must be >= 1", -14);
+        if (!s.do_k && s.kmax2 != 1) return fail("a 2-D system (do_k = 0) needs kmax2 = 1", -14);
+        if ((int64_t)s.imax2 * s.jmax2 * s.kmax2 != s.n) return fail("DIMENSION_3 != IMAX2*JMAX2*KMAX2", -14);
+        if (s.n > (int64_t)INT32_MAX - TILE_CELLS) return fail("system too large for 32-bit cell indexing", -14);
+        if (!s.a || !s.b || !s.x) return fail("null array", -14);
+    }
+    if (opt.pc != PC_LINE && opt.pc != PC_DIAG && opt.pc != PC_NONE) return fail("unknown preconditioner", -10);
+    const bool mixed = opt.precision == PREC_MIXED;
+    const int elem = mixed ? 4 : 8;
+
+    int rc = setup_batch(specs, opt);
+    if (rc) return rc;
+    const int gate_p = G_INNER, gate_s = G_INNER_NOSNORM;
+    const int src_ph = opt.pc == PC_NONE ? V_P : V_PH;
+    const int src_sh = opt.pc == PC_NONE ? V_S : V_SH;
+    h_lines_.clear();
+    list_refs_.clear();
+    if ((rc = plan_msolve(opt, V_P, V_PH, gate_p, 0))) return rc;
+    if ((rc = plan_msolve(opt, V_S, V_SH, gate_s, 1))) return rc;
+    if ((rc = bind_lists())) return rc;
+
+    jline_timing_ = opt.time_kernels;
+    jline_count_ = 0;
+    launches_ = 0;
+    timing_ = SolveTiming{};
+    if (jline_timing_ && !jt_ev_[0])
+        for (int q = 0; q < 2 * JT_EVENTS; ++q) cudaEventCreate(&jt_ev_[q]);
+    CK(cudaEventRecord(ev_t0_, stream_));
+
+    // ---- setup
+    CK(launch_scale(view_, cfg_));
+    CK(launch_after_scale(view_, cfg_));
+    launches_ += 2;
+    if (mixed) {
+        CK(launch_to_f32(view_, cfg_));
+        launches_ += 1;
+    } else {
+        CK(launch_init_residual<double>(view_, cfg_));
+        CK(launch_init_rtilde<double>(view_, cfg_, opt.seed));
+        launches_ += 2;
+    }
+
+    // ---- iteration body (kernels of this library: 6 or 5 plus the sweep plans)
+    auto body = [&]() -> int {
+        int r;
+        launches_ += mixed ? 6 : 5;
+        if (mixed) {
+            CK(launch_outer_step(view_, cfg_));
+            CK((launch_p_update<float, true>(view_, cfg_)));
+            if ((r = run_msolve_plan(0, 4))) return r;
+            CK((launch_matvec_alpha<float, true>(view_, cfg_, src_ph)));
+            CK((launch_s_update<float, true>(view_, cfg_)));
+            if ((r = run_msolve_plan(1, 4))) return r;
+            CK((launch_matvec_omega<float, true>(view_, cfg_, src_sh)));
+            CK((launch_xr_update<float, true>(view_, cfg_, src_ph, src_sh)));
+        } else {
+            CK((launch_p_update<double, false>(view_, cfg_)));
+            if ((r = run_msolve_plan(0, 8))) return r;
+            CK((launch_matvec_alpha<double, false>(view_, cfg_, src_ph)));
+            CK((launch_s_update<double, false>(view_, cfg_)));
+            if ((r = run_msolve_plan(1, 8))) return r;
+            CK((launch_matvec_omega<double, false>(view_, cfg_, src_sh)));
+            CK((launch_xr_update<double, false>(view_, cfg_, src_ph, src_sh)));
+        }
+        return 0;
+    };
+
+    int max_itmax = 0;
+    for (const auto &s : specs) max_itmax = std::max(max_itmax, s.itmax);
+    const int max_loops = std::max(1, max_itmax + 2);
+    const bool graph = opt.use_graph && !jline_timing_;
+    cudaGraphExec_t gexec = nullptr;
+    long long per_body = 0;
+    if (graph) {
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        const long long before = launches_;
+        rc = body();
+        per_body = launches_ - before;
+        launches_ = before;
+        cudaError_t ce = cudaStreamEndCapture(stream_, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ce != cudaSuccess) return fail(std::string("graph capture: ") + cudaGetErrorString(ce), -13);
+        ce = cudaGraphInstantiate(&gexec, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) return fail(std::string("graph instantiate: ") + cudaGetErrorString(ce), -13);
+    }
+    auto run_once = [&]() -> int {
+        if (graph) {
+            CK(cudaGraphLaunch(gexec, stream_));
+            launches_ += per_body;
+            return 0;
+        }
+        return body();
+    };
+
+    const int K = std::max(1, opt.check_every);
+    int loops = 0, snap = 0;
+    bool have_prev = false, finished = false;
+    while (loops < max_loops && !finished) {
+        for (int q = 0; q < K && loops < max_loops; ++q, ++loops)
+            if ((rc = run_once())) {
+                if (gexec) cudaGraphExecDestroy(gexec);
+                return rc;
+            }
+        SysState *buf = h_st_pinned_ + (size_t)(snap & 1) * nsys_;
+        CK(cudaMemcpyAsync(buf, d_st_, sizeof(SysState) * nsys_, cudaMemcpyDeviceToHost, stream_));
+        CK(cudaEventRecord((snap & 1) ? ev_b_ : ev_a_, stream_));
+        if (have_prev) {
+            const int prev = (snap - 1) & 1;
+            CK(cudaEventSynchronize(prev ? ev_b_ : ev_a_));
+            const SysState *pb = h_st_pinned_ + (size_t)prev * nsys_;
+            finished = true;
+            for (int s = 0; s < nsys_; ++s)
+                if (pb[s].status == ST_RUNNING) {
+                    finished = false;
+                    break;
+                }
+        }
+        have_prev = true;
+        ++snap;
+    }
+    if (gexec) cudaGraphExecDestroy(gexec);
+    CK(cudaEventRecord(ev_t1_, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpy(h_st_.data(), d_st_, sizeof(SysState) * nsys_, cudaMemcpyDeviceToHost));
+    cudaEventElapsedTime(&timing_.device_ms, ev_t0_, ev_t1_);
+    timing_.kernel_launches = launches_;
+
+    // ---- results back
+    for (int s = 0; s < nsys_; ++s) {
+        const SysState &st = h_st_[s];
+        SolveResult &r = out[s];
+        r.ier = st.ier;
+        r.iterations = mixed ? st.inner_total : st.iter;
+        r.iter_tot_add = st.iter_tot_add;
+        r.exit_kind = st.exit_kind;
+        r.line_skips = st.line_skips;
+        r.line_fallbacks = st.line_fallbacks;
+        r.outer_steps = st.outer_steps;
+        r.rnorm0 = mixed ? st.outer_rnorm0 : st.rnorm0;
+        r.rnorm = mixed ? st.outer_rnorm : st.rnorm;
+        if (st.status != ST_DONE) {
+            r.ier = -15;
+            r.exit_kind = EX_ERROR;
+        }
+        if (st.err & 2) {
+            r.ier = -12;  // DGTSV INFO != 0 inside a JK/IJ sweep (the reference stops there)
+            r.exit_kind = EX_ERROR;
+        }
+        const SysDev &d = h_sys_[s];
+        const SystemSpec &sp = specs[s];
+        const size_t n = (size_t)sp.n;
+        const double *xsrc = mixed ? d.x64[st.xcur] : d.x64[0];
+        if (opt.on_device) {
+            if (xsrc != sp.x) CK(cudaMemcpyAsync(sp.x, xsrc, n * 8, cudaMemcpyDeviceToDevice, stream_));
+        } else {
+            CK(cudaMemcpyAsync(sp.x, xsrc, n * 8, cudaMemcpyDeviceToHost, stream_));
+            if (opt.write_back_ab) {
+                CK(cudaMemcpyAsync(sp.a, d.a64, 7 * n * 8, cudaMemcpyDeviceToHost, stream_));
+                CK(cudaMemcpyAsync(sp.b, d.b64, n * 8, cudaMemcpyDeviceToHost, stream_));
+            }
+        }
+    }
+    CK(cudaStreamSynchronize(stream_));
+    if (jline_timing_) {
+        float js = 0.f;
+        const int nrec = std::min(jline_count_, JT_EVENTS);
+        for (int q = 0; q < nrec; ++q) {
+            float ms = 0.f;
+            cudaEventElapsedTime(&ms, jt_ev_[2 * q], jt_ev_[2 * q + 1]);
+            js += ms;
+        }
+        timing_.jline_ms = js;
+        timing_.jline_launches = nrec;
+        jline_timing_ = false;
+    }
+    return 0;
+}
+
+// ------------------------------------------------------------------ per-routine entry points
+int Engine::matvec(const SystemSpec &g, const double *a, const double *x, double *y)
+{
+    SysDev d{};
+    d.imax2 = g.imax2;
+    d.jmax2 = g.jmax2;
+    d.kmax2 = g.kmax2;
+    d.do_k = g.do_k;
+    d.n = g.n;
+    d.div_j = make_fastdiv((uint32_t)g.jmax2);
+    d.div_i = make_fastdiv((uint32_t)g.imax2);
+    if (!d_one_sys_) CK(cudaMalloc((void **)&d_one_sys_, sizeof(SysDev)));
+    CK(cudaMemcpyAsync(d_one_sys_, &d, sizeof(SysDev), cudaMemcpyHostToDevice, stream_));
+    const int grid = std::max(1, std::min((int)((g.n + CELL_THREADS - 1) / CELL_THREADS), sms_ * 8));
+    CK(launch_matvec_plain<double>(d_one_sys_, d, a, x, y, stream_, grid));
+    CK(cudaStreamSynchronize(stream_));
+    return 0;
+}
+
+int Engine::dot(const double *x, const double *y, int64_t n, double *out_host)
+{
+    const int grid = std::max(1, std::min((int)((n + 4095) / 4096), sms_ * 4));
+    if (!d_dot_partials_) {
+        CK(cudaMalloc((void **)&d_dot_partials_, sizeof(double) * (size_t)sms_ * 4));
+        CK(cudaMalloc((void **)&d_dot_counter_, sizeof(unsigned int)));
+        CK(cudaMalloc((void **)&d_dot_out_, sizeof(double)));
+        CK(cudaMemsetAsync(d_dot_counter_, 0, sizeof(unsigned int), stream_));
+    }
+    CK(launch_dot(x, y, n, d_dot_partials_, d_dot_counter_, d_dot_out_, grid, stream_));
+    CK(cudaMemcpyAsync(out_host, d_dot_out_, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    return 0;
+}
+
+// One LEQ_MSOLVE on device arrays: var = M^{-1} b (the J-line kernels run over a
+// one-system batch whose P / P_preconditioned slots point at b / var).
+int Engine::msolve(const SystemSpec &g, const double *a, const double *b, double *var, int pc, const char sweep[4])
+{
+    SolveOptions opt;
+    opt.pc = pc;
+    std::memcpy(opt.sweep, sweep, 4);
+    opt.on_device = true;
+    SystemSpec s = g;
+    s.a = const_cast<double *>(a);
+    s.b = const_cast<double *>(b);
+    s.x = var;
+    std::vector<SystemSpec> one{s};
+    int rc = setup_batch(one, opt);
+    if (rc) return rc;
+    h_sys_[0].vec[V_P] = const_cast<double *>(b);
+    h_sys_[0].vec[V_PH] = var;
+    CK(cudaMemcpyAsync(d_sys_, h_sys_.data(), sizeof(SysDev), cudaMemcpyHostToDevice, stream_));
+    h_lines_.clear();
+    list_refs_.clear();
+    if ((rc = plan_msolve(opt, V_P, V_PH, G_ANY, 0))) return rc;
+    if ((rc = bind_lists())) return rc;
+    if (pc == PC_NONE) CK(cudaMemcpyAsync(var, b, (size_t)g.n * 8, cudaMemcpyDeviceToDevice, stream_));
+    if ((rc = run_msolve_plan(0, 8))) return rc;
+    CK(cudaStreamSynchronize(stream_));
+    CK(cudaMemcpy(h_st_.data(), d_st_, sizeof(SysState), cudaMemcpyDeviceToHost));
+    if (h_st_[0].err & 2) return fail("DGTSV reported INFO != 0 in a JK/IJ sweep", -12);
+    return 0;
+}
+
+}  // namespace mfixgpu

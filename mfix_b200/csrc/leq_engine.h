@@ -1,0 +1,151 @@
+// leq_engine.h -- host-side solver engine: batches of MFIX 7-point systems,
+// device-resident state, the BiCGSTAB iteration schedule (FP64 drop-in and the
+// FP32-inner / FP64-refinement form) and the LINE-preconditioner sweep plan.
+#pragma once
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include "leq_common.cuh"
+#include "leq_kernels.cuh"
+
+namespace mfixgpu {
+
+enum Precision : int { PREC_FP64 = 0, PREC_MIXED = 1 };
+
+// One system to solve.  Pointers are host or device memory as the call says.
+struct SystemSpec {
+    int imax2 = 0, jmax2 = 0, kmax2 = 0, do_k = 1;
+    int64_t n = 0;
+    double *a = nullptr;  // 7*n, A_M(DIMENSION_3,-3:3) layout
+    double *b = nullptr;  // n
+    double *x = nullptr;  // n, initial guess in / solution out
+    double tol = 1e-8;
+    int itmax = 500;
+};
+
+struct SolveResult {
+    int ier = 0;
+    int iterations = 0;    // reference ITER counter (mixed: inner iterations)
+    int iter_tot_add = 0;  // contribution to ITER_TOT(VNO)
+    int exit_kind = 0;
+    int line_skips = 0;
+    int line_fallbacks = 0;
+    int outer_steps = 0;
+    double rnorm0 = 0.0, rnorm = 0.0;
+};
+
+struct SolveOptions {
+    int pc = PC_LINE;
+    char sweep[4] = {'R', 'S', 'R', 'S'};
+    int precision = PREC_FP64;
+    bool on_device = false;      // a/b/x are device pointers (solved in place)
+    bool write_back_ab = true;   // copy the unit-scaled A/B back to host arrays
+    uint64_t seed = 0x5EEDULL;   // Rtilde stream
+    double inner_tol = 1e-4;     // mixed form: relative drop per inner solve
+    int check_every = 4;         // iterations between host checks of the state
+    bool use_graph = true;       // capture the iteration body in a CUDA graph
+    bool time_kernels = false;   // record events around every J-line launch (no graph replay)
+};
+
+// Device-side timing of the last solve (CUDA events on the engine's stream).
+struct SolveTiming {
+    float device_ms = 0.f;    // setup + iterations, inputs already on the device
+    float jline_ms = 0.f;     // sum over J-line launches (time_kernels only)
+    int jline_launches = 0;
+    long long kernel_launches = 0;  // kernels of this library launched by the solve
+};
+
+struct DeviceArena {
+    char *base = nullptr;
+    size_t cap = 0, used = 0;
+    void *take(size_t bytes);
+    void reset() { used = 0; }
+    cudaError_t reserve(size_t bytes);
+    void release();
+};
+
+class Engine {
+public:
+    Engine();
+    ~Engine();
+    // Solve a batch.  Returns 0 or a negative error code; per-system IER in out.
+    int solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt, std::vector<SolveResult> &out);
+    const std::string &last_error() const { return err_; }
+    int device() const { return dev_; }
+    int sm_count() const { return sms_; }
+    cudaStream_t stream() const { return stream_; }
+    size_t arena_bytes() const { return arena_.cap; }
+    const SolveTiming &timing() const { return timing_; }
+
+    // per-routine entry points on device pointers (parity tests of single kernels)
+    int matvec(const SystemSpec &g, const double *a, const double *x, double *y);
+    int msolve(const SystemSpec &g, const double *a, const double *b, double *var, int pc, const char sweep[4]);
+    int dot(const double *x, const double *y, int64_t n, double *out_host);
+
+private:
+    int setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions &opt);
+    int plan_msolve(const SolveOptions &opt, int src, int dst, int gate, int elem);
+    int run_msolve_plan(int which, int elem);
+    int bind_lists();
+    int fail(const std::string &msg, int code);
+
+    int dev_ = -1, sms_ = 0, cell_bpsm_ = 4;
+    cudaStream_t stream_ = nullptr;
+    cudaEvent_t ev_a_ = nullptr, ev_b_ = nullptr, ev_t0_ = nullptr, ev_t1_ = nullptr;
+    DeviceArena arena_;
+    std::string err_;
+
+    // batch tables (host mirrors + device copies)
+    int nsys_ = 0;
+    std::vector<SysDev> h_sys_;
+    std::vector<SysState> h_st_;
+    std::vector<Tile> h_tiles_;
+    std::vector<int> h_prefix_;
+    SysDev *d_sys_ = nullptr;
+    SysState *d_st_ = nullptr;
+    Tile *d_tiles_ = nullptr;
+    int *d_prefix_ = nullptr;
+    double *d_partials_ = nullptr;
+    SysState *h_st_pinned_ = nullptr;
+    size_t h_st_pinned_cap_ = 0;
+    BatchView view_{};
+    LaunchCfg cfg_{};
+
+    // sweep plans: [0] for P -> Phat, [1] for S -> Shat
+    struct Step {
+        int type;  // 0 J-line wave, 1 copy, 2 sequential line list
+        WaveArgs w;
+        SeqLineArgs s;
+    };
+    std::vector<Step> plan_[2];
+    int2 *d_lines_ = nullptr;
+    size_t d_lines_cap_ = 0;
+    double *d_seq_scratch_ = nullptr;
+    size_t d_seq_scratch_cap_ = 0;
+    std::vector<int2> h_lines_;
+    struct ListRef {
+        int which;
+        size_t index, offset;
+    };
+    std::vector<ListRef> list_refs_;
+
+    // standalone kernels
+    SysDev *d_one_sys_ = nullptr;
+    double *d_dot_partials_ = nullptr;
+    unsigned int *d_dot_counter_ = nullptr;
+    double *d_dot_out_ = nullptr;
+    size_t sys_cap_ = 0, st_cap_ = 0, tiles_cap_ = 0, prefix_cap_ = 0, part_cap_ = 0;
+    bool jline_timing_ = false;
+    static constexpr int JT_EVENTS = 2048;
+    cudaEvent_t jt_ev_[2 * JT_EVENTS] = {};
+    int jline_count_ = 0;
+    long long launches_ = 0;
+    SolveTiming timing_;
+};
+
+// choice of lanes per J-line and rows per lane for a line of length L
+void line_shape(int L, int *G, int *c);
+
+}  // namespace mfixgpu

@@ -1,0 +1,1221 @@
+// leq_kernels.cu -- sm_100a kernels of the LEQ_BICGS path (MFIX 2016-1,
+// model/leq_bicgs.f and model/leqsol_mod.f), batch-shaped.
+//
+// Cell kernels walk a device table of TILE_CELLS-cell tiles.  Each tile's dot
+// products are reduced inside the block and stored in a per-tile slot; the
+// block that completes a system's last tile sums the slots in tile order and
+// runs the scalar step of the iteration (alpha, omega, convergence test ...).
+// The result is independent of which block finishes last and of what else is in
+// the batch, so a system gives bit-identical results alone and in a mix.
+//
+// J-line kernels give each warp one or more whole lines (G lanes per line).
+// Each lane eliminates a chunk of c consecutive rows to an interface form, the
+// 2G interface rows are solved by parallel cyclic reduction over shuffles, and
+// the interior rows are recovered in place.  Lines whose rows do not satisfy a
+// local dominance bound (under which DGTSV never interchanges rows) are solved
+// again by one lane with the exact pivoting DGTSV recurrence.
+#include <cfloat>
+#include <cstdio>
+#include <type_traits>
+
+#include "leq_kernels.cuh"
+
+namespace mfixgpu {
+
+// ------------------------------------------------------------------ helpers
+template <typename T>
+__device__ __forceinline__ const T *diag_base(const SysDev &d);
+template <>
+__device__ __forceinline__ const double *diag_base<double>(const SysDev &d) { return d.a64; }
+template <>
+__device__ __forceinline__ const float *diag_base<float>(const SysDev &d) { return d.a32; }
+
+template <typename T>
+__device__ __forceinline__ T *vec(const SysDev &d, int id)
+{
+    return reinterpret_cast<T *>(d.vec[id]);
+}
+
+struct CellIdx {
+    int i, j, k;  // 0-based
+};
+
+__device__ __forceinline__ CellIdx cell_ijk(const SysDev &d, uint32_t c)
+{
+    const uint32_t line = fdiv(c, d.div_j);
+    CellIdx r;
+    r.j = (int)(c - line * (uint32_t)d.jmax2);
+    const uint32_t k = fdiv(line, d.div_i);
+    r.k = (int)k;
+    r.i = (int)(line - k * (uint32_t)d.imax2);
+    return r;
+}
+
+// 7-point product of row c with x, in the operand order of LEQ_MATVEC
+// (model/leqsol_mod.f:240-250), neighbours clamped at the array edge.
+template <typename T, typename TX>
+__device__ __forceinline__ double stencil_row(const SysDev &d, const T *__restrict__ a, const TX *__restrict__ x,
+                                              uint32_t c, const CellIdx &q)
+{
+    const int64_t n = d.n;
+    const int64_t c1 = d.jmax2, c2 = (int64_t)d.jmax2 * d.imax2;
+    const int64_t jm = q.j > 0 ? -1 : 0, jp = q.j < d.jmax2 - 1 ? 1 : 0;
+    const int64_t im = q.i > 0 ? -c1 : 0, ip = q.i < d.imax2 - 1 ? c1 : 0;
+    const int64_t p = c;
+    using A = typename std::conditional<(sizeof(T) > sizeof(TX)), T, TX>::type;
+    A v = (A)a[1 * n + p] * (A)x[p + jm];          // A(-2) * x(j-1)
+    v = v + (A)a[2 * n + p] * (A)x[p + im];        // A(-1) * x(i-1)
+    v = v + (A)a[3 * n + p] * (A)x[p];             // A( 0) * x
+    v = v + (A)a[4 * n + p] * (A)x[p + ip];        // A( 1) * x(i+1)
+    v = v + (A)a[5 * n + p] * (A)x[p + jp];        // A( 2) * x(j+1)
+    if (d.do_k) {
+        const int64_t km = q.k > 0 ? -c2 : 0, kp = q.k < d.kmax2 - 1 ? c2 : 0;
+        v = v + (A)a[0 * n + p] * (A)x[p + km];    // A(-3) * x(k-1)
+        v = v + (A)a[6 * n + p] * (A)x[p + kp];    // A( 3) * x(k+1)
+    }
+    return (double)v;
+}
+
+template <int NV>
+__device__ __forceinline__ void warp_sum(double (&v)[NV])
+{
+#pragma unroll
+    for (int q = 0; q < NV; ++q)
+#pragma unroll
+        for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
+}
+
+// Reduce v over the block; thread 0 receives the block total in v.
+template <int NV>
+__device__ __forceinline__ void block_sum(double (&v)[NV])
+{
+    __shared__ double red[NV][32];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    warp_sum<NV>(v);
+    __syncthreads();
+    if (lane == 0)
+#pragma unroll
+        for (int q = 0; q < NV; ++q) red[q][warp] = v[q];
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int q = 0; q < NV; ++q) v[q] = lane < nw ? red[q][lane] : 0.0;
+        warp_sum<NV>(v);
+    }
+}
+
+// Store a tile's partial sums and report whether this block closed the
+// system's reduction.  When it did, `tot` holds the system totals (thread 0).
+template <int NV>
+__device__ __forceinline__ bool tile_reduce(const BatchView &b, const SysDev &d, SysState &st, int tile_idx,
+                                            double (&v)[NV], double (&tot)[NV])
+{
+    __shared__ int last;
+    block_sum<NV>(v);
+    if (threadIdx.x == 0) {
+        double *slot = b.partials + 2 * (int64_t)(d.tile_base + tile_idx);
+#pragma unroll
+        for (int q = 0; q < NV; ++q) slot[q] = v[q];
+        __threadfence();
+        const unsigned prev = atomicAdd(&st.arrivals, 1u);
+        last = (prev == (unsigned)d.ntiles - 1);
+    }
+    __syncthreads();
+    if (!last) return false;
+    __threadfence();
+    double acc[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) acc[q] = 0.0;
+    for (int t = threadIdx.x; t < d.ntiles; t += blockDim.x) {
+        const double *slot = b.partials + 2 * (int64_t)(d.tile_base + t);
+#pragma unroll
+        for (int q = 0; q < NV; ++q) acc[q] += __ldcg(slot + q);
+    }
+    block_sum<NV>(acc);
+#pragma unroll
+    for (int q = 0; q < NV; ++q) tot[q] = acc[q];
+    if (threadIdx.x == 0) st.arrivals = 0;
+    return true;
+}
+
+// ------------------------------------------------------------------ scalar steps
+// model/leq_bicgs.f:485-495 (the REAL() casts are single-precision conversions).
+__device__ inline void final_logic(SysState &s, bool converged)
+{
+    if (!converged) converged = ((double)(float)s.rnorm <= s.tol * s.rnorm0);
+    s.ier = 0;
+    s.exit_kind = converged ? EX_RNORM : EX_ITMAX;
+    if (!converged) {
+        s.ier = -1;
+        s.iter_tot_add = s.iter;
+        if ((double)(float)s.rnorm >= (double)0.2f * (double)(float)s.rnorm0) s.ier = -2;
+    }
+    s.status = ST_DONE;
+}
+
+// End of the setup: Rnorm0 (model/leq_bicgs.f:291).
+__device__ inline void fin_rnorm0(SysState &s, double rr) { s.rnorm0 = sqrt(rr); }
+
+// Entry to the main loop: rho(0) and its zero test (:315-332).
+__device__ inline void fin_rho0(SysState &s, double rtr)
+{
+    s.i = 1;
+    s.iter = 1;
+    s.rnorm = 0.0;
+    s.snorm_exit = 0;
+    if (s.itmax < 1) {
+        final_logic(s, false);
+        return;
+    }
+    s.rho = rtr;
+    if (rtr == 0.0) {
+        s.ier = 0;
+        s.exit_kind = EX_RHO0;
+        s.status = ST_DONE;
+    }
+}
+
+// ------------------------------------------------------------------ setup kernels
+// Unit-diagonal scaling of every row (model/leq_bicgs.f:211-226).
+__global__ void k_scale(BatchView b)
+{
+    for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+        const Tile tl = b.tiles[t];
+        const SysDev &d = b.sys[tl.sys];
+        if (b.st[tl.sys].status != ST_RUNNING) continue;
+        const int64_t n = d.n;
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(n, c0 + TILE_CELLS);
+        int bad = 0;
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+            double m = fabs(d.a64[c]);
+#pragma unroll
+            for (int q = 1; q < 7; ++q) {
+                const double v = fabs(d.a64[q * n + c]);
+                if (isnan(m) || v > m) m = v;
+            }
+            if (m > 0.0) {
+                const double oam = 1.0 / m;
+#pragma unroll
+                for (int q = 0; q < 7; ++q) d.a64[q * n + c] = d.a64[q * n + c] * oam;
+                d.b64[c] = d.b64[c] * oam;
+            } else {
+                bad = 1;
+            }
+        }
+        if (__syncthreads_or(bad) && threadIdx.x == 0) atomicOr(&b.st[tl.sys].err, 1);
+    }
+}
+
+// A singular row returns IER = -2 before any iteration (:232-233).
+__global__ void k_after_scale(BatchView b)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= b.nsys) return;
+    SysState &st = b.st[s];
+    if (st.status != ST_RUNNING) return;
+    if (st.err & 1) {
+        st.ier = -2;
+        st.exit_kind = EX_SINGULAR;
+        st.status = ST_DONE;
+    }
+}
+
+__global__ void k_to_f32(BatchView b)
+{
+    for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+        const Tile tl = b.tiles[t];
+        const SysDev &d = b.sys[tl.sys];
+        if (b.st[tl.sys].status != ST_RUNNING) continue;
+        const int64_t n = d.n;
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(n, c0 + TILE_CELLS);
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x)
+#pragma unroll
+            for (int q = 0; q < 7; ++q) d.a32[q * n + c] = (float)d.a64[q * n + c];
+    }
+}
+
+// R = B - A*Var and ||R|| (model/leq_bicgs.f:283-291).
+template <typename T>
+__global__ void k_init_residual(BatchView b)
+{
+    for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+        const Tile tl = b.tiles[t];
+        const SysDev &d = b.sys[tl.sys];
+        SysState &st = b.st[tl.sys];
+        if (st.status != ST_RUNNING) continue;
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
+        const T *a = diag_base<T>(d);
+        const T *x = vec<T>(d, V_X);
+        T *r = vec<T>(d, V_R);
+        double v[1] = {0.0}, tot[1];
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+            const CellIdx q = cell_ijk(d, (uint32_t)c);
+            const T ax = (T)stencil_row<T, T>(d, a, x, (uint32_t)c, q);
+            const T rv = (T)d.b64[c] - ax;
+            r[c] = rv;
+            v[0] += (double)rv * (double)rv;
+        }
+        if (tile_reduce<1>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) fin_rnorm0(st, tot[0]);
+    }
+}
+
+__device__ __forceinline__ uint64_t mix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+// The counter-based stream that replaces RANDOM_NUMBER (model/leq_bicgs.f:298).
+__device__ __forceinline__ double uniform01(uint64_t seed, uint64_t tag, uint64_t idx)
+{
+    const uint64_t key = mix64(seed * 0x9E3779B97F4A7C15ULL + tag * 0xD1B54A32D192ED03ULL + 0x632BE59BD9B4E019ULL);
+    const uint64_t v = mix64(key + (idx + 1) * 0x9E3779B97F4A7C15ULL);
+    return (double)(v >> 11) * 0x1.0p-53;
+}
+
+// Rtilde = R + (2u-1)*1e-6*Rnorm0 (:303-305) and rho(0) = (Rtilde, R) (:318).
+template <typename T>
+__global__ void k_init_rtilde(BatchView b, uint64_t seed)
+{
+    for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+        const Tile tl = b.tiles[t];
+        const SysDev &d = b.sys[tl.sys];
+        SysState &st = b.st[tl.sys];
+        if (st.status != ST_RUNNING) continue;
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
+        const double rn0 = st.rnorm0;
+        const T *r = vec<T>(d, V_R);
+        T *rt = vec<T>(d, V_RT);
+        double v[1] = {0.0}, tot[1];
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+            const double u = uniform01(seed, 0xA1, (uint64_t)c);
+            const T rv = r[c];
+            const T rtv = (T)((double)rv + (2.0 * u - 1.0) * 1.0e-6 * rn0);
+            rt[c] = rtv;
+            v[0] += (double)rtv * (double)rv;
+        }
+        if (tile_reduce<1>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) fin_rho0(st, tot[0]);
+    }
+}
+
+// ------------------------------------------------------------------ iteration kernels
+// P = R (i = 1) or P = R + beta*(P - omega*V) (model/leq_bicgs.f:334-343).
+template <typename T, bool MIXED>
+__global__ void k_p_update(BatchView b)
+{
+    for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+        const Tile tl = b.tiles[t];
+        const SysDev &d = b.sys[tl.sys];
+        const SysState &st = b.st[tl.sys];
+        if (!gate_ok(st, G_INNER)) continue;
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
+        const T *r = vec<T>(d, V_R);
+        T *p = vec<T>(d, V_P);
+        if (st.i == 1) {
+            for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) p[c] = r[c];
+        } else {
+            const T beta = (T)st.beta, omega = (T)st.omega;
+            const T *v = vec<T>(d, V_V);
+            for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) p[c] = r[c] + beta * (p[c] - omega * v[c]);
+        }
+    }
+}
+
+// DIAG preconditioner, LEQ_MSOLVE1 (model/leqsol_mod.f:719-746): var = b / A(0).
+template <typename T>
+__global__ void k_diag(BatchView b, int src, int dst, int gate)
+{
+    for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+        const Tile tl = b.tiles[t];
+        const SysDev &d = b.sys[tl.sys];
+        if (!gate_ok(b.st[tl.sys], gate)) continue;
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
+        const T *a0 = diag_base<T>(d) + 3 * d.n;
+        const T *x = vec<T>(d, src);
+        T *y = vec<T>(d, dst);
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) y[c] = x[c] / a0[c];
+    }
+}
+
+template <typename T>
+__global__ void k_copy(BatchView b, int src, int dst, int gate)
+{
+    for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+        const Tile tl = b.tiles[t];
+        const SysDev &d = b.sys[tl.sys];
+        if (!gate_ok(b.st[tl.sys], gate)) continue;
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
+        const T *x = vec<T>(d, src);
+        T *y = vec<T>(d, dst);
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) y[c] = x[c];
+    }
+}
+
+// V = A*Phat and alpha = rho / (Rtilde, V) (model/leq_bicgs.f:355-361).
+template <typename T, bool MIXED>
+__global__ void k_matvec_alpha(BatchView b, int src)
+{
+    for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+        const Tile tl = b.tiles[t];
+        const SysDev &d = b.sys[tl.sys];
+        SysState &st = b.st[tl.sys];
+        if (!gate_ok(st, G_INNER)) continue;
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
+        const T *a = diag_base<T>(d);
+        const T *x = vec<T>(d, src);
+        const T *rt = vec<T>(d, V_RT);
+        T *y = vec<T>(d, V_V);
+        double v[1] = {0.0}, tot[1];
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+            const CellIdx q = cell_ijk(d, (uint32_t)c);
+            const T yv = (T)stencil_row<T, T>(d, a, x, (uint32_t)c, q);
+            y[c] = yv;
+            v[0] += (double)rt[c] * (double)yv;
+        }
+        if (tile_reduce<1>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) st.alpha = st.rho / tot[0];
+    }
+}
+
+// S = R - alpha*V and Snorm (model/leq_bicgs.f:365-375).
+template <typename T, bool MIXED>
+__global__ void k_s_update(BatchView b)
+{
+    for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+        const Tile tl = b.tiles[t];
+        const SysDev &d = b.sys[tl.sys];
+        SysState &st = b.st[tl.sys];
+        if (!gate_ok(st, G_INNER)) continue;
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
+        const T alpha = (T)st.alpha;
+        const T *r = vec<T>(d, V_R);
+        const T *vv = vec<T>(d, V_V);
+        T *s = vec<T>(d, V_S);
+        double v[1] = {0.0}, tot[1];
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+            const T sv = r[c] - alpha * vv[c];
+            s[c] = sv;
+            v[0] += (double)sv * (double)sv;
+        }
+        if (tile_reduce<1>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) {
+            st.snorm = sqrt(tot[0]);
+            if (MIXED)
+                st.snorm_exit = (st.snorm <= st.inner_tol * st.rnorm0) ? 1 : 0;
+            else
+                st.snorm_exit = (st.snorm <= DBL_EPSILON) ? 1 : 0;  // TOLMIN = EPSILON(ONE)
+        }
+    }
+}
+
+// T = A*Shat, omega = (T,S)/(T,T) with (T,T) = 0 -> SMALL_NUMBER (model/leq_bicgs.f:409-427).
+template <typename T, bool MIXED>
+__global__ void k_matvec_omega(BatchView b, int src)
+{
+    for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+        const Tile tl = b.tiles[t];
+        const SysDev &d = b.sys[tl.sys];
+        SysState &st = b.st[tl.sys];
+        if (!gate_ok(st, G_INNER_NOSNORM)) continue;
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
+        const T *a = diag_base<T>(d);
+        const T *x = vec<T>(d, src);
+        const T *s = vec<T>(d, V_S);
+        T *y = vec<T>(d, V_T);
+        double v[2] = {0.0, 0.0}, tot[2];
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+            const CellIdx q = cell_ijk(d, (uint32_t)c);
+            const T yv = (T)stencil_row<T, T>(d, a, x, (uint32_t)c, q);
+            y[c] = yv;
+            v[0] += (double)yv * (double)s[c];
+            v[1] += (double)yv * (double)yv;
+        }
+        if (tile_reduce<2>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) {
+            double txt = tot[1];
+            if (txt == 0.0) txt = 1.0e-15;  // SMALL_NUMBER
+            st.omega = tot[0] / txt;
+        }
+    }
+}
+
+// X += alpha*Phat + omega*Shat; R = S - omega*T; Rnorm; next rho
+// (model/leq_bicgs.f:432-460 and :318 of the following iteration).
+__device__ inline void fin_xr_ref(SysState &s, double rr, double rtr)
+{
+    if (s.snorm_exit) {  // :375-395
+        s.ier = 0;
+        s.exit_kind = EX_SNORM;
+        s.status = ST_DONE;
+        return;
+    }
+    s.rnorm = sqrt(rr);
+    if (s.rnorm <= s.tol * s.rnorm0) {
+        s.iter_tot_add = s.iter + 1;
+        s.ier = 0;
+        s.exit_kind = EX_RNORM;
+        s.status = ST_DONE;
+        return;
+    }
+    s.iter += 1;
+    s.i += 1;
+    if (s.i > s.itmax) {
+        final_logic(s, false);
+        return;
+    }
+    s.beta = (rtr / s.rho) * (s.alpha / s.omega);
+    s.rho_prev = s.rho;
+    s.rho = rtr;
+    if (rtr == 0.0) {
+        s.ier = -2;
+        s.exit_kind = EX_RHO0;
+        s.status = ST_DONE;
+    }
+}
+
+// Inner solve of the mixed form: convergence hands the system to the FP64
+// refinement step instead of ending it.
+__device__ inline void fin_xr_inner(SysState &s, double rr, double rtr)
+{
+    s.inner_total += 1;
+    if (s.snorm_exit) {
+        s.phase = PH_OUTER;
+        return;
+    }
+    s.rnorm = sqrt(rr);
+    if (s.rnorm <= s.inner_tol * s.rnorm0 || s.inner_total >= s.itmax || !(s.rnorm == s.rnorm)) {
+        s.phase = PH_OUTER;
+        return;
+    }
+    s.i += 1;
+    s.beta = (rtr / s.rho) * (s.alpha / s.omega);
+    s.rho_prev = s.rho;
+    s.rho = rtr;
+    if (rtr == 0.0 || s.omega == 0.0) s.phase = PH_OUTER;
+}
+
+template <typename T, bool MIXED>
+__global__ void k_xr_update(BatchView b, int ph_id, int sh_id)
+{
+    for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+        const Tile tl = b.tiles[t];
+        const SysDev &d = b.sys[tl.sys];
+        SysState &st = b.st[tl.sys];
+        if (!gate_ok(st, G_INNER)) continue;
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
+        const T alpha = (T)st.alpha;
+        const bool fresh = MIXED && st.i == 1;  // the inner correction starts from zero
+        T *x = vec<T>(d, V_X);
+        const T *ph = vec<T>(d, ph_id);
+        double v[2] = {0.0, 0.0}, tot[2];
+        if (st.snorm_exit) {
+            for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x)
+                x[c] = fresh ? alpha * ph[c] : x[c] + alpha * ph[c];
+        } else {
+            const T omega = (T)st.omega;
+            const T *sh = vec<T>(d, sh_id);
+            const T *s = vec<T>(d, V_S);
+            const T *tv = vec<T>(d, V_T);
+            const T *rt = vec<T>(d, V_RT);
+            T *r = vec<T>(d, V_R);
+            for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+                x[c] = fresh ? alpha * ph[c] + omega * sh[c] : x[c] + alpha * ph[c] + omega * sh[c];
+                const T rv = s[c] - omega * tv[c];
+                r[c] = rv;
+                v[0] += (double)rv * (double)rv;
+                v[1] += (double)rt[c] * (double)rv;
+            }
+        }
+        if (tile_reduce<2>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) {
+            if (MIXED)
+                fin_xr_inner(st, tot[0], tot[1]);
+            else
+                fin_xr_ref(st, tot[0], tot[1]);
+        }
+    }
+}
+
+// ------------------------------------------------------------------ mixed form: FP64 refinement
+// x <- x + d (FP64), r = b - A x in FP64 with FP64 A, r handed to the FP32 inner
+// solve as its right-hand side and shadow residual.
+__device__ inline void fin_outer(SysState &s, double rr, double r32r32)
+{
+    s.outer_rnorm = sqrt(rr);
+    if (s.outer_steps == 0) s.outer_rnorm0 = s.outer_rnorm;
+    s.outer_steps += 1;
+    s.xcur ^= 1;
+    s.rnorm = s.outer_rnorm;
+    s.rnorm0 = s.outer_rnorm0;
+    if (s.outer_rnorm <= s.tol * s.outer_rnorm0) {
+        s.iter = s.inner_total;
+        s.iter_tot_add = s.inner_total + 1;
+        s.ier = 0;
+        s.exit_kind = EX_RNORM;
+        s.status = ST_DONE;
+        return;
+    }
+    if (s.inner_total >= s.itmax || !(s.outer_rnorm == s.outer_rnorm)) {
+        s.iter = s.inner_total;
+        final_logic(s, false);
+        s.rnorm0 = s.outer_rnorm0;
+        return;
+    }
+    // inner solve setup: Rtilde = R, rho = (R,R)
+    s.rnorm0 = sqrt(r32r32);
+    s.rho = r32r32;
+    s.i = 1;
+    s.snorm_exit = 0;
+    s.phase = PH_INNER;
+    if (r32r32 == 0.0) {  // the FP32 copy of a nonzero FP64 residual underflowed
+        s.iter = s.inner_total;
+        s.rnorm = s.outer_rnorm;
+        s.rnorm0 = s.outer_rnorm0;
+        final_logic(s, false);
+    }
+}
+
+__global__ void k_outer_step(BatchView b)
+{
+    for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+        const Tile tl = b.tiles[t];
+        const SysDev &d = b.sys[tl.sys];
+        SysState &st = b.st[tl.sys];
+        if (!gate_ok(st, G_OUTER)) continue;
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
+        const int64_t n = d.n;
+        const int64_t cc1 = d.jmax2, cc2 = (int64_t)d.jmax2 * d.imax2;
+        const double *xo = d.x64[st.xcur];
+        double *xn = d.x64[st.xcur ^ 1];
+        const float *dx = vec<float>(d, V_X);
+        const bool add = st.outer_steps > 0;
+        float *r32 = vec<float>(d, V_R);
+        float *rt32 = vec<float>(d, V_RT);
+        const double *a = d.a64;
+        double v[2] = {0.0, 0.0}, tot[2];
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+            const CellIdx q = cell_ijk(d, (uint32_t)c);
+            const int64_t jm = q.j > 0 ? -1 : 0, jp = q.j < d.jmax2 - 1 ? 1 : 0;
+            const int64_t im = q.i > 0 ? -cc1 : 0, ip = q.i < d.imax2 - 1 ? cc1 : 0;
+            auto X = [&](int64_t p) { return add ? xo[p] + (double)dx[p] : xo[p]; };
+            double ax = a[1 * n + c] * X(c + jm);
+            ax = ax + a[2 * n + c] * X(c + im);
+            const double xc = X(c);
+            ax = ax + a[3 * n + c] * xc;
+            ax = ax + a[4 * n + c] * X(c + ip);
+            ax = ax + a[5 * n + c] * X(c + jp);
+            if (d.do_k) {
+                const int64_t km = q.k > 0 ? -cc2 : 0, kp = q.k < d.kmax2 - 1 ? cc2 : 0;
+                ax = ax + a[0 * n + c] * X(c + km);
+                ax = ax + a[6 * n + c] * X(c + kp);
+            }
+            const double rv = d.b64[c] - ax;
+            xn[c] = xc;
+            const float rf = (float)rv;
+            r32[c] = rf;
+            rt32[c] = rf;
+            v[0] += rv * rv;
+            v[1] += (double)rf * (double)rf;
+        }
+        if (tile_reduce<2>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) fin_outer(st, tot[0], tot[1]);
+    }
+}
+
+// ------------------------------------------------------------------ J-line half-sweeps
+// Row r of the J-line at (i,k), as LEQ_IKSWEEP / LEQ_ISWEEP build it
+// (model/leqsol_mod.f:891-905, :807-819): sub = A(-2), diag = A(0),
+// super = A(2), rhs = B - A(-1)Var(i-1) - A(1)Var(i+1) [- A(-3)Var(k-1) - A(3)Var(k+1)],
+// with CC(first) = EE(last) = 0.  Neighbours that clamp onto the cell itself read
+// the cell's own value from before the sweep.
+template <typename T>
+struct LineCtx {
+    const T *a;
+    const T *rhs;
+    const T *nb_im, *nb_ip, *nb_km, *nb_kp;  // already offset to the line base
+    int64_t base, n;
+    int L, do_k;
+};
+
+template <typename T>
+__device__ __forceinline__ void line_row(const LineCtx<T> &x, int r, T &sub, T &dg, T &sup, T &f)
+{
+    const int64_t p = x.base + r;
+    const int64_t n = x.n;
+    sub = (r == 0) ? T(0) : x.a[1 * n + p];
+    dg = x.a[3 * n + p];
+    sup = (r == x.L - 1) ? T(0) : x.a[5 * n + p];
+    T v = x.rhs[p] - x.a[2 * n + p] * x.nb_im[r];
+    v = v - x.a[4 * n + p] * x.nb_ip[r];
+    if (x.do_k) {
+        v = v - x.a[0 * n + p] * x.nb_km[r];
+        v = v - x.a[6 * n + p] * x.nb_kp[r];
+    }
+    f = v;
+}
+
+// DGTSV (NRHS = 1) on shared-memory rows 0..L-1: sub[r] couples row r to r-1,
+// sup[r] couples row r to r+1.  Same pivoting and INFO as model/DGTSV.f:107-163, 231-246.
+template <typename T>
+__device__ int dgtsv_rows(int L, T *sub, T *dg, T *sup, T *f)
+{
+    // DL(i) = sub[i+1] (i = 0..L-2); DL is overwritten by the second super-diagonal.
+    for (int i = 0; i < L - 1; ++i) {
+        T dli = sub[i + 1];
+        if (fabs(dg[i]) >= fabs(dli)) {
+            if (dg[i] != T(0)) {
+                const T fact = dli / dg[i];
+                dg[i + 1] = dg[i + 1] - fact * sup[i];
+                f[i + 1] = f[i + 1] - fact * f[i];
+            } else {
+                return i + 1;
+            }
+            if (i < L - 2) sub[i + 1] = T(0);
+        } else {
+            const T fact = dg[i] / dli;
+            dg[i] = dli;
+            const T temp = dg[i + 1];
+            dg[i + 1] = sup[i] - fact * temp;
+            if (i < L - 2) {
+                sub[i + 1] = sup[i + 1];
+                sup[i + 1] = -fact * sub[i + 1];
+            }
+            sup[i] = temp;
+            const T tb = f[i];
+            f[i] = f[i + 1];
+            f[i + 1] = tb - fact * f[i + 1];
+        }
+    }
+    if (dg[L - 1] == T(0)) return L;
+    f[L - 1] = f[L - 1] / dg[L - 1];
+    if (L > 1) f[L - 2] = (f[L - 2] - sup[L - 2] * f[L - 1]) / dg[L - 2];
+    for (int i = L - 3; i >= 0; --i) f[i] = (f[i] - sup[i] * f[i + 1] - sub[i + 1] * f[i + 2]) / dg[i];
+    return 0;
+}
+
+template <typename T>
+struct Eps;
+template <>
+struct Eps<double> {
+    static constexpr double margin = 1e-12;
+};
+template <>
+struct Eps<float> {
+    static constexpr float margin = 1e-5f;
+};
+
+__device__ __forceinline__ int find_sys(const int *prefix, int nsys, int item)
+{
+    int lo = 0, hi = nsys - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (__ldg(prefix + mid) <= item)
+            lo = mid;
+        else
+            hi = mid - 1;
+    }
+    return lo;
+}
+
+template <typename T>
+__global__ void __launch_bounds__(LINE_WARPS * 32) k_jline(BatchView b, WaveArgs w, int cmax)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rows_w = 32 * cmax;
+    T *s_sub = reinterpret_cast<T *>(smem_raw) + (size_t)warp * 4 * rows_w;
+    T *s_dg = s_sub + rows_w, *s_sup = s_dg + rows_w, *s_f = s_sup + rows_w;
+
+    const int total = (w.kind == 0) ? b.line_prefix[b.nsys] : w.count;
+    for (int item = blockIdx.x * LINE_WARPS + warp; item < total; item += gridDim.x * LINE_WARPS) {
+        const int sidx = (w.kind == 0) ? find_sys(b.line_prefix, b.nsys, item) : 0;
+        SysState &st = b.st[sidx];
+        if (!gate_ok(st, w.gate)) continue;
+        const SysDev &d = b.sys[sidx];
+        const int G = d.lane_group, c = d.rows_per_lane, L = d.jmax2;
+        const int lpw = 32 / G;
+        const int seg = lane / G, gl = lane - seg * G;
+        const int item0 = (w.kind == 0) ? b.line_prefix[sidx] : 0;
+        const int q = (item - item0) * lpw + seg;
+        int i, k;
+        bool valid;
+        if (w.kind == 0) {
+            k = q / d.half_lines + 1;
+            const int slot = q - (k - 1) * d.half_lines;
+            const int i0 = (((1 + k) & 1) == w.par) ? 1 : 2;
+            i = i0 + 2 * slot;
+            valid = (k <= d.kmax2) && (i <= d.imax2);
+        } else if (w.kind == 1) {
+            const int ilo = max(1, w.par - d.kmax2), ihi = min(d.imax2, w.par - 1);
+            i = ilo + q;
+            k = w.par - i;
+            valid = (i <= ihi);
+        } else {
+            valid = q < w.nlines;
+            const int2 lk = valid ? w.list[q] : make_int2(1, 1);
+            i = lk.x;
+            k = lk.y;
+        }
+        const int64_t c1 = d.jmax2, c2 = (int64_t)d.jmax2 * d.imax2;
+        LineCtx<T> x;
+        x.a = diag_base<T>(d);
+        x.rhs = vec<T>(d, w.rhs);
+        x.n = d.n;
+        x.L = L;
+        x.do_k = d.do_k;
+        x.base = (int64_t)(i - 1) * c1 + (int64_t)(k - 1) * c2;
+        const T *nbr = vec<T>(d, w.nbr), *old = vec<T>(d, w.old);
+        x.nb_im = (i > 1) ? nbr + x.base - c1 : old + x.base;
+        x.nb_ip = (i < d.imax2) ? nbr + x.base + c1 : old + x.base;
+        x.nb_km = (k > 1) ? nbr + x.base - c2 : old + x.base;
+        x.nb_kp = (k < d.kmax2) ? nbr + x.base + c2 : old + x.base;
+
+        // ---- load: coalesced over the line, contiguous rows in shared memory
+        const int segoff = seg * G * c;
+        T *sub = s_sub + segoff, *dg = s_dg + segoff, *sup = s_sup + segoff, *f = s_f + segoff;
+        bool ok = true;
+        for (int r = gl; r < G * c; r += G) {
+            T a_ = T(0), d_ = T(1), c_ = T(0), f_ = T(0);
+            if (valid && r < L) {
+                line_row<T>(x, r, a_, d_, c_, f_);
+                const T an = (r + 1 < L) ? x.a[1 * x.n + x.base + r + 1] : T(0);
+                const T m = fabs(d_) - fabs(a_);
+                // pivot-free bound: |d_r| - |a_r| > 0 and >= |c_r|, |a_{r+1}| (with margin)
+                ok = ok && (m > T(0)) && (m >= fabs(c_) * (T(1) + Eps<T>::margin)) &&
+                     (m >= fabs(an) * (T(1) + Eps<T>::margin));
+            }
+            sub[r] = a_;
+            dg[r] = d_;
+            sup[r] = c_;
+            f[r] = f_;
+        }
+        const unsigned bad = __ballot_sync(0xffffffffu, !ok);
+        const unsigned segmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (seg * G);
+        const bool seg_ok = (bad & segmask) == 0u;
+        __syncwarp();
+
+        // ---- chunk elimination (every lane, rows gl*c .. gl*c+c-1)
+        {
+            T *ca = sub + gl * c, *cd = dg + gl * c, *cc = sup + gl * c, *cf = f + gl * c;
+            T inv = T(1) / cd[0];
+            T a0 = ca[0] * inv, c0 = cc[0] * inv, f0 = cf[0] * inv;
+            inv = T(1) / cd[1];
+            T pa = ca[1] * inv, pc = cc[1] * inv, pf = cf[1] * inv;
+            ca[1] = pa;
+            cc[1] = pc;
+            cf[1] = pf;
+            for (int t = 2; t < c; ++t) {
+                const T at = ca[t];
+                inv = T(1) / (cd[t] - at * pc);
+                pf = (cf[t] - at * pf) * inv;
+                pa = -at * pa * inv;
+                pc = cc[t] * inv;
+                ca[t] = pa;
+                cc[t] = pc;
+                cf[t] = pf;
+            }
+            // backward: rows c-3 .. 1 into  A_t x_first + x_t + C_t x_last = F_t
+            if (c >= 3) {
+                T na = ca[c - 2], nc = cc[c - 2], nf = cf[c - 2];
+                for (int t = c - 3; t >= 1; --t) {
+                    const T ct = cc[t];
+                    nf = cf[t] - ct * nf;
+                    na = ca[t] - ct * na;
+                    nc = -ct * nc;
+                    ca[t] = na;
+                    cc[t] = nc;
+                    cf[t] = nf;
+                }
+                // row 0 loses its coupling to row 1
+                const T r1a = ca[1], r1c = cc[1], r1f = cf[1];
+                inv = T(1) / (T(1) - c0 * r1a);
+                f0 = (f0 - c0 * r1f) * inv;
+                a0 = a0 * inv;
+                c0 = -c0 * r1c * inv;
+            }
+            T aL = ca[c - 1], cL = cc[c - 1], fL = cf[c - 1];
+
+            // ---- interface system (2G rows, unit diagonal): PCR over the segment
+            {
+                // stride 1: first row couples lane-1's last and own last; last row couples own first and lane+1's first
+                T la = __shfl_up_sync(0xffffffffu, aL, 1, G);
+                T lc = __shfl_up_sync(0xffffffffu, cL, 1, G);
+                T lf = __shfl_up_sync(0xffffffffu, fL, 1, G);
+                T ra = __shfl_down_sync(0xffffffffu, a0, 1, G);
+                T rc = __shfl_down_sync(0xffffffffu, c0, 1, G);
+                T rf = __shfl_down_sync(0xffffffffu, f0, 1, G);
+                if (gl < 1) la = lc = lf = T(0);
+                if (gl + 1 >= G) ra = rc = rf = T(0);
+                T den = T(1) - a0 * lc - c0 * aL;
+                inv = T(1) / den;
+                const T na0 = -a0 * la * inv, nc0 = -c0 * cL * inv, nf0 = (f0 - a0 * lf - c0 * fL) * inv;
+                den = T(1) - aL * c0 - cL * ra;
+                inv = T(1) / den;
+                const T naL = -aL * a0 * inv, ncL = -cL * rc * inv, nfL = (fL - aL * f0 - cL * rf) * inv;
+                a0 = na0; c0 = nc0; f0 = nf0;
+                aL = naL; cL = ncL; fL = nfL;
+            }
+            for (int dl = 1; dl < G; dl <<= 1) {
+                T la0 = __shfl_up_sync(0xffffffffu, a0, dl, G), lc0 = __shfl_up_sync(0xffffffffu, c0, dl, G),
+                  lf0 = __shfl_up_sync(0xffffffffu, f0, dl, G);
+                T ra0 = __shfl_down_sync(0xffffffffu, a0, dl, G), rc0 = __shfl_down_sync(0xffffffffu, c0, dl, G),
+                  rf0 = __shfl_down_sync(0xffffffffu, f0, dl, G);
+                T laL = __shfl_up_sync(0xffffffffu, aL, dl, G), lcL = __shfl_up_sync(0xffffffffu, cL, dl, G),
+                  lfL = __shfl_up_sync(0xffffffffu, fL, dl, G);
+                T raL = __shfl_down_sync(0xffffffffu, aL, dl, G), rcL = __shfl_down_sync(0xffffffffu, cL, dl, G),
+                  rfL = __shfl_down_sync(0xffffffffu, fL, dl, G);
+                if (gl < dl) la0 = lc0 = lf0 = laL = lcL = lfL = T(0);
+                if (gl + dl >= G) ra0 = rc0 = rf0 = raL = rcL = rfL = T(0);
+                inv = T(1) / (T(1) - a0 * lc0 - c0 * ra0);
+                const T na0 = -a0 * la0 * inv, nc0 = -c0 * rc0 * inv, nf0 = (f0 - a0 * lf0 - c0 * rf0) * inv;
+                inv = T(1) / (T(1) - aL * lcL - cL * raL);
+                const T naL = -aL * laL * inv, ncL = -cL * rcL * inv, nfL = (fL - aL * lfL - cL * rfL) * inv;
+                a0 = na0; c0 = nc0; f0 = nf0;
+                aL = naL; cL = ncL; fL = nfL;
+            }
+            const T xf = f0, xl = fL;
+            // ---- interior rows
+            for (int t = 1; t < c - 1; ++t) cf[t] = cf[t] - ca[t] * xf - cc[t] * xl;
+            cf[0] = xf;
+            cf[c - 1] = xl;
+        }
+        __syncwarp();
+
+        // ---- rare path: rows that may need interchanges get the exact pivoting recurrence
+        int skip = 0;
+        if (!seg_ok && valid) {
+            for (int r = gl; r < L; r += G) {
+                T a_, d_, c_, f_;
+                line_row<T>(x, r, a_, d_, c_, f_);
+                sub[r] = a_;
+                dg[r] = d_;
+                sup[r] = c_;
+                f[r] = f_;
+            }
+            __syncwarp(segmask);
+            if (gl == 0) {
+                skip = dgtsv_rows<T>(L, sub, dg, sup, f) != 0;
+                atomicAdd(&st.line_fallbacks, 1);
+                if (skip) atomicAdd(&st.line_skips, 1);
+            }
+            __syncwarp(segmask);
+        }
+        skip = __shfl_sync(0xffffffffu, skip, seg * G);
+        __syncwarp();
+
+        // ---- store: coalesced.  A line left unchanged (INFO != 0) keeps its old value.
+        if (valid) {
+            T *dst = vec<T>(d, w.dst) + x.base;
+            const T *oldl = old + x.base;
+            if (!skip) {
+                for (int r = gl; r < L; r += G) dst[r] = f[r];
+            } else if (w.write_old) {
+                for (int r = gl; r < L; r += G) dst[r] = oldl[r];
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------------ exact sequential line sweeps
+// One thread per line, the pivoting DGTSV over global scratch laid out [row][line]
+// so that neighbouring threads touch neighbouring words.
+template <typename T>
+__global__ void k_seq_lines(BatchView b, SeqLineArgs a)
+{
+    const int li = blockIdx.x * blockDim.x + threadIdx.x;
+    if (li >= a.count) return;
+    SysState &st = b.st[0];
+    if (!gate_ok(st, G_INNER)) return;
+    const SysDev &d = b.sys[0];
+    const int64_t n = d.n, c1 = d.jmax2, c2 = (int64_t)d.jmax2 * d.imax2;
+    const T *A = diag_base<T>(d);
+    const T *rhs = vec<T>(d, a.rhs);
+    T *var = vec<T>(d, a.var);
+    const int2 lc = a.lines[li];
+    int L;
+    int64_t base, step;
+    // which diagonals form the tridiagonal and which four go to the right-hand side
+    int dsub, dsup, o0, o1, o2, o3;
+    if (a.axis == 0) {  // I-line at (j,k), LEQ_JKSWEEP: CC=A(-1), EE=A(1)
+        L = d.imax2;
+        base = (int64_t)(lc.x - 1) + (int64_t)(lc.y - 1) * c2;
+        step = c1;
+        dsub = 2; dsup = 4; o0 = 1; o1 = 5; o2 = 0; o3 = 6;
+    } else if (a.axis == 1) {  // J-line at (i,k), LEQ_IKSWEEP: CC=A(-2), EE=A(2)
+        L = d.jmax2;
+        base = (int64_t)(lc.x - 1) * c1 + (int64_t)(lc.y - 1) * c2;
+        step = 1;
+        dsub = 1; dsup = 5; o0 = 2; o1 = 4; o2 = 0; o3 = 6;
+    } else {  // K-line at (i,j), LEQ_IJSWEEP: CC=A(-3), EE=A(3)
+        L = d.kmax2;
+        base = (int64_t)(lc.x - 1) * c1 + (int64_t)(lc.y - 1);
+        step = c2;
+        dsub = 0; dsup = 6; o0 = 1; o1 = 5; o2 = 2; o3 = 4;
+    }
+    // RHS operand order follows the reference routines
+    T *sub = reinterpret_cast<T *>(a.scratch), *dg = sub + (size_t)a.lmax * a.count,
+      *sup = dg + (size_t)a.lmax * a.count, *f = sup + (size_t)a.lmax * a.count;
+#define SCR(arr, r) arr[(size_t)(r)*a.count + li]
+    for (int r = 0; r < L; ++r) {
+        const int64_t p = base + r * step;
+        int ii, jj, kk;
+        {
+            const CellIdx q = cell_ijk(d, (uint32_t)p);
+            ii = q.i; jj = q.j; kk = q.k;
+        }
+        auto nb = [&](int dd) -> T {
+            int64_t o = 0;
+            switch (dd) {
+            case 0: o = kk > 0 ? -c2 : 0; break;
+            case 1: o = jj > 0 ? -1 : 0; break;
+            case 2: o = ii > 0 ? -c1 : 0; break;
+            case 4: o = ii < d.imax2 - 1 ? c1 : 0; break;
+            case 5: o = jj < d.jmax2 - 1 ? 1 : 0; break;
+            case 6: o = kk < d.kmax2 - 1 ? c2 : 0; break;
+            }
+            return var[p + o];
+        };
+        SCR(sub, r) = (r == 0) ? T(0) : A[dsub * n + p];
+        SCR(dg, r) = A[3 * n + p];
+        SCR(sup, r) = (r == L - 1) ? T(0) : A[dsup * n + p];
+        T v = rhs[p] - A[o0 * n + p] * nb(o0);
+        v = v - A[o1 * n + p] * nb(o1);
+        if (a.axis != 1 || d.do_k) {
+            v = v - A[o2 * n + p] * nb(o2);
+            v = v - A[o3 * n + p] * nb(o3);
+        }
+        SCR(f, r) = v;
+    }
+    // DGTSV on the strided scratch
+    int info = 0;
+    for (int i = 0; i < L - 1 && !info; ++i) {
+        const T dli = SCR(sub, i + 1);
+        if (fabs(SCR(dg, i)) >= fabs(dli)) {
+            if (SCR(dg, i) != T(0)) {
+                const T fact = dli / SCR(dg, i);
+                SCR(dg, i + 1) = SCR(dg, i + 1) - fact * SCR(sup, i);
+                SCR(f, i + 1) = SCR(f, i + 1) - fact * SCR(f, i);
+            } else {
+                info = i + 1;
+                break;
+            }
+            if (i < L - 2) SCR(sub, i + 1) = T(0);
+        } else {
+            const T fact = SCR(dg, i) / dli;
+            SCR(dg, i) = dli;
+            const T temp = SCR(dg, i + 1);
+            SCR(dg, i + 1) = SCR(sup, i) - fact * temp;
+            if (i < L - 2) {
+                SCR(sub, i + 1) = SCR(sup, i + 1);
+                SCR(sup, i + 1) = -fact * SCR(sub, i + 1);
+            }
+            SCR(sup, i) = temp;
+            const T tb = SCR(f, i);
+            SCR(f, i) = SCR(f, i + 1);
+            SCR(f, i + 1) = tb - fact * SCR(f, i + 1);
+        }
+    }
+    if (!info && SCR(dg, L - 1) == T(0)) info = L;
+    if (info) {
+        if (a.fatal_on_info)
+            atomicOr(&st.err, 2);
+        else
+            atomicAdd(&st.line_skips, 1);
+        return;
+    }
+    SCR(f, L - 1) = SCR(f, L - 1) / SCR(dg, L - 1);
+    if (L > 1) SCR(f, L - 2) = (SCR(f, L - 2) - SCR(sup, L - 2) * SCR(f, L - 1)) / SCR(dg, L - 2);
+    for (int i = L - 3; i >= 0; --i)
+        SCR(f, i) = (SCR(f, i) - SCR(sup, i) * SCR(f, i + 1) - SCR(sub, i + 1) * SCR(f, i + 2)) / SCR(dg, i);
+    for (int r = 0; r < L; ++r) var[base + r * step] = SCR(f, r);
+#undef SCR
+}
+
+// ------------------------------------------------------------------ standalone kernels
+template <typename T>
+__global__ void k_matvec_plain(const SysDev *sysp, const T *a, const T *x, T *y)
+{
+    const SysDev &d = *sysp;
+    const int64_t n = d.n;
+    for (int64_t c = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += (int64_t)gridDim.x * blockDim.x) {
+        const CellIdx q = cell_ijk(d, (uint32_t)c);
+        y[c] = (T)stencil_row<T, T>(d, a, x, (uint32_t)c, q);
+    }
+}
+
+// (x, y) over n values: per-block sums in fixed order, the last block adds them.
+__global__ void k_dot(const double *x, const double *y, int64_t n, double *partials, unsigned int *counter,
+                      double *out)
+{
+    __shared__ int last;
+    double v[1] = {0.0};
+    const int64_t per = (n + gridDim.x - 1) / gridDim.x;
+    const int64_t c0 = (int64_t)blockIdx.x * per, c1 = min(n, c0 + per);
+    for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) v[0] += x[c] * y[c];
+    block_sum<1>(v);
+    if (threadIdx.x == 0) {
+        partials[blockIdx.x] = v[0];
+        __threadfence();
+        last = (atomicAdd(counter, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last) return;
+    __threadfence();
+    double acc[1] = {0.0};
+    for (int t = threadIdx.x; t < (int)gridDim.x; t += blockDim.x) acc[0] += __ldcg(partials + t);
+    block_sum<1>(acc);
+    if (threadIdx.x == 0) {
+        *out = acc[0];
+        *counter = 0u;
+    }
+}
+
+// ------------------------------------------------------------------ launchers
+#define CHECK_LAUNCH() return cudaGetLastError()
+
+cudaError_t launch_scale(const BatchView &b, const LaunchCfg &c)
+{
+    k_scale<<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b);
+    CHECK_LAUNCH();
+}
+cudaError_t launch_after_scale(const BatchView &b, const LaunchCfg &c)
+{
+    k_after_scale<<<(b.nsys + 127) / 128, 128, 0, c.stream>>>(b);
+    CHECK_LAUNCH();
+}
+cudaError_t launch_to_f32(const BatchView &b, const LaunchCfg &c)
+{
+    k_to_f32<<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b);
+    CHECK_LAUNCH();
+}
+template <typename T>
+cudaError_t launch_init_residual(const BatchView &b, const LaunchCfg &c)
+{
+    k_init_residual<T><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b);
+    CHECK_LAUNCH();
+}
+template <typename T>
+cudaError_t launch_init_rtilde(const BatchView &b, const LaunchCfg &c, uint64_t seed)
+{
+    k_init_rtilde<T><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b, seed);
+    CHECK_LAUNCH();
+}
+template <typename T, bool MIXED>
+cudaError_t launch_p_update(const BatchView &b, const LaunchCfg &c)
+{
+    k_p_update<T, MIXED><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b);
+    CHECK_LAUNCH();
+}
+int kernel_smem_line_bytes(int cmax, int elem_bytes) { return LINE_WARPS * 4 * 32 * cmax * elem_bytes; }
+
+template <typename T>
+int prepare_line_kernel(int cmax)
+{
+    const int smem = kernel_smem_line_bytes(cmax, (int)sizeof(T));
+    if (cudaFuncSetAttribute(k_jline<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+        return 0;
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_jline<T>, LINE_WARPS * 32, smem) != cudaSuccess)
+        return 0;
+    return nb;
+}
+
+int cell_blocks_per_sm()
+{
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_matvec_omega<double, false>, CELL_THREADS, 0) !=
+        cudaSuccess)
+        return 4;
+    return nb > 0 ? nb : 1;
+}
+
+template <typename T>
+cudaError_t launch_jline(const BatchView &b, const LaunchCfg &c, const WaveArgs &w)
+{
+    const int smem = kernel_smem_line_bytes(c.line_cmax, (int)sizeof(T));
+    k_jline<T><<<c.line_grid, LINE_WARPS * 32, smem, c.stream>>>(b, w, c.line_cmax);
+    CHECK_LAUNCH();
+}
+template <typename T>
+cudaError_t launch_diag(const BatchView &b, const LaunchCfg &c, int src, int dst, int gate)
+{
+    k_diag<T><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b, src, dst, gate);
+    CHECK_LAUNCH();
+}
+template <typename T>
+cudaError_t launch_copy(const BatchView &b, const LaunchCfg &c, int src, int dst, int gate)
+{
+    k_copy<T><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b, src, dst, gate);
+    CHECK_LAUNCH();
+}
+template <typename T, bool MIXED>
+cudaError_t launch_matvec_alpha(const BatchView &b, const LaunchCfg &c, int src)
+{
+    k_matvec_alpha<T, MIXED><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b, src);
+    CHECK_LAUNCH();
+}
+template <typename T, bool MIXED>
+cudaError_t launch_s_update(const BatchView &b, const LaunchCfg &c)
+{
+    k_s_update<T, MIXED><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b);
+    CHECK_LAUNCH();
+}
+template <typename T, bool MIXED>
+cudaError_t launch_matvec_omega(const BatchView &b, const LaunchCfg &c, int src)
+{
+    k_matvec_omega<T, MIXED><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b, src);
+    CHECK_LAUNCH();
+}
+template <typename T, bool MIXED>
+cudaError_t launch_xr_update(const BatchView &b, const LaunchCfg &c, int ph, int sh)
+{
+    k_xr_update<T, MIXED><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b, ph, sh);
+    CHECK_LAUNCH();
+}
+cudaError_t launch_outer_step(const BatchView &b, const LaunchCfg &c)
+{
+    k_outer_step<<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b);
+    CHECK_LAUNCH();
+}
+template <typename T>
+cudaError_t launch_matvec_plain(const SysDev *sys_dev, const SysDev &h, const T *a, const T *x, T *y,
+                                cudaStream_t s, int grid)
+{
+    (void)h;
+    k_matvec_plain<T><<<grid, CELL_THREADS, 0, s>>>(sys_dev, a, x, y);
+    CHECK_LAUNCH();
+}
+cudaError_t launch_dot(const double *x, const double *y, int64_t n, double *partials, unsigned int *counter,
+                       double *out, int grid, cudaStream_t s)
+{
+    k_dot<<<grid, CELL_THREADS, 0, s>>>(x, y, n, partials, counter, out);
+    CHECK_LAUNCH();
+}
+template <typename T>
+cudaError_t launch_seq_lines(const BatchView &b, const SeqLineArgs &a, cudaStream_t s)
+{
+    if (a.count <= 0) return cudaSuccess;
+    k_seq_lines<T><<<(a.count + 127) / 128, 128, 0, s>>>(b, a);
+    CHECK_LAUNCH();
+}
+
+// explicit instantiations
+#define INST_T(T)                                                                                        \
+    template cudaError_t launch_init_residual<T>(const BatchView &, const LaunchCfg &);                  \
+    template cudaError_t launch_init_rtilde<T>(const BatchView &, const LaunchCfg &, uint64_t);          \
+    template cudaError_t launch_jline<T>(const BatchView &, const LaunchCfg &, const WaveArgs &);        \
+    template cudaError_t launch_diag<T>(const BatchView &, const LaunchCfg &, int, int, int);            \
+    template cudaError_t launch_copy<T>(const BatchView &, const LaunchCfg &, int, int, int);            \
+    template cudaError_t launch_matvec_plain<T>(const SysDev *, const SysDev &, const T *, const T *, T *, \
+                                                cudaStream_t, int);                                       \
+    template cudaError_t launch_seq_lines<T>(const BatchView &, const SeqLineArgs &, cudaStream_t);        \
+    template int prepare_line_kernel<T>(int);
+#define INST_TM(T, M)                                                                       \
+    template cudaError_t launch_p_update<T, M>(const BatchView &, const LaunchCfg &);       \
+    template cudaError_t launch_matvec_alpha<T, M>(const BatchView &, const LaunchCfg &, int); \
+    template cudaError_t launch_s_update<T, M>(const BatchView &, const LaunchCfg &);       \
+    template cudaError_t launch_matvec_omega<T, M>(const BatchView &, const LaunchCfg &, int); \
+    template cudaError_t launch_xr_update<T, M>(const BatchView &, const LaunchCfg &, int, int);
+INST_T(double)
+INST_T(float)
+INST_TM(double, false)
+INST_TM(float, true)
+
+}  // namespace mfixgpu

@@ -1,0 +1,80 @@
+// leq_kernels.cuh -- launch interface of the B200 kernels for the LEQ_BICGS path.
+#pragma once
+#include "leq_common.cuh"
+
+namespace mfixgpu {
+
+// Everything a kernel needs to find the batch.
+struct BatchView {
+    const SysDev *sys;     // [nsys]
+    SysState *st;          // [nsys]
+    const Tile *tiles;     // [ntiles]
+    int ntiles;
+    int nsys;
+    const int *line_prefix;  // [nsys+1] parity-wave work items (exclusive prefix)
+    double *partials;        // [ntiles_total * 2]
+};
+
+struct LaunchCfg {
+    int cell_grid;   // blocks for cell-tile kernels
+    int line_grid;   // blocks for J-line kernels
+    int line_cmax;   // max rows per lane over the batch (smem sizing)
+    cudaStream_t stream;
+};
+
+// Setup
+cudaError_t launch_scale(const BatchView &b, const LaunchCfg &c);
+cudaError_t launch_after_scale(const BatchView &b, const LaunchCfg &c);
+cudaError_t launch_to_f32(const BatchView &b, const LaunchCfg &c);
+template <typename T>
+cudaError_t launch_init_residual(const BatchView &b, const LaunchCfg &c);  // R = B - A X, ||R||
+template <typename T>
+cudaError_t launch_init_rtilde(const BatchView &b, const LaunchCfg &c, uint64_t seed);  // Rtilde, rho(0)
+
+// One BiCGSTAB iteration (model/leq_bicgs.f:316-466)
+template <typename T, bool MIXED>
+cudaError_t launch_p_update(const BatchView &b, const LaunchCfg &c);
+template <typename T>
+cudaError_t launch_jline(const BatchView &b, const LaunchCfg &c, const WaveArgs &w);
+template <typename T>
+cudaError_t launch_diag(const BatchView &b, const LaunchCfg &c, int src, int dst, int gate);
+template <typename T>
+cudaError_t launch_copy(const BatchView &b, const LaunchCfg &c, int src, int dst, int gate);
+template <typename T, bool MIXED>
+cudaError_t launch_matvec_alpha(const BatchView &b, const LaunchCfg &c, int src);   // V = A*Phat, alpha
+template <typename T, bool MIXED>
+cudaError_t launch_s_update(const BatchView &b, const LaunchCfg &c);               // S = R - alpha V, Snorm
+template <typename T, bool MIXED>
+cudaError_t launch_matvec_omega(const BatchView &b, const LaunchCfg &c, int src);   // T = A*Shat, omega
+template <typename T, bool MIXED>
+cudaError_t launch_xr_update(const BatchView &b, const LaunchCfg &c, int ph, int sh);  // X, R, Rnorm, rho
+
+// Mixed form: FP64 refinement step (outer residual in FP64, x accumulated in FP64)
+cudaError_t launch_outer_step(const BatchView &b, const LaunchCfg &c);
+
+// Standalone kernels behind the per-routine C entry points
+template <typename T>
+cudaError_t launch_matvec_plain(const SysDev *sys_dev, const SysDev &h, const T *a, const T *x, T *y,
+                                cudaStream_t s, int grid);
+cudaError_t launch_dot(const double *x, const double *y, int64_t n, double *partials, unsigned int *counter,
+                       double *out, int grid, cudaStream_t s);
+// Sequential-per-thread exact DGTSV over a list of lines along I or K (LEQ_JKSWEEP / LEQ_IJSWEEP)
+// or J (lexicographic / ASAS IK order), writing the error flag on INFO != 0 where the reference aborts.
+struct SeqLineArgs {
+    int axis;           // 0: line along I at (j,k); 1: along J at (i,k); 2: along K at (i,j)
+    const int2 *lines;  // line coordinates (1-based)
+    int count;
+    int rhs, var;       // VecId of right-hand side and of the vector being swept in place
+    int fatal_on_info;  // 1: INFO != 0 is an error (JK / IJ sweeps), 0: skip the line (IK sweep)
+    double *scratch;    // 4 * Lmax * count values
+    int lmax;
+};
+template <typename T>
+cudaError_t launch_seq_lines(const BatchView &b, const SeqLineArgs &a, cudaStream_t s);
+
+int kernel_smem_line_bytes(int cmax, int elem_bytes);
+template <typename T>
+int prepare_line_kernel(int cmax);  // sets the smem attribute, returns resident blocks per SM
+int cell_blocks_per_sm();
+
+}  // namespace mfixgpu

@@ -1,0 +1,208 @@
+"""Python mirror of the reference's linear-solver interface over the C ABI.
+
+``solve_lin_eq`` keeps SOLVE_LIN_EQ's dummy list and meaning
+(model/solve_lin_eq.f:17-78): VAR is updated in place, A_M(:,:,M) and
+B_M(:,M) come back unit-scaled as LEQ_BICGS0 leaves them
+(model/leq_bicgs.f:194-233), and the return value is IER.  It calls the
+gfortran-convention entry point ``mfixgpu_solve_lin_eq_`` exactly as a Fortran
+host would, hidden CHARACTER lengths included.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass
+
+import numpy as np
+
+from . import lib
+
+IER_UNSUPPORTED = -10
+IER_NOMEM = -11
+IER_DGTSV = -12
+IER_CUDA = -13
+IER_ARGS = -14
+IER_INCOMPLETE = -15
+IER_NOGEOM = -16
+
+_dp = C.POINTER(C.c_double)
+_ip = C.POINTER(C.c_int)
+
+
+class Stats(C.Structure):
+    _fields_ = [("ier", C.c_int), ("iterations", C.c_int), ("iter_tot_add", C.c_int), ("exit_kind", C.c_int),
+                ("line_skips", C.c_int), ("line_fallbacks", C.c_int), ("outer_steps", C.c_int), ("pad", C.c_int),
+                ("rnorm0", C.c_double), ("rnorm", C.c_double), ("seconds", C.c_double), ("device_ms", C.c_double),
+                ("jline_ms", C.c_double), ("jline_launches", C.c_int), ("pad2", C.c_int),
+                ("kernel_launches", C.c_longlong)]
+
+
+class Geom(C.Structure):
+    _fields_ = [("imax2", C.c_int), ("jmax2", C.c_int), ("kmax2", C.c_int), ("do_k", C.c_int),
+                ("dimension_3", C.c_int64)]
+
+
+class SystemC(C.Structure):
+    _fields_ = [("imax2", C.c_int), ("jmax2", C.c_int), ("kmax2", C.c_int), ("do_k", C.c_int),
+                ("dimension_3", C.c_int64), ("a_m", C.c_void_p), ("b_m", C.c_void_p), ("var", C.c_void_p),
+                ("tol", C.c_double), ("itmax", C.c_int), ("ier", C.c_int), ("iterations", C.c_int),
+                ("outer_steps", C.c_int), ("exit_kind", C.c_int), ("pad", C.c_int), ("rnorm0", C.c_double),
+                ("rnorm", C.c_double)]
+
+
+def _declare(L: C.CDLL) -> None:
+    L.mfixgpu_init_geometry.argtypes = [_ip, _ip, _ip, _ip, C.POINTER(C.c_int64), _ip]
+    L.mfixgpu_init_geometry.restype = C.c_int
+    L.mfixgpu_solve_lin_eq_.argtypes = [C.c_char_p, _ip, C.c_void_p, C.c_void_p, C.c_void_p, _ip, _ip, _ip,
+                                        C.c_char_p, _dp, C.c_char_p, _ip, C.c_size_t, C.c_size_t, C.c_size_t]
+    L.mfixgpu_solve_lin_eq_.restype = None
+    L.mfixgpu_solve_lin_eq.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                       C.c_int, C.c_int, C.c_char_p, C.c_int, C.c_double, C.c_char_p, C.c_int, _ip]
+    L.mfixgpu_solve_lin_eq.restype = None
+    L.mfixgpu_iter_tot.argtypes = [C.c_int]
+    L.mfixgpu_iter_tot.restype = C.c_int
+    L.mfixgpu_reset_iter_tot.argtypes = []
+    L.mfixgpu_reset_iter_tot.restype = None
+    L.mfixgpu_last_stats.argtypes = [C.POINTER(Stats)]
+    L.mfixgpu_last_stats.restype = C.c_int
+    L.mfixgpu_last_error.argtypes = []
+    L.mfixgpu_last_error.restype = C.c_char_p
+    L.mfixgpu_set_option.argtypes = [C.c_char_p, C.c_double]
+    L.mfixgpu_set_option.restype = C.c_int
+    L.mfixgpu_get_option.argtypes = [C.c_char_p]
+    L.mfixgpu_get_option.restype = C.c_double
+    L.mfixgpu_finalize.argtypes = []
+    L.mfixgpu_finalize.restype = None
+    L.mfixgpu_leq_matvec.argtypes = [C.POINTER(Geom), C.c_void_p, C.c_void_p, C.c_void_p]
+    L.mfixgpu_leq_matvec.restype = C.c_int
+    L.mfixgpu_leq_msolve.argtypes = [C.POINTER(Geom), C.c_void_p, C.c_void_p, C.c_void_p, C.c_char_p, C.c_char_p]
+    L.mfixgpu_leq_msolve.restype = C.c_int
+    L.mfixgpu_dot_product_par.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, _dp]
+    L.mfixgpu_dot_product_par.restype = C.c_int
+    L.mfixgpu_batch_solve.argtypes = [C.POINTER(SystemC), C.c_int, C.c_char_p, C.c_char_p, C.c_int, C.c_int]
+    L.mfixgpu_batch_solve.restype = C.c_int
+
+
+def _ptr(a: np.ndarray) -> int:
+    if a.dtype != np.float64 or not a.flags["C_CONTIGUOUS"]:
+        raise TypeError("arrays must be C-contiguous float64 (Fortran A_M/B_M order)")
+    return a.ctypes.data
+
+
+def init_geometry(imax2: int, jmax2: int, kmax2: int, do_k: int, dimension_3: int, dimension_m: int = 0) -> int:
+    """mfixgpu_init_geometry: the module data SOLVE_LIN_EQ relies on."""
+    L = lib()
+    return L.mfixgpu_init_geometry(C.byref(C.c_int(imax2)), C.byref(C.c_int(jmax2)), C.byref(C.c_int(kmax2)),
+                                   C.byref(C.c_int(do_k)), C.byref(C.c_int64(dimension_3)),
+                                   C.byref(C.c_int(dimension_m)))
+
+
+def solve_lin_eq(vname: str, vno: int, var: np.ndarray, a_m: np.ndarray, b_m: np.ndarray, m: int, itmax: int,
+                 method: int, sweep: str, tol1: float, pc: str) -> int:
+    """SOLVE_LIN_EQ(VNAME, VNO, VAR, A_M, B_M, M, ITMAX, METHOD, SWEEP, TOL1, PC, IER) -> IER.
+
+    ``a_m`` is A_M(DIMENSION_3, -3:3, 0:DIMENSION_M) in Fortran order, i.e. a
+    C-contiguous array of shape (DIMENSION_M+1, 7, DIMENSION_3) (or (7, N) for
+    one phase); ``b_m`` is B_M(DIMENSION_3, 0:DIMENSION_M) as (DIMENSION_M+1, N)
+    (or (N,)).  VAR, A_M(:,:,M) and B_M(:,M) are updated in place.
+    """
+    L = lib()
+    ier = C.c_int(0)
+    vn = vname.encode()
+    sw = sweep.encode()
+    pcs = pc.encode()
+    L.mfixgpu_solve_lin_eq_(vn, C.byref(C.c_int(vno)), _ptr(var), _ptr(a_m), _ptr(b_m), C.byref(C.c_int(m)),
+                            C.byref(C.c_int(itmax)), C.byref(C.c_int(method)), sw, C.byref(C.c_double(tol1)), pcs,
+                            C.byref(ier), len(vn), len(sw), len(pcs))
+    return ier.value
+
+
+def last_stats() -> dict:
+    s = Stats()
+    lib().mfixgpu_last_stats(C.byref(s))
+    return {k: getattr(s, k) for k, _ in Stats._fields_ if not k.startswith("pad")}
+
+
+def last_error() -> str:
+    return lib().mfixgpu_last_error().decode()
+
+
+def iter_tot(vno: int) -> int:
+    return lib().mfixgpu_iter_tot(vno)
+
+
+def reset_iter_tot() -> None:
+    lib().mfixgpu_reset_iter_tot()
+
+
+def set_option(name: str, value: float) -> int:
+    return lib().mfixgpu_set_option(name.encode(), float(value))
+
+
+def get_option(name: str) -> float:
+    return lib().mfixgpu_get_option(name.encode())
+
+
+def finalize() -> None:
+    lib().mfixgpu_finalize()
+
+
+def geom(imax2: int, jmax2: int, kmax2: int, do_k: int) -> Geom:
+    return Geom(imax2, jmax2, kmax2, do_k, imax2 * jmax2 * kmax2)
+
+
+def leq_matvec(g: Geom, a_dev: int, var_dev: int, avar_dev: int) -> int:
+    """LEQ_MATVEC on device pointers (ints, e.g. torch.Tensor.data_ptr())."""
+    return lib().mfixgpu_leq_matvec(C.byref(g), a_dev, var_dev, avar_dev)
+
+
+def leq_msolve(g: Geom, b_dev: int, a_dev: int, var_dev: int, sweep: str = "RSRS", pc: str = "LINE") -> int:
+    return lib().mfixgpu_leq_msolve(C.byref(g), b_dev, a_dev, var_dev, sweep.ljust(4)[:4].encode(),
+                                    pc.ljust(4)[:4].encode())
+
+
+def dot_product_par(r1_dev: int, r2_dev: int, n: int) -> float:
+    out = C.c_double(0.0)
+    rc = lib().mfixgpu_dot_product_par(r1_dev, r2_dev, n, C.byref(out))
+    if rc:
+        raise RuntimeError(f"mfixgpu_dot_product_par failed ({rc}): {last_error()}")
+    return out.value
+
+
+@dataclass
+class BatchResult:
+    ier: int
+    iterations: int
+    outer_steps: int
+    exit_kind: int
+    rnorm0: float
+    rnorm: float
+
+
+def batch_solve(systems, sweep: str = "RSRS", pc: str = "LINE", precision: int = 0, on_device: bool = False,
+                pointers=None):
+    """mfixgpu_batch_solve over host :class:`mfix_b200.systems.System` objects (solved in
+    place), or over device pointers given as ``pointers[q] = (a, b, x)`` with
+    ``on_device=True``.  Returns (rc, [BatchResult...])."""
+    arr = (SystemC * len(systems))()
+    for q, s in enumerate(systems):
+        arr[q].imax2, arr[q].jmax2, arr[q].kmax2, arr[q].do_k = s.imax2, s.jmax2, s.kmax2, s.do_k
+        arr[q].dimension_3 = s.n
+        if on_device:
+            arr[q].a_m, arr[q].b_m, arr[q].var = pointers[q]
+        else:
+            arr[q].a_m, arr[q].b_m, arr[q].var = _ptr(s.a), _ptr(s.b), _ptr(s.x)
+        arr[q].tol = s.tol
+        arr[q].itmax = s.itmax
+    rc = lib().mfixgpu_batch_solve(arr, len(systems), sweep.ljust(4)[:4].encode(), pc.ljust(4)[:4].encode(),
+                                   int(precision), int(on_device))
+    res = [BatchResult(arr[q].ier, arr[q].iterations, arr[q].outer_steps, arr[q].exit_kind, arr[q].rnorm0,
+                       arr[q].rnorm) for q in range(len(systems))]
+    return rc, res
+
+
+def solve_system(s, method: int = 2, sweep: str = "RSRS", pc: str = "LINE", vno: int = 1) -> int:
+    """Drop-in solve of one :class:`mfix_b200.systems.System` (in place)."""
+    rc = init_geometry(s.imax2, s.jmax2, s.kmax2, s.do_k, s.n, 0)
+    if rc:
+        return rc
+    return solve_lin_eq("Test", vno, s.x, s.a, s.b, 0, s.itmax, method, sweep, s.tol, pc)

@@ -1,0 +1,259 @@
+"""Seeded synthetic MFIX systems in the A_M / B_M layout.
+
+Arrays follow the reference's Fortran storage: ``a`` has shape ``(7, N)`` with
+``a[d + 3]`` the contiguous diagonal ``A_M(:, d)`` (so the buffer is exactly
+``A_M(DIMENSION_3, -3:3)`` in column-major order); the cell index puts J
+fastest, then I, then K (model/include/functions.inc:37-42), and the grid
+carries the one-cell wall layer (model/set_max2.f:48-66).  Wall rows follow
+INIT_AB_M (model/init_ab_m.f:20-78): ``A(0) = -1``, other diagonals 0, ``B = 0``.
+
+Every random draw comes from a counter-based splitmix64 stream keyed by
+(seed, tag, index), so any subset of a system can be regenerated and the
+values do not depend on evaluation order.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass
+
+import numpy as np
+
+_M1 = np.uint64(0xBF58476D1CE4E5B9)
+_M2 = np.uint64(0x94D049BB133111EB)
+_GOLD = 0x9E3779B97F4A7C15
+_TAGK = 0xD1B54A32D192ED03
+_OFF = 0x632BE59BD9B4E019
+_MASK = (1 << 64) - 1
+
+
+def _mix64(z: np.ndarray) -> np.ndarray:
+    with np.errstate(over="ignore"):
+        z = (z ^ (z >> np.uint64(30))) * _M1
+        z = (z ^ (z >> np.uint64(27))) * _M2
+        return z ^ (z >> np.uint64(31))
+
+
+def _mix64_int(z: int) -> int:
+    z &= _MASK
+    z = ((z ^ (z >> 30)) * 0xBF58476D1CE4E5B9) & _MASK
+    z = ((z ^ (z >> 27)) * 0x94D049BB133111EB) & _MASK
+    return z ^ (z >> 31)
+
+
+def uniform(seed: int, tag: int, idx) -> np.ndarray:
+    """U[0,1) draws of stream (seed, tag) at counter positions ``idx``."""
+    key = _mix64_int((seed * _GOLD + tag * _TAGK + _OFF) & _MASK)
+    idx = np.asarray(idx, dtype=np.uint64)
+    with np.errstate(over="ignore"):
+        v = _mix64(np.uint64(key) + (idx + np.uint64(1)) * np.uint64(_GOLD))
+    return (v >> np.uint64(11)).astype(np.float64) * (2.0 ** -53)
+
+
+def normal(seed: int, tag: int, idx, sigma: float) -> np.ndarray:
+    """N(0, sigma) by Box-Muller from streams (tag, tag+1)."""
+    u1 = 1.0 - uniform(seed, tag, idx)  # (0, 1]
+    u2 = uniform(seed, tag + 1, idx)
+    return sigma * np.sqrt(-2.0 * np.log(u1)) * np.cos(2.0 * np.pi * u2)
+
+
+@dataclass
+class System:
+    """One A_M / B_M / VAR triple on a box of (imax2, jmax2, kmax2) cells."""
+    imax2: int
+    jmax2: int
+    kmax2: int
+    do_k: int
+    a: np.ndarray  # (7, n) float64
+    b: np.ndarray  # (n,)
+    x: np.ndarray  # (n,) initial guess
+    tol: float = 1e-8
+    itmax: int = 500
+    kind: str = ""
+
+    @property
+    def n(self) -> int:
+        return self.imax2 * self.jmax2 * self.kmax2
+
+    def copy(self) -> "System":
+        return System(self.imax2, self.jmax2, self.kmax2, self.do_k, self.a.copy(), self.b.copy(),
+                      self.x.copy(), self.tol, self.itmax, self.kind)
+
+
+def _grid(imax: int, jmax: int, kmax: int, do_k: bool):
+    imax2, jmax2 = imax + 2, jmax + 2
+    kmax2 = kmax + 2 if do_k else 1
+    return imax2, jmax2, kmax2
+
+
+def _interior(imax2, jmax2, kmax2, do_k):
+    """Boolean [k, i, j] mask of interior (non wall-layer) cells."""
+    k = np.arange(kmax2)[:, None, None]
+    i = np.arange(imax2)[None, :, None]
+    j = np.arange(jmax2)[None, None, :]
+    m = (i >= 1) & (i <= imax2 - 2) & (j >= 1) & (j <= jmax2 - 2)
+    if do_k:
+        m = m & (k >= 1) & (k <= kmax2 - 2)
+    return np.broadcast_to(m, (kmax2, imax2, jmax2))
+
+
+def _assemble(imax2, jmax2, kmax2, do_k, face_fn, centre_factor, seed, b_tag):
+    """Build A and B from a per-face coefficient function.
+
+    face_fn(axis, low_idx, high_idx) -> (coef_in_low_row, coef_in_high_row) for
+    the faces between interior cells along `axis` (0: I, 1: J, 2: K).
+    """
+    n = imax2 * jmax2 * kmax2
+    shape = (kmax2, imax2, jmax2)
+    a = np.zeros((7, n), dtype=np.float64)
+    A = a.reshape(7, *shape)
+    inter = _interior(imax2, jmax2, kmax2, do_k)
+    flat = np.arange(n, dtype=np.int64).reshape(shape)
+    # (axis, numpy axis of the [k,i,j] grid, diagonal index in low row, in high row)
+    axes = [(0, 1, 1, -1), (1, 2, 2, -2)]
+    if do_k:
+        axes.append((2, 0, 3, -3))
+    for axis, npax, d_low, d_high in axes:
+        sl_lo = [slice(None)] * 3
+        sl_hi = [slice(None)] * 3
+        sl_lo[npax] = slice(0, shape[npax] - 1)
+        sl_hi[npax] = slice(1, shape[npax])
+        lo, hi = tuple(sl_lo), tuple(sl_hi)
+        both = inter[lo] & inter[hi]  # faces touching the wall layer stay zero
+        low_idx = flat[lo][both]
+        high_idx = flat[hi][both]
+        c_low, c_high = face_fn(axis, low_idx, high_idx)
+        a[d_low + 3][low_idx] = c_low
+        a[d_high + 3][high_idx] = c_high
+    off = a[[0, 1, 2, 4, 5, 6]].sum(axis=0)
+    wall = ~inter.reshape(-1)
+    a[3] = -off * centre_factor
+    a[:, wall] = 0.0
+    a[3][wall] = -1.0
+    b = 2.0 * uniform(seed, b_tag, np.arange(n)) - 1.0
+    b[wall] = 0.0
+    del A
+    return a, b
+
+
+def conv_diff(imax: int, jmax: int, kmax: int, seed: int = 0, do_k: bool = True, itmax: int = 500,
+              tol: float = 1e-8) -> System:
+    """3-D 7-point upwind convection-diffusion system (the 64^3 / 256^3 workloads).
+
+    Per interior face between cells P (low) and Q (high): D ~ U[0.5, 1.5] and
+    F ~ N(0, 0.5) (standard deviation 0.5); row P gets a_Q = D + max(-F, 0),
+    row Q gets a_P = D + max(F, 0).  Faces touching the wall layer are zero;
+    A(0) = -(sum of the remaining a_nb)(1 + 1e-3); B ~ U[-1, 1] on interior cells.
+    """
+    imax2, jmax2, kmax2 = _grid(imax, jmax, kmax, do_k)
+
+    def face(axis, lo, hi):
+        D = 0.5 + uniform(seed, 1 + 4 * axis, lo)
+        F = normal(seed, 2 + 4 * axis, lo, 0.5)
+        return D + np.maximum(-F, 0.0), D + np.maximum(F, 0.0)
+
+    a, b = _assemble(imax2, jmax2, kmax2, do_k, face, 1.0 + 1e-3, seed, 20)
+    return System(imax2, jmax2, kmax2, int(do_k), a, b, np.zeros(imax2 * jmax2 * kmax2), tol, itmax,
+                  "conv_diff")
+
+
+def void_fraction(imax2, jmax2, kmax2, seed, nspheres=40, rmin=6.0, rmax=20.0):
+    """eps_g field: 0.4 background, spheres of eps_g = 0.95 (radius U[rmin, rmax],
+    centres uniform over the interior)."""
+    eps = np.full((kmax2, imax2, jmax2), 0.4)
+    s = np.arange(nspheres)
+    ci = 1.0 + uniform(seed, 30, s) * (imax2 - 2)
+    cj = 1.0 + uniform(seed, 31, s) * (jmax2 - 2)
+    ck = 1.0 + uniform(seed, 32, s) * (kmax2 - 2)
+    rr = rmin + uniform(seed, 33, s) * (rmax - rmin)
+    k = np.arange(kmax2)[:, None, None]
+    i = np.arange(imax2)[None, :, None]
+    j = np.arange(jmax2)[None, None, :]
+    for q in range(nspheres):
+        r2 = rr[q] * rr[q]
+        klo, khi = int(max(0, np.floor(ck[q] - rr[q]))), int(min(kmax2, np.ceil(ck[q] + rr[q]) + 1))
+        ilo, ihi = int(max(0, np.floor(ci[q] - rr[q]))), int(min(imax2, np.ceil(ci[q] + rr[q]) + 1))
+        jlo, jhi = int(max(0, np.floor(cj[q] - rr[q]))), int(min(jmax2, np.ceil(cj[q] + rr[q]) + 1))
+        sub = ((k[klo:khi] - ck[q]) ** 2 + (i[:, ilo:ihi] - ci[q]) ** 2 + (j[:, :, jlo:jhi] - cj[q]) ** 2) <= r2
+        eps[klo:khi, ilo:ihi, jlo:jhi][sub] = 0.95
+    return eps.reshape(-1)
+
+
+def pressure_like(imax: int, jmax: int, kmax: int, seed: int = 0, nspheres: int = 40, rmin: float = 6.0,
+                  rmax: float = 20.0, delta: float = 1e-6, itmax: int = 5000, tol: float = 1e-8) -> System:
+    """Symmetric 7-point diffusion with face coefficient eps_f * D, D ~ U[0.5, 1.5],
+    eps_f the arithmetic mean of the two cells' eps_g, centre -(sum)(1 + delta)
+    (the 192x384x192 pressure-correction-like workload)."""
+    imax2, jmax2, kmax2 = _grid(imax, jmax, kmax, True)
+    eps = void_fraction(imax2, jmax2, kmax2, seed, nspheres, rmin, rmax)
+
+    def face(axis, lo, hi):
+        D = 0.5 + uniform(seed, 40 + axis, lo)
+        c = 0.5 * (eps[lo] + eps[hi]) * D
+        return c, c
+
+    a, b = _assemble(imax2, jmax2, kmax2, True, face, 1.0 + delta, seed, 44)
+    return System(imax2, jmax2, kmax2, 1, a, b, np.zeros(imax2 * jmax2 * kmax2), tol, itmax, "pressure_like")
+
+
+def known_answer(imax: int, jmax: int, kmax: int, seed: int = 0, do_k: bool = True):
+    """The recipe of model/test_lin_eq.f:63-117: off-diagonals U[0,1), A(0) =
+    -70*max(u, 0.1), x_act = u + 1e-5, b = A x_act.  Coefficients that point
+    out of the array are zeroed so that b = A x_act holds for the clamped
+    neighbours of LEQ_MATVEC as well.  Returns (system, x_act)."""
+    imax2, jmax2, kmax2 = _grid(imax, jmax, kmax, do_k)
+    n = imax2 * jmax2 * kmax2
+    idx = np.arange(n)
+    a = np.zeros((7, n))
+    for d in range(7):
+        a[d] = uniform(seed, 50 + d, idx)
+    a[3] = -np.maximum(uniform(seed, 57, idx), 0.1) * 70.0
+    if not do_k:
+        a[0] = 0.0
+        a[6] = 0.0
+    j = idx % jmax2
+    i = (idx // jmax2) % imax2
+    k = idx // (jmax2 * imax2)
+    a[1][j == 0] = 0.0
+    a[5][j == jmax2 - 1] = 0.0
+    a[2][i == 0] = 0.0
+    a[4][i == imax2 - 1] = 0.0
+    if do_k:
+        a[0][k == 0] = 0.0
+        a[6][k == kmax2 - 1] = 0.0
+    x_act = uniform(seed, 58, idx) + 1e-5
+    b = matvec_np(imax2, jmax2, kmax2, do_k, a, x_act)
+    return System(imax2, jmax2, kmax2, int(do_k), a, b, np.zeros(n), 1e-10, 500, "known_answer"), x_act
+
+
+def matvec_np(imax2, jmax2, kmax2, do_k, a, x):
+    """A*x with the clamped neighbours of LEQ_MATVEC (numpy, any size)."""
+    shape = (kmax2, imax2, jmax2)
+    X = x.reshape(shape)
+
+    def shift(ax, s):
+        idx = np.arange(shape[ax])
+        src = np.clip(idx + s, 0, shape[ax] - 1)
+        return np.take(X, src, axis=ax)
+
+    A = a.reshape(7, *shape)
+    y = A[1] * shift(2, -1) + A[2] * shift(1, -1) + A[3] * X + A[4] * shift(1, 1) + A[5] * shift(2, 1)
+    if do_k:
+        y = y + A[0] * shift(0, -1)
+        y = y + A[6] * shift(0, 1)
+    return y.reshape(-1)
+
+
+def batch_sizes(count: int, seed: int, lo: int = 16, hi: int = 96):
+    """Per-axis sizes drawn uniformly from lo..hi for `count` systems."""
+    s = np.arange(count)
+    out = []
+    for ax in range(3):
+        u = uniform(seed, 60 + ax, s)
+        out.append(lo + np.minimum((u * (hi - lo + 1)).astype(np.int64), hi - lo))
+    return [(int(out[0][q]), int(out[1][q]), int(out[2][q])) for q in range(count)]
+
+
+def coefficient_contrast(sys: System) -> float:
+    """max/min over interior rows of the nonzero off-diagonal coefficients."""
+    off = sys.a[[0, 1, 2, 4, 5, 6]]
+    nz = off[off > 0]
+    return float(nz.max() / nz.min()) if nz.size else 1.0

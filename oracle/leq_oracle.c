@@ -1,0 +1,655 @@
+/*
+ * leq_oracle.c -- TEST INFRASTRUCTURE ONLY (see leq_oracle.h).
+ *
+ * Plain-C restatement of the reference's FP64 LEQ_BICGS path for a serial,
+ * non-cyclic, non-cut-cell MFIX box.  It is the parity checker for the CUDA
+ * library and, compiled with OpenMP, the timed CPU baseline.  The OpenMP
+ * regions sit where the reference has them (model/leq_bicgs.f:211,285,303,335,
+ * 365,432; model/leqsol_mod.f:188-189,216-217,497,510); the dot products stay
+ * serial, as DOT_PRODUCT_PAR is in a serial run (model/leqsol_mod.f:1125-1136).
+ *
+ * Build with -ffp-contract=off so that every product and sum rounds the way a
+ * non-FMA Fortran build of the reference rounds it.
+ */
+#include "leq_oracle.h"
+
+#include <float.h>
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#define DIAG(a, g, d) ((a) + (int64_t)((d) + 3) * (g)->n)
+
+static inline int64_t cell(const orc_geom *g, int i, int j, int k)
+{
+    /* FUNIJK for a serial run: ijk = j + c0 + i*c1 + k*c2 with c0 = -c1 - c2 + 0 (0-based here) */
+    return (int64_t)(j - 1) + (int64_t)(i - 1) * g->jmax2 + (int64_t)(k - 1) * g->jmax2 * g->imax2;
+}
+
+int orc_num_threads(void)
+{
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+/* ------------------------------------------------------------------ random stream */
+/* splitmix64 output function (Steele, Lea & Flood, OOPSLA 2014), used counter-wise so
+ * that every cell's draw is independent of evaluation order.  Replaces Fortran
+ * RANDOM_NUMBER in model/leq_bicgs.f:298. */
+static inline uint64_t mix64(uint64_t z)
+{
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ULL;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBULL;
+    return z ^ (z >> 31);
+}
+
+double orc_uniform(uint64_t seed, uint64_t tag, uint64_t idx)
+{
+    uint64_t key = mix64(seed * 0x9E3779B97F4A7C15ULL + tag * 0xD1B54A32D192ED03ULL + 0x632BE59BD9B4E019ULL);
+    uint64_t v = mix64(key + (idx + 1) * 0x9E3779B97F4A7C15ULL);
+    return (double)(v >> 11) * 0x1.0p-53;
+}
+
+/* ------------------------------------------------------------------ LEQ_MATVEC */
+/* model/leqsol_mod.f:166-254 (non-reindexed branch).  The core-cell loop and the
+ * boundary loop evaluate the same expression; only the neighbour offsets differ,
+ * and for a serial box they are the clamped ones of model/set_increments.f:80-109. */
+void orc_matvec(const orc_geom *g, const double *a, const double *x, double *y)
+{
+    const int64_t c1 = g->jmax2, c2 = (int64_t)g->jmax2 * g->imax2;
+    const double *am3 = DIAG(a, g, -3), *am2 = DIAG(a, g, -2), *am1 = DIAG(a, g, -1);
+    const double *a0 = DIAG(a, g, 0), *ap1 = DIAG(a, g, 1), *ap2 = DIAG(a, g, 2), *ap3 = DIAG(a, g, 3);
+    const int imax2 = g->imax2, jmax2 = g->jmax2, kmax2 = g->kmax2, do_k = g->do_k;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 1; k <= kmax2; ++k) {
+        for (int i = 1; i <= imax2; ++i) {
+            const int64_t im = i > 1 ? -c1 : 0, ip = i < imax2 ? c1 : 0;
+            const int64_t km = (do_k && k > 1) ? -c2 : 0, kp = (do_k && k < kmax2) ? c2 : 0;
+            const int64_t base = cell(g, i, 1, k);
+            for (int j = 1; j <= jmax2; ++j) {
+                const int64_t p = base + (j - 1);
+                const int64_t jm = j > 1 ? -1 : 0, jp = j < jmax2 ? 1 : 0;
+                double s = am2[p] * x[p + jm] + am1[p] * x[p + im] + a0[p] * x[p] + ap1[p] * x[p + ip] +
+                           ap2[p] * x[p + jp];
+                if (do_k) {
+                    s = s + am3[p] * x[p + km];
+                    s = s + ap3[p] * x[p + kp];
+                }
+                y[p] = s;
+            }
+        }
+    }
+}
+
+/* ------------------------------------------------------------------ DOT_PRODUCT_PAR */
+/* Serial run: the Fortran DOT_PRODUCT intrinsic over the whole array,
+ * model/leqsol_mod.f:1125-1127, accumulated in index order. */
+double orc_dot(const double *x, const double *y, int64_t n)
+{
+    double s = 0.0;
+    for (int64_t p = 0; p < n; ++p) s = s + x[p] * y[p];
+    return s;
+}
+
+/* ------------------------------------------------------------------ DGTSV */
+/* Gaussian elimination with partial pivoting on a tridiagonal, NRHS = 1:
+ * model/DGTSV.f:92-163 (factor) and :231-246 (back solve).  Zero-based arrays:
+ * dl[0..n-2], d[0..n-1], du[0..n-2], b[0..n-1].  Returns INFO. */
+int orc_dgtsv(int n, double *dl, double *d, double *du, double *b)
+{
+    if (n < 0) return -1;
+    if (n == 0) return 0;
+    double fact, temp;
+    for (int i = 0; i < n - 2; ++i) {
+        if (fabs(d[i]) >= fabs(dl[i])) {
+            if (d[i] != 0.0) {
+                fact = dl[i] / d[i];
+                d[i + 1] = d[i + 1] - fact * du[i];
+                b[i + 1] = b[i + 1] - fact * b[i];
+            } else {
+                return i + 1;
+            }
+            dl[i] = 0.0;
+        } else {
+            fact = d[i] / dl[i];
+            d[i] = dl[i];
+            temp = d[i + 1];
+            d[i + 1] = du[i] - fact * temp;
+            dl[i] = du[i + 1];
+            du[i + 1] = -fact * dl[i];
+            du[i] = temp;
+            temp = b[i];
+            b[i] = b[i + 1];
+            b[i + 1] = temp - fact * b[i + 1];
+        }
+    }
+    if (n > 1) {
+        const int i = n - 2;
+        if (fabs(d[i]) >= fabs(dl[i])) {
+            if (d[i] != 0.0) {
+                fact = dl[i] / d[i];
+                d[i + 1] = d[i + 1] - fact * du[i];
+                b[i + 1] = b[i + 1] - fact * b[i];
+            } else {
+                return i + 1;
+            }
+        } else {
+            fact = d[i] / dl[i];
+            d[i] = dl[i];
+            temp = d[i + 1];
+            d[i + 1] = du[i] - fact * temp;
+            du[i] = temp;
+            temp = b[i];
+            b[i] = b[i + 1];
+            b[i + 1] = temp - fact * b[i + 1];
+        }
+    }
+    if (d[n - 1] == 0.0) return n;
+    b[n - 1] = b[n - 1] / d[n - 1];
+    if (n > 1) b[n - 2] = (b[n - 2] - du[n - 2] * b[n - 1]) / d[n - 2];
+    for (int i = n - 3; i >= 0; --i) b[i] = (b[i] - du[i] * b[i + 1] - dl[i] * b[i + 2]) / d[i];
+    return 0;
+}
+
+/* ------------------------------------------------------------------ line sweeps */
+/* LEQ_IKSWEEP, model/leqsol_mod.f:851-921: one J-line at (I,K).  On INFO != 0 the
+ * line is left as it was (:910-914). */
+int orc_iksweep(const orc_geom *g, int i, int k, double *var, const double *a, const double *b)
+{
+    const int L = g->jmax2;
+    const int64_t c1 = g->jmax2, c2 = (int64_t)g->jmax2 * g->imax2;
+    const int64_t im = i > 1 ? -c1 : 0, ip = i < g->imax2 ? c1 : 0;
+    const int64_t km = k > 1 ? -c2 : 0, kp = k < g->kmax2 ? c2 : 0;
+    const double *am3 = DIAG(a, g, -3), *am2 = DIAG(a, g, -2), *am1 = DIAG(a, g, -1);
+    const double *a0 = DIAG(a, g, 0), *ap1 = DIAG(a, g, 1), *ap2 = DIAG(a, g, 2), *ap3 = DIAG(a, g, 3);
+    double *buf = (double *)malloc(sizeof(double) * 4 * (size_t)(L + 1));
+    double *cc = buf, *dd = buf + (L + 1), *ee = buf + 2 * (L + 1), *bb = buf + 3 * (L + 1);
+    const int64_t base = cell(g, i, 1, k);
+    for (int j = 0; j < L; ++j) {
+        const int64_t p = base + j;
+        dd[j] = a0[p];
+        cc[j] = am2[p];
+        ee[j] = ap2[p];
+        bb[j] = b[p] - am1[p] * var[p + im] - ap1[p] * var[p + ip] - am3[p] * var[p + km] - ap3[p] * var[p + kp];
+    }
+    cc[0] = 0.0;
+    ee[L - 1] = 0.0;
+    const int info = orc_dgtsv(L, cc + 1, dd, ee, bb);
+    if (info == 0)
+        for (int j = 0; j < L; ++j) var[base + j] = bb[j];
+    free(buf);
+    return info;
+}
+
+/* LEQ_ISWEEP, model/leqsol_mod.f:767-834: the 2-D J-line at I (K = 1). */
+int orc_isweep(const orc_geom *g, int i, double *var, const double *a, const double *b)
+{
+    const int L = g->jmax2;
+    const int64_t c1 = g->jmax2;
+    const int64_t im = i > 1 ? -c1 : 0, ip = i < g->imax2 ? c1 : 0;
+    const double *am2 = DIAG(a, g, -2), *am1 = DIAG(a, g, -1);
+    const double *a0 = DIAG(a, g, 0), *ap1 = DIAG(a, g, 1), *ap2 = DIAG(a, g, 2);
+    double *buf = (double *)malloc(sizeof(double) * 4 * (size_t)(L + 1));
+    double *cc = buf, *dd = buf + (L + 1), *ee = buf + 2 * (L + 1), *bb = buf + 3 * (L + 1);
+    const int64_t base = cell(g, i, 1, 1);
+    for (int j = 0; j < L; ++j) {
+        const int64_t p = base + j;
+        dd[j] = a0[p];
+        cc[j] = am2[p];
+        ee[j] = ap2[p];
+        bb[j] = b[p] - am1[p] * var[p + im] - ap1[p] * var[p + ip];
+    }
+    cc[0] = 0.0;
+    ee[L - 1] = 0.0;
+    const int info = orc_dgtsv(L, cc + 1, dd, ee, bb);
+    if (info == 0)
+        for (int j = 0; j < L; ++j) var[base + j] = bb[j];
+    free(buf);
+    return info;
+}
+
+/* LEQ_JKSWEEP, model/leqsol_mod.f:939-1004: the I-line at (J,K). */
+int orc_jksweep(const orc_geom *g, int j, int k, double *var, const double *a, const double *b)
+{
+    const int L = g->imax2;
+    const int64_t c1 = g->jmax2, c2 = (int64_t)g->jmax2 * g->imax2;
+    const int64_t jm = j > 1 ? -1 : 0, jp = j < g->jmax2 ? 1 : 0;
+    const int64_t km = k > 1 ? -c2 : 0, kp = k < g->kmax2 ? c2 : 0;
+    const double *am3 = DIAG(a, g, -3), *am2 = DIAG(a, g, -2), *am1 = DIAG(a, g, -1);
+    const double *a0 = DIAG(a, g, 0), *ap1 = DIAG(a, g, 1), *ap2 = DIAG(a, g, 2), *ap3 = DIAG(a, g, 3);
+    double *buf = (double *)malloc(sizeof(double) * 4 * (size_t)(L + 1));
+    double *cc = buf, *dd = buf + (L + 1), *ee = buf + 2 * (L + 1), *bb = buf + 3 * (L + 1);
+    for (int i = 0; i < L; ++i) {
+        const int64_t p = cell(g, i + 1, j, k);
+        dd[i] = a0[p];
+        cc[i] = am1[p];
+        ee[i] = ap1[p];
+        bb[i] = b[p] - am2[p] * var[p + jm] - ap2[p] * var[p + jp] - am3[p] * var[p + km] - ap3[p] * var[p + kp];
+    }
+    (void)c1;
+    cc[0] = 0.0;
+    ee[L - 1] = 0.0;
+    const int info = orc_dgtsv(L, cc + 1, dd, ee, bb);
+    if (info == 0)
+        for (int i = 0; i < L; ++i) var[cell(g, i + 1, j, k)] = bb[i];
+    free(buf);
+    return info;
+}
+
+/* LEQ_IJSWEEP, model/leqsol_mod.f:1021-1086: the K-line at (I,J). */
+int orc_ijsweep(const orc_geom *g, int i, int j, double *var, const double *a, const double *b)
+{
+    const int L = g->kmax2;
+    const int64_t c1 = g->jmax2;
+    const int64_t jm = j > 1 ? -1 : 0, jp = j < g->jmax2 ? 1 : 0;
+    const int64_t im = i > 1 ? -c1 : 0, ip = i < g->imax2 ? c1 : 0;
+    const double *am3 = DIAG(a, g, -3), *am2 = DIAG(a, g, -2), *am1 = DIAG(a, g, -1);
+    const double *a0 = DIAG(a, g, 0), *ap1 = DIAG(a, g, 1), *ap2 = DIAG(a, g, 2), *ap3 = DIAG(a, g, 3);
+    double *buf = (double *)malloc(sizeof(double) * 4 * (size_t)(L + 1));
+    double *cc = buf, *dd = buf + (L + 1), *ee = buf + 2 * (L + 1), *bb = buf + 3 * (L + 1);
+    for (int k = 0; k < L; ++k) {
+        const int64_t p = cell(g, i, j, k + 1);
+        dd[k] = a0[p];
+        cc[k] = am3[p];
+        ee[k] = ap3[p];
+        bb[k] = b[p] - am2[p] * var[p + jm] - ap2[p] * var[p + jp] - am1[p] * var[p + im] - ap1[p] * var[p + ip];
+    }
+    cc[0] = 0.0;
+    ee[L - 1] = 0.0;
+    const int info = orc_dgtsv(L, cc + 1, dd, ee, bb);
+    if (info == 0)
+        for (int k = 0; k < L; ++k) var[cell(g, i, j, k + 1)] = bb[k];
+    free(buf);
+    return info;
+}
+
+/* ------------------------------------------------------------------ LEQ_MSOLVE */
+/* model/leqsol_mod.f:286-598: Var = B (SETGUESS, :342-357), then one action per
+ * character of the four-character sweep string.  Returns 0, or -12 when DGTSV
+ * fails inside a JK/IJ sweep (the reference aborts there, :991-996, :1073-1078). */
+int orc_msolve(const orc_geom *g, const double *b, const double *a, double *var, const char *sweep,
+               int *skips)
+{
+    const int64_t n = g->n;
+    int nskip = 0;
+    memcpy(var, b, sizeof(double) * (size_t)n);
+    for (int it = 0; it < 4; ++it) {
+        const char ch = sweep[it];
+        const int do_i = (ch == 'I' || ch == 'i');
+        const int do_kk = (ch == 'K' || ch == 'k');
+        const int do_all = (ch == 'A' || ch == 'a');
+        const int do_rb = (ch == 'R' || ch == 'r');
+        if (!g->do_k) {
+            /* two-dimensional branch, :372-391 */
+            if (do_i)
+                for (int i = 1; i <= g->imax2; ++i) nskip += orc_isweep(g, i, var, a, b) != 0;
+            if (do_rb) {
+                int s1 = 0, s2 = 0;
+#pragma omp parallel for reduction(+ : s1) schedule(static)
+                for (int i = 1; i <= g->imax2; i += 2) s1 += orc_isweep(g, i, var, a, b) != 0;
+#pragma omp parallel for reduction(+ : s2) schedule(static)
+                for (int i = 2; i <= g->imax2; i += 2) s2 += orc_isweep(g, i, var, a, b) != 0;
+                nskip += s1 + s2;
+            }
+            continue;
+        }
+        if (do_all) {
+            /* :398-470, every loop sequential as in the reference */
+            const int jsize = g->jmax2, ksize = g->kmax2, isize = g->imax2;
+            for (int icase = 1; icase <= 2; ++icase)
+                for (int jk = icase; jk <= ksize * jsize; jk += 2) {
+                    int k = (jk % jsize != 0) ? jk / jsize + 1 : jk / jsize;
+                    int j = (jk - 1 - (k - 1) * jsize) + 1 + (k % 2);
+                    if (j > jsize) j = j - jsize;
+                    if (orc_jksweep(g, j, k, var, a, b) != 0) return -12;
+                }
+            for (int icase = 1; icase <= 2; ++icase)
+                for (int ij = icase; ij <= jsize * isize; ij += 2) {
+                    int j = (ij % isize != 0) ? ij / isize + 1 : ij / isize;
+                    int i = (ij - 1 - (j - 1) * isize) + 1 + (j % 2);
+                    if (i > isize) i = i - isize;
+                    if (orc_ijsweep(g, i, j, var, a, b) != 0) return -12;
+                }
+            for (int icase = 1; icase <= 2; ++icase)
+                for (int ik = icase; ik <= ksize * isize; ik += 2) {
+                    int k = (ik % isize != 0) ? ik / isize + 1 : ik / isize;
+                    int i = (ik - 1 - (k - 1) * isize) + 1 + (k % 2);
+                    if (i > isize) i = i - isize;
+                    nskip += orc_iksweep(g, i, k, var, a, b) != 0;
+                }
+        }
+        if (do_rb) {
+            /* :497-522: first the lines with (i+k) odd, then (i+k) even */
+            int s1 = 0, s2 = 0;
+#pragma omp parallel for reduction(+ : s1) schedule(static)
+            for (int k = 1; k <= g->kmax2; ++k)
+                for (int i = (k % 2 != 0) ? 2 : 1; i <= g->imax2; i += 2) s1 += orc_iksweep(g, i, k, var, a, b) != 0;
+#pragma omp parallel for reduction(+ : s2) schedule(static)
+            for (int k = 1; k <= g->kmax2; ++k)
+                for (int i = (k % 2 != 0) ? 1 : 2; i <= g->imax2; i += 2) s2 += orc_iksweep(g, i, k, var, a, b) != 0;
+            nskip += s1 + s2;
+        }
+        if (do_i) /* :567-574 */
+            for (int k = 1; k <= g->kmax2; ++k)
+                for (int i = 1; i <= g->imax2; ++i) nskip += orc_iksweep(g, i, k, var, a, b) != 0;
+        if (do_kk) /* :575-582 */
+            for (int i = 1; i <= g->imax2; ++i)
+                for (int k = 1; k <= g->kmax2; ++k) nskip += orc_iksweep(g, i, k, var, a, b) != 0;
+    }
+    if (skips) *skips += nskip;
+    return 0;
+}
+
+/* LEQ_MSOLVE1 (DIAG), model/leqsol_mod.f:719-746 */
+void orc_msolve1(const orc_geom *g, const double *b, const double *a, double *var)
+{
+    const double *a0 = DIAG(a, g, 0);
+    const int64_t n = g->n;
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < n; ++p) var[p] = b[p] / a0[p];
+}
+
+/* ------------------------------------------------------------------ unit scaling */
+/* model/leq_bicgs.f:194-233: every row divided by max|A(ijk,:)| through a
+ * multiplication by its reciprocal; a zero row flags IER = -2. */
+int orc_scale(const orc_geom *g, double *a, double *b)
+{
+    const int64_t n = g->n;
+    int bad = 0;
+#pragma omp parallel for reduction(| : bad) schedule(static)
+    for (int64_t p = 0; p < n; ++p) {
+        double m = fabs(a[p]);
+        for (int d = 1; d < 7; ++d) {
+            const double v = fabs(a[(int64_t)d * n + p]);
+            if (isnan(m) || v > m) m = v;
+        }
+        if (m > 0.0) {
+            const double oam = 1.0 / m;
+            for (int d = 0; d < 7; ++d) a[(int64_t)d * n + p] = a[(int64_t)d * n + p] * oam;
+            b[p] = b[p] * oam;
+        } else {
+            bad |= 1;
+        }
+    }
+    return bad ? -2 : 0;
+}
+
+/* ------------------------------------------------------------------ LEQ_BICGS0 */
+#define SMALL_NUMBER 1.0e-15
+#define RATIOTOL ((double)0.2f) /* DOUBLE PRECISION, PARAMETER :: ratiotol = 0.2 (a REAL literal) */
+
+static int pc_mode(const char *pc)
+{
+    /* model/leq_bicgs.f:74-87: CHARACTER(LEN=4) compared with blank padding */
+    if (!memcmp(pc, "LINE", 4)) return 2;
+    if (!memcmp(pc, "DIAG", 4)) return 1;
+    if (!memcmp(pc, "NONE", 4)) return 0;
+    return -1;
+}
+
+static int bicgs_run(const orc_geom *g, double *var, double *a, double *b, const char *sweep, double tol,
+                     const char *pc, int itmax, uint64_t rt_seed, int max_exec, orc_stats *st)
+{
+    memset(st, 0, sizeof(*st));
+    st->exit_kind = -1;
+    const int mode = pc_mode(pc);
+    if (mode < 0) {
+        st->ier = -10;
+        return -10;
+    }
+    const int64_t n = g->n;
+    if (orc_scale(g, a, b) != 0) {
+        st->ier = -2;
+        st->exit_kind = 4;
+        return -2;
+    }
+    double *work = (double *)calloc((size_t)(8 * n), sizeof(double));
+    double *R = work, *Rt = work + n, *P = work + 2 * n, *Pp = work + 3 * n, *S = work + 4 * n,
+           *Sp = work + 5 * n, *T = work + 6 * n, *V = work + 7 * n;
+    const double tolmin = DBL_EPSILON;
+
+    orc_matvec(g, a, var, R);
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < n; ++p) R[p] = b[p] - R[p];
+    const double rnorm0 = sqrt(orc_dot(R, R, n));
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < n; ++p) Rt[p] = R[p] + (2.0 * orc_uniform(rt_seed, 0xA1, (uint64_t)p) - 1.0) * 1.0e-6 * rnorm0;
+
+    double rnorm = 0.0, rho_m1 = 0.0, rho_m2 = 0.0, alpha_m1 = 0.0, omega_m1 = 0.0;
+    int iter = 1, converged = 0, ier = 0, executed = 0, iter_tot_add = 0;
+    int exit_kind = 3;
+    for (int i = 1; i <= itmax; ++i) {
+        if (max_exec >= 0 && executed >= max_exec) break;
+        ++executed;
+        rho_m1 = orc_dot(Rt, R, n);
+        if (rho_m1 == 0.0) {
+            ier = (i != 1) ? -2 : 0;
+            st->ier = ier;
+            st->iterations = iter;
+            st->exit_kind = 2;
+            st->rnorm0 = rnorm0;
+            st->rnorm = rnorm;
+            free(work);
+            return ier;
+        }
+        if (i == 1) {
+#pragma omp parallel for schedule(static)
+            for (int64_t p = 0; p < n; ++p) P[p] = R[p];
+        } else {
+            const double beta = (rho_m1 / rho_m2) * (alpha_m1 / omega_m1);
+#pragma omp parallel for schedule(static)
+            for (int64_t p = 0; p < n; ++p) P[p] = R[p] + beta * (P[p] - omega_m1 * V[p]);
+        }
+        const double *Ph = P;
+        if (mode == 2) {
+            if (orc_msolve(g, P, a, Pp, sweep, &st->line_info_skips) != 0) { ier = -12; break; }
+            Ph = Pp;
+        } else if (mode == 1) {
+            orc_msolve1(g, P, a, Pp);
+            Ph = Pp;
+        }
+        orc_matvec(g, a, Ph, V);
+        const double rtv = orc_dot(Rt, V, n);
+        const double alpha = rho_m1 / rtv;
+#pragma omp parallel for schedule(static)
+        for (int64_t p = 0; p < n; ++p) S[p] = R[p] - alpha * V[p];
+        const double snorm = sqrt(orc_dot(S, S, n));
+        if (snorm <= tolmin) {
+#pragma omp parallel for schedule(static)
+            for (int64_t p = 0; p < n; ++p) var[p] = var[p] + alpha * Ph[p];
+            converged = 1;
+            exit_kind = 1;
+            break;
+        }
+        const double *Sh = S;
+        if (mode == 2) {
+            if (orc_msolve(g, S, a, Sp, sweep, &st->line_info_skips) != 0) { ier = -12; break; }
+            Sh = Sp;
+        } else if (mode == 1) {
+            orc_msolve1(g, S, a, Sp);
+            Sh = Sp;
+        }
+        orc_matvec(g, a, Sh, T);
+        const double txs = orc_dot(T, S, n);
+        double txt = orc_dot(T, T, n);
+        if (txt == 0.0) txt = SMALL_NUMBER;
+        const double omega = txs / txt;
+#pragma omp parallel for schedule(static)
+        for (int64_t p = 0; p < n; ++p) {
+            var[p] = var[p] + alpha * Ph[p] + omega * Sh[p];
+            R[p] = S[p] - omega * T[p];
+        }
+        rnorm = sqrt(orc_dot(R, R, n));
+        if (rnorm <= tol * rnorm0) {
+            iter_tot_add = iter + 1;
+            converged = 1;
+            exit_kind = 0;
+            break;
+        }
+        ++iter;
+        rho_m2 = rho_m1;
+        alpha_m1 = alpha;
+        omega_m1 = omega;
+    }
+    if (ier == -12) {
+        st->ier = -12;
+        st->exit_kind = -1;
+        free(work);
+        return -12;
+    }
+    /* model/leq_bicgs.f:486-495 */
+    if (!converged) converged = ((double)(float)rnorm <= tol * rnorm0);
+    ier = 0;
+    if (!converged) {
+        ier = -1;
+        iter_tot_add = iter;
+        if ((double)(float)rnorm >= RATIOTOL * (double)(float)rnorm0) ier = -2;
+    }
+    st->ier = ier;
+    st->iterations = iter;
+    st->iter_tot_add = iter_tot_add;
+    st->exit_kind = exit_kind;
+    st->rnorm0 = rnorm0;
+    st->rnorm = rnorm;
+    free(work);
+    return ier;
+}
+
+int orc_leq_bicgs(const orc_geom *g, double *var, double *a, double *b, const char *sweep, double tol,
+                  const char *pc, int itmax, uint64_t rt_seed, orc_stats *st)
+{
+    return bicgs_run(g, var, a, b, sweep, tol, pc, itmax, rt_seed, -1, st);
+}
+
+int orc_leq_bicgs_sample(const orc_geom *g, double *var, double *a, double *b, const char *sweep, double tol,
+                         const char *pc, int itmax, uint64_t rt_seed, int max_exec, orc_stats *st)
+{
+    return bicgs_run(g, var, a, b, sweep, tol, pc, itmax, rt_seed, max_exec, st);
+}
+
+/* ------------------------------------------------------------------ truth oracle */
+double orc_true_resid(const orc_geom *g, const double *a, const double *b, const double *x)
+{
+    const int64_t c1 = g->jmax2, c2 = (int64_t)g->jmax2 * g->imax2;
+    const double *am3 = DIAG(a, g, -3), *am2 = DIAG(a, g, -2), *am1 = DIAG(a, g, -1);
+    const double *a0 = DIAG(a, g, 0), *ap1 = DIAG(a, g, 1), *ap2 = DIAG(a, g, 2), *ap3 = DIAG(a, g, 3);
+    long double tot = 0.0L;
+#pragma omp parallel for collapse(2) reduction(+ : tot) schedule(static)
+    for (int k = 1; k <= g->kmax2; ++k)
+        for (int i = 1; i <= g->imax2; ++i) {
+            const int64_t im = i > 1 ? -c1 : 0, ip = i < g->imax2 ? c1 : 0;
+            const int64_t km = (g->do_k && k > 1) ? -c2 : 0, kp = (g->do_k && k < g->kmax2) ? c2 : 0;
+            const int64_t base = cell(g, i, 1, k);
+            for (int j = 1; j <= g->jmax2; ++j) {
+                const int64_t p = base + j - 1;
+                const int64_t jm = j > 1 ? -1 : 0, jp = j < g->jmax2 ? 1 : 0;
+                long double s = (long double)am2[p] * x[p + jm] + (long double)am1[p] * x[p + im] +
+                                (long double)a0[p] * x[p] + (long double)ap1[p] * x[p + ip] +
+                                (long double)ap2[p] * x[p + jp];
+                if (g->do_k) s += (long double)am3[p] * x[p + km] + (long double)ap3[p] * x[p + kp];
+                const long double r = (long double)b[p] - s;
+                tot += r * r;
+            }
+        }
+    return (double)sqrtl(tot);
+}
+
+static void true_resid_vec(const orc_geom *g, const double *a, const double *b, const double *x, double *r)
+{
+    const int64_t c1 = g->jmax2, c2 = (int64_t)g->jmax2 * g->imax2;
+    const double *am3 = DIAG(a, g, -3), *am2 = DIAG(a, g, -2), *am1 = DIAG(a, g, -1);
+    const double *a0 = DIAG(a, g, 0), *ap1 = DIAG(a, g, 1), *ap2 = DIAG(a, g, 2), *ap3 = DIAG(a, g, 3);
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 1; k <= g->kmax2; ++k)
+        for (int i = 1; i <= g->imax2; ++i) {
+            const int64_t im = i > 1 ? -c1 : 0, ip = i < g->imax2 ? c1 : 0;
+            const int64_t km = (g->do_k && k > 1) ? -c2 : 0, kp = (g->do_k && k < g->kmax2) ? c2 : 0;
+            const int64_t base = cell(g, i, 1, k);
+            for (int j = 1; j <= g->jmax2; ++j) {
+                const int64_t p = base + j - 1;
+                const int64_t jm = j > 1 ? -1 : 0, jp = j < g->jmax2 ? 1 : 0;
+                long double s = (long double)am2[p] * x[p + jm] + (long double)am1[p] * x[p + im] +
+                                (long double)a0[p] * x[p] + (long double)ap1[p] * x[p + ip] +
+                                (long double)ap2[p] * x[p + jp];
+                if (g->do_k) s += (long double)am3[p] * x[p + km] + (long double)ap3[p] * x[p + kp];
+                r[p] = (double)((long double)b[p] - s);
+            }
+        }
+}
+
+/* Plain right-preconditioned BiCGSTAB (LINE, RSRS) on A d = r, stopping when the
+ * recursive residual falls by `drop`; used for refinement steps only. */
+static void bicgs_inner(const orc_geom *g, const double *a, const double *r0, double *d, double drop, int maxit,
+                        uint64_t seed, double *work)
+{
+    const int64_t n = g->n;
+    double *R = work, *Rt = work + n, *P = work + 2 * n, *Pp = work + 3 * n, *S = work + 4 * n,
+           *Sp = work + 5 * n, *T = work + 6 * n, *V = work + 7 * n;
+    memset(d, 0, sizeof(double) * (size_t)n);
+    memcpy(R, r0, sizeof(double) * (size_t)n);
+    const double rn0 = sqrt(orc_dot(R, R, n));
+    for (int64_t p = 0; p < n; ++p) Rt[p] = R[p] + (2.0 * orc_uniform(seed, 0xA2, (uint64_t)p) - 1.0) * 1e-6 * rn0;
+    double rho_m2 = 1, alpha_m1 = 0, omega_m1 = 1;
+    for (int i = 1; i <= maxit; ++i) {
+        const double rho = orc_dot(Rt, R, n);
+        if (rho == 0.0) break;
+        if (i == 1)
+            memcpy(P, R, sizeof(double) * (size_t)n);
+        else {
+            const double beta = (rho / rho_m2) * (alpha_m1 / omega_m1);
+#pragma omp parallel for schedule(static)
+            for (int64_t p = 0; p < n; ++p) P[p] = R[p] + beta * (P[p] - omega_m1 * V[p]);
+        }
+        orc_msolve(g, P, a, Pp, "RSRS", NULL);
+        orc_matvec(g, a, Pp, V);
+        const double alpha = rho / orc_dot(Rt, V, n);
+#pragma omp parallel for schedule(static)
+        for (int64_t p = 0; p < n; ++p) S[p] = R[p] - alpha * V[p];
+        orc_msolve(g, S, a, Sp, "RSRS", NULL);
+        orc_matvec(g, a, Sp, T);
+        const double txt = orc_dot(T, T, n);
+        const double omega = txt == 0.0 ? 0.0 : orc_dot(T, S, n) / txt;
+#pragma omp parallel for schedule(static)
+        for (int64_t p = 0; p < n; ++p) {
+            d[p] = d[p] + alpha * Pp[p] + omega * Sp[p];
+            R[p] = S[p] - omega * T[p];
+        }
+        if (sqrt(orc_dot(R, R, n)) <= drop * rn0 || omega == 0.0) break;
+        rho_m2 = rho;
+        alpha_m1 = alpha;
+        omega_m1 = omega;
+    }
+}
+
+int orc_truth_solve(const orc_geom *g, const double *a, const double *b, double *x, double rtol, int max_iter,
+                    uint64_t rt_seed, double *final_rel)
+{
+    const int64_t n = g->n;
+    double *work = (double *)calloc((size_t)(10 * n), sizeof(double));
+    double *r = work + 8 * n, *d = work + 9 * n;
+    const double r0 = orc_true_resid(g, a, b, x);
+    double rel = 1.0;
+    int steps = 0;
+    if (r0 == 0.0) {
+        rel = 0.0;
+    } else {
+        for (steps = 0; steps < max_iter; ++steps) {
+            true_resid_vec(g, a, b, x, r);
+            rel = orc_true_resid(g, a, b, x) / r0;
+            if (rel <= rtol) break;
+            bicgs_inner(g, a, r, d, 1e-6, 400, rt_seed + (uint64_t)steps, work);
+#pragma omp parallel for schedule(static)
+            for (int64_t p = 0; p < n; ++p) x[p] += d[p];
+        }
+        rel = orc_true_resid(g, a, b, x) / r0;
+    }
+    if (final_rel) *final_rel = rel;
+    free(work);
+    return rel <= rtol ? steps : -1;
+}

@@ -1,0 +1,92 @@
+"""CPU checks of the C ABI: the library loads, exports every declared symbol,
+and its host-side logic answers without touching a GPU."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import mfix_b200
+from mfix_b200 import leq
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared():
+    names = set()
+    for fn in os.listdir(os.path.join(ROOT, "include")):
+        if fn.endswith(".h"):
+            txt = open(os.path.join(ROOT, "include", fn)).read()
+            txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+            names |= set(re.findall(r"\b(mfixgpu_\w+)\s*\(", txt))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    L = mfix_b200.lib()
+    names = _declared()
+    assert len(names) >= 14
+    for nm in names:
+        assert hasattr(L, nm), nm
+
+
+def _gpu_visible():
+    try:
+        import torch
+
+        return torch.cuda.is_available()
+    except Exception:
+        return False
+
+
+def test_geometry_validation():
+    assert leq.init_geometry(4, 5, 6, 1, 120, 0) == 0
+    assert leq.init_geometry(4, 5, 6, 1, 121, 0) == leq.IER_ARGS
+    assert leq.init_geometry(4, 5, 2, 0, 40, 0) == leq.IER_ARGS  # 2-D needs KMAX2 = 1
+    assert leq.init_geometry(0, 5, 6, 1, 0, 0) == leq.IER_ARGS
+
+
+def test_options_roundtrip():
+    assert leq.set_option("precision", 1) == 0 and leq.get_option("precision") == 1
+    assert leq.set_option("precision", 0) == 0
+    assert leq.set_option("precision", 3) == leq.IER_ARGS
+    assert leq.set_option("no_such_option", 1) == leq.IER_ARGS
+    assert leq.get_option("write_back_ab") == 1
+
+
+def test_argument_errors_before_device_work():
+    a = np.zeros((2, 7, 120))
+    b = np.zeros((2, 120))
+    x = np.zeros(120)
+    assert leq.init_geometry(4, 5, 6, 1, 120, 1) == 0
+    assert leq.solve_lin_eq("U_g", 3, x, a, b, 5, 10, 2, "RSRS", 1e-8, "LINE") == leq.IER_ARGS  # M > DIMENSION_M
+    assert leq.solve_lin_eq("U_g", 3, x, a, b, 0, 10, 3, "RSRS", 1e-8, "LINE") == leq.IER_UNSUPPORTED  # GMRES
+    assert leq.solve_lin_eq("U_g", 3, x, a, b, 0, 10, 2, "RSRS", 1e-8, "ILU") == leq.IER_UNSUPPORTED
+
+
+@pytest.mark.skipif(_gpu_visible(), reason="checks the behaviour without a GPU")
+def test_no_cpu_fallback_without_gpu():
+    a = np.zeros((7, 120))
+    a[3] = -1.0
+    b = np.ones(120)
+    x = np.zeros(120)
+    assert leq.init_geometry(4, 5, 6, 1, 120, 0) == 0
+    assert leq.solve_lin_eq("U_g", 3, x, a, b, 0, 10, 2, "RSRS", 1e-8, "LINE") == leq.IER_CUDA
+    assert "no CUDA device" in leq.last_error()
+    assert not x.any()
+
+
+def test_fastdiv_formula():
+    """The host/device magic-number division used for cell -> (i, j, k)."""
+    rng = np.random.default_rng(0)
+    for d in list(range(1, 70)) + [193, 194, 258, 386, 1000, 65537]:
+        l = 0
+        while (1 << l) < d:
+            l += 1
+        m = ((1 << 32) * ((1 << l) - d)) // d + 1
+        m &= 0xFFFFFFFF
+        ns = np.concatenate([rng.integers(0, 2**31, 2000), np.arange(0, 5000), [2**31 - 1, 2**32 - 1]])
+        for n in ns.tolist():
+            q = (((n * m) >> 32) + n) >> l
+            assert q == n // d, (d, n)
