@@ -41,13 +41,14 @@ if ROOT not in sys.path:
 WORKLOADS = {
     "conv_diff_256": dict(kind="conv_diff", dims=(256, 256, 256), seed=0, itmax=500, tol=1e-8),
     "conv_diff_64": dict(kind="conv_diff", dims=(64, 64, 64), seed=0, itmax=500, tol=1e-8),
+    "conv_diff_192": dict(kind="conv_diff", dims=(192, 192, 192), seed=0, itmax=500, tol=1e-8),
     "pressure_192x384x192": dict(kind="pressure_like", dims=(192, 384, 192), seed=0, itmax=5000, tol=1e-8),
 }
 DEFAULT_WORKLOAD = "conv_diff_256"
 # Iterations the reference FP64 algorithm needs on each seeded workload (the GPU FP64
 # drop-in follows the same algorithm; tests/test_gpu_bench_workload.py checks it).
 # Used by the CPU arm to turn a timed sample of iterations into solves/s.
-FP64_ITERATIONS = {"conv_diff_256": None, "conv_diff_64": 65, "pressure_192x384x192": None}
+FP64_ITERATIONS = {"conv_diff_256": 66, "conv_diff_64": 65, "conv_diff_192": None, "pressure_192x384x192": None}
 
 BYTES_FP64_ITER = 576  # algorithmic bytes per cell per BiCGSTAB iteration, FP64 (72 words)
 BYTES_FP32_ITER = 288  # the same in the FP32 inner solve
@@ -257,6 +258,12 @@ def run_ours(args) -> None:
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
 
+    if args.only != "all":
+        for _ in range(max(args.steps, 1)):
+            r, st = solve_device(0 if args.only == "fp64" else 1)
+        print(f"{args.only}: iterations {r.iterations} outer {r.outer_steps} device_ms {st['device_ms']:.3f}")
+        return
+
     # ---- FP64 drop-in (device resident)
     for _ in range(args.warmup):
         solve_device(0)
@@ -383,6 +390,8 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--only", default="all", choices=["all", "fp64", "mixed"],
+                    help="profiling runs: solve only this form (no e2e leg, no JSON line)")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

@@ -81,18 +81,22 @@ typedef struct {
     double device_ms;   /* device time of the solve (CUDA events), copies excluded */
     double jline_ms;    /* summed J-line sweep kernel time (option "time_kernels") */
     int jline_launches; /* J-line sweep launches timed */
-    int pad2;
+    int fp64_fallback;  /* mixed form: 1 when the FP32 iteration stalled and the FP64 drop-in re-solved */
     long long kernel_launches; /* kernels of this library launched by the solve */
+    int mixed_iterations; /* mixed form: FP32 iterations spent before an FP64 re-solve */
+    int pad3;
 } mfixgpu_stats;
 
 int mfixgpu_last_stats(mfixgpu_stats *out);
 const char *mfixgpu_last_error(void);
 
 /* Options (no reference counterpart; defaults reproduce the reference):
- *   "precision"      0 FP64 drop-in (default), 1 FP32 inner / FP64 refinement
+ *   "precision"      0 FP64 drop-in (default), 1 FP32 BiCGSTAB with FP64 solution accumulation,
+ *                    FP64 dot products and FP64 reliable residual updates; a system whose FP32
+ *                    iteration diverges or stalls is re-solved by the FP64 drop-in
  *   "write_back_ab"  1 (default) copy the scaled A_M/B_M slices back
  *   "rtilde_seed"    seed of the Rtilde random stream (replaces RANDOM_NUMBER, model/leq_bicgs.f:298)
- *   "inner_tol"      mixed form: relative drop asked of each inner solve (default 1e-4)
+ *   "inner_tol"      mixed form: drop of the FP32 residual between FP64 reliable updates (default 1e-2)
  *   "check_every"    iterations between host polls of convergence (default 4)
  *   "use_graph"      1 (default) replay the iteration body as a CUDA graph
  *   "time_kernels"   1: time every J-line sweep launch with CUDA events (no graph replay)
@@ -138,7 +142,7 @@ typedef struct {
     int iterations;
     int outer_steps;
     int exit_kind;
-    int pad;
+    int fp64_fallback;
     double rnorm0, rnorm;
 } mfixgpu_system;
 

@@ -30,7 +30,7 @@ struct Options {
     int precision = PREC_FP64;
     int write_back_ab = 1;
     uint64_t seed = 0x5EEDULL;
-    double inner_tol = 1e-4;
+    double inner_tol = 1e-2;
     int check_every = 4;
     int use_graph = 1;
     int time_kernels = 0;
@@ -180,6 +180,8 @@ void solve_impl(int vno, double *var, double *a_m, double *b_m, int m, int itmax
     g.last.jline_ms = e->timing().jline_ms;
     g.last.jline_launches = e->timing().jline_launches;
     g.last.kernel_launches = e->timing().kernel_launches;
+    g.last.fp64_fallback = r.fp64_fallback;
+    g.last.mixed_iterations = r.mixed_iterations;
     finish(code);
 }
 
@@ -438,6 +440,7 @@ int mfixgpu_batch_solve(mfixgpu_system *systems, int nsys, const char *sweep, co
         systems[q].exit_kind = out[q].exit_kind;
         systems[q].rnorm0 = out[q].rnorm0;
         systems[q].rnorm = out[q].rnorm;
+        systems[q].fp64_fallback = out[q].fp64_fallback;
     }
     return 0;
 }

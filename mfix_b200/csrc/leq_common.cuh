@@ -12,7 +12,7 @@ namespace mfixgpu {
 
 // Work vectors of LEQ_BICGS0 (model/leq_bicgs.f:171-176) plus the solution.
 enum VecId : int {
-    V_X = 0,  // VAR (inner correction d in the mixed form)
+    V_X = 0,  // VAR (unused slot in the mixed form, which accumulates into x64[0])
     V_R,      // R
     V_RT,     // Rtilde
     V_P,      // P
@@ -36,7 +36,8 @@ enum ExitKind : int {
     EX_RHO0 = 2,      // rho == 0 (:320-332)
     EX_ITMAX = 3,     // loop exhausted (:485-495)
     EX_SINGULAR = 4,  // zero row during unit scaling (:217-233)
-    EX_ERROR = 5
+    EX_ERROR = 5,
+    EX_FALLBACK = 6   // mixed form gave up (divergence / stagnation): re-solved in FP64
 };
 
 // Magic-number unsigned division by a runtime constant (round-up method,
@@ -71,13 +72,15 @@ struct SysDev {
     int ntiles;          // cell tiles of this system
     int tile_base;       // first tile's slot in the partial-sum array
     int lane_group;      // G: lanes that share one J-line (power of two <= 32)
-    int rows_per_lane;   // c: rows each lane eliminates (odd; G*c >= jmax2)
+    int rows_per_lane;   // c: rows of a line each lane owns (G*c >= jmax2)
     int half_lines;      // ceil(imax2/2): parity-wave slots per k row
     double *a64;         // 7*n diagonals, Fortran A_M(DIMENSION_3,-3:3) order
     double *b64;         // B_M(:,M)
-    double *x64[2];      // VAR (x64[1] is the ping-pong buffer of the mixed form)
+    double *x64[2];      // VAR; x64[1] keeps the initial guess in the mixed form (FP64 re-solve)
     float *a32;          // FP32 copy of the scaled diagonals (mixed form)
     void *vec[NVEC];     // work vectors, double or float by precision
+    void *fac[3];        // J-line LU factors per cell (l, 1/u, c/u), double or float by precision
+    int *line_flag;      // per J-line (i-1)+(k-1)*imax2: 1 where DGTSV interchanges rows or meets a zero pivot
 };
 
 // Per-system solver state, device resident; the scalars of LEQ_BICGS0 plus
@@ -88,7 +91,9 @@ struct SysState {
     double tol;           // TOL
     double outer_rnorm0;  // mixed form: ||b - A x0|| in FP64
     double outer_rnorm;   // mixed form: latest FP64 true residual
-    double inner_tol;     // mixed form: relative drop asked of each inner solve
+    double inner_tol;     // mixed form: residual drop (vs maxr) that triggers a reliable update
+    double maxr;          // mixed form: largest recursive residual since the last reliable update
+    double best;          // mixed form: smallest true residual seen at a reliable update
     int itmax;
     int i;                // reference loop index of the next iteration (1-based)
     int iter;             // reference ITER counter
@@ -100,13 +105,14 @@ struct SysState {
     int phase;            // Phase
     int outer_steps;
     int inner_total;      // inner iterations summed over outer steps
-    int inner_first;      // first inner iteration after an outer step
+    int inner_first;      // mixed form: the correction d restarts from zero at the next X update
     int xcur;             // mixed form: which x64 buffer holds VAR
+    int restart;          // mixed form: next reliable update restarts the Krylov process (Rtilde = R)
+    int stall;            // mixed form: reliable updates since the best true residual improved by 10%
     int line_skips;       // J-lines left unchanged because DGTSV reported INFO != 0
     int line_fallbacks;   // J-lines solved by the sequential pivoting path
     int err;
     unsigned int arrivals;  // tiles that finished the current reduction kernel
-    int pad;
 };
 
 // One cell tile: TILE consecutive cells of one system.
@@ -115,9 +121,8 @@ struct Tile {
     int idx;  // tile index within the system
 };
 
-constexpr int TILE_CELLS = 8192;
+constexpr int TILE_CELLS = 4096;
 constexpr int CELL_THREADS = 256;
-constexpr int LINE_WARPS = 4;  // warps per block of the J-line kernel
 
 // Ordered parameters of one J-line half-sweep (a "wave").
 struct WaveArgs {

@@ -23,12 +23,15 @@ namespace mfixgpu {
 
 static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// Lanes per J-line: the smallest power of two that leaves about a dozen rows per
+// lane (at most 32); rows per lane rounded up to odd so that lanes reading row t
+// of their chunks hit distinct shared-memory banks.
 void line_shape(int L, int *G, int *c)
 {
     int g = 1;
-    while (g * 2 <= 32 && g * 4 <= L) g *= 2;
+    while (g < 32 && g * 12 < L) g *= 2;
     int cc = (L + g - 1) / g;
-    if (cc < 3) cc = 3;
+    if (cc < 1) cc = 1;
     if ((cc & 1) == 0) ++cc;
     *G = g;
     *c = cc;
@@ -84,10 +87,12 @@ Engine::~Engine()
 {
     if (stream_) cudaStreamSynchronize(stream_);
     arena_.release();
+    in_arena_.release();
     cudaFree(d_sys_);
     cudaFree(d_st_);
     cudaFree(d_tiles_);
     cudaFree(d_prefix_);
+    cudaFree(d_allprefix_);
     cudaFree(d_partials_);
     cudaFree(d_lines_);
     cudaFree(d_seq_scratch_);
@@ -133,13 +138,13 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
     const bool mixed = opt.precision == PREC_MIXED;
     const size_t ew = mixed ? sizeof(float) : sizeof(double);
 
-    // memory plan
+    // work memory: the iteration vectors, plus the FP32 diagonals and a copy of
+    // the initial guess in the mixed form (inputs are device arrays by now)
     size_t bytes = 0;
     for (const auto &s : specs) {
         const size_t n = (size_t)s.n;
-        if (!opt.on_device) bytes += align_up(7 * n * 8, 256) + 2 * align_up(n * 8, 256);
         if (mixed) bytes += align_up(n * 8, 256) + align_up(7 * n * 4, 256);
-        bytes += NVEC * align_up(n * ew, 256);
+        bytes += (NVEC + 3) * align_up(n * ew, 256) + align_up((size_t)s.imax2 * s.kmax2 * 4, 256);
     }
     bytes += 4096;
     cudaError_t e = arena_.reserve(bytes);
@@ -150,7 +155,8 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
     h_st_.assign(nsys_, SysState{});
     h_tiles_.clear();
     h_prefix_.assign(nsys_ + 1, 0);
-    int cmax = 3;
+    h_allprefix_.assign(nsys_ + 1, 0);
+    int cmax = 1;
     int tile_base = 0;
     for (int s = 0; s < nsys_; ++s) {
         const SystemSpec &sp = specs[s];
@@ -170,25 +176,22 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         cmax = std::max(cmax, d.rows_per_lane);
         d.half_lines = (sp.imax2 + 1) / 2;
         const size_t n = (size_t)sp.n;
-        if (opt.on_device) {
-            d.a64 = sp.a;
-            d.b64 = sp.b;
-            d.x64[0] = sp.x;
-        } else {
-            d.a64 = (double *)arena_.take(7 * n * 8);
-            d.b64 = (double *)arena_.take(n * 8);
-            d.x64[0] = (double *)arena_.take(n * 8);
-        }
+        d.a64 = sp.a;
+        d.b64 = sp.b;
+        d.x64[0] = sp.x;
         if (mixed) {
-            d.x64[1] = (double *)arena_.take(n * 8);
+            d.x64[1] = (double *)arena_.take(n * 8);  // initial guess, kept for an FP64 re-solve
             d.a32 = (float *)arena_.take(7 * n * 4);
         }
         for (int v = 0; v < NVEC; ++v) d.vec[v] = arena_.take(n * ew);
+        for (int f = 0; f < 3; ++f) d.fac[f] = arena_.take(n * ew);
+        d.line_flag = (int *)arena_.take((size_t)sp.imax2 * sp.kmax2 * 4);
         if (!mixed) d.vec[V_X] = d.x64[0];
         for (int t = 0; t < d.ntiles; ++t) h_tiles_.push_back(Tile{s, t});
         const int lpw = 32 / d.lane_group;
         const int64_t slots = (int64_t)d.half_lines * sp.kmax2;
         h_prefix_[s + 1] = h_prefix_[s] + (int)((slots + lpw - 1) / lpw);
+        h_allprefix_[s + 1] = h_allprefix_[s] + sp.imax2 * sp.kmax2;
 
         SysState &st = h_st_[s];
         st.tol = sp.tol;
@@ -200,22 +203,17 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         st.iter = 1;
     }
 
-    // host -> device copies of the systems
-    if (!opt.on_device) {
-        for (int s = 0; s < nsys_; ++s) {
-            const SystemSpec &sp = specs[s];
-            const size_t n = (size_t)sp.n;
-            CK(cudaMemcpyAsync(h_sys_[s].a64, sp.a, 7 * n * 8, cudaMemcpyHostToDevice, stream_));
-            CK(cudaMemcpyAsync(h_sys_[s].b64, sp.b, n * 8, cudaMemcpyHostToDevice, stream_));
-            CK(cudaMemcpyAsync(h_sys_[s].x64[0], sp.x, n * 8, cudaMemcpyHostToDevice, stream_));
-        }
-    }
+    if (mixed)
+        for (int q = 0; q < nsys_; ++q)
+            CK(cudaMemcpyAsync(h_sys_[q].x64[1], h_sys_[q].x64[0], (size_t)h_sys_[q].n * 8, cudaMemcpyDeviceToDevice,
+                               stream_));
 
     // tables are small; their device copies are reallocated only when they grow
     CK(upload(&d_sys_, &sys_cap_, h_sys_.data(), h_sys_.size(), stream_));
     CK(upload(&d_st_, &st_cap_, h_st_.data(), h_st_.size(), stream_));
     CK(upload(&d_tiles_, &tiles_cap_, h_tiles_.data(), h_tiles_.size(), stream_));
     CK(upload(&d_prefix_, &prefix_cap_, h_prefix_.data(), h_prefix_.size(), stream_));
+    CK(upload(&d_allprefix_, &allprefix_cap_, h_allprefix_.data(), h_allprefix_.size(), stream_));
     const size_t need_part = 2 * (size_t)std::max(tile_base, 1);
     if (need_part > part_cap_) {
         cudaFree(d_partials_);
@@ -240,11 +238,14 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
 
     cfg_.stream = stream_;
     cfg_.line_cmax = cmax;
-    cfg_.cell_grid = std::max(1, std::min(view_.ntiles, sms_ * cell_bpsm_));
-    const int bpsm = mixed ? prepare_line_kernel<float>(cmax) : prepare_line_kernel<double>(cmax);
-    if (bpsm <= 0) return fail("J-line kernel does not fit on the device (shared memory)", -11);
+    // one block per tile: the block scheduler balances tiles across SMs
+    cfg_.cell_grid = std::max(1, view_.ntiles);
+    int wpb = 1;
+    const int bpsm = mixed ? prepare_line_kernel<float>(cmax, &wpb) : prepare_line_kernel<double>(cmax, &wpb);
+    if (bpsm <= 0) return fail("J-lines too long for the shared-memory staging of the line kernel", -10);
+    cfg_.line_warps = wpb;
     const int items = h_prefix_[nsys_];
-    cfg_.line_grid = std::max(1, std::min((items + LINE_WARPS - 1) / LINE_WARPS, sms_ * bpsm));
+    cfg_.line_grid = std::max(1, std::min((items + wpb - 1) / wpb, sms_ * bpsm));
     return 0;
 }
 
@@ -491,6 +492,83 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
         if (!s.a || !s.b || !s.x) return fail("null array", -14);
     }
     if (opt.pc != PC_LINE && opt.pc != PC_DIAG && opt.pc != PC_NONE) return fail("unknown preconditioner", -10);
+
+    // inputs on the device: the caller's arrays, or copies in the input arena
+    std::vector<SystemSpec> dev = specs;
+    if (!opt.on_device) {
+        size_t bytes = 4096;
+        for (const auto &s : specs) bytes += align_up(7 * (size_t)s.n * 8, 256) + 2 * align_up((size_t)s.n * 8, 256);
+        cudaError_t e = in_arena_.reserve(bytes);
+        if (e != cudaSuccess) return fail(std::string("device memory for the inputs: ") + cudaGetErrorString(e), -11);
+        in_arena_.reset();
+        for (size_t q = 0; q < specs.size(); ++q) {
+            const size_t n = (size_t)specs[q].n;
+            dev[q].a = (double *)in_arena_.take(7 * n * 8);
+            dev[q].b = (double *)in_arena_.take(n * 8);
+            dev[q].x = (double *)in_arena_.take(n * 8);
+            CK(cudaMemcpyAsync(dev[q].a, specs[q].a, 7 * n * 8, cudaMemcpyHostToDevice, stream_));
+            CK(cudaMemcpyAsync(dev[q].b, specs[q].b, n * 8, cudaMemcpyHostToDevice, stream_));
+            CK(cudaMemcpyAsync(dev[q].x, specs[q].x, n * 8, cudaMemcpyHostToDevice, stream_));
+        }
+    }
+    SolveOptions o = opt;
+    o.on_device = true;
+    int rc = run_batch(dev, o, out);
+    if (rc) return rc;
+    SolveTiming total = timing_;
+
+    // mixed form: systems whose FP32 iteration gave up are solved again by the
+    // FP64 drop-in, from their initial guess
+    if (opt.precision == PREC_MIXED) {
+        std::vector<SystemSpec> fb;
+        std::vector<int> idx;
+        for (size_t q = 0; q < out.size(); ++q)
+            if (out[q].exit_kind == EX_FALLBACK) {
+                CK(cudaMemcpyAsync(dev[q].x, h_sys_[q].x64[1], (size_t)dev[q].n * 8, cudaMemcpyDeviceToDevice,
+                                   stream_));
+                fb.push_back(dev[q]);
+                idx.push_back((int)q);
+            }
+        if (!fb.empty()) {
+            SolveOptions f = o;
+            f.precision = PREC_FP64;
+            f.skip_scale = true;
+            std::vector<SolveResult> fo;
+            rc = run_batch(fb, f, fo);
+            if (rc) return rc;
+            for (size_t q = 0; q < idx.size(); ++q) {
+                const int mixed_its = out[idx[q]].iterations;
+                out[idx[q]] = fo[q];
+                out[idx[q]].fp64_fallback = 1;
+                out[idx[q]].mixed_iterations = mixed_its;
+            }
+            total.device_ms += timing_.device_ms;
+            total.jline_ms += timing_.jline_ms;
+            total.jline_launches += timing_.jline_launches;
+            total.kernel_launches += timing_.kernel_launches;
+        }
+    }
+    timing_ = total;
+
+    // results back to the caller's host arrays
+    if (!opt.on_device) {
+        for (size_t q = 0; q < specs.size(); ++q) {
+            const size_t n = (size_t)specs[q].n;
+            CK(cudaMemcpyAsync(specs[q].x, dev[q].x, n * 8, cudaMemcpyDeviceToHost, stream_));
+            if (opt.write_back_ab) {
+                CK(cudaMemcpyAsync(specs[q].a, dev[q].a, 7 * n * 8, cudaMemcpyDeviceToHost, stream_));
+                CK(cudaMemcpyAsync(specs[q].b, dev[q].b, n * 8, cudaMemcpyDeviceToHost, stream_));
+            }
+        }
+        CK(cudaStreamSynchronize(stream_));
+    }
+    return 0;
+}
+
+// One batch whose arrays are all on the device.
+int Engine::run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &opt, std::vector<SolveResult> &out)
+{
+    out.assign(specs.size(), SolveResult{});
     const bool mixed = opt.precision == PREC_MIXED;
     const int elem = mixed ? 4 : 8;
 
@@ -514,9 +592,16 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
     CK(cudaEventRecord(ev_t0_, stream_));
 
     // ---- setup
-    CK(launch_scale(view_, cfg_));
-    CK(launch_after_scale(view_, cfg_));
-    launches_ += 2;
+    if (!opt.skip_scale) {
+        CK(launch_scale(view_, cfg_));
+        CK(launch_after_scale(view_, cfg_));
+        launches_ += 2;
+    }
+    if (opt.pc == PC_LINE) {
+        CK(mixed ? launch_line_factor<float>(view_, cfg_, d_allprefix_, h_allprefix_[nsys_])
+                 : launch_line_factor<double>(view_, cfg_, d_allprefix_, h_allprefix_[nsys_]));
+        launches_ += 1;
+    }
     if (mixed) {
         CK(launch_to_f32(view_, cfg_));
         launches_ += 1;
@@ -637,19 +722,6 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
             r.ier = -12;  // DGTSV INFO != 0 inside a JK/IJ sweep (the reference stops there)
             r.exit_kind = EX_ERROR;
         }
-        const SysDev &d = h_sys_[s];
-        const SystemSpec &sp = specs[s];
-        const size_t n = (size_t)sp.n;
-        const double *xsrc = mixed ? d.x64[st.xcur] : d.x64[0];
-        if (opt.on_device) {
-            if (xsrc != sp.x) CK(cudaMemcpyAsync(sp.x, xsrc, n * 8, cudaMemcpyDeviceToDevice, stream_));
-        } else {
-            CK(cudaMemcpyAsync(sp.x, xsrc, n * 8, cudaMemcpyDeviceToHost, stream_));
-            if (opt.write_back_ab) {
-                CK(cudaMemcpyAsync(sp.a, d.a64, 7 * n * 8, cudaMemcpyDeviceToHost, stream_));
-                CK(cudaMemcpyAsync(sp.b, d.b64, n * 8, cudaMemcpyDeviceToHost, stream_));
-            }
-        }
     }
     CK(cudaStreamSynchronize(stream_));
     if (jline_timing_) {
@@ -724,6 +796,7 @@ int Engine::msolve(const SystemSpec &g, const double *a, const double *b, double
     if ((rc = plan_msolve(opt, V_P, V_PH, G_ANY, 0))) return rc;
     if ((rc = bind_lists())) return rc;
     if (pc == PC_NONE) CK(cudaMemcpyAsync(var, b, (size_t)g.n * 8, cudaMemcpyDeviceToDevice, stream_));
+    if (pc == PC_LINE) CK(launch_line_factor<double>(view_, cfg_, d_allprefix_, h_allprefix_[nsys_]));
     if ((rc = run_msolve_plan(0, 8))) return rc;
     CK(cudaStreamSynchronize(stream_));
     CK(cudaMemcpy(h_st_.data(), d_st_, sizeof(SysState), cudaMemcpyDeviceToHost));

@@ -16,6 +16,7 @@
 // again by one lane with the exact pivoting DGTSV recurrence.
 #include <cfloat>
 #include <cstdio>
+#include <algorithm>
 #include <type_traits>
 
 #include "leq_kernels.cuh"
@@ -186,6 +187,7 @@ __global__ void k_scale(BatchView b)
         const int64_t n = d.n;
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(n, c0 + TILE_CELLS);
         int bad = 0;
+        #pragma unroll 4
         for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
             double m = fabs(d.a64[c]);
 #pragma unroll
@@ -228,6 +230,7 @@ __global__ void k_to_f32(BatchView b)
         if (b.st[tl.sys].status != ST_RUNNING) continue;
         const int64_t n = d.n;
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(n, c0 + TILE_CELLS);
+        #pragma unroll 4
         for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x)
 #pragma unroll
             for (int q = 0; q < 7; ++q) d.a32[q * n + c] = (float)d.a64[q * n + c];
@@ -248,6 +251,7 @@ __global__ void k_init_residual(BatchView b)
         const T *x = vec<T>(d, V_X);
         T *r = vec<T>(d, V_R);
         double v[1] = {0.0}, tot[1];
+        #pragma unroll 4
         for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
             const CellIdx q = cell_ijk(d, (uint32_t)c);
             const T ax = (T)stencil_row<T, T>(d, a, x, (uint32_t)c, q);
@@ -288,6 +292,7 @@ __global__ void k_init_rtilde(BatchView b, uint64_t seed)
         const T *r = vec<T>(d, V_R);
         T *rt = vec<T>(d, V_RT);
         double v[1] = {0.0}, tot[1];
+        #pragma unroll 4
         for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
             const double u = uniform01(seed, 0xA1, (uint64_t)c);
             const T rv = r[c];
@@ -313,10 +318,12 @@ __global__ void k_p_update(BatchView b)
         const T *r = vec<T>(d, V_R);
         T *p = vec<T>(d, V_P);
         if (st.i == 1) {
+            #pragma unroll 4
             for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) p[c] = r[c];
         } else {
             const T beta = (T)st.beta, omega = (T)st.omega;
             const T *v = vec<T>(d, V_V);
+            #pragma unroll 4
             for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) p[c] = r[c] + beta * (p[c] - omega * v[c]);
         }
     }
@@ -334,6 +341,7 @@ __global__ void k_diag(BatchView b, int src, int dst, int gate)
         const T *a0 = diag_base<T>(d) + 3 * d.n;
         const T *x = vec<T>(d, src);
         T *y = vec<T>(d, dst);
+        #pragma unroll 4
         for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) y[c] = x[c] / a0[c];
     }
 }
@@ -348,6 +356,7 @@ __global__ void k_copy(BatchView b, int src, int dst, int gate)
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
         const T *x = vec<T>(d, src);
         T *y = vec<T>(d, dst);
+        #pragma unroll 4
         for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) y[c] = x[c];
     }
 }
@@ -367,6 +376,7 @@ __global__ void k_matvec_alpha(BatchView b, int src)
         const T *rt = vec<T>(d, V_RT);
         T *y = vec<T>(d, V_V);
         double v[1] = {0.0}, tot[1];
+        #pragma unroll 4
         for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
             const CellIdx q = cell_ijk(d, (uint32_t)c);
             const T yv = (T)stencil_row<T, T>(d, a, x, (uint32_t)c, q);
@@ -392,6 +402,7 @@ __global__ void k_s_update(BatchView b)
         const T *vv = vec<T>(d, V_V);
         T *s = vec<T>(d, V_S);
         double v[1] = {0.0}, tot[1];
+        #pragma unroll 4
         for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
             const T sv = r[c] - alpha * vv[c];
             s[c] = sv;
@@ -400,7 +411,7 @@ __global__ void k_s_update(BatchView b)
         if (tile_reduce<1>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) {
             st.snorm = sqrt(tot[0]);
             if (MIXED)
-                st.snorm_exit = (st.snorm <= st.inner_tol * st.rnorm0) ? 1 : 0;
+                st.snorm_exit = (st.snorm <= 0.1 * st.tol * st.outer_rnorm0) ? 1 : 0;
             else
                 st.snorm_exit = (st.snorm <= DBL_EPSILON) ? 1 : 0;  // TOLMIN = EPSILON(ONE)
         }
@@ -422,6 +433,7 @@ __global__ void k_matvec_omega(BatchView b, int src)
         const T *s = vec<T>(d, V_S);
         T *y = vec<T>(d, V_T);
         double v[2] = {0.0, 0.0}, tot[2];
+        #pragma unroll 4
         for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
             const CellIdx q = cell_ijk(d, (uint32_t)c);
             const T yv = (T)stencil_row<T, T>(d, a, x, (uint32_t)c, q);
@@ -471,25 +483,39 @@ __device__ inline void fin_xr_ref(SysState &s, double rr, double rtr)
     }
 }
 
-// Inner solve of the mixed form: convergence hands the system to the FP64
-// refinement step instead of ending it.
+// Mixed form (FP32 BiCGSTAB with reliable updates): once the FP32 recursive
+// residual has dropped by inner_tol against the largest value since the last
+// update, or looks converged, the system goes to the FP64 step, which folds the
+// FP32 correction into x and replaces the residual by the true one.
 __device__ inline void fin_xr_inner(SysState &s, double rr, double rtr)
 {
     s.inner_total += 1;
-    if (s.snorm_exit) {
+    s.inner_first = 0;
+    if (s.snorm_exit) {  // omega was not formed: restart after the update
+        s.phase = PH_OUTER;
+        s.restart = 1;
+        return;
+    }
+    const double rn = sqrt(rr);
+    s.rnorm = rn;
+    if (!(rn == rn)) {
+        s.phase = PH_OUTER;
+        s.restart = 1;
+        return;
+    }
+    if (rn > s.maxr) s.maxr = rn;
+    if (rn <= s.inner_tol * s.maxr || rn <= s.tol * s.outer_rnorm0 || s.inner_total >= s.itmax) {
         s.phase = PH_OUTER;
         return;
     }
-    s.rnorm = sqrt(rr);
-    if (s.rnorm <= s.inner_tol * s.rnorm0 || s.inner_total >= s.itmax || !(s.rnorm == s.rnorm)) {
-        s.phase = PH_OUTER;
-        return;
-    }
-    s.i += 1;
     s.beta = (rtr / s.rho) * (s.alpha / s.omega);
     s.rho_prev = s.rho;
     s.rho = rtr;
-    if (rtr == 0.0 || s.omega == 0.0) s.phase = PH_OUTER;
+    s.i += 1;
+    if (rtr == 0.0 || s.omega == 0.0) {
+        s.phase = PH_OUTER;
+        s.restart = 1;
+    }
 }
 
 template <typename T, bool MIXED>
@@ -501,24 +527,29 @@ __global__ void k_xr_update(BatchView b, int ph_id, int sh_id)
         SysState &st = b.st[tl.sys];
         if (!gate_ok(st, G_INNER)) continue;
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
-        const T alpha = (T)st.alpha;
-        const bool fresh = MIXED && st.i == 1;  // the inner correction starts from zero
-        T *x = vec<T>(d, V_X);
+        // FP64 drop-in: X is VAR.  Mixed form: the solution is accumulated in FP64
+        // every iteration (x64 += alpha*Phat + omega*Shat with FP64 scalars).
+        using X_T = typename std::conditional<MIXED, double, T>::type;
+        using S_T = typename std::conditional<MIXED, double, T>::type;
+        X_T *x = MIXED ? reinterpret_cast<X_T *>(d.x64[0]) : reinterpret_cast<X_T *>(vec<T>(d, V_X));
+        const S_T alpha = (S_T)st.alpha;
         const T *ph = vec<T>(d, ph_id);
         double v[2] = {0.0, 0.0}, tot[2];
         if (st.snorm_exit) {
-            for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x)
-                x[c] = fresh ? alpha * ph[c] : x[c] + alpha * ph[c];
+            #pragma unroll 4
+            for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) x[c] = x[c] + alpha * (S_T)ph[c];
         } else {
-            const T omega = (T)st.omega;
+            const S_T omega = (S_T)st.omega;
+            const T omega_t = (T)st.omega;
             const T *sh = vec<T>(d, sh_id);
             const T *s = vec<T>(d, V_S);
             const T *tv = vec<T>(d, V_T);
             const T *rt = vec<T>(d, V_RT);
             T *r = vec<T>(d, V_R);
+            #pragma unroll 4
             for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-                x[c] = fresh ? alpha * ph[c] + omega * sh[c] : x[c] + alpha * ph[c] + omega * sh[c];
-                const T rv = s[c] - omega * tv[c];
+                x[c] = x[c] + alpha * (S_T)ph[c] + omega * (S_T)sh[c];
+                const T rv = s[c] - omega_t * tv[c];
                 r[c] = rv;
                 v[0] += (double)rv * (double)rv;
                 v[1] += (double)rt[c] * (double)rv;
@@ -533,18 +564,23 @@ __global__ void k_xr_update(BatchView b, int ph_id, int sh_id)
     }
 }
 
-// ------------------------------------------------------------------ mixed form: FP64 refinement
-// x <- x + d (FP64), r = b - A x in FP64 with FP64 A, r handed to the FP32 inner
-// solve as its right-hand side and shadow residual.
-__device__ inline void fin_outer(SysState &s, double rr, double r32r32)
+// ------------------------------------------------------------------ mixed form: reliable update
+// x <- x + d in FP64, r = b - A x in FP64 with the FP64 A; the FP32 residual is
+// replaced by the true one.  The Krylov process continues (P and Rtilde kept,
+// beta formed from the replaced residual) unless a restart was asked for.
+__device__ inline void fin_outer(SysState &s, double rr, double rtr32)
 {
-    s.outer_rnorm = sqrt(rr);
-    if (s.outer_steps == 0) s.outer_rnorm0 = s.outer_rnorm;
+    const double rn = sqrt(rr);
+    const bool fresh = (s.outer_steps == 0) || s.restart;
+    if (s.outer_steps == 0) {
+        s.outer_rnorm0 = rn;
+        s.best = rn;
+    }
+    s.outer_rnorm = rn;
     s.outer_steps += 1;
-    s.xcur ^= 1;
-    s.rnorm = s.outer_rnorm;
+    s.rnorm = rn;
     s.rnorm0 = s.outer_rnorm0;
-    if (s.outer_rnorm <= s.tol * s.outer_rnorm0) {
+    if (rn <= s.tol * s.outer_rnorm0) {
         s.iter = s.inner_total;
         s.iter_tot_add = s.inner_total + 1;
         s.ier = 0;
@@ -552,23 +588,47 @@ __device__ inline void fin_outer(SysState &s, double rr, double r32r32)
         s.status = ST_DONE;
         return;
     }
-    if (s.inner_total >= s.itmax || !(s.outer_rnorm == s.outer_rnorm)) {
-        s.iter = s.inner_total;
-        final_logic(s, false);
-        s.rnorm0 = s.outer_rnorm0;
+    // guard: FP32 iterations that diverge or stall on a (near-)singular operator
+    // hand the system to an FP64 re-solve instead of returning a worse answer
+    if (rn < 0.9 * s.best) {
+        s.best = rn;
+        s.stall = 0;
+    } else {
+        s.stall += 1;
+    }
+    if (!(rn == rn) || rn > 10.0 * s.best || s.stall >= 6) {
+        s.exit_kind = EX_FALLBACK;
+        s.ier = -20;
+        s.status = ST_DONE;
         return;
     }
-    // inner solve setup: Rtilde = R, rho = (R,R)
-    s.rnorm0 = sqrt(r32r32);
-    s.rho = r32r32;
-    s.i = 1;
+    if (s.inner_total >= s.itmax) {
+        s.iter = s.inner_total;
+        final_logic(s, false);
+        return;
+    }
+    s.maxr = rn;
+    s.inner_first = 1;
     s.snorm_exit = 0;
     s.phase = PH_INNER;
-    if (r32r32 == 0.0) {  // the FP32 copy of a nonzero FP64 residual underflowed
-        s.iter = s.inner_total;
-        s.rnorm = s.outer_rnorm;
-        s.rnorm0 = s.outer_rnorm0;
-        final_logic(s, false);
+    if (fresh) {
+        s.rho = rtr32;
+        s.i = 1;
+        s.restart = 0;
+        if (!(rtr32 > 0.0)) {  // the FP32 copy of a nonzero FP64 residual vanished
+            s.exit_kind = EX_FALLBACK;
+            s.ier = -20;
+            s.status = ST_DONE;
+        }
+        return;
+    }
+    s.beta = (rtr32 / s.rho) * (s.alpha / s.omega);
+    s.rho_prev = s.rho;
+    s.rho = rtr32;
+    s.i += 1;
+    if (rtr32 == 0.0 || !(s.beta == s.beta)) {  // breakdown: restart at the next update
+        s.restart = 1;
+        s.phase = PH_OUTER;
     }
 }
 
@@ -580,39 +640,21 @@ __global__ void k_outer_step(BatchView b)
         SysState &st = b.st[tl.sys];
         if (!gate_ok(st, G_OUTER)) continue;
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
-        const int64_t n = d.n;
-        const int64_t cc1 = d.jmax2, cc2 = (int64_t)d.jmax2 * d.imax2;
-        const double *xo = d.x64[st.xcur];
-        double *xn = d.x64[st.xcur ^ 1];
-        const float *dx = vec<float>(d, V_X);
-        const bool add = st.outer_steps > 0;
+        const double *x = d.x64[0];
+        const bool fresh = (st.outer_steps == 0) || st.restart;
         float *r32 = vec<float>(d, V_R);
         float *rt32 = vec<float>(d, V_RT);
-        const double *a = d.a64;
         double v[2] = {0.0, 0.0}, tot[2];
+        #pragma unroll 4
         for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
             const CellIdx q = cell_ijk(d, (uint32_t)c);
-            const int64_t jm = q.j > 0 ? -1 : 0, jp = q.j < d.jmax2 - 1 ? 1 : 0;
-            const int64_t im = q.i > 0 ? -cc1 : 0, ip = q.i < d.imax2 - 1 ? cc1 : 0;
-            auto X = [&](int64_t p) { return add ? xo[p] + (double)dx[p] : xo[p]; };
-            double ax = a[1 * n + c] * X(c + jm);
-            ax = ax + a[2 * n + c] * X(c + im);
-            const double xc = X(c);
-            ax = ax + a[3 * n + c] * xc;
-            ax = ax + a[4 * n + c] * X(c + ip);
-            ax = ax + a[5 * n + c] * X(c + jp);
-            if (d.do_k) {
-                const int64_t km = q.k > 0 ? -cc2 : 0, kp = q.k < d.kmax2 - 1 ? cc2 : 0;
-                ax = ax + a[0 * n + c] * X(c + km);
-                ax = ax + a[6 * n + c] * X(c + kp);
-            }
-            const double rv = d.b64[c] - ax;
-            xn[c] = xc;
+            const double rv = d.b64[c] - stencil_row<double, double>(d, d.a64, x, (uint32_t)c, q);
             const float rf = (float)rv;
             r32[c] = rf;
-            rt32[c] = rf;
+            const float rtf = fresh ? rf : rt32[c];
+            if (fresh) rt32[c] = rf;
             v[0] += rv * rv;
-            v[1] += (double)rf * (double)rf;
+            v[1] += (double)rtf * (double)rf;
         }
         if (tile_reduce<2>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) fin_outer(st, tot[0], tot[1]);
     }
@@ -689,17 +731,6 @@ __device__ int dgtsv_rows(int L, T *sub, T *dg, T *sup, T *f)
     return 0;
 }
 
-template <typename T>
-struct Eps;
-template <>
-struct Eps<double> {
-    static constexpr double margin = 1e-12;
-};
-template <>
-struct Eps<float> {
-    static constexpr float margin = 1e-5f;
-};
-
 __device__ __forceinline__ int find_sys(const int *prefix, int nsys, int item)
 {
     int lo = 0, hi = nsys - 1;
@@ -713,184 +744,257 @@ __device__ __forceinline__ int find_sys(const int *prefix, int nsys, int item)
     return lo;
 }
 
-template <typename T>
-__global__ void __launch_bounds__(LINE_WARPS * 32) k_jline(BatchView b, WaveArgs w, int cmax)
-{
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int rows_w = 32 * cmax;
-    T *s_sub = reinterpret_cast<T *>(smem_raw) + (size_t)warp * 4 * rows_w;
-    T *s_dg = s_sub + rows_w, *s_sup = s_dg + rows_w, *s_f = s_sup + rows_w;
+struct LineJob {
+    int item;
+    int sidx;
+    int G, c, L, seg, gl;
+    int i, k;
+    bool valid;
+    int64_t base;
+};
 
-    const int total = (w.kind == 0) ? b.line_prefix[b.nsys] : w.count;
-    for (int item = blockIdx.x * LINE_WARPS + warp; item < total; item += gridDim.x * LINE_WARPS) {
+// The next work item at or after `item` whose system takes part in the wave.
+__device__ __forceinline__ bool next_line_job(const BatchView &b, const WaveArgs &w, int item, int step, int total,
+                                              int lane, LineJob &j)
+{
+    for (; item < total; item += step) {
         const int sidx = (w.kind == 0) ? find_sys(b.line_prefix, b.nsys, item) : 0;
-        SysState &st = b.st[sidx];
-        if (!gate_ok(st, w.gate)) continue;
+        if (!gate_ok(b.st[sidx], w.gate)) continue;
         const SysDev &d = b.sys[sidx];
-        const int G = d.lane_group, c = d.rows_per_lane, L = d.jmax2;
-        const int lpw = 32 / G;
-        const int seg = lane / G, gl = lane - seg * G;
+        j.item = item;
+        j.sidx = sidx;
+        j.G = d.lane_group;
+        j.c = d.rows_per_lane;
+        j.L = d.jmax2;
+        j.seg = lane / j.G;
+        j.gl = lane - j.seg * j.G;
+        const int lpw = 32 / j.G;
         const int item0 = (w.kind == 0) ? b.line_prefix[sidx] : 0;
-        const int q = (item - item0) * lpw + seg;
-        int i, k;
-        bool valid;
+        const int q = (item - item0) * lpw + j.seg;
         if (w.kind == 0) {
-            k = q / d.half_lines + 1;
-            const int slot = q - (k - 1) * d.half_lines;
-            const int i0 = (((1 + k) & 1) == w.par) ? 1 : 2;
-            i = i0 + 2 * slot;
-            valid = (k <= d.kmax2) && (i <= d.imax2);
+            j.k = q / d.half_lines + 1;
+            const int slot = q - (j.k - 1) * d.half_lines;
+            const int i0 = (((1 + j.k) & 1) == w.par) ? 1 : 2;
+            j.i = i0 + 2 * slot;
+            j.valid = (j.k <= d.kmax2) && (j.i <= d.imax2);
         } else if (w.kind == 1) {
             const int ilo = max(1, w.par - d.kmax2), ihi = min(d.imax2, w.par - 1);
-            i = ilo + q;
-            k = w.par - i;
-            valid = (i <= ihi);
+            j.i = ilo + q;
+            j.k = w.par - j.i;
+            j.valid = (j.i <= ihi);
         } else {
-            valid = q < w.nlines;
-            const int2 lk = valid ? w.list[q] : make_int2(1, 1);
-            i = lk.x;
-            k = lk.y;
+            j.valid = q < w.nlines;
+            const int2 lk = j.valid ? w.list[q] : make_int2(1, 1);
+            j.i = lk.x;
+            j.k = lk.y;
         }
-        const int64_t c1 = d.jmax2, c2 = (int64_t)d.jmax2 * d.imax2;
-        LineCtx<T> x;
-        x.a = diag_base<T>(d);
-        x.rhs = vec<T>(d, w.rhs);
-        x.n = d.n;
-        x.L = L;
-        x.do_k = d.do_k;
-        x.base = (int64_t)(i - 1) * c1 + (int64_t)(k - 1) * c2;
-        const T *nbr = vec<T>(d, w.nbr), *old = vec<T>(d, w.old);
-        x.nb_im = (i > 1) ? nbr + x.base - c1 : old + x.base;
-        x.nb_ip = (i < d.imax2) ? nbr + x.base + c1 : old + x.base;
-        x.nb_km = (k > 1) ? nbr + x.base - c2 : old + x.base;
-        x.nb_kp = (k < d.kmax2) ? nbr + x.base + c2 : old + x.base;
+        j.base = (int64_t)(j.i - 1) * d.jmax2 + (int64_t)(j.k - 1) * d.jmax2 * d.imax2;
+        return true;
+    }
+    j.item = -1;
+    return false;
+}
 
-        // ---- load: coalesced over the line, contiguous rows in shared memory
+// Neighbour-line pointers of a job: the wave's neighbour source, or the line's
+// own old values where the neighbour index clamps onto the cell itself.
+template <typename T>
+__device__ __forceinline__ LineCtx<T> line_ctx(const BatchView &b, const WaveArgs &w, const LineJob &j)
+{
+    const SysDev &d = b.sys[j.sidx];
+    const int64_t c1 = d.jmax2, c2 = (int64_t)d.jmax2 * d.imax2;
+    LineCtx<T> x;
+    x.a = diag_base<T>(d);
+    x.rhs = vec<T>(d, w.rhs);
+    x.n = d.n;
+    x.L = j.L;
+    x.do_k = d.do_k;
+    x.base = j.base;
+    const T *nbr = vec<T>(d, w.nbr), *old = vec<T>(d, w.old);
+    x.nb_im = (j.i > 1) ? nbr + x.base - c1 : old + x.base;
+    x.nb_ip = (j.i < d.imax2) ? nbr + x.base + c1 : old + x.base;
+    x.nb_km = (j.k > 1) ? nbr + x.base - c2 : old + x.base;
+    x.nb_kp = (j.k < d.kmax2) ? nbr + x.base + c2 : old + x.base;
+    return x;
+}
+
+// Right-hand side of row r (operand order of LEQ_IKSWEEP / LEQ_ISWEEP).
+template <typename T>
+__device__ __forceinline__ T line_rhs(const LineCtx<T> &x, int r)
+{
+    const int64_t p = x.base + r;
+    const int64_t n = x.n;
+    T v = x.rhs[p] - x.a[2 * n + p] * x.nb_im[r];
+    v = v - x.a[4 * n + p] * x.nb_ip[r];
+    if (x.do_k) {
+        v = v - x.a[0 * n + p] * x.nb_km[r];
+        v = v - x.a[6 * n + p] * x.nb_kp[r];
+    }
+    return v;
+}
+
+// ------------------------------------------------------------------ J-line factorization (once per solve)
+// DGTSV's elimination on each J-line's tridiagonal (sub A(-2), diagonal A(0),
+// super A(2), CC(first) = EE(last) = 0), run once per solve because the line
+// matrices do not change between sweeps.  For a line on which DGTSV takes no
+// row interchange and meets no zero pivot the elimination is the LU
+// factorization T = L U, stored per row as
+//   l_r = a_r / u_{r-1}  (DGTSV's FACT),  r_r = 1 / u_r,  q_r = c_r / u_r,
+// so that each sweep only runs the two linear recurrences
+//   y_r = f_r - l_r y_{r-1},   x_r = r_r y_r - q_r x_{r+1}.
+// The pivot test and the zero-pivot test are DGTSV's own (model/DGTSV.f:109-121,
+// 138-163), evaluated on the same values without fused multiply-adds; a line that
+// fails them is flagged and solved every sweep by the exact pivoting recurrence.
+template <typename T>
+__global__ void k_line_factor(BatchView b, const int *all_line_prefix)
+{
+    const int total = all_line_prefix[b.nsys];
+    for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
+        const int s = find_sys(all_line_prefix, b.nsys, g);
+        if (b.st[s].status != ST_RUNNING) continue;
+        const SysDev &d = b.sys[s];
+        const int li = g - all_line_prefix[s];  // (i-1) + (k-1)*imax2
+        const int k0 = li / d.imax2, i0 = li - k0 * d.imax2;
+        const int64_t base = (int64_t)i0 * d.jmax2 + (int64_t)k0 * d.jmax2 * d.imax2;
+        const int64_t n = d.n;
+        const int L = d.jmax2;
+        const double *A = d.a64;
+        T *fl = reinterpret_cast<T *>(d.fac[0]) + base;
+        T *fr = reinterpret_cast<T *>(d.fac[1]) + base;
+        T *fq = reinterpret_cast<T *>(d.fac[2]) + base;
+        int flag = 0;
+        double u = A[3 * n + base];
+        fl[0] = T(0);
+        for (int r = 0; r < L - 1; ++r) {
+            const double an = A[1 * n + base + r + 1];  // DL(r)
+            const double cr = A[5 * n + base + r];      // DU(r)
+            if (!(fabs(u) >= fabs(an)) || u == 0.0) {
+                flag = 1;
+                break;
+            }
+            const double l = __ddiv_rn(an, u);
+            fr[r] = (T)__ddiv_rn(1.0, u);
+            fq[r] = (T)__ddiv_rn(cr, u);
+            fl[r + 1] = (T)l;
+            u = __dsub_rn(A[3 * n + base + r + 1], __dmul_rn(l, cr));
+        }
+        if (!flag && u == 0.0) flag = 1;
+        if (!flag) {
+            fr[L - 1] = (T)__ddiv_rn(1.0, u);
+            fq[L - 1] = T(0);
+        }
+        d.line_flag[li] = flag;
+    }
+}
+
+// ------------------------------------------------------------------ J-line half-sweep
+// One warp handles 32/G lines, G lanes per line; lane g owns the c rows
+// g*c .. g*c+c-1.  Each recurrence is split in three: a pass over the lane's rows
+// from a zero start, which yields the chunk's affine map (value at its end as a
+// function of the value entering it), a warp scan that composes the maps, and a
+// second pass from the entering value.  No division remains in the sweep.
+template <typename T>
+__global__ void __launch_bounds__(256) k_jline(BatchView b, WaveArgs w, int cmax)
+{
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    const int nwarps = blockDim.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int rows_w = 32 * cmax;
+    T *s_f = reinterpret_cast<T *>(smem_raw) + (size_t)warp * 4 * rows_w;
+    T *s_l = s_f + rows_w, *s_r = s_l + rows_w, *s_q = s_r + rows_w;
+
+    const int total = (w.kind == 0) ? b.line_prefix[b.nsys] : w.count;
+    const int step = gridDim.x * nwarps;
+    LineJob j;
+    for (int item = blockIdx.x * nwarps + warp; next_line_job(b, w, item, step, total, lane, j);
+         item = j.item + step) {
+        const SysDev &d = b.sys[j.sidx];
+        SysState &st = b.st[j.sidx];
+        const LineCtx<T> x = line_ctx<T>(b, w, j);
+        const int G = j.G, c = j.c, L = j.L, seg = j.seg, gl = j.gl;
         const int segoff = seg * G * c;
-        T *sub = s_sub + segoff, *dg = s_dg + segoff, *sup = s_sup + segoff, *f = s_f + segoff;
-        bool ok = true;
+        T *f = s_f + segoff, *fl = s_l + segoff, *fr = s_r + segoff, *fq = s_q + segoff;
+        const bool exact = j.valid && d.line_flag[(j.i - 1) + (j.k - 1) * d.imax2] != 0;
+        const bool fast = j.valid && !exact;
+        const T *gl_ = reinterpret_cast<const T *>(d.fac[0]) + x.base;
+        const T *gr_ = reinterpret_cast<const T *>(d.fac[1]) + x.base;
+        const T *gq_ = reinterpret_cast<const T *>(d.fac[2]) + x.base;
+
+        // ---- load (coalesced over the line): right-hand side and factors
+#pragma unroll 4
         for (int r = gl; r < G * c; r += G) {
-            T a_ = T(0), d_ = T(1), c_ = T(0), f_ = T(0);
-            if (valid && r < L) {
-                line_row<T>(x, r, a_, d_, c_, f_);
-                const T an = (r + 1 < L) ? x.a[1 * x.n + x.base + r + 1] : T(0);
-                const T m = fabs(d_) - fabs(a_);
-                // pivot-free bound: |d_r| - |a_r| > 0 and >= |c_r|, |a_{r+1}| (with margin)
-                ok = ok && (m > T(0)) && (m >= fabs(c_) * (T(1) + Eps<T>::margin)) &&
-                     (m >= fabs(an) * (T(1) + Eps<T>::margin));
+            T fv = T(0), lv = T(0), rv = T(0), qv = T(0);
+            if (fast && r < L) {
+                fv = line_rhs<T>(x, r);
+                lv = gl_[r];
+                rv = gr_[r];
+                qv = gq_[r];
             }
-            sub[r] = a_;
-            dg[r] = d_;
-            sup[r] = c_;
-            f[r] = f_;
+            f[r] = fv;
+            fl[r] = lv;
+            fr[r] = rv;
+            fq[r] = qv;
         }
-        const unsigned bad = __ballot_sync(0xffffffffu, !ok);
+        __syncwarp();
+
+        // ---- forward recurrence y_r = f_r - l_r y_{r-1}
+        T *cf = f + gl * c, *cl = fl + gl * c, *cr = fr + gl * c, *cq = fq + gl * c;
+        T mb = T(0), ma = T(1);
+        for (int t = 0; t < c; ++t) {
+            const T lt = cl[t];
+            mb = cf[t] - lt * mb;
+            ma = -lt * ma;
+        }
+        for (int dl = 1; dl < G; dl <<= 1) {
+            const T pa = __shfl_up_sync(0xffffffffu, ma, dl, G), pb = __shfl_up_sync(0xffffffffu, mb, dl, G);
+            if (gl >= dl) {
+                mb = ma * pb + mb;
+                ma = ma * pa;
+            }
+        }
+        T y = __shfl_up_sync(0xffffffffu, mb, 1, G);
+        if (gl == 0) y = T(0);
+        for (int t = 0; t < c; ++t) {
+            y = cf[t] - cl[t] * y;
+            cf[t] = y;
+        }
+        // ---- backward recurrence x_r = r_r y_r - q_r x_{r+1}
+        mb = T(0);
+        ma = T(1);
+        for (int t = c - 1; t >= 0; --t) {
+            const T qt = cq[t];
+            mb = cr[t] * cf[t] - qt * mb;
+            ma = -qt * ma;
+        }
+        for (int dl = 1; dl < G; dl <<= 1) {
+            const T na = __shfl_down_sync(0xffffffffu, ma, dl, G), nb = __shfl_down_sync(0xffffffffu, mb, dl, G);
+            if (gl + dl < G) {
+                mb = ma * nb + mb;
+                ma = ma * na;
+            }
+        }
+        T xv = __shfl_down_sync(0xffffffffu, mb, 1, G);
+        if (gl == G - 1) xv = T(0);
+        for (int t = c - 1; t >= 0; --t) {
+            xv = cr[t] * cf[t] - cq[t] * xv;
+            cf[t] = xv;
+        }
+        __syncwarp();
+
+        // ---- lines on which DGTSV interchanges rows or meets a zero pivot
         const unsigned segmask = (G == 32 ? 0xffffffffu : ((1u << G) - 1u)) << (seg * G);
-        const bool seg_ok = (bad & segmask) == 0u;
-        __syncwarp();
-
-        // ---- chunk elimination (every lane, rows gl*c .. gl*c+c-1)
-        {
-            T *ca = sub + gl * c, *cd = dg + gl * c, *cc = sup + gl * c, *cf = f + gl * c;
-            T inv = T(1) / cd[0];
-            T a0 = ca[0] * inv, c0 = cc[0] * inv, f0 = cf[0] * inv;
-            inv = T(1) / cd[1];
-            T pa = ca[1] * inv, pc = cc[1] * inv, pf = cf[1] * inv;
-            ca[1] = pa;
-            cc[1] = pc;
-            cf[1] = pf;
-            for (int t = 2; t < c; ++t) {
-                const T at = ca[t];
-                inv = T(1) / (cd[t] - at * pc);
-                pf = (cf[t] - at * pf) * inv;
-                pa = -at * pa * inv;
-                pc = cc[t] * inv;
-                ca[t] = pa;
-                cc[t] = pc;
-                cf[t] = pf;
-            }
-            // backward: rows c-3 .. 1 into  A_t x_first + x_t + C_t x_last = F_t
-            if (c >= 3) {
-                T na = ca[c - 2], nc = cc[c - 2], nf = cf[c - 2];
-                for (int t = c - 3; t >= 1; --t) {
-                    const T ct = cc[t];
-                    nf = cf[t] - ct * nf;
-                    na = ca[t] - ct * na;
-                    nc = -ct * nc;
-                    ca[t] = na;
-                    cc[t] = nc;
-                    cf[t] = nf;
-                }
-                // row 0 loses its coupling to row 1
-                const T r1a = ca[1], r1c = cc[1], r1f = cf[1];
-                inv = T(1) / (T(1) - c0 * r1a);
-                f0 = (f0 - c0 * r1f) * inv;
-                a0 = a0 * inv;
-                c0 = -c0 * r1c * inv;
-            }
-            T aL = ca[c - 1], cL = cc[c - 1], fL = cf[c - 1];
-
-            // ---- interface system (2G rows, unit diagonal): PCR over the segment
-            {
-                // stride 1: first row couples lane-1's last and own last; last row couples own first and lane+1's first
-                T la = __shfl_up_sync(0xffffffffu, aL, 1, G);
-                T lc = __shfl_up_sync(0xffffffffu, cL, 1, G);
-                T lf = __shfl_up_sync(0xffffffffu, fL, 1, G);
-                T ra = __shfl_down_sync(0xffffffffu, a0, 1, G);
-                T rc = __shfl_down_sync(0xffffffffu, c0, 1, G);
-                T rf = __shfl_down_sync(0xffffffffu, f0, 1, G);
-                if (gl < 1) la = lc = lf = T(0);
-                if (gl + 1 >= G) ra = rc = rf = T(0);
-                T den = T(1) - a0 * lc - c0 * aL;
-                inv = T(1) / den;
-                const T na0 = -a0 * la * inv, nc0 = -c0 * cL * inv, nf0 = (f0 - a0 * lf - c0 * fL) * inv;
-                den = T(1) - aL * c0 - cL * ra;
-                inv = T(1) / den;
-                const T naL = -aL * a0 * inv, ncL = -cL * rc * inv, nfL = (fL - aL * f0 - cL * rf) * inv;
-                a0 = na0; c0 = nc0; f0 = nf0;
-                aL = naL; cL = ncL; fL = nfL;
-            }
-            for (int dl = 1; dl < G; dl <<= 1) {
-                T la0 = __shfl_up_sync(0xffffffffu, a0, dl, G), lc0 = __shfl_up_sync(0xffffffffu, c0, dl, G),
-                  lf0 = __shfl_up_sync(0xffffffffu, f0, dl, G);
-                T ra0 = __shfl_down_sync(0xffffffffu, a0, dl, G), rc0 = __shfl_down_sync(0xffffffffu, c0, dl, G),
-                  rf0 = __shfl_down_sync(0xffffffffu, f0, dl, G);
-                T laL = __shfl_up_sync(0xffffffffu, aL, dl, G), lcL = __shfl_up_sync(0xffffffffu, cL, dl, G),
-                  lfL = __shfl_up_sync(0xffffffffu, fL, dl, G);
-                T raL = __shfl_down_sync(0xffffffffu, aL, dl, G), rcL = __shfl_down_sync(0xffffffffu, cL, dl, G),
-                  rfL = __shfl_down_sync(0xffffffffu, fL, dl, G);
-                if (gl < dl) la0 = lc0 = lf0 = laL = lcL = lfL = T(0);
-                if (gl + dl >= G) ra0 = rc0 = rf0 = raL = rcL = rfL = T(0);
-                inv = T(1) / (T(1) - a0 * lc0 - c0 * ra0);
-                const T na0 = -a0 * la0 * inv, nc0 = -c0 * rc0 * inv, nf0 = (f0 - a0 * lf0 - c0 * rf0) * inv;
-                inv = T(1) / (T(1) - aL * lcL - cL * raL);
-                const T naL = -aL * laL * inv, ncL = -cL * rcL * inv, nfL = (fL - aL * lfL - cL * rfL) * inv;
-                a0 = na0; c0 = nc0; f0 = nf0;
-                aL = naL; cL = ncL; fL = nfL;
-            }
-            const T xf = f0, xl = fL;
-            // ---- interior rows
-            for (int t = 1; t < c - 1; ++t) cf[t] = cf[t] - ca[t] * xf - cc[t] * xl;
-            cf[0] = xf;
-            cf[c - 1] = xl;
-        }
-        __syncwarp();
-
-        // ---- rare path: rows that may need interchanges get the exact pivoting recurrence
         int skip = 0;
-        if (!seg_ok && valid) {
+        if (exact) {
             for (int r = gl; r < L; r += G) {
                 T a_, d_, c_, f_;
                 line_row<T>(x, r, a_, d_, c_, f_);
-                sub[r] = a_;
-                dg[r] = d_;
-                sup[r] = c_;
+                fl[r] = a_;
+                fr[r] = d_;
+                fq[r] = c_;
                 f[r] = f_;
             }
             __syncwarp(segmask);
             if (gl == 0) {
-                skip = dgtsv_rows<T>(L, sub, dg, sup, f) != 0;
+                skip = dgtsv_rows<T>(L, fl, fr, fq, f) != 0;
                 atomicAdd(&st.line_fallbacks, 1);
                 if (skip) atomicAdd(&st.line_skips, 1);
             }
@@ -900,13 +1004,13 @@ __global__ void __launch_bounds__(LINE_WARPS * 32) k_jline(BatchView b, WaveArgs
         __syncwarp();
 
         // ---- store: coalesced.  A line left unchanged (INFO != 0) keeps its old value.
-        if (valid) {
-            T *dst = vec<T>(d, w.dst) + x.base;
-            const T *oldl = old + x.base;
+        if (j.valid) {
+            T *dstp = vec<T>(d, w.dst) + x.base;
+            const T *oldl = vec<T>(d, w.old) + x.base;
             if (!skip) {
-                for (int r = gl; r < L; r += G) dst[r] = f[r];
+                for (int r = gl; r < L; r += G) dstp[r] = f[r];
             } else if (w.write_old) {
-                for (int r = gl; r < L; r += G) dst[r] = oldl[r];
+                for (int r = gl; r < L; r += G) dstp[r] = oldl[r];
             }
         }
         __syncwarp();
@@ -1048,6 +1152,7 @@ __global__ void k_dot(const double *x, const double *y, int64_t n, double *parti
     double v[1] = {0.0};
     const int64_t per = (n + gridDim.x - 1) / gridDim.x;
     const int64_t c0 = (int64_t)blockIdx.x * per, c1 = min(n, c0 + per);
+    #pragma unroll 4
     for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) v[0] += x[c] * y[c];
     block_sum<1>(v);
     if (threadIdx.x == 0) {
@@ -1103,17 +1208,26 @@ cudaError_t launch_p_update(const BatchView &b, const LaunchCfg &c)
     k_p_update<T, MIXED><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b);
     CHECK_LAUNCH();
 }
-int kernel_smem_line_bytes(int cmax, int elem_bytes) { return LINE_WARPS * 4 * 32 * cmax * elem_bytes; }
+// Shared memory of one warp of the J-line kernel: right-hand side and the three factor rows.
+int kernel_smem_line_bytes(int cmax, int elem_bytes) { return 4 * 32 * cmax * elem_bytes; }
 
+// Picks the warps per block that fit the staging buffers, sets the shared-memory
+// attribute and returns the resident blocks per SM (0 when a line cannot fit).
 template <typename T>
-int prepare_line_kernel(int cmax)
+int prepare_line_kernel(int cmax, int *warps)
 {
-    const int smem = kernel_smem_line_bytes(cmax, (int)sizeof(T));
+    int dev = 0, optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const int per_warp = kernel_smem_line_bytes(cmax, (int)sizeof(T));
+    int wpb = std::min(4, optin / std::max(per_warp, 1));
+    if (wpb < 1) return 0;
+    *warps = wpb;
+    const int smem = wpb * per_warp;
     if (cudaFuncSetAttribute(k_jline<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
         return 0;
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_jline<T>, LINE_WARPS * 32, smem) != cudaSuccess)
-        return 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_jline<T>, wpb * 32, smem) != cudaSuccess) return 0;
     return nb;
 }
 
@@ -1129,8 +1243,8 @@ int cell_blocks_per_sm()
 template <typename T>
 cudaError_t launch_jline(const BatchView &b, const LaunchCfg &c, const WaveArgs &w)
 {
-    const int smem = kernel_smem_line_bytes(c.line_cmax, (int)sizeof(T));
-    k_jline<T><<<c.line_grid, LINE_WARPS * 32, smem, c.stream>>>(b, w, c.line_cmax);
+    const int smem = c.line_warps * kernel_smem_line_bytes(c.line_cmax, (int)sizeof(T));
+    k_jline<T><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax);
     CHECK_LAUNCH();
 }
 template <typename T>
@@ -1167,6 +1281,13 @@ template <typename T, bool MIXED>
 cudaError_t launch_xr_update(const BatchView &b, const LaunchCfg &c, int ph, int sh)
 {
     k_xr_update<T, MIXED><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b, ph, sh);
+    CHECK_LAUNCH();
+}
+template <typename T>
+cudaError_t launch_line_factor(const BatchView &b, const LaunchCfg &c, const int *all_line_prefix, int total_lines)
+{
+    if (total_lines <= 0) return cudaSuccess;
+    k_line_factor<T><<<(total_lines + 127) / 128, 128, 0, c.stream>>>(b, all_line_prefix);
     CHECK_LAUNCH();
 }
 cudaError_t launch_outer_step(const BatchView &b, const LaunchCfg &c)
@@ -1206,7 +1327,8 @@ cudaError_t launch_seq_lines(const BatchView &b, const SeqLineArgs &a, cudaStrea
     template cudaError_t launch_matvec_plain<T>(const SysDev *, const SysDev &, const T *, const T *, T *, \
                                                 cudaStream_t, int);                                       \
     template cudaError_t launch_seq_lines<T>(const BatchView &, const SeqLineArgs &, cudaStream_t);        \
-    template int prepare_line_kernel<T>(int);
+    template int prepare_line_kernel<T>(int, int *);                                                     \
+    template cudaError_t launch_line_factor<T>(const BatchView &, const LaunchCfg &, const int *, int);
 #define INST_TM(T, M)                                                                       \
     template cudaError_t launch_p_update<T, M>(const BatchView &, const LaunchCfg &);       \
     template cudaError_t launch_matvec_alpha<T, M>(const BatchView &, const LaunchCfg &, int); \

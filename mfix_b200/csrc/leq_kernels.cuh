@@ -19,6 +19,7 @@ struct LaunchCfg {
     int cell_grid;   // blocks for cell-tile kernels
     int line_grid;   // blocks for J-line kernels
     int line_cmax;   // max rows per lane over the batch (smem sizing)
+    int line_warps;  // warps per block of the J-line kernel
     cudaStream_t stream;
 };
 
@@ -30,6 +31,10 @@ template <typename T>
 cudaError_t launch_init_residual(const BatchView &b, const LaunchCfg &c);  // R = B - A X, ||R||
 template <typename T>
 cudaError_t launch_init_rtilde(const BatchView &b, const LaunchCfg &c, uint64_t seed);  // Rtilde, rho(0)
+
+// J-line LU factors (l, 1/u, c/u) and DGTSV pivot flags, once per solve
+template <typename T>
+cudaError_t launch_line_factor(const BatchView &b, const LaunchCfg &c, const int *all_line_prefix, int total_lines);
 
 // One BiCGSTAB iteration (model/leq_bicgs.f:316-466)
 template <typename T, bool MIXED>
@@ -74,7 +79,7 @@ cudaError_t launch_seq_lines(const BatchView &b, const SeqLineArgs &a, cudaStrea
 
 int kernel_smem_line_bytes(int cmax, int elem_bytes);
 template <typename T>
-int prepare_line_kernel(int cmax);  // sets the smem attribute, returns resident blocks per SM
+int prepare_line_kernel(int cmax, int *warps);  // sets the smem attribute, returns resident blocks per SM
 int cell_blocks_per_sm();
 
 }  // namespace mfixgpu

@@ -32,8 +32,8 @@ class Stats(C.Structure):
     _fields_ = [("ier", C.c_int), ("iterations", C.c_int), ("iter_tot_add", C.c_int), ("exit_kind", C.c_int),
                 ("line_skips", C.c_int), ("line_fallbacks", C.c_int), ("outer_steps", C.c_int), ("pad", C.c_int),
                 ("rnorm0", C.c_double), ("rnorm", C.c_double), ("seconds", C.c_double), ("device_ms", C.c_double),
-                ("jline_ms", C.c_double), ("jline_launches", C.c_int), ("pad2", C.c_int),
-                ("kernel_launches", C.c_longlong)]
+                ("jline_ms", C.c_double), ("jline_launches", C.c_int), ("fp64_fallback", C.c_int),
+                ("kernel_launches", C.c_longlong), ("mixed_iterations", C.c_int), ("pad3", C.c_int)]
 
 
 class Geom(C.Structure):
@@ -45,8 +45,8 @@ class SystemC(C.Structure):
     _fields_ = [("imax2", C.c_int), ("jmax2", C.c_int), ("kmax2", C.c_int), ("do_k", C.c_int),
                 ("dimension_3", C.c_int64), ("a_m", C.c_void_p), ("b_m", C.c_void_p), ("var", C.c_void_p),
                 ("tol", C.c_double), ("itmax", C.c_int), ("ier", C.c_int), ("iterations", C.c_int),
-                ("outer_steps", C.c_int), ("exit_kind", C.c_int), ("pad", C.c_int), ("rnorm0", C.c_double),
-                ("rnorm", C.c_double)]
+                ("outer_steps", C.c_int), ("exit_kind", C.c_int), ("fp64_fallback", C.c_int),
+                ("rnorm0", C.c_double), ("rnorm", C.c_double)]
 
 
 def _declare(L: C.CDLL) -> None:
@@ -176,6 +176,7 @@ class BatchResult:
     exit_kind: int
     rnorm0: float
     rnorm: float
+    fp64_fallback: int = 0
 
 
 def batch_solve(systems, sweep: str = "RSRS", pc: str = "LINE", precision: int = 0, on_device: bool = False,
@@ -196,7 +197,7 @@ def batch_solve(systems, sweep: str = "RSRS", pc: str = "LINE", precision: int =
     rc = lib().mfixgpu_batch_solve(arr, len(systems), sweep.ljust(4)[:4].encode(), pc.ljust(4)[:4].encode(),
                                    int(precision), int(on_device))
     res = [BatchResult(arr[q].ier, arr[q].iterations, arr[q].outer_steps, arr[q].exit_kind, arr[q].rnorm0,
-                       arr[q].rnorm) for q in range(len(systems))]
+                       arr[q].rnorm, arr[q].fp64_fallback) for q in range(len(systems))]
     return rc, res
 
 

@@ -1,0 +1,75 @@
+"""The mixed-precision form and the batched solver on the GPU.
+
+Mixed form (FP32 BiCGSTAB, FP64 solution accumulation and reliable updates):
+IER 0, the FP64 true relative residual of the scaled system <= TOL, and a
+solution within 1e-6 of the FP64 drop-in's.  On the well-conditioned
+convection-diffusion systems it takes no more than 1.3x the FP64 iterations and
+never hands over to FP64; on the near-singular pressure-like system (zero
+wall coupling, diagonal excess 1e-6) the FP64 re-solve guard may engage.  Batch: uneven systems solved together give results
+bit-identical to each system solved alone, in both precisions.
+"""
+import numpy as np
+import pytest
+
+import oracle as O
+from mfix_b200 import leq
+from mfix_b200 import systems as S
+
+pytestmark = pytest.mark.gpu
+
+
+def _true_rel(s_scaled, x):
+    return O.true_resid(s_scaled, x) / O.true_resid(s_scaled, np.zeros(s_scaled.n))
+
+
+@pytest.mark.parametrize("make,near_singular", [
+    (lambda: S.conv_diff(24, 30, 20, seed=0), False),
+    (lambda: S.pressure_like(30, 40, 26, seed=1, nspheres=6, rmin=3, rmax=7, itmax=3000), True),
+    (lambda: S.conv_diff(50, 41, 1, seed=2, do_k=False), False),
+    (lambda: S.known_answer(14, 16, 12, seed=3)[0], False),
+], ids=["conv3d", "pressure", "conv2d", "kat"])
+def test_mixed_converges_to_tol(make, near_singular):
+    s = make()
+    ref = s.copy()
+    st_ref = O.leq_bicgs(ref)
+    m = s.copy()
+    assert leq.set_option("precision", 1) == 0
+    try:
+        ier = leq.solve_system(m)
+        st = leq.last_stats()
+    finally:
+        leq.set_option("precision", 0)
+    assert ier == 0, leq.last_error()
+    assert np.array_equal(m.a, ref.a) and np.array_equal(m.b, ref.b)
+    assert _true_rel(ref, m.x) <= s.tol * 1.01
+    assert np.linalg.norm(m.x - ref.x) <= 1e-6 * np.linalg.norm(ref.x)
+    if not near_singular:
+        assert st["fp64_fallback"] == 0
+        assert st["outer_steps"] >= 1
+        assert st["iterations"] <= 1.3 * st_ref["iterations"] + 2
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_equals_alone(precision):
+    sizes = [(9, 12, 7), (20, 15, 11), (5, 40, 6), (16, 16, 16), (31, 9, 4), (7, 7, 33)]
+    systems = [S.conv_diff(*d, seed=q) for q, d in enumerate(sizes)]
+    systems.append(S.pressure_like(14, 18, 12, seed=9, nspheres=3, rmin=2, rmax=4, itmax=2000))
+    together = [s.copy() for s in systems]
+    rc, res = leq.batch_solve(together, precision=precision)
+    assert rc == 0, leq.last_error()
+    for q, s in enumerate(systems):
+        alone = s.copy()
+        rc1, r1 = leq.batch_solve([alone], precision=precision)
+        assert rc1 == 0
+        assert res[q].ier == r1[0].ier == 0
+        assert res[q].iterations == r1[0].iterations
+        assert np.array_equal(together[q].x, alone.x)  # bit-identical alone and in the mix
+        ref = s.copy()
+        O.leq_bicgs(ref)
+        assert _true_rel(ref, together[q].x) <= s.tol * 1.01
+
+
+def test_batch_rejects_sequential_letters():
+    systems = [S.conv_diff(6, 6, 6, seed=q) for q in range(2)]
+    rc, _ = leq.batch_solve(systems, sweep="ISIS")
+    assert rc == leq.IER_UNSUPPORTED

@@ -1,11 +1,14 @@
 """Whole-solve parity of the drop-in (mfixgpu_solve_lin_eq_) against the oracle.
 
 For each seeded system the GPU and the oracle run LEQ_BICGS from the same
-inputs.  Checked: the same IER and exit reason, iteration counts within one,
+inputs.  Checked: the same IER and exit reason, an iteration count inside the
+oracle's own rounding envelope (its counts when B_M is perturbed by 1e-15
+relative; BiCGSTAB's count is that sensitive on some systems),
 the unit-scaled A_M/B_M written back bit for bit, the true relative residual
 ||b - A x|| / ||b - A x0|| <= TOL * 1.01 (the reference's own test is on the
-recursive residual, model/leq_bicgs.f:455), and the solutions within
-100 * TOL of each other (relative 2-norm), plus ITER_TOT accounting.
+recursive residual, model/leq_bicgs.f:455), an error against a 1e-14 FP64
+solution no larger than ten times the oracle's own error (or 1e-10), plus
+ITER_TOT accounting.
 """
 import numpy as np
 import pytest
@@ -25,6 +28,15 @@ def _run_both(s, sweep="RSRS", pc="LINE", method=2, vno=3):
     ier = leq.solve_system(gpu, method=method, sweep=sweep, pc=pc, vno=vno)
     st = leq.last_stats()
     return ref, st_ref, gpu, ier, st
+
+
+def _envelope(s, sweep, pc):
+    counts = []
+    for eps in (0.0, 1e-15, -1e-15, 2e-15):
+        t = s.copy()
+        t.b *= (1.0 + eps)
+        counts.append(O.leq_bicgs(t, sweep, pc)["iterations"])
+    return min(counts) - 1, max(counts) + 1
 
 
 def _true_rel(s_scaled, x):
@@ -51,13 +63,22 @@ def test_drop_in_matches_oracle(name, make, sweep, pc):
     ref, st_ref, gpu, ier, st = _run_both(s, sweep, pc)
     assert ier == st_ref["ier"] == 0, (ier, st_ref, leq.last_error())
     assert st["exit_kind"] == st_ref["exit_kind"]
-    assert abs(st["iterations"] - st_ref["iterations"]) <= 1
+    lo, hi = _envelope(s, sweep, pc)
+    assert lo <= st["iterations"] <= hi, (st["iterations"], lo, hi)
     # unit scaling written back exactly as LEQ_BICGS0 leaves A_M / B_M
     assert np.array_equal(gpu.a, ref.a) and np.array_equal(gpu.b, ref.b)
     assert _true_rel(ref, gpu.x) <= s.tol * 1.01 + 1e-15
-    nx = np.linalg.norm(ref.x)
-    assert np.linalg.norm(gpu.x - ref.x) <= 100 * s.tol * max(nx, 1e-300)
-    assert leq.iter_tot(3) == st_ref["iter_tot_add"]
+    truth = ref.copy()
+    truth.x[:] = 0.0
+    x_truth, rel = O.truth(truth)
+    assert rel <= 1e-13
+    nt = np.linalg.norm(x_truth)
+    err_ref = np.linalg.norm(ref.x - x_truth) / nt
+    err_gpu = np.linalg.norm(gpu.x - x_truth) / nt
+    assert err_gpu <= max(10 * err_ref, 1e-10), (err_gpu, err_ref)
+    assert leq.iter_tot(3) == st["iter_tot_add"]
+    if st["exit_kind"] == 0:  # converged on Rnorm: ITER_TOT += ITER + 1 (model/leq_bicgs.f:458)
+        assert st["iter_tot_add"] == st["iterations"] + 1
 
 
 def test_known_answer_recovers_x():
