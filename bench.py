@@ -223,6 +223,8 @@ def run_ours(args) -> None:
     sys0 = make_system(w)
     n = sys0.n
     dev = torch.device("cuda", local)
+    if args.line_lanes:
+        leq.set_option("line_lanes", args.line_lanes)
     A0 = torch.from_numpy(sys0.a).to(dev)
     B0 = torch.from_numpy(sys0.b).to(dev)
     A = torch.empty_like(A0)
@@ -261,7 +263,8 @@ def run_ours(args) -> None:
     if args.only != "all":
         for _ in range(max(args.steps, 1)):
             r, st = solve_device(0 if args.only == "fp64" else 1)
-        print(f"{args.only}: iterations {r.iterations} outer {r.outer_steps} device_ms {st['device_ms']:.3f}")
+        print(f"{args.only}: iterations {r.iterations} outer {r.outer_steps} device_ms {st['device_ms']:.3f} "
+              f"line_lanes {leq.autotune_table()}")
         return
 
     # ---- FP64 drop-in (device resident)
@@ -367,6 +370,7 @@ def run_ours(args) -> None:
                  "true_rel_resid": rel64, "alg_gbs": fp64_bytes / (tot_64 / args.steps / 1e3) / 1e9,
                  "gpu_launches": int(fp64_launch)},
         "mixed_vs_fp64": value / fp64_value,
+        "line_tiles": [{"elem_bytes": e, "line_length": l, "lanes_per_line": g} for e, l, g in leq.autotune_table()],
         "wall_s_timed_mixed": wall,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -390,6 +394,7 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--line-lanes", type=int, default=0, help="force lanes per J-line (0: autotuned)")
     ap.add_argument("--only", default="all", choices=["all", "fp64", "mixed"],
                     help="profiling runs: solve only this form (no e2e leg, no JSON line)")
     args = ap.parse_args()

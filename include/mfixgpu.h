@@ -100,9 +100,19 @@ const char *mfixgpu_last_error(void);
  *   "check_every"    iterations between host polls of convergence (default 4)
  *   "use_graph"      1 (default) replay the iteration body as a CUDA graph
  *   "time_kernels"   1: time every J-line sweep launch with CUDA events (no graph replay)
+ *   "autotune"       1 (default): lanes per J-line picked by measurement for each new line length
+ *   "line_lanes"     0 (default) automatic, else lanes per J-line (1..32, rounded down to a power of two)
  * Returns 0, or MFIXGPU_ERR_ARGS for an unknown name. */
 int mfixgpu_set_option(const char *name, double value);
 double mfixgpu_get_option(const char *name);
+
+/* Autotuner of the J-line kernel (no reference counterpart): its choices,
+ * keyed by precision and line length, are read from and written to the JSON
+ * file at `path` (NULL or "" keeps them in memory only). */
+int mfixgpu_autotune_cache(const char *path);
+/* Copies up to max_entries (element bytes, line length, lanes per line) triples
+ * into out[3*i..3*i+2]; returns the number of entries recorded. */
+int mfixgpu_autotune_table(int *out, int max_entries);
 
 /* Releases device memory and the per-device engine. */
 void mfixgpu_finalize(void);

@@ -34,6 +34,8 @@ struct Options {
     int check_every = 4;
     int use_graph = 1;
     int time_kernels = 0;
+    int autotune = 1;
+    int line_lanes = 0;
 };
 
 struct Global {
@@ -103,6 +105,8 @@ SolveOptions make_opts(const Options &o, int pc, const char sweep4[4])
     so.check_every = o.check_every;
     so.use_graph = o.use_graph != 0;
     so.time_kernels = o.time_kernels != 0;
+    so.autotune = o.autotune != 0;
+    so.force_lanes = o.line_lanes;
     return so;
 }
 
@@ -288,6 +292,11 @@ int mfixgpu_set_option(const char *name, double value)
         g.opt.use_graph = value != 0;
     } else if (k == "time_kernels") {
         g.opt.time_kernels = value != 0;
+    } else if (k == "autotune") {
+        g.opt.autotune = value != 0;
+    } else if (k == "line_lanes") {
+        if (value < 0 || value > 32) return MFIXGPU_ERR_ARGS;
+        g.opt.line_lanes = (int)value;
     } else {
         return MFIXGPU_ERR_ARGS;
     }
@@ -307,7 +316,27 @@ double mfixgpu_get_option(const char *name)
     if (k == "check_every") return g.opt.check_every;
     if (k == "use_graph") return g.opt.use_graph;
     if (k == "time_kernels") return g.opt.time_kernels;
+    if (k == "autotune") return g.opt.autotune;
+    if (k == "line_lanes") return g.opt.line_lanes;
     return 0.0;
+}
+
+int mfixgpu_autotune_cache(const char *path)
+{
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    Engine *e = engine_locked(g);
+    if (!e) return MFIXGPU_ERR_CUDA;
+    e->load_tune_cache(path ? std::string(path) : std::string());
+    return 0;
+}
+
+int mfixgpu_autotune_table(int *out, int max_entries)
+{
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    if (!g.engine) return 0;
+    return g.engine->tune_table(out, out ? max_entries : 0);
 }
 
 void mfixgpu_finalize(void)

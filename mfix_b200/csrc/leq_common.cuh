@@ -68,6 +68,7 @@ struct SysDev {
     int64_t n;           // DIMENSION_3 (cells incl. the wall layer)
     FastDiv div_j;       // division by jmax2
     FastDiv div_i;       // division by imax2
+    FastDiv div_h;       // division by half_lines
     int pc;              // PcKind
     int ntiles;          // cell tiles of this system
     int tile_base;       // first tile's slot in the partial-sum array

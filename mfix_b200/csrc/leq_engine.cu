@@ -11,6 +11,7 @@
 
 #include <algorithm>
 #include <cstring>
+#include <cstdio>
 #include <map>
 
 namespace mfixgpu {
@@ -23,8 +24,8 @@ namespace mfixgpu {
 
 static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-// Lanes per J-line: the smallest power of two that leaves about a dozen rows per
-// lane (at most 32); rows per lane rounded up to odd so that lanes reading row t
+// Lanes per J-line: the smallest power of two that leaves at most 12 rows per
+// lane (at most 32 lanes); rows per lane rounded up to odd so that lanes reading row t
 // of their chunks hit distinct shared-memory banks.
 void line_shape(int L, int *G, int *c)
 {
@@ -80,7 +81,8 @@ Engine::Engine()
     cudaEventCreateWithFlags(&ev_b_, cudaEventDisableTiming);
     cudaEventCreate(&ev_t0_);
     cudaEventCreate(&ev_t1_);
-    cell_bpsm_ = cell_blocks_per_sm();
+    cell_occupancy(false, &occ_[0]);
+    cell_occupancy(true, &occ_[1]);
 }
 
 Engine::~Engine()
@@ -156,7 +158,6 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
     h_tiles_.clear();
     h_prefix_.assign(nsys_ + 1, 0);
     h_allprefix_.assign(nsys_ + 1, 0);
-    int cmax = 1;
     int tile_base = 0;
     for (int s = 0; s < nsys_; ++s) {
         const SystemSpec &sp = specs[s];
@@ -172,9 +173,9 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         d.ntiles = (int)((sp.n + TILE_CELLS - 1) / TILE_CELLS);
         d.tile_base = tile_base;
         tile_base += d.ntiles;
-        line_shape(sp.jmax2, &d.lane_group, &d.rows_per_lane);
-        cmax = std::max(cmax, d.rows_per_lane);
+        shape_for(sp.jmax2, mixed ? 4 : 8, opt.force_lanes, &d.lane_group, &d.rows_per_lane);
         d.half_lines = (sp.imax2 + 1) / 2;
+        d.div_h = make_fastdiv((uint32_t)d.half_lines);
         const size_t n = (size_t)sp.n;
         d.a64 = sp.a;
         d.b64 = sp.b;
@@ -188,9 +189,6 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         d.line_flag = (int *)arena_.take((size_t)sp.imax2 * sp.kmax2 * 4);
         if (!mixed) d.vec[V_X] = d.x64[0];
         for (int t = 0; t < d.ntiles; ++t) h_tiles_.push_back(Tile{s, t});
-        const int lpw = 32 / d.lane_group;
-        const int64_t slots = (int64_t)d.half_lines * sp.kmax2;
-        h_prefix_[s + 1] = h_prefix_[s] + (int)((slots + lpw - 1) / lpw);
         h_allprefix_[s + 1] = h_allprefix_[s] + sp.imax2 * sp.kmax2;
 
         SysState &st = h_st_[s];
@@ -209,10 +207,8 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
                                stream_));
 
     // tables are small; their device copies are reallocated only when they grow
-    CK(upload(&d_sys_, &sys_cap_, h_sys_.data(), h_sys_.size(), stream_));
     CK(upload(&d_st_, &st_cap_, h_st_.data(), h_st_.size(), stream_));
     CK(upload(&d_tiles_, &tiles_cap_, h_tiles_.data(), h_tiles_.size(), stream_));
-    CK(upload(&d_prefix_, &prefix_cap_, h_prefix_.data(), h_prefix_.size(), stream_));
     CK(upload(&d_allprefix_, &allprefix_cap_, h_allprefix_.data(), h_allprefix_.size(), stream_));
     const size_t need_part = 2 * (size_t)std::max(tile_base, 1);
     if (need_part > part_cap_) {
@@ -228,25 +224,197 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         h_st_pinned_cap_ = 2 * (size_t)nsys_;
     }
 
-    view_.sys = d_sys_;
     view_.st = d_st_;
     view_.tiles = d_tiles_;
     view_.ntiles = (int)h_tiles_.size();
     view_.nsys = nsys_;
-    view_.line_prefix = d_prefix_;
     view_.partials = d_partials_;
 
     cfg_.stream = stream_;
-    cfg_.line_cmax = cmax;
-    // one block per tile: the block scheduler balances tiles across SMs
+
+    // setup kernels: one block per tile; iteration kernels: persistent grids of
+    // resident blocks that stride over the tiles
     cfg_.cell_grid = std::max(1, view_.ntiles);
+    cfg_.stencil_grid = std::max(1, view_.ntiles);
+    const CellOcc &oc = occ_[mixed ? 1 : 0];
+    auto grid = [&](int bpsm) { return std::max(1, std::min(view_.ntiles, sms_ * bpsm)); };
+    cfg_.g_p = grid(oc.p_update);
+    cfg_.g_s = grid(oc.s_update);
+    cfg_.g_xr = grid(oc.xr_update);
+    cfg_.g_mv = grid(oc.matvec);
+    cfg_.g_copy = grid(oc.copy);
+    cfg_.g_outer = grid(oc.outer);
+    return configure_lines(mixed ? 4 : 8);
+    return 0;
+}
+
+// Work items of the J-line kernel (parity waves) and its launch shape, from each
+// system's lanes per line; the system table goes to the device here.
+int Engine::configure_lines(int elem)
+{
+    h_prefix_.assign(nsys_ + 1, 0);
+    int cmax = 1;
+    for (int s = 0; s < nsys_; ++s) {
+        const SysDev &d = h_sys_[s];
+        cmax = std::max(cmax, d.rows_per_lane);
+        const int lpw = 32 / d.lane_group;
+        const int64_t slots = (int64_t)d.half_lines * d.kmax2;
+        h_prefix_[s + 1] = h_prefix_[s] + (int)((slots + lpw - 1) / lpw);
+    }
+    CK(upload(&d_sys_, &sys_cap_, h_sys_.data(), h_sys_.size(), stream_));
+    CK(upload(&d_prefix_, &prefix_cap_, h_prefix_.data(), h_prefix_.size(), stream_));
+    // the uploads may have (re)allocated the tables: the kernels' view follows them
+    view_.sys = d_sys_;
+    view_.line_prefix = d_prefix_;
+    if (!view_.sys || !view_.st || !view_.tiles || !view_.line_prefix || !view_.partials)
+        return fail("internal: batch tables missing on the device", -13);
+    cfg_.line_cmax = cmax;
     int wpb = 1;
-    const int bpsm = mixed ? prepare_line_kernel<float>(cmax, &wpb) : prepare_line_kernel<double>(cmax, &wpb);
+    const int bpsm = elem == 4 ? prepare_line_kernel<float>(cmax, &wpb) : prepare_line_kernel<double>(cmax, &wpb);
     if (bpsm <= 0) return fail("J-lines too long for the shared-memory staging of the line kernel", -10);
     cfg_.line_warps = wpb;
     const int items = h_prefix_[nsys_];
     cfg_.line_grid = std::max(1, std::min((items + wpb - 1) / wpb, sms_ * bpsm));
     return 0;
+}
+
+static int rows_for(int L, int G)
+{
+    int c = (L + G - 1) / G;
+    if (c < 1) c = 1;
+    if ((c & 1) == 0) ++c;
+    return c;
+}
+
+// Lanes per J-line for a line of length L: a forced value, the autotuner's
+// choice for (precision, L), or the default of line_shape().
+void Engine::shape_for(int L, int elem, int forced, int *G, int *c)
+{
+    if (forced > 0) {
+        int g = 1;
+        while (g * 2 <= std::min(forced, 32)) g *= 2;
+        *G = g;
+        *c = rows_for(L, g);
+        return;
+    }
+    auto it = line_tune_.find(std::make_pair(elem, L));
+    if (it != line_tune_.end()) {
+        *G = it->second;
+        *c = rows_for(L, it->second);
+        return;
+    }
+    line_shape(L, G, c);
+}
+
+// The autotuner: for every line length of the batch without a recorded choice,
+// time a red/black pass of the J-line kernel over the whole batch for each
+// lanes-per-line candidate whose staging fits 48 KB per warp, keep the fastest.
+int Engine::autotune_lines(const SolveOptions &opt, int elem)
+{
+    std::vector<int> todo;
+    for (int s = 0; s < nsys_; ++s) {
+        const int L = h_sys_[s].jmax2;
+        if (line_tune_.count(std::make_pair(elem, L))) continue;
+        if (std::find(todo.begin(), todo.end(), L) == todo.end()) todo.push_back(L);
+    }
+    if (todo.empty()) return 0;
+    WaveArgs w[2] = {};
+    for (int q = 0; q < 2; ++q) {
+        w[q].kind = 0;
+        w[q].par = 1 - q;
+        w[q].rhs = V_P;
+        w[q].nbr = V_PH;
+        w[q].old = V_P;
+        w[q].dst = V_PH;
+        w[q].write_old = 1;
+        w[q].gate = G_ANY;
+    }
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    for (int L : todo) {
+        int best_g = 0;
+        float best_ms = 1e30f;
+        for (int g = 1; g <= 32; g *= 2) {
+            const int c = rows_for(L, g);
+            if ((size_t)kernel_smem_line_bytes(c, elem) > 48 * 1024) continue;
+            for (int s = 0; s < nsys_; ++s)
+                if (h_sys_[s].jmax2 == L) {
+                    h_sys_[s].lane_group = g;
+                    h_sys_[s].rows_per_lane = c;
+                }
+            int rc = configure_lines(elem);
+            if (rc) return rc;
+            float tot = 0.f;
+            for (int rep = 0; rep < 4; ++rep) {
+                if (rep == 1) CK(cudaEventRecord(e0, stream_));
+                for (int q = 0; q < 2; ++q) CK(elem == 4 ? launch_jline<float>(view_, cfg_, w[q]) : launch_jline<double>(view_, cfg_, w[q]));
+            }
+            CK(cudaEventRecord(e1, stream_));
+            CK(cudaEventSynchronize(e1));
+            cudaEventElapsedTime(&tot, e0, e1);
+            if (tot < best_ms) {
+                best_ms = tot;
+                best_g = g;
+            }
+        }
+        if (best_g == 0) {
+            int c_unused = 0;
+            line_shape(L, &best_g, &c_unused);
+        }
+        line_tune_[std::make_pair(elem, L)] = best_g;
+        for (int s = 0; s < nsys_; ++s)
+            if (h_sys_[s].jmax2 == L) {
+                h_sys_[s].lane_group = best_g;
+                h_sys_[s].rows_per_lane = rows_for(L, best_g);
+            }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    (void)opt;
+    save_tune_cache();
+    return configure_lines(elem);
+}
+
+void Engine::load_tune_cache(const std::string &path)
+{
+    tune_path_ = path;
+    FILE *f = path.empty() ? nullptr : std::fopen(path.c_str(), "r");
+    if (!f) return;
+    int elem, L, G;
+    char buf[256];
+    while (std::fgets(buf, sizeof buf, f))
+        if (std::sscanf(buf, " {\"elem\": %d, \"L\": %d, \"lanes\": %d}", &elem, &L, &G) == 3 && G >= 1 && G <= 32)
+            line_tune_[std::make_pair(elem, L)] = G;
+    std::fclose(f);
+}
+
+void Engine::save_tune_cache()
+{
+    if (tune_path_.empty()) return;
+    FILE *f = std::fopen(tune_path_.c_str(), "w");
+    if (!f) return;
+    std::fprintf(f, "[\n");
+    size_t q = 0;
+    for (const auto &kv : line_tune_)
+        std::fprintf(f, "  {\"elem\": %d, \"L\": %d, \"lanes\": %d}%s\n", kv.first.first, kv.first.second, kv.second,
+                     ++q < line_tune_.size() ? "," : "");
+    std::fprintf(f, "]\n");
+    std::fclose(f);
+}
+
+int Engine::tune_table(int *out, int max_entries) const
+{
+    int q = 0;
+    for (const auto &kv : line_tune_) {
+        if (q < max_entries) {
+            out[3 * q] = kv.first.first;
+            out[3 * q + 1] = kv.first.second;
+            out[3 * q + 2] = kv.second;
+        }
+        ++q;
+    }
+    return q;
 }
 
 // ------------------------------------------------------------------ LINE preconditioner plan
@@ -609,6 +777,21 @@ int Engine::run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &
         CK(launch_init_residual<double>(view_, cfg_));
         CK(launch_init_rtilde<double>(view_, cfg_, opt.seed));
         launches_ += 2;
+    }
+    if (opt.pc == PC_LINE && opt.autotune && opt.force_lanes <= 0) {
+        bool rs_only = true;
+        for (int q = 0; q < 4; ++q) {
+            const char ch = opt.sweep[q];
+            if (ch == 'I' || ch == 'i' || ch == 'K' || ch == 'k' || ch == 'A' || ch == 'a') rs_only = false;
+        }
+        if (rs_only) {
+            if ((rc = autotune_lines(opt, elem))) return rc;
+            h_lines_.clear();
+            list_refs_.clear();
+            if ((rc = plan_msolve(opt, V_P, V_PH, gate_p, 0))) return rc;
+            if ((rc = plan_msolve(opt, V_S, V_SH, gate_s, 1))) return rc;
+            if ((rc = bind_lists())) return rc;
+        }
     }
 
     // ---- iteration body (kernels of this library: 6 or 5 plus the sweep plans)

@@ -3,6 +3,7 @@
 // FP32-inner / FP64-refinement form) and the LINE-preconditioner sweep plan.
 #pragma once
 #include <cstdint>
+#include <map>
 #include <mutex>
 #include <string>
 #include <vector>
@@ -50,6 +51,8 @@ struct SolveOptions {
     bool use_graph = true;       // capture the iteration body in a CUDA graph
     bool time_kernels = false;   // record events around every J-line launch (no graph replay)
     bool skip_scale = false;     // the system is unit-scaled already (FP64 re-solve after a mixed attempt)
+    bool autotune = true;        // pick lanes per J-line by measurement for unseen line lengths
+    int force_lanes = 0;         // > 0: lanes per J-line for every system (experiments)
 };
 
 // Device-side timing of the last solve (CUDA events on the engine's stream).
@@ -93,9 +96,22 @@ private:
     int plan_msolve(const SolveOptions &opt, int src, int dst, int gate, int elem);
     int run_msolve_plan(int which, int elem);
     int bind_lists();
+    int configure_lines(int elem);
+    void shape_for(int L, int elem, int forced, int *G, int *c);
+    int autotune_lines(const SolveOptions &opt, int elem);
+    void save_tune_cache();
+
+public:
+    void load_tune_cache(const std::string &path);
+    int tune_table(int *out, int max_entries) const;
+
+private:
+    std::map<std::pair<int, int>, int> line_tune_;  // (element bytes, line length) -> lanes per line
+    std::string tune_path_;
     int fail(const std::string &msg, int code);
 
-    int dev_ = -1, sms_ = 0, cell_bpsm_ = 4;
+    int dev_ = -1, sms_ = 0;
+    CellOcc occ_[2] = {};  // resident blocks per SM of each cell kernel, [fp32]
     cudaStream_t stream_ = nullptr;
     cudaEvent_t ev_a_ = nullptr, ev_b_ = nullptr, ev_t0_ = nullptr, ev_t1_ = nullptr;
     DeviceArena arena_;     // iteration vectors and other per-solve work memory

@@ -305,83 +305,237 @@ __global__ void k_init_rtilde(BatchView b, uint64_t seed)
 }
 
 // ------------------------------------------------------------------ iteration kernels
+// Every cell kernel is persistent (grid = resident blocks) and strides over the
+// batch's tiles.  Inside a tile each thread first loads the operands of U cells
+// into registers and only then computes and stores, so the loads of U cells are
+// in flight together (the stores could otherwise alias the next cells' loads and
+// serialize them).
+
+// Clamped neighbour offsets of cell c (model/set_increments.f:80-109).
+struct Offs {
+    int64_t jm, jp, im, ip, km, kp;
+};
+
+__device__ __forceinline__ Offs cell_offs(const SysDev &d, uint32_t c)
+{
+    const CellIdx q = cell_ijk(d, c);
+    const int64_t c1 = d.jmax2, c2 = (int64_t)d.jmax2 * d.imax2;
+    Offs o;
+    o.jm = q.j > 0 ? -1 : 0;
+    o.jp = q.j < d.jmax2 - 1 ? 1 : 0;
+    o.im = q.i > 0 ? -c1 : 0;
+    o.ip = q.i < d.imax2 - 1 ? c1 : 0;
+    o.km = (d.do_k && q.k > 0) ? -c2 : 0;
+    o.kp = (d.do_k && q.k < d.kmax2 - 1) ? c2 : 0;
+    return o;
+}
+
+// The seven operands of row c of A*x: a[0..6] = A(-2), A(-1), A(0), A(1), A(2), A(-3), A(3)
+// (the order LEQ_MATVEC adds them in, model/leqsol_mod.f:240-250), x alike.
+template <typename T>
+struct Row7 {
+    T a[7], x[7];
+};
+
+template <typename T, typename TX>
+__device__ __forceinline__ void load_row7(const SysDev &d, const T *__restrict__ A, const TX *__restrict__ X,
+                                          int64_t c, Row7<T> &r)
+{
+    const int64_t n = d.n;
+    const Offs o = cell_offs(d, (uint32_t)c);
+    r.a[0] = A[1 * n + c];
+    r.x[0] = (T)X[c + o.jm];
+    r.a[1] = A[2 * n + c];
+    r.x[1] = (T)X[c + o.im];
+    r.a[2] = A[3 * n + c];
+    r.x[2] = (T)X[c];
+    r.a[3] = A[4 * n + c];
+    r.x[3] = (T)X[c + o.ip];
+    r.a[4] = A[5 * n + c];
+    r.x[4] = (T)X[c + o.jp];
+    if (d.do_k) {
+        r.a[5] = A[0 * n + c];
+        r.x[5] = (T)X[c + o.km];
+        r.a[6] = A[6 * n + c];
+        r.x[6] = (T)X[c + o.kp];
+    } else {
+        r.a[5] = r.a[6] = T(0);
+        r.x[5] = r.x[6] = T(0);
+    }
+}
+
+template <typename T>
+__device__ __forceinline__ T dot_row7(const Row7<T> &r, bool do_k)
+{
+    T v = r.a[0] * r.x[0];
+    v = v + r.a[1] * r.x[1];
+    v = v + r.a[2] * r.x[2];
+    v = v + r.a[3] * r.x[3];
+    v = v + r.a[4] * r.x[4];
+    if (do_k) {
+        v = v + r.a[5] * r.x[5];
+        v = v + r.a[6] * r.x[6];
+    }
+    return v;
+}
+
+// cells handled per thread per batch: stencil kernels, streaming kernels
+template <typename T>
+struct Batch {
+    static constexpr int STENCIL = sizeof(T) == 8 ? 2 : 4;
+    static constexpr int STREAM = sizeof(T) == 8 ? 4 : 8;
+};
+
 // P = R (i = 1) or P = R + beta*(P - omega*V) (model/leq_bicgs.f:334-343).
 template <typename T, bool MIXED>
-__global__ void k_p_update(BatchView b)
+__global__ void __launch_bounds__(256, 4) k_p_update(BatchView b)
 {
+    constexpr int U = Batch<T>::STREAM;
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
         const SysState &st = b.st[tl.sys];
         if (!gate_ok(st, G_INNER)) continue;
-        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
-        const T *r = vec<T>(d, V_R);
-        T *p = vec<T>(d, V_P);
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
+        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
+        const T *__restrict__ r = vec<T>(d, V_R) + c0;
+        T *__restrict__ p = vec<T>(d, V_P) + c0;
         if (st.i == 1) {
-            #pragma unroll 4
-            for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) p[c] = r[c];
+            for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
+                T rv[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int c = base + u * blockDim.x;
+                    if (c < cnt) rv[u] = r[c];
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int c = base + u * blockDim.x;
+                    if (c < cnt) p[c] = rv[u];
+                }
+            }
         } else {
             const T beta = (T)st.beta, omega = (T)st.omega;
-            const T *v = vec<T>(d, V_V);
-            #pragma unroll 4
-            for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) p[c] = r[c] + beta * (p[c] - omega * v[c]);
+            const T *__restrict__ v = vec<T>(d, V_V) + c0;
+            for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
+                T rv[U], pv[U], vv[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int c = base + u * blockDim.x;
+                    if (c < cnt) {
+                        rv[u] = r[c];
+                        pv[u] = p[c];
+                        vv[u] = v[c];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int c = base + u * blockDim.x;
+                    if (c < cnt) p[c] = rv[u] + beta * (pv[u] - omega * vv[u]);
+                }
+            }
         }
     }
 }
 
 // DIAG preconditioner, LEQ_MSOLVE1 (model/leqsol_mod.f:719-746): var = b / A(0).
 template <typename T>
-__global__ void k_diag(BatchView b, int src, int dst, int gate)
+__global__ void __launch_bounds__(256, 4) k_diag(BatchView b, int src, int dst, int gate)
 {
+    constexpr int U = Batch<T>::STREAM;
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
         if (!gate_ok(b.st[tl.sys], gate)) continue;
-        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
-        const T *a0 = diag_base<T>(d) + 3 * d.n;
-        const T *x = vec<T>(d, src);
-        T *y = vec<T>(d, dst);
-        #pragma unroll 4
-        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) y[c] = x[c] / a0[c];
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
+        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
+        const T *__restrict__ a0 = diag_base<T>(d) + 3 * d.n + c0;
+        const T *__restrict__ x = vec<T>(d, src) + c0;
+        T *__restrict__ y = vec<T>(d, dst) + c0;
+        for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
+            T xv[U], av[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int c = base + u * blockDim.x;
+                if (c < cnt) {
+                    xv[u] = x[c];
+                    av[u] = a0[c];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int c = base + u * blockDim.x;
+                if (c < cnt) y[c] = xv[u] / av[u];
+            }
+        }
     }
 }
 
 template <typename T>
-__global__ void k_copy(BatchView b, int src, int dst, int gate)
+__global__ void __launch_bounds__(256, 4) k_copy(BatchView b, int src, int dst, int gate)
 {
+    constexpr int U = Batch<T>::STREAM;
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
         if (!gate_ok(b.st[tl.sys], gate)) continue;
-        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
-        const T *x = vec<T>(d, src);
-        T *y = vec<T>(d, dst);
-        #pragma unroll 4
-        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) y[c] = x[c];
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
+        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
+        const T *__restrict__ x = vec<T>(d, src) + c0;
+        T *__restrict__ y = vec<T>(d, dst) + c0;
+        for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
+            T xv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int c = base + u * blockDim.x;
+                if (c < cnt) xv[u] = x[c];
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int c = base + u * blockDim.x;
+                if (c < cnt) y[c] = xv[u];
+            }
+        }
     }
 }
 
 // V = A*Phat and alpha = rho / (Rtilde, V) (model/leq_bicgs.f:355-361).
 template <typename T, bool MIXED>
-__global__ void k_matvec_alpha(BatchView b, int src)
+__global__ void __launch_bounds__(256) k_matvec_alpha(BatchView b, int src)
 {
+    constexpr int U = Batch<T>::STENCIL;
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
         SysState &st = b.st[tl.sys];
         if (!gate_ok(st, G_INNER)) continue;
-        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
-        const T *a = diag_base<T>(d);
-        const T *x = vec<T>(d, src);
-        const T *rt = vec<T>(d, V_RT);
-        T *y = vec<T>(d, V_V);
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
+        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
+        const T *__restrict__ a = diag_base<T>(d);
+        const T *__restrict__ x = vec<T>(d, src);
+        const T *__restrict__ rt = vec<T>(d, V_RT);
+        T *__restrict__ y = vec<T>(d, V_V);
         double v[1] = {0.0}, tot[1];
-        #pragma unroll 4
-        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-            const CellIdx q = cell_ijk(d, (uint32_t)c);
-            const T yv = (T)stencil_row<T, T>(d, a, x, (uint32_t)c, q);
-            y[c] = yv;
-            v[0] += (double)rt[c] * (double)yv;
+        for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
+            Row7<T> rw[U];
+            T rtv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int c = base + u * blockDim.x;
+                if (c < cnt) {
+                    load_row7<T, T>(d, a, x, c0 + c, rw[u]);
+                    rtv[u] = rt[c0 + c];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int c = base + u * blockDim.x;
+                if (c < cnt) {
+                    const T yv = dot_row7<T>(rw[u], d.do_k);
+                    y[c0 + c] = yv;
+                    v[0] += (double)rtv[u] * (double)yv;
+                }
+            }
         }
         if (tile_reduce<1>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) st.alpha = st.rho / tot[0];
     }
@@ -389,24 +543,40 @@ __global__ void k_matvec_alpha(BatchView b, int src)
 
 // S = R - alpha*V and Snorm (model/leq_bicgs.f:365-375).
 template <typename T, bool MIXED>
-__global__ void k_s_update(BatchView b)
+__global__ void __launch_bounds__(256, 4) k_s_update(BatchView b)
 {
+    constexpr int U = Batch<T>::STREAM;
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
         SysState &st = b.st[tl.sys];
         if (!gate_ok(st, G_INNER)) continue;
-        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
+        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
         const T alpha = (T)st.alpha;
-        const T *r = vec<T>(d, V_R);
-        const T *vv = vec<T>(d, V_V);
-        T *s = vec<T>(d, V_S);
+        const T *__restrict__ r = vec<T>(d, V_R) + c0;
+        const T *__restrict__ vv = vec<T>(d, V_V) + c0;
+        T *__restrict__ s = vec<T>(d, V_S) + c0;
         double v[1] = {0.0}, tot[1];
-        #pragma unroll 4
-        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-            const T sv = r[c] - alpha * vv[c];
-            s[c] = sv;
-            v[0] += (double)sv * (double)sv;
+        for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
+            T rv[U], wv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int c = base + u * blockDim.x;
+                if (c < cnt) {
+                    rv[u] = r[c];
+                    wv[u] = vv[c];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int c = base + u * blockDim.x;
+                if (c < cnt) {
+                    const T sv = rv[u] - alpha * wv[u];
+                    s[c] = sv;
+                    v[0] += (double)sv * (double)sv;
+                }
+            }
         }
         if (tile_reduce<1>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) {
             st.snorm = sqrt(tot[0]);
@@ -420,26 +590,42 @@ __global__ void k_s_update(BatchView b)
 
 // T = A*Shat, omega = (T,S)/(T,T) with (T,T) = 0 -> SMALL_NUMBER (model/leq_bicgs.f:409-427).
 template <typename T, bool MIXED>
-__global__ void k_matvec_omega(BatchView b, int src)
+__global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
 {
+    constexpr int U = Batch<T>::STENCIL;
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
         SysState &st = b.st[tl.sys];
         if (!gate_ok(st, G_INNER_NOSNORM)) continue;
-        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
-        const T *a = diag_base<T>(d);
-        const T *x = vec<T>(d, src);
-        const T *s = vec<T>(d, V_S);
-        T *y = vec<T>(d, V_T);
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
+        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
+        const T *__restrict__ a = diag_base<T>(d);
+        const T *__restrict__ x = vec<T>(d, src);
+        const T *__restrict__ s = vec<T>(d, V_S);
+        T *__restrict__ y = vec<T>(d, V_T);
         double v[2] = {0.0, 0.0}, tot[2];
-        #pragma unroll 4
-        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-            const CellIdx q = cell_ijk(d, (uint32_t)c);
-            const T yv = (T)stencil_row<T, T>(d, a, x, (uint32_t)c, q);
-            y[c] = yv;
-            v[0] += (double)yv * (double)s[c];
-            v[1] += (double)yv * (double)yv;
+        for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
+            Row7<T> rw[U];
+            T sv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int c = base + u * blockDim.x;
+                if (c < cnt) {
+                    load_row7<T, T>(d, a, x, c0 + c, rw[u]);
+                    sv[u] = s[c0 + c];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int c = base + u * blockDim.x;
+                if (c < cnt) {
+                    const T yv = dot_row7<T>(rw[u], d.do_k);
+                    y[c0 + c] = yv;
+                    v[0] += (double)yv * (double)sv[u];
+                    v[1] += (double)yv * (double)yv;
+                }
+            }
         }
         if (tile_reduce<2>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) {
             double txt = tot[1];
@@ -519,40 +705,76 @@ __device__ inline void fin_xr_inner(SysState &s, double rr, double rtr)
 }
 
 template <typename T, bool MIXED>
-__global__ void k_xr_update(BatchView b, int ph_id, int sh_id)
+__global__ void __launch_bounds__(256) k_xr_update(BatchView b, int ph_id, int sh_id)
 {
+    constexpr int U = sizeof(T) == 8 ? 2 : 4;
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
         SysState &st = b.st[tl.sys];
         if (!gate_ok(st, G_INNER)) continue;
-        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
+        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
         // FP64 drop-in: X is VAR.  Mixed form: the solution is accumulated in FP64
         // every iteration (x64 += alpha*Phat + omega*Shat with FP64 scalars).
         using X_T = typename std::conditional<MIXED, double, T>::type;
-        using S_T = typename std::conditional<MIXED, double, T>::type;
-        X_T *x = MIXED ? reinterpret_cast<X_T *>(d.x64[0]) : reinterpret_cast<X_T *>(vec<T>(d, V_X));
-        const S_T alpha = (S_T)st.alpha;
-        const T *ph = vec<T>(d, ph_id);
+        X_T *__restrict__ x =
+            (MIXED ? reinterpret_cast<X_T *>(d.x64[0]) : reinterpret_cast<X_T *>(vec<T>(d, V_X))) + c0;
+        const X_T alpha = (X_T)st.alpha;
+        const T *__restrict__ ph = vec<T>(d, ph_id) + c0;
         double v[2] = {0.0, 0.0}, tot[2];
         if (st.snorm_exit) {
-            #pragma unroll 4
-            for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) x[c] = x[c] + alpha * (S_T)ph[c];
+            for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
+                X_T xv[U];
+                T pv[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int c = base + u * blockDim.x;
+                    if (c < cnt) {
+                        xv[u] = x[c];
+                        pv[u] = ph[c];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int c = base + u * blockDim.x;
+                    if (c < cnt) x[c] = xv[u] + alpha * (X_T)pv[u];
+                }
+            }
         } else {
-            const S_T omega = (S_T)st.omega;
+            const X_T omega = (X_T)st.omega;
             const T omega_t = (T)st.omega;
-            const T *sh = vec<T>(d, sh_id);
-            const T *s = vec<T>(d, V_S);
-            const T *tv = vec<T>(d, V_T);
-            const T *rt = vec<T>(d, V_RT);
-            T *r = vec<T>(d, V_R);
-            #pragma unroll 4
-            for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-                x[c] = x[c] + alpha * (S_T)ph[c] + omega * (S_T)sh[c];
-                const T rv = s[c] - omega_t * tv[c];
-                r[c] = rv;
-                v[0] += (double)rv * (double)rv;
-                v[1] += (double)rt[c] * (double)rv;
+            const T *__restrict__ sh = vec<T>(d, sh_id) + c0;
+            const T *__restrict__ s = vec<T>(d, V_S) + c0;
+            const T *__restrict__ tv = vec<T>(d, V_T) + c0;
+            const T *__restrict__ rt = vec<T>(d, V_RT) + c0;
+            T *__restrict__ r = vec<T>(d, V_R) + c0;
+            for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
+                X_T xv[U];
+                T pv[U], hv[U], sv[U], tw[U], rtv[U];
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int c = base + u * blockDim.x;
+                    if (c < cnt) {
+                        xv[u] = x[c];
+                        pv[u] = ph[c];
+                        hv[u] = sh[c];
+                        sv[u] = s[c];
+                        tw[u] = tv[c];
+                        rtv[u] = rt[c];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int c = base + u * blockDim.x;
+                    if (c < cnt) {
+                        x[c] = xv[u] + alpha * (X_T)pv[u] + omega * (X_T)hv[u];
+                        const T rv = sv[u] - omega_t * tw[u];
+                        r[c] = rv;
+                        v[0] += (double)rv * (double)rv;
+                        v[1] += (double)rtv[u] * (double)rv;
+                    }
+                }
             }
         }
         if (tile_reduce<2>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) {
@@ -632,29 +854,47 @@ __device__ inline void fin_outer(SysState &s, double rr, double rtr32)
     }
 }
 
-__global__ void k_outer_step(BatchView b)
+__global__ void __launch_bounds__(256) k_outer_step(BatchView b)
 {
+    constexpr int U = 2;
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
         SysState &st = b.st[tl.sys];
         if (!gate_ok(st, G_OUTER)) continue;
-        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
-        const double *x = d.x64[0];
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
+        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
+        const double *__restrict__ x = d.x64[0];
         const bool fresh = (st.outer_steps == 0) || st.restart;
-        float *r32 = vec<float>(d, V_R);
-        float *rt32 = vec<float>(d, V_RT);
+        float *__restrict__ r32 = vec<float>(d, V_R);
+        float *__restrict__ rt32 = vec<float>(d, V_RT);
         double v[2] = {0.0, 0.0}, tot[2];
-        #pragma unroll 4
-        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-            const CellIdx q = cell_ijk(d, (uint32_t)c);
-            const double rv = d.b64[c] - stencil_row<double, double>(d, d.a64, x, (uint32_t)c, q);
-            const float rf = (float)rv;
-            r32[c] = rf;
-            const float rtf = fresh ? rf : rt32[c];
-            if (fresh) rt32[c] = rf;
-            v[0] += rv * rv;
-            v[1] += (double)rtf * (double)rf;
+        for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
+            Row7<double> rw[U];
+            double bv[U];
+            float rtv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int c = base + u * blockDim.x;
+                if (c < cnt) {
+                    load_row7<double, double>(d, d.a64, x, c0 + c, rw[u]);
+                    bv[u] = d.b64[c0 + c];
+                    rtv[u] = fresh ? 0.f : rt32[c0 + c];
+                }
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int c = base + u * blockDim.x;
+                if (c < cnt) {
+                    const double rv = bv[u] - dot_row7<double>(rw[u], d.do_k);
+                    const float rf = (float)rv;
+                    r32[c0 + c] = rf;
+                    const float rtf = fresh ? rf : rtv[u];
+                    if (fresh) rt32[c0 + c] = rf;
+                    v[0] += rv * rv;
+                    v[1] += (double)rtf * (double)rf;
+                }
+            }
         }
         if (tile_reduce<2>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) fin_outer(st, tot[0], tot[1]);
     }
@@ -772,7 +1012,7 @@ __device__ __forceinline__ bool next_line_job(const BatchView &b, const WaveArgs
         const int item0 = (w.kind == 0) ? b.line_prefix[sidx] : 0;
         const int q = (item - item0) * lpw + j.seg;
         if (w.kind == 0) {
-            j.k = q / d.half_lines + 1;
+            j.k = (int)fdiv((uint32_t)q, d.div_h) + 1;
             const int slot = q - (j.k - 1) * d.half_lines;
             const int i0 = (((1 + j.k) & 1) == w.par) ? 1 : 2;
             j.i = i0 + 2 * slot;
@@ -853,7 +1093,7 @@ __global__ void k_line_factor(BatchView b, const int *all_line_prefix)
         if (b.st[s].status != ST_RUNNING) continue;
         const SysDev &d = b.sys[s];
         const int li = g - all_line_prefix[s];  // (i-1) + (k-1)*imax2
-        const int k0 = li / d.imax2, i0 = li - k0 * d.imax2;
+        const int k0 = (int)fdiv((uint32_t)li, d.div_i), i0 = li - k0 * d.imax2;
         const int64_t base = (int64_t)i0 * d.jmax2 + (int64_t)k0 * d.jmax2 * d.imax2;
         const int64_t n = d.n;
         const int L = d.jmax2;
@@ -893,7 +1133,7 @@ __global__ void k_line_factor(BatchView b, const int *all_line_prefix)
 // function of the value entering it), a warp scan that composes the maps, and a
 // second pass from the entering value.  No division remains in the sweep.
 template <typename T>
-__global__ void __launch_bounds__(256) k_jline(BatchView b, WaveArgs w, int cmax)
+__global__ void __launch_bounds__(128) k_jline(BatchView b, WaveArgs w, int cmax)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nwarps = blockDim.x >> 5;
@@ -919,20 +1159,53 @@ __global__ void __launch_bounds__(256) k_jline(BatchView b, WaveArgs w, int cmax
         const T *gr_ = reinterpret_cast<const T *>(d.fac[1]) + x.base;
         const T *gq_ = reinterpret_cast<const T *>(d.fac[2]) + x.base;
 
-        // ---- load (coalesced over the line): right-hand side and factors
-#pragma unroll 4
-        for (int r = gl; r < G * c; r += G) {
-            T fv = T(0), lv = T(0), rv = T(0), qv = T(0);
-            if (fast && r < L) {
-                fv = line_rhs<T>(x, r);
-                lv = gl_[r];
-                rv = gr_[r];
-                qv = gq_[r];
+        // ---- load (coalesced over the line): right-hand side and factors, U rows at a time
+        constexpr int U = sizeof(T) == 8 ? 2 : 4;
+        for (int r0 = gl; r0 < G * c; r0 += U * G) {
+            T rhs[U], am1[U], ap1[U], am3[U], ap3[U], nim[U], nip[U], nkm[U], nkp[U], lv[U], rv[U], qv[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int r = r0 + u * G;
+                if (fast && r < L) {
+                    const int64_t p = x.base + r;
+                    rhs[u] = x.rhs[p];
+                    am1[u] = x.a[2 * x.n + p];
+                    ap1[u] = x.a[4 * x.n + p];
+                    nim[u] = x.nb_im[r];
+                    nip[u] = x.nb_ip[r];
+                    if (x.do_k) {
+                        am3[u] = x.a[0 * x.n + p];
+                        ap3[u] = x.a[6 * x.n + p];
+                        nkm[u] = x.nb_km[r];
+                        nkp[u] = x.nb_kp[r];
+                    }
+                    lv[u] = gl_[r];
+                    rv[u] = gr_[r];
+                    qv[u] = gq_[r];
+                }
             }
-            f[r] = fv;
-            fl[r] = lv;
-            fr[r] = rv;
-            fq[r] = qv;
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int r = r0 + u * G;
+                if (r < G * c) {
+                    T fv = T(0), l_ = T(0), r_ = T(0), q_ = T(0);
+                    if (fast && r < L) {
+                        fv = rhs[u] - am1[u] * nim[u];
+                        fv = fv - ap1[u] * nip[u];
+                        if (x.do_k) {
+                            fv = fv - am3[u] * nkm[u];
+                            fv = fv - ap3[u] * nkp[u];
+                        }
+                        l_ = lv[u];
+                        r_ = rv[u];
+                        q_ = qv[u];
+                    }
+                    f[r] = fv;
+                    fl[r] = l_;
+                    fr[r] = r_;
+                    fq[r] = q_;
+                }
+            }
         }
         __syncwarp();
 
@@ -1193,7 +1466,7 @@ cudaError_t launch_to_f32(const BatchView &b, const LaunchCfg &c)
 template <typename T>
 cudaError_t launch_init_residual(const BatchView &b, const LaunchCfg &c)
 {
-    k_init_residual<T><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b);
+    k_init_residual<T><<<c.stencil_grid, CELL_THREADS, 0, c.stream>>>(b);
     CHECK_LAUNCH();
 }
 template <typename T>
@@ -1205,7 +1478,7 @@ cudaError_t launch_init_rtilde(const BatchView &b, const LaunchCfg &c, uint64_t 
 template <typename T, bool MIXED>
 cudaError_t launch_p_update(const BatchView &b, const LaunchCfg &c)
 {
-    k_p_update<T, MIXED><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b);
+    k_p_update<T, MIXED><<<c.g_p, CELL_THREADS, 0, c.stream>>>(b);
     CHECK_LAUNCH();
 }
 // Shared memory of one warp of the J-line kernel: right-hand side and the three factor rows.
@@ -1231,13 +1504,35 @@ int prepare_line_kernel(int cmax, int *warps)
     return nb;
 }
 
-int cell_blocks_per_sm()
+template <typename K>
+static int occ(K kern)
 {
     int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_matvec_omega<double, false>, CELL_THREADS, 0) !=
-        cudaSuccess)
-        return 4;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, kern, CELL_THREADS, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return 2;
+    }
     return nb > 0 ? nb : 1;
+}
+
+// Resident blocks per SM of each cell kernel (persistent grids).
+void cell_occupancy(bool fp32, CellOcc *o)
+{
+    if (fp32) {
+        o->p_update = occ(k_p_update<float, true>);
+        o->s_update = occ(k_s_update<float, true>);
+        o->xr_update = occ(k_xr_update<float, true>);
+        o->matvec = occ(k_matvec_omega<float, true>);
+        o->copy = occ(k_copy<float>);
+        o->outer = occ(k_outer_step);
+    } else {
+        o->p_update = occ(k_p_update<double, false>);
+        o->s_update = occ(k_s_update<double, false>);
+        o->xr_update = occ(k_xr_update<double, false>);
+        o->matvec = occ(k_matvec_omega<double, false>);
+        o->copy = occ(k_copy<double>);
+        o->outer = occ(k_outer_step);
+    }
 }
 
 template <typename T>
@@ -1250,37 +1545,37 @@ cudaError_t launch_jline(const BatchView &b, const LaunchCfg &c, const WaveArgs 
 template <typename T>
 cudaError_t launch_diag(const BatchView &b, const LaunchCfg &c, int src, int dst, int gate)
 {
-    k_diag<T><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b, src, dst, gate);
+    k_diag<T><<<c.g_copy, CELL_THREADS, 0, c.stream>>>(b, src, dst, gate);
     CHECK_LAUNCH();
 }
 template <typename T>
 cudaError_t launch_copy(const BatchView &b, const LaunchCfg &c, int src, int dst, int gate)
 {
-    k_copy<T><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b, src, dst, gate);
+    k_copy<T><<<c.g_copy, CELL_THREADS, 0, c.stream>>>(b, src, dst, gate);
     CHECK_LAUNCH();
 }
 template <typename T, bool MIXED>
 cudaError_t launch_matvec_alpha(const BatchView &b, const LaunchCfg &c, int src)
 {
-    k_matvec_alpha<T, MIXED><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b, src);
+    k_matvec_alpha<T, MIXED><<<c.g_mv, CELL_THREADS, 0, c.stream>>>(b, src);
     CHECK_LAUNCH();
 }
 template <typename T, bool MIXED>
 cudaError_t launch_s_update(const BatchView &b, const LaunchCfg &c)
 {
-    k_s_update<T, MIXED><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b);
+    k_s_update<T, MIXED><<<c.g_s, CELL_THREADS, 0, c.stream>>>(b);
     CHECK_LAUNCH();
 }
 template <typename T, bool MIXED>
 cudaError_t launch_matvec_omega(const BatchView &b, const LaunchCfg &c, int src)
 {
-    k_matvec_omega<T, MIXED><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b, src);
+    k_matvec_omega<T, MIXED><<<c.g_mv, CELL_THREADS, 0, c.stream>>>(b, src);
     CHECK_LAUNCH();
 }
 template <typename T, bool MIXED>
 cudaError_t launch_xr_update(const BatchView &b, const LaunchCfg &c, int ph, int sh)
 {
-    k_xr_update<T, MIXED><<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b, ph, sh);
+    k_xr_update<T, MIXED><<<c.g_xr, CELL_THREADS, 0, c.stream>>>(b, ph, sh);
     CHECK_LAUNCH();
 }
 template <typename T>
@@ -1292,7 +1587,7 @@ cudaError_t launch_line_factor(const BatchView &b, const LaunchCfg &c, const int
 }
 cudaError_t launch_outer_step(const BatchView &b, const LaunchCfg &c)
 {
-    k_outer_step<<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b);
+    k_outer_step<<<c.g_outer, CELL_THREADS, 0, c.stream>>>(b);
     CHECK_LAUNCH();
 }
 template <typename T>

@@ -16,7 +16,9 @@ struct BatchView {
 };
 
 struct LaunchCfg {
-    int cell_grid;   // blocks for cell-tile kernels
+    int cell_grid;     // blocks of the setup cell kernels (one per tile)
+    int stencil_grid;  // blocks of the setup stencil kernels
+    int g_p, g_s, g_xr, g_mv, g_copy, g_outer;  // persistent grids of the iteration kernels
     int line_grid;   // blocks for J-line kernels
     int line_cmax;   // max rows per lane over the batch (smem sizing)
     int line_warps;  // warps per block of the J-line kernel
@@ -80,6 +82,9 @@ cudaError_t launch_seq_lines(const BatchView &b, const SeqLineArgs &a, cudaStrea
 int kernel_smem_line_bytes(int cmax, int elem_bytes);
 template <typename T>
 int prepare_line_kernel(int cmax, int *warps);  // sets the smem attribute, returns resident blocks per SM
-int cell_blocks_per_sm();
+struct CellOcc {
+    int p_update, s_update, xr_update, matvec, copy, outer;
+};
+void cell_occupancy(bool fp32, CellOcc *o);
 
 }  // namespace mfixgpu

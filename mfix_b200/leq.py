@@ -80,6 +80,10 @@ def _declare(L: C.CDLL) -> None:
     L.mfixgpu_dot_product_par.restype = C.c_int
     L.mfixgpu_batch_solve.argtypes = [C.POINTER(SystemC), C.c_int, C.c_char_p, C.c_char_p, C.c_int, C.c_int]
     L.mfixgpu_batch_solve.restype = C.c_int
+    L.mfixgpu_autotune_cache.argtypes = [C.c_char_p]
+    L.mfixgpu_autotune_cache.restype = C.c_int
+    L.mfixgpu_autotune_table.argtypes = [C.POINTER(C.c_int), C.c_int]
+    L.mfixgpu_autotune_table.restype = C.c_int
 
 
 def _ptr(a: np.ndarray) -> int:
@@ -144,6 +148,19 @@ def get_option(name: str) -> float:
 
 def finalize() -> None:
     lib().mfixgpu_finalize()
+
+
+def autotune_cache(path: str | None) -> int:
+    """Read/write the J-line autotuner's choices from/to a JSON file."""
+    return lib().mfixgpu_autotune_cache((path or "").encode())
+
+
+def autotune_table() -> list[tuple[int, int, int]]:
+    """(element bytes, line length, lanes per line) choices recorded so far."""
+    n = lib().mfixgpu_autotune_table(None, 0)
+    buf = (C.c_int * max(3 * n, 3))()
+    n = lib().mfixgpu_autotune_table(buf, n)
+    return [(buf[3 * q], buf[3 * q + 1], buf[3 * q + 2]) for q in range(n)]
 
 
 def geom(imax2: int, jmax2: int, kmax2: int, do_k: int) -> Geom:
