@@ -137,6 +137,21 @@ int mfixgpu_leq_msolve(const mfixgpu_geom *g, const double *b_dev, const double 
  * (the whole array): *out = sum r1*r2, reduced in a fixed order. */
 int mfixgpu_dot_product_par(const double *r1_dev, const double *r2_dev, int64_t n, double *out);
 
+/* No counterpart in the reference.  The dot product of DOT_PRODUCT_PAR for
+ * callers that cannot allocate device memory: hosts whose own pool owns all
+ * device memory or that run under a hard device-memory budget, and timing-
+ * critical loops that cannot take the implicit synchronization of
+ * cudaMalloc/cudaFree.  *out_dev (device memory) = sum r1*r2, reduced in a fixed
+ * order, enqueued on `stream` (a cudaStream_t; NULL: the default stream).  Its
+ * scratch is a fixed array inside this library, one per device, kept until the
+ * process exits and shared by every call: calls whose work overlaps on the GPU
+ * race.  n may not exceed MFIXGPU_NOALLOC_MAX_N (MFIXGPU_ERR_ARGS otherwise).
+ * The first call on a device looks up the array's address; make it before any
+ * stream capture. */
+#define MFIXGPU_NOALLOC_MAX_N (268435456LL) /* 2^28 elements */
+int mfixgpu_dot_product_par_noalloc(const double *r1_dev, const double *r2_dev, int64_t n, double *out_dev,
+                                    void *stream);
+
 /* ---------------------------------------------------------------- batches */
 
 typedef struct {

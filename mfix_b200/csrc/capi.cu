@@ -191,6 +191,15 @@ void solve_impl(int vno, double *var, double *a_m, double *b_m, int m, int itmax
 
 }  // namespace
 
+namespace mfixgpu {
+void set_last_error(const std::string &msg)
+{
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    g.err = msg;
+}
+}  // namespace mfixgpu
+
 extern "C" {
 
 int mfixgpu_init_geometry(const int *imax2, const int *jmax2, const int *kmax2, const int *do_k,

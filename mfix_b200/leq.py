@@ -80,6 +80,8 @@ def _declare(L: C.CDLL) -> None:
     L.mfixgpu_dot_product_par.restype = C.c_int
     L.mfixgpu_batch_solve.argtypes = [C.POINTER(SystemC), C.c_int, C.c_char_p, C.c_char_p, C.c_int, C.c_int]
     L.mfixgpu_batch_solve.restype = C.c_int
+    L.mfixgpu_dot_product_par_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
+    L.mfixgpu_dot_product_par_noalloc.restype = C.c_int
     L.mfixgpu_autotune_cache.argtypes = [C.c_char_p]
     L.mfixgpu_autotune_cache.restype = C.c_int
     L.mfixgpu_autotune_table.argtypes = [C.POINTER(C.c_int), C.c_int]
@@ -183,6 +185,15 @@ def dot_product_par(r1_dev: int, r2_dev: int, n: int) -> float:
     if rc:
         raise RuntimeError(f"mfixgpu_dot_product_par failed ({rc}): {last_error()}")
     return out.value
+
+
+NOALLOC_MAX_N = 268435456  # MFIXGPU_NOALLOC_MAX_N
+
+
+def dot_product_par_noalloc(r1_dev: int, r2_dev: int, n: int, out_dev: int, stream: int = 0) -> int:
+    """mfixgpu_dot_product_par_noalloc: writes sum(r1*r2) to the device double at out_dev
+    without allocating device memory.  Returns 0 or an error code."""
+    return lib().mfixgpu_dot_product_par_noalloc(r1_dev, r2_dev, n, out_dev, stream or None)
 
 
 @dataclass
