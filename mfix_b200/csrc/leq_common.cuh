@@ -27,7 +27,10 @@ enum VecId : int {
 enum PcKind : int { PC_NONE = 0, PC_DIAG = 1, PC_LINE = 2 };
 
 enum Status : int { ST_RUNNING = 0, ST_DONE = 1 };
-enum Phase : int { PH_INNER = 0, PH_OUTER = 1 };
+// PH_SETUP: unit scaling pending; PH_INIT: line factors / FP32 copy / initial
+// residual pending; then PH_INNER (BiCGSTAB iterations) and, in the mixed form,
+// PH_OUTER (FP64 reliable update).
+enum Phase : int { PH_INNER = 0, PH_OUTER = 1, PH_SETUP = 2, PH_INIT = 3 };
 
 // exit_kind values reported per solve
 enum ExitKind : int {
@@ -110,6 +113,7 @@ struct SysState {
     int xcur;             // mixed form: which x64 buffer holds VAR
     int restart;          // mixed form: next reliable update restarts the Krylov process (Rtilde = R)
     int stall;            // mixed form: reliable updates since the best true residual improved by 10%
+    int mixed;            // 1: mixed form (setup ends in PH_OUTER), 0: FP64 drop-in
     int line_skips;       // J-lines left unchanged because DGTSV reported INFO != 0
     int line_fallbacks;   // J-lines solved by the sequential pivoting path
     int err;
@@ -141,7 +145,9 @@ enum Gate : int {
     G_INNER = 0,        // running, inner phase
     G_INNER_NOSNORM = 1,// running, inner phase, no Snorm exit this iteration
     G_OUTER = 2,        // running, outer phase
-    G_ANY = 3           // running
+    G_ANY = 3,          // running
+    G_SETUP = 4,        // running, scaling pending
+    G_INIT = 5          // running, setup after scaling pending
 };
 
 __device__ __forceinline__ bool gate_ok(const SysState &s, int gate)
@@ -151,6 +157,8 @@ __device__ __forceinline__ bool gate_ok(const SysState &s, int gate)
     case G_INNER: return s.phase == PH_INNER;
     case G_INNER_NOSNORM: return s.phase == PH_INNER && !s.snorm_exit;
     case G_OUTER: return s.phase == PH_OUTER;
+    case G_SETUP: return s.phase == PH_SETUP;
+    case G_INIT: return s.phase == PH_INIT;
     default: return true;
     }
 }

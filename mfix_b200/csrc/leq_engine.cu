@@ -195,7 +195,8 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         st.tol = sp.tol;
         st.itmax = sp.itmax;
         st.status = ST_RUNNING;
-        st.phase = mixed ? PH_OUTER : PH_INNER;
+        st.phase = opt.skip_scale ? PH_INIT : PH_SETUP;
+        st.mixed = mixed ? 1 : 0;
         st.inner_tol = opt.inner_tol;
         st.i = 1;
         st.iter = 1;
@@ -573,6 +574,7 @@ int Engine::plan_msolve(const SolveOptions &opt, int src, int dst, int gate, int
                         st.s.rhs = src;
                         st.s.var = dst;
                         st.s.fatal_on_info = 1;
+                        st.s.gate = gate;
                         st.s.lmax = std::max(d0.imax2, d0.kmax2);
                         if (!fused_guess || waves_done >= 2) {
                             plan_[which].push_back(st);
@@ -778,6 +780,8 @@ int Engine::run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &
         CK(launch_init_rtilde<double>(view_, cfg_, opt.seed));
         launches_ += 2;
     }
+    CK(launch_init_done(view_, cfg_));
+    launches_ += 1;
     if (opt.pc == PC_LINE && opt.autotune && opt.force_lanes <= 0) {
         bool rs_only = true;
         for (int q = 0; q < 4; ++q) {
@@ -979,7 +983,11 @@ int Engine::msolve(const SystemSpec &g, const double *a, const double *b, double
     if ((rc = plan_msolve(opt, V_P, V_PH, G_ANY, 0))) return rc;
     if ((rc = bind_lists())) return rc;
     if (pc == PC_NONE) CK(cudaMemcpyAsync(var, b, (size_t)g.n * 8, cudaMemcpyDeviceToDevice, stream_));
-    if (pc == PC_LINE) CK(launch_line_factor<double>(view_, cfg_, d_allprefix_, h_allprefix_[nsys_]));
+    if (pc == PC_LINE) {
+        h_st_[0].phase = PH_INIT;  // the factorization kernel serves systems in their setup
+        CK(cudaMemcpyAsync(d_st_, h_st_.data(), sizeof(SysState), cudaMemcpyHostToDevice, stream_));
+        CK(launch_line_factor<double>(view_, cfg_, d_allprefix_, h_allprefix_[nsys_]));
+    }
     if ((rc = run_msolve_plan(0, 8))) return rc;
     CK(cudaStreamSynchronize(stream_));
     CK(cudaMemcpy(h_st_.data(), d_st_, sizeof(SysState), cudaMemcpyDeviceToHost));

@@ -164,6 +164,7 @@ __device__ inline void fin_rho0(SysState &s, double rtr)
     s.iter = 1;
     s.rnorm = 0.0;
     s.snorm_exit = 0;
+    s.phase = PH_INNER;
     if (s.itmax < 1) {
         final_logic(s, false);
         return;
@@ -183,7 +184,7 @@ __global__ void k_scale(BatchView b)
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
-        if (b.st[tl.sys].status != ST_RUNNING) continue;
+        if (!gate_ok(b.st[tl.sys], G_SETUP)) continue;
         const int64_t n = d.n;
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(n, c0 + TILE_CELLS);
         int bad = 0;
@@ -214,12 +215,25 @@ __global__ void k_after_scale(BatchView b)
     const int s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= b.nsys) return;
     SysState &st = b.st[s];
-    if (st.status != ST_RUNNING) return;
+    if (!gate_ok(st, G_SETUP)) return;
     if (st.err & 1) {
         st.ier = -2;
         st.exit_kind = EX_SINGULAR;
         st.status = ST_DONE;
+        return;
     }
+    st.phase = PH_INIT;
+}
+
+// End of the setup: the FP64 drop-in enters the loop (its Rtilde step already
+// moved it to PH_INNER unless it finished), the mixed form starts with an FP64 update.
+__global__ void k_init_done(BatchView b)
+{
+    const int s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= b.nsys) return;
+    SysState &st = b.st[s];
+    if (!gate_ok(st, G_INIT)) return;
+    st.phase = st.mixed ? PH_OUTER : PH_INNER;
 }
 
 __global__ void k_to_f32(BatchView b)
@@ -227,7 +241,7 @@ __global__ void k_to_f32(BatchView b)
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
-        if (b.st[tl.sys].status != ST_RUNNING) continue;
+        if (!gate_ok(b.st[tl.sys], G_INIT)) continue;
         const int64_t n = d.n;
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(n, c0 + TILE_CELLS);
         #pragma unroll 4
@@ -245,7 +259,7 @@ __global__ void k_init_residual(BatchView b)
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
         SysState &st = b.st[tl.sys];
-        if (st.status != ST_RUNNING) continue;
+        if (!gate_ok(st, G_INIT)) continue;
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
         const T *a = diag_base<T>(d);
         const T *x = vec<T>(d, V_X);
@@ -286,7 +300,7 @@ __global__ void k_init_rtilde(BatchView b, uint64_t seed)
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
         SysState &st = b.st[tl.sys];
-        if (st.status != ST_RUNNING) continue;
+        if (!gate_ok(st, G_INIT)) continue;
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
         const double rn0 = st.rnorm0;
         const T *r = vec<T>(d, V_R);
@@ -1090,7 +1104,7 @@ __global__ void k_line_factor(BatchView b, const int *all_line_prefix)
     const int total = all_line_prefix[b.nsys];
     for (int g = blockIdx.x * blockDim.x + threadIdx.x; g < total; g += gridDim.x * blockDim.x) {
         const int s = find_sys(all_line_prefix, b.nsys, g);
-        if (b.st[s].status != ST_RUNNING) continue;
+        if (!gate_ok(b.st[s], G_INIT)) continue;
         const SysDev &d = b.sys[s];
         const int li = g - all_line_prefix[s];  // (i-1) + (k-1)*imax2
         const int k0 = (int)fdiv((uint32_t)li, d.div_i), i0 = li - k0 * d.imax2;
@@ -1299,7 +1313,7 @@ __global__ void k_seq_lines(BatchView b, SeqLineArgs a)
     const int li = blockIdx.x * blockDim.x + threadIdx.x;
     if (li >= a.count) return;
     SysState &st = b.st[0];
-    if (!gate_ok(st, G_INNER)) return;
+    if (!gate_ok(st, a.gate)) return;
     const SysDev &d = b.sys[0];
     const int64_t n = d.n, c1 = d.jmax2, c2 = (int64_t)d.jmax2 * d.imax2;
     const T *A = diag_base<T>(d);
@@ -1456,6 +1470,11 @@ cudaError_t launch_scale(const BatchView &b, const LaunchCfg &c)
 cudaError_t launch_after_scale(const BatchView &b, const LaunchCfg &c)
 {
     k_after_scale<<<(b.nsys + 127) / 128, 128, 0, c.stream>>>(b);
+    CHECK_LAUNCH();
+}
+cudaError_t launch_init_done(const BatchView &b, const LaunchCfg &c)
+{
+    k_init_done<<<(b.nsys + 127) / 128, 128, 0, c.stream>>>(b);
     CHECK_LAUNCH();
 }
 cudaError_t launch_to_f32(const BatchView &b, const LaunchCfg &c)

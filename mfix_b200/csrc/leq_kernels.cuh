@@ -29,6 +29,7 @@ struct LaunchCfg {
 cudaError_t launch_scale(const BatchView &b, const LaunchCfg &c);
 cudaError_t launch_after_scale(const BatchView &b, const LaunchCfg &c);
 cudaError_t launch_to_f32(const BatchView &b, const LaunchCfg &c);
+cudaError_t launch_init_done(const BatchView &b, const LaunchCfg &c);
 template <typename T>
 cudaError_t launch_init_residual(const BatchView &b, const LaunchCfg &c);  // R = B - A X, ||R||
 template <typename T>
@@ -75,6 +76,7 @@ struct SeqLineArgs {
     int fatal_on_info;  // 1: INFO != 0 is an error (JK / IJ sweeps), 0: skip the line (IK sweep)
     double *scratch;    // 4 * Lmax * count values
     int lmax;
+    int gate;           // which systems take part (Gate)
 };
 template <typename T>
 cudaError_t launch_seq_lines(const BatchView &b, const SeqLineArgs &a, cudaStream_t s);
