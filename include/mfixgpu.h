@@ -181,6 +181,80 @@ int mfixgpu_batch_solve(mfixgpu_system *systems, int nsys, const char *sweep, co
                         int on_device);
 /* mfixgpu_last_stats after a batch: seconds, device_ms, jline_*, kernel_launches of the whole batch. */
 
+/* ---------------------------------------------------------------- serving (no reference counterpart)
+ *
+ * A request loop for solves that arrive from concurrent cases.  A worker
+ * thread owns the device: it admits requests in arrival order while their
+ * device memory fits the HBM budget and a slot is free, copies their arrays
+ * in on a copy stream, and joins them to a live batch between iterations, so
+ * requests that arrive while others are on the GPU share every kernel launch
+ * with them (continuous batching).  Each request runs the drop-in's algorithm
+ * (LEQ_BICGS, model/leq_bicgs.f:107-509) exactly as when solved alone, and
+ * its result is bit-identical to a solve of it alone with the same options.
+ * In the mixed form a request whose FP32 iteration gives up moves to an FP64
+ * live batch and is solved again from its initial guess. */
+
+typedef struct {
+    int precision;          /* 1 (default): FP32 inner / FP64 outer with FP64 hand-over; 0: FP64 drop-in */
+    int max_systems;        /* slots of each live batch (default 256) */
+    int check_every;        /* iterations between reads of the batch state (default 4) */
+    int device;             /* CUDA device (default 0) */
+    double hbm_budget;      /* bytes of device memory the requests may hold (0: 85% of free memory) */
+    double inner_tol;       /* mixed form: as the "inner_tol" option (0: 1e-2) */
+    char sweep[4];          /* "RSRS" when blank; letters R and S only */
+    char pc[4];             /* "LINE", "DIAG" or "NONE"; "LINE" when blank */
+} mfixgpu_server_config;
+
+/* submit flags */
+#define MFIXGPU_REQ_ZERO_GUESS 1   /* the initial guess is zero: var is output only */
+#define MFIXGPU_REQ_WRITE_AB 2     /* copy the unit-scaled A_M/B_M back (model/leq_bicgs.f:202-203) */
+#define MFIXGPU_REQ_ON_DEVICE 4    /* a_m/b_m/var are device memory, solved in place */
+
+typedef struct {
+    int status;             /* 0 queued, 1 copying in, 2 in a batch, 3 copying out, 4 done */
+    int ier;
+    int iterations;         /* the reference's ITER at exit (mixed form: inner iterations) */
+    int iter_tot_add;
+    int exit_kind;
+    int outer_steps;
+    int fp64_fallback;
+    int mixed_iterations;
+    double rnorm0, rnorm;
+    double t_submit, t_admit, t_start, t_done; /* seconds on the server's clock */
+} mfixgpu_request;
+
+typedef struct {
+    long long submitted, completed, queued, copying, running;
+    long long commits;          /* membership changes applied to the live batches */
+    long long iterations;       /* iteration bodies launched, summed over the live batches */
+    long long kernel_launches;  /* kernels of this library launched by the server */
+    long long fp64_fallbacks;
+    long long max_running;      /* most requests in the live batches at once */
+    double reserved_bytes, peak_reserved_bytes, budget_bytes;
+    double seconds;             /* server clock now */
+} mfixgpu_server_counters;
+
+/* Starts a server (its worker thread, streams, live batches).  cfg may be NULL
+ * for the defaults.  Returns 0 and *server, or an error code. */
+int mfixgpu_server_create(const mfixgpu_server_config *cfg, void **server);
+/* Queues one solve.  a_m (7*DIMENSION_3), b_m and var belong to the caller and
+ * stay valid and untouched until the request is done; tol and itmax come from
+ * sys, results go to the request record (sys's result fields are not
+ * written).  Returns a ticket >= 0, or MFIXGPU_ERR_ARGS, MFIXGPU_ERR_NOMEM
+ * (larger than the whole budget) or MFIXGPU_ERR_CUDA (the server failed). */
+long long mfixgpu_server_submit(void *server, const mfixgpu_system *sys, int flags);
+/* 1: done, *out filled and the ticket released; 0: not done (*out holds its
+ * status and times so far); MFIXGPU_ERR_ARGS for an unknown ticket. */
+int mfixgpu_server_poll(void *server, long long ticket, mfixgpu_request *out);
+/* Waits up to timeout_s seconds (< 0: no limit) for the ticket; returns as poll. */
+int mfixgpu_server_wait(void *server, long long ticket, double timeout_s, mfixgpu_request *out);
+/* Waits up to timeout_s for any request to finish that nobody has collected:
+ * 1 with *ticket and *out (released), 0 on timeout. */
+int mfixgpu_server_wait_any(void *server, double timeout_s, long long *ticket, mfixgpu_request *out);
+int mfixgpu_server_counters_get(void *server, mfixgpu_server_counters *out);
+/* Finishes every submitted request, stops the worker and frees the server. */
+int mfixgpu_server_destroy(void *server);
+
 #ifdef __cplusplus
 }
 #endif

@@ -24,6 +24,22 @@ namespace mfixgpu {
 
 static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
+// The autotuner's choices are shared by every engine of the process (one-shot
+// solves and live batches pick the same lanes per line for the same line length,
+// so a system gives the same bits in either).
+namespace {
+struct TuneTable {
+    std::mutex mu;
+    std::map<std::pair<int, int>, int> lanes;  // (element bytes, line length) -> lanes per line
+    std::string path;
+};
+TuneTable &tunes()
+{
+    static TuneTable t;
+    return t;
+}
+}  // namespace
+
 // Lanes per J-line: the smallest power of two that leaves at most 12 rows per
 // lane (at most 32 lanes); rows per lane rounded up to odd so that lanes reading row t
 // of their chunks hit distinct shared-memory banks.
@@ -103,6 +119,8 @@ Engine::~Engine()
     cudaFree(d_dot_counter_);
     cudaFree(d_dot_out_);
     if (h_st_pinned_) cudaFreeHost(h_st_pinned_);
+    if (live_exec_) cudaGraphExecDestroy(live_exec_);
+    if (ev_fence_) cudaEventDestroy(ev_fence_);
     if (ev_a_) cudaEventDestroy(ev_a_);
     if (ev_b_) cudaEventDestroy(ev_b_);
     if (ev_t0_) cudaEventDestroy(ev_t0_);
@@ -118,19 +136,79 @@ int Engine::fail(const std::string &msg, int code)
     return code;
 }
 
-template <typename T>
-static cudaError_t upload(T **dptr, size_t *cap_elems, const T *src, size_t n, cudaStream_t s)
+
+// The result of one system from its final device state.
+SolveResult result_of(const SysState &st, bool mixed)
 {
-    if (n > *cap_elems || *dptr == nullptr) {
-        if (*dptr) cudaFree(*dptr);
-        *dptr = nullptr;
-        const size_t want = std::max<size_t>(n, 16);
-        cudaError_t e = cudaMalloc((void **)dptr, want * sizeof(T));
-        if (e != cudaSuccess) return e;
-        *cap_elems = want;
+    SolveResult r;
+    r.ier = st.ier;
+    r.iterations = mixed ? st.inner_total : st.iter;
+    r.iter_tot_add = st.iter_tot_add;
+    r.exit_kind = st.exit_kind;
+    r.line_skips = st.line_skips;
+    r.line_fallbacks = st.line_fallbacks;
+    r.outer_steps = st.outer_steps;
+    r.rnorm0 = mixed ? st.outer_rnorm0 : st.rnorm0;
+    r.rnorm = mixed ? st.outer_rnorm : st.rnorm;
+    if (st.status != ST_DONE) {
+        r.ier = -15;
+        r.exit_kind = EX_ERROR;
     }
-    if (n == 0) return cudaSuccess;
-    return cudaMemcpyAsync(*dptr, src, n * sizeof(T), cudaMemcpyHostToDevice, s);
+    if (st.err & 2) {
+        r.ier = -12;  // DGTSV INFO != 0 inside a JK/IJ sweep (the reference stops there)
+        r.exit_kind = EX_ERROR;
+    }
+    return r;
+}
+
+// ------------------------------------------------------------------ work memory
+// One system's work memory: in the mixed form the FP32 diagonals first, then the
+// nine iteration vectors and the three J-line factor arrays (elements of the
+// form's precision), then the per-line flags; the mixed form's copy of the
+// initial guess follows that region.
+size_t vec_region_bytes(int64_t n, int64_t lines, int precision)
+{
+    const size_t ew = precision == PREC_MIXED ? 4 : 8;
+    size_t b = 0;
+    if (precision == PREC_MIXED) b += align_up(7 * (size_t)n * 4, 256);
+    b += (NVEC + 3) * align_up((size_t)n * ew, 256) + align_up((size_t)lines * 4, 256);
+    return b;
+}
+
+size_t work_bytes(int64_t n, int64_t lines, int precision)
+{
+    return vec_region_bytes(n, lines, precision) + (precision == PREC_MIXED ? align_up((size_t)n * 8, 256) : 0);
+}
+
+// A block that serves a mixed attempt and then, if it gives up, the FP64
+// re-solve: the FP64 region (larger than the mixed one) followed by the initial guess.
+size_t live_work_bytes(int64_t n, int64_t lines, int precision)
+{
+    if (precision != PREC_MIXED) return vec_region_bytes(n, lines, PREC_FP64);
+    return std::max(vec_region_bytes(n, lines, PREC_FP64), vec_region_bytes(n, lines, PREC_MIXED)) +
+           align_up((size_t)n * 8, 256);
+}
+
+void carve_work(SysDev &d, char *work, int64_t lines, int precision, char *x0)
+{
+    const size_t n = (size_t)d.n;
+    const size_t ew = precision == PREC_MIXED ? 4 : 8;
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        char *p = work + off;
+        off += align_up(bytes, 256);
+        return p;
+    };
+    d.a32 = nullptr;
+    d.x64[1] = nullptr;
+    if (precision == PREC_MIXED) {
+        d.a32 = (float *)take(7 * n * 4);
+        d.x64[1] = (double *)x0;  // initial guess, kept for an FP64 re-solve
+    }
+    for (int v = 0; v < NVEC; ++v) d.vec[v] = take(n * ew);
+    for (int f = 0; f < 3; ++f) d.fac[f] = take(n * ew);
+    d.line_flag = (int *)take((size_t)lines * 4);
+    if (precision != PREC_MIXED) d.vec[V_X] = d.x64[0];
 }
 
 // ------------------------------------------------------------------ batch setup
@@ -138,17 +216,11 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
 {
     nsys_ = (int)specs.size();
     const bool mixed = opt.precision == PREC_MIXED;
-    const size_t ew = mixed ? sizeof(float) : sizeof(double);
 
     // work memory: the iteration vectors, plus the FP32 diagonals and a copy of
     // the initial guess in the mixed form (inputs are device arrays by now)
-    size_t bytes = 0;
-    for (const auto &s : specs) {
-        const size_t n = (size_t)s.n;
-        if (mixed) bytes += align_up(n * 8, 256) + align_up(7 * n * 4, 256);
-        bytes += (NVEC + 3) * align_up(n * ew, 256) + align_up((size_t)s.imax2 * s.kmax2 * 4, 256);
-    }
-    bytes += 4096;
+    size_t bytes = 4096;
+    for (const auto &s : specs) bytes += work_bytes(s.n, (int64_t)s.imax2 * s.kmax2, opt.precision) + 256;
     cudaError_t e = arena_.reserve(bytes);
     if (e != cudaSuccess) return fail(std::string("device memory for the batch: ") + cudaGetErrorString(e), -11);
     arena_.reset();
@@ -176,18 +248,12 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         shape_for(sp.jmax2, mixed ? 4 : 8, opt.force_lanes, &d.lane_group, &d.rows_per_lane);
         d.half_lines = (sp.imax2 + 1) / 2;
         d.div_h = make_fastdiv((uint32_t)d.half_lines);
-        const size_t n = (size_t)sp.n;
         d.a64 = sp.a;
         d.b64 = sp.b;
         d.x64[0] = sp.x;
-        if (mixed) {
-            d.x64[1] = (double *)arena_.take(n * 8);  // initial guess, kept for an FP64 re-solve
-            d.a32 = (float *)arena_.take(7 * n * 4);
-        }
-        for (int v = 0; v < NVEC; ++v) d.vec[v] = arena_.take(n * ew);
-        for (int f = 0; f < 3; ++f) d.fac[f] = arena_.take(n * ew);
-        d.line_flag = (int *)arena_.take((size_t)sp.imax2 * sp.kmax2 * 4);
-        if (!mixed) d.vec[V_X] = d.x64[0];
+        const int64_t lines = (int64_t)sp.imax2 * sp.kmax2;
+        char *work = (char *)arena_.take(work_bytes(sp.n, lines, opt.precision));
+        carve_work(d, work, lines, opt.precision, mixed ? work + vec_region_bytes(sp.n, lines, opt.precision) : nullptr);
         for (int t = 0; t < d.ntiles; ++t) h_tiles_.push_back(Tile{s, t});
         h_allprefix_[s + 1] = h_allprefix_[s] + sp.imax2 * sp.kmax2;
 
@@ -259,7 +325,7 @@ int Engine::configure_lines(int elem)
         const SysDev &d = h_sys_[s];
         cmax = std::max(cmax, d.rows_per_lane);
         const int lpw = 32 / d.lane_group;
-        const int64_t slots = (int64_t)d.half_lines * d.kmax2;
+        const int64_t slots = d.n > 0 ? (int64_t)d.half_lines * d.kmax2 : 0;  // empty slot of a live batch
         h_prefix_[s + 1] = h_prefix_[s] + (int)((slots + lpw - 1) / lpw);
     }
     CK(upload(&d_sys_, &sys_cap_, h_sys_.data(), h_sys_.size(), stream_));
@@ -298,11 +364,14 @@ void Engine::shape_for(int L, int elem, int forced, int *G, int *c)
         *c = rows_for(L, g);
         return;
     }
-    auto it = line_tune_.find(std::make_pair(elem, L));
-    if (it != line_tune_.end()) {
-        *G = it->second;
-        *c = rows_for(L, it->second);
-        return;
+    {
+        std::lock_guard<std::mutex> lk(tunes().mu);
+        auto it = tunes().lanes.find(std::make_pair(elem, L));
+        if (it != tunes().lanes.end()) {
+            *G = it->second;
+            *c = rows_for(L, it->second);
+            return;
+        }
     }
     line_shape(L, G, c);
 }
@@ -315,7 +384,10 @@ int Engine::autotune_lines(const SolveOptions &opt, int elem)
     std::vector<int> todo;
     for (int s = 0; s < nsys_; ++s) {
         const int L = h_sys_[s].jmax2;
-        if (line_tune_.count(std::make_pair(elem, L))) continue;
+        {
+            std::lock_guard<std::mutex> lk(tunes().mu);
+            if (tunes().lanes.count(std::make_pair(elem, L))) continue;
+        }
         if (std::find(todo.begin(), todo.end(), L) == todo.end()) todo.push_back(L);
     }
     if (todo.empty()) return 0;
@@ -363,7 +435,10 @@ int Engine::autotune_lines(const SolveOptions &opt, int elem)
             int c_unused = 0;
             line_shape(L, &best_g, &c_unused);
         }
-        line_tune_[std::make_pair(elem, L)] = best_g;
+        {
+            std::lock_guard<std::mutex> lk(tunes().mu);
+            tunes().lanes[std::make_pair(elem, L)] = best_g;
+        }
         for (int s = 0; s < nsys_; ++s)
             if (h_sys_[s].jmax2 == L) {
                 h_sys_[s].lane_group = best_g;
@@ -379,21 +454,24 @@ int Engine::autotune_lines(const SolveOptions &opt, int elem)
 
 void Engine::load_tune_cache(const std::string &path)
 {
-    tune_path_ = path;
+    std::lock_guard<std::mutex> lk(tunes().mu);
+    tunes().path = path;
     FILE *f = path.empty() ? nullptr : std::fopen(path.c_str(), "r");
     if (!f) return;
     int elem, L, G;
     char buf[256];
     while (std::fgets(buf, sizeof buf, f))
         if (std::sscanf(buf, " {\"elem\": %d, \"L\": %d, \"lanes\": %d}", &elem, &L, &G) == 3 && G >= 1 && G <= 32)
-            line_tune_[std::make_pair(elem, L)] = G;
+            tunes().lanes[std::make_pair(elem, L)] = G;
     std::fclose(f);
 }
 
 void Engine::save_tune_cache()
 {
-    if (tune_path_.empty()) return;
-    FILE *f = std::fopen(tune_path_.c_str(), "w");
+    std::lock_guard<std::mutex> lk(tunes().mu);
+    const auto &line_tune_ = tunes().lanes;
+    if (tunes().path.empty()) return;
+    FILE *f = std::fopen(tunes().path.c_str(), "w");
     if (!f) return;
     std::fprintf(f, "[\n");
     size_t q = 0;
@@ -406,8 +484,9 @@ void Engine::save_tune_cache()
 
 int Engine::tune_table(int *out, int max_entries) const
 {
+    std::lock_guard<std::mutex> lk(tunes().mu);
     int q = 0;
-    for (const auto &kv : line_tune_) {
+    for (const auto &kv : tunes().lanes) {
         if (q < max_entries) {
             out[3 * q] = kv.first.first;
             out[3 * q + 1] = kv.first.second;
@@ -436,7 +515,15 @@ int Engine::plan_msolve(const SolveOptions &opt, int src, int dst, int gate, int
         plan_[which].push_back(st);
         return 0;
     }
-    const SysDev &d0 = h_sys_[0];
+    // the 2-D branch of LEQ_MSOLVE applies when no system of the batch is 3-D;
+    // letters I/K/A (single systems only) read d0's geometry
+    int any3d = -1;
+    for (int s = 0; s < nsys_; ++s)
+        if (h_sys_[s].n > 0) any3d = std::max(any3d, h_sys_[s].do_k ? 1 : 0);
+    int s0 = 0;
+    while (s0 + 1 < nsys_ && h_sys_[s0].n == 0) ++s0;
+    SysDev d0 = h_sys_[s0];
+    d0.do_k = any3d != 0;
     const bool single = nsys_ == 1;
     auto letter = [&](char ch) -> int {
         if (ch == 'R' || ch == 'r') return 'R';
@@ -504,9 +591,9 @@ int Engine::plan_msolve(const SolveOptions &opt, int src, int dst, int gate, int
         const int L = letter(opt.sweep[q]);
         if (!L) continue;
         if (!d0.do_k) {
-            if (L == 'R') {  // :382-391, i odd then i even
-                wave(0, 0, 0, nullptr, 0);
+            if (L == 'R') {  // :382-391, i odd then i even (the kernel flips the 3-D parity)
                 wave(0, 1, 0, nullptr, 0);
+                wave(0, 0, 0, nullptr, 0);
             } else if (L == 'I') {  // :374-379, i = 1..imax2 in order
                 if (!single) return fail("sweep letter 'I' is served for single-system solves only", -10);
                 for (int dgl = 2; dgl <= d0.imax2 + 1; ++dgl) wave(1, dgl, 1, nullptr, 0);
@@ -735,34 +822,13 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
     return 0;
 }
 
-// One batch whose arrays are all on the device.
-int Engine::run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &opt, std::vector<SolveResult> &out)
+// The per-system setup, each step gated on the system's phase (so it is a no-op
+// for systems past it): unit scaling, J-line factors, FP32 copy or initial
+// residual and Rtilde, entry to the loop.
+int Engine::launch_setup(const SolveOptions &opt, bool scale)
 {
-    out.assign(specs.size(), SolveResult{});
     const bool mixed = opt.precision == PREC_MIXED;
-    const int elem = mixed ? 4 : 8;
-
-    int rc = setup_batch(specs, opt);
-    if (rc) return rc;
-    const int gate_p = G_INNER, gate_s = G_INNER_NOSNORM;
-    const int src_ph = opt.pc == PC_NONE ? V_P : V_PH;
-    const int src_sh = opt.pc == PC_NONE ? V_S : V_SH;
-    h_lines_.clear();
-    list_refs_.clear();
-    if ((rc = plan_msolve(opt, V_P, V_PH, gate_p, 0))) return rc;
-    if ((rc = plan_msolve(opt, V_S, V_SH, gate_s, 1))) return rc;
-    if ((rc = bind_lists())) return rc;
-
-    jline_timing_ = opt.time_kernels;
-    jline_count_ = 0;
-    launches_ = 0;
-    timing_ = SolveTiming{};
-    if (jline_timing_ && !jt_ev_[0])
-        for (int q = 0; q < 2 * JT_EVENTS; ++q) cudaEventCreate(&jt_ev_[q]);
-    CK(cudaEventRecord(ev_t0_, stream_));
-
-    // ---- setup
-    if (!opt.skip_scale) {
+    if (scale) {
         CK(launch_scale(view_, cfg_));
         CK(launch_after_scale(view_, cfg_));
         launches_ += 2;
@@ -782,6 +848,64 @@ int Engine::run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &
     }
     CK(launch_init_done(view_, cfg_));
     launches_ += 1;
+    return 0;
+}
+
+// One BiCGSTAB iteration for every system of the batch (model/leq_bicgs.f:316-466).
+int Engine::launch_body(const SolveOptions &opt)
+{
+    const bool mixed = opt.precision == PREC_MIXED;
+    const int src_ph = opt.pc == PC_NONE ? V_P : V_PH;
+    const int src_sh = opt.pc == PC_NONE ? V_S : V_SH;
+    int r;
+    launches_ += mixed ? 6 : 5;
+    if (mixed) {
+        CK(launch_outer_step(view_, cfg_));
+        CK((launch_p_update<float, true>(view_, cfg_)));
+        if ((r = run_msolve_plan(0, 4))) return r;
+        CK((launch_matvec_alpha<float, true>(view_, cfg_, src_ph)));
+        CK((launch_s_update<float, true>(view_, cfg_)));
+        if ((r = run_msolve_plan(1, 4))) return r;
+        CK((launch_matvec_omega<float, true>(view_, cfg_, src_sh)));
+        CK((launch_xr_update<float, true>(view_, cfg_, src_ph, src_sh)));
+    } else {
+        CK((launch_p_update<double, false>(view_, cfg_)));
+        if ((r = run_msolve_plan(0, 8))) return r;
+        CK((launch_matvec_alpha<double, false>(view_, cfg_, src_ph)));
+        CK((launch_s_update<double, false>(view_, cfg_)));
+        if ((r = run_msolve_plan(1, 8))) return r;
+        CK((launch_matvec_omega<double, false>(view_, cfg_, src_sh)));
+        CK((launch_xr_update<double, false>(view_, cfg_, src_ph, src_sh)));
+    }
+    return 0;
+}
+
+// One batch whose arrays are all on the device.
+int Engine::run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &opt, std::vector<SolveResult> &out)
+{
+    out.assign(specs.size(), SolveResult{});
+    const bool mixed = opt.precision == PREC_MIXED;
+    const int elem = mixed ? 4 : 8;
+
+    int rc = setup_batch(specs, opt);
+    if (rc) return rc;
+    const int gate_p = G_INNER, gate_s = G_INNER_NOSNORM;
+    h_lines_.clear();
+    list_refs_.clear();
+    if ((rc = plan_msolve(opt, V_P, V_PH, gate_p, 0))) return rc;
+    if ((rc = plan_msolve(opt, V_S, V_SH, gate_s, 1))) return rc;
+    if ((rc = bind_lists())) return rc;
+
+    jline_timing_ = opt.time_kernels;
+    jline_count_ = 0;
+    launches_ = 0;
+    timing_ = SolveTiming{};
+    if (jline_timing_ && !jt_ev_[0])
+        for (int q = 0; q < 2 * JT_EVENTS; ++q) cudaEventCreate(&jt_ev_[q]);
+    CK(cudaEventRecord(ev_t0_, stream_));
+
+    // ---- setup
+    if ((rc = launch_setup(opt, !opt.skip_scale))) return rc;
     if (opt.pc == PC_LINE && opt.autotune && opt.force_lanes <= 0) {
         bool rs_only = true;
         for (int q = 0; q < 4; ++q) {
@@ -798,30 +922,7 @@ int Engine::run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &
         }
     }
 
-    // ---- iteration body (kernels of this library: 6 or 5 plus the sweep plans)
-    auto body = [&]() -> int {
-        int r;
-        launches_ += mixed ? 6 : 5;
-        if (mixed) {
-            CK(launch_outer_step(view_, cfg_));
-            CK((launch_p_update<float, true>(view_, cfg_)));
-            if ((r = run_msolve_plan(0, 4))) return r;
-            CK((launch_matvec_alpha<float, true>(view_, cfg_, src_ph)));
-            CK((launch_s_update<float, true>(view_, cfg_)));
-            if ((r = run_msolve_plan(1, 4))) return r;
-            CK((launch_matvec_omega<float, true>(view_, cfg_, src_sh)));
-            CK((launch_xr_update<float, true>(view_, cfg_, src_ph, src_sh)));
-        } else {
-            CK((launch_p_update<double, false>(view_, cfg_)));
-            if ((r = run_msolve_plan(0, 8))) return r;
-            CK((launch_matvec_alpha<double, false>(view_, cfg_, src_ph)));
-            CK((launch_s_update<double, false>(view_, cfg_)));
-            if ((r = run_msolve_plan(1, 8))) return r;
-            CK((launch_matvec_omega<double, false>(view_, cfg_, src_sh)));
-            CK((launch_xr_update<double, false>(view_, cfg_, src_ph, src_sh)));
-        }
-        return 0;
-    };
+    auto body = [&]() -> int { return launch_body(opt); };
 
     int max_itmax = 0;
     for (const auto &s : specs) max_itmax = std::max(max_itmax, s.itmax);
@@ -889,27 +990,7 @@ int Engine::run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &
     timing_.kernel_launches = launches_;
 
     // ---- results back
-    for (int s = 0; s < nsys_; ++s) {
-        const SysState &st = h_st_[s];
-        SolveResult &r = out[s];
-        r.ier = st.ier;
-        r.iterations = mixed ? st.inner_total : st.iter;
-        r.iter_tot_add = st.iter_tot_add;
-        r.exit_kind = st.exit_kind;
-        r.line_skips = st.line_skips;
-        r.line_fallbacks = st.line_fallbacks;
-        r.outer_steps = st.outer_steps;
-        r.rnorm0 = mixed ? st.outer_rnorm0 : st.rnorm0;
-        r.rnorm = mixed ? st.outer_rnorm : st.rnorm;
-        if (st.status != ST_DONE) {
-            r.ier = -15;
-            r.exit_kind = EX_ERROR;
-        }
-        if (st.err & 2) {
-            r.ier = -12;  // DGTSV INFO != 0 inside a JK/IJ sweep (the reference stops there)
-            r.exit_kind = EX_ERROR;
-        }
-    }
+    for (int s = 0; s < nsys_; ++s) out[s] = result_of(h_st_[s], mixed);
     CK(cudaStreamSynchronize(stream_));
     if (jline_timing_) {
         float js = 0.f;

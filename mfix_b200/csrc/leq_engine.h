@@ -2,6 +2,7 @@
 // device-resident state, the BiCGSTAB iteration schedule (FP64 drop-in and the
 // FP32-inner / FP64-refinement form) and the LINE-preconditioner sweep plan.
 #pragma once
+#include <algorithm>
 #include <cstdint>
 #include <map>
 #include <mutex>
@@ -63,6 +64,38 @@ struct SolveTiming {
     long long kernel_launches = 0;  // kernels of this library launched by the solve
 };
 
+// Host table -> device copy; the device array is reallocated (with headroom)
+// only when it must grow.  cudaFree waits for the kernels still using it.
+template <typename T>
+inline cudaError_t upload(T **dptr, size_t *cap_elems, const T *src, size_t n, cudaStream_t s)
+{
+    if (n > *cap_elems || *dptr == nullptr) {
+        if (*dptr) cudaFree(*dptr);
+        *dptr = nullptr;
+        const size_t want = std::max<size_t>(n + n / 2, 16);
+        cudaError_t e = cudaMalloc((void **)dptr, want * sizeof(T));
+        if (e != cudaSuccess) return e;
+        *cap_elems = want;
+    }
+    if (n == 0) return cudaSuccess;
+    return cudaMemcpyAsync(*dptr, src, n * sizeof(T), cudaMemcpyHostToDevice, s);
+}
+
+// A system joining a live batch: device arrays (a/b/x of `dev`) and a work
+// block of live_work_bytes(); the caller keeps both until the system has left.
+struct LiveSystem {
+    SystemSpec dev;
+    char *work = nullptr;
+    bool scaled = false;      // A/B unit-scaled already: the setup starts after the scaling
+    const double *x0 = nullptr;  // non-null: x = x0 before the setup (FP64 re-solve of a mixed attempt)
+    cudaEvent_t after = nullptr; // non-null: the engine's stream waits for it before touching the system
+};
+
+struct LiveDone {
+    int slot;
+    SolveResult res;
+};
+
 struct DeviceArena {
     char *base = nullptr;
     size_t cap = 0, used = 0;
@@ -85,6 +118,28 @@ public:
     size_t arena_bytes() const { return arena_.cap; }
     const SolveTiming &timing() const { return timing_; }
 
+    // ---- live batch: a fixed table of slots whose systems join and leave
+    // between iterations (continuous batching).  Every system follows the same
+    // kernel sequence as when solved alone: setup, then one body per iteration.
+    int live_open(int capacity, const SolveOptions &opt);
+    int live_add(const LiveSystem &s);  // slot, or MFIXGPU_ERR_NOMEM-style -11 when full
+    void live_remove(int slot);         // the slot's system takes no further part
+    // Applies joins and leaves (tables, graph, setup of new systems), then runs
+    // `iterations` bodies and records a snapshot of the states.
+    int live_step(int iterations);
+    // Systems found finished in the previous snapshot (latest: the newest one,
+    // waited for); each is reported once.
+    int live_collect(std::vector<LiveDone> &done, bool latest);
+    int live_used() const { return live_used_; }
+    int live_capacity() const { return (int)slot_used_.size(); }
+    bool live_dirty() const { return live_dirty_; }
+    // Recorded after the last commit: kernels enqueued before it may still read
+    // the tables of systems removed by that commit, none after it.
+    cudaEvent_t live_fence() const { return ev_fence_; }
+    long long live_commits() const { return commits_; }
+    long long live_bodies() const { return body_total_; }
+    long long launches() const { return launches_; }
+
     // per-routine entry points on device pointers (parity tests of single kernels)
     int matvec(const SystemSpec &g, const double *a, const double *x, double *y);
     int msolve(const SystemSpec &g, const double *a, const double *b, double *var, int pc, const char sweep[4]);
@@ -92,6 +147,8 @@ public:
 
 private:
     int run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &opt, std::vector<SolveResult> &out);
+    int launch_setup(const SolveOptions &opt, bool scale);
+    int launch_body(const SolveOptions &opt);
     int setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions &opt);
     int plan_msolve(const SolveOptions &opt, int src, int dst, int gate, int elem);
     int run_msolve_plan(int which, int elem);
@@ -106,8 +163,6 @@ public:
     int tune_table(int *out, int max_entries) const;
 
 private:
-    std::map<std::pair<int, int>, int> line_tune_;  // (element bytes, line length) -> lanes per line
-    std::string tune_path_;
     int fail(const std::string &msg, int code);
 
     int dev_ = -1, sms_ = 0;
@@ -166,9 +221,36 @@ private:
     int jline_count_ = 0;
     long long launches_ = 0;
     SolveTiming timing_;
+
+    // live batch
+    int live_commit();
+    SolveOptions live_opt_{};
+    std::vector<char> slot_used_, slot_fresh_, slot_reported_, slot_cleared_;
+    std::vector<LiveSystem> slot_sys_;
+    std::vector<long long> slot_join_snap_, slot_join_body_;
+    int live_used_ = 0;
+    bool live_dirty_ = false;
+    cudaGraphExec_t live_exec_ = nullptr;
+    long long live_per_body_ = 0;
+    long long snap_count_ = 0, body_total_ = 0, collected_upto_ = -1, commits_ = 0;
+    long long snap_bodies_[2] = {0, 0};
+    cudaEvent_t ev_fence_ = nullptr;
 };
+
+SolveResult result_of(const SysState &st, bool mixed);
 
 // choice of lanes per J-line and rows per lane for a line of length L
 void line_shape(int L, int *G, int *c);
+
+// Work memory of one system with n cells and `lines` J-lines: the iteration
+// vectors and factors of the given precision, plus the initial-guess copy of
+// the mixed form (work_bytes); live_work_bytes also leaves room for an FP64
+// re-solve of a mixed attempt in the same block.
+size_t vec_region_bytes(int64_t n, int64_t lines, int precision);
+size_t work_bytes(int64_t n, int64_t lines, int precision);
+size_t live_work_bytes(int64_t n, int64_t lines, int precision);
+// Points d's work arrays into `work` (d.n and d.x64[0] set); x0: where the
+// mixed form keeps the initial guess.
+void carve_work(SysDev &d, char *work, int64_t lines, int precision, char *x0);
 
 }  // namespace mfixgpu

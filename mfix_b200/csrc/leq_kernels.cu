@@ -21,6 +21,8 @@
 
 #include "leq_kernels.cuh"
 
+#include <mutex>
+
 namespace mfixgpu {
 
 // ------------------------------------------------------------------ helpers
@@ -1028,7 +1030,11 @@ __device__ __forceinline__ bool next_line_job(const BatchView &b, const WaveArgs
         if (w.kind == 0) {
             j.k = (int)fdiv((uint32_t)q, d.div_h) + 1;
             const int slot = q - (j.k - 1) * d.half_lines;
-            const int i0 = (((1 + j.k) & 1) == w.par) ? 1 : 2;
+            // 3-D sweeps take (i+k) odd first (model/leqsol_mod.f:497-509), 2-D
+            // sweeps i odd first (:382-391), i.e. (i+k) even with k = 1: the wave's
+            // parity is stated for 3-D and flipped for a 2-D system
+            const int par = d.do_k ? w.par : (w.par ^ 1);
+            const int i0 = (((1 + j.k) & 1) == par) ? 1 : 2;
             j.i = i0 + 2 * slot;
             j.valid = (j.k <= d.kmax2) && (j.i <= d.imax2);
         } else if (w.kind == 1) {
@@ -1516,8 +1522,18 @@ int prepare_line_kernel(int cmax, int *warps)
     if (wpb < 1) return 0;
     *warps = wpb;
     const int smem = wpb * per_warp;
-    if (cudaFuncSetAttribute(k_jline<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
-        return 0;
+    // the limit is a property of the kernel, shared by every engine of the
+    // process (some on other threads): it only ever grows
+    static std::mutex mu;
+    static int granted = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        if (smem > granted) {
+            if (cudaFuncSetAttribute(k_jline<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+                return 0;
+            granted = smem;
+        }
+    }
     int nb = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_jline<T>, wpb * 32, smem) != cudaSuccess) return 0;
     return nb;

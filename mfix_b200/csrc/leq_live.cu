@@ -1,0 +1,333 @@
+// leq_live.cu -- the engine's live batch: continuous batching of LEQ_BICGS solves.
+//
+// A live batch is a fixed table of slots.  Systems join and leave between
+// iterations; each join or leave rebuilds the small batch tables (cell tiles,
+// line-work prefixes, partial-sum slots), re-captures the iteration body as a
+// CUDA graph and launches the gated setup kernels, which only touch systems
+// still in their setup phases.  A system therefore runs exactly the kernel
+// sequence it runs when solved alone (setup, then one body per iteration, its
+// reductions over its own tiles in a fixed order), and its result is the same
+// bits in a mix as alone.
+#include "leq_engine.h"
+
+#include <algorithm>
+#include <cstring>
+
+namespace mfixgpu {
+
+#define CK(call)                                                                                   \
+    do {                                                                                           \
+        cudaError_t e_ = (call);                                                                   \
+        if (e_ != cudaSuccess) return fail(std::string(#call) + ": " + cudaGetErrorString(e_), -13); \
+    } while (0)
+
+// An empty slot: no cells, no tiles, no line work; its state is never running.
+static SysDev idle_sys()
+{
+    SysDev d{};
+    d.imax2 = d.jmax2 = d.kmax2 = 1;
+    d.do_k = 1;
+    d.n = 0;
+    d.div_j = d.div_i = d.div_h = make_fastdiv(1);
+    d.pc = PC_NONE;
+    d.lane_group = 32;
+    d.rows_per_lane = 1;
+    d.half_lines = 1;
+    return d;
+}
+
+static SysState idle_state()
+{
+    SysState s{};
+    s.status = ST_DONE;
+    s.exit_kind = EX_ERROR;
+    return s;
+}
+
+int Engine::live_open(int capacity, const SolveOptions &opt)
+{
+    err_.clear();
+    if (capacity < 1 || capacity > 65536) return fail("live batch capacity must be 1..65536", -14);
+    if (opt.pc != PC_LINE && opt.pc != PC_DIAG && opt.pc != PC_NONE) return fail("unknown preconditioner", -10);
+    for (int q = 0; q < 4; ++q) {
+        const char ch = opt.sweep[q];
+        if (ch == 'I' || ch == 'i' || ch == 'K' || ch == 'k' || ch == 'A' || ch == 'a')
+            return fail("sweep letters I/K/A are served for single-system solves only", -10);
+    }
+    live_opt_ = opt;
+    live_opt_.on_device = true;
+    live_opt_.time_kernels = false;
+    const bool mixed = opt.precision == PREC_MIXED;
+
+    nsys_ = capacity;
+    h_sys_.assign(capacity, idle_sys());
+    h_st_.assign(capacity, idle_state());
+    slot_used_.assign(capacity, 0);
+    slot_fresh_.assign(capacity, 0);
+    slot_reported_.assign(capacity, 0);
+    slot_cleared_.assign(capacity, 0);
+    slot_sys_.assign(capacity, LiveSystem{});
+    slot_join_snap_.assign(capacity, 0);
+    slot_join_body_.assign(capacity, 0);
+    live_used_ = 0;
+    snap_count_ = body_total_ = commits_ = 0;
+    collected_upto_ = -1;
+
+    h_tiles_.clear();
+    h_allprefix_.assign(capacity + 1, 0);
+    if (upload(&d_st_, &st_cap_, h_st_.data(), h_st_.size(), stream_) != cudaSuccess ||
+        upload(&d_tiles_, &tiles_cap_, h_tiles_.data(), 0, stream_) != cudaSuccess ||
+        upload(&d_allprefix_, &allprefix_cap_, h_allprefix_.data(), h_allprefix_.size(), stream_) != cudaSuccess)
+        return fail("device memory for the live batch tables", -11);
+    if (!d_partials_) {
+        CK(cudaMalloc((void **)&d_partials_, 2 * 1024 * sizeof(double)));
+        part_cap_ = 2 * 1024;
+    }
+    if ((size_t)capacity * 2 > h_st_pinned_cap_) {
+        if (h_st_pinned_) cudaFreeHost(h_st_pinned_);
+        h_st_pinned_ = nullptr;
+        CK(cudaMallocHost((void **)&h_st_pinned_, sizeof(SysState) * 2 * (size_t)capacity));
+        h_st_pinned_cap_ = 2 * (size_t)capacity;
+    }
+    if (!ev_fence_) CK(cudaEventCreateWithFlags(&ev_fence_, cudaEventDisableTiming));
+    view_.st = d_st_;
+    view_.tiles = d_tiles_;
+    view_.ntiles = 0;
+    view_.nsys = capacity;
+    view_.partials = d_partials_;
+    cfg_.stream = stream_;
+    int rc = configure_lines(mixed ? 4 : 8);
+    if (rc) return rc;
+
+    // the sweep plans of R/S sweeps depend on no system: built once
+    h_lines_.clear();
+    list_refs_.clear();
+    if ((rc = plan_msolve(live_opt_, V_P, V_PH, G_INNER, 0))) return rc;
+    if ((rc = plan_msolve(live_opt_, V_S, V_SH, G_INNER_NOSNORM, 1))) return rc;
+    if ((rc = bind_lists())) return rc;
+    live_dirty_ = false;
+    CK(cudaEventRecord(ev_fence_, stream_));
+    return 0;
+}
+
+int Engine::live_add(const LiveSystem &ls)
+{
+    const SystemSpec &sp = ls.dev;
+    if (slot_used_.empty()) return fail("live batch not open", -14);
+    if (sp.imax2 < 1 || sp.jmax2 < 1 || sp.kmax2 < 1) return fail("grid extents must be >= 1", -14);
+    if (!sp.do_k && sp.kmax2 != 1) return fail("a 2-D system (do_k = 0) needs kmax2 = 1", -14);
+    if ((int64_t)sp.imax2 * sp.jmax2 * sp.kmax2 != sp.n) return fail("DIMENSION_3 != IMAX2*JMAX2*KMAX2", -14);
+    if (sp.n > (int64_t)INT32_MAX - TILE_CELLS) return fail("system too large for 32-bit cell indexing", -14);
+    if (!sp.a || !sp.b || !sp.x || !ls.work) return fail("null array", -14);
+    int slot = -1;
+    for (int s = 0; s < (int)slot_used_.size() && slot < 0; ++s)
+        if (!slot_used_[s]) slot = s;
+    if (slot < 0) return fail("live batch full", -11);
+
+    const int prec = live_opt_.precision;
+    const bool mixed = prec == PREC_MIXED;
+    SysDev d{};
+    d.imax2 = sp.imax2;
+    d.jmax2 = sp.jmax2;
+    d.kmax2 = sp.kmax2;
+    d.do_k = sp.do_k;
+    d.n = sp.n;
+    d.div_j = make_fastdiv((uint32_t)sp.jmax2);
+    d.div_i = make_fastdiv((uint32_t)sp.imax2);
+    d.pc = live_opt_.pc;
+    d.ntiles = (int)((sp.n + TILE_CELLS - 1) / TILE_CELLS);
+    shape_for(sp.jmax2, mixed ? 4 : 8, live_opt_.force_lanes, &d.lane_group, &d.rows_per_lane);
+    d.half_lines = (sp.imax2 + 1) / 2;
+    d.div_h = make_fastdiv((uint32_t)d.half_lines);
+    d.a64 = sp.a;
+    d.b64 = sp.b;
+    d.x64[0] = sp.x;
+    const int64_t lines = (int64_t)sp.imax2 * sp.kmax2;
+    char *x0 = mixed ? ls.work + std::max(vec_region_bytes(sp.n, lines, PREC_FP64),
+                                          vec_region_bytes(sp.n, lines, PREC_MIXED))
+                     : nullptr;
+    carve_work(d, ls.work, lines, prec, x0);
+
+    SysState st{};
+    st.tol = sp.tol;
+    st.itmax = sp.itmax;
+    st.status = ST_RUNNING;
+    st.phase = ls.scaled ? PH_INIT : PH_SETUP;
+    st.mixed = mixed ? 1 : 0;
+    st.inner_tol = live_opt_.inner_tol;
+    st.i = 1;
+    st.iter = 1;
+
+    h_sys_[slot] = d;
+    h_st_[slot] = st;
+    slot_sys_[slot] = ls;
+    slot_used_[slot] = 1;
+    slot_fresh_[slot] = 1;
+    slot_reported_[slot] = 0;
+    slot_cleared_[slot] = 0;
+    ++live_used_;
+    live_dirty_ = true;
+    return slot;
+}
+
+void Engine::live_remove(int slot)
+{
+    if (slot < 0 || slot >= (int)slot_used_.size() || !slot_used_[slot]) return;
+    slot_used_[slot] = 0;
+    slot_fresh_[slot] = 0;
+    slot_cleared_[slot] = 1;
+    h_sys_[slot] = idle_sys();
+    h_st_[slot] = idle_state();
+    slot_sys_[slot] = LiveSystem{};
+    --live_used_;
+    live_dirty_ = true;
+}
+
+int Engine::live_commit()
+{
+    const int cap = (int)slot_used_.size();
+    const bool mixed = live_opt_.precision == PREC_MIXED;
+    bool any_fresh = false;
+
+    // states of the slots that changed hands; the copies are stream ordered
+    // after every kernel already enqueued
+    for (int s = 0; s < cap; ++s) {
+        if (slot_cleared_[s]) {
+            CK(cudaMemcpyAsync(d_st_ + s, &h_st_[s], sizeof(SysState), cudaMemcpyHostToDevice, stream_));
+            slot_cleared_[s] = 0;
+        }
+        if (!slot_fresh_[s]) continue;
+        any_fresh = true;
+        const LiveSystem &ls = slot_sys_[s];
+        const size_t n = (size_t)ls.dev.n;
+        if (ls.after) CK(cudaStreamWaitEvent(stream_, ls.after, 0));
+        if (ls.x0) CK(cudaMemcpyAsync(ls.dev.x, ls.x0, n * 8, cudaMemcpyDeviceToDevice, stream_));
+        if (mixed) CK(cudaMemcpyAsync(h_sys_[s].x64[1], ls.dev.x, n * 8, cudaMemcpyDeviceToDevice, stream_));
+        CK(cudaMemcpyAsync(d_st_ + s, &h_st_[s], sizeof(SysState), cudaMemcpyHostToDevice, stream_));
+    }
+
+    // tables of the systems now in the batch
+    h_tiles_.clear();
+    h_allprefix_.assign(cap + 1, 0);
+    int tile_base = 0;
+    for (int s = 0; s < cap; ++s) {
+        SysDev &d = h_sys_[s];
+        d.tile_base = tile_base;
+        if (slot_used_[s]) {
+            for (int t = 0; t < d.ntiles; ++t) h_tiles_.push_back(Tile{s, t});
+            tile_base += d.ntiles;
+        }
+        h_allprefix_[s + 1] = h_allprefix_[s] + (slot_used_[s] ? d.imax2 * d.kmax2 : 0);
+    }
+    CK(upload(&d_tiles_, &tiles_cap_, h_tiles_.data(), h_tiles_.size(), stream_));
+    CK(upload(&d_allprefix_, &allprefix_cap_, h_allprefix_.data(), h_allprefix_.size(), stream_));
+    const size_t need_part = 2 * (size_t)std::max(tile_base, 1);
+    if (need_part > part_cap_) {
+        cudaFree(d_partials_);  // waits for the kernels that still use it
+        d_partials_ = nullptr;
+        const size_t want = std::max(need_part, part_cap_ * 2);
+        CK(cudaMalloc((void **)&d_partials_, want * sizeof(double)));
+        part_cap_ = want;
+    }
+    view_.st = d_st_;
+    view_.tiles = d_tiles_;
+    view_.ntiles = (int)h_tiles_.size();
+    view_.nsys = cap;
+    view_.partials = d_partials_;
+    cfg_.cell_grid = std::max(1, view_.ntiles);
+    cfg_.stencil_grid = std::max(1, view_.ntiles);
+    const CellOcc &oc = occ_[mixed ? 1 : 0];
+    auto grid = [&](int bpsm) { return std::max(1, std::min(view_.ntiles, sms_ * bpsm)); };
+    cfg_.g_p = grid(oc.p_update);
+    cfg_.g_s = grid(oc.s_update);
+    cfg_.g_xr = grid(oc.xr_update);
+    cfg_.g_mv = grid(oc.matvec);
+    cfg_.g_copy = grid(oc.copy);
+    cfg_.g_outer = grid(oc.outer);
+    int rc = configure_lines(mixed ? 4 : 8);
+    if (rc) return rc;
+
+    // the iteration body for this membership
+    if (live_exec_) cudaGraphExecDestroy(live_exec_);  // freed once its launches finish
+    live_exec_ = nullptr;
+    if (live_used_ > 0 && live_opt_.use_graph) {
+        cudaGraph_t g = nullptr;
+        CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeThreadLocal));
+        const long long before = launches_;
+        rc = launch_body(live_opt_);
+        live_per_body_ = launches_ - before;
+        launches_ = before;
+        cudaError_t ce = cudaStreamEndCapture(stream_, &g);
+        if (rc) {
+            if (g) cudaGraphDestroy(g);
+            return rc;
+        }
+        if (ce != cudaSuccess) return fail(std::string("graph capture: ") + cudaGetErrorString(ce), -13);
+        ce = cudaGraphInstantiate(&live_exec_, g, 0);
+        cudaGraphDestroy(g);
+        if (ce != cudaSuccess) return fail(std::string("graph instantiate: ") + cudaGetErrorString(ce), -13);
+    }
+
+    // setup of the systems that joined (gated: a no-op for the others)
+    if (any_fresh && (rc = launch_setup(live_opt_, true))) return rc;
+    for (int s = 0; s < cap; ++s)
+        if (slot_fresh_[s]) {
+            slot_fresh_[s] = 0;
+            slot_join_snap_[s] = snap_count_;
+            slot_join_body_[s] = body_total_;
+        }
+    CK(cudaEventRecord(ev_fence_, stream_));
+    live_dirty_ = false;
+    ++commits_;
+    return 0;
+}
+
+int Engine::live_step(int iterations)
+{
+    if (slot_used_.empty()) return fail("live batch not open", -14);
+    int rc;
+    if (live_dirty_ && (rc = live_commit())) return rc;
+    if (live_used_ == 0 || iterations <= 0) return 0;
+    for (int q = 0; q < iterations; ++q) {
+        if (live_exec_) {
+            CK(cudaGraphLaunch(live_exec_, stream_));
+            launches_ += live_per_body_;
+        } else if ((rc = launch_body(live_opt_))) {
+            return rc;
+        }
+    }
+    body_total_ += iterations;
+    const int cap = (int)slot_used_.size();
+    const int b = (int)(snap_count_ & 1);
+    CK(cudaMemcpyAsync(h_st_pinned_ + (size_t)b * cap, d_st_, sizeof(SysState) * cap, cudaMemcpyDeviceToHost,
+                       stream_));
+    CK(cudaEventRecord(b ? ev_b_ : ev_a_, stream_));
+    snap_bodies_[b] = body_total_;
+    ++snap_count_;
+    return 0;
+}
+
+int Engine::live_collect(std::vector<LiveDone> &done, bool latest)
+{
+    const long long q = latest ? snap_count_ - 1 : snap_count_ - 2;
+    if (q < 0 || q <= collected_upto_) return 0;
+    const int b = (int)(q & 1);
+    CK(cudaEventSynchronize(b ? ev_b_ : ev_a_));
+    const int cap = (int)slot_used_.size();
+    const bool mixed = live_opt_.precision == PREC_MIXED;
+    const SysState *ps = h_st_pinned_ + (size_t)b * cap;
+    for (int s = 0; s < cap; ++s) {
+        if (!slot_used_[s] || slot_reported_[s] || slot_fresh_[s] || q < slot_join_snap_[s]) continue;
+        const SysState &st = ps[s];
+        // a system still running after ITMAX + 2 bodies is reported incomplete, as
+        // the one-shot solve reports it
+        if (st.status != ST_RUNNING || snap_bodies_[b] - slot_join_body_[s] >= (long long)st.itmax + 2) {
+            done.push_back(LiveDone{s, result_of(st, mixed)});
+            slot_reported_[s] = 1;
+        }
+    }
+    collected_upto_ = q;
+    return 0;
+}
+
+}  // namespace mfixgpu

@@ -49,7 +49,47 @@ class SystemC(C.Structure):
                 ("rnorm0", C.c_double), ("rnorm", C.c_double)]
 
 
+class ServerConfigC(C.Structure):
+    _fields_ = [("precision", C.c_int), ("max_systems", C.c_int), ("check_every", C.c_int), ("device", C.c_int),
+                ("hbm_budget", C.c_double), ("inner_tol", C.c_double), ("sweep", C.c_char * 4),
+                ("pc", C.c_char * 4)]
+
+
+class RequestC(C.Structure):
+    _fields_ = [("status", C.c_int), ("ier", C.c_int), ("iterations", C.c_int), ("iter_tot_add", C.c_int),
+                ("exit_kind", C.c_int), ("outer_steps", C.c_int), ("fp64_fallback", C.c_int),
+                ("mixed_iterations", C.c_int), ("rnorm0", C.c_double), ("rnorm", C.c_double),
+                ("t_submit", C.c_double), ("t_admit", C.c_double), ("t_start", C.c_double), ("t_done", C.c_double)]
+
+
+class ServerCountersC(C.Structure):
+    _fields_ = [("submitted", C.c_longlong), ("completed", C.c_longlong), ("queued", C.c_longlong),
+                ("copying", C.c_longlong), ("running", C.c_longlong), ("commits", C.c_longlong),
+                ("iterations", C.c_longlong), ("kernel_launches", C.c_longlong), ("fp64_fallbacks", C.c_longlong),
+                ("max_running", C.c_longlong), ("reserved_bytes", C.c_double), ("peak_reserved_bytes", C.c_double),
+                ("budget_bytes", C.c_double), ("seconds", C.c_double)]
+
+
+REQ_ZERO_GUESS = 1
+REQ_WRITE_AB = 2
+REQ_ON_DEVICE = 4
+
+
 def _declare(L: C.CDLL) -> None:
+    L.mfixgpu_server_create.argtypes = [C.POINTER(ServerConfigC), C.POINTER(C.c_void_p)]
+    L.mfixgpu_server_create.restype = C.c_int
+    L.mfixgpu_server_submit.argtypes = [C.c_void_p, C.POINTER(SystemC), C.c_int]
+    L.mfixgpu_server_submit.restype = C.c_longlong
+    L.mfixgpu_server_poll.argtypes = [C.c_void_p, C.c_longlong, C.POINTER(RequestC)]
+    L.mfixgpu_server_poll.restype = C.c_int
+    L.mfixgpu_server_wait.argtypes = [C.c_void_p, C.c_longlong, C.c_double, C.POINTER(RequestC)]
+    L.mfixgpu_server_wait.restype = C.c_int
+    L.mfixgpu_server_wait_any.argtypes = [C.c_void_p, C.c_double, C.POINTER(C.c_longlong), C.POINTER(RequestC)]
+    L.mfixgpu_server_wait_any.restype = C.c_int
+    L.mfixgpu_server_counters_get.argtypes = [C.c_void_p, C.POINTER(ServerCountersC)]
+    L.mfixgpu_server_counters_get.restype = C.c_int
+    L.mfixgpu_server_destroy.argtypes = [C.c_void_p]
+    L.mfixgpu_server_destroy.restype = C.c_int
     L.mfixgpu_init_geometry.argtypes = [_ip, _ip, _ip, _ip, C.POINTER(C.c_int64), _ip]
     L.mfixgpu_init_geometry.restype = C.c_int
     L.mfixgpu_solve_lin_eq_.argtypes = [C.c_char_p, _ip, C.c_void_p, C.c_void_p, C.c_void_p, _ip, _ip, _ip,
@@ -235,3 +275,96 @@ def solve_system(s, method: int = 2, sweep: str = "RSRS", pc: str = "LINE", vno:
     if rc:
         return rc
     return solve_lin_eq("Test", vno, s.x, s.a, s.b, 0, s.itmax, method, sweep, s.tol, pc)
+
+
+def _struct_dict(st) -> dict:
+    return {name: getattr(st, name) for name, _ in st._fields_ if not name.startswith("pad")}
+
+
+class Server:
+    """The request server (mfixgpu_server_*): continuous batching of solves.
+
+    ``submit`` takes host arrays (or device pointers with ``on_device``) that
+    must stay alive and untouched until the request is done; results come back
+    as dicts with the IER fields and the server-clock times t_submit, t_admit,
+    t_start and t_done."""
+
+    def __init__(self, precision: int = 1, max_systems: int = 256, check_every: int = 4, hbm_budget: float = 0.0,
+                 sweep: str = "RSRS", pc: str = "LINE", device: int = 0, inner_tol: float = 0.0):
+        cfg = ServerConfigC(int(precision), int(max_systems), int(check_every), int(device), float(hbm_budget),
+                            float(inner_tol), sweep.ljust(4)[:4].encode(), pc.ljust(4)[:4].encode())
+        h = C.c_void_p()
+        rc = lib().mfixgpu_server_create(C.byref(cfg), C.byref(h))
+        if rc:
+            raise RuntimeError(f"mfixgpu_server_create: {rc} ({last_error()})")
+        self._h = h
+        self._keep: dict[int, tuple] = {}
+
+    def submit(self, s, zero_guess: bool = False, write_ab: bool = False, on_device: bool = False,
+               pointers=None) -> int:
+        """Queues System ``s`` (host arrays) or, with ``on_device``, the device
+        pointers ``pointers = (a, b, x)``.  Returns the ticket (>= 0) or an error code."""
+        c = SystemC()
+        c.imax2, c.jmax2, c.kmax2, c.do_k = s.imax2, s.jmax2, s.kmax2, s.do_k
+        c.dimension_3 = s.n
+        if on_device:
+            c.a_m, c.b_m, c.var = pointers
+        else:
+            c.a_m, c.b_m, c.var = _ptr(s.a), _ptr(s.b), _ptr(s.x)
+        c.tol = s.tol
+        c.itmax = s.itmax
+        flags = (REQ_ZERO_GUESS if zero_guess else 0) | (REQ_WRITE_AB if write_ab else 0) | \
+                (REQ_ON_DEVICE if on_device else 0)
+        t = int(lib().mfixgpu_server_submit(self._h, C.byref(c), flags))
+        if t >= 0:
+            self._keep[t] = (s, pointers)
+        return t
+
+    def _done(self, t: int, rc: int, r: RequestC):
+        if rc == 1:
+            self._keep.pop(t, None)
+            return _struct_dict(r)
+        if rc == 0:
+            return None
+        raise KeyError(f"ticket {t}: {rc}")
+
+    def poll(self, t: int):
+        r = RequestC()
+        return self._done(t, lib().mfixgpu_server_poll(self._h, t, C.byref(r)), r)
+
+    def wait(self, t: int, timeout: float = -1.0):
+        r = RequestC()
+        return self._done(t, lib().mfixgpu_server_wait(self._h, t, float(timeout), C.byref(r)), r)
+
+    def wait_any(self, timeout: float = -1.0):
+        """(ticket, result) of a finished request nobody has collected, or None on timeout."""
+        r = RequestC()
+        t = C.c_longlong(-1)
+        rc = lib().mfixgpu_server_wait_any(self._h, float(timeout), C.byref(t), C.byref(r))
+        if rc != 1:
+            return None
+        self._keep.pop(t.value, None)
+        return t.value, _struct_dict(r)
+
+    def counters(self) -> dict:
+        c = ServerCountersC()
+        lib().mfixgpu_server_counters_get(self._h, C.byref(c))
+        return _struct_dict(c)
+
+    def close(self) -> None:
+        if self._h:
+            lib().mfixgpu_server_destroy(self._h)
+            self._h = None
+            self._keep.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -90,3 +90,50 @@ def test_fastdiv_formula():
         for n in ns.tolist():
             q = (((n * m) >> 32) + n) >> l
             assert q == n // d, (d, n)
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """The ctypes mirrors have the sizes and field offsets of include/mfixgpu.h."""
+    import ctypes as C
+    import subprocess
+
+    structs = {"mfixgpu_stats": leq.Stats, "mfixgpu_geom": leq.Geom, "mfixgpu_system": leq.SystemC,
+               "mfixgpu_server_config": leq.ServerConfigC, "mfixgpu_request": leq.RequestC,
+               "mfixgpu_server_counters": leq.ServerCountersC}
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "mfixgpu.h"', 'int main(void){']
+    for cname, py in structs.items():
+        lines.append(f'printf("{cname} size %zu\\n", sizeof({cname}));')
+        for f, _ in py._fields_:
+            lines.append(f'printf("{cname} {f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append("return 0;}")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.split("\n")
+    got = {tuple(l.split()[:2]): int(l.split()[2]) for l in out if l.strip()}
+    for cname, py in structs.items():
+        assert got[(cname, "size")] == C.sizeof(py), cname
+        for f, _ in py._fields_:
+            assert got[(cname, f)] == getattr(py, f).offset, (cname, f)
+
+
+def test_server_config_errors_before_device_work():
+    import ctypes as C
+
+    L = mfix_b200.lib()
+    h = C.c_void_p()
+
+    def create(**kw):
+        cfg = leq.ServerConfigC(kw.get("precision", 1), 0, 0, 0, 0.0, 0.0, kw.get("sweep", b"RSRS"),
+                                kw.get("pc", b"LINE"))
+        return L.mfixgpu_server_create(C.byref(cfg), C.byref(h))
+
+    assert create(precision=2) == leq.IER_ARGS
+    assert create(pc=b"ILU ") == leq.IER_UNSUPPORTED
+    assert create(sweep=b"ISIS") == leq.IER_UNSUPPORTED
+    assert create(sweep=b"ASAS") == leq.IER_UNSUPPORTED
+    assert L.mfixgpu_server_create(None, None) == leq.IER_ARGS
+    if not _gpu_visible():
+        assert create() == leq.IER_CUDA
+        assert "no CUDA device" in leq.last_error()
