@@ -31,6 +31,7 @@ extern "C" {
 #define MFIXGPU_ERR_ARGS (-14)        /* inconsistent arguments */
 #define MFIXGPU_ERR_INCOMPLETE (-15)  /* solve stopped without a verdict */
 #define MFIXGPU_ERR_NOGEOM (-16)      /* mfixgpu_init_geometry was not called */
+#define MFIXGPU_ERR_CANCELLED (-17)   /* serving: the request was withdrawn before it was admitted */
 
 /* ---------------------------------------------------------------- drop-in */
 
@@ -252,6 +253,9 @@ int mfixgpu_server_wait(void *server, long long ticket, double timeout_s, mfixgp
  * 1 with *ticket and *out (released), 0 on timeout. */
 int mfixgpu_server_wait_any(void *server, double timeout_s, long long *ticket, mfixgpu_request *out);
 int mfixgpu_server_counters_get(void *server, mfixgpu_server_counters *out);
+/* Withdraws every request not yet admitted (copied in): they finish with IER
+ * MFIXGPU_ERR_CANCELLED.  Requests already admitted run to the end. */
+int mfixgpu_server_cancel_queued(void *server);
 /* Finishes every submitted request, stops the worker and frees the server. */
 int mfixgpu_server_destroy(void *server);
 

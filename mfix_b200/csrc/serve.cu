@@ -173,6 +173,13 @@ public:
         o->seconds = now();
     }
 
+    void cancel_queued()
+    {
+        std::lock_guard<std::mutex> lk(mu_);
+        cancel_ = true;
+        cv_work_.notify_all();
+    }
+
     void shutdown()
     {
         {
@@ -549,6 +556,13 @@ private:
                     incoming_.pop_front();
                 }
                 fatal = fatal_ != 0;
+                if (cancel_) {
+                    cancel_ = false;
+                    lk.unlock();
+                    for (Req *r : queue_) fail_request(r, MFIXGPU_ERR_CANCELLED);
+                    queue_.clear();
+                    lk.lock();
+                }
                 const bool busy = !queue_.empty() || !copying_.empty() || running_ > 0 || !handover_.empty() ||
                                   !unloading_.empty() || !frees_.empty() || (mix_ && mix_->live_dirty()) ||
                                   f64_->live_dirty();
@@ -616,7 +630,7 @@ private:
     // shared with callers (mu_)
     std::mutex mu_;
     std::condition_variable cv_work_, cv_done_;
-    bool started_ = false, stop_ = false;
+    bool started_ = false, stop_ = false, cancel_ = false;
     int setup_rc_ = 0, fatal_ = 0;
     double budget_ = 0;
     long long next_id_ = 0, submitted_ = 0, completed_ = 0, commits_ = 0, bodies_ = 0, launches_ = 0,
@@ -730,6 +744,13 @@ int mfixgpu_server_counters_get(void *server, mfixgpu_server_counters *out)
 {
     if (!server || !out) return MFIXGPU_ERR_ARGS;
     static_cast<Server *>(server)->counters(out);
+    return 0;
+}
+
+int mfixgpu_server_cancel_queued(void *server)
+{
+    if (!server) return MFIXGPU_ERR_ARGS;
+    static_cast<Server *>(server)->cancel_queued();
     return 0;
 }
 

@@ -23,6 +23,7 @@ IER_CUDA = -13
 IER_ARGS = -14
 IER_INCOMPLETE = -15
 IER_NOGEOM = -16
+IER_CANCELLED = -17
 
 _dp = C.POINTER(C.c_double)
 _ip = C.POINTER(C.c_int)
@@ -88,6 +89,8 @@ def _declare(L: C.CDLL) -> None:
     L.mfixgpu_server_wait_any.restype = C.c_int
     L.mfixgpu_server_counters_get.argtypes = [C.c_void_p, C.POINTER(ServerCountersC)]
     L.mfixgpu_server_counters_get.restype = C.c_int
+    L.mfixgpu_server_cancel_queued.argtypes = [C.c_void_p]
+    L.mfixgpu_server_cancel_queued.restype = C.c_int
     L.mfixgpu_server_destroy.argtypes = [C.c_void_p]
     L.mfixgpu_server_destroy.restype = C.c_int
     L.mfixgpu_init_geometry.argtypes = [_ip, _ip, _ip, _ip, C.POINTER(C.c_int64), _ip]
@@ -350,6 +353,10 @@ class Server:
         c = ServerCountersC()
         lib().mfixgpu_server_counters_get(self._h, C.byref(c))
         return _struct_dict(c)
+
+    def cancel_queued(self) -> None:
+        """Requests not yet admitted finish with IER_CANCELLED."""
+        lib().mfixgpu_server_cancel_queued(self._h)
 
     def close(self) -> None:
         if self._h:

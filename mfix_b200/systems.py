@@ -257,3 +257,39 @@ def coefficient_contrast(sys: System) -> float:
     off = sys.a[[0, 1, 2, 4, 5, 6]]
     nz = off[off > 0]
     return float(nz.max() / nz.min()) if nz.size else 1.0
+
+
+def pressure_scaled(imax: int, jmax: int, kmax: int, seed: int = 0, itmax: int = 5000, tol: float = 1e-8) -> System:
+    """The pressure-like recipe on a smaller box, its bubbles scaled with it:
+    40 spheres of radius U[6, 20] on 192x384x192 interior cells become
+    round(40 s^3) spheres (at least one) of radius U[6 s, 20 s] (at least
+    U[1.5, 2.5]), s the cube root of the volume ratio."""
+    s = (imax * jmax * kmax / (192.0 * 384.0 * 192.0)) ** (1.0 / 3.0)
+    nsph = max(1, int(round(40 * s ** 3)))
+    rmin = max(1.5, 6.0 * s)
+    rmax = max(rmin + 1.0, 20.0 * s)
+    return pressure_like(imax, jmax, kmax, seed=seed, nspheres=nsph, rmin=rmin, rmax=rmax, itmax=itmax, tol=tol)
+
+
+def serve_mix(count: int, seed: int, lo: int = 24, hi: int = 160, pressure_share: float = 0.2,
+              tols=(1e-6, 1e-8)):
+    """Request mix of the serving workload: per-axis sizes log-uniform on
+    [lo, hi], a `pressure_share` of pressure-like systems (the rest
+    convection-diffusion), TOL drawn uniformly from `tols`.  Returns a list of
+    (kind, (imax, jmax, kmax), tol, system_seed)."""
+    q = np.arange(count)
+    dims = []
+    for ax in range(3):
+        u = uniform(seed, 70 + ax, q)
+        v = np.exp(np.log(lo) + u * (np.log(hi + 1) - np.log(lo)))
+        dims.append(np.minimum(np.floor(v).astype(np.int64), hi))
+    kind = uniform(seed, 73, q) < pressure_share
+    tsel = np.minimum((uniform(seed, 74, q) * len(tols)).astype(np.int64), len(tols) - 1)
+    return [("pressure_like" if kind[i] else "conv_diff", (int(dims[0][i]), int(dims[1][i]), int(dims[2][i])),
+             float(tols[tsel[i]]), int(seed * 100003 + i)) for i in range(count)]
+
+
+def make_request_system(kind: str, dims, tol: float, seed: int) -> System:
+    if kind == "pressure_like":
+        return pressure_scaled(*dims, seed=seed, tol=tol)
+    return conv_diff(*dims, seed=seed, tol=tol)
