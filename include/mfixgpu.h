@@ -95,6 +95,9 @@ const char *mfixgpu_last_error(void);
  *   "precision"      0 FP64 drop-in (default), 1 FP32 BiCGSTAB with FP64 solution accumulation,
  *                    FP64 dot products and FP64 reliable residual updates; a system whose FP32
  *                    iteration diverges or stalls is re-solved by the FP64 drop-in
+ *   "mixed_growth"   mixed form: hand over to FP64 when a true residual exceeds this multiple of
+ *                    the best one seen (default 10)
+ *   "mixed_stalls"   mixed form: hand over after this many reliable updates without a 10% gain (default 6)
  *   "write_back_ab"  1 (default) copy the scaled A_M/B_M slices back
  *   "rtilde_seed"    seed of the Rtilde random stream (replaces RANDOM_NUMBER, model/leq_bicgs.f:298)
  *   "inner_tol"      mixed form: drop of the FP32 residual between FP64 reliable updates (default 1e-2)

@@ -31,6 +31,8 @@ struct Options {
     int write_back_ab = 1;
     uint64_t seed = 0x5EEDULL;
     double inner_tol = 1e-2;
+    double mixed_growth = 10.0;
+    int mixed_stalls = 6;
     int check_every = 4;
     int use_graph = 1;
     int time_kernels = 0;
@@ -102,6 +104,8 @@ SolveOptions make_opts(const Options &o, int pc, const char sweep4[4])
     so.write_back_ab = o.write_back_ab != 0;
     so.seed = o.seed;
     so.inner_tol = o.inner_tol;
+    so.mixed_growth = o.mixed_growth;
+    so.mixed_stalls = o.mixed_stalls;
     so.check_every = o.check_every;
     so.use_graph = o.use_graph != 0;
     so.time_kernels = o.time_kernels != 0;
@@ -294,6 +298,12 @@ int mfixgpu_set_option(const char *name, double value)
     } else if (k == "inner_tol") {
         if (!(value > 0 && value < 1)) return MFIXGPU_ERR_ARGS;
         g.opt.inner_tol = value;
+    } else if (k == "mixed_growth") {
+        if (!(value > 1)) return MFIXGPU_ERR_ARGS;
+        g.opt.mixed_growth = value;
+    } else if (k == "mixed_stalls") {
+        if (value < 1) return MFIXGPU_ERR_ARGS;
+        g.opt.mixed_stalls = (int)value;
     } else if (k == "check_every") {
         if (value < 1) return MFIXGPU_ERR_ARGS;
         g.opt.check_every = (int)value;
@@ -322,6 +332,8 @@ double mfixgpu_get_option(const char *name)
     if (k == "write_back_ab") return g.opt.write_back_ab;
     if (k == "rtilde_seed") return (double)g.opt.seed;
     if (k == "inner_tol") return g.opt.inner_tol;
+    if (k == "mixed_growth") return g.opt.mixed_growth;
+    if (k == "mixed_stalls") return g.opt.mixed_stalls;
     if (k == "check_every") return g.opt.check_every;
     if (k == "use_graph") return g.opt.use_graph;
     if (k == "time_kernels") return g.opt.time_kernels;

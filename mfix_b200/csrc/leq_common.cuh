@@ -98,6 +98,8 @@ struct SysState {
     double inner_tol;     // mixed form: residual drop (vs maxr) that triggers a reliable update
     double maxr;          // mixed form: largest recursive residual since the last reliable update
     double best;          // mixed form: smallest true residual seen at a reliable update
+    double growth_limit;  // mixed form: hand over when a true residual exceeds growth_limit * best
+    int stall_limit;      // mixed form: hand over after this many updates without a 10% gain
     int itmax;
     int i;                // reference loop index of the next iteration (1-based)
     int iter;             // reference ITER counter

@@ -264,6 +264,8 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         st.phase = opt.skip_scale ? PH_INIT : PH_SETUP;
         st.mixed = mixed ? 1 : 0;
         st.inner_tol = opt.inner_tol;
+        st.growth_limit = opt.mixed_growth;
+        st.stall_limit = opt.mixed_stalls;
         st.i = 1;
         st.iter = 1;
     }
@@ -309,6 +311,10 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
     cfg_.g_s = grid(oc.s_update);
     cfg_.g_xr = grid(oc.xr_update);
     cfg_.g_mv = grid(oc.matvec);
+    cfg_.g_mv_pair = grid(oc.matvec_pair);
+    cfg_.rows_pair = cfg_.rows_single = 0;
+    for (int q = 0; q < nsys_; ++q)
+        if (h_sys_[q].n > 0) ((h_sys_[q].jmax2 & 1) ? cfg_.rows_single : cfg_.rows_pair) = 1;
     cfg_.g_copy = grid(oc.copy);
     cfg_.g_outer = grid(oc.outer);
     return configure_lines(mixed ? 4 : 8);
@@ -747,6 +753,8 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
         if ((int64_t)s.imax2 * s.jmax2 * s.kmax2 != s.n) return fail("DIMENSION_3 != IMAX2*JMAX2*KMAX2", -14);
         if (s.n > (int64_t)INT32_MAX - TILE_CELLS) return fail("system too large for 32-bit cell indexing", -14);
         if (!s.a || !s.b || !s.x) return fail("null array", -14);
+        if (opt.on_device && !aligned16(s))
+            return fail("device arrays must start on 16-byte boundaries (cudaMalloc gives 256)", -14);
     }
     if (opt.pc != PC_LINE && opt.pc != PC_DIAG && opt.pc != PC_NONE) return fail("unknown preconditioner", -10);
 
@@ -858,7 +866,7 @@ int Engine::launch_body(const SolveOptions &opt)
     const int src_ph = opt.pc == PC_NONE ? V_P : V_PH;
     const int src_sh = opt.pc == PC_NONE ? V_S : V_SH;
     int r;
-    launches_ += mixed ? 6 : 5;
+    launches_ += (mixed ? 6 : 5) + 2 * (cfg_.rows_pair + cfg_.rows_single - 1);
     if (mixed) {
         CK(launch_outer_step(view_, cfg_));
         CK((launch_p_update<float, true>(view_, cfg_)));

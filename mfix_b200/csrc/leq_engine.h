@@ -27,6 +27,12 @@ struct SystemSpec {
     int itmax = 500;
 };
 
+// The kernels read A_M, B_M and VAR two cells at a time (16-byte loads).
+inline bool aligned16(const SystemSpec &s)
+{
+    return !(((uintptr_t)s.a | (uintptr_t)s.b | (uintptr_t)s.x) & 15);
+}
+
 struct SolveResult {
     int ier = 0;
     int iterations = 0;    // reference ITER counter (mixed: inner iterations)
@@ -48,6 +54,8 @@ struct SolveOptions {
     bool write_back_ab = true;   // copy the unit-scaled A/B back to host arrays
     uint64_t seed = 0x5EEDULL;   // Rtilde stream
     double inner_tol = 1e-2;     // mixed form: residual drop between reliable updates
+    double mixed_growth = 10.0;  // mixed form: true-residual growth over the best that hands over to FP64
+    int mixed_stalls = 6;        // mixed form: reliable updates without a 10% gain that hand over
     int check_every = 4;         // iterations between host checks of the state
     bool use_graph = true;       // capture the iteration body in a CUDA graph
     bool time_kernels = false;   // record events around every J-line launch (no graph replay)

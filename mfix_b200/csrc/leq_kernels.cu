@@ -107,24 +107,44 @@ __device__ __forceinline__ void block_sum(double (&v)[NV])
     }
 }
 
-// Store a tile's partial sums and report whether this block closed the
-// system's reduction.  When it did, `tot` holds the system totals (thread 0).
+// Deterministic per-system reductions.  Each tile's sum is formed in a fixed
+// order and stored in the tile's slot; once every tile of a system has
+// arrived, the block that completed it adds the slots in tile order.  Arrivals
+// are counted once per run of consecutive tiles of one system a block has
+// processed (one fence and one atomic per run instead of per tile).
+struct TileRun {
+    int sys;
+    int count;
+};
+
 template <int NV>
-__device__ __forceinline__ bool tile_reduce(const BatchView &b, const SysDev &d, SysState &st, int tile_idx,
-                                            double (&v)[NV], double (&tot)[NV])
+__device__ __forceinline__ void tile_partial(const BatchView &b, const SysDev &d, int tile_idx, double (&v)[NV])
 {
-    __shared__ int last;
     block_sum<NV>(v);
     if (threadIdx.x == 0) {
         double *slot = b.partials + 2 * (int64_t)(d.tile_base + tile_idx);
 #pragma unroll
         for (int q = 0; q < NV; ++q) slot[q] = v[q];
-        __threadfence();
-        const unsigned prev = atomicAdd(&st.arrivals, 1u);
-        last = (prev == (unsigned)d.ntiles - 1);
+    }
+}
+
+// Reports the run's tiles; the block that completes the system's count forms
+// the totals and calls fin(state, totals) on thread 0.
+template <int NV, typename Fin>
+__device__ __forceinline__ void run_close(const BatchView &b, TileRun &run, Fin &fin)
+{
+    if (run.count == 0) return;
+    __shared__ int last;
+    const SysDev &d = b.sys[run.sys];
+    SysState &st = b.st[run.sys];
+    if (threadIdx.x == 0) {
+        __threadfence();  // this thread's slot stores before the arrival count
+        const unsigned prev = atomicAdd(&st.arrivals, (unsigned)run.count);
+        last = (prev + (unsigned)run.count == (unsigned)d.ntiles);
     }
     __syncthreads();
-    if (!last) return false;
+    run.count = 0;
+    if (!last) return;
     __threadfence();
     double acc[NV];
 #pragma unroll
@@ -135,10 +155,20 @@ __device__ __forceinline__ bool tile_reduce(const BatchView &b, const SysDev &d,
         for (int q = 0; q < NV; ++q) acc[q] += __ldcg(slot + q);
     }
     block_sum<NV>(acc);
-#pragma unroll
-    for (int q = 0; q < NV; ++q) tot[q] = acc[q];
-    if (threadIdx.x == 0) st.arrivals = 0;
-    return true;
+    if (threadIdx.x == 0) {
+        st.arrivals = 0;
+        fin(st, acc);
+    }
+}
+
+template <int NV, typename Fin>
+__device__ __forceinline__ void run_add(const BatchView &b, TileRun &run, int sys, Fin &fin)
+{
+    if (run.sys != sys) {
+        run_close<NV>(b, run, fin);
+        run.sys = sys;
+    }
+    run.count += 1;
 }
 
 // ------------------------------------------------------------------ scalar steps
@@ -257,6 +287,8 @@ __global__ void k_to_f32(BatchView b)
 template <typename T>
 __global__ void k_init_residual(BatchView b)
 {
+    TileRun run{-1, 0};
+    auto fin = [&](SysState &st, const double(&tot)[1]) { fin_rnorm0(st, tot[0]); };
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
@@ -266,7 +298,7 @@ __global__ void k_init_residual(BatchView b)
         const T *a = diag_base<T>(d);
         const T *x = vec<T>(d, V_X);
         T *r = vec<T>(d, V_R);
-        double v[1] = {0.0}, tot[1];
+        double v[1] = {0.0};
         #pragma unroll 4
         for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
             const CellIdx q = cell_ijk(d, (uint32_t)c);
@@ -275,8 +307,10 @@ __global__ void k_init_residual(BatchView b)
             r[c] = rv;
             v[0] += (double)rv * (double)rv;
         }
-        if (tile_reduce<1>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) fin_rnorm0(st, tot[0]);
+        tile_partial<1>(b, d, tl.idx, v);
+        run_add<1>(b, run, tl.sys, fin);
     }
+    run_close<1>(b, run, fin);
 }
 
 __device__ __forceinline__ uint64_t mix64(uint64_t z)
@@ -298,6 +332,8 @@ __device__ __forceinline__ double uniform01(uint64_t seed, uint64_t tag, uint64_
 template <typename T>
 __global__ void k_init_rtilde(BatchView b, uint64_t seed)
 {
+    TileRun run{-1, 0};
+    auto fin = [&](SysState &st, const double(&tot)[1]) { fin_rho0(st, tot[0]); };
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
@@ -307,7 +343,7 @@ __global__ void k_init_rtilde(BatchView b, uint64_t seed)
         const double rn0 = st.rnorm0;
         const T *r = vec<T>(d, V_R);
         T *rt = vec<T>(d, V_RT);
-        double v[1] = {0.0}, tot[1];
+        double v[1] = {0.0};
         #pragma unroll 4
         for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
             const double u = uniform01(seed, 0xA1, (uint64_t)c);
@@ -316,8 +352,10 @@ __global__ void k_init_rtilde(BatchView b, uint64_t seed)
             rt[c] = rtv;
             v[0] += (double)rtv * (double)rv;
         }
-        if (tile_reduce<1>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) fin_rho0(st, tot[0]);
+        tile_partial<1>(b, d, tl.idx, v);
+        run_add<1>(b, run, tl.sys, fin);
     }
+    run_close<1>(b, run, fin);
 }
 
 // ------------------------------------------------------------------ iteration kernels
@@ -395,6 +433,108 @@ __device__ __forceinline__ T dot_row7(const Row7<T> &r, bool do_k)
     return v;
 }
 
+// Two neighbouring cells per thread: 8-byte (FP32) or 16-byte (FP64) loads
+// halve the load instructions a streaming kernel needs for the same bytes.
+// Tiles start at multiples of TILE_CELLS and vectors at 256-byte boundaries,
+// so the pair (c, c+1) with c even is aligned.
+template <typename T>
+struct Vec2;
+template <>
+struct Vec2<float> {
+    using type = float2;
+};
+template <>
+struct Vec2<double> {
+    using type = double2;
+};
+template <typename T>
+using vec2_t = typename Vec2<T>::type;
+
+template <typename T>
+__device__ __forceinline__ vec2_t<T> ld2(const T *p)
+{
+    return *reinterpret_cast<const vec2_t<T> *>(p);
+}
+template <typename T>
+__device__ __forceinline__ void st2(T *p, const vec2_t<T> &v)
+{
+    *reinterpret_cast<vec2_t<T> *>(p) = v;
+}
+template <typename T>
+__device__ __forceinline__ vec2_t<T> mk2(T a, T b)
+{
+    vec2_t<T> r;
+    r.x = a;
+    r.y = b;
+    return r;
+}
+
+// The operands of rows c and c+1 (c even) of one J-line.  Used when JMAX2 is
+// even: then both cells share i and k, DIMENSION_3 is even so every diagonal's
+// pair is aligned, and so are the pairs at the i and k neighbours.
+__device__ __forceinline__ bool pair_rows(const SysDev &d) { return (d.jmax2 & 1) == 0; }
+
+template <typename T>
+struct Pair7 {
+    vec2_t<T> a[7], x[7];
+};
+
+template <typename T>
+__device__ __forceinline__ void load_pair7(const SysDev &d, const T *__restrict__ A, const T *__restrict__ X,
+                                           int64_t c, Pair7<T> &r)
+{
+    const int64_t n = d.n;
+    const CellIdx q = cell_ijk(d, (uint32_t)c);
+    const int64_t c1 = d.jmax2, c2 = (int64_t)d.jmax2 * d.imax2;
+    const int64_t im = q.i > 0 ? -c1 : 0, ip = q.i < d.imax2 - 1 ? c1 : 0;
+    const vec2_t<T> xc = ld2(X + c);
+    const T xl = X[c + (q.j > 0 ? -1 : 0)];              // x(j-1) of cell c (clamped)
+    const T xr = X[c + 1 + (q.j + 1 < d.jmax2 - 1 ? 1 : 0)];  // x(j+1) of cell c+1 (clamped)
+    r.a[0] = ld2(A + 1 * n + c);
+    r.x[0] = mk2<T>(xl, xc.x);
+    r.a[1] = ld2(A + 2 * n + c);
+    r.x[1] = ld2(X + c + im);
+    r.a[2] = ld2(A + 3 * n + c);
+    r.x[2] = xc;
+    r.a[3] = ld2(A + 4 * n + c);
+    r.x[3] = ld2(X + c + ip);
+    r.a[4] = ld2(A + 5 * n + c);
+    r.x[4] = mk2<T>(xc.y, xr);
+    if (d.do_k) {
+        const int64_t km = q.k > 0 ? -c2 : 0, kp = q.k < d.kmax2 - 1 ? c2 : 0;
+        r.a[5] = ld2(A + 0 * n + c);
+        r.x[5] = ld2(X + c + km);
+        r.a[6] = ld2(A + 6 * n + c);
+        r.x[6] = ld2(X + c + kp);
+    } else {
+        r.a[5] = r.a[6] = mk2<T>(T(0), T(0));
+        r.x[5] = r.x[6] = mk2<T>(T(0), T(0));
+    }
+}
+
+// dot_row7 of both rows, in the same operand order
+template <typename T>
+__device__ __forceinline__ vec2_t<T> dot_pair7(const Pair7<T> &r, bool do_k)
+{
+    T u = r.a[0].x * r.x[0].x;
+    T w = r.a[0].y * r.x[0].y;
+    u = u + r.a[1].x * r.x[1].x;
+    w = w + r.a[1].y * r.x[1].y;
+    u = u + r.a[2].x * r.x[2].x;
+    w = w + r.a[2].y * r.x[2].y;
+    u = u + r.a[3].x * r.x[3].x;
+    w = w + r.a[3].y * r.x[3].y;
+    u = u + r.a[4].x * r.x[4].x;
+    w = w + r.a[4].y * r.x[4].y;
+    if (do_k) {
+        u = u + r.a[5].x * r.x[5].x;
+        w = w + r.a[5].y * r.x[5].y;
+        u = u + r.a[6].x * r.x[6].x;
+        w = w + r.a[6].y * r.x[6].y;
+    }
+    return mk2<T>(u, w);
+}
+
 // cells handled per thread per batch: stencil kernels, streaming kernels
 template <typename T>
 struct Batch {
@@ -406,7 +546,7 @@ struct Batch {
 template <typename T, bool MIXED>
 __global__ void __launch_bounds__(256, 4) k_p_update(BatchView b)
 {
-    constexpr int U = Batch<T>::STREAM;
+    constexpr int U2 = Batch<T>::STREAM / 2;
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
@@ -416,39 +556,47 @@ __global__ void __launch_bounds__(256, 4) k_p_update(BatchView b)
         const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
         const T *__restrict__ r = vec<T>(d, V_R) + c0;
         T *__restrict__ p = vec<T>(d, V_P) + c0;
+        const int np = cnt >> 1;  // cell pairs; an odd last cell is done by thread 0
         if (st.i == 1) {
-            for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
-                T rv[U];
+            for (int base = threadIdx.x; base < np; base += U2 * blockDim.x) {
+                vec2_t<T> rv[U2];
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int c = base + u * blockDim.x;
-                    if (c < cnt) rv[u] = r[c];
+                for (int u = 0; u < U2; ++u) {
+                    const int q = base + u * blockDim.x;
+                    if (q < np) rv[u] = ld2(r + 2 * q);
                 }
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int c = base + u * blockDim.x;
-                    if (c < cnt) p[c] = rv[u];
+                for (int u = 0; u < U2; ++u) {
+                    const int q = base + u * blockDim.x;
+                    if (q < np) st2(p + 2 * q, rv[u]);
                 }
             }
+            if ((cnt & 1) && threadIdx.x == 0) p[cnt - 1] = r[cnt - 1];
         } else {
             const T beta = (T)st.beta, omega = (T)st.omega;
             const T *__restrict__ v = vec<T>(d, V_V) + c0;
-            for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
-                T rv[U], pv[U], vv[U];
+            for (int base = threadIdx.x; base < np; base += U2 * blockDim.x) {
+                vec2_t<T> rv[U2], pv[U2], vv[U2];
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int c = base + u * blockDim.x;
-                    if (c < cnt) {
-                        rv[u] = r[c];
-                        pv[u] = p[c];
-                        vv[u] = v[c];
+                for (int u = 0; u < U2; ++u) {
+                    const int q = base + u * blockDim.x;
+                    if (q < np) {
+                        rv[u] = ld2(r + 2 * q);
+                        pv[u] = ld2(p + 2 * q);
+                        vv[u] = ld2(v + 2 * q);
                     }
                 }
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int c = base + u * blockDim.x;
-                    if (c < cnt) p[c] = rv[u] + beta * (pv[u] - omega * vv[u]);
+                for (int u = 0; u < U2; ++u) {
+                    const int q = base + u * blockDim.x;
+                    if (q < np)
+                        st2(p + 2 * q, mk2<T>(rv[u].x + beta * (pv[u].x - omega * vv[u].x),
+                                              rv[u].y + beta * (pv[u].y - omega * vv[u].y)));
                 }
+            }
+            if ((cnt & 1) && threadIdx.x == 0) {
+                const int c = cnt - 1;
+                p[c] = r[c] + beta * (p[c] - omega * v[c]);
             }
         }
     }
@@ -516,22 +664,50 @@ __global__ void __launch_bounds__(256, 4) k_copy(BatchView b, int src, int dst, 
 }
 
 // V = A*Phat and alpha = rho / (Rtilde, V) (model/leq_bicgs.f:355-361).
-template <typename T, bool MIXED>
+template <typename T, bool MIXED, bool PAIR>
 __global__ void __launch_bounds__(256) k_matvec_alpha(BatchView b, int src)
 {
     constexpr int U = Batch<T>::STENCIL;
+    constexpr int UP = Batch<T>::STENCIL / 2;
+    TileRun run{-1, 0};
+    auto fin = [&](SysState &st, const double(&tot)[1]) { st.alpha = st.rho / tot[0]; };
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
         SysState &st = b.st[tl.sys];
-        if (!gate_ok(st, G_INNER)) continue;
+        if (!gate_ok(st, G_INNER) || pair_rows(d) != PAIR) continue;
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
         const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
         const T *__restrict__ a = diag_base<T>(d);
         const T *__restrict__ x = vec<T>(d, src);
         const T *__restrict__ rt = vec<T>(d, V_RT);
         T *__restrict__ y = vec<T>(d, V_V);
-        double v[1] = {0.0}, tot[1];
+        double v[1] = {0.0};
+        if constexpr (PAIR) {
+            const int np = cnt >> 1;
+            for (int base = threadIdx.x; base < np; base += UP * blockDim.x) {
+                Pair7<T> rw[UP];
+                vec2_t<T> rtv[UP];
+#pragma unroll
+                for (int u = 0; u < UP; ++u) {
+                    const int q = base + u * blockDim.x;
+                    if (q < np) {
+                        load_pair7<T>(d, a, x, c0 + 2 * q, rw[u]);
+                        rtv[u] = ld2(rt + c0 + 2 * q);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < UP; ++u) {
+                    const int q = base + u * blockDim.x;
+                    if (q < np) {
+                        const vec2_t<T> yv = dot_pair7<T>(rw[u], d.do_k);
+                        st2(y + c0 + 2 * q, yv);
+                        v[0] += (double)rtv[u].x * (double)yv.x;
+                        v[0] += (double)rtv[u].y * (double)yv.y;
+                    }
+                }
+            }
+        } else {
         for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
             Row7<T> rw[U];
             T rtv[U];
@@ -553,15 +729,26 @@ __global__ void __launch_bounds__(256) k_matvec_alpha(BatchView b, int src)
                 }
             }
         }
-        if (tile_reduce<1>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) st.alpha = st.rho / tot[0];
+        }
+        tile_partial<1>(b, d, tl.idx, v);
+        run_add<1>(b, run, tl.sys, fin);
     }
+    run_close<1>(b, run, fin);
 }
 
 // S = R - alpha*V and Snorm (model/leq_bicgs.f:365-375).
 template <typename T, bool MIXED>
 __global__ void __launch_bounds__(256, 4) k_s_update(BatchView b)
 {
-    constexpr int U = Batch<T>::STREAM;
+    constexpr int U2 = Batch<T>::STREAM / 2;
+    TileRun run{-1, 0};
+    auto fin = [&](SysState &st, const double(&tot)[1]) {
+        st.snorm = sqrt(tot[0]);
+        if (MIXED)
+            st.snorm_exit = (st.snorm <= 0.1 * st.tol * st.outer_rnorm0) ? 1 : 0;
+        else
+            st.snorm_exit = (st.snorm <= DBL_EPSILON) ? 1 : 0;  // TOLMIN = EPSILON(ONE)
+    };
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
@@ -573,54 +760,92 @@ __global__ void __launch_bounds__(256, 4) k_s_update(BatchView b)
         const T *__restrict__ r = vec<T>(d, V_R) + c0;
         const T *__restrict__ vv = vec<T>(d, V_V) + c0;
         T *__restrict__ s = vec<T>(d, V_S) + c0;
-        double v[1] = {0.0}, tot[1];
-        for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
-            T rv[U], wv[U];
+        double v[1] = {0.0};
+        const int np = cnt >> 1;
+        for (int base = threadIdx.x; base < np; base += U2 * blockDim.x) {
+            vec2_t<T> rv[U2], wv[U2];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int c = base + u * blockDim.x;
-                if (c < cnt) {
-                    rv[u] = r[c];
-                    wv[u] = vv[c];
+            for (int u = 0; u < U2; ++u) {
+                const int q = base + u * blockDim.x;
+                if (q < np) {
+                    rv[u] = ld2(r + 2 * q);
+                    wv[u] = ld2(vv + 2 * q);
                 }
             }
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int c = base + u * blockDim.x;
-                if (c < cnt) {
-                    const T sv = rv[u] - alpha * wv[u];
-                    s[c] = sv;
-                    v[0] += (double)sv * (double)sv;
+            for (int u = 0; u < U2; ++u) {
+                const int q = base + u * blockDim.x;
+                if (q < np) {
+                    const T s0 = rv[u].x - alpha * wv[u].x, s1 = rv[u].y - alpha * wv[u].y;
+                    st2(s + 2 * q, mk2<T>(s0, s1));
+                    v[0] += (double)s0 * (double)s0;
+                    v[0] += (double)s1 * (double)s1;
                 }
             }
         }
-        if (tile_reduce<1>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) {
-            st.snorm = sqrt(tot[0]);
-            if (MIXED)
-                st.snorm_exit = (st.snorm <= 0.1 * st.tol * st.outer_rnorm0) ? 1 : 0;
-            else
-                st.snorm_exit = (st.snorm <= DBL_EPSILON) ? 1 : 0;  // TOLMIN = EPSILON(ONE)
+        if ((cnt & 1) && threadIdx.x == 0) {
+            const int c = cnt - 1;
+            const T sv = r[c] - alpha * vv[c];
+            s[c] = sv;
+            v[0] += (double)sv * (double)sv;
         }
+        tile_partial<1>(b, d, tl.idx, v);
+        run_add<1>(b, run, tl.sys, fin);
     }
+    run_close<1>(b, run, fin);
 }
 
 // T = A*Shat, omega = (T,S)/(T,T) with (T,T) = 0 -> SMALL_NUMBER (model/leq_bicgs.f:409-427).
-template <typename T, bool MIXED>
+template <typename T, bool MIXED, bool PAIR>
 __global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
 {
     constexpr int U = Batch<T>::STENCIL;
+    constexpr int UP = Batch<T>::STENCIL / 2;
+    TileRun run{-1, 0};
+    auto fin = [&](SysState &st, const double(&tot)[2]) {
+        double txt = tot[1];
+        if (txt == 0.0) txt = 1.0e-15;  // SMALL_NUMBER
+        st.omega = tot[0] / txt;
+    };
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
         SysState &st = b.st[tl.sys];
-        if (!gate_ok(st, G_INNER_NOSNORM)) continue;
+        if (!gate_ok(st, G_INNER_NOSNORM) || pair_rows(d) != PAIR) continue;
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
         const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
         const T *__restrict__ a = diag_base<T>(d);
         const T *__restrict__ x = vec<T>(d, src);
         const T *__restrict__ s = vec<T>(d, V_S);
         T *__restrict__ y = vec<T>(d, V_T);
-        double v[2] = {0.0, 0.0}, tot[2];
+        double v[2] = {0.0, 0.0};
+        if constexpr (PAIR) {
+            const int np = cnt >> 1;
+            for (int base = threadIdx.x; base < np; base += UP * blockDim.x) {
+                Pair7<T> rw[UP];
+                vec2_t<T> sv[UP];
+#pragma unroll
+                for (int u = 0; u < UP; ++u) {
+                    const int q = base + u * blockDim.x;
+                    if (q < np) {
+                        load_pair7<T>(d, a, x, c0 + 2 * q, rw[u]);
+                        sv[u] = ld2(s + c0 + 2 * q);
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < UP; ++u) {
+                    const int q = base + u * blockDim.x;
+                    if (q < np) {
+                        const vec2_t<T> yv = dot_pair7<T>(rw[u], d.do_k);
+                        st2(y + c0 + 2 * q, yv);
+                        v[0] += (double)yv.x * (double)sv[u].x;
+                        v[1] += (double)yv.x * (double)yv.x;
+                        v[0] += (double)yv.y * (double)sv[u].y;
+                        v[1] += (double)yv.y * (double)yv.y;
+                    }
+                }
+            }
+        } else {
         for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
             Row7<T> rw[U];
             T sv[U];
@@ -643,12 +868,11 @@ __global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
                 }
             }
         }
-        if (tile_reduce<2>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) {
-            double txt = tot[1];
-            if (txt == 0.0) txt = 1.0e-15;  // SMALL_NUMBER
-            st.omega = tot[0] / txt;
         }
+        tile_partial<2>(b, d, tl.idx, v);
+        run_add<2>(b, run, tl.sys, fin);
     }
+    run_close<2>(b, run, fin);
 }
 
 // X += alpha*Phat + omega*Shat; R = S - omega*T; Rnorm; next rho
@@ -723,7 +947,14 @@ __device__ inline void fin_xr_inner(SysState &s, double rr, double rtr)
 template <typename T, bool MIXED>
 __global__ void __launch_bounds__(256) k_xr_update(BatchView b, int ph_id, int sh_id)
 {
-    constexpr int U = sizeof(T) == 8 ? 2 : 4;
+    constexpr int U2 = sizeof(T) == 8 ? 1 : 2;
+    TileRun run{-1, 0};
+    auto fin = [&](SysState &st, const double(&tot)[2]) {
+        if (MIXED)
+            fin_xr_inner(st, tot[0], tot[1]);
+        else
+            fin_xr_ref(st, tot[0], tot[1]);
+    };
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
@@ -738,25 +969,28 @@ __global__ void __launch_bounds__(256) k_xr_update(BatchView b, int ph_id, int s
             (MIXED ? reinterpret_cast<X_T *>(d.x64[0]) : reinterpret_cast<X_T *>(vec<T>(d, V_X))) + c0;
         const X_T alpha = (X_T)st.alpha;
         const T *__restrict__ ph = vec<T>(d, ph_id) + c0;
-        double v[2] = {0.0, 0.0}, tot[2];
+        double v[2] = {0.0, 0.0};
+        const int np = cnt >> 1;
         if (st.snorm_exit) {
-            for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
-                X_T xv[U];
-                T pv[U];
+            for (int base = threadIdx.x; base < np; base += U2 * blockDim.x) {
+                vec2_t<X_T> xv[U2];
+                vec2_t<T> pv[U2];
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int c = base + u * blockDim.x;
-                    if (c < cnt) {
-                        xv[u] = x[c];
-                        pv[u] = ph[c];
+                for (int u = 0; u < U2; ++u) {
+                    const int q = base + u * blockDim.x;
+                    if (q < np) {
+                        xv[u] = ld2(x + 2 * q);
+                        pv[u] = ld2(ph + 2 * q);
                     }
                 }
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int c = base + u * blockDim.x;
-                    if (c < cnt) x[c] = xv[u] + alpha * (X_T)pv[u];
+                for (int u = 0; u < U2; ++u) {
+                    const int q = base + u * blockDim.x;
+                    if (q < np)
+                        st2(x + 2 * q, mk2<X_T>(xv[u].x + alpha * (X_T)pv[u].x, xv[u].y + alpha * (X_T)pv[u].y));
                 }
             }
+            if ((cnt & 1) && threadIdx.x == 0) x[cnt - 1] = x[cnt - 1] + alpha * (X_T)ph[cnt - 1];
         } else {
             const X_T omega = (X_T)st.omega;
             const T omega_t = (T)st.omega;
@@ -765,41 +999,49 @@ __global__ void __launch_bounds__(256) k_xr_update(BatchView b, int ph_id, int s
             const T *__restrict__ tv = vec<T>(d, V_T) + c0;
             const T *__restrict__ rt = vec<T>(d, V_RT) + c0;
             T *__restrict__ r = vec<T>(d, V_R) + c0;
-            for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
-                X_T xv[U];
-                T pv[U], hv[U], sv[U], tw[U], rtv[U];
+            for (int base = threadIdx.x; base < np; base += U2 * blockDim.x) {
+                vec2_t<X_T> xv[U2];
+                vec2_t<T> pv[U2], hv[U2], sv[U2], tw[U2], rtv[U2];
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int c = base + u * blockDim.x;
-                    if (c < cnt) {
-                        xv[u] = x[c];
-                        pv[u] = ph[c];
-                        hv[u] = sh[c];
-                        sv[u] = s[c];
-                        tw[u] = tv[c];
-                        rtv[u] = rt[c];
+                for (int u = 0; u < U2; ++u) {
+                    const int q = base + u * blockDim.x;
+                    if (q < np) {
+                        xv[u] = ld2(x + 2 * q);
+                        pv[u] = ld2(ph + 2 * q);
+                        hv[u] = ld2(sh + 2 * q);
+                        sv[u] = ld2(s + 2 * q);
+                        tw[u] = ld2(tv + 2 * q);
+                        rtv[u] = ld2(rt + 2 * q);
                     }
                 }
 #pragma unroll
-                for (int u = 0; u < U; ++u) {
-                    const int c = base + u * blockDim.x;
-                    if (c < cnt) {
-                        x[c] = xv[u] + alpha * (X_T)pv[u] + omega * (X_T)hv[u];
-                        const T rv = sv[u] - omega_t * tw[u];
-                        r[c] = rv;
-                        v[0] += (double)rv * (double)rv;
-                        v[1] += (double)rtv[u] * (double)rv;
+                for (int u = 0; u < U2; ++u) {
+                    const int q = base + u * blockDim.x;
+                    if (q < np) {
+                        st2(x + 2 * q, mk2<X_T>(xv[u].x + alpha * (X_T)pv[u].x + omega * (X_T)hv[u].x,
+                                                xv[u].y + alpha * (X_T)pv[u].y + omega * (X_T)hv[u].y));
+                        const T r0 = sv[u].x - omega_t * tw[u].x, r1 = sv[u].y - omega_t * tw[u].y;
+                        st2(r + 2 * q, mk2<T>(r0, r1));
+                        v[0] += (double)r0 * (double)r0;
+                        v[1] += (double)rtv[u].x * (double)r0;
+                        v[0] += (double)r1 * (double)r1;
+                        v[1] += (double)rtv[u].y * (double)r1;
                     }
                 }
             }
+            if ((cnt & 1) && threadIdx.x == 0) {
+                const int c = cnt - 1;
+                x[c] = x[c] + alpha * (X_T)ph[c] + omega * (X_T)sh[c];
+                const T rv = s[c] - omega_t * tv[c];
+                r[c] = rv;
+                v[0] += (double)rv * (double)rv;
+                v[1] += (double)rt[c] * (double)rv;
+            }
         }
-        if (tile_reduce<2>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) {
-            if (MIXED)
-                fin_xr_inner(st, tot[0], tot[1]);
-            else
-                fin_xr_ref(st, tot[0], tot[1]);
-        }
+        tile_partial<2>(b, d, tl.idx, v);
+        run_add<2>(b, run, tl.sys, fin);
     }
+    run_close<2>(b, run, fin);
 }
 
 // ------------------------------------------------------------------ mixed form: reliable update
@@ -834,7 +1076,7 @@ __device__ inline void fin_outer(SysState &s, double rr, double rtr32)
     } else {
         s.stall += 1;
     }
-    if (!(rn == rn) || rn > 10.0 * s.best || s.stall >= 6) {
+    if (!(rn == rn) || rn > s.growth_limit * s.best || s.stall >= s.stall_limit) {
         s.exit_kind = EX_FALLBACK;
         s.ier = -20;
         s.status = ST_DONE;
@@ -873,6 +1115,8 @@ __device__ inline void fin_outer(SysState &s, double rr, double rtr32)
 __global__ void __launch_bounds__(256) k_outer_step(BatchView b)
 {
     constexpr int U = 2;
+    TileRun run{-1, 0};
+    auto fin = [&](SysState &st, const double(&tot)[2]) { fin_outer(st, tot[0], tot[1]); };
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
@@ -884,7 +1128,7 @@ __global__ void __launch_bounds__(256) k_outer_step(BatchView b)
         const bool fresh = (st.outer_steps == 0) || st.restart;
         float *__restrict__ r32 = vec<float>(d, V_R);
         float *__restrict__ rt32 = vec<float>(d, V_RT);
-        double v[2] = {0.0, 0.0}, tot[2];
+        double v[2] = {0.0, 0.0};
         for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
             Row7<double> rw[U];
             double bv[U];
@@ -912,8 +1156,10 @@ __global__ void __launch_bounds__(256) k_outer_step(BatchView b)
                 }
             }
         }
-        if (tile_reduce<2>(b, d, st, tl.idx, v, tot) && threadIdx.x == 0) fin_outer(st, tot[0], tot[1]);
+        tile_partial<2>(b, d, tl.idx, v);
+        run_add<2>(b, run, tl.sys, fin);
     }
+    run_close<2>(b, run, fin);
 }
 
 // ------------------------------------------------------------------ J-line half-sweeps
@@ -1557,14 +1803,16 @@ void cell_occupancy(bool fp32, CellOcc *o)
         o->p_update = occ(k_p_update<float, true>);
         o->s_update = occ(k_s_update<float, true>);
         o->xr_update = occ(k_xr_update<float, true>);
-        o->matvec = occ(k_matvec_omega<float, true>);
+        o->matvec = occ(k_matvec_omega<float, true, false>);
+        o->matvec_pair = occ(k_matvec_omega<float, true, true>);
         o->copy = occ(k_copy<float>);
         o->outer = occ(k_outer_step);
     } else {
         o->p_update = occ(k_p_update<double, false>);
         o->s_update = occ(k_s_update<double, false>);
         o->xr_update = occ(k_xr_update<double, false>);
-        o->matvec = occ(k_matvec_omega<double, false>);
+        o->matvec = occ(k_matvec_omega<double, false, false>);
+        o->matvec_pair = occ(k_matvec_omega<double, false, true>);
         o->copy = occ(k_copy<double>);
         o->outer = occ(k_outer_step);
     }
@@ -1592,7 +1840,9 @@ cudaError_t launch_copy(const BatchView &b, const LaunchCfg &c, int src, int dst
 template <typename T, bool MIXED>
 cudaError_t launch_matvec_alpha(const BatchView &b, const LaunchCfg &c, int src)
 {
-    k_matvec_alpha<T, MIXED><<<c.g_mv, CELL_THREADS, 0, c.stream>>>(b, src);
+    // two-cell rows for systems with an even JMAX2, one-cell rows for the others
+    if (c.rows_pair) k_matvec_alpha<T, MIXED, true><<<c.g_mv_pair, CELL_THREADS, 0, c.stream>>>(b, src);
+    if (c.rows_single) k_matvec_alpha<T, MIXED, false><<<c.g_mv, CELL_THREADS, 0, c.stream>>>(b, src);
     CHECK_LAUNCH();
 }
 template <typename T, bool MIXED>
@@ -1604,7 +1854,8 @@ cudaError_t launch_s_update(const BatchView &b, const LaunchCfg &c)
 template <typename T, bool MIXED>
 cudaError_t launch_matvec_omega(const BatchView &b, const LaunchCfg &c, int src)
 {
-    k_matvec_omega<T, MIXED><<<c.g_mv, CELL_THREADS, 0, c.stream>>>(b, src);
+    if (c.rows_pair) k_matvec_omega<T, MIXED, true><<<c.g_mv_pair, CELL_THREADS, 0, c.stream>>>(b, src);
+    if (c.rows_single) k_matvec_omega<T, MIXED, false><<<c.g_mv, CELL_THREADS, 0, c.stream>>>(b, src);
     CHECK_LAUNCH();
 }
 template <typename T, bool MIXED>

@@ -19,6 +19,9 @@ struct LaunchCfg {
     int cell_grid;     // blocks of the setup cell kernels (one per tile)
     int stencil_grid;  // blocks of the setup stencil kernels
     int g_p, g_s, g_xr, g_mv, g_copy, g_outer;  // persistent grids of the iteration kernels
+    int g_mv_pair;        // grid of the matvec kernels' two-cell form
+    int rows_pair;        // 1: some system has an even JMAX2 (two-cell matvec rows)
+    int rows_single;      // 1: some system has an odd JMAX2 (one-cell matvec rows)
     int line_grid;   // blocks for J-line kernels
     int line_cmax;   // max rows per lane over the batch (smem sizing)
     int line_warps;  // warps per block of the J-line kernel
@@ -85,7 +88,7 @@ int kernel_smem_line_bytes(int cmax, int elem_bytes);
 template <typename T>
 int prepare_line_kernel(int cmax, int *warps);  // sets the smem attribute, returns resident blocks per SM
 struct CellOcc {
-    int p_update, s_update, xr_update, matvec, copy, outer;
+    int p_update, s_update, xr_update, matvec, matvec_pair, copy, outer;
 };
 void cell_occupancy(bool fp32, CellOcc *o);
 

@@ -119,6 +119,8 @@ int Engine::live_add(const LiveSystem &ls)
     if ((int64_t)sp.imax2 * sp.jmax2 * sp.kmax2 != sp.n) return fail("DIMENSION_3 != IMAX2*JMAX2*KMAX2", -14);
     if (sp.n > (int64_t)INT32_MAX - TILE_CELLS) return fail("system too large for 32-bit cell indexing", -14);
     if (!sp.a || !sp.b || !sp.x || !ls.work) return fail("null array", -14);
+    if (!aligned16(sp) || ((uintptr_t)ls.work & 255))
+        return fail("device arrays must start on 16-byte boundaries (work blocks on 256)", -14);
     int slot = -1;
     for (int s = 0; s < (int)slot_used_.size() && slot < 0; ++s)
         if (!slot_used_[s]) slot = s;
@@ -155,6 +157,8 @@ int Engine::live_add(const LiveSystem &ls)
     st.phase = ls.scaled ? PH_INIT : PH_SETUP;
     st.mixed = mixed ? 1 : 0;
     st.inner_tol = live_opt_.inner_tol;
+    st.growth_limit = live_opt_.mixed_growth;
+    st.stall_limit = live_opt_.mixed_stalls;
     st.i = 1;
     st.iter = 1;
 
@@ -242,6 +246,10 @@ int Engine::live_commit()
     cfg_.g_s = grid(oc.s_update);
     cfg_.g_xr = grid(oc.xr_update);
     cfg_.g_mv = grid(oc.matvec);
+    cfg_.g_mv_pair = grid(oc.matvec_pair);
+    cfg_.rows_pair = cfg_.rows_single = 0;
+    for (int q = 0; q < nsys_; ++q)
+        if (h_sys_[q].n > 0) ((h_sys_[q].jmax2 & 1) ? cfg_.rows_single : cfg_.rows_pair) = 1;
     cfg_.g_copy = grid(oc.copy);
     cfg_.g_outer = grid(oc.outer);
     int rc = configure_lines(mixed ? 4 : 8);

@@ -79,6 +79,8 @@ public:
             (!s.do_k && s.kmax2 != 1) || s.dimension_3 > (int64_t)INT32_MAX - TILE_CELLS)
             return MFIXGPU_ERR_ARGS;
         if (!s.a_m || !s.b_m || !s.var || (flags & ~7)) return MFIXGPU_ERR_ARGS;
+        if ((flags & MFIXGPU_REQ_ON_DEVICE) && (((uintptr_t)s.a_m | (uintptr_t)s.b_m | (uintptr_t)s.var) & 15))
+            return MFIXGPU_ERR_ARGS;  // device arrays on 16-byte boundaries
         auto r = std::unique_ptr<Req>(new (std::nothrow) Req());
         if (!r) return MFIXGPU_ERR_NOMEM;
         r->user.imax2 = s.imax2;
