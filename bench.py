@@ -50,15 +50,41 @@ WORKLOADS = {
     "serve_poisson": dict(kind="serve", rate=2000.0, seconds=20.0, pool=64, seed=0, budget=150e9),
 }
 DEFAULT_WORKLOAD = "conv_diff_256"
-# Iterations the reference FP64 algorithm needs on each seeded workload (the GPU FP64
-# drop-in follows the same algorithm; tests/test_gpu_bench_workload.py checks it).
-# Used by the CPU arm to turn a timed sample of iterations into solves/s.
+# Iterations the oracle (the reference's FP64 LEQ_BICGS restated in C) takes to
+# converge on each seeded workload, from complete oracle solves of them; the CPU
+# arm times a bounded sample of iterations and scales it by these counts.
 FP64_ITERATIONS = {"conv_diff_256": 66, "conv_diff_64": 65, "conv_diff_192": None, "pressure_192x384x192": None}
 
 BYTES_FP64_ITER = 576  # algorithmic bytes per cell per BiCGSTAB iteration, FP64 (72 words)
 BYTES_FP32_ITER = 288  # the same in the FP32 inner solve
 BYTES_OUTER = 104      # FP64 refinement step: r = b - A x (80) + x update (24)
 BYTES_SETUP = 128      # unit scaling (16 w) of FP64 A and B
+# Algorithmic bytes per cell of one launch of each kernel class (FP32 inner form,
+# FP64 drop-in): operands read + results written, reductions fused.
+CLASS_BYTES = {
+    "jline": (20, 40),          # half the cells: 3 factors + 4 off-line diagonals + rhs + old + new
+    "p_update": (16, 32),       # R, P, V in, P out
+    "matvec_alpha": (40, 80),   # 7 diagonals, x, Rtilde in, V out
+    "s_update": (12, 24),       # R, V in, S out
+    "matvec_omega": (40, 80),   # 7 diagonals, x, S in, T out
+    "xr_update": (40, 64),      # FP32: x64 in/out (16), Phat, Shat, S, T, Rtilde in, R out
+    "outer_step": (80, 80),     # FP64 A (56), x64, B in; FP32 R, Rtilde out
+}
+
+
+def class_table(kt: dict, cells: int, fp32: bool, peak: float) -> dict:
+    """Per kernel class: total ms, launches, mean us, achieved GB/s of algorithmic bytes, fraction of peak."""
+    out = {}
+    for name, (ms, n) in kt.items():
+        if n == 0:
+            continue
+        row = {"ms": round(ms, 3), "launches": int(n), "us_per_launch": round(1e3 * ms / n, 2)}
+        if name in CLASS_BYTES:
+            b = CLASS_BYTES[name][0 if fp32 else 1] * cells
+            gbs = b * n / (ms / 1e3) / 1e9 if ms > 0 else 0.0
+            row.update({"gbs": round(gbs, 1), "frac": round(gbs / peak, 3)})
+        out[name] = row
+    return out
 
 
 def _gen_system(spec):
@@ -360,6 +386,9 @@ def run_ours(args) -> None:
     # J-line launch (direct launches instead of graph replay) for the roofline
     _, st = solve_device(1, time_kernels=True)
     jl_ms, jl_n = st["jline_ms"], st["jline_launches"]
+    kt_mixed = leq.last_kernel_times()
+    _, st64 = solve_device(0, time_kernels=True)
+    kt_fp64 = leq.last_kernel_times()
     leq.set_option("time_kernels", 0)
 
     # accuracy of both forms on the scaled system (A, B hold the scaled copies)
@@ -434,6 +463,8 @@ def run_ours(args) -> None:
                  "gpu_launches": int(fp64_launch)},
         "mixed_vs_fp64": value / fp64_value,
         "line_tiles": [{"elem_bytes": e, "line_length": l, "lanes_per_line": g} for e, l, g in leq.autotune_table()],
+        "kernels_mixed": class_table(kt_mixed, n, True, peak),
+        "kernels_fp64": class_table(kt_fp64, n, False, peak),
         "wall_s_timed_mixed": wall,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -466,15 +497,34 @@ def run_batch_bench(args) -> None:
     from mfix_b200 import leq
     from mfix_b200 import systems as S
 
+    from mfix_b200 import shard
+
+    rank, world, local = dist_env()
     w = WORKLOADS[args.workload]
     sizes = S.batch_sizes(w["count"], w["seed"])
-    specs = [("conv_diff", d, w["tol"], q) for q, d in enumerate(sizes)]
+    specs_all = [("conv_diff", d, w["tol"], q) for q, d in enumerate(sizes)]
+    # ranks share the independent systems (no collective on the data path)
+    mine = shard.assign([(i + 2) * (j + 2) * (k + 2) for i, j, k in sizes], world)[rank]
+    specs = [specs_all[q] for q in mine]
     t0 = time.perf_counter()
     systems = generate_systems(specs)
     t_gen = time.perf_counter() - t0
     cells = sum(x.n for x in systems)
-    dev = torch.device("cuda", 0)
+    dev = torch.device("cuda", local)
     torch.cuda.set_device(dev)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+        torch.cuda.synchronize()
     pristine = [(torch.from_numpy(x.a).to(dev), torch.from_numpy(x.b).to(dev)) for x in systems]
     work = [(torch.empty_like(a), torch.empty_like(b), torch.zeros(x.n, dtype=torch.float64, device=dev))
             for (a, b), x in zip(pristine, systems)]
@@ -511,29 +561,53 @@ def run_batch_bench(args) -> None:
             res.append(r[0])
         return res, dev_s, time.perf_counter() - t, launches
 
+    if args.only != "all":  # profiling runs: the batched solve of one form only
+        if args.line_lanes:
+            leq.set_option("line_lanes", args.line_lanes)
+        for _ in range(args.warmup + args.steps):
+            res, t_dev, t_wall, nl = batched(1 if args.only == "mixed" else 0)
+        print(f"{args.only} batch: {len(systems)} systems, {t_dev * 1e3:.1f} ms, {nl} launches, "
+              f"iterations max {max(r.iterations for r in res)} mean {np.mean([r.iterations for r in res]):.1f}")
+        leq.set_option("time_kernels", 1)  # fixed batch with events around every J-line launch
+        res, t_dev, t_wall, nl = batched(1 if args.only == "mixed" else 0)
+        st = leq.last_stats()
+        leq.set_option("time_kernels", 0)
+        print(f"  timed J-line launches: {st['jline_launches']} in {st['jline_ms']:.1f} ms of {t_dev * 1e3:.1f} ms; "
+              f"lanes {sorted(set(g for e, l, g in leq.autotune_table()))}")
+        for k, (ms, nl) in leq.last_kernel_times().items():
+            print(f"  {k:14s} {ms:9.2f} ms {nl:6d} launches")
+        return
     for _ in range(args.warmup):
         batched(1)
     loop_fp64()  # warm: autotuning of every line length, graph paths
-    sampler = ClockSampler(0)
+    barrier()
+    sampler = ClockSampler(local)
     mixed = []
     with sampler:
         for _ in range(args.steps):
             mixed.append(batched(1))
+        barrier()
     fp64b = [batched(0) for _ in range(max(1, args.steps // 2))]
     loop = loop_fp64()
+    barrier()
     peak, peak_kind = measured_peak_hbm()
     rm = mixed[-1][0]
-    m_dev = float(np.mean([m[1] for m in mixed]))
-    m_wall = float(np.mean([m[2] for m in mixed]))
-    alg_m = sum(_alg_bytes(x.n, 1, r.iterations, r.outer_steps) for x, r in zip(systems, rm))
-    alg_64 = sum(_alg_bytes(x.n, 0, r.iterations, 0) for x, r in zip(systems, loop[0]))
-    f_dev = float(np.mean([m[1] for m in fp64b]))
-    nsys = len(systems)
+    mx = lambda v: shard.max_over_ranks(v, dev)
+    sm = lambda v: shard.sum_over_ranks(v, dev)
+    m_dev = mx(float(np.mean([m[1] for m in mixed])))
+    m_wall = mx(float(np.mean([m[2] for m in mixed])))
+    alg_m = sm(sum(_alg_bytes(x.n, 1, r.iterations, r.outer_steps) for x, r in zip(systems, rm)))
+    alg_64 = sm(sum(_alg_bytes(x.n, 0, r.iterations, 0) for x, r in zip(systems, loop[0])))
+    f_dev = mx(float(np.mean([m[1] for m in fp64b])))
+    loop = (loop[0], mx(loop[1]), mx(loop[2]), int(sm(loop[3])))
+    nsys = int(sm(len(systems)))
+    cells = int(sm(cells))
     line = {
-        "metric": "solves/s", "value": nsys / m_dev, "unit": "solves/s", "n_gpus": 1, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": m_dev * 1e3, "higher_is_better": True, "scaling": "weak",
+        "metric": "solves/s", "value": nsys / m_dev, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": m_dev * 1e3, "higher_is_better": True, "scaling": "strong",
         "vs_baseline": None, "dtype": "fp32-inner/fp64-refinement", "data": "synthetic",
         "config": {"workload": args.workload, "systems": nsys, "cells": cells, "sizes": "per axis U{16..96}",
+                   "parallelism": f"systems sharded over {world} rank(s), longest first",
                    "pc": "LINE", "sweep": "RSRS", "tol": w["tol"], "itmax": w["itmax"],
                    "l2_policy": "inputs larger than L2 (A_M of the batch 7*8*cells bytes)"},
         "roofline": {"kernel": "whole batched solve (algorithmic bytes)", "bound": "hbm",
@@ -553,7 +627,7 @@ def run_batch_bench(args) -> None:
         "mixed_batched_vs_fp64_loop_wall": loop[2] / m_wall,
         "generation_s": t_gen,
     }
-    if not args.no_cpu:
+    if not args.no_cpu and rank == 0 and world == 1:
         import oracle as O
 
         t = time.perf_counter()
@@ -565,7 +639,13 @@ def run_batch_bench(args) -> None:
         dt = time.perf_counter() - t
         line["cpu_baseline"] = {"value": k / dt, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
                                 "sample": f"the first {k} of the {nsys} systems solved completely"}
-    print(json.dumps(line), flush=True)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
 
 
 class _Req:

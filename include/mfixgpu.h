@@ -89,6 +89,15 @@ typedef struct {
 } mfixgpu_stats;
 
 int mfixgpu_last_stats(mfixgpu_stats *out);
+
+/* With option "time_kernels" set: the summed launch durations (ms, CUDA events)
+ * and launch counts of the last solve or batch per kernel class, in this order:
+ * 0 J-line half-sweeps (LINE preconditioner), 1 P update, 2 V = A*Phat with
+ * alpha, 3 S update with Snorm, 4 T = A*Shat with omega, 5 X/R update with
+ * Rnorm and rho, 6 mixed form's FP64 reliable update, 7 copies / DIAG /
+ * sequential line sweeps.  Fills up to max_classes entries of each non-NULL
+ * array and returns the number of classes (8). */
+int mfixgpu_last_kernel_times(double *ms, long long *launches, int max_classes);
 const char *mfixgpu_last_error(void);
 
 /* Options (no reference counterpart; defaults reproduce the reference):

@@ -47,6 +47,7 @@ struct Global {
     Options opt;
     int iter_tot[10] = {0};
     mfixgpu_stats last{};
+    SolveTiming last_timing{};
     std::string err;
 };
 
@@ -190,6 +191,7 @@ void solve_impl(int vno, double *var, double *a_m, double *b_m, int m, int itmax
     g.last.kernel_launches = e->timing().kernel_launches;
     g.last.fp64_fallback = r.fp64_fallback;
     g.last.mixed_iterations = r.mixed_iterations;
+    g.last_timing = e->timing();
     finish(code);
 }
 
@@ -280,6 +282,17 @@ const char *mfixgpu_last_error(void)
 {
     Global &g = G();
     return g.err.c_str();
+}
+
+int mfixgpu_last_kernel_times(double *ms, long long *launches, int max_classes)
+{
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    for (int k = 0; k < KC_COUNT && k < max_classes; ++k) {
+        if (ms) ms[k] = g.last_timing.class_ms[k];
+        if (launches) launches[k] = g.last_timing.class_launches[k];
+    }
+    return KC_COUNT;
 }
 
 int mfixgpu_set_option(const char *name, double value)
@@ -483,6 +496,7 @@ int mfixgpu_batch_solve(mfixgpu_system *systems, int nsys, const char *sweep, co
     g.last.jline_ms = e->timing().jline_ms;
     g.last.jline_launches = e->timing().jline_launches;
     g.last.kernel_launches = e->timing().kernel_launches;
+    g.last_timing = e->timing();
     for (int q = 0; q < nsys; ++q) {
         systems[q].ier = out[q].ier;
         systems[q].iterations = out[q].iterations;

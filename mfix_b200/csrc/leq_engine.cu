@@ -125,7 +125,7 @@ Engine::~Engine()
     if (ev_b_) cudaEventDestroy(ev_b_);
     if (ev_t0_) cudaEventDestroy(ev_t0_);
     if (ev_t1_) cudaEventDestroy(ev_t1_);
-    for (auto &e : jt_ev_)
+    for (auto &e : kt_ev_)
         if (e) cudaEventDestroy(e);
     if (stream_) cudaStreamDestroy(stream_);
 }
@@ -270,10 +270,13 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         st.iter = 1;
     }
 
+    x0_.assign(nsys_, nullptr);
     if (mixed)
-        for (int q = 0; q < nsys_; ++q)
+        for (int q = 0; q < nsys_; ++q) {
+            x0_[q] = h_sys_[q].x64[1];
             CK(cudaMemcpyAsync(h_sys_[q].x64[1], h_sys_[q].x64[0], (size_t)h_sys_[q].n * 8, cudaMemcpyDeviceToDevice,
                                stream_));
+        }
 
     // tables are small; their device copies are reallocated only when they grow
     CK(upload(&d_st_, &st_cap_, h_st_.data(), h_st_.size(), stream_));
@@ -322,8 +325,9 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
 }
 
 // Work items of the J-line kernel (parity waves) and its launch shape, from each
-// system's lanes per line; the system table goes to the device here.
-int Engine::configure_lines(int elem)
+// system's lanes per line; the system table goes to the device here.  only_L > 0
+// keeps the line work of the systems with that line length only (autotuning).
+int Engine::configure_lines(int elem, int only_L)
 {
     h_prefix_.assign(nsys_ + 1, 0);
     int cmax = 1;
@@ -331,7 +335,8 @@ int Engine::configure_lines(int elem)
         const SysDev &d = h_sys_[s];
         cmax = std::max(cmax, d.rows_per_lane);
         const int lpw = 32 / d.lane_group;
-        const int64_t slots = d.n > 0 ? (int64_t)d.half_lines * d.kmax2 : 0;  // empty slot of a live batch
+        const bool keep = d.n > 0 && (only_L == 0 || d.jmax2 == only_L);  // n = 0: empty slot of a live batch
+        const int64_t slots = keep ? (int64_t)d.half_lines * d.kmax2 : 0;
         h_prefix_[s + 1] = h_prefix_[s] + (int)((slots + lpw - 1) / lpw);
     }
     CK(upload(&d_sys_, &sys_cap_, h_sys_.data(), h_sys_.size(), stream_));
@@ -350,6 +355,8 @@ int Engine::configure_lines(int elem)
     cfg_.line_grid = std::max(1, std::min((items + wpb - 1) / wpb, sms_ * bpsm));
     return 0;
 }
+
+static constexpr int MAX_TUNED_ROWS = 17;
 
 static int rows_for(int L, int G)
 {
@@ -383,12 +390,16 @@ void Engine::shape_for(int L, int elem, int forced, int *G, int *c)
 }
 
 // The autotuner: for every line length of the batch without a recorded choice,
-// time a red/black pass of the J-line kernel over the whole batch for each
-// lanes-per-line candidate whose staging fits 48 KB per warp, keep the fastest.
+// time a red/black pass of the J-line kernel over the lines of that length only
+// (the other systems' line work masked out) for each lanes-per-line candidate
+// with at most MAX_TUNED_ROWS rows per lane, and keep the fastest.  The row
+// bound keeps the kernel's shared-memory staging, sized by the batch's largest
+// rows per lane, small enough for full occupancy.
 int Engine::autotune_lines(const SolveOptions &opt, int elem)
 {
     std::vector<int> todo;
     for (int s = 0; s < nsys_; ++s) {
+        if (h_sys_[s].n == 0) continue;  // empty slot of a live batch
         const int L = h_sys_[s].jmax2;
         {
             std::lock_guard<std::mutex> lk(tunes().mu);
@@ -416,13 +427,13 @@ int Engine::autotune_lines(const SolveOptions &opt, int elem)
         float best_ms = 1e30f;
         for (int g = 1; g <= 32; g *= 2) {
             const int c = rows_for(L, g);
-            if ((size_t)kernel_smem_line_bytes(c, elem) > 48 * 1024) continue;
+            if (c > MAX_TUNED_ROWS || (size_t)kernel_smem_line_bytes(c, elem) > 48 * 1024) continue;
             for (int s = 0; s < nsys_; ++s)
-                if (h_sys_[s].jmax2 == L) {
+                if (h_sys_[s].jmax2 == L && h_sys_[s].n > 0) {
                     h_sys_[s].lane_group = g;
                     h_sys_[s].rows_per_lane = c;
                 }
-            int rc = configure_lines(elem);
+            int rc = configure_lines(elem, L);
             if (rc) return rc;
             float tot = 0.f;
             for (int rep = 0; rep < 4; ++rep) {
@@ -446,7 +457,7 @@ int Engine::autotune_lines(const SolveOptions &opt, int elem)
             tunes().lanes[std::make_pair(elem, L)] = best_g;
         }
         for (int s = 0; s < nsys_; ++s)
-            if (h_sys_[s].jmax2 == L) {
+            if (h_sys_[s].jmax2 == L && h_sys_[s].n > 0) {
                 h_sys_[s].lane_group = best_g;
                 h_sys_[s].rows_per_lane = rows_for(L, best_g);
             }
@@ -715,17 +726,47 @@ int Engine::bind_lists()
     return 0;
 }
 
+// ---- time_kernels: events around each launch, summed per kernel class at the end
+void Engine::kt_begin()
+{
+    if (!ktime_ || kt_count_ >= KT_MAX) return;
+    if ((int)kt_ev_.size() < 2 * (kt_count_ + 1)) {
+        const size_t old = kt_ev_.size();
+        kt_ev_.resize(std::max<size_t>(2 * (kt_count_ + 1), old * 2), nullptr);
+        for (size_t q = old; q < kt_ev_.size(); ++q) cudaEventCreate(&kt_ev_[q]);
+    }
+    cudaEventRecord(kt_ev_[2 * kt_count_], stream_);
+}
+
+void Engine::kt_end(int kclass)
+{
+    if (!ktime_ || kt_count_ >= KT_MAX) return;
+    cudaEventRecord(kt_ev_[2 * kt_count_ + 1], stream_);
+    if ((int)kt_class_.size() <= kt_count_) kt_class_.resize(kt_count_ + 1);
+    kt_class_[kt_count_++] = kclass;
+}
+
+void Engine::kt_harvest()
+{
+    for (int q = 0; q < kt_count_; ++q) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, kt_ev_[2 * q], kt_ev_[2 * q + 1]);
+        timing_.class_ms[kt_class_[q]] += ms;
+        timing_.class_launches[kt_class_[q]] += 1;
+    }
+    timing_.jline_ms = timing_.class_ms[KC_JLINE];
+    timing_.jline_launches = timing_.class_launches[KC_JLINE];
+    kt_count_ = 0;
+    ktime_ = false;
+}
+
 int Engine::run_msolve_plan(int which, int elem)
 {
     for (const Step &st : plan_[which]) {
         cudaError_t e = cudaSuccess;
+        kt_begin();
         if (st.type == 0) {
-            if (jline_timing_) cudaEventRecord(jt_ev_[2 * (jline_count_ % JT_EVENTS)], stream_);
             e = (elem == 8) ? launch_jline<double>(view_, cfg_, st.w) : launch_jline<float>(view_, cfg_, st.w);
-            if (jline_timing_) {
-                cudaEventRecord(jt_ev_[2 * (jline_count_ % JT_EVENTS) + 1], stream_);
-                ++jline_count_;
-            }
         } else if (st.type == 1) {
             e = (elem == 8) ? launch_copy<double>(view_, cfg_, st.w.rhs, st.w.dst, st.w.gate)
                             : launch_copy<float>(view_, cfg_, st.w.rhs, st.w.dst, st.w.gate);
@@ -735,6 +776,7 @@ int Engine::run_msolve_plan(int which, int elem)
             e = (elem == 8) ? launch_diag<double>(view_, cfg_, st.w.rhs, st.w.dst, st.w.gate)
                             : launch_diag<float>(view_, cfg_, st.w.rhs, st.w.dst, st.w.gate);
         }
+        kt_end(st.type == 0 ? KC_JLINE : KC_OTHER);
         if (e != cudaSuccess) return fail(std::string("sweep launch: ") + cudaGetErrorString(e), -13);
         ++launches_;
     }
@@ -778,7 +820,14 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
     }
     SolveOptions o = opt;
     o.on_device = true;
-    int rc = run_batch(dev, o, out);
+    // several systems with red/black sweeps: a live batch, which drops systems
+    // as they finish; otherwise the fixed batch (also the timed-kernel path)
+    bool rs_only = true;
+    for (int q = 0; q < 4; ++q) {
+        const char ch = opt.sweep[q];
+        if (ch == 'I' || ch == 'i' || ch == 'K' || ch == 'k' || ch == 'A' || ch == 'a') rs_only = false;
+    }
+    int rc = (specs.size() > 1 && rs_only && !opt.time_kernels) ? run_batch_live(dev, o, out) : run_batch(dev, o, out);
     if (rc) return rc;
     SolveTiming total = timing_;
 
@@ -789,7 +838,7 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
         std::vector<int> idx;
         for (size_t q = 0; q < out.size(); ++q)
             if (out[q].exit_kind == EX_FALLBACK) {
-                CK(cudaMemcpyAsync(dev[q].x, h_sys_[q].x64[1], (size_t)dev[q].n * 8, cudaMemcpyDeviceToDevice,
+                CK(cudaMemcpyAsync(dev[q].x, x0_[q], (size_t)dev[q].n * 8, cudaMemcpyDeviceToDevice,
                                    stream_));
                 fb.push_back(dev[q]);
                 idx.push_back((int)q);
@@ -811,6 +860,10 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
             total.jline_ms += timing_.jline_ms;
             total.jline_launches += timing_.jline_launches;
             total.kernel_launches += timing_.kernel_launches;
+            for (int k = 0; k < KC_COUNT; ++k) {
+                total.class_ms[k] += timing_.class_ms[k];
+                total.class_launches[k] += timing_.class_launches[k];
+            }
         }
     }
     timing_ = total;
@@ -867,24 +920,31 @@ int Engine::launch_body(const SolveOptions &opt)
     const int src_sh = opt.pc == PC_NONE ? V_S : V_SH;
     int r;
     launches_ += (mixed ? 6 : 5) + 2 * (cfg_.rows_pair + cfg_.rows_single - 1);
+#define TK(kc, call)  \
+    do {              \
+        kt_begin();   \
+        CK(call);     \
+        kt_end(kc);   \
+    } while (0)
     if (mixed) {
-        CK(launch_outer_step(view_, cfg_));
-        CK((launch_p_update<float, true>(view_, cfg_)));
+        TK(KC_OUTER, launch_outer_step(view_, cfg_));
+        TK(KC_P_UPDATE, (launch_p_update<float, true>(view_, cfg_)));
         if ((r = run_msolve_plan(0, 4))) return r;
-        CK((launch_matvec_alpha<float, true>(view_, cfg_, src_ph)));
-        CK((launch_s_update<float, true>(view_, cfg_)));
+        TK(KC_MATVEC_ALPHA, (launch_matvec_alpha<float, true>(view_, cfg_, src_ph)));
+        TK(KC_S_UPDATE, (launch_s_update<float, true>(view_, cfg_)));
         if ((r = run_msolve_plan(1, 4))) return r;
-        CK((launch_matvec_omega<float, true>(view_, cfg_, src_sh)));
-        CK((launch_xr_update<float, true>(view_, cfg_, src_ph, src_sh)));
+        TK(KC_MATVEC_OMEGA, (launch_matvec_omega<float, true>(view_, cfg_, src_sh)));
+        TK(KC_XR_UPDATE, (launch_xr_update<float, true>(view_, cfg_, src_ph, src_sh)));
     } else {
-        CK((launch_p_update<double, false>(view_, cfg_)));
+        TK(KC_P_UPDATE, (launch_p_update<double, false>(view_, cfg_)));
         if ((r = run_msolve_plan(0, 8))) return r;
-        CK((launch_matvec_alpha<double, false>(view_, cfg_, src_ph)));
-        CK((launch_s_update<double, false>(view_, cfg_)));
+        TK(KC_MATVEC_ALPHA, (launch_matvec_alpha<double, false>(view_, cfg_, src_ph)));
+        TK(KC_S_UPDATE, (launch_s_update<double, false>(view_, cfg_)));
         if ((r = run_msolve_plan(1, 8))) return r;
-        CK((launch_matvec_omega<double, false>(view_, cfg_, src_sh)));
-        CK((launch_xr_update<double, false>(view_, cfg_, src_ph, src_sh)));
+        TK(KC_MATVEC_OMEGA, (launch_matvec_omega<double, false>(view_, cfg_, src_sh)));
+        TK(KC_XR_UPDATE, (launch_xr_update<double, false>(view_, cfg_, src_ph, src_sh)));
     }
+#undef TK
     return 0;
 }
 
@@ -904,12 +964,10 @@ int Engine::run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &
     if ((rc = plan_msolve(opt, V_S, V_SH, gate_s, 1))) return rc;
     if ((rc = bind_lists())) return rc;
 
-    jline_timing_ = opt.time_kernels;
-    jline_count_ = 0;
+    ktime_ = opt.time_kernels;
+    kt_count_ = 0;
     launches_ = 0;
     timing_ = SolveTiming{};
-    if (jline_timing_ && !jt_ev_[0])
-        for (int q = 0; q < 2 * JT_EVENTS; ++q) cudaEventCreate(&jt_ev_[q]);
     CK(cudaEventRecord(ev_t0_, stream_));
 
     // ---- setup
@@ -935,7 +993,7 @@ int Engine::run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &
     int max_itmax = 0;
     for (const auto &s : specs) max_itmax = std::max(max_itmax, s.itmax);
     const int max_loops = std::max(1, max_itmax + 2);
-    const bool graph = opt.use_graph && !jline_timing_;
+    const bool graph = opt.use_graph && !ktime_;
     cudaGraphExec_t gexec = nullptr;
     long long per_body = 0;
     if (graph) {
@@ -1000,18 +1058,7 @@ int Engine::run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &
     // ---- results back
     for (int s = 0; s < nsys_; ++s) out[s] = result_of(h_st_[s], mixed);
     CK(cudaStreamSynchronize(stream_));
-    if (jline_timing_) {
-        float js = 0.f;
-        const int nrec = std::min(jline_count_, JT_EVENTS);
-        for (int q = 0; q < nrec; ++q) {
-            float ms = 0.f;
-            cudaEventElapsedTime(&ms, jt_ev_[2 * q], jt_ev_[2 * q + 1]);
-            js += ms;
-        }
-        timing_.jline_ms = js;
-        timing_.jline_launches = nrec;
-        jline_timing_ = false;
-    }
+    if (ktime_) kt_harvest();
     return 0;
 }
 
@@ -1061,6 +1108,7 @@ int Engine::msolve(const SystemSpec &g, const double *a, const double *b, double
     s.a = const_cast<double *>(a);
     s.b = const_cast<double *>(b);
     s.x = var;
+    if (!aligned16(s)) return fail("device arrays must start on 16-byte boundaries (cudaMalloc gives 256)", -14);
     std::vector<SystemSpec> one{s};
     int rc = setup_batch(one, opt);
     if (rc) return rc;

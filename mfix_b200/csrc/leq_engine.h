@@ -64,12 +64,27 @@ struct SolveOptions {
     int force_lanes = 0;         // > 0: lanes per J-line for every system (experiments)
 };
 
+// Kernel classes timed one by one with option time_kernels.
+enum KernelClass : int {
+    KC_JLINE = 0,     // LINE preconditioner half-sweep (J-line solves)
+    KC_P_UPDATE,      // P = R + beta (P - omega V)
+    KC_MATVEC_ALPHA,  // V = A Phat, alpha
+    KC_S_UPDATE,      // S = R - alpha V, Snorm
+    KC_MATVEC_OMEGA,  // T = A Shat, omega
+    KC_XR_UPDATE,     // X, R, Rnorm, rho
+    KC_OUTER,         // mixed form: FP64 reliable update
+    KC_OTHER,         // copies, DIAG, sequential line sweeps
+    KC_COUNT
+};
+
 // Device-side timing of the last solve (CUDA events on the engine's stream).
 struct SolveTiming {
     float device_ms = 0.f;    // setup + iterations, inputs already on the device
     float jline_ms = 0.f;     // sum over J-line launches (time_kernels only)
     int jline_launches = 0;
     long long kernel_launches = 0;  // kernels of this library launched by the solve
+    float class_ms[KC_COUNT] = {};  // time_kernels only: summed launch durations per class
+    int class_launches[KC_COUNT] = {};
 };
 
 // Host table -> device copy; the device array is reallocated (with headroom)
@@ -97,6 +112,7 @@ struct LiveSystem {
     bool scaled = false;      // A/B unit-scaled already: the setup starts after the scaling
     const double *x0 = nullptr;  // non-null: x = x0 before the setup (FP64 re-solve of a mixed attempt)
     cudaEvent_t after = nullptr; // non-null: the engine's stream waits for it before touching the system
+    char *x0_slot = nullptr;     // mixed form: where the initial guess is kept (default: after the FP64 region)
 };
 
 struct LiveDone {
@@ -155,13 +171,15 @@ public:
 
 private:
     int run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &opt, std::vector<SolveResult> &out);
+    int run_batch_live(const std::vector<SystemSpec> &specs, const SolveOptions &opt, std::vector<SolveResult> &out);
+    std::vector<double *> x0_;  // per system of the last batch: the mixed form's copy of the initial guess
     int launch_setup(const SolveOptions &opt, bool scale);
     int launch_body(const SolveOptions &opt);
     int setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions &opt);
     int plan_msolve(const SolveOptions &opt, int src, int dst, int gate, int elem);
     int run_msolve_plan(int which, int elem);
     int bind_lists();
-    int configure_lines(int elem);
+    int configure_lines(int elem, int only_L = 0);
     void shape_for(int L, int elem, int forced, int *G, int *c);
     int autotune_lines(const SolveOptions &opt, int elem);
     void save_tune_cache();
@@ -223,10 +241,15 @@ private:
     unsigned int *d_dot_counter_ = nullptr;
     double *d_dot_out_ = nullptr;
     size_t sys_cap_ = 0, st_cap_ = 0, tiles_cap_ = 0, prefix_cap_ = 0, part_cap_ = 0, allprefix_cap_ = 0;
-    bool jline_timing_ = false;
-    static constexpr int JT_EVENTS = 2048;
-    cudaEvent_t jt_ev_[2 * JT_EVENTS] = {};
-    int jline_count_ = 0;
+    // time_kernels: an event pair around every launch of the iteration body
+    bool ktime_ = false;
+    static constexpr int KT_MAX = 1 << 16;
+    std::vector<cudaEvent_t> kt_ev_;  // 2 per timed launch, created on first use
+    std::vector<int> kt_class_;
+    int kt_count_ = 0;
+    void kt_begin();
+    void kt_end(int kclass);
+    void kt_harvest();
     long long launches_ = 0;
     SolveTiming timing_;
 
@@ -238,6 +261,7 @@ private:
     std::vector<long long> slot_join_snap_, slot_join_body_;
     int live_used_ = 0;
     bool live_dirty_ = false;
+    bool live_tune_ = false;  // autotune new line lengths at the next commit
     cudaGraphExec_t live_exec_ = nullptr;
     long long live_per_body_ = 0;
     long long snap_count_ = 0, body_total_ = 0, collected_upto_ = -1, commits_ = 0;

@@ -1256,13 +1256,16 @@ struct LineJob {
 };
 
 // The next work item at or after `item` whose system takes part in the wave.
+// pair: the two-row instance, which takes systems with an even JMAX2 only (the
+// one-row instance takes every system).
 __device__ __forceinline__ bool next_line_job(const BatchView &b, const WaveArgs &w, int item, int step, int total,
-                                              int lane, LineJob &j)
+                                              int lane, bool pair, LineJob &j)
 {
     for (; item < total; item += step) {
         const int sidx = (w.kind == 0) ? find_sys(b.line_prefix, b.nsys, item) : 0;
         if (!gate_ok(b.st[sidx], w.gate)) continue;
         const SysDev &d = b.sys[sidx];
+        if (pair && (d.jmax2 & 1)) continue;
         j.item = item;
         j.sidx = sidx;
         j.G = d.lane_group;
@@ -1398,8 +1401,8 @@ __global__ void k_line_factor(BatchView b, const int *all_line_prefix)
 // from a zero start, which yields the chunk's affine map (value at its end as a
 // function of the value entering it), a warp scan that composes the maps, and a
 // second pass from the entering value.  No division remains in the sweep.
-template <typename T>
-__global__ void __launch_bounds__(128) k_jline(BatchView b, WaveArgs w, int cmax)
+template <typename T, bool PAIR>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView b, WaveArgs w, int cmax)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nwarps = blockDim.x >> 5;
@@ -1411,7 +1414,7 @@ __global__ void __launch_bounds__(128) k_jline(BatchView b, WaveArgs w, int cmax
     const int total = (w.kind == 0) ? b.line_prefix[b.nsys] : w.count;
     const int step = gridDim.x * nwarps;
     LineJob j;
-    for (int item = blockIdx.x * nwarps + warp; next_line_job(b, w, item, step, total, lane, j);
+    for (int item = blockIdx.x * nwarps + warp; next_line_job(b, w, item, step, total, lane, PAIR, j);
          item = j.item + step) {
         const SysDev &d = b.sys[j.sidx];
         SysState &st = b.st[j.sidx];
@@ -1425,51 +1428,121 @@ __global__ void __launch_bounds__(128) k_jline(BatchView b, WaveArgs w, int cmax
         const T *gr_ = reinterpret_cast<const T *>(d.fac[1]) + x.base;
         const T *gq_ = reinterpret_cast<const T *>(d.fac[2]) + x.base;
 
-        // ---- load (coalesced over the line): right-hand side and factors, U rows at a time
-        constexpr int U = sizeof(T) == 8 ? 2 : 4;
-        for (int r0 = gl; r0 < G * c; r0 += U * G) {
-            T rhs[U], am1[U], ap1[U], am3[U], ap3[U], nim[U], nip[U], nkm[U], nkp[U], lv[U], rv[U], qv[U];
+        // ---- load (coalesced over the line): right-hand side and factors.  With an
+        // even JMAX2 every line starts on an even cell, so lanes read two rows per
+        // access; otherwise U single rows at a time.
+        if constexpr (PAIR) {  // L is even
+            constexpr int U2 = 1;  // one row pair per lane and pass: FP32 fits 80 registers
+            using V2 = vec2_t<T>;
+            const int span = G * c;
+            const T *rhs_l = x.rhs + x.base, *am1_l = x.a + 2 * x.n + x.base, *ap1_l = x.a + 4 * x.n + x.base;
+            const T *am3_l = x.a + x.base, *ap3_l = x.a + 6 * x.n + x.base;
+            for (int r0 = 2 * gl; r0 < span; r0 += 2 * U2 * G) {
+                V2 rhs[U2], am1[U2], ap1[U2], am3[U2], ap3[U2], nim[U2], nip[U2], nkm[U2], nkp[U2], lv[U2], rv[U2],
+                    qv[U2];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int r = r0 + u * G;
-                if (fast && r < L) {
-                    const int64_t p = x.base + r;
-                    rhs[u] = x.rhs[p];
-                    am1[u] = x.a[2 * x.n + p];
-                    ap1[u] = x.a[4 * x.n + p];
-                    nim[u] = x.nb_im[r];
-                    nip[u] = x.nb_ip[r];
-                    if (x.do_k) {
-                        am3[u] = x.a[0 * x.n + p];
-                        ap3[u] = x.a[6 * x.n + p];
-                        nkm[u] = x.nb_km[r];
-                        nkp[u] = x.nb_kp[r];
+                for (int u = 0; u < U2; ++u) {
+                    const int r = r0 + u * 2 * G;
+                    if (fast && r < L) {  // r even and L even: rows r and r+1 both on the line
+                        rhs[u] = ld2(rhs_l + r);
+                        am1[u] = ld2(am1_l + r);
+                        ap1[u] = ld2(ap1_l + r);
+                        nim[u] = ld2(x.nb_im + r);
+                        nip[u] = ld2(x.nb_ip + r);
+                        if (x.do_k) {
+                            am3[u] = ld2(am3_l + r);
+                            ap3[u] = ld2(ap3_l + r);
+                            nkm[u] = ld2(x.nb_km + r);
+                            nkp[u] = ld2(x.nb_kp + r);
+                        }
+                        lv[u] = ld2(gl_ + r);
+                        rv[u] = ld2(gr_ + r);
+                        qv[u] = ld2(gq_ + r);
                     }
-                    lv[u] = gl_[r];
-                    rv[u] = gr_[r];
-                    qv[u] = gq_[r];
+                }
+#pragma unroll
+                for (int u = 0; u < U2; ++u) {
+                    const int r = r0 + u * 2 * G;
+                    if (r < span) {
+                        T f0 = T(0), f1 = T(0), l0 = T(0), l1 = T(0), s0 = T(0), s1 = T(0), q0 = T(0), q1 = T(0);
+                        if (fast && r < L) {
+                            f0 = rhs[u].x - am1[u].x * nim[u].x;
+                            f1 = rhs[u].y - am1[u].y * nim[u].y;
+                            f0 = f0 - ap1[u].x * nip[u].x;
+                            f1 = f1 - ap1[u].y * nip[u].y;
+                            if (x.do_k) {
+                                f0 = f0 - am3[u].x * nkm[u].x;
+                                f1 = f1 - am3[u].y * nkm[u].y;
+                                f0 = f0 - ap3[u].x * nkp[u].x;
+                                f1 = f1 - ap3[u].y * nkp[u].y;
+                            }
+                            l0 = lv[u].x;
+                            l1 = lv[u].y;
+                            s0 = rv[u].x;
+                            s1 = rv[u].y;
+                            q0 = qv[u].x;
+                            q1 = qv[u].y;
+                        }
+                        f[r] = f0;
+                        fl[r] = l0;
+                        fr[r] = s0;
+                        fq[r] = q0;
+                        if (r + 1 < span) {  // an odd span (one lane per line) ends on an even row
+                            f[r + 1] = f1;
+                            fl[r + 1] = l1;
+                            fr[r + 1] = s1;
+                            fq[r + 1] = q1;
+                        }
+                    }
                 }
             }
+        } else {
+            constexpr int U = 2;
+            const T *rhs_l = x.rhs + x.base, *am1_l = x.a + 2 * x.n + x.base, *ap1_l = x.a + 4 * x.n + x.base;
+            const T *am3_l = x.a + x.base, *ap3_l = x.a + 6 * x.n + x.base;
+            for (int r0 = gl; r0 < G * c; r0 += U * G) {
+                T rhs[U], am1[U], ap1[U], am3[U], ap3[U], nim[U], nip[U], nkm[U], nkp[U], lv[U], rv[U], qv[U];
 #pragma unroll
-            for (int u = 0; u < U; ++u) {
-                const int r = r0 + u * G;
-                if (r < G * c) {
-                    T fv = T(0), l_ = T(0), r_ = T(0), q_ = T(0);
+                for (int u = 0; u < U; ++u) {
+                    const int r = r0 + u * G;
                     if (fast && r < L) {
-                        fv = rhs[u] - am1[u] * nim[u];
-                        fv = fv - ap1[u] * nip[u];
+                        rhs[u] = rhs_l[r];
+                        am1[u] = am1_l[r];
+                        ap1[u] = ap1_l[r];
+                        nim[u] = x.nb_im[r];
+                        nip[u] = x.nb_ip[r];
                         if (x.do_k) {
-                            fv = fv - am3[u] * nkm[u];
-                            fv = fv - ap3[u] * nkp[u];
+                            am3[u] = am3_l[r];
+                            ap3[u] = ap3_l[r];
+                            nkm[u] = x.nb_km[r];
+                            nkp[u] = x.nb_kp[r];
                         }
-                        l_ = lv[u];
-                        r_ = rv[u];
-                        q_ = qv[u];
+                        lv[u] = gl_[r];
+                        rv[u] = gr_[r];
+                        qv[u] = gq_[r];
                     }
-                    f[r] = fv;
-                    fl[r] = l_;
-                    fr[r] = r_;
-                    fq[r] = q_;
+                }
+#pragma unroll
+                for (int u = 0; u < U; ++u) {
+                    const int r = r0 + u * G;
+                    if (r < G * c) {
+                        T fv = T(0), l_ = T(0), r_ = T(0), q_ = T(0);
+                        if (fast && r < L) {
+                            fv = rhs[u] - am1[u] * nim[u];
+                            fv = fv - ap1[u] * nip[u];
+                            if (x.do_k) {
+                                fv = fv - am3[u] * nkm[u];
+                                fv = fv - ap3[u] * nkp[u];
+                            }
+                            l_ = lv[u];
+                            r_ = rv[u];
+                            q_ = qv[u];
+                        }
+                        f[r] = fv;
+                        fl[r] = l_;
+                        fr[r] = r_;
+                        fq[r] = q_;
+                    }
                 }
             }
         }
@@ -1775,14 +1848,19 @@ int prepare_line_kernel(int cmax, int *warps)
     {
         std::lock_guard<std::mutex> lk(mu);
         if (smem > granted) {
-            if (cudaFuncSetAttribute(k_jline<T>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess)
+            if (cudaFuncSetAttribute(k_jline<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+                    cudaSuccess ||
+                cudaFuncSetAttribute(k_jline<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+                    cudaSuccess)
                 return 0;
             granted = smem;
         }
     }
-    int nb = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_jline<T>, wpb * 32, smem) != cudaSuccess) return 0;
-    return nb;
+    int nb = 0, nb1 = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_jline<T, true>, wpb * 32, smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb1, k_jline<T, false>, wpb * 32, smem) != cudaSuccess)
+        return 0;
+    return std::min(nb, nb1);
 }
 
 template <typename K>
@@ -1822,7 +1900,12 @@ template <typename T>
 cudaError_t launch_jline(const BatchView &b, const LaunchCfg &c, const WaveArgs &w)
 {
     const int smem = c.line_warps * kernel_smem_line_bytes(c.line_cmax, (int)sizeof(T));
-    k_jline<T><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax);
+    // two-row loads for lines of even length, one-row loads for the others
+    // one launch per wave: two-row loads when every line has even length
+    if (c.rows_single)
+        k_jline<T, false><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax);
+    else
+        k_jline<T, true><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax);
     CHECK_LAUNCH();
 }
 template <typename T>

@@ -145,9 +145,10 @@ int Engine::live_add(const LiveSystem &ls)
     d.b64 = sp.b;
     d.x64[0] = sp.x;
     const int64_t lines = (int64_t)sp.imax2 * sp.kmax2;
-    char *x0 = mixed ? ls.work + std::max(vec_region_bytes(sp.n, lines, PREC_FP64),
-                                          vec_region_bytes(sp.n, lines, PREC_MIXED))
-                     : nullptr;
+    char *x0 = !mixed      ? nullptr
+               : ls.x0_slot ? ls.x0_slot
+                            : ls.work + std::max(vec_region_bytes(sp.n, lines, PREC_FP64),
+                                                 vec_region_bytes(sp.n, lines, PREC_MIXED));
     carve_work(d, ls.work, lines, prec, x0);
 
     SysState st{};
@@ -255,6 +256,11 @@ int Engine::live_commit()
     int rc = configure_lines(mixed ? 4 : 8);
     if (rc) return rc;
 
+    // setup of the systems that joined (gated: a no-op for the others)
+    if (any_fresh && (rc = launch_setup(live_opt_, true))) return rc;
+    // new line lengths: lanes per line picked by measurement (one-shot batches)
+    if (any_fresh && live_tune_ && (rc = autotune_lines(live_opt_, mixed ? 4 : 8))) return rc;
+
     // the iteration body for this membership
     if (live_exec_) cudaGraphExecDestroy(live_exec_);  // freed once its launches finish
     live_exec_ = nullptr;
@@ -276,8 +282,6 @@ int Engine::live_commit()
         if (ce != cudaSuccess) return fail(std::string("graph instantiate: ") + cudaGetErrorString(ce), -13);
     }
 
-    // setup of the systems that joined (gated: a no-op for the others)
-    if (any_fresh && (rc = launch_setup(live_opt_, true))) return rc;
     for (int s = 0; s < cap; ++s)
         if (slot_fresh_[s]) {
             slot_fresh_[s] = 0;
@@ -335,6 +339,76 @@ int Engine::live_collect(std::vector<LiveDone> &done, bool latest)
         }
     }
     collected_upto_ = q;
+    return 0;
+}
+
+}  // namespace mfixgpu
+
+namespace mfixgpu {
+
+// A one-shot batch of several systems run as a live batch: all join at once,
+// each leaves when it finishes, so the kernels stop visiting finished systems.
+int Engine::run_batch_live(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
+                           std::vector<SolveResult> &out)
+{
+    const int ns = (int)specs.size();
+    out.assign(ns, SolveResult{});
+    size_t bytes = 4096;
+    for (const auto &s : specs) bytes += work_bytes(s.n, (int64_t)s.imax2 * s.kmax2, opt.precision) + 512;
+    cudaError_t e = arena_.reserve(bytes);
+    if (e != cudaSuccess) return fail(std::string("device memory for the batch: ") + cudaGetErrorString(e), -11);
+    arena_.reset();
+    int rc = live_open(ns, opt);
+    if (rc) return rc;
+    launches_ = 0;
+    timing_ = SolveTiming{};
+    x0_.assign(ns, nullptr);
+    int max_itmax = 0;
+    for (int q = 0; q < ns; ++q) {
+        const SystemSpec &sp = specs[q];
+        const int64_t lines = (int64_t)sp.imax2 * sp.kmax2;
+        LiveSystem ls;
+        ls.dev = sp;
+        ls.work = (char *)arena_.take(work_bytes(sp.n, lines, opt.precision));
+        ls.scaled = opt.skip_scale;
+        if (opt.precision == PREC_MIXED) ls.x0_slot = ls.work + vec_region_bytes(sp.n, lines, PREC_MIXED);
+        const int slot = live_add(ls);
+        if (slot != q) return slot < 0 ? slot : fail("internal: live slot order", -13);
+        x0_[q] = h_sys_[q].x64[1];
+        max_itmax = std::max(max_itmax, sp.itmax);
+    }
+    CK(cudaEventRecord(ev_t0_, stream_));
+    // the first commit runs the setup; new line lengths are tuned right after it
+    live_tune_ = opt.autotune && opt.force_lanes <= 0 && opt.pc == PC_LINE;
+    const int K = std::max(1, opt.check_every);
+    int remaining = ns;
+    std::vector<LiveDone> done;
+    while (remaining > 0) {
+        if ((rc = live_step(K))) {
+            live_tune_ = false;
+            return rc;
+        }
+        done.clear();
+        if ((rc = live_collect(done, false))) return rc;
+        for (const LiveDone &d : done) {
+            out[d.slot] = d.res;
+            live_remove(d.slot);
+            --remaining;
+        }
+        if (body_total_ > (long long)max_itmax + 2 + 4LL * K + 8) break;  // every system reports by itmax + 2
+    }
+    live_tune_ = false;
+    CK(cudaEventRecord(ev_t1_, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    cudaEventElapsedTime(&timing_.device_ms, ev_t0_, ev_t1_);
+    timing_.kernel_launches = launches_;
+    if (remaining > 0)
+        for (int q = 0; q < ns; ++q)
+            if (slot_used_[q] && !slot_reported_[q]) {
+                out[q] = SolveResult{};
+                out[q].ier = -15;
+                out[q].exit_kind = EX_ERROR;
+            }
     return 0;
 }
 

@@ -77,6 +77,8 @@ REQ_ON_DEVICE = 4
 
 
 def _declare(L: C.CDLL) -> None:
+    L.mfixgpu_last_kernel_times.argtypes = [C.POINTER(C.c_double), C.POINTER(C.c_longlong), C.c_int]
+    L.mfixgpu_last_kernel_times.restype = C.c_int
     L.mfixgpu_server_create.argtypes = [C.POINTER(ServerConfigC), C.POINTER(C.c_void_p)]
     L.mfixgpu_server_create.restype = C.c_int
     L.mfixgpu_server_submit.argtypes = [C.c_void_p, C.POINTER(SystemC), C.c_int]
@@ -169,6 +171,18 @@ def last_stats() -> dict:
     s = Stats()
     lib().mfixgpu_last_stats(C.byref(s))
     return {k: getattr(s, k) for k, _ in Stats._fields_ if not k.startswith("pad")}
+
+
+KERNEL_CLASSES = ("jline", "p_update", "matvec_alpha", "s_update", "matvec_omega", "xr_update", "outer_step",
+                  "other_sweep")
+
+
+def last_kernel_times() -> dict:
+    """Per kernel class of the last solve (option time_kernels): (ms, launches)."""
+    ms = (C.c_double * 16)()
+    n = (C.c_longlong * 16)()
+    k = lib().mfixgpu_last_kernel_times(ms, n, 16)
+    return {KERNEL_CLASSES[q] if q < len(KERNEL_CLASSES) else str(q): (ms[q], n[q]) for q in range(k)}
 
 
 def last_error() -> str:
