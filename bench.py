@@ -47,7 +47,7 @@ WORKLOADS = {
     "batch_512": dict(kind="batch", count=512, seed=0, itmax=500, tol=1e-8),
     # Poisson request stream: sizes log-uniform per axis on [24, 160], 20% pressure-like,
     # TOL from {1e-6, 1e-8}, 150 GB HBM admission budget
-    "serve_poisson": dict(kind="serve", rate=2000.0, seconds=20.0, pool=64, seed=0, budget=150e9),
+    "serve_poisson": dict(kind="serve", rate=2000.0, seconds=15.0, pool=64, seed=0, budget=150e9),
 }
 DEFAULT_WORKLOAD = "conv_diff_256"
 # Iterations the oracle (the reference's FP64 LEQ_BICGS restated in C) takes to
@@ -738,9 +738,68 @@ def _serve_run(leq, pool, precision, rate, seconds, seed, budget, check_every=2,
     }
 
 
+def _serve_closed(leq, pool, precision, inflight, seconds, seed, budget, check_every=2, max_systems=512):
+    """Closed loop: `inflight` requests outstanding, each completion replaced by a
+    new request, for `seconds`; the completion rate is the server's capacity for
+    the request mix (completions follow the submission mix in steady state)."""
+    rng = np.random.default_rng(seed)
+    xs = [np.empty(p.n) for p in pool]  # outputs (never read)
+    srv = leq.Server(precision=precision, max_systems=max_systems, check_every=check_every, hbm_budget=budget)
+    which = {}
+
+    def submit():
+        q = int(rng.integers(0, len(pool)))
+        t = srv.submit(_Req(pool[q], xs[q], float(1e-6 if rng.random() < 0.5 else 1e-8)), zero_guess=True)
+        if t < 0:
+            raise RuntimeError(f"submit failed: {t} {leq.last_error()}")
+        which[t] = q
+        return t
+
+    for _ in range(min(16, inflight)):  # warm the live batches
+        t = submit()
+        srv.wait(t, 600)
+        which.pop(t)
+    c0 = srv.counters()
+    t_end = c0["seconds"] + seconds
+    warm_until = c0["seconds"] + 0.2 * seconds
+    for _ in range(inflight):
+        submit()
+    done = []
+    stall = 0
+    while True:
+        got = srv.wait_any(5.0)
+        if got is None:
+            stall += 1
+            if stall > 120:  # ten minutes without a completion
+                raise RuntimeError("serving run made no progress")
+            continue
+        stall = 0
+        t, r = got
+        done.append((which.pop(t), r))
+        if r["t_done"] < t_end:
+            submit()
+        elif not which:
+            break
+    c1 = srv.counters()
+    srv.close()
+    win = [(q, r) for q, r in done if warm_until <= r["t_done"] < t_end]
+    span = t_end - warm_until
+    alg = sum(_alg_bytes(pool[q].n, precision, r["mixed_iterations"] if r["fp64_fallback"] else r["iterations"],
+                         r["outer_steps"], r["iterations"] if r["fp64_fallback"] else 0) for q, r in win)
+    lat = np.array([r["t_done"] - r["t_submit"] for _, r in win]) * 1e3
+    return {"precision": "mixed" if precision == 1 else "fp64", "inflight": inflight, "seconds": seconds,
+            "window_s": span, "completed_in_window": len(win), "capacity": len(win) / span,
+            "alg_gbs": alg / span / 1e9, "latency_ms_at_capacity": {"p50": float(np.percentile(lat, 50)),
+                                                                    "p99": float(np.percentile(lat, 99))},
+            "fp64_handovers": int(c1["fp64_fallbacks"] - c0["fp64_fallbacks"]),
+            "nonzero_ier": sum(1 for _, r in done if r["ier"] != 0)}
+
+
 def run_serve_bench(args) -> None:
-    """Poisson request stream against the server, mixed form vs FP64 form, at the
-    offered rate and below saturation; latency from submit to result on the host."""
+    """The request server on a stream of mixed-size requests, mixed form vs FP64
+    form: capacity from closed-loop runs, p50/p99 latency from Poisson streams at
+    50% and 80% of the FP64 capacity (the same offered load for both forms), and
+    the workload's own offered rate (saturating) with served rate and backlog."""
     import torch
 
     from mfix_b200 import leq
@@ -763,49 +822,54 @@ def run_serve_bench(args) -> None:
         p.a, p.b = a, b
     peak, peak_kind = measured_peak_hbm()
     sampler = ClockSampler(0)
-    runs = []
     with sampler:
-        sat_m = _serve_run(leq, pool, 1, rate, seconds, 1, w["budget"])
-        sat_f = _serve_run(leq, pool, 0, rate, seconds, 1, w["budget"])
-        sub_rate = 0.5 * sat_m["served_rate"]
-        sub_m = _serve_run(leq, pool, 1, sub_rate, seconds, 2, w["budget"])
-        sub_f = _serve_run(leq, pool, 0, sub_rate, seconds, 2, w["budget"])
-    runs = [sat_m, sat_f, sub_m, sub_f]
-    # verify the requests that had private outputs: FP64 true relative residual <= TOL
+        cap_m = _serve_closed(leq, pool, 1, 256, seconds, 11, w["budget"])
+        cap_f = _serve_closed(leq, pool, 0, 256, seconds, 11, w["budget"])
+        loads = []
+        for frac in (0.5, 0.8):
+            lam = frac * cap_f["capacity"]
+            loads.append((frac, _serve_run(leq, pool, 1, lam, seconds, 2, w["budget"]),
+                          _serve_run(leq, pool, 0, lam, seconds, 2, w["budget"])))
+        sat = _serve_run(leq, pool, 1, rate, min(seconds, 10.0), 1, w["budget"])
     import oracle as O
 
-    worst = 0.0
-    checked = 0
-    for r in runs:
-        for i, (q, x) in list(r["_private"].items())[:6]:
-            res = r["_results"].get(i)
-            if res is None or res["ier"] != 0:
-                continue
-            sc = pool[q].copy()
-            O.scale(sc)
-            rel = O.true_resid(sc, x) / O.true_resid(sc, np.zeros(sc.n))
-            worst = max(worst, rel / float(r["_tols"][i]))
-            checked += 1
-    for r in runs:
-        for k in ("_private", "_results", "_tols"):
-            r.pop(k)
+    worst, checked = 0.0, 0
+    for _, rm, rf in loads:
+        for r in (rm, rf):
+            for i, (q, x) in list(r["_private"].items())[:6]:
+                res = r["_results"].get(i)
+                if res is None or res["ier"] != 0:
+                    continue
+                sc = pool[q].copy()
+                O.scale(sc)
+                rel = O.true_resid(sc, x) / O.true_resid(sc, np.zeros(sc.n))
+                worst = max(worst, rel / float(r["_tols"][i]))
+                checked += 1
+    strip = lambda r: {k: v for k, v in r.items() if not k.startswith("_")}
+    lat = {f"{int(100 * frac)}pct_of_fp64_capacity": {"offered_rate": rm["offered_rate"], "mixed": strip(rm),
+                                                       "fp64": strip(rf)} for frac, rm, rf in loads}
+    half = loads[0]
     line = {
-        "metric": "solves/s & p50/p99 latency", "value": sat_m["served_rate"], "unit": "solves/s", "n_gpus": 1,
+        "metric": "solves/s & p50/p99 latency", "value": cap_m["capacity"], "unit": "solves/s", "n_gpus": 1,
         "steps": 1, "warmup": 1, "ms_per_step": seconds * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "fp32-inner/fp64-refinement", "data": "synthetic",
-        "config": {"workload": args.workload, "offered_rate": rate, "seconds": seconds, "pool_systems": len(pool),
+        "config": {"workload": args.workload, "seconds_per_run": seconds, "pool_systems": len(pool),
                    "pool_cells_mean": float(np.mean([p.n for p in pool])),
                    "sizes": "per axis log-uniform on [24, 160]", "pressure_share": 0.2, "tol": [1e-6, 1e-8],
                    "hbm_budget_gb": w["budget"] / 1e9, "max_systems_per_batch": 512, "check_every": 2,
+                   "capacity": "closed loop, 256 requests in flight, completions after the first 20% of the run",
                    "inputs": "pinned host A_M/B_M copied in per request, VAR copied out; zero initial guess"},
-        "roofline": {"kernel": "served solves (algorithmic bytes of requests completed in the window)",
-                     "bound": "hbm", "achieved": sat_m["alg_gbs"], "peak": peak, "unit": "GB/s",
-                     "frac": sat_m["alg_gbs"] / peak, "peak_kind": peak_kind, "traffic": None},
-        "e2e": {"value": sat_m["served_rate"], "unit": "solves/s", "note": "host arrays in and out per request"},
-        "gpu_launches": sat_m["gpu_launches"],
+        "roofline": {"kernel": "served solves at capacity (algorithmic bytes of completed requests)", "bound": "hbm",
+                     "achieved": cap_m["alg_gbs"], "peak": peak, "unit": "GB/s", "frac": cap_m["alg_gbs"] / peak,
+                     "peak_kind": peak_kind, "traffic": None},
+        "e2e": {"value": cap_m["capacity"], "unit": "solves/s", "note": "host arrays in and out per request"},
+        "gpu_launches": half[1]["gpu_launches"],
         "clocks": sampler.summary(),
-        "runs": runs,
-        "mixed_vs_fp64_saturated": sat_m["served_rate"] / max(sat_f["served_rate"], 1e-9),
+        "capacity": {"mixed": cap_m, "fp64": cap_f, "mixed_vs_fp64": cap_m["capacity"] / cap_f["capacity"]},
+        "latency": lat,
+        "p50_p99_ms_at_half_fp64_capacity": {"mixed": [half[1]["latency_ms"]["p50"], half[1]["latency_ms"]["p99"]],
+                                             "fp64": [half[2]["latency_ms"]["p50"], half[2]["latency_ms"]["p99"]]},
+        "offered_stream": strip(sat),
         "verified_requests": checked, "worst_true_resid_over_tol": worst,
         "generation_s": t_gen,
     }

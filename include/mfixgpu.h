@@ -107,6 +107,9 @@ const char *mfixgpu_last_error(void);
  *   "mixed_growth"   mixed form: hand over to FP64 when a true residual exceeds this multiple of
  *                    the best one seen (default 10)
  *   "mixed_stalls"   mixed form: hand over after this many reliable updates without a 10% gain (default 6)
+ *   "mixed_min_margin" mixed form: a system whose smallest diagonal-dominance margin,
+ *                    min over rows of |sum of A's row| / |A(0)|, is below this is solved by the
+ *                    FP64 drop-in from the start (default 1e-4; 0 never)
  *   "write_back_ab"  1 (default) copy the scaled A_M/B_M slices back
  *   "rtilde_seed"    seed of the Rtilde random stream (replaces RANDOM_NUMBER, model/leq_bicgs.f:298)
  *   "inner_tol"      mixed form: drop of the FP32 residual between FP64 reliable updates (default 1e-2)

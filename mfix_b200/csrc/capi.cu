@@ -33,6 +33,7 @@ struct Options {
     double inner_tol = 1e-2;
     double mixed_growth = 10.0;
     int mixed_stalls = 6;
+    double mixed_min_margin = 1e-4;
     int check_every = 4;
     int use_graph = 1;
     int time_kernels = 0;
@@ -107,6 +108,7 @@ SolveOptions make_opts(const Options &o, int pc, const char sweep4[4])
     so.inner_tol = o.inner_tol;
     so.mixed_growth = o.mixed_growth;
     so.mixed_stalls = o.mixed_stalls;
+    so.mixed_min_margin = o.mixed_min_margin;
     so.check_every = o.check_every;
     so.use_graph = o.use_graph != 0;
     so.time_kernels = o.time_kernels != 0;
@@ -314,6 +316,9 @@ int mfixgpu_set_option(const char *name, double value)
     } else if (k == "mixed_growth") {
         if (!(value > 1)) return MFIXGPU_ERR_ARGS;
         g.opt.mixed_growth = value;
+    } else if (k == "mixed_min_margin") {
+        if (!(value >= 0)) return MFIXGPU_ERR_ARGS;
+        g.opt.mixed_min_margin = value;
     } else if (k == "mixed_stalls") {
         if (value < 1) return MFIXGPU_ERR_ARGS;
         g.opt.mixed_stalls = (int)value;
@@ -347,6 +352,7 @@ double mfixgpu_get_option(const char *name)
     if (k == "inner_tol") return g.opt.inner_tol;
     if (k == "mixed_growth") return g.opt.mixed_growth;
     if (k == "mixed_stalls") return g.opt.mixed_stalls;
+    if (k == "mixed_min_margin") return g.opt.mixed_min_margin;
     if (k == "check_every") return g.opt.check_every;
     if (k == "use_graph") return g.opt.use_graph;
     if (k == "time_kernels") return g.opt.time_kernels;

@@ -82,6 +82,7 @@ struct SysDev {
     double *b64;         // B_M(:,M)
     double *x64[2];      // VAR; x64[1] keeps the initial guess in the mixed form (FP64 re-solve)
     float *a32;          // FP32 copy of the scaled diagonals (mixed form)
+    float *defect;       // mixed form: row sums of the scaled A, formed in FP64 (A x = sum a_nb (x_nb - x) + defect x)
     void *vec[NVEC];     // work vectors, double or float by precision
     void *fac[3];        // J-line LU factors per cell (l, 1/u, c/u), double or float by precision
     int *line_flag;      // per J-line (i-1)+(k-1)*imax2: 1 where DGTSV interchanges rows or meets a zero pivot
@@ -99,6 +100,8 @@ struct SysState {
     double maxr;          // mixed form: largest recursive residual since the last reliable update
     double best;          // mixed form: smallest true residual seen at a reliable update
     double growth_limit;  // mixed form: hand over when a true residual exceeds growth_limit * best
+    double min_margin;    // mixed form: systems whose diagonal-dominance margin is below this go to FP64
+    unsigned int margin_bits;  // mixed form: min over rows of |row sum| / |A(0)| (float bits, set in setup)
     int stall_limit;      // mixed form: hand over after this many updates without a 10% gain
     int itmax;
     int i;                // reference loop index of the next iteration (1-based)

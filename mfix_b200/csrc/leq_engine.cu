@@ -170,7 +170,7 @@ size_t vec_region_bytes(int64_t n, int64_t lines, int precision)
 {
     const size_t ew = precision == PREC_MIXED ? 4 : 8;
     size_t b = 0;
-    if (precision == PREC_MIXED) b += align_up(7 * (size_t)n * 4, 256);
+    if (precision == PREC_MIXED) b += align_up(7 * (size_t)n * 4, 256) + align_up((size_t)n * 4, 256);
     b += (NVEC + 3) * align_up((size_t)n * ew, 256) + align_up((size_t)lines * 4, 256);
     return b;
 }
@@ -200,9 +200,11 @@ void carve_work(SysDev &d, char *work, int64_t lines, int precision, char *x0)
         return p;
     };
     d.a32 = nullptr;
+    d.defect = nullptr;
     d.x64[1] = nullptr;
     if (precision == PREC_MIXED) {
         d.a32 = (float *)take(7 * n * 4);
+        d.defect = (float *)take(n * 4);
         d.x64[1] = (double *)x0;  // initial guess, kept for an FP64 re-solve
     }
     for (int v = 0; v < NVEC; ++v) d.vec[v] = take(n * ew);
@@ -266,6 +268,8 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         st.inner_tol = opt.inner_tol;
         st.growth_limit = opt.mixed_growth;
         st.stall_limit = opt.mixed_stalls;
+        st.min_margin = opt.mixed_min_margin;
+        st.margin_bits = 0x7f800000u;
         st.i = 1;
         st.iter = 1;
     }

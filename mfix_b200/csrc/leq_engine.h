@@ -56,6 +56,7 @@ struct SolveOptions {
     double inner_tol = 1e-2;     // mixed form: residual drop between reliable updates
     double mixed_growth = 10.0;  // mixed form: true-residual growth over the best that hands over to FP64
     int mixed_stalls = 6;        // mixed form: reliable updates without a 10% gain that hand over
+    double mixed_min_margin = 1e-4;  // mixed form: smaller diagonal-dominance margins go straight to FP64
     int check_every = 4;         // iterations between host checks of the state
     bool use_graph = true;       // capture the iteration body in a CUDA graph
     bool time_kernels = false;   // record events around every J-line launch (no graph replay)

@@ -265,9 +265,23 @@ __global__ void k_init_done(BatchView b)
     if (s >= b.nsys) return;
     SysState &st = b.st[s];
     if (!gate_ok(st, G_INIT)) return;
+    // a nearly singular operator (pressure correction) goes to the FP64 drop-in
+    // before any FP32 iteration: its FP32 Krylov process stagnates
+    if (st.mixed && __uint_as_float(st.margin_bits) < st.min_margin) {
+        st.exit_kind = EX_FALLBACK;
+        st.ier = -20;
+        st.status = ST_DONE;
+        return;
+    }
     st.phase = st.mixed ? PH_OUTER : PH_INNER;
 }
 
+// Mixed form's FP32 operator: the scaled diagonals rounded to FP32, and each
+// row's sum formed in FP64 first.  The FP32 matvec evaluates
+//   sum_nb a_nb (x_nb - x) + defect * x,
+// algebraically the same as the seven products, but exact to FP32 rounding in
+// the smooth (near-null) mode of nearly singular operators such as pressure
+// correction, where the seven products cancel to a millionth of their size.
 __global__ void k_to_f32(BatchView b)
 {
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
@@ -276,10 +290,23 @@ __global__ void k_to_f32(BatchView b)
         if (!gate_ok(b.st[tl.sys], G_INIT)) continue;
         const int64_t n = d.n;
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(n, c0 + TILE_CELLS);
+        float margin = __int_as_float(0x7f800000);  // +inf
         #pragma unroll 4
-        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x)
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+            double sum = 0.0;
 #pragma unroll
-            for (int q = 0; q < 7; ++q) d.a32[q * n + c] = (float)d.a64[q * n + c];
+            for (int q = 0; q < 7; ++q) {
+                const double v = d.a64[q * n + c];
+                d.a32[q * n + c] = (float)v;
+                if (d.do_k || (q != 0 && q != 6)) sum += v;
+            }
+            d.defect[c] = (float)sum;  // the row sum, exact to FP32 rounding however small
+            const double a0 = fabs(d.a64[3 * n + c]);
+            if (a0 > 0.0) margin = fminf(margin, (float)(fabs(sum) / a0));
+        }
+        // the system's smallest margin (order-free, so the same in any batch)
+        for (int o = 16; o > 0; o >>= 1) margin = fminf(margin, __shfl_xor_sync(0xffffffffu, margin, o));
+        if ((threadIdx.x & 31) == 0) atomicMin(&b.st[tl.sys].margin_bits, __float_as_uint(margin));
     }
 }
 
@@ -391,7 +418,7 @@ struct Row7 {
     T a[7], x[7];
 };
 
-template <typename T, typename TX>
+template <typename T, typename TX, bool DEFECT = false>
 __device__ __forceinline__ void load_row7(const SysDev &d, const T *__restrict__ A, const TX *__restrict__ X,
                                           int64_t c, Row7<T> &r)
 {
@@ -401,7 +428,10 @@ __device__ __forceinline__ void load_row7(const SysDev &d, const T *__restrict__
     r.x[0] = (T)X[c + o.jm];
     r.a[1] = A[2 * n + c];
     r.x[1] = (T)X[c + o.im];
-    r.a[2] = A[3 * n + c];
+    if constexpr (DEFECT)
+        r.a[2] = (T)d.defect[c];
+    else
+        r.a[2] = A[3 * n + c];
     r.x[2] = (T)X[c];
     r.a[3] = A[4 * n + c];
     r.x[3] = (T)X[c + o.ip];
@@ -418,9 +448,22 @@ __device__ __forceinline__ void load_row7(const SysDev &d, const T *__restrict__
     }
 }
 
-template <typename T>
+template <typename T, bool DEFECT = false>
 __device__ __forceinline__ T dot_row7(const Row7<T> &r, bool do_k)
 {
+    if constexpr (DEFECT) {  // a[2] holds the row sum
+        const T xc = r.x[2];
+        T v = r.a[0] * (r.x[0] - xc);
+        v = v + r.a[1] * (r.x[1] - xc);
+        v = v + r.a[2] * xc;
+        v = v + r.a[3] * (r.x[3] - xc);
+        v = v + r.a[4] * (r.x[4] - xc);
+        if (do_k) {
+            v = v + r.a[5] * (r.x[5] - xc);
+            v = v + r.a[6] * (r.x[6] - xc);
+        }
+        return v;
+    }
     T v = r.a[0] * r.x[0];
     v = v + r.a[1] * r.x[1];
     v = v + r.a[2] * r.x[2];
@@ -479,7 +522,7 @@ struct Pair7 {
     vec2_t<T> a[7], x[7];
 };
 
-template <typename T>
+template <typename T, bool DEFECT = false>
 __device__ __forceinline__ void load_pair7(const SysDev &d, const T *__restrict__ A, const T *__restrict__ X,
                                            int64_t c, Pair7<T> &r)
 {
@@ -494,7 +537,10 @@ __device__ __forceinline__ void load_pair7(const SysDev &d, const T *__restrict_
     r.x[0] = mk2<T>(xl, xc.x);
     r.a[1] = ld2(A + 2 * n + c);
     r.x[1] = ld2(X + c + im);
-    r.a[2] = ld2(A + 3 * n + c);
+    if constexpr (DEFECT)
+        r.a[2] = ld2(reinterpret_cast<const T *>(d.defect) + c);
+    else
+        r.a[2] = ld2(A + 3 * n + c);
     r.x[2] = xc;
     r.a[3] = ld2(A + 4 * n + c);
     r.x[3] = ld2(X + c + ip);
@@ -513,9 +559,29 @@ __device__ __forceinline__ void load_pair7(const SysDev &d, const T *__restrict_
 }
 
 // dot_row7 of both rows, in the same operand order
-template <typename T>
+template <typename T, bool DEFECT = false>
 __device__ __forceinline__ vec2_t<T> dot_pair7(const Pair7<T> &r, bool do_k)
 {
+    if constexpr (DEFECT) {  // a[2] holds the row sums
+        const T cx = r.x[2].x, cy = r.x[2].y;
+        T u = r.a[0].x * (r.x[0].x - cx);
+        T w = r.a[0].y * (r.x[0].y - cy);
+        u = u + r.a[1].x * (r.x[1].x - cx);
+        w = w + r.a[1].y * (r.x[1].y - cy);
+        u = u + r.a[2].x * cx;
+        w = w + r.a[2].y * cy;
+        u = u + r.a[3].x * (r.x[3].x - cx);
+        w = w + r.a[3].y * (r.x[3].y - cy);
+        u = u + r.a[4].x * (r.x[4].x - cx);
+        w = w + r.a[4].y * (r.x[4].y - cy);
+        if (do_k) {
+            u = u + r.a[5].x * (r.x[5].x - cx);
+            w = w + r.a[5].y * (r.x[5].y - cy);
+            u = u + r.a[6].x * (r.x[6].x - cx);
+            w = w + r.a[6].y * (r.x[6].y - cy);
+        }
+        return mk2<T>(u, w);
+    }
     T u = r.a[0].x * r.x[0].x;
     T w = r.a[0].y * r.x[0].y;
     u = u + r.a[1].x * r.x[1].x;
@@ -692,7 +758,7 @@ __global__ void __launch_bounds__(256) k_matvec_alpha(BatchView b, int src)
                 for (int u = 0; u < UP; ++u) {
                     const int q = base + u * blockDim.x;
                     if (q < np) {
-                        load_pair7<T>(d, a, x, c0 + 2 * q, rw[u]);
+                        load_pair7<T, MIXED>(d, a, x, c0 + 2 * q, rw[u]);
                         rtv[u] = ld2(rt + c0 + 2 * q);
                     }
                 }
@@ -700,7 +766,7 @@ __global__ void __launch_bounds__(256) k_matvec_alpha(BatchView b, int src)
                 for (int u = 0; u < UP; ++u) {
                     const int q = base + u * blockDim.x;
                     if (q < np) {
-                        const vec2_t<T> yv = dot_pair7<T>(rw[u], d.do_k);
+                        const vec2_t<T> yv = dot_pair7<T, MIXED>(rw[u], d.do_k);
                         st2(y + c0 + 2 * q, yv);
                         v[0] += (double)rtv[u].x * (double)yv.x;
                         v[0] += (double)rtv[u].y * (double)yv.y;
@@ -715,7 +781,7 @@ __global__ void __launch_bounds__(256) k_matvec_alpha(BatchView b, int src)
             for (int u = 0; u < U; ++u) {
                 const int c = base + u * blockDim.x;
                 if (c < cnt) {
-                    load_row7<T, T>(d, a, x, c0 + c, rw[u]);
+                    load_row7<T, T, MIXED>(d, a, x, c0 + c, rw[u]);
                     rtv[u] = rt[c0 + c];
                 }
             }
@@ -723,7 +789,7 @@ __global__ void __launch_bounds__(256) k_matvec_alpha(BatchView b, int src)
             for (int u = 0; u < U; ++u) {
                 const int c = base + u * blockDim.x;
                 if (c < cnt) {
-                    const T yv = dot_row7<T>(rw[u], d.do_k);
+                    const T yv = dot_row7<T, MIXED>(rw[u], d.do_k);
                     y[c0 + c] = yv;
                     v[0] += (double)rtv[u] * (double)yv;
                 }
@@ -828,7 +894,7 @@ __global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
                 for (int u = 0; u < UP; ++u) {
                     const int q = base + u * blockDim.x;
                     if (q < np) {
-                        load_pair7<T>(d, a, x, c0 + 2 * q, rw[u]);
+                        load_pair7<T, MIXED>(d, a, x, c0 + 2 * q, rw[u]);
                         sv[u] = ld2(s + c0 + 2 * q);
                     }
                 }
@@ -836,7 +902,7 @@ __global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
                 for (int u = 0; u < UP; ++u) {
                     const int q = base + u * blockDim.x;
                     if (q < np) {
-                        const vec2_t<T> yv = dot_pair7<T>(rw[u], d.do_k);
+                        const vec2_t<T> yv = dot_pair7<T, MIXED>(rw[u], d.do_k);
                         st2(y + c0 + 2 * q, yv);
                         v[0] += (double)yv.x * (double)sv[u].x;
                         v[1] += (double)yv.x * (double)yv.x;
@@ -853,7 +919,7 @@ __global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
             for (int u = 0; u < U; ++u) {
                 const int c = base + u * blockDim.x;
                 if (c < cnt) {
-                    load_row7<T, T>(d, a, x, c0 + c, rw[u]);
+                    load_row7<T, T, MIXED>(d, a, x, c0 + c, rw[u]);
                     sv[u] = s[c0 + c];
                 }
             }
@@ -861,7 +927,7 @@ __global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
             for (int u = 0; u < U; ++u) {
                 const int c = base + u * blockDim.x;
                 if (c < cnt) {
-                    const T yv = dot_row7<T>(rw[u], d.do_k);
+                    const T yv = dot_row7<T, MIXED>(rw[u], d.do_k);
                     y[c0 + c] = yv;
                     v[0] += (double)yv * (double)sv[u];
                     v[1] += (double)yv * (double)yv;

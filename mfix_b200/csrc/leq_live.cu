@@ -160,6 +160,8 @@ int Engine::live_add(const LiveSystem &ls)
     st.inner_tol = live_opt_.inner_tol;
     st.growth_limit = live_opt_.mixed_growth;
     st.stall_limit = live_opt_.mixed_stalls;
+    st.min_margin = live_opt_.mixed_min_margin;
+    st.margin_bits = 0x7f800000u;
     st.i = 1;
     st.iter = 1;
 

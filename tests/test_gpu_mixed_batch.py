@@ -4,8 +4,9 @@ Mixed form (FP32 BiCGSTAB, FP64 solution accumulation and reliable updates):
 IER 0, the FP64 true relative residual of the scaled system <= TOL, and a
 solution within 1e-6 of the FP64 drop-in's.  On the well-conditioned
 convection-diffusion systems it takes no more than 1.3x the FP64 iterations and
-never hands over to FP64; on the near-singular pressure-like system (zero
-wall coupling, diagonal excess 1e-6) the FP64 re-solve guard may engage.  Batch: uneven systems solved together give results
+never hands over to FP64; the near-singular pressure-like system (zero wall
+coupling, diagonal excess 1e-6, so a diagonal-dominance margin of 1e-6) goes
+to the FP64 drop-in before any FP32 iteration.  Batch: uneven systems solved together give results
 bit-identical to each system solved alone, in both precisions.
 """
 import numpy as np
@@ -47,6 +48,30 @@ def test_mixed_converges_to_tol(make, near_singular):
         assert st["fp64_fallback"] == 0
         assert st["outer_steps"] >= 1
         assert st["iterations"] <= 1.3 * st_ref["iterations"] + 2
+    else:  # diagonal-dominance margin 1e-6 < 1e-4: FP64 from the start, no FP32 iteration spent
+        assert st["fp64_fallback"] == 1 and st["mixed_iterations"] == 0
+
+
+def test_margin_routing_threshold():
+    """The routing follows the option: with mixed_min_margin = 0 the pressure-like
+    system is attempted in FP32 (and may still hand over later)."""
+    s = S.pressure_like(20, 22, 18, seed=5, nspheres=3, rmin=2, rmax=4, itmax=3000)
+    assert leq.set_option("precision", 1) == 0 and leq.set_option("mixed_min_margin", 0.0) == 0
+    try:
+        m = s.copy()
+        assert leq.solve_system(m) == 0
+        st = leq.last_stats()
+        assert st["fp64_fallback"] == 0 or st["mixed_iterations"] > 0
+    finally:
+        leq.set_option("mixed_min_margin", 1e-4)
+        leq.set_option("precision", 0)
+    c = S.conv_diff(20, 22, 18, seed=6)  # margin 1e-3: stays in the mixed form
+    assert leq.set_option("precision", 1) == 0
+    try:
+        assert leq.solve_system(c) == 0
+        assert leq.last_stats()["fp64_fallback"] == 0
+    finally:
+        leq.set_option("precision", 0)
 
 
 @pytest.mark.parametrize("precision", [0, 1])
