@@ -734,7 +734,7 @@ template <typename T, bool MIXED, bool PAIR>
 __global__ void __launch_bounds__(256) k_matvec_alpha(BatchView b, int src)
 {
     constexpr int U = Batch<T>::STENCIL;
-    constexpr int UP = Batch<T>::STENCIL / 2;
+    constexpr int UP = 1;  // one cell pair per thread and pass: fewer registers, more resident warps
     TileRun run{-1, 0};
     auto fin = [&](SysState &st, const double(&tot)[1]) { st.alpha = st.rho / tot[0]; };
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
@@ -866,7 +866,7 @@ template <typename T, bool MIXED, bool PAIR>
 __global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
 {
     constexpr int U = Batch<T>::STENCIL;
-    constexpr int UP = Batch<T>::STENCIL / 2;
+    constexpr int UP = 1;  // one cell pair per thread and pass: fewer registers, more resident warps
     TileRun run{-1, 0};
     auto fin = [&](SysState &st, const double(&tot)[2]) {
         double txt = tot[1];
@@ -1013,7 +1013,7 @@ __device__ inline void fin_xr_inner(SysState &s, double rr, double rtr)
 template <typename T, bool MIXED>
 __global__ void __launch_bounds__(256) k_xr_update(BatchView b, int ph_id, int sh_id)
 {
-    constexpr int U2 = sizeof(T) == 8 ? 1 : 2;
+    constexpr int U2 = 1;  // one cell pair per thread and pass: 60-64 registers, 4 blocks per SM
     TileRun run{-1, 0};
     auto fin = [&](SysState &st, const double(&tot)[2]) {
         if (MIXED)
