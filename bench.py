@@ -657,8 +657,9 @@ class _Req:
         self.n, self.a, self.b, self.x, self.tol, self.itmax = s.n, s.a, s.b, x, tol, s.itmax
 
 
-def _serve_run(leq, pool, precision, rate, seconds, seed, budget, check_every=2, max_systems=512,
+def _serve_run(leq, pool, precision, rate, seconds, seed, budget, check_every=8, max_systems=512,
                verify_every=40):
+    check_every = SERVE_CHECK_EVERY or check_every
     """One open-loop Poisson run against a fresh server; returns its statistics."""
     rng = np.random.default_rng(seed)
     nreq = int(rate * seconds * 1.2) + 16
@@ -738,7 +739,11 @@ def _serve_run(leq, pool, precision, rate, seconds, seed, budget, check_every=2,
     }
 
 
-def _serve_closed(leq, pool, precision, inflight, seconds, seed, budget, check_every=2, max_systems=512):
+SERVE_CHECK_EVERY = 0  # --serve-check: iterations between state reads in the serving runs (0: 8)
+
+
+def _serve_closed(leq, pool, precision, inflight, seconds, seed, budget, check_every=8, max_systems=512):
+    check_every = SERVE_CHECK_EVERY or check_every
     """Closed loop: `inflight` requests outstanding, each completion replaced by a
     new request, for `seconds`; the completion rate is the server's capacity for
     the request mix (completions follow the submission mix in steady state)."""
@@ -792,6 +797,8 @@ def _serve_closed(leq, pool, precision, inflight, seconds, seed, budget, check_e
             "alg_gbs": alg / span / 1e9, "latency_ms_at_capacity": {"p50": float(np.percentile(lat, 50)),
                                                                     "p99": float(np.percentile(lat, 99))},
             "fp64_handovers": int(c1["fp64_fallbacks"] - c0["fp64_fallbacks"]),
+            "device_busy_frac": [round((c1["busy_ms"][k] - c0["busy_ms"][k]) / (1e3 * (c1["seconds"] - c0["seconds"])), 3)
+                                 for k in range(2)],
             "nonzero_ier": sum(1 for _, r in done if r["ier"] != 0)}
 
 
@@ -825,6 +832,9 @@ def run_serve_bench(args) -> None:
     with sampler:
         cap_m = _serve_closed(leq, pool, 1, 256, seconds, 11, w["budget"])
         cap_f = _serve_closed(leq, pool, 0, 256, seconds, 11, w["budget"])
+        if args.capacity_only:
+            print(json.dumps({"capacity": {"mixed": cap_m, "fp64": cap_f}}), flush=True)
+            return
         loads = []
         for frac in (0.5, 0.8):
             lam = frac * cap_f["capacity"]
@@ -856,7 +866,7 @@ def run_serve_bench(args) -> None:
         "config": {"workload": args.workload, "seconds_per_run": seconds, "pool_systems": len(pool),
                    "pool_cells_mean": float(np.mean([p.n for p in pool])),
                    "sizes": "per axis log-uniform on [24, 160]", "pressure_share": 0.2, "tol": [1e-6, 1e-8],
-                   "hbm_budget_gb": w["budget"] / 1e9, "max_systems_per_batch": 512, "check_every": 2,
+                   "hbm_budget_gb": w["budget"] / 1e9, "max_systems_per_batch": 512, "check_every": SERVE_CHECK_EVERY or 8,
                    "capacity": "closed loop, 256 requests in flight, completions after the first 20% of the run",
                    "inputs": "pinned host A_M/B_M copied in per request, VAR copied out; zero initial guess"},
         "roofline": {"kernel": "served solves at capacity (algorithmic bytes of completed requests)", "bound": "hbm",
@@ -886,10 +896,14 @@ def main() -> None:
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
     ap.add_argument("--line-lanes", type=int, default=0, help="force lanes per J-line (0: autotuned)")
     ap.add_argument("--rate", type=float, default=0.0, help="serving: offered requests/s (0: the workload's)")
+    ap.add_argument("--serve-check", type=int, default=0, help="serving: iterations between state reads")
+    ap.add_argument("--capacity-only", action="store_true", help="serving: the closed-loop capacity runs only")
     ap.add_argument("--seconds", type=float, default=0.0, help="serving: arrival window (0: the workload's)")
     ap.add_argument("--only", default="all", choices=["all", "fp64", "mixed"],
                     help="profiling runs: solve only this form (no e2e leg, no JSON line)")
     args = ap.parse_args()
+    global SERVE_CHECK_EVERY
+    SERVE_CHECK_EVERY = args.serve_check
     kind = WORKLOADS[args.workload]["kind"]
     if args.impl == "reference":
         run_reference(args)

@@ -213,7 +213,7 @@ int mfixgpu_batch_solve(mfixgpu_system *systems, int nsys, const char *sweep, co
 typedef struct {
     int precision;          /* 1 (default): FP32 inner / FP64 outer with FP64 hand-over; 0: FP64 drop-in */
     int max_systems;        /* slots of each live batch (default 256) */
-    int check_every;        /* iterations between reads of the batch state (default 4) */
+    int check_every;        /* iterations between reads of the batch state (default 8) */
     int device;             /* CUDA device (default 0) */
     double hbm_budget;      /* bytes of device memory the requests may hold (0: 85% of free memory) */
     double inner_tol;       /* mixed form: as the "inner_tol" option (0: 1e-2) */
@@ -248,6 +248,7 @@ typedef struct {
     long long max_running;      /* most requests in the live batches at once */
     double reserved_bytes, peak_reserved_bytes, budget_bytes;
     double seconds;             /* server clock now */
+    double busy_ms[2];          /* device time of the form's live batch and of the FP64 hand-over batch */
 } mfixgpu_server_counters;
 
 /* Starts a server (its worker thread, streams, live batches).  cfg may be NULL

@@ -110,6 +110,7 @@ Engine::~Engine()
     cudaFree(d_st_);
     cudaFree(d_tiles_);
     cudaFree(d_prefix_);
+    cudaFree(d_line_sys_);
     cudaFree(d_allprefix_);
     cudaFree(d_partials_);
     cudaFree(d_lines_);
@@ -120,6 +121,10 @@ Engine::~Engine()
     cudaFree(d_dot_out_);
     if (h_st_pinned_) cudaFreeHost(h_st_pinned_);
     if (live_exec_) cudaGraphExecDestroy(live_exec_);
+    for (int q = 0; q < 2; ++q) {
+        if (ev_c0_[q]) cudaEventDestroy(ev_c0_[q]);
+        if (ev_c1_[q]) cudaEventDestroy(ev_c1_[q]);
+    }
     if (ev_fence_) cudaEventDestroy(ev_fence_);
     if (ev_a_) cudaEventDestroy(ev_a_);
     if (ev_b_) cudaEventDestroy(ev_b_);
@@ -343,12 +348,17 @@ int Engine::configure_lines(int elem, int only_L)
         const int64_t slots = keep ? (int64_t)d.half_lines * d.kmax2 : 0;
         h_prefix_[s + 1] = h_prefix_[s] + (int)((slots + lpw - 1) / lpw);
     }
+    h_line_sys_.resize(std::max(h_prefix_[nsys_], 1));
+    for (int s = 0; s < nsys_; ++s)
+        std::fill(h_line_sys_.begin() + h_prefix_[s], h_line_sys_.begin() + h_prefix_[s + 1], s);
     CK(upload(&d_sys_, &sys_cap_, h_sys_.data(), h_sys_.size(), stream_));
     CK(upload(&d_prefix_, &prefix_cap_, h_prefix_.data(), h_prefix_.size(), stream_));
+    CK(upload(&d_line_sys_, &line_sys_cap_, h_line_sys_.data(), (size_t)h_prefix_[nsys_], stream_));
     // the uploads may have (re)allocated the tables: the kernels' view follows them
     view_.sys = d_sys_;
     view_.line_prefix = d_prefix_;
-    if (!view_.sys || !view_.st || !view_.tiles || !view_.line_prefix || !view_.partials)
+    view_.line_sys = d_line_sys_;
+    if (!view_.sys || !view_.st || !view_.tiles || !view_.line_prefix || !view_.line_sys || !view_.partials)
         return fail("internal: batch tables missing on the device", -13);
     cfg_.line_cmax = cmax;
     int wpb = 1;

@@ -163,6 +163,7 @@ public:
     cudaEvent_t live_fence() const { return ev_fence_; }
     long long live_commits() const { return commits_; }
     long long live_bodies() const { return body_total_; }
+    double live_busy_ms() const { return busy_ms_; }  // device time of the collected chunks (commits included)
     long long launches() const { return launches_; }
 
     // per-routine entry points on device pointers (parity tests of single kernels)
@@ -211,6 +212,9 @@ private:
     SysState *d_st_ = nullptr;
     Tile *d_tiles_ = nullptr;
     int *d_prefix_ = nullptr;
+    int *d_line_sys_ = nullptr;  // system of each parity-wave work item
+    std::vector<int> h_line_sys_;
+    size_t line_sys_cap_ = 0;
     int *d_allprefix_ = nullptr;
     double *d_partials_ = nullptr;
     SysState *h_st_pinned_ = nullptr;
@@ -267,6 +271,8 @@ private:
     long long live_per_body_ = 0;
     long long snap_count_ = 0, body_total_ = 0, collected_upto_ = -1, commits_ = 0;
     long long snap_bodies_[2] = {0, 0};
+    cudaEvent_t ev_c0_[2] = {}, ev_c1_[2] = {};  // around each chunk (commit + iterations)
+    double busy_ms_ = 0.0;
     cudaEvent_t ev_fence_ = nullptr;
 };
 

@@ -1328,7 +1328,7 @@ __device__ __forceinline__ bool next_line_job(const BatchView &b, const WaveArgs
                                               int lane, bool pair, LineJob &j)
 {
     for (; item < total; item += step) {
-        const int sidx = (w.kind == 0) ? find_sys(b.line_prefix, b.nsys, item) : 0;
+        const int sidx = (w.kind == 0) ? __ldg(b.line_sys + item) : 0;
         if (!gate_ok(b.st[sidx], w.gate)) continue;
         const SysDev &d = b.sys[sidx];
         if (pair && (d.jmax2 & 1)) continue;

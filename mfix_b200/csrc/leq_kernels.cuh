@@ -12,6 +12,7 @@ struct BatchView {
     int ntiles;
     int nsys;
     const int *line_prefix;  // [nsys+1] parity-wave work items (exclusive prefix)
+    const int *line_sys;     // [items] the system of each parity-wave work item
     double *partials;        // [ntiles_total * 2]
 };
 

@@ -90,6 +90,11 @@ int Engine::live_open(int capacity, const SolveOptions &opt)
         h_st_pinned_cap_ = 2 * (size_t)capacity;
     }
     if (!ev_fence_) CK(cudaEventCreateWithFlags(&ev_fence_, cudaEventDisableTiming));
+    for (int q = 0; q < 2; ++q) {
+        if (!ev_c0_[q]) CK(cudaEventCreate(&ev_c0_[q]));
+        if (!ev_c1_[q]) CK(cudaEventCreate(&ev_c1_[q]));
+    }
+    busy_ms_ = 0.0;
     view_.st = d_st_;
     view_.tiles = d_tiles_;
     view_.ntiles = 0;
@@ -300,6 +305,8 @@ int Engine::live_step(int iterations)
 {
     if (slot_used_.empty()) return fail("live batch not open", -14);
     int rc;
+    const int b = (int)(snap_count_ & 1);
+    CK(cudaEventRecord(ev_c0_[b], stream_));
     if (live_dirty_ && (rc = live_commit())) return rc;
     if (live_used_ == 0 || iterations <= 0) return 0;
     for (int q = 0; q < iterations; ++q) {
@@ -312,7 +319,7 @@ int Engine::live_step(int iterations)
     }
     body_total_ += iterations;
     const int cap = (int)slot_used_.size();
-    const int b = (int)(snap_count_ & 1);
+    CK(cudaEventRecord(ev_c1_[b], stream_));
     CK(cudaMemcpyAsync(h_st_pinned_ + (size_t)b * cap, d_st_, sizeof(SysState) * cap, cudaMemcpyDeviceToHost,
                        stream_));
     CK(cudaEventRecord(b ? ev_b_ : ev_a_, stream_));
@@ -327,6 +334,9 @@ int Engine::live_collect(std::vector<LiveDone> &done, bool latest)
     if (q < 0 || q <= collected_upto_) return 0;
     const int b = (int)(q & 1);
     CK(cudaEventSynchronize(b ? ev_b_ : ev_a_));
+    float chunk_ms = 0.f;
+    if (cudaEventElapsedTime(&chunk_ms, ev_c0_[b], ev_c1_[b]) == cudaSuccess) busy_ms_ += chunk_ms;
+    cudaGetLastError();
     const int cap = (int)slot_used_.size();
     const bool mixed = live_opt_.precision == PREC_MIXED;
     const SysState *ps = h_st_pinned_ + (size_t)b * cap;

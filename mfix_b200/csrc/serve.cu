@@ -173,6 +173,8 @@ public:
         o->peak_reserved_bytes = (double)peak_reserved_;
         o->budget_bytes = budget_;
         o->seconds = now();
+        o->busy_ms[0] = busy_ms_[0];
+        o->busy_ms[1] = busy_ms_[1];
     }
 
     void cancel_queued()
@@ -445,6 +447,10 @@ private:
             if (!e) continue;
             done_.clear();
             if (e->live_collect(done_, false)) return go_fatal(e->last_error());
+            {
+                std::lock_guard<std::mutex> lk(mu_);
+                busy_ms_[(e == first_engine()) ? 0 : 1] = e->live_busy_ms();
+            }
             for (const LiveDone &d : done_) {
                 Req *r = owner(e)[d.slot];
                 owner(e)[d.slot] = nullptr;
@@ -616,7 +622,7 @@ public:
     struct Config {
         int precision = PREC_MIXED;
         int max_systems = 256;
-        int check_every = 4;
+        int check_every = 8;
         int device = 0;
         double hbm_budget = 0;
         double inner_tol = 1e-2;
@@ -635,6 +641,7 @@ private:
     bool started_ = false, stop_ = false, cancel_ = false;
     int setup_rc_ = 0, fatal_ = 0;
     double budget_ = 0;
+    double busy_ms_[2] = {0.0, 0.0};
     long long next_id_ = 0, submitted_ = 0, completed_ = 0, commits_ = 0, bodies_ = 0, launches_ = 0,
               fallbacks_ = 0, max_running_ = 0;
     std::deque<Req *> incoming_;

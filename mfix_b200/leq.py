@@ -68,7 +68,7 @@ class ServerCountersC(C.Structure):
                 ("copying", C.c_longlong), ("running", C.c_longlong), ("commits", C.c_longlong),
                 ("iterations", C.c_longlong), ("kernel_launches", C.c_longlong), ("fp64_fallbacks", C.c_longlong),
                 ("max_running", C.c_longlong), ("reserved_bytes", C.c_double), ("peak_reserved_bytes", C.c_double),
-                ("budget_bytes", C.c_double), ("seconds", C.c_double)]
+                ("budget_bytes", C.c_double), ("seconds", C.c_double), ("busy_ms", C.c_double * 2)]
 
 
 REQ_ZERO_GUESS = 1
@@ -295,7 +295,13 @@ def solve_system(s, method: int = 2, sweep: str = "RSRS", pc: str = "LINE", vno:
 
 
 def _struct_dict(st) -> dict:
-    return {name: getattr(st, name) for name, _ in st._fields_ if not name.startswith("pad")}
+    out = {}
+    for name, _ in st._fields_:
+        if name.startswith("pad"):
+            continue
+        v = getattr(st, name)
+        out[name] = list(v) if isinstance(v, C.Array) else v
+    return out
 
 
 class Server:
