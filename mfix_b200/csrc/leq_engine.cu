@@ -120,7 +120,12 @@ Engine::~Engine()
     cudaFree(d_dot_counter_);
     cudaFree(d_dot_out_);
     if (h_st_pinned_) cudaFreeHost(h_st_pinned_);
+    for (int q = 0; q < STAGES; ++q) {
+        if (stage_buf_[q]) cudaFreeHost(stage_buf_[q]);
+        if (stage_ev_[q]) cudaEventDestroy(stage_ev_[q]);
+    }
     if (live_exec_) cudaGraphExecDestroy(live_exec_);
+    for (auto &r : retired_execs_) cudaGraphExecDestroy(r.first);
     for (int q = 0; q < 2; ++q) {
         if (ev_c0_[q]) cudaEventDestroy(ev_c0_[q]);
         if (ev_c1_[q]) cudaEventDestroy(ev_c1_[q]);
@@ -165,6 +170,32 @@ SolveResult result_of(const SysState &st, bool mixed)
     }
     return r;
 }
+
+// ------------------------------------------------------------------ staged uploads
+cudaError_t Engine::stage_open(size_t bytes)
+{
+    stage_cur_ = (stage_cur_ + 1) % STAGES;
+    stage_used_ = 0;
+    if (stage_ev_[stage_cur_]) {
+        cudaError_t e = cudaEventSynchronize(stage_ev_[stage_cur_]);  // its last copies are done
+        if (e != cudaSuccess) return e;
+    } else {
+        cudaError_t e = cudaEventCreateWithFlags(&stage_ev_[stage_cur_], cudaEventDisableTiming);
+        if (e != cudaSuccess) return e;
+    }
+    if (bytes > stage_cap_[stage_cur_]) {
+        if (stage_buf_[stage_cur_]) cudaFreeHost(stage_buf_[stage_cur_]);
+        stage_buf_[stage_cur_] = nullptr;
+        stage_cap_[stage_cur_] = 0;
+        const size_t want = std::max<size_t>(2 * bytes, 1 << 20);
+        cudaError_t e = cudaMallocHost((void **)&stage_buf_[stage_cur_], want);
+        if (e != cudaSuccess) return e;
+        stage_cap_[stage_cur_] = want;
+    }
+    return cudaSuccess;
+}
+
+cudaError_t Engine::stage_close() { return cudaEventRecord(stage_ev_[stage_cur_], stream_); }
 
 // ------------------------------------------------------------------ work memory
 // One system's work memory: in the mixed form the FP32 diagonals first, then the
@@ -351,9 +382,11 @@ int Engine::configure_lines(int elem, int only_L)
     h_line_sys_.resize(std::max(h_prefix_[nsys_], 1));
     for (int s = 0; s < nsys_; ++s)
         std::fill(h_line_sys_.begin() + h_prefix_[s], h_line_sys_.begin() + h_prefix_[s + 1], s);
-    CK(upload(&d_sys_, &sys_cap_, h_sys_.data(), h_sys_.size(), stream_));
-    CK(upload(&d_prefix_, &prefix_cap_, h_prefix_.data(), h_prefix_.size(), stream_));
-    CK(upload(&d_line_sys_, &line_sys_cap_, h_line_sys_.data(), (size_t)h_prefix_[nsys_], stream_));
+    CK(stage_open(sizeof(SysDev) * h_sys_.size() + sizeof(int) * (h_prefix_.size() + h_line_sys_.size()) + 256));
+    CK(upload_staged(&d_sys_, &sys_cap_, h_sys_.data(), h_sys_.size()));
+    CK(upload_staged(&d_prefix_, &prefix_cap_, h_prefix_.data(), h_prefix_.size()));
+    CK(upload_staged(&d_line_sys_, &line_sys_cap_, h_line_sys_.data(), (size_t)h_prefix_[nsys_]));
+    CK(stage_close());
     // the uploads may have (re)allocated the tables: the kernels' view follows them
     view_.sys = d_sys_;
     view_.line_prefix = d_prefix_;

@@ -4,6 +4,7 @@
 #pragma once
 #include <algorithm>
 #include <cstdint>
+#include <cstring>
 #include <map>
 #include <mutex>
 #include <string>
@@ -201,6 +202,42 @@ private:
     DeviceArena in_arena_;  // device copies of host inputs (A_M, B_M, VAR)
     std::string err_;
 
+    // Table uploads go through a ring of pinned staging buffers: a copy from
+    // pageable memory would first wait for the stream to drain, which idles the
+    // GPU while a live batch's host work runs.  A buffer is reused after the
+    // event recorded behind its copies.
+    static constexpr int STAGES = 4;
+    char *stage_buf_[STAGES] = {};
+    size_t stage_cap_[STAGES] = {}, stage_used_ = 0;
+    cudaEvent_t stage_ev_[STAGES] = {};
+    int stage_cur_ = 0;
+    cudaError_t stage_open(size_t bytes);
+    cudaError_t stage_close();
+    template <typename T>
+    cudaError_t stage_copy(T *dst, const T *src, size_t n)
+    {
+        if (n == 0) return cudaSuccess;
+        const size_t off = (stage_used_ + 63) / 64 * 64, bytes = n * sizeof(T);
+        if (off + bytes > stage_cap_[stage_cur_])  // not foreseen by stage_open: a plain copy
+            return cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, stream_);
+        std::memcpy(stage_buf_[stage_cur_] + off, src, bytes);
+        stage_used_ = off + bytes;
+        return cudaMemcpyAsync(dst, stage_buf_[stage_cur_] + off, bytes, cudaMemcpyHostToDevice, stream_);
+    }
+    template <typename T>
+    cudaError_t upload_staged(T **dptr, size_t *cap_elems, const T *src, size_t n)
+    {
+        if (n > *cap_elems || *dptr == nullptr) {
+            if (*dptr) cudaFree(*dptr);
+            *dptr = nullptr;
+            const size_t want = std::max<size_t>(n + n / 2, 16);
+            cudaError_t e = cudaMalloc((void **)dptr, want * sizeof(T));
+            if (e != cudaSuccess) return e;
+            *cap_elems = want;
+        }
+        return stage_copy(*dptr, src, n);
+    }
+
     // batch tables (host mirrors + device copies)
     int nsys_ = 0;
     std::vector<SysDev> h_sys_;
@@ -268,6 +305,8 @@ private:
     bool live_dirty_ = false;
     bool live_tune_ = false;  // autotune new line lengths at the next commit
     cudaGraphExec_t live_exec_ = nullptr;
+    // replaced body graphs, destroyed once a snapshot taken after their last launch has been read
+    std::vector<std::pair<cudaGraphExec_t, long long>> retired_execs_;
     long long live_per_body_ = 0;
     long long snap_count_ = 0, body_total_ = 0, collected_upto_ = -1, commits_ = 0;
     long long snap_bodies_[2] = {0, 0};

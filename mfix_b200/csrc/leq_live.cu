@@ -57,6 +57,12 @@ int Engine::live_open(int capacity, const SolveOptions &opt)
     live_opt_ = opt;
     live_opt_.on_device = true;
     live_opt_.time_kernels = false;
+    // graphs of an earlier live batch on this engine
+    CK(cudaStreamSynchronize(stream_));
+    for (auto &r : retired_execs_) cudaGraphExecDestroy(r.first);
+    retired_execs_.clear();
+    if (live_exec_) cudaGraphExecDestroy(live_exec_);
+    live_exec_ = nullptr;
     const bool mixed = opt.precision == PREC_MIXED;
 
     nsys_ = capacity;
@@ -203,9 +209,13 @@ int Engine::live_commit()
 
     // states of the slots that changed hands; the copies are stream ordered
     // after every kernel already enqueued
+    size_t ntiles = 0;
+    for (int s = 0; s < cap; ++s)
+        if (slot_used_[s]) ntiles += h_sys_[s].ntiles;
+    CK(stage_open(sizeof(SysState) * cap + sizeof(Tile) * ntiles + sizeof(int) * (cap + 1) + 1024));
     for (int s = 0; s < cap; ++s) {
         if (slot_cleared_[s]) {
-            CK(cudaMemcpyAsync(d_st_ + s, &h_st_[s], sizeof(SysState), cudaMemcpyHostToDevice, stream_));
+            CK(stage_copy(d_st_ + s, &h_st_[s], 1));
             slot_cleared_[s] = 0;
         }
         if (!slot_fresh_[s]) continue;
@@ -215,7 +225,7 @@ int Engine::live_commit()
         if (ls.after) CK(cudaStreamWaitEvent(stream_, ls.after, 0));
         if (ls.x0) CK(cudaMemcpyAsync(ls.dev.x, ls.x0, n * 8, cudaMemcpyDeviceToDevice, stream_));
         if (mixed) CK(cudaMemcpyAsync(h_sys_[s].x64[1], ls.dev.x, n * 8, cudaMemcpyDeviceToDevice, stream_));
-        CK(cudaMemcpyAsync(d_st_ + s, &h_st_[s], sizeof(SysState), cudaMemcpyHostToDevice, stream_));
+        CK(stage_copy(d_st_ + s, &h_st_[s], 1));
     }
 
     // tables of the systems now in the batch
@@ -231,8 +241,9 @@ int Engine::live_commit()
         }
         h_allprefix_[s + 1] = h_allprefix_[s] + (slot_used_[s] ? d.imax2 * d.kmax2 : 0);
     }
-    CK(upload(&d_tiles_, &tiles_cap_, h_tiles_.data(), h_tiles_.size(), stream_));
-    CK(upload(&d_allprefix_, &allprefix_cap_, h_allprefix_.data(), h_allprefix_.size(), stream_));
+    CK(upload_staged(&d_tiles_, &tiles_cap_, h_tiles_.data(), h_tiles_.size()));
+    CK(upload_staged(&d_allprefix_, &allprefix_cap_, h_allprefix_.data(), h_allprefix_.size()));
+    CK(stage_close());
     const size_t need_part = 2 * (size_t)std::max(tile_base, 1);
     if (need_part > part_cap_) {
         cudaFree(d_partials_);  // waits for the kernels that still use it
@@ -269,7 +280,7 @@ int Engine::live_commit()
     if (any_fresh && live_tune_ && (rc = autotune_lines(live_opt_, mixed ? 4 : 8))) return rc;
 
     // the iteration body for this membership
-    if (live_exec_) cudaGraphExecDestroy(live_exec_);  // freed once its launches finish
+    if (live_exec_) retired_execs_.push_back({live_exec_, snap_count_});  // its launches may still run
     live_exec_ = nullptr;
     if (live_used_ > 0 && live_opt_.use_graph) {
         cudaGraph_t g = nullptr;
@@ -337,6 +348,15 @@ int Engine::live_collect(std::vector<LiveDone> &done, bool latest)
     float chunk_ms = 0.f;
     if (cudaEventElapsedTime(&chunk_ms, ev_c0_[b], ev_c1_[b]) == cudaSuccess) busy_ms_ += chunk_ms;
     cudaGetLastError();
+    // snapshot q follows every launch of the graphs retired before it was taken
+    for (size_t r = 0; r < retired_execs_.size();)
+        if (retired_execs_[r].second <= q) {
+            cudaGraphExecDestroy(retired_execs_[r].first);
+            retired_execs_[r] = retired_execs_.back();
+            retired_execs_.pop_back();
+        } else {
+            ++r;
+        }
     const int cap = (int)slot_used_.size();
     const bool mixed = live_opt_.precision == PREC_MIXED;
     const SysState *ps = h_st_pinned_ + (size_t)b * cap;
