@@ -733,7 +733,7 @@ __global__ void __launch_bounds__(256, 4) k_copy(BatchView b, int src, int dst, 
 template <typename T, bool MIXED, bool PAIR>
 __global__ void __launch_bounds__(256) k_matvec_alpha(BatchView b, int src)
 {
-    constexpr int U = Batch<T>::STENCIL;
+    constexpr int U = 2;  // one-cell rows: two cells per thread and pass (80 registers in FP32)
     constexpr int UP = 1;  // one cell pair per thread and pass: fewer registers, more resident warps
     TileRun run{-1, 0};
     auto fin = [&](SysState &st, const double(&tot)[1]) { st.alpha = st.rho / tot[0]; };
@@ -865,7 +865,7 @@ __global__ void __launch_bounds__(256, 4) k_s_update(BatchView b)
 template <typename T, bool MIXED, bool PAIR>
 __global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
 {
-    constexpr int U = Batch<T>::STENCIL;
+    constexpr int U = 2;  // one-cell rows: two cells per thread and pass (80 registers in FP32)
     constexpr int UP = 1;  // one cell pair per thread and pass: fewer registers, more resident warps
     TileRun run{-1, 0};
     auto fin = [&](SysState &st, const double(&tot)[2]) {
