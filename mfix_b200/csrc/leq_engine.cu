@@ -51,7 +51,7 @@ void line_shape(int L, int *G, int *c)
     if (cc < 1) cc = 1;
     if ((cc & 1) == 0) ++cc;
     *G = g;
-    *c = cc;
+    *c = g == 1 ? 1 : cc;  // one lane per line stages nothing
 }
 
 void *DeviceArena::take(size_t bytes)
@@ -400,13 +400,30 @@ int Engine::configure_lines(int elem, int only_L)
     cfg_.line_warps = wpb;
     const int items = h_prefix_[nsys_];
     cfg_.line_grid = std::max(1, std::min((items + wpb - 1) / wpb, sms_ * bpsm));
+    // which line kernels the batch needs (systems with no line work count for none)
+    cfg_.line_thread = cfg_.line_warp = cfg_.line_single = 0;
+    for (int s = 0; s < nsys_; ++s) {
+        if (h_prefix_[s + 1] == h_prefix_[s]) continue;
+        const SysDev &d = h_sys_[s];
+        if (d.lane_group == 1) {
+            cfg_.line_thread = 1;
+        } else {
+            cfg_.line_warp = 1;
+            if (d.jmax2 & 1) cfg_.line_single = 1;
+        }
+    }
+    if (!cfg_.line_thread && !cfg_.line_warp) cfg_.line_warp = 1;  // empty batch: a no-op launch
+    const int tocc = elem == 4 ? line_thread_occupancy<float>() : line_thread_occupancy<double>();
+    cfg_.line_grid_thread = std::max(1, std::min((items + 3) / 4, sms_ * tocc));
     return 0;
 }
 
 static constexpr int MAX_TUNED_ROWS = 17;
 
+// Rows per lane; one lane per line (G = 1) stages nothing, so it counts as one.
 static int rows_for(int L, int G)
 {
+    if (G == 1) return 1;
     int c = (L + G - 1) / G;
     if (c < 1) c = 1;
     if ((c & 1) == 0) ++c;
@@ -474,7 +491,7 @@ int Engine::autotune_lines(const SolveOptions &opt, int elem)
         float best_ms = 1e30f;
         for (int g = 1; g <= 32; g *= 2) {
             const int c = rows_for(L, g);
-            if (c > MAX_TUNED_ROWS || (size_t)kernel_smem_line_bytes(c, elem) > 48 * 1024) continue;
+            if (g > 1 && (c > MAX_TUNED_ROWS || (size_t)kernel_smem_line_bytes(c, elem) > 48 * 1024)) continue;
             for (int s = 0; s < nsys_; ++s)
                 if (h_sys_[s].jmax2 == L && h_sys_[s].n > 0) {
                     h_sys_[s].lane_group = g;

@@ -601,10 +601,9 @@ __device__ __forceinline__ vec2_t<T> dot_pair7(const Pair7<T> &r, bool do_k)
     return mk2<T>(u, w);
 }
 
-// cells handled per thread per batch: stencil kernels, streaming kernels
+// cells handled per thread per batch: streaming kernels
 template <typename T>
 struct Batch {
-    static constexpr int STENCIL = sizeof(T) == 8 ? 2 : 4;
     static constexpr int STREAM = sizeof(T) == 8 ? 4 : 8;
 };
 
@@ -1323,14 +1322,16 @@ struct LineJob {
 
 // The next work item at or after `item` whose system takes part in the wave.
 // pair: the two-row instance, which takes systems with an even JMAX2 only (the
-// one-row instance takes every system).
+// one-row instance takes every system).  thread: the one-lane-per-line kernel,
+// which takes the systems with one lane per line (the warp kernels the others).
 __device__ __forceinline__ bool next_line_job(const BatchView &b, const WaveArgs &w, int item, int step, int total,
-                                              int lane, bool pair, LineJob &j)
+                                              int lane, bool pair, bool thread, LineJob &j)
 {
     for (; item < total; item += step) {
         const int sidx = (w.kind == 0) ? __ldg(b.line_sys + item) : 0;
         if (!gate_ok(b.st[sidx], w.gate)) continue;
         const SysDev &d = b.sys[sidx];
+        if ((d.lane_group == 1) != thread) continue;
         if (pair && (d.jmax2 & 1)) continue;
         j.item = item;
         j.sidx = sidx;
@@ -1480,7 +1481,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
     const int total = (w.kind == 0) ? b.line_prefix[b.nsys] : w.count;
     const int step = gridDim.x * nwarps;
     LineJob j;
-    for (int item = blockIdx.x * nwarps + warp; next_line_job(b, w, item, step, total, lane, PAIR, j);
+    for (int item = blockIdx.x * nwarps + warp; next_line_job(b, w, item, step, total, lane, PAIR, false, j);
          item = j.item + step) {
         const SysDev &d = b.sys[j.sidx];
         SysState &st = b.st[j.sidx];
@@ -1493,6 +1494,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
         const T *gl_ = reinterpret_cast<const T *>(d.fac[0]) + x.base;
         const T *gr_ = reinterpret_cast<const T *>(d.fac[1]) + x.base;
         const T *gq_ = reinterpret_cast<const T *>(d.fac[2]) + x.base;
+
 
         // ---- load (coalesced over the line): right-hand side and factors.  With an
         // even JMAX2 every line starts on an even cell, so lanes read two rows per
@@ -1692,6 +1694,79 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
             }
         }
         __syncwarp();
+    }
+}
+
+// ------------------------------------------------------------------ J-line half-sweep, one lane per line
+// For short lines in large numbers (batches and serving) each lane runs the two
+// recurrences down its own line, keeping y in the destination (the line's own
+// cells, which no other line of the wave reads); no staging, few instructions
+// per row.  A flagged line runs DGTSV with interchanges in global scratch: the
+// line's factor cells (unused for a flagged line) and its cells of T (dead
+// during MSOLVE), so that a line left unchanged (INFO != 0) keeps VAR.
+template <typename T>
+__global__ void __launch_bounds__(128) k_jline_thread(BatchView b, WaveArgs w)
+{
+    const int nwarps = blockDim.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int total = (w.kind == 0) ? b.line_prefix[b.nsys] : w.count;
+    const int step = gridDim.x * nwarps;
+    LineJob j;
+    for (int item = blockIdx.x * nwarps + warp; next_line_job(b, w, item, step, total, lane, false, true, j);
+         item = j.item + step) {
+        const SysDev &d = b.sys[j.sidx];
+        SysState &st = b.st[j.sidx];
+        const LineCtx<T> x = line_ctx<T>(b, w, j);
+        const int L = j.L;
+        const bool exact = j.valid && d.line_flag[(j.i - 1) + (j.k - 1) * d.imax2] != 0;
+        const bool fast = j.valid && !exact;
+        const T *gl_ = reinterpret_cast<const T *>(d.fac[0]) + x.base;
+        const T *gr_ = reinterpret_cast<const T *>(d.fac[1]) + x.base;
+        const T *gq_ = reinterpret_cast<const T *>(d.fac[2]) + x.base;
+        // ---- one lane per line (short lines, many of them): each lane runs the two
+        // recurrences down its own line, keeping y in the destination (the line's
+        // own cells, which no other line of the wave reads).
+        if (j.valid) {
+            T *dstp = vec<T>(d, w.dst) + x.base;
+            const T *rhs_l = x.rhs + x.base, *am1_l = x.a + 2 * x.n + x.base, *ap1_l = x.a + 4 * x.n + x.base;
+            const T *am3_l = x.a + x.base, *ap3_l = x.a + 6 * x.n + x.base;
+            if (fast) {
+                T y = T(0);
+#pragma unroll 4
+                for (int r = 0; r < L; ++r) {
+                    T fv = rhs_l[r] - am1_l[r] * x.nb_im[r];
+                    fv = fv - ap1_l[r] * x.nb_ip[r];
+                    if (x.do_k) {
+                        fv = fv - am3_l[r] * x.nb_km[r];
+                        fv = fv - ap3_l[r] * x.nb_kp[r];
+                    }
+                    y = fv - gl_[r] * y;
+                    dstp[r] = y;
+                }
+                T xv = T(0);
+#pragma unroll 4
+                for (int r = L - 1; r >= 0; --r) {
+                    xv = gr_[r] * dstp[r] - gq_[r] * xv;
+                    dstp[r] = xv;
+                }
+            } else {
+                // DGTSV with interchanges, in global scratch: the line's factor cells
+                // (unused for a flagged line) and its cells of T (dead during MSOLVE)
+                T *sub = reinterpret_cast<T *>(d.fac[0]) + x.base;
+                T *dg = reinterpret_cast<T *>(d.fac[1]) + x.base;
+                T *sup = reinterpret_cast<T *>(d.fac[2]) + x.base;
+                T *rs = vec<T>(d, V_T) + x.base;
+                for (int r = 0; r < L; ++r) line_row<T>(x, r, sub[r], dg[r], sup[r], rs[r]);
+                const int skip = dgtsv_rows<T>(L, sub, dg, sup, rs) != 0;
+                atomicAdd(&st.line_fallbacks, 1);
+                if (skip) atomicAdd(&st.line_skips, 1);
+                const T *oldl = vec<T>(d, w.old) + x.base;
+                if (!skip)
+                    for (int r = 0; r < L; ++r) dstp[r] = rs[r];
+                else if (w.write_old)
+                    for (int r = 0; r < L; ++r) dstp[r] = oldl[r];
+            }
+        }
     }
 }
 
@@ -1929,6 +2004,17 @@ int prepare_line_kernel(int cmax, int *warps)
     return std::min(nb, nb1);
 }
 
+template <typename T>
+int line_thread_occupancy()
+{
+    int nb = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_jline_thread<T>, 128, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return 4;
+    }
+    return nb > 0 ? nb : 1;
+}
+
 template <typename K>
 static int occ(K kern)
 {
@@ -1965,13 +2051,16 @@ void cell_occupancy(bool fp32, CellOcc *o)
 template <typename T>
 cudaError_t launch_jline(const BatchView &b, const LaunchCfg &c, const WaveArgs &w)
 {
-    const int smem = c.line_warps * kernel_smem_line_bytes(c.line_cmax, (int)sizeof(T));
-    // two-row loads for lines of even length, one-row loads for the others
-    // one launch per wave: two-row loads when every line has even length
-    if (c.rows_single)
-        k_jline<T, false><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax);
-    else
-        k_jline<T, true><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax);
+    // systems with one lane per line, then those with several: one warp-kernel
+    // launch, the two-row instance when all their lines have even length
+    if (c.line_thread) k_jline_thread<T><<<c.line_grid_thread, 128, 0, c.stream>>>(b, w);
+    if (c.line_warp) {
+        const int smem = c.line_warps * kernel_smem_line_bytes(c.line_cmax, (int)sizeof(T));
+        if (c.line_single)
+            k_jline<T, false><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax);
+        else
+            k_jline<T, true><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax);
+    }
     CHECK_LAUNCH();
 }
 template <typename T>
@@ -2058,6 +2147,7 @@ cudaError_t launch_seq_lines(const BatchView &b, const SeqLineArgs &a, cudaStrea
                                                 cudaStream_t, int);                                       \
     template cudaError_t launch_seq_lines<T>(const BatchView &, const SeqLineArgs &, cudaStream_t);        \
     template int prepare_line_kernel<T>(int, int *);                                                     \
+    template int line_thread_occupancy<T>();                                                             \
     template cudaError_t launch_line_factor<T>(const BatchView &, const LaunchCfg &, const int *, int);
 #define INST_TM(T, M)                                                                       \
     template cudaError_t launch_p_update<T, M>(const BatchView &, const LaunchCfg &);       \

@@ -26,6 +26,10 @@ struct LaunchCfg {
     int line_grid;   // blocks for J-line kernels
     int line_cmax;   // max rows per lane over the batch (smem sizing)
     int line_warps;  // warps per block of the J-line kernel
+    int line_grid_thread;  // blocks of the one-lane-per-line kernel (4 warps each)
+    int line_thread;       // 1: some system has one lane per line
+    int line_warp;         // 1: some system has several lanes per line
+    int line_single;       // 1: some system with several lanes per line has an odd line length
     cudaStream_t stream;
 };
 
@@ -87,7 +91,10 @@ cudaError_t launch_seq_lines(const BatchView &b, const SeqLineArgs &a, cudaStrea
 
 int kernel_smem_line_bytes(int cmax, int elem_bytes);
 template <typename T>
-int prepare_line_kernel(int cmax, int *warps);  // sets the smem attribute, returns resident blocks per SM
+int prepare_line_kernel(int cmax, int *warps);
+template <typename T>
+int line_thread_occupancy();  // resident blocks per SM of the one-lane-per-line kernel
+//  // sets the smem attribute, returns resident blocks per SM
 struct CellOcc {
     int p_update, s_update, xr_update, matvec, matvec_pair, copy, outer;
 };

@@ -98,3 +98,23 @@ def test_batch_rejects_sequential_letters():
     systems = [S.conv_diff(6, 6, 6, seed=q) for q in range(2)]
     rc, _ = leq.batch_solve(systems, sweep="ISIS")
     assert rc == leq.IER_UNSUPPORTED
+
+
+@pytest.mark.parametrize("lanes", [1, 4])
+@pytest.mark.parametrize("precision", [0, 1])
+def test_forced_lanes_per_line(lanes, precision):
+    """Every line kernel shape gives a correct solve: one lane per line (each lane
+    runs a whole line) and the warp-cooperative shapes."""
+    s = S.conv_diff(12, 31, 10, seed=40)
+    ref = s.copy()
+    st_ref = O.leq_bicgs(ref)
+    assert leq.set_option("line_lanes", lanes) == 0 and leq.set_option("precision", precision) == 0
+    try:
+        m = s.copy()
+        assert leq.solve_system(m) == 0, leq.last_error()
+    finally:
+        leq.set_option("line_lanes", 0)
+        leq.set_option("precision", 0)
+    assert np.array_equal(m.a, ref.a)
+    assert _true_rel(ref, m.x) <= s.tol * 1.01
+    assert np.linalg.norm(m.x - ref.x) <= 1e-6 * np.linalg.norm(ref.x)
