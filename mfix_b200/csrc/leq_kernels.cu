@@ -1619,6 +1619,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
         // ---- forward recurrence y_r = f_r - l_r y_{r-1}
         T *cf = f + gl * c, *cl = fl + gl * c, *cr = fr + gl * c, *cq = fq + gl * c;
         T mb = T(0), ma = T(1);
+#pragma unroll 4
         for (int t = 0; t < c; ++t) {
             const T lt = cl[t];
             mb = cf[t] - lt * mb;
@@ -1633,6 +1634,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
         }
         T y = __shfl_up_sync(0xffffffffu, mb, 1, G);
         if (gl == 0) y = T(0);
+#pragma unroll 4
         for (int t = 0; t < c; ++t) {
             y = cf[t] - cl[t] * y;
             cf[t] = y;
@@ -1640,6 +1642,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
         // ---- backward recurrence x_r = r_r y_r - q_r x_{r+1}
         mb = T(0);
         ma = T(1);
+#pragma unroll 4
         for (int t = c - 1; t >= 0; --t) {
             const T qt = cq[t];
             mb = cr[t] * cf[t] - qt * mb;
@@ -1654,6 +1657,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
         }
         T xv = __shfl_down_sync(0xffffffffu, mb, 1, G);
         if (gl == G - 1) xv = T(0);
+#pragma unroll 4
         for (int t = c - 1; t >= 0; --t) {
             xv = cr[t] * cf[t] - cq[t] * xv;
             cf[t] = xv;
