@@ -156,6 +156,11 @@ public:
     // Systems found finished in the previous snapshot (latest: the newest one,
     // waited for); each is reported once.
     int live_collect(std::vector<LiveDone> &done, bool latest);
+    // The oldest unread snapshot, if it is complete (never waits); *collected says
+    // whether one was read.  Snapshots are read in order.
+    int live_collect_ready(std::vector<LiveDone> &done, bool *collected);
+    // snapshots recorded and not read yet (chunks whose results are pending)
+    int live_inflight() const { return (int)(snap_count_ - 1 - collected_upto_); }
     int live_used() const { return live_used_; }
     int live_capacity() const { return (int)slot_used_.size(); }
     bool live_dirty() const { return live_dirty_; }
@@ -297,6 +302,7 @@ private:
 
     // live batch
     int live_commit();
+    int live_take(long long q, std::vector<LiveDone> &done);
     SolveOptions live_opt_{};
     std::vector<char> slot_used_, slot_fresh_, slot_reported_, slot_cleared_;
     std::vector<LiveSystem> slot_sys_;

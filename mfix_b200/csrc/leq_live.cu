@@ -345,6 +345,26 @@ int Engine::live_collect(std::vector<LiveDone> &done, bool latest)
     if (q < 0 || q <= collected_upto_) return 0;
     const int b = (int)(q & 1);
     CK(cudaEventSynchronize(b ? ev_b_ : ev_a_));
+    return live_take(q, done);
+}
+
+int Engine::live_collect_ready(std::vector<LiveDone> &done, bool *collected)
+{
+    *collected = false;
+    const long long q = collected_upto_ + 1;
+    if (q >= snap_count_) return 0;
+    const int b = (int)(q & 1);
+    const cudaError_t e = cudaEventQuery(b ? ev_b_ : ev_a_);
+    if (e == cudaErrorNotReady) return 0;
+    if (e != cudaSuccess) return fail(std::string("state snapshot: ") + cudaGetErrorString(e), -13);
+    *collected = true;
+    return live_take(q, done);
+}
+
+// Reads snapshot q (complete): finished systems, busy time, retired graphs.
+int Engine::live_take(long long q, std::vector<LiveDone> &done)
+{
+    const int b = (int)(q & 1);
     float chunk_ms = 0.f;
     if (cudaEventElapsedTime(&chunk_ms, ev_c0_[b], ev_c1_[b]) == cudaSuccess) busy_ms_ += chunk_ms;
     cudaGetLastError();

@@ -50,6 +50,7 @@ struct Req {
     Engine *eng = nullptr;
     int slot = -1;
     int fallback = 0, mixed_iterations = 0;
+    long long handover_after = 0;  // the mixed batch's commit count after which it may join the FP64 batch
     SolveResult res;
     double t_submit = 0, t_admit = 0, t_start = 0, t_done = 0;
 };
@@ -396,6 +397,7 @@ private:
         // batch's commit that removed them
         while (!handover_.empty() && f64_->live_used() < f64_->live_capacity()) {
             Req *r = handover_.front();
+            if (mix_->live_commits() < r->handover_after) break;
             LiveSystem ls;
             ls.dev = r->dev;
             ls.work = r->work;
@@ -421,11 +423,14 @@ private:
         return v;
     }
 
+    // Each live batch keeps up to two chunks of iterations queued and is stepped
+    // on its own: a batch whose chunk finished never waits for the other's.
     bool step()
     {
         bool stepped = false;
         for (Engine *e : {mix_.get(), f64_.get()}) {
             if (!e || (e->live_used() == 0 && !e->live_dirty())) continue;
+            if (e->live_inflight() >= 2) continue;
             const long long b0 = e->live_bodies(), l0 = e->launches(), c0 = e->live_commits();
             if (e->live_step(cfg_.check_every)) {
                 go_fatal(e->last_error());
@@ -441,12 +446,19 @@ private:
         return stepped;
     }
 
-    void collect()
+    bool collect()
     {
+        bool any = false;
         for (Engine *e : {mix_.get(), f64_.get()}) {
             if (!e) continue;
             done_.clear();
-            if (e->live_collect(done_, false)) return go_fatal(e->last_error());
+            bool got = false;
+            if (e->live_collect_ready(done_, &got)) {
+                go_fatal(e->last_error());
+                return any;
+            }
+            if (!got) continue;
+            any = true;
             {
                 std::lock_guard<std::mutex> lk(mu_);
                 busy_ms_[(e == first_engine()) ? 0 : 1] = e->live_busy_ms();
@@ -464,12 +476,14 @@ private:
                         std::lock_guard<std::mutex> lk(mu_);
                         ++fallbacks_;
                     }
+                    r->handover_after = mix_->live_commits() + 1;  // the commit that removes it
                     handover_.push_back(r);
                     continue;
                 }
                 copy_out(r, e, d.res);
             }
         }
+        return any;
     }
 
     void copy_out(Req *r, Engine *e, const SolveResult &res)
@@ -589,12 +603,14 @@ private:
             admit();
             join();
             const bool stepped = step();
-            collect();
+            const bool collected = collect();
             retire();
-            if (!stepped) {
-                // nothing on the engines: wait for the oldest copy instead of spinning
-                if (!copying_.empty())
-                    cudaEventSynchronize(copying_.front()->ev);
+            if (!stepped && !collected) {
+                const bool chunks = (mix_ && mix_->live_inflight() > 0) || f64_->live_inflight() > 0;
+                if (chunks)
+                    std::this_thread::sleep_for(std::chrono::microseconds(50));  // chunks still running
+                else if (!copying_.empty())
+                    cudaEventSynchronize(copying_.front()->ev);  // nothing on the engines: wait for a copy
                 else if (!unloading_.empty())
                     cudaEventSynchronize(unloading_.front()->ev);
             }
