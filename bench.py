@@ -897,6 +897,8 @@ def main() -> None:
     ap.add_argument("--line-lanes", type=int, default=0, help="force lanes per J-line (0: autotuned)")
     ap.add_argument("--rate", type=float, default=0.0, help="serving: offered requests/s (0: the workload's)")
     ap.add_argument("--serve-check", type=int, default=0, help="serving: iterations between state reads")
+    ap.add_argument("--tune-cache", default="", help="JSON file of J-line lanes choices: loaded, and new choices "
+                    "saved (a profiling run reuses the shapes of the timed run instead of tuning under the profiler)")
     ap.add_argument("--capacity-only", action="store_true", help="serving: the closed-loop capacity runs only")
     ap.add_argument("--seconds", type=float, default=0.0, help="serving: arrival window (0: the workload's)")
     ap.add_argument("--only", default="all", choices=["all", "fp64", "mixed"],
@@ -904,6 +906,10 @@ def main() -> None:
     args = ap.parse_args()
     global SERVE_CHECK_EVERY
     SERVE_CHECK_EVERY = args.serve_check
+    if args.tune_cache and args.impl != "reference":
+        from mfix_b200 import leq
+
+        leq.autotune_cache(args.tune_cache)
     kind = WORKLOADS[args.workload]["kind"]
     if args.impl == "reference":
         run_reference(args)
