@@ -7,7 +7,7 @@ equals the FP64 drop-in; a mixed request whose FP32 iteration cannot run
 (residual beyond FP32 range) moves to the FP64 batch and equals the one-shot
 mixed solve, which hands over the same way; admission never holds more device
 memory than the budget; the copy-back / device-pointer flags; submits from
-several threads.
+several threads; withdrawing queued requests, wait_any and the counters.
 """
 import threading
 
@@ -188,3 +188,42 @@ def test_batch_mixes_2d_and_3d(cuda):
     assert rc == 0 and all(r.ier == 0 for r in res)
     for a, t in zip(alone, together):
         assert np.array_equal(a.x, t.x)
+
+
+def test_cancel_queued_and_wait_any(cuda):
+    """Requests not yet admitted can be withdrawn (IER -17); admitted ones finish;
+    wait_any hands out every finished request once; the counters add up."""
+    systems = [S.conv_diff(30, 30, 30, seed=90 + q) for q in range(10)]
+    per = (72 + 110) * systems[0].n
+    with leq.Server(precision=1, hbm_budget=1.5 * per) as srv:  # one request on the device at a time
+        ts = [srv.submit(s) for s in systems]
+        for _ in range(5000):  # withdraw once the first request has been admitted
+            c = srv.counters()
+            if c["copying"] + c["running"] + c["completed"] >= 1:
+                break
+            threading.Event().wait(0.001)
+        srv.cancel_queued()
+        got = {}
+        while len(got) < len(ts):
+            r = srv.wait_any(60)
+            assert r is not None
+            t, res = r
+            assert t not in got
+            got[t] = res
+        c = srv.counters()
+    iers = [got[t]["ier"] for t in ts]
+    assert all(i in (0, leq.IER_CANCELLED) for i in iers)
+    assert iers.count(leq.IER_CANCELLED) >= 1 and iers.count(0) >= 1
+    for t, s in zip(ts, systems):
+        if got[t]["ier"] == 0:
+            assert got[t]["t_submit"] <= got[t]["t_admit"] <= got[t]["t_start"] <= got[t]["t_done"]
+            assert O.true_resid(_scaled(s), s.x) / O.true_resid(_scaled(s), np.zeros(s.n)) <= s.tol * 1.01
+    assert c["completed"] == c["submitted"] == len(ts)
+    assert c["queued"] == c["copying"] == c["running"] == 0
+    assert c["busy_ms"][0] > 0 and c["iterations"] > 0 and c["kernel_launches"] > 0
+
+
+def _scaled(s):
+    t = s.copy()
+    O.scale(t)
+    return t
