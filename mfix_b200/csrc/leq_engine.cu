@@ -93,6 +93,8 @@ Engine::Engine()
     cudaGetDevice(&dev_);
     cudaDeviceGetAttribute(&sms_, cudaDevAttrMultiProcessorCount, dev_);
     cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking);
+    cudaStreamCreateWithFlags(&side_, cudaStreamNonBlocking);
+    cudaEventCreateWithFlags(&ev_setup_, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ev_a_, cudaEventDisableTiming);
     cudaEventCreateWithFlags(&ev_b_, cudaEventDisableTiming);
     cudaEventCreate(&ev_t0_);
@@ -104,6 +106,7 @@ Engine::Engine()
 Engine::~Engine()
 {
     if (stream_) cudaStreamSynchronize(stream_);
+    if (side_) cudaStreamSynchronize(side_);
     arena_.release();
     in_arena_.release();
     cudaFree(d_sys_);
@@ -137,6 +140,8 @@ Engine::~Engine()
     if (ev_t1_) cudaEventDestroy(ev_t1_);
     for (auto &e : kt_ev_)
         if (e) cudaEventDestroy(e);
+    if (ev_setup_) cudaEventDestroy(ev_setup_);
+    if (side_) cudaStreamDestroy(side_);
     if (stream_) cudaStreamDestroy(stream_);
 }
 
@@ -884,6 +889,13 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
     }
     SolveOptions o = opt;
     o.on_device = true;
+    writeback_.clear();
+    if (!opt.on_device && opt.write_back_ab)
+        for (size_t q = 0; q < specs.size(); ++q) {
+            const size_t n = (size_t)specs[q].n;
+            writeback_.push_back({specs[q].a, dev[q].a, 7 * n * 8});
+            writeback_.push_back({specs[q].b, dev[q].b, n * 8});
+        }
     // several systems with red/black sweeps: a live batch, which drops systems
     // as they finish; otherwise the fixed batch (also the timed-kernel path)
     bool rs_only = true;
@@ -932,18 +944,28 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
     }
     timing_ = total;
 
-    // results back to the caller's host arrays
+    // results back to the caller's host arrays (A/B went back during the iterations)
+    if ((rc = issue_writeback())) return rc;  // a batch that ended before issuing them
     if (!opt.on_device) {
         for (size_t q = 0; q < specs.size(); ++q) {
             const size_t n = (size_t)specs[q].n;
             CK(cudaMemcpyAsync(specs[q].x, dev[q].x, n * 8, cudaMemcpyDeviceToHost, stream_));
-            if (opt.write_back_ab) {
-                CK(cudaMemcpyAsync(specs[q].a, dev[q].a, 7 * n * 8, cudaMemcpyDeviceToHost, stream_));
-                CK(cudaMemcpyAsync(specs[q].b, dev[q].b, n * 8, cudaMemcpyDeviceToHost, stream_));
-            }
         }
         CK(cudaStreamSynchronize(stream_));
+        CK(cudaStreamSynchronize(side_));
     }
+    return 0;
+}
+
+// Queues the pending copy-back of the scaled A/B on the side stream, behind
+// everything enqueued so far on the engine stream (the scaling).
+int Engine::issue_writeback()
+{
+    if (writeback_.empty()) return 0;
+    CK(cudaEventRecord(ev_setup_, stream_));
+    CK(cudaStreamWaitEvent(side_, ev_setup_, 0));
+    for (const Writeback &w : writeback_) CK(cudaMemcpyAsync(w.dst, w.src, w.bytes, cudaMemcpyDeviceToHost, side_));
+    writeback_.clear();
     return 0;
 }
 
@@ -1036,6 +1058,7 @@ int Engine::run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &
 
     // ---- setup
     if ((rc = launch_setup(opt, !opt.skip_scale))) return rc;
+    if ((rc = issue_writeback())) return rc;
     if (opt.pc == PC_LINE && opt.autotune && opt.force_lanes <= 0) {
         bool rs_only = true;
         for (int q = 0; q < 4; ++q) {

@@ -202,6 +202,18 @@ private:
     int dev_ = -1, sms_ = 0;
     CellOcc occ_[2] = {};  // resident blocks per SM of each cell kernel, [fp32]
     cudaStream_t stream_ = nullptr;
+    // Copy-back of the unit-scaled A/B to host arrays: A and B are final once
+    // the setup has scaled them, so the copies run on a side stream during the
+    // iterations.
+    struct Writeback {
+        void *dst;
+        const void *src;
+        size_t bytes;
+    };
+    std::vector<Writeback> writeback_;
+    cudaStream_t side_ = nullptr;
+    cudaEvent_t ev_setup_ = nullptr;
+    int issue_writeback();
     cudaEvent_t ev_a_ = nullptr, ev_b_ = nullptr, ev_t0_ = nullptr, ev_t1_ = nullptr;
     DeviceArena arena_;     // iteration vectors and other per-solve work memory
     DeviceArena in_arena_;  // device copies of host inputs (A_M, B_M, VAR)

@@ -440,6 +440,7 @@ int Engine::run_batch_live(const std::vector<SystemSpec> &specs, const SolveOpti
             live_tune_ = false;
             return rc;
         }
+        if ((rc = issue_writeback())) return rc;  // A/B are scaled: copy them back meanwhile
         done.clear();
         if ((rc = live_collect(done, false))) return rc;
         for (const LiveDone &d : done) {
