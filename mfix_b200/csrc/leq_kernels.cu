@@ -514,7 +514,10 @@ __device__ __forceinline__ vec2_t<T> mk2(T a, T b)
 
 // The operands of rows c and c+1 (c even) of one J-line.  Used when JMAX2 is
 // even: then both cells share i and k, DIMENSION_3 is even so every diagonal's
-// pair is aligned, and so are the pairs at the i and k neighbours.
+// pair is aligned, and so are the pairs at the i and k neighbours.  (A pair
+// form for odd JMAX2, whose cells may straddle two lines, needs one-by-one loads
+// of the i and k neighbours; in the same kernel it slowed the even form by
+// 10-25%.)
 __device__ __forceinline__ bool pair_rows(const SysDev &d) { return (d.jmax2 & 1) == 0; }
 
 template <typename T>
@@ -1324,11 +1327,12 @@ struct LineJob {
 // pair: the two-row instance, which takes systems with an even JMAX2 only (the
 // one-row instance takes every system).  thread: the one-lane-per-line kernel,
 // which takes the systems with one lane per line (the warp kernels the others).
+// pf: the system of `item` when the caller has already loaded it, else -1.
 __device__ __forceinline__ bool next_line_job(const BatchView &b, const WaveArgs &w, int item, int step, int total,
-                                              int lane, bool pair, bool thread, LineJob &j)
+                                              int lane, bool pair, bool thread, LineJob &j, int pf = -1)
 {
-    for (; item < total; item += step) {
-        const int sidx = (w.kind == 0) ? __ldg(b.line_sys + item) : 0;
+    for (; item < total; item += step, pf = -1) {
+        const int sidx = (w.kind == 0) ? (pf >= 0 ? pf : __ldg(b.line_sys + item)) : 0;
         if (!gate_ok(b.st[sidx], w.gate)) continue;
         const SysDev &d = b.sys[sidx];
         if ((d.lane_group == 1) != thread) continue;
@@ -1462,6 +1466,18 @@ __global__ void k_line_factor(BatchView b, const int *all_line_prefix)
     }
 }
 
+// Asynchronous global -> shared copy of B bytes (4, 8 or 16); src_bytes = 0
+// fills the destination with zeros and reads nothing.
+template <int B>
+__device__ __forceinline__ void cp_async(void *smem_dst, const void *gmem_src, int src_bytes)
+{
+    const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], %2, %3;\n" ::"r"(dst), "l"(gmem_src), "n"(B), "r"(src_bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
 // ------------------------------------------------------------------ J-line half-sweep
 // One warp handles 32/G lines, G lanes per line; lane g owns the c rows
 // g*c .. g*c+c-1.  Each recurrence is split in three: a pass over the lane's rows
@@ -1481,8 +1497,11 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
     const int total = (w.kind == 0) ? b.line_prefix[b.nsys] : w.count;
     const int step = gridDim.x * nwarps;
     LineJob j;
-    for (int item = blockIdx.x * nwarps + warp; next_line_job(b, w, item, step, total, lane, PAIR, false, j);
+    int pf = -1;
+    for (int item = blockIdx.x * nwarps + warp; next_line_job(b, w, item, step, total, lane, PAIR, false, j, pf);
          item = j.item + step) {
+        // the next item's system, loaded while this one is processed
+        pf = (w.kind == 0 && j.item + step < total) ? __ldg(b.line_sys + j.item + step) : -1;
         const SysDev &d = b.sys[j.sidx];
         SysState &st = b.st[j.sidx];
         const LineCtx<T> x = line_ctx<T>(b, w, j);
@@ -1498,7 +1517,8 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
 
         // ---- load (coalesced over the line): right-hand side and factors.  With an
         // even JMAX2 every line starts on an even cell, so lanes read two rows per
-        // access; otherwise U single rows at a time.
+        // access; otherwise U single rows at a time.  The loads do not wait for the
+        // line's pivot flag (a flagged line ignores them).
         if constexpr (PAIR) {  // L is even
             constexpr int U2 = 1;  // one row pair per lane and pass: FP32 fits 80 registers
             using V2 = vec2_t<T>;
@@ -1506,12 +1526,18 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
             const T *rhs_l = x.rhs + x.base, *am1_l = x.a + 2 * x.n + x.base, *ap1_l = x.a + 4 * x.n + x.base;
             const T *am3_l = x.a + x.base, *ap3_l = x.a + 6 * x.n + x.base;
             for (int r0 = 2 * gl; r0 < span; r0 += 2 * U2 * G) {
-                V2 rhs[U2], am1[U2], ap1[U2], am3[U2], ap3[U2], nim[U2], nip[U2], nkm[U2], nkp[U2], lv[U2], rv[U2],
-                    qv[U2];
+                V2 rhs[U2], am1[U2], ap1[U2], am3[U2], ap3[U2], nim[U2], nip[U2], nkm[U2], nkp[U2];
 #pragma unroll
                 for (int u = 0; u < U2; ++u) {
                     const int r = r0 + u * 2 * G;
-                    if (fast && r < L) {  // r even and L even: rows r and r+1 both on the line
+                    if (r < span) {  // factors straight to shared memory, zeros past the line (span is even: G > 1)
+                        const bool ok = j.valid && r < L;
+                        const void *z = d.fac[0];
+                        cp_async<2 * sizeof(T)>(fl + r, ok ? (const void *)(gl_ + r) : z, ok ? 2 * sizeof(T) : 0);
+                        cp_async<2 * sizeof(T)>(fr + r, ok ? (const void *)(gr_ + r) : z, ok ? 2 * sizeof(T) : 0);
+                        cp_async<2 * sizeof(T)>(fq + r, ok ? (const void *)(gq_ + r) : z, ok ? 2 * sizeof(T) : 0);
+                    }
+                    if (j.valid && r < L) {  // r even and L even: rows r and r+1 both on the line
                         rhs[u] = ld2(rhs_l + r);
                         am1[u] = ld2(am1_l + r);
                         ap1[u] = ld2(ap1_l + r);
@@ -1523,16 +1549,13 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
                             nkm[u] = ld2(x.nb_km + r);
                             nkp[u] = ld2(x.nb_kp + r);
                         }
-                        lv[u] = ld2(gl_ + r);
-                        rv[u] = ld2(gr_ + r);
-                        qv[u] = ld2(gq_ + r);
                     }
                 }
 #pragma unroll
                 for (int u = 0; u < U2; ++u) {
                     const int r = r0 + u * 2 * G;
                     if (r < span) {
-                        T f0 = T(0), f1 = T(0), l0 = T(0), l1 = T(0), s0 = T(0), s1 = T(0), q0 = T(0), q1 = T(0);
+                        T f0 = T(0), f1 = T(0);
                         if (fast && r < L) {
                             f0 = rhs[u].x - am1[u].x * nim[u].x;
                             f1 = rhs[u].y - am1[u].y * nim[u].y;
@@ -1544,23 +1567,8 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
                                 f0 = f0 - ap3[u].x * nkp[u].x;
                                 f1 = f1 - ap3[u].y * nkp[u].y;
                             }
-                            l0 = lv[u].x;
-                            l1 = lv[u].y;
-                            s0 = rv[u].x;
-                            s1 = rv[u].y;
-                            q0 = qv[u].x;
-                            q1 = qv[u].y;
                         }
-                        f[r] = f0;
-                        fl[r] = l0;
-                        fr[r] = s0;
-                        fq[r] = q0;
-                        if (r + 1 < span) {  // an odd span (one lane per line) ends on an even row
-                            f[r + 1] = f1;
-                            fl[r + 1] = l1;
-                            fr[r + 1] = s1;
-                            fq[r + 1] = q1;
-                        }
+                        st2(f + r, mk2<T>(f0, f1));
                     }
                 }
             }
@@ -1573,7 +1581,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
 #pragma unroll
                 for (int u = 0; u < U; ++u) {
                     const int r = r0 + u * G;
-                    if (fast && r < L) {
+                    if (j.valid && r < L) {
                         rhs[u] = rhs_l[r];
                         am1[u] = am1_l[r];
                         ap1[u] = ap1_l[r];
@@ -1614,6 +1622,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
                 }
             }
         }
+        if constexpr (PAIR) cp_async_wait_all();
         __syncwarp();
 
         // ---- forward recurrence y_r = f_r - l_r y_{r-1}
