@@ -45,6 +45,8 @@ WORKLOADS = {
     "pressure_192x384x192": dict(kind="pressure_like", dims=(192, 384, 192), seed=0, itmax=5000, tol=1e-8),
     # 512 independent convection-diffusion systems, per-axis sizes U{16..96}, seeds 0..511
     "batch_512": dict(kind="batch", count=512, seed=0, itmax=500, tol=1e-8),
+    # its first 64 systems (1.25e7 cells): the profiling case of the batched kernels
+    "batch_64": dict(kind="batch", count=64, seed=0, itmax=500, tol=1e-8),
     # Poisson request stream: sizes log-uniform per axis on [24, 160], 20% pressure-like,
     # TOL from {1e-6, 1e-8}, 150 GB HBM admission budget
     "serve_poisson": dict(kind="serve", rate=2000.0, seconds=15.0, pool=64, seed=0, budget=150e9),
