@@ -49,9 +49,11 @@ int mfixgpu_init_geometry(const int *imax2, const int *jmax2, const int *kmax2, 
  * reference, CHARACTER lengths appended by value.  METHOD 2 (BiCGSTAB,
  * :137-153) is served; METHOD 4 (:161-171) is served while BiCGSTAB does not
  * break down, and returns MFIXGPU_ERR_UNSUPPORTED where the reference would
- * fall back to GMRES; others return MFIXGPU_ERR_UNSUPPORTED.  As in
- * model/leq_bicgs.f:194-233, A_M(:,:,M) and B_M(:,M) come back unit-scaled
- * (option "write_back_ab"). */
+ * fall back to GMRES; METHOD 5 (CG, :173-176, model/leq_cg.f) is served in
+ * FP64 whatever the "precision" option; others return MFIXGPU_ERR_UNSUPPORTED.
+ * As in model/leq_bicgs.f:194-233 (BiCGSTAB: rows divided by max|A(ijk,:)|) and
+ * model/leq_cg.f:197-211 (CG: rows divided by A(ijk,0)), A_M(:,:,M) and B_M(:,M)
+ * come back unit-scaled (option "write_back_ab"). */
 void mfixgpu_solve_lin_eq_(const char *vname, const int *vno, double *var, double *a_m, double *b_m,
                            const int *m, const int *itmax, const int *method, const char *sweep,
                            const double *tol1, const char *pc, int *ier, size_t vname_len, size_t sweep_len,

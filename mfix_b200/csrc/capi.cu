@@ -142,9 +142,9 @@ void solve_impl(int vno, double *var, double *a_m, double *b_m, int m, int itmax
         g.err = "phase index M outside 0:DIMENSION_M";
         return finish(MFIXGPU_ERR_ARGS);
     }
-    // model/solve_lin_eq.f:131-191
-    if (method != 2 && method != 4) {
-        g.err = "LEQ_METHOD " + std::to_string(method) + " is not served by the GPU path (BiCGSTAB only)";
+    // model/solve_lin_eq.f:131-191: BiCGSTAB (2), BiCGSTAB then GMRES (4), CG (5)
+    if (method != 2 && method != 4 && method != 5) {
+        g.err = "LEQ_METHOD " + std::to_string(method) + " is not served by the GPU path (BiCGSTAB and CG)";
         return finish(MFIXGPU_ERR_UNSUPPORTED);
     }
     const int pc = decode_pc(pc4);
@@ -167,7 +167,9 @@ void solve_impl(int vno, double *var, double *a_m, double *b_m, int m, int itmax
     s.tol = tol;
     s.itmax = itmax;
     std::vector<SolveResult> out;
-    const int rc = e->solve({s}, make_opts(g.opt, pc, sweep4), out);
+    SolveOptions so = make_opts(g.opt, pc, sweep4);
+    so.method = method == 5 ? 5 : 2;
+    const int rc = e->solve({s}, so, out);
     if (rc) {
         g.err = e->last_error();
         return finish(rc);

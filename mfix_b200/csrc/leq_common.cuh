@@ -119,6 +119,7 @@ struct SysState {
     int restart;          // mixed form: next reliable update restarts the Krylov process (Rtilde = R)
     int stall;            // mixed form: reliable updates since the best true residual improved by 10%
     int mixed;            // 1: mixed form (setup ends in PH_OUTER), 0: FP64 drop-in
+    int method;           // LEQ_METHOD: 2 BiCGSTAB, 5 CG
     int line_skips;       // J-lines left unchanged because DGTSV reported INFO != 0
     int line_fallbacks;   // J-lines solved by the sequential pivoting path
     int err;

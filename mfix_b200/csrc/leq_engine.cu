@@ -306,6 +306,7 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         st.status = ST_RUNNING;
         st.phase = opt.skip_scale ? PH_INIT : PH_SETUP;
         st.mixed = mixed ? 1 : 0;
+        st.method = opt.method;
         st.inner_tol = opt.inner_tol;
         st.growth_limit = opt.mixed_growth;
         st.stall_limit = opt.mixed_stalls;
@@ -889,6 +890,8 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
     }
     SolveOptions o = opt;
     o.on_device = true;
+    if (opt.method != 2 && opt.method != 5) return fail("LEQ_METHOD not served (2 BiCGSTAB, 5 CG)", -10);
+    if (opt.method == 5) o.precision = PREC_FP64;  // CG runs the FP64 reference form only
     writeback_.clear();
     if (!opt.on_device && opt.write_back_ab)
         for (size_t q = 0; q < specs.size(); ++q) {
@@ -903,13 +906,14 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
         const char ch = opt.sweep[q];
         if (ch == 'I' || ch == 'i' || ch == 'K' || ch == 'k' || ch == 'A' || ch == 'a') rs_only = false;
     }
-    int rc = (specs.size() > 1 && rs_only && !opt.time_kernels) ? run_batch_live(dev, o, out) : run_batch(dev, o, out);
+    int rc = (specs.size() > 1 && rs_only && !opt.time_kernels && opt.method == 2) ? run_batch_live(dev, o, out)
+                                                                                   : run_batch(dev, o, out);
     if (rc) return rc;
     SolveTiming total = timing_;
 
     // mixed form: systems whose FP32 iteration gave up are solved again by the
     // FP64 drop-in, from their initial guess
-    if (opt.precision == PREC_MIXED) {
+    if (o.precision == PREC_MIXED) {
         std::vector<SystemSpec> fb;
         std::vector<int> idx;
         for (size_t q = 0; q < out.size(); ++q)
@@ -975,8 +979,9 @@ int Engine::issue_writeback()
 int Engine::launch_setup(const SolveOptions &opt, bool scale)
 {
     const bool mixed = opt.precision == PREC_MIXED;
+    const bool cg = opt.method == 5;
     if (scale) {
-        CK(launch_scale(view_, cfg_));
+        CK(cg ? launch_scale_diag(view_, cfg_) : launch_scale(view_, cfg_));
         CK(launch_after_scale(view_, cfg_));
         launches_ += 2;
     }
@@ -987,6 +992,9 @@ int Engine::launch_setup(const SolveOptions &opt, bool scale)
     }
     if (mixed) {
         CK(launch_to_f32(view_, cfg_));
+        launches_ += 1;
+    } else if (cg) {  // R = B - A Var and Rnorm0 (model/leq_cg.f:236-259)
+        CK(launch_init_residual<double>(view_, cfg_));
         launches_ += 1;
     } else {
         CK(launch_init_residual<double>(view_, cfg_));
@@ -1012,7 +1020,15 @@ int Engine::launch_body(const SolveOptions &opt)
         CK(call);     \
         kt_end(kc);   \
     } while (0)
-    if (mixed) {
+    if (opt.method == 5) {  // LEQ_CG0, model/leq_cg.f:271-410
+        const int z_id = opt.pc == PC_NONE ? V_R : V_PH;
+        if ((r = run_msolve_plan(0, 8))) return r;
+        launches_ += 4 - ((mixed ? 6 : 5) + 2 * (cfg_.rows_pair + cfg_.rows_single - 1));
+        TK(KC_S_UPDATE, launch_cg_rho(view_, cfg_, z_id));
+        TK(KC_P_UPDATE, launch_cg_p(view_, cfg_, z_id));
+        TK(KC_MATVEC_ALPHA, launch_cg_matvec(view_, cfg_));
+        TK(KC_XR_UPDATE, launch_cg_xr(view_, cfg_));
+    } else if (mixed) {
         TK(KC_OUTER, launch_outer_step(view_, cfg_));
         TK(KC_P_UPDATE, (launch_p_update<float, true>(view_, cfg_)));
         if ((r = run_msolve_plan(0, 4))) return r;
@@ -1046,8 +1062,13 @@ int Engine::run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &
     const int gate_p = G_INNER, gate_s = G_INNER_NOSNORM;
     h_lines_.clear();
     list_refs_.clear();
-    if ((rc = plan_msolve(opt, V_P, V_PH, gate_p, 0))) return rc;
-    if ((rc = plan_msolve(opt, V_S, V_SH, gate_s, 1))) return rc;
+    auto plans = [&]() -> int {
+        int r;
+        if (opt.method == 5) return plan_msolve(opt, V_R, V_PH, gate_p, 0);  // Z = MSOLVE(R)
+        if ((r = plan_msolve(opt, V_P, V_PH, gate_p, 0))) return r;
+        return plan_msolve(opt, V_S, V_SH, gate_s, 1);
+    };
+    if ((rc = plans())) return rc;
     if ((rc = bind_lists())) return rc;
 
     ktime_ = opt.time_kernels;
@@ -1069,8 +1090,7 @@ int Engine::run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &
             if ((rc = autotune_lines(opt, elem))) return rc;
             h_lines_.clear();
             list_refs_.clear();
-            if ((rc = plan_msolve(opt, V_P, V_PH, gate_p, 0))) return rc;
-            if ((rc = plan_msolve(opt, V_S, V_SH, gate_s, 1))) return rc;
+            if ((rc = plans())) return rc;
             if ((rc = bind_lists())) return rc;
         }
     }

@@ -48,6 +48,7 @@ struct SolveResult {
 };
 
 struct SolveOptions {
+    int method = 2;              // LEQ_METHOD: 2 BiCGSTAB (model/leq_bicgs.f), 5 CG (model/leq_cg.f, FP64 only)
     int pc = PC_LINE;
     char sweep[4] = {'R', 'S', 'R', 'S'};
     int precision = PREC_FP64;

@@ -257,6 +257,26 @@ __global__ void k_after_scale(BatchView b)
     st.phase = PH_INIT;
 }
 
+// LEQ_CG0 (model/leq_cg.f): IER rules after the loop (:443-450): REAL() values in the ratio test.
+__device__ inline void cg_final(SysState &s)
+{
+    s.ier = -1;
+    s.iter_tot_add = s.iter;
+    if ((double)(float)s.rnorm >= (double)0.2f * (double)(float)s.rnorm0) s.ier = -2;
+    s.exit_kind = EX_ITMAX;
+    s.status = ST_DONE;
+}
+
+// Entry to the loop (:269-271).
+__device__ inline void cg_begin(SysState &s)
+{
+    s.i = 1;
+    s.iter = 1;
+    s.rnorm = 0.0;
+    s.phase = PH_INNER;
+    if (s.itmax < 1) cg_final(s);
+}
+
 // End of the setup: the FP64 drop-in enters the loop (its Rtilde step already
 // moved it to PH_INNER unless it finished), the mixed form starts with an FP64 update.
 __global__ void k_init_done(BatchView b)
@@ -265,6 +285,10 @@ __global__ void k_init_done(BatchView b)
     if (s >= b.nsys) return;
     SysState &st = b.st[s];
     if (!gate_ok(st, G_INIT)) return;
+    if (st.method == 5) {  // LEQ_CG0
+        cg_begin(st);
+        return;
+    }
     // a nearly singular operator (pressure correction) goes to the FP64 drop-in
     // before any FP32 iteration: its FP32 Krylov process stagnates
     if (st.mixed && __uint_as_float(st.margin_bits) < st.min_margin) {
@@ -1938,8 +1962,215 @@ __global__ void k_dot(const double *x, const double *y, int64_t n, double *parti
     }
 }
 
+// ------------------------------------------------------------------ LEQ_CG0 (METHOD 5)
+// Preconditioned conjugate gradients, FP64 (model/leq_cg.f:96-455).  One
+// iteration is Z = MSOLVE(R) (the J-line machinery), then four kernels:
+// rho = (R, Z); P = Z + beta P; Q = A P with (P, Q); R -= alpha Q, X += alpha P
+// with (R, R).
+
+// Unit scaling by the reciprocal of each row's diagonal, no zero test (:197-211).
+__global__ void k_scale_diag(BatchView b)
+{
+    for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+        const Tile tl = b.tiles[t];
+        const SysDev &d = b.sys[tl.sys];
+        if (!gate_ok(b.st[tl.sys], G_SETUP)) continue;
+        const int64_t n = d.n;
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(n, c0 + TILE_CELLS);
+        #pragma unroll 4
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+            const double oam = 1.0 / d.a64[3 * n + c];
+#pragma unroll
+            for (int q = 0; q < 7; ++q) d.a64[q * n + c] = d.a64[q * n + c] * oam;
+            d.b64[c] = d.b64[c] * oam;
+        }
+    }
+}
+
+// rho(i-1) = (R, Z), its zero test and beta(i-1) (:276-325).
+__global__ void __launch_bounds__(256) k_cg_rho(BatchView b, int z_id)
+{
+    TileRun run{-1, 0};
+    auto fin = [&](SysState &st, const double(&tot)[1]) {
+        const double rho = tot[0];
+        if (rho == 0.0) {  // :294-303, no ITER_TOT update
+            st.ier = (st.i != 1) ? -2 : 0;
+            st.exit_kind = EX_RHO0;
+            st.status = ST_DONE;
+            return;
+        }
+        st.beta = (st.i == 1) ? 0.0 : rho / st.rho;
+        st.rho = rho;
+    };
+    for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+        const Tile tl = b.tiles[t];
+        const SysDev &d = b.sys[tl.sys];
+        if (!gate_ok(b.st[tl.sys], G_INNER)) continue;
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
+        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
+        const double *__restrict__ r = vec<double>(d, V_R) + c0;
+        const double *__restrict__ z = vec<double>(d, z_id) + c0;
+        double v[1] = {0.0};
+        const int np = cnt >> 1;
+        for (int q = threadIdx.x; q < np; q += blockDim.x) {
+            const double2 rv = ld2(r + 2 * q), zv = ld2(z + 2 * q);
+            v[0] += rv.x * zv.x;
+            v[0] += rv.y * zv.y;
+        }
+        if ((cnt & 1) && threadIdx.x == 0) v[0] += r[cnt - 1] * z[cnt - 1];
+        tile_partial<1>(b, d, tl.idx, v);
+        run_add<1>(b, run, tl.sys, fin);
+    }
+    run_close<1>(b, run, fin);
+}
+
+// P = Z (i = 1) or P = Z + beta P (:305-334).
+__global__ void __launch_bounds__(256) k_cg_p(BatchView b, int z_id)
+{
+    for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+        const Tile tl = b.tiles[t];
+        const SysDev &d = b.sys[tl.sys];
+        const SysState &st = b.st[tl.sys];
+        if (!gate_ok(st, G_INNER)) continue;
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
+        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
+        const double *__restrict__ z = vec<double>(d, z_id) + c0;
+        double *__restrict__ p = vec<double>(d, V_P) + c0;
+        const bool first = st.i == 1;
+        const double beta = st.beta;
+        const int np = cnt >> 1;
+        for (int q = threadIdx.x; q < np; q += blockDim.x) {
+            const double2 zv = ld2(z + 2 * q);
+            if (first) {
+                st2(p + 2 * q, zv);
+            } else {
+                const double2 pv = ld2(p + 2 * q);
+                st2(p + 2 * q, mk2<double>(zv.x + beta * pv.x, zv.y + beta * pv.y));
+            }
+        }
+        if ((cnt & 1) && threadIdx.x == 0) p[cnt - 1] = first ? z[cnt - 1] : z[cnt - 1] + beta * p[cnt - 1];
+    }
+}
+
+// Q = A P and alpha(i) = rho(i-1) / (P, Q) (:336-354).
+__global__ void __launch_bounds__(256) k_cg_matvec(BatchView b)
+{
+    constexpr int U = 2;
+    TileRun run{-1, 0};
+    auto fin = [&](SysState &st, const double(&tot)[1]) { st.alpha = st.rho / tot[0]; };
+    for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+        const Tile tl = b.tiles[t];
+        const SysDev &d = b.sys[tl.sys];
+        if (!gate_ok(b.st[tl.sys], G_INNER)) continue;
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
+        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
+        const double *__restrict__ a = d.a64;
+        const double *__restrict__ p = vec<double>(d, V_P);
+        double *__restrict__ q = vec<double>(d, V_V);
+        double v[1] = {0.0};
+        for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
+            Row7<double> rw[U];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int c = base + u * blockDim.x;
+                if (c < cnt) load_row7<double, double>(d, a, p, c0 + c, rw[u]);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int c = base + u * blockDim.x;
+                if (c < cnt) {
+                    const double yv = dot_row7<double>(rw[u], d.do_k);
+                    q[c0 + c] = yv;
+                    v[0] += rw[u].x[2] * yv;  // x[2] is P at the cell itself
+                }
+            }
+        }
+        tile_partial<1>(b, d, tl.idx, v);
+        run_add<1>(b, run, tl.sys, fin);
+    }
+    run_close<1>(b, run, fin);
+}
+
+// R = R - alpha Q, Var = Var + alpha P, Rnorm and the convergence test (:356-410).
+__global__ void __launch_bounds__(256) k_cg_xr(BatchView b)
+{
+    TileRun run{-1, 0};
+    auto fin = [&](SysState &st, const double(&tot)[1]) {
+        st.rnorm = sqrt(tot[0]);
+        if (st.rnorm <= st.tol * st.rnorm0) {  // :396-401
+            st.iter_tot_add = st.iter + 1;
+            st.ier = 0;
+            st.exit_kind = EX_RNORM;
+            st.status = ST_DONE;
+            return;
+        }
+        st.iter += 1;
+        st.i += 1;
+        if (st.i > st.itmax) cg_final(st);
+    };
+    for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+        const Tile tl = b.tiles[t];
+        const SysDev &d = b.sys[tl.sys];
+        const SysState &st = b.st[tl.sys];
+        if (!gate_ok(st, G_INNER)) continue;
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
+        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
+        const double alpha = st.alpha;
+        double *__restrict__ r = vec<double>(d, V_R) + c0;
+        double *__restrict__ x = vec<double>(d, V_X) + c0;
+        const double *__restrict__ p = vec<double>(d, V_P) + c0;
+        const double *__restrict__ q = vec<double>(d, V_V) + c0;
+        double v[1] = {0.0};
+        const int np = cnt >> 1;
+        for (int k = threadIdx.x; k < np; k += blockDim.x) {
+            const double2 rv = ld2(r + 2 * k), qv = ld2(q + 2 * k), xv = ld2(x + 2 * k), pv = ld2(p + 2 * k);
+            const double r0 = rv.x - alpha * qv.x, r1 = rv.y - alpha * qv.y;
+            st2(r + 2 * k, mk2<double>(r0, r1));
+            st2(x + 2 * k, mk2<double>(xv.x + alpha * pv.x, xv.y + alpha * pv.y));
+            v[0] += r0 * r0;
+            v[0] += r1 * r1;
+        }
+        if ((cnt & 1) && threadIdx.x == 0) {
+            const int c = cnt - 1;
+            const double rv = r[c] - alpha * q[c];
+            r[c] = rv;
+            x[c] = x[c] + alpha * p[c];
+            v[0] += rv * rv;
+        }
+        tile_partial<1>(b, d, tl.idx, v);
+        run_add<1>(b, run, tl.sys, fin);
+    }
+    run_close<1>(b, run, fin);
+}
+
 // ------------------------------------------------------------------ launchers
 #define CHECK_LAUNCH() return cudaGetLastError()
+
+cudaError_t launch_scale_diag(const BatchView &b, const LaunchCfg &c)
+{
+    k_scale_diag<<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b);
+    CHECK_LAUNCH();
+}
+cudaError_t launch_cg_rho(const BatchView &b, const LaunchCfg &c, int z_id)
+{
+    k_cg_rho<<<c.g_p, CELL_THREADS, 0, c.stream>>>(b, z_id);
+    CHECK_LAUNCH();
+}
+cudaError_t launch_cg_p(const BatchView &b, const LaunchCfg &c, int z_id)
+{
+    k_cg_p<<<c.g_p, CELL_THREADS, 0, c.stream>>>(b, z_id);
+    CHECK_LAUNCH();
+}
+cudaError_t launch_cg_matvec(const BatchView &b, const LaunchCfg &c)
+{
+    k_cg_matvec<<<c.g_mv, CELL_THREADS, 0, c.stream>>>(b);
+    CHECK_LAUNCH();
+}
+cudaError_t launch_cg_xr(const BatchView &b, const LaunchCfg &c)
+{
+    k_cg_xr<<<c.g_xr, CELL_THREADS, 0, c.stream>>>(b);
+    CHECK_LAUNCH();
+}
 
 cudaError_t launch_scale(const BatchView &b, const LaunchCfg &c)
 {

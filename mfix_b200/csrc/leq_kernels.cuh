@@ -38,10 +38,17 @@ cudaError_t launch_scale(const BatchView &b, const LaunchCfg &c);
 cudaError_t launch_after_scale(const BatchView &b, const LaunchCfg &c);
 cudaError_t launch_to_f32(const BatchView &b, const LaunchCfg &c);
 cudaError_t launch_init_done(const BatchView &b, const LaunchCfg &c);
+cudaError_t launch_scale_diag(const BatchView &b, const LaunchCfg &c);  // LEQ_CG0's scaling by A(0)
 template <typename T>
 cudaError_t launch_init_residual(const BatchView &b, const LaunchCfg &c);  // R = B - A X, ||R||
 template <typename T>
 cudaError_t launch_init_rtilde(const BatchView &b, const LaunchCfg &c, uint64_t seed);  // Rtilde, rho(0)
+
+// One CG iteration after Z = MSOLVE(R) (model/leq_cg.f:271-410), FP64
+cudaError_t launch_cg_rho(const BatchView &b, const LaunchCfg &c, int z_id);  // rho = (R, Z), beta
+cudaError_t launch_cg_p(const BatchView &b, const LaunchCfg &c, int z_id);    // P = Z + beta P
+cudaError_t launch_cg_matvec(const BatchView &b, const LaunchCfg &c);         // Q = A P, alpha
+cudaError_t launch_cg_xr(const BatchView &b, const LaunchCfg &c);             // R, Var, Rnorm, exit
 
 // J-line LU factors (l, 1/u, c/u) and DGTSV pivot flags, once per solve
 template <typename T>

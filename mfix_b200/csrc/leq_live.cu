@@ -168,6 +168,7 @@ int Engine::live_add(const LiveSystem &ls)
     st.status = ST_RUNNING;
     st.phase = ls.scaled ? PH_INIT : PH_SETUP;
     st.mixed = mixed ? 1 : 0;
+    st.method = live_opt_.method;
     st.inner_tol = live_opt_.inner_tol;
     st.growth_limit = live_opt_.mixed_growth;
     st.stall_limit = live_opt_.mixed_stalls;

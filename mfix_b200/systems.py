@@ -155,6 +155,26 @@ def conv_diff(imax: int, jmax: int, kmax: int, seed: int = 0, do_k: bool = True,
                   "conv_diff")
 
 
+def diffusion_sym(imax: int, jmax: int, kmax: int, seed: int = 0, do_k: bool = True, delta: float = 1e-3,
+                  itmax: int = 500, tol: float = 1e-8) -> System:
+    """Symmetric 7-point diffusion, face coefficient D ~ U[0.5, 1.5], with one
+    centre for every interior row: -(largest row sum)(1 + delta).  Dividing
+    each row by its diagonal (LEQ_CG0's scaling, model/leq_cg.f:197-211) then
+    keeps the operator symmetric, which conjugate gradients needs; rows with
+    different diagonals would make the scaled operator non-symmetric."""
+    imax2, jmax2, kmax2 = _grid(imax, jmax, kmax, do_k)
+
+    def face(axis, lo, hi):
+        c = 0.5 + uniform(seed, 70 + axis, lo)
+        return c, c
+
+    a, b = _assemble(imax2, jmax2, kmax2, do_k, face, 1.0, seed, 74)
+    interior = _interior(imax2, jmax2, kmax2, do_k).reshape(-1)
+    a[3][interior] = -(1.0 + delta) * np.max(-a[3][interior])
+    return System(imax2, jmax2, kmax2, int(do_k), a, b, np.zeros(imax2 * jmax2 * kmax2), tol, itmax,
+                  "diffusion_sym")
+
+
 def void_fraction(imax2, jmax2, kmax2, seed, nspheres=40, rmin=6.0, rmax=20.0):
     """eps_g field: 0.4 background, spheres of eps_g = 0.95 (radius U[rmin, rmax],
     centres uniform over the interior)."""

@@ -56,6 +56,10 @@ def lib() -> C.CDLL:
         L.orc_leq_bicgs_sample.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_char_p, C.c_double, C.c_char_p,
                                            C.c_int, C.c_uint64, C.c_int, C.POINTER(Stats)]
         L.orc_leq_bicgs_sample.restype = C.c_int
+        L.orc_leq_cg.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_char_p, C.c_double, C.c_char_p, C.c_int,
+                                 C.POINTER(Stats)]
+        L.orc_leq_cg.restype = C.c_int
+        L.orc_scale_diag.argtypes = [C.POINTER(Geom), vp, vp]
         L.orc_true_resid.argtypes = [C.POINTER(Geom), vp, vp, vp]
         L.orc_true_resid.restype = C.c_double
         L.orc_truth_solve.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_double, C.c_int, C.c_uint64, _dp]
@@ -131,6 +135,19 @@ def leq_bicgs(s, sweep: str = "RSRS", pc: str = "LINE", seed: int = 0x5EED, max_
         lib().orc_leq_bicgs_sample(C.byref(geom(s)), _p(s.x), _p(s.a), _p(s.b), sw, s.tol, pcs, s.itmax, seed,
                                    max_exec, C.byref(st))
     return {k: getattr(st, k) for k, _ in Stats._fields_}
+
+
+def leq_cg(s, sweep: str = "RSRS", pc: str = "LINE") -> dict:
+    """LEQ_CG (METHOD 5) on s (in place: s.x solution, s.a / s.b scaled by the diagonal)."""
+    st = Stats()
+    lib().orc_leq_cg(C.byref(geom(s)), _p(s.x), _p(s.a), _p(s.b), sweep.ljust(4)[:4].encode(), s.tol,
+                     pc.ljust(4)[:4].encode(), s.itmax, C.byref(st))
+    return {k: getattr(st, k) for k, _ in Stats._fields_}
+
+
+def scale_diag(s) -> None:
+    """LEQ_CG0's unit scaling of s in place (rows divided by their diagonal)."""
+    lib().orc_scale_diag(C.byref(geom(s)), _p(s.a), _p(s.b))
 
 
 def true_resid(s, x: np.ndarray, a: np.ndarray | None = None, b: np.ndarray | None = None) -> float:

@@ -380,6 +380,21 @@ int orc_scale(const orc_geom *g, double *a, double *b)
     return bad ? -2 : 0;
 }
 
+/* ------------------------------------------------------------------ LEQ_CG0 unit scaling */
+/* model/leq_cg.f:197-211: every row multiplied by the reciprocal of its diagonal
+ * A(ijk,0), with no zero test (a zero diagonal gives infinities, as in the
+ * reference). */
+void orc_scale_diag(const orc_geom *g, double *a, double *b)
+{
+    const int64_t n = g->n;
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < n; ++p) {
+        const double oam = 1.0 / a[3 * n + p];
+        for (int d = 0; d < 7; ++d) a[(int64_t)d * n + p] = a[(int64_t)d * n + p] * oam;
+        b[p] = b[p] * oam;
+    }
+}
+
 /* ------------------------------------------------------------------ LEQ_BICGS0 */
 #define SMALL_NUMBER 1.0e-15
 #define RATIOTOL ((double)0.2f) /* DOUBLE PRECISION, PARAMETER :: ratiotol = 0.2 (a REAL literal) */
@@ -652,4 +667,100 @@ int orc_truth_solve(const orc_geom *g, const double *a, const double *b, double 
     if (final_rel) *final_rel = rel;
     free(work);
     return rel <= rtol ? steps : -1;
+}
+
+/* ------------------------------------------------------------------ LEQ_CG0 */
+/* Preconditioned conjugate gradients, METHOD 5 of SOLVE_LIN_EQ
+ * (model/solve_lin_eq.f:173-176, model/leq_cg.f:96-455).  PC dispatch :62-76;
+ * R = B - A Var and Rnorm0 :236-259; per iteration Z = MSOLVE(R) :274,
+ * rho = (R, Z) with the rho == 0 exit :294-303 (IER 0 at i = 1, else -2, no
+ * ITER_TOT update), P = Z or Z + beta P :305-334, Q = A P, alpha = rho / (P, Q)
+ * :336-354, R -= alpha Q and Var += alpha P :366-367, Rnorm and the
+ * convergence test :396-401; IER rules after the loop :443-450 (the ratio test
+ * on REAL() values, ratiotol a REAL literal). */
+int orc_leq_cg(const orc_geom *g, double *var, double *a, double *b, const char *sweep, double tol,
+               const char *pc, int itmax, orc_stats *st)
+{
+    memset(st, 0, sizeof(*st));
+    st->exit_kind = -1;
+    const int mode = pc_mode(pc);
+    if (mode < 0) {
+        st->ier = -10;
+        return -10;
+    }
+    const int64_t n = g->n;
+    orc_scale_diag(g, a, b);
+    double *work = (double *)calloc((size_t)(4 * n), sizeof(double));
+    double *R = work, *P = work + n, *Z = work + 2 * n, *Q = work + 3 * n;
+    orc_matvec(g, a, var, R);
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < n; ++p) R[p] = b[p] - R[p];
+    const double rnorm0 = sqrt(orc_dot(R, R, n));
+
+    double rnorm = 0.0, rho_m2 = 0.0;
+    int iter = 1, converged = 0, iter_tot_add = 0, exit_kind = 3;
+    for (int i = 1; i <= itmax; ++i) {
+        const double *Zp = R;
+        if (mode == 2) {
+            if (orc_msolve(g, R, a, Z, sweep, &st->line_info_skips) != 0) {
+                st->ier = -12;
+                free(work);
+                return -12;
+            }
+            Zp = Z;
+        } else if (mode == 1) {
+            orc_msolve1(g, R, a, Z);
+            Zp = Z;
+        }
+        const double rho = orc_dot(R, Zp, n);
+        if (rho == 0.0) {
+            const int ier = (i != 1) ? -2 : 0;
+            st->ier = ier;
+            st->iterations = iter;
+            st->exit_kind = 2;
+            st->rnorm0 = rnorm0;
+            st->rnorm = rnorm;
+            free(work);
+            return ier;
+        }
+        if (i == 1) {
+#pragma omp parallel for schedule(static)
+            for (int64_t p = 0; p < n; ++p) P[p] = Zp[p];
+        } else {
+            const double beta = rho / rho_m2;
+#pragma omp parallel for schedule(static)
+            for (int64_t p = 0; p < n; ++p) P[p] = Zp[p] + beta * P[p];
+        }
+        orc_matvec(g, a, P, Q);
+        const double pxq = orc_dot(P, Q, n);
+        const double alpha = rho / pxq;
+#pragma omp parallel for schedule(static)
+        for (int64_t p = 0; p < n; ++p) {
+            R[p] = R[p] - alpha * Q[p];
+            var[p] = var[p] + alpha * P[p];
+        }
+        rnorm = sqrt(orc_dot(R, R, n));
+        if (rnorm <= tol * rnorm0) {
+            iter_tot_add = iter + 1;
+            converged = 1;
+            exit_kind = 0;
+            break;
+        }
+        ++iter;
+        rho_m2 = rho;
+    }
+    int ier = 0;
+    if (!converged) {
+        ier = -1;
+        iter_tot_add = iter;
+        if ((double)(float)rnorm >= RATIOTOL * (double)(float)rnorm0) ier = -2;
+    }
+    st->ier = ier;
+    st->iterations = iter;
+    st->iter_tot_add = iter_tot_add;
+    st->exit_kind = exit_kind;
+    st->rnorm0 = rnorm0;
+    st->rnorm = rnorm;
+    free(work);
+    return ier;
 }

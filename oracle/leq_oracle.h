@@ -54,6 +54,7 @@ int orc_msolve(const orc_geom *g, const double *b, const double *a, double *var,
                int *skips);
 void orc_msolve1(const orc_geom *g, const double *b, const double *a, double *var);
 int orc_scale(const orc_geom *g, double *a, double *b);
+void orc_scale_diag(const orc_geom *g, double *a, double *b);
 
 /* Rtilde's random stream: counter-based splitmix64, the same on CPU and GPU */
 double orc_uniform(uint64_t seed, uint64_t tag, uint64_t idx);
@@ -66,6 +67,10 @@ int orc_leq_bicgs(const orc_geom *g, double *var, double *a, double *b, const ch
 int orc_leq_bicgs_sample(const orc_geom *g, double *var, double *a, double *b, const char *sweep,
                          double tol, const char *pc, int itmax, uint64_t rt_seed, int max_exec,
                          orc_stats *st);
+
+/* LEQ_CG(VNAME,VNO,VAR,A_M,B_M,CMETHOD,TOL,PC,ITMAX,IER) on one phase slice (METHOD 5) */
+int orc_leq_cg(const orc_geom *g, double *var, double *a, double *b, const char *sweep, double tol,
+               const char *pc, int itmax, orc_stats *st);
 
 /* true residual ||b - A x||_2 in long double */
 double orc_true_resid(const orc_geom *g, const double *a, const double *b, const double *x);

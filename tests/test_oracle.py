@@ -138,3 +138,72 @@ def test_convergence_residual_below_tol():
     O.leq_bicgs(ref)
     r0 = O.true_resid(ref, np.zeros(s.n))
     assert O.true_resid(ref, ref.x) / r0 <= 1.01e-8
+
+
+# ---------------------------------------------------------------- LEQ_CG0 (METHOD 5)
+def _cg_numpy(s, k):
+    """k iterations of textbook unpreconditioned CG from x = 0 on the
+    diagonal-scaled system, numpy vector operations (an independent restatement
+    of model/leq_cg.f:271-410 with MSOLVE0)."""
+    t = s.copy()
+    O.scale_diag(t)
+    mv = lambda v: S.matvec_np(t.imax2, t.jmax2, t.kmax2, t.do_k, t.a, v)
+    x = np.zeros(t.n)
+    r = t.b - mv(x)
+    p = np.zeros(t.n)
+    rho_old = 0.0
+    for i in range(1, k + 1):
+        z = r.copy()
+        rho = float(r @ z)
+        p = z.copy() if i == 1 else z + (rho / rho_old) * p
+        q = mv(p)
+        alpha = rho / float(p @ q)
+        r = r - alpha * q
+        x = x + alpha * p
+        rho_old = rho
+    return x
+
+
+def test_cg_iterates_match_numpy():
+    s = S.diffusion_sym(12, 17, 9, seed=3)
+    for k in (1, 4, 12):
+        t = s.copy()
+        t.tol = 0.0  # never converged: the oracle runs exactly k iterations
+        t.itmax = k
+        st = O.leq_cg(t, pc="NONE")
+        assert st["iterations"] == k + 1 and st["ier"] in (-1, -2)
+        xr = _cg_numpy(s, k)
+        assert np.max(np.abs(t.x - xr)) <= 1e-10 * np.max(np.abs(xr))
+
+
+def test_cg_converges_on_symmetric_systems():
+    for dims, do_k in (((14, 20, 12), True), ((21, 19, 1), False), ((40, 3, 30), True)):
+        s = S.diffusion_sym(*dims, seed=5, do_k=do_k)
+        for pc in ("LINE", "DIAG", "NONE"):
+            t = s.copy()
+            st = O.leq_cg(t, pc=pc)
+            ref = s.copy()
+            O.scale_diag(ref)
+            assert st["ier"] == 0 and st["exit_kind"] == 0
+            assert st["iter_tot_add"] == st["iterations"] + 1
+            assert O.true_resid(ref, t.x) <= s.tol * O.true_resid(ref, np.zeros(s.n)) * 1.01
+            assert np.array_equal(t.a, ref.a) and np.array_equal(t.b, ref.b)  # rows scaled by 1/A(0)
+
+
+def test_cg_ier_rules():
+    s = S.diffusion_sym(8, 9, 7, seed=1)
+    # R = 0: rho(0) = 0 at i = 1 -> IER 0, no iteration (model/leq_cg.f:294-303)
+    t = s.copy()
+    t.b[:] = 0.0
+    st = O.leq_cg(t)
+    assert st["ier"] == 0 and st["exit_kind"] == 2 and st["iter_tot_add"] == 0
+    assert not np.any(t.x)
+    # ITMAX = 0: the loop does not run; Rnorm = 0 < 0.2 Rnorm0 -> IER -1, ITER_TOT += 1
+    t = s.copy()
+    t.itmax = 0
+    st = O.leq_cg(t)
+    assert st["ier"] == -1 and st["iter_tot_add"] == 1
+    # the reference's CG on a non-symmetric scaled operator diverges: IER -2 after ITMAX
+    p = S.pressure_like(14, 20, 12, seed=3, nspheres=4, rmin=2, rmax=5, itmax=60)
+    st = O.leq_cg(p)
+    assert st["ier"] == -2 and st["iterations"] == 61 and st["iter_tot_add"] == 61
