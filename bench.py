@@ -43,6 +43,8 @@ WORKLOADS = {
     "conv_diff_64": dict(kind="conv_diff", dims=(64, 64, 64), seed=0, itmax=500, tol=1e-8),
     "conv_diff_192": dict(kind="conv_diff", dims=(192, 192, 192), seed=0, itmax=500, tol=1e-8),
     "pressure_192x384x192": dict(kind="pressure_like", dims=(192, 384, 192), seed=0, itmax=5000, tol=1e-8),
+    # METHOD 5 (LEQ_CG, FP64): symmetric diffusion whose diagonal-scaled operator stays symmetric
+    "cg_diffusion_256": dict(kind="cg", dims=(256, 256, 256), seed=0, itmax=500, tol=1e-8),
     # 512 independent convection-diffusion systems, per-axis sizes U{16..96}, seeds 0..511
     "batch_512": dict(kind="batch", count=512, seed=0, itmax=500, tol=1e-8),
     # its first 64 systems (1.25e7 cells): the profiling case of the batched kernels
@@ -74,16 +76,31 @@ CLASS_BYTES = {
 }
 
 
-def class_table(kt: dict, cells: int, fp32: bool, peak: float) -> dict:
-    """Per kernel class: total ms, launches, mean us, achieved GB/s of algorithmic bytes, fraction of peak."""
+def work_launches(inner: int, outer: int, jline_per_iter: int = 8) -> dict:
+    """Launches of each kernel class that did work in one solve.  The host polls
+    convergence every few iterations, so some launches run after a system is
+    done, and in the mixed form the inner-iteration kernels idle while an FP64
+    update runs; those launches return at once and carry no algorithmic bytes."""
+    w = {k: inner for k in CLASS_BYTES}
+    w["jline"] = jline_per_iter * inner
+    w["outer_step"] = outer
+    return w
+
+
+def class_table(kt: dict, cells: int, fp32: bool, peak: float, work: dict) -> dict:
+    """Per kernel class: total ms over all launches, launches, launches that did
+    work, mean us per working launch, achieved GB/s of algorithmic bytes over the
+    total time, fraction of peak."""
     out = {}
     for name, (ms, n) in kt.items():
         if n == 0:
             continue
-        row = {"ms": round(ms, 3), "launches": int(n), "us_per_launch": round(1e3 * ms / n, 2)}
+        nw = min(int(work.get(name, n)), int(n))
+        row = {"ms": round(ms, 3), "launches": int(n), "work_launches": nw,
+               "us_per_launch": round(1e3 * ms / max(nw, 1), 2)}
         if name in CLASS_BYTES:
             b = CLASS_BYTES[name][0 if fp32 else 1] * cells
-            gbs = b * n / (ms / 1e3) / 1e9 if ms > 0 else 0.0
+            gbs = b * nw / (ms / 1e3) / 1e9 if ms > 0 else 0.0
             row.update({"gbs": round(gbs, 1), "frac": round(gbs / peak, 3)})
         out[name] = row
     return out
@@ -114,6 +131,8 @@ def make_system(name: str):
     i, j, k = w["dims"]
     if w["kind"] == "conv_diff":
         return S.conv_diff(i, j, k, seed=w["seed"], itmax=w["itmax"], tol=w["tol"])
+    if w["kind"] == "cg":
+        return S.diffusion_sym(i, j, k, seed=w["seed"], itmax=w["itmax"], tol=w["tol"])
     return S.pressure_like(i, j, k, seed=w["seed"], itmax=w["itmax"], tol=w["tol"])
 
 
@@ -234,6 +253,8 @@ def run_reference(args) -> None:
     w = args.workload
     if WORKLOADS[w]["kind"] in ("batch", "serve"):
         return run_reference_sample(args)
+    if WORKLOADS[w]["kind"] == "cg":
+        return run_reference_cg(args)
     sys0 = make_system(w)
     iters = FP64_ITERATIONS.get(w)
     vals = []
@@ -252,6 +273,33 @@ def run_reference(args) -> None:
                              "sample": vals[0]["sample"]},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
             "wall_s": wall, "cpu_gbs": float(np.mean([x["gbs"] for x in vals]))}
+    print(json.dumps(line), flush=True)
+
+
+def run_reference_cg(args) -> None:
+    """CPU arm of the CG workload: complete oracle LEQ_CG solves, one per step."""
+    import oracle as O
+
+    w = args.workload
+    sys0 = make_system(w)
+    vals, its = [], 0
+    for step in range(args.warmup + args.steps):
+        s = sys0.copy()
+        t0 = time.perf_counter()
+        st = O.leq_cg(s)
+        dt = time.perf_counter() - t0
+        if step >= args.warmup:
+            vals.append(1.0 / dt)
+            its = st["iterations"]
+    v = float(np.mean(vals))
+    sample = f"{args.steps} complete oracle CG solves of the {w} system ({its} iterations each)"
+    line = {"impl": "reference", "metric": "solves/s", "value": v, "unit": "solves/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": w, "grid": list(WORKLOADS[w]["dims"]), "cells": sys0.n, "method": 5},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
+                             "sample": sample},
+            "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
 
 
@@ -386,10 +434,12 @@ def run_ours(args) -> None:
     xm = X.clone()
     # one more mixed solve, outside the timed steps, with events around every
     # J-line launch (direct launches instead of graph replay) for the roofline
-    _, st = solve_device(1, time_kernels=True)
+    r_tk, st = solve_device(1, time_kernels=True)
     jl_ms, jl_n = st["jline_ms"], st["jline_launches"]
+    work_m = work_launches(r_tk.iterations, r_tk.outer_steps)
     kt_mixed = leq.last_kernel_times()
-    _, st64 = solve_device(0, time_kernels=True)
+    r64_tk, st64 = solve_device(0, time_kernels=True)
+    work_64 = work_launches(r64_tk.iterations, 0)
     kt_fp64 = leq.last_kernel_times()
     leq.set_option("time_kernels", 0)
 
@@ -436,13 +486,14 @@ def run_ours(args) -> None:
     # ---- roofline of the J-line sweep kernel (FP32 in the mixed form)
     peak, peak_kind = measured_peak_hbm()
     alg_bytes_launch = 5 * 4 * n  # half the cells x (7 diagonals + rhs + guess + write) x 4 bytes
-    avg_launch_s = (jl_ms / 1e3) / max(jl_n, 1)
+    jl_work = min(work_m["jline"], jl_n)  # launches that did work (the rest returned at once)
+    avg_launch_s = (jl_ms / 1e3) / max(jl_work, 1)
     achieved = alg_bytes_launch / avg_launch_s / 1e9
     traffic = ncu_traffic(f"jline_f32_{w}.md")
     roof = {"kernel": "k_jline<float> (LINE preconditioner half-sweep)", "bound": "hbm", "achieved": achieved,
             "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)",
             "alg_bytes_per_launch": alg_bytes_launch, "avg_launch_ms": avg_launch_s * 1e3, "launches": jl_n,
-            "traffic": traffic}
+            "work_launches": jl_work, "traffic": traffic}
 
     # whole-solve algorithmic bandwidth
     mixed_bytes = n * (rm.iterations * BYTES_FP32_ITER + rm.outer_steps * BYTES_OUTER + BYTES_SETUP + 7 * 12)
@@ -465,14 +516,150 @@ def run_ours(args) -> None:
                  "gpu_launches": int(fp64_launch)},
         "mixed_vs_fp64": value / fp64_value,
         "line_tiles": [{"elem_bytes": e, "line_length": l, "lanes_per_line": g} for e, l, g in leq.autotune_table()],
-        "kernels_mixed": class_table(kt_mixed, n, True, peak),
-        "kernels_fp64": class_table(kt_fp64, n, False, peak),
+        "kernels_mixed": class_table(kt_mixed, n, True, peak, work_m),
+        "kernels_fp64": class_table(kt_fp64, n, False, peak, work_64),
         "wall_s_timed_mixed": wall,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
         cb = cpu_sample(sys0, fp64_iters)
         line["cpu_baseline"] = {"value": cb.get("value"), "unit": "solves/s", "cores": cb["cores"], "kind": "port",
                                 "sample": cb["sample"], "gbs": cb["gbs"]}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+# Algorithmic bytes per cell of one FP64 CG iteration (model/leq_cg.f:271-410),
+# fused minimum in words: MSOLVE 20 (two R letters: 2 reads of the 7 diagonals,
+# 2 red/black passes of rhs + guess + write), matvec 9, rho 2, P 3, X/R 6.
+BYTES_CG_ITER = 8 * (20 + 9 + 2 + 3 + 6)
+
+
+def run_cg_bench(args) -> None:
+    """METHOD 5 through the drop-in: device time of the solve with its inputs
+    already on the device (setup + iterations, from the library's events), and
+    end to end with pinned host arrays; the J-line kernel's roofline from a
+    solve with events around every launch."""
+    import torch
+
+    from mfix_b200 import leq
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=300))
+    w = args.workload
+    sys0 = make_system(w)
+    n = sys0.n
+    dev = torch.device("cuda", local)
+    a_h = torch.empty((7, n), dtype=torch.float64).pin_memory().numpy()
+    b_h = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    x_h = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
+    leq.init_geometry(sys0.imax2, sys0.jmax2, sys0.kmax2, 1, n, 0)
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+        torch.cuda.synchronize(dev)
+
+    def max_over_ranks(v: float) -> float:
+        if world == 1:
+            return v
+        import torch.distributed as dist
+
+        t = torch.tensor([v], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def solve():
+        np.copyto(a_h, sys0.a)
+        np.copyto(b_h, sys0.b)
+        x_h[:] = 0.0
+        barrier()
+        t0 = time.perf_counter()
+        ier = leq.solve_lin_eq("Pp_g", 1, x_h, a_h, b_h, 0, sys0.itmax, 5, "RSRS", sys0.tol, "LINE")
+        t1 = time.perf_counter()
+        if ier != 0:
+            raise RuntimeError(f"CG solve IER {ier}: {leq.last_error()}")
+        return t1 - t0, leq.last_stats()
+
+    for _ in range(args.warmup):
+        solve()
+    sampler = ClockSampler(local)
+    walls, dev_ms, launches = [], [], 0
+    with sampler:
+        for _ in range(args.steps):
+            wl, st = solve()
+            walls.append(wl)
+            dev_ms.append(st["device_ms"])
+            launches += st["kernel_launches"]
+        barrier()
+    iters = st["iterations"]
+    leq.set_option("time_kernels", 1)
+    _, stk = solve()
+    kt = leq.last_kernel_times()
+    leq.set_option("time_kernels", 0)
+    peak, peak_kind = measured_peak_hbm()
+    tot_dev = max_over_ranks(sum(dev_ms))
+    value = world * args.steps / (tot_dev / 1e3)
+    e2e_value = world * args.steps / max_over_ranks(sum(walls))
+    jl_ms, jl_n = stk["jline_ms"], stk["jline_launches"]
+    its_tk = stk["iterations"]
+    jl_work = min(4 * its_tk, jl_n)  # one MSOLVE (two R letters, four half-sweeps) per iteration
+    alg_launch = 5 * 8 * n
+    avg_s = (jl_ms / 1e3) / max(jl_work, 1)
+    achieved = alg_launch / avg_s / 1e9
+    ref = sys0.copy()
+    import oracle as O  # the checker: true residual of the scaled system
+
+    O.scale_diag(ref)
+    rel = O.true_resid(ref, x_h) / O.true_resid(ref, np.zeros(n))
+    kernels = {}
+    names = {"jline": "jline", "s_update": "cg_rho", "p_update": "cg_p", "matvec_alpha": "cg_matvec",
+             "xr_update": "cg_xr"}
+    cls_bytes = {"jline": 40, "s_update": 16, "p_update": 24, "matvec_alpha": 72, "xr_update": 48}
+    for k, (ms, nl) in kt.items():
+        if nl == 0 or k not in names:
+            continue
+        nw = min(jl_work if k == "jline" else its_tk, nl)  # launches after convergence return at once
+        gbs = cls_bytes[k] * n * nw / (ms / 1e3) / 1e9
+        kernels[names[k]] = {"ms": round(ms, 3), "launches": nl, "work_launches": nw,
+                             "us_per_launch": round(1e3 * ms / max(nw, 1), 2), "gbs": round(gbs, 1),
+                             "frac": round(gbs / peak, 3)}
+    line = {
+        "metric": "solves/s", "value": value, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": tot_dev / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": w, "grid": list(WORKLOADS[w]["dims"]), "cells": n, "method": 5, "pc": "LINE",
+                   "sweep": "RSRS", "tol": sys0.tol, "itmax": sys0.itmax,
+                   "l2_policy": "inputs larger than L2 (A_M 7*8*cells bytes), no flush needed"},
+        "roofline": {"kernel": "k_jline<double> (LINE preconditioner half-sweep)", "bound": "hbm",
+                     "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_kind": peak_kind, "alg_bytes_per_launch": alg_launch, "avg_launch_ms": avg_s * 1e3,
+                     "launches": jl_n, "work_launches": jl_work, "traffic": ncu_traffic(f"jline_f64_{w}.md")},
+        "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": 9 * 8 * n,
+                "d2h_bytes_per_step": 9 * 8 * n, "entry": "mfixgpu_solve_lin_eq_ METHOD 5 (pinned host arrays)"},
+        "gpu_launches": int(launches),
+        "clocks": sampler.summary(),
+        "iterations": iters, "true_rel_resid": rel,
+        "alg_gbs": n * (iters * BYTES_CG_ITER + BYTES_SETUP + 80) / (tot_dev / args.steps / 1e3) / 1e9,
+        "kernels": kernels,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu:
+        t = sys0.copy()
+        t0 = time.perf_counter()
+        st_ref = O.leq_cg(t)
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": 1.0 / dt, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
+                                "sample": f"one complete oracle CG solve ({st_ref['iterations']} iterations)"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -919,6 +1106,8 @@ def main() -> None:
         run_batch_bench(args)
     elif kind == "serve":
         run_serve_bench(args)
+    elif kind == "cg":
+        run_cg_bench(args)
     else:
         run_ours(args)
 
