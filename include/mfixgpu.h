@@ -119,7 +119,8 @@ const char *mfixgpu_last_error(void);
  *   "use_graph"      1 (default) replay the iteration body as a CUDA graph
  *   "time_kernels"   1: time every J-line sweep launch with CUDA events (no graph replay)
  *   "autotune"       1 (default): lanes per J-line picked by measurement for each new line length
- *   "line_lanes"     0 (default) automatic, else lanes per J-line (1..32, rounded down to a power of two)
+ *   "line_lanes"     0 (default) automatic, else lanes per J-line (1..32, rounded down to a power of two;
+ *                    64: 32 lanes with the line's rows staged by bulk copies, FP32 lines of 32..1024)
  * Returns 0, or MFIXGPU_ERR_ARGS for an unknown name. */
 int mfixgpu_set_option(const char *name, double value);
 double mfixgpu_get_option(const char *name);

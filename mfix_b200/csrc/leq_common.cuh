@@ -65,6 +65,11 @@ __device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv &f)
     return (uint32_t)(((uint64_t)__umulhi(n, f.m) + n) >> f.l);
 }
 
+// J-line kernels: lanes of one warp share a line and stage its rows through
+// registers (k_jline), one lane runs a whole line (k_jline_thread), or 32 lanes
+// share a line whose rows arrive by bulk copies (k_jline_bulk, FP32 only).
+enum LineKind : int { LK_WARP = 0, LK_THREAD = 1, LK_BULK = 2 };
+
 // One system of the batch.
 struct SysDev {
     int imax2, jmax2, kmax2, do_k;
@@ -76,6 +81,7 @@ struct SysDev {
     int ntiles;          // cell tiles of this system
     int tile_base;       // first tile's slot in the partial-sum array
     int lane_group;      // G: lanes that share one J-line (power of two <= 32)
+    int line_kind;       // LineKind: which J-line kernel sweeps this system's lines
     int rows_per_lane;   // c: rows of a line each lane owns (G*c >= jmax2)
     int half_lines;      // ceil(imax2/2): parity-wave slots per k row
     double *a64;         // 7*n diagonals, Fortran A_M(DIMENSION_3,-3:3) order

@@ -189,7 +189,7 @@ private:
     int run_msolve_plan(int which, int elem);
     int bind_lists();
     int configure_lines(int elem, int only_L = 0);
-    void shape_for(int L, int elem, int forced, int *G, int *c);
+    void shape_for(int L, int elem, int forced, int *G, int *c, int *kind);
     int autotune_lines(const SolveOptions &opt, int elem);
     void save_tune_cache();
 

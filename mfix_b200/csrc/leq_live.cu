@@ -31,6 +31,7 @@ static SysDev idle_sys()
     d.div_j = d.div_i = d.div_h = make_fastdiv(1);
     d.pc = PC_NONE;
     d.lane_group = 32;
+    d.line_kind = LK_WARP;
     d.rows_per_lane = 1;
     d.half_lines = 1;
     return d;
@@ -149,7 +150,7 @@ int Engine::live_add(const LiveSystem &ls)
     d.div_i = make_fastdiv((uint32_t)sp.imax2);
     d.pc = live_opt_.pc;
     d.ntiles = (int)((sp.n + TILE_CELLS - 1) / TILE_CELLS);
-    shape_for(sp.jmax2, mixed ? 4 : 8, live_opt_.force_lanes, &d.lane_group, &d.rows_per_lane);
+    shape_for(sp.jmax2, mixed ? 4 : 8, live_opt_.force_lanes, &d.lane_group, &d.rows_per_lane, &d.line_kind);
     d.half_lines = (sp.imax2 + 1) / 2;
     d.div_h = make_fastdiv((uint32_t)d.half_lines);
     d.a64 = sp.a;

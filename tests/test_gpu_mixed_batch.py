@@ -118,3 +118,61 @@ def test_forced_lanes_per_line(lanes, precision):
     assert np.array_equal(m.a, ref.a)
     assert _true_rel(ref, m.x) <= s.tol * 1.01
     assert np.linalg.norm(m.x - ref.x) <= 1e-6 * np.linalg.norm(ref.x)
+
+
+def _pivoting(s, seed=0):
+    """Rows whose diagonal is shrunk a hundredfold on a few J-lines: DGTSV takes
+    row interchanges there, so those lines run the exact elimination."""
+    t = s.copy()
+    rng = np.random.default_rng(seed)
+    lines = rng.choice(t.imax2 * t.kmax2, size=6, replace=False)
+    for li in lines:
+        i, k = li % t.imax2, li // t.imax2
+        if 0 < i < t.imax2 - 1 and 0 < k < t.kmax2 - 1:
+            base = i * t.jmax2 + k * t.jmax2 * t.imax2
+            t.a[3, base + 1:base + t.jmax2 - 1] *= 0.01
+    return t
+
+
+def test_bulk_staged_lines_equal_register_staged():
+    """The bulk-staged J-line kernel (rows brought in by asynchronous bulk copies)
+    runs the same recurrences as the 32-lane register-staged kernel: the same
+    bits, iteration counts and exact-line counts, odd and even line lengths,
+    2-D, lines that need DGTSV's interchanges, alone and in a batch."""
+    systems = [S.conv_diff(20, 33, 14, seed=90), S.conv_diff(9, 100, 8, seed=91),
+               S.conv_diff(31, 64, 1, seed=92, do_k=False), S.conv_diff(12, 257, 6, seed=93)]
+    piv = _pivoting(S.conv_diff(14, 47, 12, seed=94), seed=3)
+    piv.itmax = 40
+    out = {}
+    for lanes in (32, 64):
+        assert leq.set_option("line_lanes", lanes) == 0 and leq.set_option("precision", 1) == 0
+        try:
+            alone = []
+            for s in systems + [piv]:
+                t = s.copy()
+                ier = leq.solve_system(t)
+                st = leq.last_stats()
+                alone.append((t.x, ier, st["iterations"], st["line_fallbacks"], st["line_skips"]))
+            together = [s.copy() for s in systems]
+            rc, res = leq.batch_solve(together, precision=1)
+            assert rc == 0 and all(r.ier == 0 for r in res), leq.last_error()
+        finally:
+            leq.set_option("line_lanes", 0)
+            leq.set_option("precision", 0)
+        out[lanes] = (alone, together, [r.iterations for r in res])
+    for a32, a64 in zip(out[32][0], out[64][0]):
+        assert np.array_equal(a32[0], a64[0])
+        assert a32[1:] == a64[1:]
+    assert out[32][0][-1][3] > 0  # the pivoting lines took the exact elimination
+    for t32, t64 in zip(out[32][1], out[64][1]):
+        assert np.array_equal(t32.x, t64.x)
+    assert out[32][2] == out[64][2]
+    for s, (x, ier, *_) in zip(systems, out[64][0]):
+        assert ier == 0
+        assert _true_rel(_scaled_ref(s), x) <= s.tol * 1.01
+
+
+def _scaled_ref(s):
+    ref = s.copy()
+    O.scale(ref)
+    return ref
