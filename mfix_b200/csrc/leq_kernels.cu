@@ -1736,11 +1736,11 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
 }
 
 // ------------------------------------------------------------------ J-line half-sweep, bulk-staged
-// Long lines of the mixed form: one line per warp.  Its twelve operand rows
-// (right-hand side, A(-1), A(1), A(-3), A(3), the four neighbour lines, the
-// three LU factors) come into shared memory by asynchronous bulk copies, one row
-// per lane, their completion counted in bytes on an mbarrier; two buffers per
-// warp, so that the next line's rows arrive while this line's recurrences run.
+// Lines of the mixed form, one per warp, an autotuner candidate beside the
+// register-staged shapes.  The line's twelve operand rows (right-hand side,
+// A(-1), A(1), A(-3), A(3), the four neighbour lines, the three LU factors) come
+// into shared memory by asynchronous bulk copies, one row per lane, their
+// completion counted in bytes on an mbarrier; no registers hold them in flight.
 // The recurrences are k_jline's with 32 lanes per line and the same rows per
 // lane, in the same order.  Each copy covers the 16-byte-aligned span around
 // its row: every row lies in the engine's work block (256-byte-aligned arrays)
@@ -1781,6 +1781,11 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
 }
 
 constexpr int BULK_ROWS = 12;
+// Row buffers per warp.  With two, the next line's rows arrive during this line's
+// sweep, but a 258-row line then takes 29 KB per warp and 7 warps fit an SM; with
+// one, 15 warps fit and other warps cover the copies (256^3: 167 vs 110 us per
+// half-sweep; the register-staged kernel takes 95 us there).
+constexpr int BULK_BUFS = 1;
 constexpr int BULK_HDR = 128;  // bytes per warp: two mbarriers, then two sets of row offsets
 
 // Elements per staged row: at least 32 rows per lane-chunk and the row's span.
@@ -1789,7 +1794,7 @@ __host__ __device__ inline int bulk_lpad(int L, int c) { return ((L + 8 > 32 * c
 template <typename T>
 __host__ __device__ inline int bulk_warp_bytes(int lpad)
 {
-    return BULK_HDR + (2 * BULK_ROWS + 1) * lpad * (int)sizeof(T);
+    return BULK_HDR + (BULK_BUFS * BULK_ROWS + 1) * lpad * (int)sizeof(T);
 }
 
 template <typename T>
@@ -1802,7 +1807,7 @@ __global__ void __launch_bounds__(128) k_jline_bulk(BatchView b, WaveArgs w, int
     const uint32_t bars = smem_u32(ws);  // two mbarriers, 8 bytes each
     int *offs = reinterpret_cast<int *>(ws + 16);           // [2][BULK_ROWS] element offsets of the rows
     T *rows = reinterpret_cast<T *>(ws + BULK_HDR);         // [2][BULK_ROWS][lpad]
-    T *fb = rows + 2 * BULK_ROWS * lpad;                     // [lpad]: f, y, then the new values
+    T *fb = rows + BULK_BUFS * BULK_ROWS * lpad;             // [lpad]: f, y, then the new values
     if (lane == 0) {
         mbar_init(bars, 1);
         mbar_init(bars + 8, 1);
@@ -1858,14 +1863,14 @@ __global__ void __launch_bounds__(128) k_jline_bulk(BatchView b, WaveArgs w, int
     if (have) issue(jc, 0);
     while (have) {
         const bool have_n = next_line_job(b, w, jc.item + step, step, total, lane, false, LK_BULK, jn);
-        if (have_n) issue(jn, q ^ 1);
+        if (BULK_BUFS == 2 && have_n) issue(jn, q ^ 1);
         const bool ok = __all_sync(0xffffffffu, mbar_wait(bars + 8 * q, (phase >> q) & 1u));
         phase ^= 1u << q;
         const SysDev &d = b.sys[jc.sidx];
         SysState &st = b.st[jc.sidx];
         if (!ok) {  // a copy never completed: flag the system, drain the other buffer, stop
             if (lane == 0) atomicOr(&st.err, 4);
-            if (have_n) mbar_wait(bars + 8 * (q ^ 1), (phase >> (q ^ 1)) & 1u);
+            if (BULK_BUFS == 2 && have_n) mbar_wait(bars + 8 * (q ^ 1), (phase >> (q ^ 1)) & 1u);
             return;
         }
         const LineCtx<T> x = line_ctx<T>(b, w, jc);
@@ -1986,7 +1991,10 @@ __global__ void __launch_bounds__(128) k_jline_bulk(BatchView b, WaveArgs w, int
         __syncwarp();
         jc = jn;
         have = have_n;
-        q ^= 1;
+        if (BULK_BUFS == 2)
+            q ^= 1;
+        else if (have)
+            issue(jc, 0);
     }
 }
 
