@@ -173,6 +173,10 @@ SolveResult result_of(const SysState &st, bool mixed)
         r.ier = -12;  // DGTSV INFO != 0 inside a JK/IJ sweep (the reference stops there)
         r.exit_kind = EX_ERROR;
     }
+    if (st.err & 4) {
+        r.ier = -13;  // a bulk copy of the J-line kernel did not complete within its bounded wait
+        r.exit_kind = EX_ERROR;
+    }
     return r;
 }
 
