@@ -60,6 +60,8 @@ def lib() -> C.CDLL:
                                  C.POINTER(Stats)]
         L.orc_leq_cg.restype = C.c_int
         L.orc_scale_diag.argtypes = [C.POINTER(Geom), vp, vp]
+        L.orc_leq_gmres.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_char_p, C.c_double, C.c_int, C.POINTER(Stats)]
+        L.orc_leq_gmres.restype = C.c_int
         L.orc_true_resid.argtypes = [C.POINTER(Geom), vp, vp, vp]
         L.orc_true_resid.restype = C.c_double
         L.orc_truth_solve.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_double, C.c_int, C.c_uint64, _dp]
@@ -142,6 +144,14 @@ def leq_cg(s, sweep: str = "RSRS", pc: str = "LINE") -> dict:
     st = Stats()
     lib().orc_leq_cg(C.byref(geom(s)), _p(s.x), _p(s.a), _p(s.b), sweep.ljust(4)[:4].encode(), s.tol,
                      pc.ljust(4)[:4].encode(), s.itmax, C.byref(st))
+    return {k: getattr(st, k) for k, _ in Stats._fields_}
+
+
+def leq_gmres(s, sweep: str = "RSRS") -> dict:
+    """LEQ_GMRES (METHOD 3) on s (s.x updated; A and B untouched).  IER 0 or 1."""
+    st = Stats()
+    lib().orc_leq_gmres(C.byref(geom(s)), _p(s.x), _p(s.a), _p(s.b), sweep.ljust(4)[:4].encode(), s.tol, s.itmax,
+                        C.byref(st))
     return {k: getattr(st, k) for k, _ in Stats._fields_}
 
 

@@ -764,3 +764,152 @@ int orc_leq_cg(const orc_geom *g, double *var, double *a, double *b, const char 
     free(work);
     return ier;
 }
+
+/* ------------------------------------------------------------------ LEQ_GMRES0 */
+/* ROTMAT (model/leq_gmres.f:593-628): the Givens rotation that zeroes b. */
+static void rotmat(double a, double b, double *c, double *s)
+{
+    if (b == 0.0) {
+        *c = 1.0;
+        *s = 0.0;
+    } else if (fabs(b) > fabs(a)) {
+        const double t = a / b;
+        *s = 1.0 / sqrt(1.0 + t * t);
+        *c = t * *s;
+    } else {
+        const double t = b / a;
+        *c = 1.0 / sqrt(1.0 + t * t);
+        *s = t * *c;
+    }
+}
+
+/* Back substitution of H(1:m,1:m) y = SS(1:m) and Var += V(:,1:m) y with the
+ * per-cell sum taken over the basis in order (:362-426, :447-507). */
+static void gmres_update(int64_t n, int m, const double *H, int ldh, const double *ss, const double *V, double *var)
+{
+    double *y = (double *)malloc((size_t)(m > 0 ? m : 1) * sizeof(double));
+    for (int i = 0; i < m; ++i) y[i] = ss[i];
+    for (int i = m - 1; i >= 0; --i) {
+        const double yi = y[i] / H[i + (size_t)i * ldh];
+        y[i] = yi;
+        for (int j = 0; j < i; ++j) y[j] = y[j] - H[j + (size_t)i * ldh] * yi;
+    }
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < n; ++p) {
+        double d = 0.0;
+        for (int k = 0; k < m; ++k) d = d + V[(size_t)k * n + p] * y[k];
+        var[p] = var[p] + d;
+    }
+    free(y);
+}
+
+/* GMRES(ITMAX) with one restart cycle (SOLVE_LIN_EQ passes MAX_IT = 1,
+ * model/solve_lin_eq.f:86,147-150,161-171), left-preconditioned by LEQ_MSOLVE
+ * with the sweep letters; no unit scaling, A and B untouched.  LEQ_GMRES
+ * (model/leq_gmres.f:17-76) returns Var = 0 for B = 0.  LEQ_GMRES0 (:94-584):
+ * BNRM2 = ||B|| (:209-218); R = MSOLVE(B - A Var), ERROR0 = ||R|| / BNRM2
+ * (:220-246); the Arnoldi loop with modified Gram-Schmidt (:296-327), the
+ * rotations and the convergence test (:329-360), the update on convergence
+ * (:361-426) or after ITMAX steps with the new true residual (:445-540); IER = 1
+ * when not converged (:545-549).  The condition checks of :371-411 run only in a
+ * debug build of the reference (JDEBUG = 0) and are not restated. */
+int orc_leq_gmres(const orc_geom *g, double *var, const double *a, const double *b, const char *sweep, double tol,
+                  int itmax, orc_stats *st)
+{
+    memset(st, 0, sizeof(*st));
+    st->exit_kind = -1;
+    const int64_t n = g->n;
+    double bmax = 0.0;
+    for (int64_t p = 0; p < n; ++p) bmax = fabs(b[p]) > bmax ? fabs(b[p]) : bmax;
+    if (bmax == 0.0) {
+        for (int64_t p = 0; p < n; ++p) var[p] = 0.0;
+        st->exit_kind = 2;
+        return 0;
+    }
+    const int M = itmax > 0 ? itmax : 0;
+    double *V = (double *)calloc((size_t)(M + 1) * (size_t)n, sizeof(double));
+    double *R = (double *)calloc((size_t)n, sizeof(double)), *T = (double *)calloc((size_t)n, sizeof(double));
+    double *W = (double *)calloc((size_t)n, sizeof(double));
+    const int ldh = M + 1;
+    double *H = (double *)calloc((size_t)ldh * (size_t)(M > 0 ? M : 1), sizeof(double));
+    double *cs = (double *)calloc((size_t)M + 1, sizeof(double)), *sn = (double *)calloc((size_t)M + 1, sizeof(double));
+    double *ss = (double *)calloc((size_t)M + 2, sizeof(double));
+    int skips = 0, rc = 0;
+    double bnrm2 = sqrt(orc_dot(b, b, n));
+    if (bnrm2 == 0.0) bnrm2 = 1.0;
+    orc_matvec(g, a, var, R);
+    for (int64_t p = 0; p < n; ++p) T[p] = b[p] - R[p];
+    if (orc_msolve(g, T, a, R, sweep, &skips) != 0) rc = -12;
+    double norm_r = sqrt(orc_dot(R, R, n));
+    double error = norm_r / bnrm2;
+    const double error0 = error;
+    int steps = 0, converged = 0;
+    if (rc == 0) {
+        /* the single restart cycle recomputes the same R (:256-283) */
+        const double inv = 1.0 / norm_r;
+        for (int64_t p = 0; p < n; ++p) V[p] = R[p] * inv;
+        for (int k = 0; k < M + 2; ++k) ss[k] = 0.0;
+        ss[0] = norm_r;
+        for (int i = 0; i < M && !converged; ++i) {
+            double *vi = V + (size_t)i * n, *vn = V + (size_t)(i + 1) * n;
+            double *h = H + (size_t)i * ldh;
+            orc_matvec(g, a, vi, T);
+            if (orc_msolve(g, T, a, W, sweep, &skips) != 0) {
+                rc = -12;
+                break;
+            }
+            for (int k = 0; k <= i; ++k) {
+                const double *vk = V + (size_t)k * n;
+                h[k] = orc_dot(W, vk, n);
+                for (int64_t p = 0; p < n; ++p) W[p] = W[p] - h[k] * vk[p];
+            }
+            h[i + 1] = sqrt(orc_dot(W, W, n));
+            const double invh = 1.0 / h[i + 1];
+            for (int64_t p = 0; p < n; ++p) vn[p] = W[p] * invh;
+            for (int k = 0; k < i; ++k) {
+                const double d = cs[k] * h[k] + sn[k] * h[k + 1];
+                h[k + 1] = -sn[k] * h[k] + cs[k] * h[k + 1];
+                h[k] = d;
+            }
+            rotmat(h[i], h[i + 1], &cs[i], &sn[i]);
+            const double d = cs[i] * ss[i];
+            ss[i + 1] = -sn[i] * ss[i];
+            ss[i] = d;
+            h[i] = cs[i] * h[i] + sn[i] * h[i + 1];
+            h[i + 1] = 0.0;
+            error = fabs(ss[i + 1]) / bnrm2;
+            steps = i + 1;
+            if (error <= tol * error0) {
+                gmres_update(n, i + 1, H, ldh, ss, V, var);
+                converged = 1;
+            }
+        }
+        if (rc == 0 && !converged) {
+            gmres_update(n, M, H, ldh, ss, V, var);
+            orc_matvec(g, a, var, R);
+            for (int64_t p = 0; p < n; ++p) T[p] = b[p] - R[p];
+            if (orc_msolve(g, T, a, R, sweep, &skips) != 0) rc = -12;
+            norm_r = sqrt(orc_dot(R, R, n));
+            error = norm_r / bnrm2;
+        }
+    }
+    free(V);
+    free(R);
+    free(T);
+    free(W);
+    free(H);
+    free(cs);
+    free(sn);
+    free(ss);
+    st->line_info_skips = skips;
+    if (rc) {
+        st->ier = rc;
+        return rc;
+    }
+    st->ier = (error > tol * error0) ? 1 : 0;
+    st->iterations = steps;
+    st->exit_kind = st->ier ? 3 : 0;
+    st->rnorm0 = error0 * bnrm2;
+    st->rnorm = error * bnrm2;
+    return st->ier;
+}

@@ -72,6 +72,11 @@ int orc_leq_bicgs_sample(const orc_geom *g, double *var, double *a, double *b, c
 int orc_leq_cg(const orc_geom *g, double *var, double *a, double *b, const char *sweep, double tol,
                const char *pc, int itmax, orc_stats *st);
 
+/* LEQ_GMRES (METHOD 3, one restart cycle of ITMAX steps, left-preconditioned by
+ * LEQ_MSOLVE with the sweep letters; A and B are not scaled).  IER 0 or 1. */
+int orc_leq_gmres(const orc_geom *g, double *var, const double *a, const double *b, const char *sweep, double tol,
+                  int itmax, orc_stats *st);
+
 /* true residual ||b - A x||_2 in long double */
 double orc_true_resid(const orc_geom *g, const double *a, const double *b, const double *x);
 

@@ -207,3 +207,64 @@ def test_cg_ier_rules():
     p = S.pressure_like(14, 20, 12, seed=3, nspheres=4, rmin=2, rmax=5, itmax=60)
     st = O.leq_cg(p)
     assert st["ier"] == -2 and st["iterations"] == 61 and st["iter_tot_add"] == 61
+
+
+# ---------------------------------------------------------------- LEQ_GMRES0 (METHOD 3)
+def _gmres_numpy(s, m, sweep="RSRS"):
+    """m steps of left-preconditioned GMRES from x0 = s.x, the least-squares
+    problem solved by numpy (an independent restatement of
+    model/leq_gmres.f:220-507 without its Givens rotations)."""
+    prec = lambda v: O.msolve(s, np.ascontiguousarray(v), sweep=sweep)[1]
+    mv = lambda v: S.matvec_np(s.imax2, s.jmax2, s.kmax2, s.do_k, s.a, v)
+    r = prec(s.b - mv(s.x))
+    beta = np.linalg.norm(r)
+    V = [r / beta]
+    H = np.zeros((m + 1, m))
+    for i in range(m):
+        w = prec(mv(V[i]))
+        for k in range(i + 1):
+            H[k, i] = w @ V[k]
+            w = w - H[k, i] * V[k]
+        H[i + 1, i] = np.linalg.norm(w)
+        V.append(w / H[i + 1, i])
+    e1 = np.zeros(m + 1)
+    e1[0] = beta
+    y = np.linalg.lstsq(H, e1, rcond=None)[0]
+    return s.x + np.array(V[:m]).T @ y
+
+
+@pytest.mark.parametrize("m", [1, 5, 15])
+def test_gmres_iterate_matches_numpy(m):
+    s = S.conv_diff(11, 16, 9, seed=4)
+    t = s.copy()
+    t.tol = 0.0  # never converged: ITMAX steps, then the update with all m vectors
+    t.itmax = m
+    st = O.leq_gmres(t)
+    assert st["ier"] == 1 and st["iterations"] == m
+    xr = _gmres_numpy(s, m)
+    assert np.max(np.abs(t.x - xr)) <= 1e-9 * np.max(np.abs(xr))
+
+
+def test_gmres_converges_and_leaves_a_b():
+    for s in (S.conv_diff(14, 20, 12, seed=3), S.conv_diff(21, 19, 1, seed=5, do_k=False),
+              S.pressure_like(14, 20, 12, seed=3, nspheres=4, rmin=2, rmax=5, itmax=200)):
+        s.itmax = 200
+        t = s.copy()
+        st = O.leq_gmres(t)
+        assert st["ier"] == 0 and st["exit_kind"] == 0 and st["iter_tot_add"] == 0
+        assert np.array_equal(t.a, s.a) and np.array_equal(t.b, s.b)  # no unit scaling in GMRES
+        # ERROR is the preconditioned residual; the true one follows it within a few orders
+        assert O.true_resid(s, t.x) <= 1e-5 * O.true_resid(s, np.zeros(s.n))
+
+
+def test_gmres_zero_rhs_and_itmax():
+    s = S.conv_diff(8, 9, 7, seed=1)
+    t = s.copy()
+    t.b[:] = 0.0
+    t.x[:] = 3.0
+    st = O.leq_gmres(t)  # model/leq_gmres.f:64-70: Var = 0, no iteration
+    assert st["ier"] == 0 and st["exit_kind"] == 2 and not np.any(t.x)
+    t = s.copy()
+    t.itmax = 3
+    st = O.leq_gmres(t)
+    assert st["ier"] == 1 and st["iterations"] == 3
