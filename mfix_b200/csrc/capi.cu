@@ -142,12 +142,13 @@ void solve_impl(int vno, double *var, double *a_m, double *b_m, int m, int itmax
         g.err = "phase index M outside 0:DIMENSION_M";
         return finish(MFIXGPU_ERR_ARGS);
     }
-    // model/solve_lin_eq.f:131-191: BiCGSTAB (2), BiCGSTAB then GMRES (4), CG (5)
-    if (method != 2 && method != 4 && method != 5) {
-        g.err = "LEQ_METHOD " + std::to_string(method) + " is not served by the GPU path (BiCGSTAB and CG)";
+    // model/solve_lin_eq.f:131-191: BiCGSTAB (2), GMRES (3), BiCGSTAB then GMRES (4), CG (5)
+    if (method < 2 || method > 5) {
+        g.err = "LEQ_METHOD " + std::to_string(method) + " is not served by the GPU path (2, 3, 4, 5)";
         return finish(MFIXGPU_ERR_UNSUPPORTED);
     }
-    const int pc = decode_pc(pc4);
+    // LEQ_GMRES takes no PC argument and always sweeps with LEQ_MSOLVE (:145-150)
+    const int pc = method == 3 ? PC_LINE : decode_pc(pc4);
     if (pc < 0) {
         g.err = "preconditioner option not found";  // the reference's message, model/leq_bicgs.f:84-85
         return finish(MFIXGPU_ERR_UNSUPPORTED);
@@ -168,18 +169,14 @@ void solve_impl(int vno, double *var, double *a_m, double *b_m, int m, int itmax
     s.itmax = itmax;
     std::vector<SolveResult> out;
     SolveOptions so = make_opts(g.opt, pc, sweep4);
-    so.method = method == 5 ? 5 : 2;
+    so.method = method;
     const int rc = e->solve({s}, so, out);
     if (rc) {
         g.err = e->last_error();
         return finish(rc);
     }
     const SolveResult &r = out[0];
-    int code = r.ier;
-    if (method == 4 && code == -2) {  // :166-171 would continue with GMRES
-        g.err = "BiCGSTAB broke down and METHOD=4 asks for GMRES, which the GPU path does not serve";
-        code = MFIXGPU_ERR_UNSUPPORTED;
-    }
+    const int code = r.ier;
     if (vno >= 1 && vno <= 10) g.iter_tot[vno - 1] += r.iter_tot_add;
     g.last.iterations = r.iterations;
     g.last.iter_tot_add = r.iter_tot_add;

@@ -120,6 +120,9 @@ Engine::~Engine()
     cudaFree(d_seq_scratch_);
     cudaFree(d_one_sys_);
     cudaFree(d_dot_partials_);
+    cudaFree(gm_basis_);
+    cudaFree(gm_scal_);
+    cudaFree(gm_max_);
     cudaFree(d_dot_counter_);
     cudaFree(d_dot_out_);
     if (h_st_pinned_) cudaFreeHost(h_st_pinned_);
@@ -932,10 +935,12 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
     }
     SolveOptions o = opt;
     o.on_device = true;
-    if (opt.method != 2 && opt.method != 5) return fail("LEQ_METHOD not served (2 BiCGSTAB, 5 CG)", -10);
-    if (opt.method == 5) o.precision = PREC_FP64;  // CG runs the FP64 reference form only
+    if (opt.method < 2 || opt.method > 5) return fail("LEQ_METHOD not served (2 BiCGSTAB, 3 GMRES, 4, 5 CG)", -10);
+    if ((opt.method == 3 || opt.method == 4) && specs.size() != 1)
+        return fail("GMRES (METHOD 3/4) serves single systems", -10);
+    if (opt.method == 5 || opt.method == 3) o.precision = PREC_FP64;  // CG and GMRES run their FP64 form only
     writeback_.clear();
-    if (!opt.on_device && opt.write_back_ab)
+    if (!opt.on_device && opt.write_back_ab && opt.method != 3)  // GMRES leaves A and B as they are
         for (size_t q = 0; q < specs.size(); ++q) {
             const size_t n = (size_t)specs[q].n;
             writeback_.push_back({specs[q].a, dev[q].a, 7 * n * 8});
@@ -948,8 +953,18 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
         const char ch = opt.sweep[q];
         if (ch == 'I' || ch == 'i' || ch == 'K' || ch == 'k' || ch == 'A' || ch == 'a') rs_only = false;
     }
-    int rc = (specs.size() > 1 && rs_only && !opt.time_kernels && opt.method == 2) ? run_batch_live(dev, o, out)
-                                                                                   : run_batch(dev, o, out);
+    if (opt.method == 3) {  // LEQ_GMRES
+        int rc = run_gmres(dev[0], o, out[0]);
+        if (rc) return rc;
+        if (!opt.on_device) {
+            CK(cudaMemcpyAsync(specs[0].x, dev[0].x, (size_t)specs[0].n * 8, cudaMemcpyDeviceToHost, stream_));
+            CK(cudaStreamSynchronize(stream_));
+        }
+        return 0;
+    }
+    if (opt.method == 4) o.method = 2;  // BiCGSTAB first (model/solve_lin_eq.f:161-171)
+    int rc = (specs.size() > 1 && rs_only && !opt.time_kernels && o.method == 2) ? run_batch_live(dev, o, out)
+                                                                                 : run_batch(dev, o, out);
     if (rc) return rc;
     SolveTiming total = timing_;
 
@@ -989,6 +1004,19 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
         }
     }
     timing_ = total;
+
+    // METHOD 4: a BiCGSTAB breakdown (IER -2) continues with GMRES on the scaled
+    // system from BiCGSTAB's VAR, IER reset to 0 first (model/solve_lin_eq.f:161-171)
+    if (opt.method == 4 && out[0].ier == -2) {
+        SolveOptions g = o;
+        g.method = 3;
+        g.precision = PREC_FP64;
+        SolveResult gr;
+        if ((rc = run_gmres(dev[0], g, gr))) return rc;
+        gr.iter_tot_add = out[0].iter_tot_add;  // LEQ_BICGS's ITER_TOT; GMRES adds none
+        out[0] = gr;
+        timing_.device_ms += total.device_ms;
+    }
 
     // results back to the caller's host arrays (A/B went back during the iterations)
     if ((rc = issue_writeback())) return rc;  // a batch that ended before issuing them
@@ -1212,6 +1240,209 @@ int Engine::run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &
     for (int s = 0; s < nsys_; ++s) out[s] = result_of(h_st_[s], mixed);
     CK(cudaStreamSynchronize(stream_));
     if (ktime_) kt_harvest();
+    return 0;
+}
+
+// ------------------------------------------------------------------ LEQ_GMRES
+// GMRES(ITMAX) with one restart cycle (MAX_IT = 1, model/solve_lin_eq.f:86),
+// left-preconditioned by LEQ_MSOLVE with the sweep letters; A and B are not
+// scaled (model/leq_gmres.f:17-584).  The vector work runs on the device (matvec,
+// the J-line sweeps, fused modified Gram-Schmidt passes with deterministic
+// sums); the Hessenberg column comes to the host once per step, where the Givens
+// rotations (ROTMAT, :593-628), the convergence test and the back substitution
+// run in FP64 as in the reference.  IER 0, or 1 when not converged.
+int Engine::run_gmres(const SystemSpec &s, const SolveOptions &opt, SolveResult &r)
+{
+    r = SolveResult{};
+    SolveOptions o = opt;
+    o.method = 3;
+    o.precision = PREC_FP64;
+    o.skip_scale = true;
+    o.pc = PC_LINE;  // LEQ_GMRES always preconditions with LEQ_MSOLVE (model/leq_gmres.f:73-74)
+    const int64_t n = s.n;
+    const int M = std::max(0, s.itmax);
+    const int grid = std::max(1, std::min((int)((n + 255) / 256), sms_ * 8));
+    ktime_ = false;
+    timing_ = SolveTiming{};
+    cudaEvent_t t0, t1;
+    CK(cudaEventCreate(&t0));
+    CK(cudaEventCreate(&t1));
+    CK(cudaEventRecord(t0, stream_));
+    launches_ = 0;
+
+    // B = 0: Var = 0 and nothing else (:64-70)
+    if (!gm_max_) CK(cudaMalloc((void **)&gm_max_, sizeof(unsigned long long)));
+    CK(cudaMemsetAsync(gm_max_, 0, sizeof(unsigned long long), stream_));
+    CK(launch_gm_maxabs(s.b, n, gm_max_, grid, stream_));
+    unsigned long long bmax = 0;
+    CK(cudaMemcpyAsync(&bmax, gm_max_, sizeof bmax, cudaMemcpyDeviceToHost, stream_));
+    CK(cudaStreamSynchronize(stream_));
+    launches_ += 1;
+    if (bmax == 0) {
+        CK(cudaMemsetAsync(s.x, 0, (size_t)n * 8, stream_));
+        r.exit_kind = EX_RHO0;
+        CK(cudaEventRecord(t1, stream_));
+        CK(cudaEventSynchronize(t1));
+        cudaEventElapsedTime(&timing_.device_ms, t0, t1);
+        cudaEventDestroy(t0);
+        cudaEventDestroy(t1);
+        timing_.kernel_launches = launches_;
+        return 0;
+    }
+    // the system's tables and work vectors, the J-line factors, the sweep plan
+    int rc = setup_batch({s}, o);
+    if (rc) return rc;
+    h_lines_.clear();
+    list_refs_.clear();
+    if ((rc = plan_msolve(o, V_T, V_S, G_INNER, 0))) return rc;  // WW = MSOLVE(TEMP)
+    if ((rc = bind_lists())) return rc;
+    CK(launch_line_factor<double>(view_, cfg_, d_allprefix_, h_allprefix_[nsys_]));
+    CK(launch_init_done(view_, cfg_));
+    launches_ += 2;
+    const SysDev &d = h_sys_[0];
+    double *T = (double *)d.vec[V_T], *W = (double *)d.vec[V_S];
+    const size_t basis = (size_t)(M + 1) * (size_t)n * 8;
+    if (basis > gm_basis_bytes_) {
+        cudaFree(gm_basis_);
+        gm_basis_ = nullptr;
+        gm_basis_bytes_ = 0;
+        if (cudaMalloc((void **)&gm_basis_, basis) != cudaSuccess) {
+            cudaGetLastError();
+            return fail("device memory for the GMRES basis ((ITMAX+1) x DIMENSION_3 doubles)", -11);
+        }
+        gm_basis_bytes_ = basis;
+    }
+    const int need = grid + M + 2 + std::max(M, 1);
+    if (need > gm_scal_cap_) {
+        cudaFree(gm_scal_);
+        CK(cudaMalloc((void **)&gm_scal_, sizeof(double) * (size_t)need));
+        gm_scal_cap_ = need;
+    }
+    double *partials = gm_scal_, *dh = gm_scal_ + grid, *dy = dh + M + 2;
+    double *V = gm_basis_;
+    auto norm2 = [&](const double *x, const double *y, double *out) -> int {
+        CK(launch_gm_mgs(const_cast<double *>(x), nullptr, nullptr, y, n, partials, grid, stream_));
+        CK(launch_gm_sum(partials, grid, dh, stream_));
+        CK(cudaMemcpyAsync(out, dh, sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
+        launches_ += 2;
+        return 0;
+    };
+    // R = MSOLVE(B - A Var) into W (:220-239)
+    auto residual = [&]() -> int {
+        CK(launch_matvec_plain<double>(view_.sys, d, s.a, s.x, T, stream_, grid));
+        CK(launch_gm_sub(s.b, T, n, grid, stream_));
+        launches_ += 2;
+        return run_msolve_plan(0, 8);
+    };
+    // back substitution of H(1:m,1:m) y = SS(1:m) and Var += V(:,1:m) y (:361-426)
+    std::vector<double> H((size_t)(M + 1) * std::max(M, 1), 0.0), cs(M + 1, 0.0), sn(M + 1, 0.0), ss(M + 2, 0.0);
+    const int ldh = M + 1;
+    auto update = [&](int m) -> int {
+        std::vector<double> y(std::max(m, 1), 0.0);
+        for (int i = 0; i < m; ++i) y[i] = ss[i];
+        for (int i = m - 1; i >= 0; --i) {
+            const double yi = y[i] / H[i + (size_t)i * ldh];
+            y[i] = yi;
+            for (int j = 0; j < i; ++j) y[j] = y[j] - H[j + (size_t)i * ldh] * yi;
+        }
+        if (m > 0) {
+            CK(cudaMemcpyAsync(dy, y.data(), sizeof(double) * (size_t)m, cudaMemcpyHostToDevice, stream_));
+            CK(launch_gm_update(s.x, V, dy, m, n, grid, stream_));
+            launches_ += 1;
+        }
+        return 0;
+    };
+
+    double bb = 0.0;
+    if ((rc = norm2(s.b, s.b, &bb))) return rc;
+    double bnrm2 = std::sqrt(bb);
+    if (bnrm2 == 0.0) bnrm2 = 1.0;
+    if ((rc = residual())) return rc;
+    double rr = 0.0;
+    if ((rc = norm2(W, W, &rr))) return rc;
+    double norm_r = std::sqrt(rr);
+    double error = norm_r / bnrm2;
+    const double error0 = error;
+    const double rnorm0 = norm_r;
+    // the single restart cycle (:255-540); its opening residual equals the one above
+    CK(launch_gm_scale(W, 1.0 / norm_r, V, n, grid, stream_));
+    launches_ += 1;
+    ss[0] = norm_r;
+    int steps = 0;
+    bool converged = false;
+    std::vector<double> h(M + 2, 0.0);
+    for (int i = 0; i < M && !converged; ++i) {
+        double *vi = V + (size_t)i * n;
+        CK(launch_matvec_plain<double>(view_.sys, d, s.a, vi, T, stream_, grid));
+        launches_ += 1;
+        if ((rc = run_msolve_plan(0, 8))) return rc;  // WW = MSOLVE(A V(:,I)) (:297-298)
+        // modified Gram-Schmidt, each axpy fused with the next dot (:299-322)
+        for (int k = 0; k <= i; ++k) {
+            CK(launch_gm_mgs(W, k ? V + (size_t)(k - 1) * n : nullptr, dh + k - 1, V + (size_t)k * n, n, partials, grid,
+                             stream_));
+            CK(launch_gm_sum(partials, grid, dh + k, stream_));
+        }
+        CK(launch_gm_mgs(W, vi, dh + i, W, n, partials, grid, stream_));
+        CK(launch_gm_sum(partials, grid, dh + i + 1, stream_));
+        launches_ += 2 * (i + 2);
+        CK(cudaMemcpyAsync(h.data(), dh, sizeof(double) * (size_t)(i + 2), cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
+        double *col = H.data() + (size_t)i * ldh;
+        for (int k = 0; k <= i; ++k) col[k] = h[k];
+        col[i + 1] = std::sqrt(h[i + 1]);  // NORM_W
+        CK(launch_gm_scale(W, 1.0 / col[i + 1], V + (size_t)(i + 1) * n, n, grid, stream_));
+        launches_ += 1;
+        for (int k = 0; k < i; ++k) {  // earlier rotations (:329-333)
+            const double t = cs[k] * col[k] + sn[k] * col[k + 1];
+            col[k + 1] = -sn[k] * col[k] + cs[k] * col[k + 1];
+            col[k] = t;
+        }
+        // ROTMAT (:593-628)
+        const double a = col[i], b = col[i + 1];
+        if (b == 0.0) {
+            cs[i] = 1.0;
+            sn[i] = 0.0;
+        } else if (std::fabs(b) > std::fabs(a)) {
+            const double t = a / b;
+            sn[i] = 1.0 / std::sqrt(1.0 + t * t);
+            cs[i] = t * sn[i];
+        } else {
+            const double t = b / a;
+            cs[i] = 1.0 / std::sqrt(1.0 + t * t);
+            sn[i] = t * cs[i];
+        }
+        const double t = cs[i] * ss[i];
+        ss[i + 1] = -sn[i] * ss[i];
+        ss[i] = t;
+        col[i] = cs[i] * col[i] + sn[i] * col[i + 1];
+        col[i + 1] = 0.0;
+        error = std::fabs(ss[i + 1]) / bnrm2;
+        steps = i + 1;
+        if (error <= s.tol * error0) {  // (:352-360)
+            if ((rc = update(i + 1))) return rc;
+            converged = true;
+        }
+    }
+    if (!converged) {  // ITMAX steps: update with them all, then the new residual (:445-540)
+        if ((rc = update(M))) return rc;
+        if ((rc = residual())) return rc;
+        if ((rc = norm2(W, W, &rr))) return rc;
+        norm_r = std::sqrt(rr);
+        error = norm_r / bnrm2;
+    }
+    CK(cudaEventRecord(t1, stream_));
+    CK(cudaEventSynchronize(t1));
+    cudaEventElapsedTime(&timing_.device_ms, t0, t1);
+    cudaEventDestroy(t0);
+    cudaEventDestroy(t1);
+    timing_.kernel_launches = launches_;
+    r.ier = error > s.tol * error0 ? 1 : 0;
+    r.iterations = steps;
+    r.exit_kind = r.ier ? EX_ITMAX : EX_RNORM;
+    r.rnorm0 = rnorm0;
+    r.rnorm = error * bnrm2;
+    r.line_skips = 0;
     return 0;
 }
 

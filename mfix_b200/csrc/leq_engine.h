@@ -48,7 +48,8 @@ struct SolveResult {
 };
 
 struct SolveOptions {
-    int method = 2;              // LEQ_METHOD: 2 BiCGSTAB (model/leq_bicgs.f), 5 CG (model/leq_cg.f, FP64 only)
+    int method = 2;              // LEQ_METHOD: 2 BiCGSTAB (model/leq_bicgs.f), 3 GMRES (model/leq_gmres.f),
+                                 // 4 BiCGSTAB then GMRES on breakdown, 5 CG (model/leq_cg.f); 3-5 in FP64
     int pc = PC_LINE;
     char sweep[4] = {'R', 'S', 'R', 'S'};
     int precision = PREC_FP64;
@@ -181,6 +182,7 @@ public:
 private:
     int run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &opt, std::vector<SolveResult> &out);
     int run_batch_live(const std::vector<SystemSpec> &specs, const SolveOptions &opt, std::vector<SolveResult> &out);
+    int run_gmres(const SystemSpec &s, const SolveOptions &opt, SolveResult &out);
     std::vector<double *> x0_;  // per system of the last batch: the mixed form's copy of the initial guess
     int launch_setup(const SolveOptions &opt, bool scale);
     int launch_body(const SolveOptions &opt);
@@ -298,6 +300,11 @@ private:
     // standalone kernels
     SysDev *d_one_sys_ = nullptr;
     double *d_dot_partials_ = nullptr;
+    double *gm_basis_ = nullptr;  // GMRES Krylov basis, (ITMAX+1) x DIMENSION_3
+    size_t gm_basis_bytes_ = 0;
+    double *gm_scal_ = nullptr;   // GMRES: block partials, then the current Hessenberg column and y
+    int gm_scal_cap_ = 0;
+    unsigned long long *gm_max_ = nullptr;
     unsigned int *d_dot_counter_ = nullptr;
     double *d_dot_out_ = nullptr;
     size_t sys_cap_ = 0, st_cap_ = 0, tiles_cap_ = 0, prefix_cap_ = 0, part_cap_ = 0, allprefix_cap_ = 0;

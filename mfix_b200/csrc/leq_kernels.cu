@@ -289,6 +289,10 @@ __global__ void k_init_done(BatchView b)
         cg_begin(st);
         return;
     }
+    if (st.method == 3) {  // LEQ_GMRES0: the host drives the iteration; the sweeps run in PH_INNER
+        st.phase = PH_INNER;
+        return;
+    }
     // a nearly singular operator (pressure correction) goes to the FP64 drop-in
     // before any FP32 iteration: its FP32 Krylov process stagnates
     if (st.mixed && __uint_as_float(st.margin_bits) < st.min_margin) {
@@ -2407,8 +2411,113 @@ __global__ void __launch_bounds__(256) k_cg_xr(BatchView b)
     run_close<1>(b, run, fin);
 }
 
+// ------------------------------------------------------------------ LEQ_GMRES0 (METHOD 3)
+// FP64 vector steps of model/leq_gmres.f on one system's device arrays; the
+// Hessenberg and Givens scalars live on the host.  Sums are per-block partials
+// over a fixed grid, added in block order by one block: deterministic.
+
+// W -= h_prev V_prev (when V_prev is given; h_prev read from device memory),
+// then the block partial of (W, V_k): one modified Gram-Schmidt step fused with
+// the next one's dot (:303-314).  V_k may be W itself (the final norm).
+__global__ void __launch_bounds__(256) k_gm_mgs(double *w, const double *vprev, const double *hprev, const double *vk,
+                                                int64_t n, double *partials)
+{
+    const double h = vprev ? *hprev : 0.0;
+    double v[1] = {0.0};
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        double wv = w[p];
+        if (vprev) {
+            wv = wv - h * vprev[p];
+            w[p] = wv;
+        }
+        v[0] += wv * vk[p];
+    }
+    block_sum<1>(v);
+    if (threadIdx.x == 0) partials[blockIdx.x] = v[0];
+}
+
+// out = the partials added in block order (one block).
+__global__ void __launch_bounds__(256) k_gm_sum(const double *partials, int np, double *out)
+{
+    double v[1] = {0.0};
+    for (int t = threadIdx.x; t < np; t += blockDim.x) v[0] += partials[t];
+    block_sum<1>(v);
+    if (threadIdx.x == 0) *out = v[0];
+}
+
+// dst = src * s (V(:,1) = R / NORM_R, V(:,I+1) = WW / H(I+1,I): :283-287, :323-327).
+__global__ void __launch_bounds__(256) k_gm_scale(const double *src, double s, double *dst, int64_t n)
+{
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
+        dst[p] = src[p] * s;
+}
+
+// t = b - t (TEMP = B - A Var, :221-228).
+__global__ void __launch_bounds__(256) k_gm_sub(const double *b, double *t, int64_t n)
+{
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x)
+        t[p] = b[p] - t[p];
+}
+
+// Var += sum_k V(:,k) y(k), the sum over the basis taken per cell in order (:417-426).
+__global__ void __launch_bounds__(256) k_gm_update(double *x, const double *V, const double *y, int m, int64_t n)
+{
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        double d = 0.0;
+        for (int k = 0; k < m; ++k) d = d + V[(size_t)k * n + p] * y[k];
+        x[p] = x[p] + d;
+    }
+}
+
+// max |b| as the bits of a non-negative double (they order like the values).
+__global__ void __launch_bounds__(256) k_gm_maxabs(const double *b, int64_t n, unsigned long long *out)
+{
+    unsigned long long m = 0;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        const unsigned long long bits = (unsigned long long)__double_as_longlong(fabs(b[p]));
+        m = bits > m ? bits : m;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        const unsigned long long other = __shfl_xor_sync(0xffffffffu, m, o);
+        m = other > m ? other : m;
+    }
+    if ((threadIdx.x & 31) == 0) atomicMax(out, m);
+}
+
 // ------------------------------------------------------------------ launchers
 #define CHECK_LAUNCH() return cudaGetLastError()
+
+cudaError_t launch_gm_mgs(double *w, const double *vprev, const double *hprev, const double *vk, int64_t n,
+                          double *partials, int grid, cudaStream_t s)
+{
+    k_gm_mgs<<<grid, 256, 0, s>>>(w, vprev, hprev, vk, n, partials);
+    CHECK_LAUNCH();
+}
+cudaError_t launch_gm_sum(const double *partials, int np, double *out, cudaStream_t s)
+{
+    k_gm_sum<<<1, 256, 0, s>>>(partials, np, out);
+    CHECK_LAUNCH();
+}
+cudaError_t launch_gm_scale(const double *src, double f, double *dst, int64_t n, int grid, cudaStream_t s)
+{
+    k_gm_scale<<<grid, 256, 0, s>>>(src, f, dst, n);
+    CHECK_LAUNCH();
+}
+cudaError_t launch_gm_sub(const double *b, double *t, int64_t n, int grid, cudaStream_t s)
+{
+    k_gm_sub<<<grid, 256, 0, s>>>(b, t, n);
+    CHECK_LAUNCH();
+}
+cudaError_t launch_gm_update(double *x, const double *V, const double *y, int m, int64_t n, int grid, cudaStream_t s)
+{
+    k_gm_update<<<grid, 256, 0, s>>>(x, V, y, m, n);
+    CHECK_LAUNCH();
+}
+cudaError_t launch_gm_maxabs(const double *b, int64_t n, unsigned long long *out, int grid, cudaStream_t s)
+{
+    k_gm_maxabs<<<grid, 256, 0, s>>>(b, n, out);
+    CHECK_LAUNCH();
+}
 
 cudaError_t launch_scale_diag(const BatchView &b, const LaunchCfg &c)
 {

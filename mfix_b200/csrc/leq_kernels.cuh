@@ -54,6 +54,16 @@ cudaError_t launch_cg_p(const BatchView &b, const LaunchCfg &c, int z_id);    //
 cudaError_t launch_cg_matvec(const BatchView &b, const LaunchCfg &c);         // Q = A P, alpha
 cudaError_t launch_cg_xr(const BatchView &b, const LaunchCfg &c);             // R, Var, Rnorm, exit
 
+// LEQ_GMRES0 vector steps (model/leq_gmres.f), FP64 on raw device arrays
+cudaError_t launch_gm_mgs(double *w, const double *vprev, const double *hprev, const double *vk, int64_t n,
+                          double *partials, int grid, cudaStream_t s);  // W -= h V_prev; partials of (W, V_k)
+cudaError_t launch_gm_sum(const double *partials, int np, double *out, cudaStream_t s);
+cudaError_t launch_gm_scale(const double *src, double f, double *dst, int64_t n, int grid, cudaStream_t s);
+cudaError_t launch_gm_sub(const double *b, double *t, int64_t n, int grid, cudaStream_t s);  // t = b - t
+cudaError_t launch_gm_update(double *x, const double *V, const double *y, int m, int64_t n, int grid,
+                             cudaStream_t s);  // x += V y
+cudaError_t launch_gm_maxabs(const double *b, int64_t n, unsigned long long *out, int grid, cudaStream_t s);
+
 // J-line LU factors (l, 1/u, c/u) and DGTSV pivot flags, once per solve
 template <typename T>
 cudaError_t launch_line_factor(const BatchView &b, const LaunchCfg &c, const int *all_line_prefix, int total_lines);
