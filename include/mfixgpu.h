@@ -46,13 +46,15 @@ int mfixgpu_init_geometry(const int *imax2, const int *jmax2, const int *kmax2, 
 
 /* SOLVE_LIN_EQ(VNAME, VNO, VAR, A_M, B_M, M, ITMAX, METHOD, SWEEP, TOL1, PC, IER),
  * model/solve_lin_eq.f:17-78, in gfortran's convention: every argument by
- * reference, CHARACTER lengths appended by value.  Served: METHOD 2 (BiCGSTAB,
+ * reference, CHARACTER lengths appended by value.  Served: METHOD 1 (LEQ_SOR,
+ * :133-135, model/leq_sor.f: rows scaled by 1/A(0), one point-Jacobi step,
+ * ITER_TOT(VNO) set to ITMAX+1, IER left as passed); METHOD 2 (BiCGSTAB,
  * :137-153); METHOD 3 (GMRES, :156-158, model/leq_gmres.f: one restart cycle of
  * ITMAX steps, left-preconditioned by the sweeps, PC ignored, A/B not scaled,
  * IER 0 or 1, FP64); METHOD 4 (:161-171: BiCGSTAB, and on IER -2 GMRES from its
  * result with IER reset to 0); METHOD 5 (CG, :173-176, model/leq_cg.f, FP64).
- * "precision" applies to the BiCGSTAB solves only.  Others return
- * MFIXGPU_ERR_UNSUPPORTED.
+ * "precision" applies to the BiCGSTAB solves only.  Other values return
+ * MFIXGPU_ERR_UNSUPPORTED (the reference stops in MFIX_EXIT).
  * As in model/leq_bicgs.f:194-233 (BiCGSTAB: rows divided by max|A(ijk,:)|) and
  * model/leq_cg.f:197-211 (CG: rows divided by A(ijk,0)), A_M(:,:,M) and B_M(:,M)
  * come back unit-scaled (option "write_back_ab"). */

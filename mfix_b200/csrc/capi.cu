@@ -142,13 +142,13 @@ void solve_impl(int vno, double *var, double *a_m, double *b_m, int m, int itmax
         g.err = "phase index M outside 0:DIMENSION_M";
         return finish(MFIXGPU_ERR_ARGS);
     }
-    // model/solve_lin_eq.f:131-191: BiCGSTAB (2), GMRES (3), BiCGSTAB then GMRES (4), CG (5)
-    if (method < 2 || method > 5) {
-        g.err = "LEQ_METHOD " + std::to_string(method) + " is not served by the GPU path (2, 3, 4, 5)";
+    // model/solve_lin_eq.f:131-191: SOR (1), BiCGSTAB (2), GMRES (3), BiCGSTAB then GMRES (4), CG (5)
+    if (method < 1 || method > 5) {
+        g.err = "LEQ_METHOD " + std::to_string(method) + " is not served by the GPU path (1-5)";
         return finish(MFIXGPU_ERR_UNSUPPORTED);
     }
-    // LEQ_GMRES takes no PC argument and always sweeps with LEQ_MSOLVE (:145-150)
-    const int pc = method == 3 ? PC_LINE : decode_pc(pc4);
+    // LEQ_GMRES and LEQ_SOR take no PC argument (:133-135, :156-158)
+    const int pc = (method == 1 || method == 3) ? PC_LINE : decode_pc(pc4);
     if (pc < 0) {
         g.err = "preconditioner option not found";  // the reference's message, model/leq_bicgs.f:84-85
         return finish(MFIXGPU_ERR_UNSUPPORTED);
@@ -176,8 +176,13 @@ void solve_impl(int vno, double *var, double *a_m, double *b_m, int m, int itmax
         return finish(rc);
     }
     const SolveResult &r = out[0];
-    const int code = r.ier;
-    if (vno >= 1 && vno <= 10) g.iter_tot[vno - 1] += r.iter_tot_add;
+    const int code = method == 1 ? *ier : r.ier;  // LEQ_SOR leaves IER alone
+    if (vno >= 1 && vno <= 10) {
+        if (method == 1)
+            g.iter_tot[vno - 1] = r.iter_tot_add;  // ITER_TOT(VNO) = ITER (model/leq_sor.f:119)
+        else
+            g.iter_tot[vno - 1] += r.iter_tot_add;
+    }
     g.last.iterations = r.iterations;
     g.last.iter_tot_add = r.iter_tot_add;
     g.last.exit_kind = r.exit_kind;

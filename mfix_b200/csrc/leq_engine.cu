@@ -935,9 +935,9 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
     }
     SolveOptions o = opt;
     o.on_device = true;
-    if (opt.method < 2 || opt.method > 5) return fail("LEQ_METHOD not served (2 BiCGSTAB, 3 GMRES, 4, 5 CG)", -10);
-    if ((opt.method == 3 || opt.method == 4) && specs.size() != 1)
-        return fail("GMRES (METHOD 3/4) serves single systems", -10);
+    if (opt.method < 1 || opt.method > 5) return fail("LEQ_METHOD not served (1 SOR, 2 BiCGSTAB, 3 GMRES, 4, 5 CG)", -10);
+    if ((opt.method == 1 || opt.method == 3 || opt.method == 4) && specs.size() != 1)
+        return fail("METHOD 1, 3 and 4 serve single systems", -10);
     if (opt.method == 5 || opt.method == 3) o.precision = PREC_FP64;  // CG and GMRES run their FP64 form only
     writeback_.clear();
     if (!opt.on_device && opt.write_back_ab && opt.method != 3)  // GMRES leaves A and B as they are
@@ -952,6 +952,49 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
     for (int q = 0; q < 4; ++q) {
         const char ch = opt.sweep[q];
         if (ch == 'I' || ch == 'i' || ch == 'K' || ch == 'k' || ch == 'A' || ch == 'a') rs_only = false;
+    }
+    if (opt.method == 1) {  // LEQ_SOR: the scaling and one point-Jacobi step (model/leq_sor.f)
+        const int64_t n = dev[0].n;
+        SysDev d{};
+        d.imax2 = dev[0].imax2;
+        d.jmax2 = dev[0].jmax2;
+        d.kmax2 = dev[0].kmax2;
+        d.do_k = dev[0].do_k;
+        d.n = n;
+        d.div_j = make_fastdiv((uint32_t)d.jmax2);
+        d.div_i = make_fastdiv((uint32_t)d.imax2);
+        if (!d_one_sys_) CK(cudaMalloc((void **)&d_one_sys_, sizeof(SysDev)));
+        CK(cudaMemcpyAsync(d_one_sys_, &d, sizeof(SysDev), cudaMemcpyHostToDevice, stream_));
+        if ((size_t)n * 8 > gm_basis_bytes_) {  // VAR_tmp in the GMRES scratch
+            cudaFree(gm_basis_);
+            gm_basis_bytes_ = 0;
+            if (cudaMalloc((void **)&gm_basis_, (size_t)n * 8) != cudaSuccess) {
+                gm_basis_ = nullptr;
+                cudaGetLastError();
+                return fail("device memory for VAR_tmp", -11);
+            }
+            gm_basis_bytes_ = (size_t)n * 8;
+        }
+        timing_ = SolveTiming{};
+        CK(cudaEventRecord(ev_t0_, stream_));
+        const int grid = std::max(1, std::min((int)((n + 255) / 256), sms_ * 8));
+        CK(launch_sor(d_one_sys_, dev[0].a, dev[0].b, dev[0].x, gm_basis_, dev[0].itmax, n, grid, stream_));
+        CK(cudaEventRecord(ev_t1_, stream_));
+        CK(cudaEventSynchronize(ev_t1_));
+        cudaEventElapsedTime(&timing_.device_ms, ev_t0_, ev_t1_);
+        timing_.kernel_launches = dev[0].itmax >= 1 ? 2 : 1;
+        out[0] = SolveResult{};
+        out[0].iterations = std::max(dev[0].itmax, 0) + 1;
+        out[0].iter_tot_add = out[0].iterations;  // the value ITER_TOT(VNO) is set to (:119)
+        out[0].exit_kind = EX_ITMAX;
+        int rc = issue_writeback();
+        if (rc) return rc;
+        if (!opt.on_device) {
+            CK(cudaMemcpyAsync(specs[0].x, dev[0].x, (size_t)n * 8, cudaMemcpyDeviceToHost, stream_));
+            CK(cudaStreamSynchronize(stream_));
+            CK(cudaStreamSynchronize(side_));
+        }
+        return 0;
     }
     if (opt.method == 3) {  // LEQ_GMRES
         int rc = run_gmres(dev[0], o, out[0]);

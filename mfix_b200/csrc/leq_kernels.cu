@@ -2484,8 +2484,62 @@ __global__ void __launch_bounds__(256) k_gm_maxabs(const double *b, int64_t n, u
     if ((threadIdx.x & 31) == 0) atomicMax(out, m);
 }
 
+// ------------------------------------------------------------------ LEQ_SOR (METHOD 1)
+// model/leq_sor.f: each row times 1/A(ijk,0), A(ijk,0) set to one (:75-85).
+__global__ void __launch_bounds__(256) k_sor_scale(const SysDev *sysp, double *a, double *b)
+{
+    const int64_t n = sysp->n;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        const double oam = 1.0 / a[3 * n + p];
+        a[3 * n + p] = 1.0;
+#pragma unroll
+        for (int q = 0; q < 7; ++q)
+            if (q != 3) a[q * n + p] = a[q * n + p] * oam;
+        b[p] = b[p] * oam;
+    }
+}
+
+// VAR_tmp = VAR + OMEGA (B - sum_nb A_nb VAR_nb - VAR) with OMEGA = 1 and the
+// neighbour order of :93-110 (3-D: i, j, k pairs; 2-D: j pair, then i pair).
+__global__ void __launch_bounds__(256) k_sor_step(const SysDev *sysp, const double *a, const double *b,
+                                                  const double *x, double *tmp)
+{
+    const SysDev &d = *sysp;
+    const int64_t n = d.n;
+    for (int64_t p = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (int64_t)gridDim.x * blockDim.x) {
+        const Offs o = cell_offs(d, (uint32_t)p);
+        double v;
+        if (d.do_k) {
+            v = b[p] - a[2 * n + p] * x[p + o.im];
+            v = v - a[4 * n + p] * x[p + o.ip];
+            v = v - a[1 * n + p] * x[p + o.jm];
+            v = v - a[5 * n + p] * x[p + o.jp];
+            v = v - a[0 * n + p] * x[p + o.km];
+            v = v - a[6 * n + p] * x[p + o.kp];
+        } else {
+            v = b[p] - a[1 * n + p] * x[p + o.jm];
+            v = v - a[5 * n + p] * x[p + o.jp];
+            v = v - a[2 * n + p] * x[p + o.im];
+            v = v - a[4 * n + p] * x[p + o.ip];
+        }
+        v = v - x[p];
+        tmp[p] = x[p] + 1.0 * v;
+    }
+}
+
 // ------------------------------------------------------------------ launchers
 #define CHECK_LAUNCH() return cudaGetLastError()
+
+cudaError_t launch_sor(const SysDev *sys_dev, double *a, double *b, double *x, double *tmp, int steps, int64_t n,
+                       int grid, cudaStream_t s)
+{
+    k_sor_scale<<<grid, 256, 0, s>>>(sys_dev, a, b);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || steps < 1) return e;
+    k_sor_step<<<grid, 256, 0, s>>>(sys_dev, a, b, x, tmp);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    return cudaMemcpyAsync(x, tmp, (size_t)n * sizeof(double), cudaMemcpyDeviceToDevice, s);
+}
 
 cudaError_t launch_gm_mgs(double *w, const double *vprev, const double *hprev, const double *vk, int64_t n,
                           double *partials, int grid, cudaStream_t s)

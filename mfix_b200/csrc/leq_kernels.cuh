@@ -54,6 +54,10 @@ cudaError_t launch_cg_p(const BatchView &b, const LaunchCfg &c, int z_id);    //
 cudaError_t launch_cg_matvec(const BatchView &b, const LaunchCfg &c);         // Q = A P, alpha
 cudaError_t launch_cg_xr(const BatchView &b, const LaunchCfg &c);             // R, Var, Rnorm, exit
 
+// LEQ_SOR (model/leq_sor.f): the scaling, then (steps >= 1) one point-Jacobi step through tmp
+cudaError_t launch_sor(const SysDev *sys_dev, double *a, double *b, double *x, double *tmp, int steps, int64_t n,
+                       int grid, cudaStream_t s);
+
 // LEQ_GMRES0 vector steps (model/leq_gmres.f), FP64 on raw device arrays
 cudaError_t launch_gm_mgs(double *w, const double *vprev, const double *hprev, const double *vk, int64_t n,
                           double *partials, int grid, cudaStream_t s);  // W -= h V_prev; partials of (W, V_k)

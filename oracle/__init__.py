@@ -62,6 +62,8 @@ def lib() -> C.CDLL:
         L.orc_scale_diag.argtypes = [C.POINTER(Geom), vp, vp]
         L.orc_leq_gmres.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_char_p, C.c_double, C.c_int, C.POINTER(Stats)]
         L.orc_leq_gmres.restype = C.c_int
+        L.orc_leq_sor.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_int, C.POINTER(Stats)]
+        L.orc_leq_sor.restype = C.c_int
         L.orc_true_resid.argtypes = [C.POINTER(Geom), vp, vp, vp]
         L.orc_true_resid.restype = C.c_double
         L.orc_truth_solve.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_double, C.c_int, C.c_uint64, _dp]
@@ -152,6 +154,14 @@ def leq_gmres(s, sweep: str = "RSRS") -> dict:
     st = Stats()
     lib().orc_leq_gmres(C.byref(geom(s)), _p(s.x), _p(s.a), _p(s.b), sweep.ljust(4)[:4].encode(), s.tol, s.itmax,
                         C.byref(st))
+    return {k: getattr(st, k) for k, _ in Stats._fields_}
+
+
+def leq_sor(s) -> dict:
+    """LEQ_SOR (METHOD 1) on s in place (rows scaled by 1/A(0), A(0) = 1; s.x one
+    point-Jacobi step).  iter_tot_add is the value ITER_TOT(VNO) is set to."""
+    st = Stats()
+    lib().orc_leq_sor(C.byref(geom(s)), _p(s.x), _p(s.a), _p(s.b), s.itmax, C.byref(st))
     return {k: getattr(st, k) for k, _ in Stats._fields_}
 
 

@@ -913,3 +913,50 @@ int orc_leq_gmres(const orc_geom *g, double *var, const double *a, const double 
     st->rnorm = error * bnrm2;
     return st->ier;
 }
+
+/* ------------------------------------------------------------------ LEQ_SOR */
+/* METHOD 1 (model/solve_lin_eq.f:133-135, model/leq_sor.f:17-122).  Each row is
+ * multiplied by 1/A(ijk,0) with A(ijk,0) set to one (:75-85).  Every one of the
+ * ITMAX passes forms VAR_tmp = VAR + OMEGA (B - sum_nb A_nb VAR_nb - VAR) from the
+ * same VAR (OMEGA = 1, :57, :87-113; the neighbour order differs between 3-D and
+ * 2-D), and VAR takes VAR_tmp once after the loop (:115-117), so the result is
+ * one point-Jacobi step.  ITER_TOT(VNO) is set, not increased, to the loop
+ * counter's final value ITMAX + 1 (:119); IER is left alone.  With ITMAX < 1 the
+ * reference copies an array it never wrote; here VAR is left unchanged. */
+int orc_leq_sor(const orc_geom *g, double *var, double *a, double *b, int itmax, orc_stats *st)
+{
+    memset(st, 0, sizeof(*st));
+    const int64_t n = g->n, c1 = g->jmax2, c2 = (int64_t)g->jmax2 * g->imax2;
+    for (int64_t p = 0; p < n; ++p) {
+        const double oam = 1.0 / a[3 * n + p];
+        a[3 * n + p] = 1.0;
+        for (int d = 0; d < 7; ++d)
+            if (d != 3) a[(int64_t)d * n + p] = a[(int64_t)d * n + p] * oam;
+        b[p] = b[p] * oam;
+    }
+    st->iter_tot_add = (itmax > 0 ? itmax : 0) + 1;
+    st->iterations = st->iter_tot_add;
+    st->exit_kind = 3;
+    if (itmax < 1) return 0;
+    double *tmp = (double *)malloc((size_t)n * sizeof(double));
+#pragma omp parallel for schedule(static)
+    for (int64_t p = 0; p < n; ++p) {
+        const int64_t line = p / g->jmax2;
+        const int j = (int)(p - line * g->jmax2), k = (int)(line / g->imax2), i = (int)(line - (int64_t)k * g->imax2);
+        const int64_t jm = j > 0 ? -1 : 0, jp = j < g->jmax2 - 1 ? 1 : 0;
+        const int64_t im = i > 0 ? -c1 : 0, ip = i < g->imax2 - 1 ? c1 : 0;
+        double v;
+        if (g->do_k) {
+            const int64_t km = k > 0 ? -c2 : 0, kp = k < g->kmax2 - 1 ? c2 : 0;
+            v = b[p] - a[2 * n + p] * var[p + im] - a[4 * n + p] * var[p + ip] - a[1 * n + p] * var[p + jm] -
+                a[5 * n + p] * var[p + jp] - a[0 * n + p] * var[p + km] - a[6 * n + p] * var[p + kp] - var[p];
+        } else {
+            v = b[p] - a[1 * n + p] * var[p + jm] - a[5 * n + p] * var[p + jp] - a[2 * n + p] * var[p + im] -
+                a[4 * n + p] * var[p + ip] - var[p];
+        }
+        tmp[p] = var[p] + 1.0 * v;
+    }
+    memcpy(var, tmp, (size_t)n * sizeof(double));
+    free(tmp);
+    return 0;
+}

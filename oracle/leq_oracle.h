@@ -77,6 +77,10 @@ int orc_leq_cg(const orc_geom *g, double *var, double *a, double *b, const char 
 int orc_leq_gmres(const orc_geom *g, double *var, const double *a, const double *b, const char *sweep, double tol,
                   int itmax, orc_stats *st);
 
+/* LEQ_SOR (METHOD 1): one point-Jacobi step after scaling each row by 1/A(0);
+ * st->iter_tot_add is the value ITER_TOT(VNO) is set to (ITMAX + 1). */
+int orc_leq_sor(const orc_geom *g, double *var, double *a, double *b, int itmax, orc_stats *st);
+
 /* true residual ||b - A x||_2 in long double */
 double orc_true_resid(const orc_geom *g, const double *a, const double *b, const double *x);
 

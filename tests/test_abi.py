@@ -61,7 +61,7 @@ def test_argument_errors_before_device_work():
     x = np.zeros(120)
     assert leq.init_geometry(4, 5, 6, 1, 120, 1) == 0
     assert leq.solve_lin_eq("U_g", 3, x, a, b, 5, 10, 2, "RSRS", 1e-8, "LINE") == leq.IER_ARGS  # M > DIMENSION_M
-    assert leq.solve_lin_eq("U_g", 3, x, a, b, 0, 10, 1, "RSRS", 1e-8, "LINE") == leq.IER_UNSUPPORTED  # SOR
+    assert leq.solve_lin_eq("U_g", 3, x, a, b, 0, 10, 0, "RSRS", 1e-8, "LINE") == leq.IER_UNSUPPORTED
     assert leq.solve_lin_eq("U_g", 3, x, a, b, 0, 10, 6, "RSRS", 1e-8, "LINE") == leq.IER_UNSUPPORTED
     assert leq.solve_lin_eq("U_g", 3, x, a, b, 0, 10, 2, "RSRS", 1e-8, "ILU") == leq.IER_UNSUPPORTED
 

@@ -120,7 +120,7 @@ def test_ier_itmax_exhausted(itmax):
 
 def test_unsupported_method_and_pc():
     s = S.conv_diff(6, 6, 6, seed=15)
-    assert leq.solve_system(s.copy(), method=1) == leq.IER_UNSUPPORTED
+    assert leq.solve_system(s.copy(), method=6) == leq.IER_UNSUPPORTED
     assert leq.solve_system(s.copy(), pc="line") == leq.IER_UNSUPPORTED
     assert leq.solve_system(s.copy(), pc="ILU ") == leq.IER_UNSUPPORTED
 

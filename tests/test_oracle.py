@@ -268,3 +268,19 @@ def test_gmres_zero_rhs_and_itmax():
     t.itmax = 3
     st = O.leq_gmres(t)
     assert st["ier"] == 1 and st["iterations"] == 3
+
+
+def test_sor_is_one_jacobi_step():
+    """LEQ_SOR as the reference has it: every pass starts from the same VAR, so
+    the result is one point-Jacobi step on the diagonal-scaled rows."""
+    s = S.conv_diff(6, 7, 5, seed=1)
+    s.x = np.random.default_rng(0).standard_normal(s.n)
+    s.itmax = 4
+    t = s.copy()
+    st = O.leq_sor(t)
+    a = s.a / s.a[3]
+    a[3] = 1.0
+    b = s.b / s.a[3]
+    xj = s.x + (b - S.matvec_np(s.imax2, s.jmax2, s.kmax2, s.do_k, a, s.x))
+    assert np.max(np.abs(xj - t.x)) <= 1e-14 * np.max(np.abs(xj))
+    assert np.array_equal(t.a[3], np.ones(s.n)) and st["iter_tot_add"] == 5
