@@ -618,7 +618,7 @@ def run_cg_bench(args) -> None:
     avg_s = (jl_ms / 1e3) / max(jl_work, 1)
     achieved = alg_launch / avg_s / 1e9
     ref = sys0.copy()
-    import oracle as O  # the checker: true residual of the scaled system
+    import oracle as O  # the oracle: true residual of the scaled system
 
     O.scale_diag(ref)
     rel = O.true_resid(ref, x_h) / O.true_resid(ref, np.zeros(n))
