@@ -76,3 +76,20 @@ def test_uniform_stream_matches_oracle():
     got = S.uniform(0x5EED, 0xA1, idx)
     for q, v in zip(idx, got):
         assert O.uniform(0x5EED, 0xA1, int(q)) == v
+
+
+def test_diffusion_sym_scaled_operator_is_symmetric():
+    """One interior diagonal: dividing each row by its diagonal (LEQ_CG0's
+    scaling) keeps the operator symmetric, which conjugate gradients needs."""
+    s = S.diffusion_sym(7, 9, 6, seed=2)
+    a = s.a / s.a[3]
+    n = s.n
+    rng = np.random.default_rng(0)
+    u, v = rng.standard_normal(n), rng.standard_normal(n)
+    interior = s.a[3] != -1.0  # wall rows are identity rows, decoupled from the interior
+    u[~interior] = 0.0
+    v[~interior] = 0.0
+    Au = S.matvec_np(s.imax2, s.jmax2, s.kmax2, s.do_k, a, u)
+    Av = S.matvec_np(s.imax2, s.jmax2, s.kmax2, s.do_k, a, v)
+    assert abs(v @ Au - u @ Av) <= 1e-12 * abs(v @ Au)
+    assert np.allclose(s.a[3][interior], s.a[3][interior][0])
