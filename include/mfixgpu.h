@@ -71,6 +71,26 @@ void mfixgpu_solve_lin_eq(const char *vname, int vname_len, int vno, double *var
 /* ITER_TOT(VNO) of MODULE leqsol (model/leqsol_mod.f:17), 1-based VNO in
  * 1..10 (DIM_EQS, model/param_mod.f:97); the accounting of
  * model/leq_bicgs.f:458,491. */
+/* Batching the SIMPLE loop's independent SOLVE_LIN_EQ calls (no reference
+ * counterpart).  The per-phase calls of one transport equation solve
+ * independent slices A_M(:,:,M) / B_M(:,M) back to back (for example the U_g and
+ * U_s(M) calls of model/solve_vel_star.f:308-331); a caller that replaces them by
+ * mfixgpu_solve_lin_eq_defer_ (the same dummy list and convention as
+ * mfixgpu_solve_lin_eq_) and then calls mfixgpu_solve_lin_eq_flush solves them
+ * as one batch, each with the result it gets alone.  A deferred call is checked
+ * at once (a failing check sets its IER at once); a METHOD 2 call with red/black
+ * sweeps is queued with IER = MFIXGPU_ERR_INCOMPLETE, any other call is solved at
+ * once.  Until the flush the arrays and IER must stay in place and untouched.
+ * The flush solves the queue, one batch per (PC, SWEEP), writes every IER, adds
+ * to ITER_TOT, and returns 0 or the first error code (also written to the IER of
+ * every call of the batch that failed). */
+void mfixgpu_solve_lin_eq_defer_(const char *vname, const int *vno, double *var, double *a_m, double *b_m,
+                                 const int *m, const int *itmax, const int *method, const char *sweep,
+                                 const double *tol1, const char *pc, int *ier, size_t vname_len, size_t sweep_len,
+                                 size_t pc_len);
+int mfixgpu_solve_lin_eq_flush(void);
+int mfixgpu_solve_lin_eq_pending(void); /* calls queued */
+
 int mfixgpu_iter_tot(int vno);
 void mfixgpu_reset_iter_tot(void);
 

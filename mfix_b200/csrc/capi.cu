@@ -50,6 +50,14 @@ struct Global {
     mfixgpu_stats last{};
     SolveTiming last_timing{};
     std::string err;
+    // SOLVE_LIN_EQ calls queued by mfixgpu_solve_lin_eq_defer_ until the next flush
+    struct Deferred {
+        int vno, m, itmax;
+        double *var, *a_m, *b_m, tol;
+        char sweep[4], pc[4];
+        int *ier;
+    };
+    std::vector<Deferred> deferred;
 };
 
 Global &G()
@@ -201,6 +209,51 @@ void solve_impl(int vno, double *var, double *a_m, double *b_m, int m, int itmax
     finish(code);
 }
 
+// A SOLVE_LIN_EQ call queued for the next flush when it can join a batch
+// (METHOD 2 with red/black sweeps); any other call is solved at once.  The
+// checks are solve_impl's, so a call that would fail fails here, at once.
+void defer_impl(int vno, double *var, double *a_m, double *b_m, int m, int itmax, int method, const char sweep4[4],
+                double tol, const char pc4[4], int *ier)
+{
+    if (!ier) return;
+    bool batchable = method == 2;
+    for (int q = 0; q < 4; ++q) {
+        const char ch = sweep4[q];
+        if (ch == 'I' || ch == 'i' || ch == 'K' || ch == 'k' || ch == 'A' || ch == 'a') batchable = false;
+    }
+    {
+        Global &g = G();
+        std::lock_guard<std::mutex> lk(g.mu);
+        int code = 0;
+        if (!g.geom.set) {
+            g.err = "mfixgpu_init_geometry has not been called";
+            code = MFIXGPU_ERR_NOGEOM;
+        } else if (!var || !a_m || !b_m) {
+            g.err = "null array argument";
+            code = MFIXGPU_ERR_ARGS;
+        } else if (m < 0 || m > g.geom.dimension_m) {
+            g.err = "phase index M outside 0:DIMENSION_M";
+            code = MFIXGPU_ERR_ARGS;
+        } else if (batchable && decode_pc(pc4) < 0) {
+            g.err = "preconditioner option not found";
+            code = MFIXGPU_ERR_UNSUPPORTED;
+        }
+        if (code) {
+            *ier = code;
+            return;
+        }
+        if (batchable) {
+            Global::Deferred d{vno, m, itmax, var, a_m, b_m, tol, {}, {}, ier};
+            std::memcpy(d.sweep, sweep4, 4);
+            std::memcpy(d.pc, pc4, 4);
+            g.deferred.push_back(d);
+            *ier = MFIXGPU_ERR_INCOMPLETE;  // until the flush
+            return;
+        }
+    }
+    solve_impl(vno, var, a_m, b_m, m, itmax, method, sweep4, tol, pc4, ier);
+}
+
 }  // namespace
 
 namespace mfixgpu {
@@ -259,6 +312,96 @@ void mfixgpu_solve_lin_eq(const char *vname, int vname_len, int vno, double *var
     fortran_char4(sweep, sweep_len < 0 ? 0 : (size_t)sweep_len, s4);
     fortran_char4(pc, pc_len < 0 ? 0 : (size_t)pc_len, p4);
     solve_impl(vno, var, a_m, b_m, m, itmax, method, s4, tol1, p4, ier);
+}
+
+void mfixgpu_solve_lin_eq_defer_(const char *vname, const int *vno, double *var, double *a_m, double *b_m,
+                                 const int *m, const int *itmax, const int *method, const char *sweep,
+                                 const double *tol1, const char *pc, int *ier, size_t vname_len, size_t sweep_len,
+                                 size_t pc_len)
+{
+    (void)vname;
+    (void)vname_len;
+    if (!vno || !m || !itmax || !method || !tol1) {
+        if (ier) *ier = MFIXGPU_ERR_ARGS;
+        return;
+    }
+    char s4[4], p4[4];
+    fortran_char4(sweep, sweep_len, s4);
+    fortran_char4(pc, pc_len, p4);
+    defer_impl(*vno, var, a_m, b_m, *m, *itmax, *method, s4, *tol1, p4, ier);
+}
+
+int mfixgpu_solve_lin_eq_pending(void)
+{
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    return (int)g.deferred.size();
+}
+
+int mfixgpu_solve_lin_eq_flush(void)
+{
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    std::vector<Global::Deferred> all;
+    all.swap(g.deferred);
+    if (all.empty()) return 0;
+    Engine *e = engine_locked(g);
+    if (!e) {
+        for (auto &d : all) *d.ier = MFIXGPU_ERR_CUDA;
+        return MFIXGPU_ERR_CUDA;
+    }
+    const double t0 = now_s();
+    int first_rc = 0;
+    std::vector<bool> done(all.size(), false);
+    mfixgpu_stats agg{};
+    for (size_t q0 = 0; q0 < all.size(); ++q0) {
+        if (done[q0]) continue;
+        // one batch per (PC, SWEEP): every call of the group shares the solver options
+        std::vector<size_t> grp;
+        for (size_t q = q0; q < all.size(); ++q)
+            if (!done[q] && !std::memcmp(all[q].pc, all[q0].pc, 4) && !std::memcmp(all[q].sweep, all[q0].sweep, 4)) {
+                grp.push_back(q);
+                done[q] = true;
+            }
+        const int64_t n = g.geom.n;
+        std::vector<SystemSpec> specs(grp.size());
+        for (size_t k = 0; k < grp.size(); ++k) {
+            const Global::Deferred &d = all[grp[k]];
+            SystemSpec &s = specs[k];
+            s.imax2 = g.geom.imax2;
+            s.jmax2 = g.geom.jmax2;
+            s.kmax2 = g.geom.kmax2;
+            s.do_k = g.geom.do_k;
+            s.n = n;
+            s.a = d.a_m + (size_t)d.m * 7 * (size_t)n;  // A_M(:,:,M)
+            s.b = d.b_m + (size_t)d.m * (size_t)n;      // B_M(:,M)
+            s.x = d.var;
+            s.tol = d.tol;
+            s.itmax = d.itmax;
+        }
+        std::vector<SolveResult> out;
+        const int rc = e->solve(specs, make_opts(g.opt, decode_pc(all[q0].pc), all[q0].sweep), out);
+        if (rc) {
+            g.err = e->last_error();
+            for (size_t q : grp) *all[q].ier = rc;
+            if (!first_rc) first_rc = rc;
+            continue;
+        }
+        for (size_t k = 0; k < grp.size(); ++k) {
+            const Global::Deferred &d = all[grp[k]];
+            *d.ier = out[k].ier;
+            if (d.vno >= 1 && d.vno <= 10) g.iter_tot[d.vno - 1] += out[k].iter_tot_add;
+            agg.iterations = std::max(agg.iterations, out[k].iterations);
+            agg.iter_tot_add += out[k].iter_tot_add;
+        }
+        agg.device_ms += e->timing().device_ms;
+        agg.kernel_launches += e->timing().kernel_launches;
+        g.last_timing = e->timing();
+    }
+    agg.seconds = now_s() - t0;
+    agg.ier = first_rc;
+    g.last = agg;
+    return first_rc;
 }
 
 int mfixgpu_iter_tot(int vno)

@@ -103,6 +103,12 @@ def _declare(L: C.CDLL) -> None:
     L.mfixgpu_solve_lin_eq.argtypes = [C.c_char_p, C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
                                        C.c_int, C.c_int, C.c_char_p, C.c_int, C.c_double, C.c_char_p, C.c_int, _ip]
     L.mfixgpu_solve_lin_eq.restype = None
+    L.mfixgpu_solve_lin_eq_defer_.argtypes = L.mfixgpu_solve_lin_eq_.argtypes
+    L.mfixgpu_solve_lin_eq_defer_.restype = None
+    L.mfixgpu_solve_lin_eq_flush.argtypes = []
+    L.mfixgpu_solve_lin_eq_flush.restype = C.c_int
+    L.mfixgpu_solve_lin_eq_pending.argtypes = []
+    L.mfixgpu_solve_lin_eq_pending.restype = C.c_int
     L.mfixgpu_iter_tot.argtypes = [C.c_int]
     L.mfixgpu_iter_tot.restype = C.c_int
     L.mfixgpu_reset_iter_tot.argtypes = []
@@ -165,6 +171,29 @@ def solve_lin_eq(vname: str, vno: int, var: np.ndarray, a_m: np.ndarray, b_m: np
                             C.byref(C.c_int(itmax)), C.byref(C.c_int(method)), sw, C.byref(C.c_double(tol1)), pcs,
                             C.byref(ier), len(vn), len(sw), len(pcs))
     return ier.value
+
+
+def defer_lin_eq(vname: str, vno: int, var: np.ndarray, a_m: np.ndarray, b_m: np.ndarray, m: int, itmax: int,
+                 method: int, sweep: str, tol1: float, pc: str) -> C.c_int:
+    """mfixgpu_solve_lin_eq_defer_: SOLVE_LIN_EQ's arguments, queued for flush_lin_eq().
+    Returns the IER cell (MFIXGPU_ERR_INCOMPLETE until the flush writes it); the
+    arrays and the cell must stay alive and untouched until then."""
+    L = lib()
+    ier = C.c_int(0)
+    vn, sw, pcs = vname.encode(), sweep.encode(), pc.encode()
+    L.mfixgpu_solve_lin_eq_defer_(vn, C.byref(C.c_int(vno)), _ptr(var), _ptr(a_m), _ptr(b_m), C.byref(C.c_int(m)),
+                                  C.byref(C.c_int(itmax)), C.byref(C.c_int(method)), sw, C.byref(C.c_double(tol1)),
+                                  pcs, C.byref(ier), len(vn), len(sw), len(pcs))
+    return ier
+
+
+def flush_lin_eq() -> int:
+    """mfixgpu_solve_lin_eq_flush: solve every deferred call; 0 or the first error code."""
+    return lib().mfixgpu_solve_lin_eq_flush()
+
+
+def pending_lin_eq() -> int:
+    return lib().mfixgpu_solve_lin_eq_pending()
 
 
 def last_stats() -> dict:

@@ -142,3 +142,23 @@ def test_server_config_errors_before_device_work():
     if not _gpu_visible():
         assert create() == leq.IER_CUDA
         assert "no CUDA device" in leq.last_error()
+
+
+@pytest.mark.skipif(_gpu_visible(), reason="checks the behaviour without a GPU")
+def test_deferred_calls_without_gpu():
+    """mfixgpu_solve_lin_eq_defer_ checks each call at once and queues the
+    batchable ones (IER = INCOMPLETE until the flush); the flush writes every
+    queued IER, here the no-device code."""
+    n = 120
+    a = np.zeros((3, 7, n))
+    a[:, 3] = -1.0
+    b = np.ones((3, n))
+    xs = [np.zeros(n) for _ in range(3)]
+    assert leq.init_geometry(4, 5, 6, 1, n, 2) == 0
+    bad = leq.defer_lin_eq("U_s", 3, xs[0], a, b, 5, 10, 2, "RSRS", 1e-8, "LINE")  # M > DIMENSION_M
+    assert bad.value == leq.IER_ARGS and leq.pending_lin_eq() == 0
+    cells = [leq.defer_lin_eq("U_s", 3, xs[m], a, b, m, 10, 2, "RSRS", 1e-8, "LINE") for m in range(3)]
+    assert [c.value for c in cells] == [leq.IER_INCOMPLETE] * 3 and leq.pending_lin_eq() == 3
+    assert leq.flush_lin_eq() == leq.IER_CUDA
+    assert [c.value for c in cells] == [leq.IER_CUDA] * 3 and leq.pending_lin_eq() == 0
+    assert leq.flush_lin_eq() == 0  # nothing queued

@@ -151,3 +151,33 @@ def test_solution_vs_truth():
     assert ier == 0
     err = np.linalg.norm(s.x - x_truth) / np.linalg.norm(x_truth)
     assert err < 1e-6
+
+
+def test_deferred_phase_calls_equal_single_calls():
+    """The phases M = 0..2 of one A_M(:,:,0:DIMENSION_M), as the SIMPLE loop
+    solves them back to back (model/solve_vel_star.f:308-331), deferred and
+    flushed as one batch: each phase's result, IER and ITER_TOT contribution
+    equal its single call's, bit for bit."""
+    phases = [S.conv_diff(12, 15, 10, seed=70 + m) for m in range(3)]
+    s0 = phases[0]
+    n = s0.n
+    a = np.ascontiguousarray(np.stack([p.a for p in phases]))  # A_M(DIMENSION_3, -3:3, 0:2)
+    b = np.ascontiguousarray(np.stack([p.b for p in phases]))  # B_M(DIMENSION_3, 0:2)
+    assert leq.init_geometry(s0.imax2, s0.jmax2, s0.kmax2, s0.do_k, n, 2) == 0
+    a1, b1 = a.copy(), b.copy()
+    x1 = [np.zeros(n) for _ in range(3)]
+    t0 = leq.iter_tot(3)
+    iers1 = [leq.solve_lin_eq("U_s", 3, x1[m], a1, b1, m, 500, 2, "RSRS", 1e-8, "LINE") for m in range(3)]
+    single_tot = leq.iter_tot(3) - t0
+    a2, b2 = a.copy(), b.copy()
+    x2 = [np.zeros(n) for _ in range(3)]
+    t0 = leq.iter_tot(3)
+    cells = [leq.defer_lin_eq("U_s", 3, x2[m], a2, b2, m, 500, 2, "RSRS", 1e-8, "LINE") for m in range(3)]
+    assert leq.pending_lin_eq() == 3
+    assert leq.flush_lin_eq() == 0, leq.last_error()
+    assert leq.pending_lin_eq() == 0
+    assert [c.value for c in cells] == iers1 == [0, 0, 0]
+    assert leq.iter_tot(3) - t0 == single_tot
+    for m in range(3):
+        assert np.array_equal(x1[m], x2[m])
+    assert np.array_equal(a1, a2) and np.array_equal(b1, b2)  # every slice came back unit-scaled
