@@ -9,7 +9,7 @@ module mfixgpu_mod
    use iso_c_binding, only: c_int, c_int64_t, c_double, c_char, c_ptr, c_null_char
    implicit none
    private
-   public :: mfixgpu_setup, mfixgpu_set_option, mfixgpu_iter_tot, mfixgpu_finalize
+   public :: mfixgpu_setup, mfixgpu_set_option, mfixgpu_iter_tot, mfixgpu_finalize, mfixgpu_flush
 
    interface
       integer(c_int) function c_init_geometry(imax2, jmax2, kmax2, do_k, dimension_3, dimension_m) &
@@ -44,6 +44,10 @@ module mfixgpu_mod
 
       subroutine c_finalize() bind(C, name="mfixgpu_finalize")
       end subroutine c_finalize
+
+      integer(c_int) function c_flush() bind(C, name="mfixgpu_solve_lin_eq_flush")
+         import :: c_int
+      end function c_flush
    end interface
 
 contains
@@ -74,6 +78,12 @@ contains
    subroutine mfixgpu_finalize()
       call c_finalize()
    end subroutine mfixgpu_finalize
+
+   !> Solves every call queued by SOLVE_LIN_EQ_DEFER as one batch and writes their
+   !> IERs; returns 0 or the first error code.
+   integer function mfixgpu_flush()
+      mfixgpu_flush = c_flush()
+   end function mfixgpu_flush
 
 end module mfixgpu_mod
 
@@ -113,3 +123,26 @@ subroutine solve_lin_eq(vname, vno, var, a_m, b_m, m, itmax, method, sweep, tol1
                        int(itmax, c_int), int(method, c_int), sweep, 4_c_int, real(tol1, c_double), pc, 4_c_int, cier)
    ier = int(cier)
 end subroutine solve_lin_eq
+
+!> SOLVE_LIN_EQ_DEFER: SOLVE_LIN_EQ's dummy list, the call queued for MFIXGPU_FLUSH
+!> (the per-phase calls of one equation, e.g. model/solve_vel_star.f:308-331, then
+!> solve as one batch).  VAR, A_M, B_M and IER must stay in place and untouched
+!> until the flush; IER reads -15 until then.  The library's entry point takes
+!> gfortran's implicit convention (every argument by reference, the CHARACTER
+!> lengths appended), so it is called without an interface block.
+subroutine solve_lin_eq_defer(vname, vno, var, a_m, b_m, m, itmax, method, sweep, tol1, pc, ier)
+   use param, only: dimension_3, dimension_m
+   implicit none
+   character(len=*), intent(in) :: vname
+   integer, intent(in) :: vno
+   double precision, intent(inout) :: var(dimension_3)
+   double precision, intent(inout) :: a_m(dimension_3, -3:3, 0:dimension_m)
+   double precision, intent(inout) :: b_m(dimension_3, 0:dimension_m)
+   integer, intent(in) :: m, itmax, method
+   character(len=4), intent(in) :: sweep
+   double precision, intent(in) :: tol1
+   character(len=4), intent(in) :: pc
+   integer, intent(inout) :: ier
+   external mfixgpu_solve_lin_eq_defer
+   call mfixgpu_solve_lin_eq_defer(vname, vno, var, a_m, b_m, m, itmax, method, sweep, tol1, pc, ier)
+end subroutine solve_lin_eq_defer
