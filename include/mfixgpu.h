@@ -68,9 +68,6 @@ void mfixgpu_solve_lin_eq(const char *vname, int vname_len, int vno, double *var
                           int m, int itmax, int method, const char *sweep, int sweep_len, double tol1,
                           const char *pc, int pc_len, int *ier);
 
-/* ITER_TOT(VNO) of MODULE leqsol (model/leqsol_mod.f:17), 1-based VNO in
- * 1..10 (DIM_EQS, model/param_mod.f:97); the accounting of
- * model/leq_bicgs.f:458,491. */
 /* Batching the SIMPLE loop's independent SOLVE_LIN_EQ calls (no reference
  * counterpart).  The per-phase calls of one transport equation solve
  * independent slices A_M(:,:,M) / B_M(:,M) back to back (for example the U_g and
@@ -91,6 +88,9 @@ void mfixgpu_solve_lin_eq_defer_(const char *vname, const int *vno, double *var,
 int mfixgpu_solve_lin_eq_flush(void);
 int mfixgpu_solve_lin_eq_pending(void); /* calls queued */
 
+/* ITER_TOT(VNO) of MODULE leqsol (model/leqsol_mod.f:17), 1-based VNO in
+ * 1..10 (DIM_EQS, model/param_mod.f:97); the accounting of
+ * model/leq_bicgs.f:458,491. */
 int mfixgpu_iter_tot(int vno);
 void mfixgpu_reset_iter_tot(void);
 
@@ -143,8 +143,7 @@ const char *mfixgpu_last_error(void);
  *   "use_graph"      1 (default) replay the iteration body as a CUDA graph
  *   "time_kernels"   1: time every J-line sweep launch with CUDA events (no graph replay)
  *   "autotune"       1 (default): lanes per J-line picked by measurement for each new line length
- *   "line_lanes"     0 (default) automatic, else lanes per J-line (1..32, rounded down to a power of two;
- *                    64: 32 lanes with the line's rows staged by bulk copies, FP32 lines of 32..1024)
+ *   "line_lanes"     0 (default) automatic, else lanes per J-line (1..32, rounded down to a power of two)
  * Returns 0, or MFIXGPU_ERR_ARGS for an unknown name. */
 int mfixgpu_set_option(const char *name, double value);
 double mfixgpu_get_option(const char *name);

@@ -479,7 +479,7 @@ int mfixgpu_set_option(const char *name, double value)
     } else if (k == "autotune") {
         g.opt.autotune = value != 0;
     } else if (k == "line_lanes") {
-        if (value < 0 || (value > 32 && value != 64)) return MFIXGPU_ERR_ARGS;
+        if (value < 0 || value > 32) return MFIXGPU_ERR_ARGS;
         g.opt.line_lanes = (int)value;
     } else {
         return MFIXGPU_ERR_ARGS;

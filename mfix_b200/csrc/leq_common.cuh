@@ -66,9 +66,8 @@ __device__ __forceinline__ uint32_t fdiv(uint32_t n, const FastDiv &f)
 }
 
 // J-line kernels: lanes of one warp share a line and stage its rows through
-// registers (k_jline), one lane runs a whole line (k_jline_thread), or 32 lanes
-// share a line whose rows arrive by bulk copies (k_jline_bulk, FP32 only).
-enum LineKind : int { LK_WARP = 0, LK_THREAD = 1, LK_BULK = 2 };
+// registers (k_jline), or one lane runs a whole line (k_jline_thread).
+enum LineKind : int { LK_WARP = 0, LK_THREAD = 1 };
 
 // One system of the batch.
 struct SysDev {

@@ -176,10 +176,6 @@ SolveResult result_of(const SysState &st, bool mixed)
         r.ier = -12;  // DGTSV INFO != 0 inside a JK/IJ sweep (the reference stops there)
         r.exit_kind = EX_ERROR;
     }
-    if (st.err & 4) {
-        r.ier = -13;  // a bulk copy of the J-line kernel did not complete within its bounded wait
-        r.exit_kind = EX_ERROR;
-    }
     return r;
 }
 
@@ -383,13 +379,10 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
 int Engine::configure_lines(int elem, int only_L)
 {
     h_prefix_.assign(nsys_ + 1, 0);
-    int cmax = 1, lpad = 0;
+    int cmax = 1;
     for (int s = 0; s < nsys_; ++s) {
         const SysDev &d = h_sys_[s];
-        if (d.line_kind == LK_BULK)
-            lpad = std::max(lpad, line_bulk_lpad(d.jmax2, d.rows_per_lane));
-        else
-            cmax = std::max(cmax, d.rows_per_lane);
+        cmax = std::max(cmax, d.rows_per_lane);
         const int lpw = 32 / d.lane_group;
         const bool keep = d.n > 0 && (only_L == 0 || d.jmax2 == only_L);  // n = 0: empty slot of a live batch
         const int64_t slots = keep ? (int64_t)d.half_lines * d.kmax2 : 0;
@@ -417,30 +410,18 @@ int Engine::configure_lines(int elem, int only_L)
     const int items = h_prefix_[nsys_];
     cfg_.line_grid = std::max(1, std::min((items + wpb - 1) / wpb, sms_ * bpsm));
     // which line kernels the batch needs (systems with no line work count for none)
-    cfg_.line_thread = cfg_.line_warp = cfg_.line_single = cfg_.line_bulk = 0;
+    cfg_.line_thread = cfg_.line_warp = cfg_.line_single = 0;
     for (int s = 0; s < nsys_; ++s) {
         if (h_prefix_[s + 1] == h_prefix_[s]) continue;
         const SysDev &d = h_sys_[s];
         if (d.line_kind == LK_THREAD) {
             cfg_.line_thread = 1;
-        } else if (d.line_kind == LK_BULK) {
-            cfg_.line_bulk = 1;
         } else {
             cfg_.line_warp = 1;
             if (d.jmax2 & 1) cfg_.line_single = 1;
         }
     }
-    if (!cfg_.line_thread && !cfg_.line_warp && !cfg_.line_bulk) cfg_.line_warp = 1;  // empty batch: a no-op launch
-    cfg_.line_lpad = std::max(lpad, 8);
-    cfg_.line_bulk_warps = 1;
-    cfg_.line_grid_bulk = 1;
-    if (cfg_.line_bulk) {
-        int bw = 1;
-        const int bb = prepare_line_bulk(cfg_.line_lpad, &bw);
-        if (bb <= 0) return fail("J-lines too long for the bulk-staged line kernel", -10);
-        cfg_.line_bulk_warps = bw;
-        cfg_.line_grid_bulk = std::max(1, std::min((items + bw - 1) / bw, sms_ * bb));
-    }
+    if (!cfg_.line_thread && !cfg_.line_warp) cfg_.line_warp = 1;  // empty batch: a no-op launch
     const int tocc = elem == 4 ? line_thread_occupancy<float>() : line_thread_occupancy<double>();
     cfg_.line_grid_thread = std::max(1, std::min((items + 3) / 4, sms_ * tocc));
     return 0;
@@ -458,22 +439,9 @@ static int rows_for(int L, int G)
     return c;
 }
 
-// Lanes-per-line code LANES_BULK: 32 lanes per line, rows staged by bulk copies
-// (k_jline_bulk, FP32 only); its rows per lane are those of 32 lanes.
-static constexpr int LANES_BULK = 64;
-// The bulk kernel wants two buffers of twelve rows per warp; longer lines than
-// this stay with the register-staged kernels.
-static bool bulk_fits(int L) { return L >= 32 && L <= 1024; }
-
-static void set_shape(int L, int elem, int lanes, int *G, int *c, int *kind)
+static void set_shape(int L, int lanes, int *G, int *c, int *kind)
 {
-    if (lanes == LANES_BULK && elem == 4 && bulk_fits(L)) {
-        *G = 32;
-        *c = rows_for(L, 32);
-        *kind = LK_BULK;
-        return;
-    }
-    const int g = lanes == LANES_BULK ? 32 : lanes;
+    const int g = std::max(1, std::min(lanes, 32));
     *G = g;
     *c = rows_for(L, g);
     *kind = g == 1 ? LK_THREAD : LK_WARP;
@@ -486,14 +454,14 @@ void Engine::shape_for(int L, int elem, int forced, int *G, int *c, int *kind)
     if (forced > 0) {
         int g = 1;
         while (g * 2 <= std::min(forced, 32)) g *= 2;
-        set_shape(L, elem, forced == LANES_BULK ? LANES_BULK : g, G, c, kind);
+        set_shape(L, g, G, c, kind);
         return;
     }
     {
         std::lock_guard<std::mutex> lk(tunes().mu);
         auto it = tunes().lanes.find(std::make_pair(elem, L));
         if (it != tunes().lanes.end()) {
-            set_shape(L, elem, it->second, G, c, kind);
+            set_shape(L, it->second, G, c, kind);
             return;
         }
     }
@@ -537,10 +505,9 @@ int Engine::autotune_lines(const SolveOptions &opt, int elem)
     for (int L : todo) {
         int best_g = 0;
         float best_ms = 1e30f;
-        for (int g = 1; g <= LANES_BULK; g *= 2) {
-            if (g == LANES_BULK && !(elem == 4 && bulk_fits(L))) continue;
+        for (int g = 1; g <= 32; g *= 2) {
             int G = 1, c = 1, kind = LK_WARP;
-            set_shape(L, elem, g, &G, &c, &kind);
+            set_shape(L, g, &G, &c, &kind);
             if (kind == LK_WARP && (c > MAX_TUNED_ROWS || (size_t)kernel_smem_line_bytes(c, elem) > 48 * 1024))
                 continue;
             for (int s = 0; s < nsys_; ++s)
@@ -574,7 +541,7 @@ int Engine::autotune_lines(const SolveOptions &opt, int elem)
         }
         for (int s = 0; s < nsys_; ++s)
             if (h_sys_[s].jmax2 == L && h_sys_[s].n > 0)
-                set_shape(L, elem, best_g, &h_sys_[s].lane_group, &h_sys_[s].rows_per_lane, &h_sys_[s].line_kind);
+                set_shape(L, best_g, &h_sys_[s].lane_group, &h_sys_[s].rows_per_lane, &h_sys_[s].line_kind);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -593,7 +560,7 @@ void Engine::load_tune_cache(const std::string &path)
     char buf[256];
     while (std::fgets(buf, sizeof buf, f))
         if (std::sscanf(buf, " {\"elem\": %d, \"L\": %d, \"lanes\": %d}", &elem, &L, &G) == 3 && G >= 1 &&
-            (G <= 32 || G == LANES_BULK))
+            G <= 32)
             tunes().lanes[std::make_pair(elem, L)] = G;
     std::fclose(f);
 }

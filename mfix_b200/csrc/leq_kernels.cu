@@ -1354,7 +1354,7 @@ struct LineJob {
 // The next work item at or after `item` whose system takes part in the wave.
 // pair: the two-row instance, which takes systems with an even JMAX2 only (the
 // one-row instance takes every system).  kind: which line kernel asks
-// (SysDev::line_kind: warp-staged, one lane per line, bulk-staged); each takes
+// (SysDev::line_kind: warp-staged or one lane per line); each takes
 // its own systems.  pf: the system of `item` when the caller has already
 // loaded it, else -1.
 __device__ __forceinline__ bool next_line_job(const BatchView &b, const WaveArgs &w, int item, int step, int total,
@@ -1736,269 +1736,6 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
             }
         }
         __syncwarp();
-    }
-}
-
-// ------------------------------------------------------------------ J-line half-sweep, bulk-staged
-// Lines of the mixed form, one per warp, an autotuner candidate beside the
-// register-staged shapes.  The line's twelve operand rows (right-hand side,
-// A(-1), A(1), A(-3), A(3), the four neighbour lines, the three LU factors) come
-// into shared memory by asynchronous bulk copies, one row per lane, their
-// completion counted in bytes on an mbarrier; no registers hold them in flight.
-// The recurrences are k_jline's with 32 lanes per line and the same rows per
-// lane, in the same order.  Each copy covers the 16-byte-aligned span around
-// its row: every row lies in the engine's work block (256-byte-aligned arrays)
-// and is followed there by at least 16 more bytes, so the span stays in it.
-__device__ __forceinline__ uint32_t smem_u32(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
-{
-    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_arrive_expect(uint32_t bar, uint32_t bytes)
-{
-    asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(bar),
-                 "r"(bytes)
-                 : "memory");
-}
-
-__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void *src, uint32_t bytes, uint32_t bar)
-{
-    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(dst),
-                 "l"(src), "r"(bytes), "r"(bar)
-                 : "memory");
-}
-
-// Bounded wait for the phase with the given parity to complete.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity)
-{
-    for (int it = 0; it < (1 << 22); ++it) {
-        uint32_t ok;
-        asm volatile("{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
-                     : "=r"(ok)
-                     : "r"(bar), "r"(parity)
-                     : "memory");
-        if (ok) return true;
-    }
-    return false;
-}
-
-constexpr int BULK_ROWS = 12;
-// Row buffers per warp.  With two, the next line's rows arrive during this line's
-// sweep, but a 258-row line then takes 29 KB per warp and 7 warps fit an SM; with
-// one, 15 warps fit and other warps cover the copies (256^3: 167 vs 110 us per
-// half-sweep; the register-staged kernel takes 95 us there).
-constexpr int BULK_BUFS = 1;
-constexpr int BULK_HDR = 128;  // bytes per warp: two mbarriers, then two sets of row offsets
-
-// Elements per staged row: at least 32 rows per lane-chunk and the row's span.
-__host__ __device__ inline int bulk_lpad(int L, int c) { return ((L + 8 > 32 * c ? L + 8 : 32 * c) + 3) & ~3; }
-
-template <typename T>
-__host__ __device__ inline int bulk_warp_bytes(int lpad)
-{
-    return BULK_HDR + (BULK_BUFS * BULK_ROWS + 1) * lpad * (int)sizeof(T);
-}
-
-template <typename T>
-__global__ void __launch_bounds__(128) k_jline_bulk(BatchView b, WaveArgs w, int lpad)
-{
-    extern __shared__ __align__(16) unsigned char bulk_smem[];
-    const int nwarps = blockDim.x >> 5;
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    unsigned char *ws = bulk_smem + (size_t)warp * bulk_warp_bytes<T>(lpad);
-    const uint32_t bars = smem_u32(ws);  // two mbarriers, 8 bytes each
-    int *offs = reinterpret_cast<int *>(ws + 16);           // [2][BULK_ROWS] element offsets of the rows
-    T *rows = reinterpret_cast<T *>(ws + BULK_HDR);         // [2][BULK_ROWS][lpad]
-    T *fb = rows + BULK_BUFS * BULK_ROWS * lpad;             // [lpad]: f, y, then the new values
-    if (lane == 0) {
-        mbar_init(bars, 1);
-        mbar_init(bars + 8, 1);
-    }
-    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
-    __syncwarp();
-
-    const int total = (w.kind == 0) ? b.line_prefix[b.nsys] : w.count;
-    const int step = gridDim.x * nwarps;
-
-    // lane a < BULK_ROWS starts the copy of row a of line j into buffer q
-    auto issue = [&](const LineJob &j, int q) {
-        const SysDev &d = b.sys[j.sidx];
-        const LineCtx<T> x = line_ctx<T>(b, w, j);
-        const T *src = nullptr;
-        switch (lane) {
-        case 0: src = x.rhs + x.base; break;
-        case 1: src = x.a + 2 * x.n + x.base; break;
-        case 2: src = x.a + 4 * x.n + x.base; break;
-        case 3: src = x.do_k ? x.a + x.base : nullptr; break;
-        case 4: src = x.do_k ? x.a + 6 * x.n + x.base : nullptr; break;
-        case 5: src = x.nb_im; break;
-        case 6: src = x.nb_ip; break;
-        case 7: src = x.do_k ? x.nb_km : nullptr; break;
-        case 8: src = x.do_k ? x.nb_kp : nullptr; break;
-        case 9: src = reinterpret_cast<const T *>(d.fac[0]) + x.base; break;
-        case 10: src = reinterpret_cast<const T *>(d.fac[1]) + x.base; break;
-        case 11: src = reinterpret_cast<const T *>(d.fac[2]) + x.base; break;
-        default: break;
-        }
-        uint32_t bytes = 0;
-        int off = 0;
-        const void *from = nullptr;
-        if (j.valid && src) {
-            const uintptr_t a = reinterpret_cast<uintptr_t>(src);
-            const uintptr_t lo = a & ~(uintptr_t)15, hi = (a + (uintptr_t)j.L * sizeof(T) + 15) & ~(uintptr_t)15;
-            bytes = (uint32_t)(hi - lo);
-            off = (int)((a - lo) / sizeof(T));
-            from = reinterpret_cast<const void *>(lo);
-        }
-        uint32_t tot = bytes;
-        for (int o = 16; o > 0; o >>= 1) tot += __shfl_xor_sync(0xffffffffu, tot, o);
-        if (lane < BULK_ROWS) offs[q * BULK_ROWS + lane] = off;
-        if (lane == 0) mbar_arrive_expect(bars + 8 * q, tot);
-        __syncwarp();
-        if (bytes) bulk_g2s(smem_u32(rows + (size_t)(q * BULK_ROWS + lane) * lpad), from, bytes, bars + 8 * q);
-    };
-
-    LineJob jc, jn;
-    bool have = next_line_job(b, w, blockIdx.x * nwarps + warp, step, total, lane, false, LK_BULK, jc);
-    uint32_t phase = 0;  // bit q: parity of buffer q's next completion
-    int q = 0;
-    if (have) issue(jc, 0);
-    while (have) {
-        const bool have_n = next_line_job(b, w, jc.item + step, step, total, lane, false, LK_BULK, jn);
-        if (BULK_BUFS == 2 && have_n) issue(jn, q ^ 1);
-        const bool ok = __all_sync(0xffffffffu, mbar_wait(bars + 8 * q, (phase >> q) & 1u));
-        phase ^= 1u << q;
-        const SysDev &d = b.sys[jc.sidx];
-        SysState &st = b.st[jc.sidx];
-        if (!ok) {  // a copy never completed: flag the system, drain the other buffer, stop
-            if (lane == 0) atomicOr(&st.err, 4);
-            if (BULK_BUFS == 2 && have_n) mbar_wait(bars + 8 * (q ^ 1), (phase >> (q ^ 1)) & 1u);
-            return;
-        }
-        const LineCtx<T> x = line_ctx<T>(b, w, jc);
-        const int L = jc.L, c = jc.c;
-        const bool exact = jc.valid && d.line_flag[(jc.i - 1) + (jc.k - 1) * d.imax2] != 0;
-        const bool fast = jc.valid && !exact;
-        const T *R = rows + (size_t)q * BULK_ROWS * lpad;
-        const int *of = offs + q * BULK_ROWS;
-        const T *rhs = R + of[0], *am1 = R + lpad + of[1], *ap1 = R + 2 * lpad + of[2];
-        const T *am3 = R + 3 * lpad + of[3], *ap3 = R + 4 * lpad + of[4];
-        const T *nim = R + 5 * lpad + of[5], *nip = R + 6 * lpad + of[6];
-        const T *nkm = R + 7 * lpad + of[7], *nkp = R + 8 * lpad + of[8];
-        const T *gl_ = R + 9 * lpad + of[9], *gr_ = R + 10 * lpad + of[10], *gq_ = R + 11 * lpad + of[11];
-        const int r0 = lane * c;
-
-        // ---- forward recurrence y_r = f_r - l_r y_{r-1}, f formed on the way
-        T mb = T(0), ma = T(1);
-#pragma unroll 4
-        for (int t = 0; t < c; ++t) {
-            const int r = r0 + t;
-            T ft = T(0), lt = T(0);
-            if (fast && r < L) {
-                ft = rhs[r] - am1[r] * nim[r];
-                ft = ft - ap1[r] * nip[r];
-                if (x.do_k) {
-                    ft = ft - am3[r] * nkm[r];
-                    ft = ft - ap3[r] * nkp[r];
-                }
-                lt = gl_[r];
-            }
-            fb[r] = ft;
-            mb = ft - lt * mb;
-            ma = -lt * ma;
-        }
-        for (int dl = 1; dl < 32; dl <<= 1) {
-            const T pa = __shfl_up_sync(0xffffffffu, ma, dl), pb = __shfl_up_sync(0xffffffffu, mb, dl);
-            if (lane >= dl) {
-                mb = ma * pb + mb;
-                ma = ma * pa;
-            }
-        }
-        T y = __shfl_up_sync(0xffffffffu, mb, 1);
-        if (lane == 0) y = T(0);
-#pragma unroll 4
-        for (int t = 0; t < c; ++t) {
-            const int r = r0 + t;
-            const T lt = (fast && r < L) ? gl_[r] : T(0);
-            y = fb[r] - lt * y;
-            fb[r] = y;
-        }
-        // ---- backward recurrence x_r = r_r y_r - q_r x_{r+1}
-        mb = T(0);
-        ma = T(1);
-#pragma unroll 4
-        for (int t = c - 1; t >= 0; --t) {
-            const int r = r0 + t;
-            const bool in = fast && r < L;
-            const T qt = in ? gq_[r] : T(0), rt = in ? gr_[r] : T(0);
-            mb = rt * fb[r] - qt * mb;
-            ma = -qt * ma;
-        }
-        for (int dl = 1; dl < 32; dl <<= 1) {
-            const T na = __shfl_down_sync(0xffffffffu, ma, dl), nb = __shfl_down_sync(0xffffffffu, mb, dl);
-            if (lane + dl < 32) {
-                mb = ma * nb + mb;
-                ma = ma * na;
-            }
-        }
-        T xv = __shfl_down_sync(0xffffffffu, mb, 1);
-        if (lane == 31) xv = T(0);
-#pragma unroll 4
-        for (int t = c - 1; t >= 0; --t) {
-            const int r = r0 + t;
-            const bool in = fast && r < L;
-            const T qt = in ? gq_[r] : T(0), rt = in ? gr_[r] : T(0);
-            xv = rt * fb[r] - qt * xv;
-            fb[r] = xv;
-        }
-        __syncwarp();
-
-        // ---- a line on which DGTSV interchanges rows or meets a zero pivot: the
-        // exact elimination, with this buffer's factor rows as scratch
-        int skip = 0;
-        if (exact) {
-            T *s_sub = const_cast<T *>(R) + 9 * lpad, *s_dg = const_cast<T *>(R) + 10 * lpad;
-            T *s_sup = const_cast<T *>(R) + 11 * lpad;
-            for (int r = lane; r < L; r += 32) {
-                T a_, d_, c_, f_;
-                line_row<T>(x, r, a_, d_, c_, f_);
-                s_sub[r] = a_;
-                s_dg[r] = d_;
-                s_sup[r] = c_;
-                fb[r] = f_;
-            }
-            __syncwarp();
-            if (lane == 0) {
-                skip = dgtsv_rows<T>(L, s_sub, s_dg, s_sup, fb) != 0;
-                atomicAdd(&st.line_fallbacks, 1);
-                if (skip) atomicAdd(&st.line_skips, 1);
-            }
-            __syncwarp();
-        }
-        skip = __shfl_sync(0xffffffffu, skip, 0);
-
-        // ---- store: coalesced.  A line left unchanged (INFO != 0) keeps its old value.
-        if (jc.valid) {
-            T *dstp = vec<T>(d, w.dst) + x.base;
-            const T *oldl = vec<T>(d, w.old) + x.base;
-            if (!skip) {
-                for (int r = lane; r < L; r += 32) dstp[r] = fb[r];
-            } else if (w.write_old) {
-                for (int r = lane; r < L; r += 32) dstp[r] = oldl[r];
-            }
-        }
-        // this buffer's rows were read (and maybe written) through the generic
-        // proxy; the bulk copy that refills it two lines later goes through the async proxy
-        asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-        __syncwarp();
-        jc = jn;
-        have = have_n;
-        if (BULK_BUFS == 2)
-            q ^= 1;
-        else if (have)
-            issue(jc, 0);
     }
 }
 
@@ -2675,46 +2412,6 @@ int prepare_line_kernel(int cmax, int *warps)
     return std::min(nb, nb1);
 }
 
-int line_bulk_lpad(int L, int c) { return bulk_lpad(L, c); }
-
-// Shared memory attribute and resident blocks per SM of the bulk-staged kernel
-// for rows of lpad elements (0 when the buffers do not fit).
-int prepare_line_bulk(int lpad, int *warps)
-{
-    int dev = 0, optin = 0;
-    cudaGetDevice(&dev);
-    cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const int per_warp = bulk_warp_bytes<float>(lpad);
-    const int most = std::min(4, optin / std::max(per_warp, 1));
-    if (most < 1) return 0;
-    static std::mutex mu;
-    static int granted = 0;
-    {
-        std::lock_guard<std::mutex> lk(mu);
-        if (most * per_warp > granted) {
-            if (cudaFuncSetAttribute(k_jline_bulk<float>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                     most * per_warp) != cudaSuccess)
-                return 0;
-            granted = most * per_warp;
-        }
-    }
-    // the warps per block that keep the most warps resident per SM
-    int best = 0, best_nb = 0;
-    for (int wpb = 1; wpb <= most; ++wpb) {
-        int nb = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_jline_bulk<float>, wpb * 32, wpb * per_warp) !=
-            cudaSuccess)
-            return 0;
-        if (nb * wpb > best_nb * best) {
-            best = wpb;
-            best_nb = nb;
-        }
-    }
-    if (best == 0) return 0;
-    *warps = best;
-    return best_nb;
-}
-
 template <typename T>
 int line_thread_occupancy()
 {
@@ -2765,11 +2462,6 @@ cudaError_t launch_jline(const BatchView &b, const LaunchCfg &c, const WaveArgs 
     // systems with one lane per line, then those with several: one warp-kernel
     // launch, the two-row instance when all their lines have even length
     if (c.line_thread) k_jline_thread<T><<<c.line_grid_thread, 128, 0, c.stream>>>(b, w);
-    if constexpr (sizeof(T) == 4) {
-        if (c.line_bulk)
-            k_jline_bulk<T><<<c.line_grid_bulk, c.line_bulk_warps * 32, c.line_bulk_warps * bulk_warp_bytes<T>(c.line_lpad),
-                              c.stream>>>(b, w, c.line_lpad);
-    }
     if (c.line_warp) {
         const int smem = c.line_warps * kernel_smem_line_bytes(c.line_cmax, (int)sizeof(T));
         if (c.line_single)

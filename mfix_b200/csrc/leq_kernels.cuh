@@ -30,10 +30,6 @@ struct LaunchCfg {
     int line_thread;       // 1: some system has one lane per line
     int line_warp;         // 1: some system has several lanes per line
     int line_single;       // 1: some system with several lanes per line has an odd line length
-    int line_bulk;         // 1: some system's lines go to the bulk-staged kernel (FP32)
-    int line_grid_bulk;    // its blocks
-    int line_bulk_warps;   // its warps per block
-    int line_lpad;         // its staged row length (elements)
     cudaStream_t stream;
 };
 
@@ -114,10 +110,6 @@ struct SeqLineArgs {
 template <typename T>
 cudaError_t launch_seq_lines(const BatchView &b, const SeqLineArgs &a, cudaStream_t s);
 
-// Bulk-staged J-line kernel (FP32): staged row length for lines of length L
-// with c rows per lane, and the kernel's blocks per SM for rows of lpad elements.
-int line_bulk_lpad(int L, int c);
-int prepare_line_bulk(int lpad, int *warps);
 int kernel_smem_line_bytes(int cmax, int elem_bytes);
 template <typename T>
 int prepare_line_kernel(int cmax, int *warps);

@@ -53,9 +53,10 @@ def test_options_roundtrip():
     assert leq.set_option("precision", 3) == leq.IER_ARGS
     assert leq.set_option("no_such_option", 1) == leq.IER_ARGS
     assert leq.get_option("write_back_ab") == 1
-    # lanes per J-line: powers of two up to 32, or 64 for the bulk-staged kernel
-    assert leq.set_option("line_lanes", 64) == 0 and leq.get_option("line_lanes") == 64
+    # lanes per J-line: 1..32
+    assert leq.set_option("line_lanes", 32) == 0 and leq.get_option("line_lanes") == 32
     assert leq.set_option("line_lanes", 33) == leq.IER_ARGS
+    assert leq.set_option("line_lanes", 64) == leq.IER_ARGS
     assert leq.set_option("line_lanes", 0) == 0
 
 

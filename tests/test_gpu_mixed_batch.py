@@ -134,42 +134,29 @@ def _pivoting(s, seed=0):
     return t
 
 
-def test_bulk_staged_lines_equal_register_staged():
-    """The bulk-staged J-line kernel (rows brought in by asynchronous bulk copies)
-    runs the same recurrences as the 32-lane register-staged kernel: the same
-    bits, iteration counts and exact-line counts, odd and even line lengths,
-    2-D, lines that need DGTSV's interchanges, alone and in a batch."""
-    systems = [S.conv_diff(20, 33, 14, seed=90), S.conv_diff(9, 100, 8, seed=91),
-               S.conv_diff(31, 64, 1, seed=92, do_k=False), S.conv_diff(12, 257, 6, seed=93)]
-    piv = _pivoting(S.conv_diff(14, 47, 12, seed=94), seed=3)
-    piv.itmax = 40
-    out = {}
-    for lanes in (32, 64):
-        assert leq.set_option("line_lanes", lanes) == 0 and leq.set_option("precision", 1) == 0
-        try:
-            alone = []
-            for s in systems + [piv]:
-                t = s.copy()
-                ier = leq.solve_system(t)
-                st = leq.last_stats()
-                alone.append((t.x, ier, st["iterations"], st["line_fallbacks"], st["line_skips"]))
-            together = [s.copy() for s in systems]
-            rc, res = leq.batch_solve(together, precision=1)
-            assert rc == 0 and all(r.ier == 0 for r in res), leq.last_error()
-        finally:
-            leq.set_option("line_lanes", 0)
-            leq.set_option("precision", 0)
-        out[lanes] = (alone, together, [r.iterations for r in res])
-    for a32, a64 in zip(out[32][0], out[64][0]):
-        assert np.array_equal(a32[0], a64[0])
-        assert a32[1:] == a64[1:]
-    assert out[32][0][-1][3] > 0  # the pivoting lines took the exact elimination
-    for t32, t64 in zip(out[32][1], out[64][1]):
-        assert np.array_equal(t32.x, t64.x)
-    assert out[32][2] == out[64][2]
-    for s, (x, ier, *_) in zip(systems, out[64][0]):
-        assert ier == 0
-        assert _true_rel(_scaled_ref(s), x) <= s.tol * 1.01
+@pytest.mark.parametrize("lanes", [1, 32])
+def test_pivoting_lines_each_shape(lanes):
+    """J-lines on which DGTSV interchanges rows take the exact elimination in both
+    line kernel shapes (one lane per line, 32 lanes per line), alone and batched."""
+    s = _pivoting(S.conv_diff(14, 47, 12, seed=94), seed=3)
+    ref = s.copy()
+    st_ref = O.leq_bicgs(ref)
+    assert leq.set_option("line_lanes", lanes) == 0
+    try:
+        m = s.copy()
+        ier = leq.solve_system(m)
+        st = leq.last_stats()
+        pair = [s.copy(), S.conv_diff(9, 20, 8, seed=95)]
+        rc, res = leq.batch_solve(pair, precision=0)
+    finally:
+        leq.set_option("line_lanes", 0)
+    assert ier == st_ref["ier"] == 0, leq.last_error()
+    assert st["line_fallbacks"] > 0
+    assert np.array_equal(m.a, ref.a)
+    assert _true_rel(ref, m.x) <= s.tol * 1.01
+    assert np.linalg.norm(m.x - ref.x) <= 1e-6 * np.linalg.norm(ref.x)
+    assert rc == 0 and res[0].ier == 0
+    assert np.array_equal(pair[0].x, m.x)  # the same bits in a batch
 
 
 def _scaled_ref(s):
