@@ -9,7 +9,8 @@ module mfixgpu_mod
    use iso_c_binding, only: c_int, c_int64_t, c_double, c_char, c_ptr, c_null_char
    implicit none
    private
-   public :: mfixgpu_setup, mfixgpu_set_option, mfixgpu_iter_tot, mfixgpu_finalize, mfixgpu_flush
+   public :: mfixgpu_setup, mfixgpu_set_option, mfixgpu_iter_tot, mfixgpu_finalize, mfixgpu_flush, &
+             solve_lin_eq_defer
 
    interface
       integer(c_int) function c_init_geometry(imax2, jmax2, kmax2, do_k, dimension_3, dimension_m) &
@@ -85,6 +86,36 @@ contains
       mfixgpu_flush = c_flush()
    end function mfixgpu_flush
 
+   !> SOLVE_LIN_EQ_DEFER: SOLVE_LIN_EQ's dummy list, the call queued for MFIXGPU_FLUSH
+   !> (the per-phase calls of one equation, e.g. model/solve_vel_star.f:308-331, then
+   !> solve as one batch).  The library keeps the addresses of VAR, A_M, B_M and IER
+   !> and writes through them at the flush, after this call has returned, so:
+   !>  * the dummies carry ASYNCHRONOUS, and the caller declares the actual arguments
+   !>    ASYNCHRONOUS (or TARGET) in the scope that calls SOLVE_LIN_EQ_DEFER and
+   !>    MFIXGPU_FLUSH, so that no value of them is kept in a register across the flush;
+   !>  * VAR, A_M and B_M are whole contiguous arrays (no array sections: a section
+   !>    would be passed as a copy that is gone by the flush; the explicit interface of
+   !>    this module procedure makes the compiler refuse one);
+   !>  * VAR, A_M, B_M and IER stay in place and untouched until the flush; IER reads
+   !>    -15 until then.
+   !> The library's entry point takes gfortran's implicit convention (every argument by
+   !> reference, the CHARACTER lengths appended), so it is called without an interface.
+   subroutine solve_lin_eq_defer(vname, vno, var, a_m, b_m, m, itmax, method, sweep, tol1, pc, ier)
+      use param, only: dimension_3, dimension_m
+      character(len=*), intent(in) :: vname
+      integer, intent(in) :: vno
+      double precision, intent(inout), asynchronous :: var(dimension_3)
+      double precision, intent(inout), asynchronous :: a_m(dimension_3, -3:3, 0:dimension_m)
+      double precision, intent(inout), asynchronous :: b_m(dimension_3, 0:dimension_m)
+      integer, intent(in) :: m, itmax, method
+      character(len=4), intent(in) :: sweep
+      double precision, intent(in) :: tol1
+      character(len=4), intent(in) :: pc
+      integer, intent(inout), asynchronous :: ier
+      external mfixgpu_solve_lin_eq_defer
+      call mfixgpu_solve_lin_eq_defer(vname, vno, var, a_m, b_m, m, itmax, method, sweep, tol1, pc, ier)
+   end subroutine solve_lin_eq_defer
+
 end module mfixgpu_mod
 
 !> SOLVE_LIN_EQ with the reference's dummy list (model/solve_lin_eq.f:17-78):
@@ -124,25 +155,3 @@ subroutine solve_lin_eq(vname, vno, var, a_m, b_m, m, itmax, method, sweep, tol1
    ier = int(cier)
 end subroutine solve_lin_eq
 
-!> SOLVE_LIN_EQ_DEFER: SOLVE_LIN_EQ's dummy list, the call queued for MFIXGPU_FLUSH
-!> (the per-phase calls of one equation, e.g. model/solve_vel_star.f:308-331, then
-!> solve as one batch).  VAR, A_M, B_M and IER must stay in place and untouched
-!> until the flush; IER reads -15 until then.  The library's entry point takes
-!> gfortran's implicit convention (every argument by reference, the CHARACTER
-!> lengths appended), so it is called without an interface block.
-subroutine solve_lin_eq_defer(vname, vno, var, a_m, b_m, m, itmax, method, sweep, tol1, pc, ier)
-   use param, only: dimension_3, dimension_m
-   implicit none
-   character(len=*), intent(in) :: vname
-   integer, intent(in) :: vno
-   double precision, intent(inout) :: var(dimension_3)
-   double precision, intent(inout) :: a_m(dimension_3, -3:3, 0:dimension_m)
-   double precision, intent(inout) :: b_m(dimension_3, 0:dimension_m)
-   integer, intent(in) :: m, itmax, method
-   character(len=4), intent(in) :: sweep
-   double precision, intent(in) :: tol1
-   character(len=4), intent(in) :: pc
-   integer, intent(inout) :: ier
-   external mfixgpu_solve_lin_eq_defer
-   call mfixgpu_solve_lin_eq_defer(vname, vno, var, a_m, b_m, m, itmax, method, sweep, tol1, pc, ier)
-end subroutine solve_lin_eq_defer

@@ -50,15 +50,19 @@ struct Global {
     mfixgpu_stats last{};
     SolveTiming last_timing{};
     std::string err;
-    // SOLVE_LIN_EQ calls queued by mfixgpu_solve_lin_eq_defer_ until the next flush
+    // SOLVE_LIN_EQ calls queued by mfixgpu_solve_lin_eq_defer_ until the next flush;
+    // each keeps the geometry registered when it was queued
     struct Deferred {
         int vno, m, itmax;
         double *var, *a_m, *b_m, tol;
         char sweep[4], pc[4];
         int *ier;
+        Geometry geom;
     };
     std::vector<Deferred> deferred;
 };
+
+int flush_locked(Global &g);
 
 Global &G()
 {
@@ -243,7 +247,16 @@ void defer_impl(int vno, double *var, double *a_m, double *b_m, int m, int itmax
             return;
         }
         if (batchable) {
-            Global::Deferred d{vno, m, itmax, var, a_m, b_m, tol, {}, {}, ier};
+            // a call that reads or writes the arrays of a queued call (the same VAR,
+            // or the same A_M(:,:,M) slice) would be solved beside it; the queue is
+            // solved first, so that the calls see each other in call order
+            const double *slice = a_m + (size_t)m * 7 * (size_t)g.geom.n;
+            for (const auto &q : g.deferred)
+                if (q.var == var || q.a_m + (size_t)q.m * 7 * (size_t)q.geom.n == slice) {
+                    flush_locked(g);
+                    break;
+                }
+            Global::Deferred d{vno, m, itmax, var, a_m, b_m, tol, {}, {}, ier, g.geom};
             std::memcpy(d.sweep, sweep4, 4);
             std::memcpy(d.pc, pc4, 4);
             g.deferred.push_back(d);
@@ -252,6 +265,79 @@ void defer_impl(int vno, double *var, double *a_m, double *b_m, int m, int itmax
         }
     }
     solve_impl(vno, var, a_m, b_m, m, itmax, method, sweep4, tol, pc4, ier);
+}
+
+// Solves the queue, one batch per (PC, SWEEP, geometry), and writes the IERs in
+// the order the calls were queued (calls that share one IER variable see the
+// verdict of the last call, as the reference's back-to-back calls leave it).
+int flush_locked(Global &g)
+{
+    std::vector<Global::Deferred> all;
+    all.swap(g.deferred);
+    if (all.empty()) return 0;
+    Engine *e = engine_locked(g);
+    if (!e) {
+        for (auto &d : all) *d.ier = MFIXGPU_ERR_CUDA;
+        return MFIXGPU_ERR_CUDA;
+    }
+    const double t0 = now_s();
+    int first_rc = 0;
+    std::vector<bool> done(all.size(), false);
+    std::vector<int> code(all.size(), MFIXGPU_ERR_INCOMPLETE);
+    mfixgpu_stats agg{};
+    auto same_geom = [](const Geometry &a, const Geometry &b) {
+        return a.imax2 == b.imax2 && a.jmax2 == b.jmax2 && a.kmax2 == b.kmax2 && a.do_k == b.do_k && a.n == b.n;
+    };
+    for (size_t q0 = 0; q0 < all.size(); ++q0) {
+        if (done[q0]) continue;
+        // one batch per (PC, SWEEP, geometry): every call of the group shares the solver options
+        std::vector<size_t> grp;
+        for (size_t q = q0; q < all.size(); ++q)
+            if (!done[q] && !std::memcmp(all[q].pc, all[q0].pc, 4) && !std::memcmp(all[q].sweep, all[q0].sweep, 4) &&
+                same_geom(all[q].geom, all[q0].geom)) {
+                grp.push_back(q);
+                done[q] = true;
+            }
+        std::vector<SystemSpec> specs(grp.size());
+        for (size_t k = 0; k < grp.size(); ++k) {
+            const Global::Deferred &d = all[grp[k]];
+            const int64_t n = d.geom.n;
+            SystemSpec &s = specs[k];
+            s.imax2 = d.geom.imax2;
+            s.jmax2 = d.geom.jmax2;
+            s.kmax2 = d.geom.kmax2;
+            s.do_k = d.geom.do_k;
+            s.n = n;
+            s.a = d.a_m + (size_t)d.m * 7 * (size_t)n;  // A_M(:,:,M)
+            s.b = d.b_m + (size_t)d.m * (size_t)n;      // B_M(:,M)
+            s.x = d.var;
+            s.tol = d.tol;
+            s.itmax = d.itmax;
+        }
+        std::vector<SolveResult> out;
+        const int rc = e->solve(specs, make_opts(g.opt, decode_pc(all[q0].pc), all[q0].sweep), out);
+        if (rc) {
+            g.err = e->last_error();
+            for (size_t q : grp) code[q] = rc;
+            if (!first_rc) first_rc = rc;
+            continue;
+        }
+        for (size_t k = 0; k < grp.size(); ++k) {
+            const Global::Deferred &d = all[grp[k]];
+            code[grp[k]] = out[k].ier;
+            if (d.vno >= 1 && d.vno <= 10) g.iter_tot[d.vno - 1] += out[k].iter_tot_add;
+            agg.iterations = std::max(agg.iterations, out[k].iterations);
+            agg.iter_tot_add += out[k].iter_tot_add;
+        }
+        agg.device_ms += e->timing().device_ms;
+        agg.kernel_launches += e->timing().kernel_launches;
+        g.last_timing = e->timing();
+    }
+    for (size_t q = 0; q < all.size(); ++q) *all[q].ier = code[q];
+    agg.seconds = now_s() - t0;
+    agg.ier = first_rc;
+    g.last = agg;
+    return first_rc;
 }
 
 }  // namespace
@@ -342,66 +428,7 @@ int mfixgpu_solve_lin_eq_flush(void)
 {
     Global &g = G();
     std::lock_guard<std::mutex> lk(g.mu);
-    std::vector<Global::Deferred> all;
-    all.swap(g.deferred);
-    if (all.empty()) return 0;
-    Engine *e = engine_locked(g);
-    if (!e) {
-        for (auto &d : all) *d.ier = MFIXGPU_ERR_CUDA;
-        return MFIXGPU_ERR_CUDA;
-    }
-    const double t0 = now_s();
-    int first_rc = 0;
-    std::vector<bool> done(all.size(), false);
-    mfixgpu_stats agg{};
-    for (size_t q0 = 0; q0 < all.size(); ++q0) {
-        if (done[q0]) continue;
-        // one batch per (PC, SWEEP): every call of the group shares the solver options
-        std::vector<size_t> grp;
-        for (size_t q = q0; q < all.size(); ++q)
-            if (!done[q] && !std::memcmp(all[q].pc, all[q0].pc, 4) && !std::memcmp(all[q].sweep, all[q0].sweep, 4)) {
-                grp.push_back(q);
-                done[q] = true;
-            }
-        const int64_t n = g.geom.n;
-        std::vector<SystemSpec> specs(grp.size());
-        for (size_t k = 0; k < grp.size(); ++k) {
-            const Global::Deferred &d = all[grp[k]];
-            SystemSpec &s = specs[k];
-            s.imax2 = g.geom.imax2;
-            s.jmax2 = g.geom.jmax2;
-            s.kmax2 = g.geom.kmax2;
-            s.do_k = g.geom.do_k;
-            s.n = n;
-            s.a = d.a_m + (size_t)d.m * 7 * (size_t)n;  // A_M(:,:,M)
-            s.b = d.b_m + (size_t)d.m * (size_t)n;      // B_M(:,M)
-            s.x = d.var;
-            s.tol = d.tol;
-            s.itmax = d.itmax;
-        }
-        std::vector<SolveResult> out;
-        const int rc = e->solve(specs, make_opts(g.opt, decode_pc(all[q0].pc), all[q0].sweep), out);
-        if (rc) {
-            g.err = e->last_error();
-            for (size_t q : grp) *all[q].ier = rc;
-            if (!first_rc) first_rc = rc;
-            continue;
-        }
-        for (size_t k = 0; k < grp.size(); ++k) {
-            const Global::Deferred &d = all[grp[k]];
-            *d.ier = out[k].ier;
-            if (d.vno >= 1 && d.vno <= 10) g.iter_tot[d.vno - 1] += out[k].iter_tot_add;
-            agg.iterations = std::max(agg.iterations, out[k].iterations);
-            agg.iter_tot_add += out[k].iter_tot_add;
-        }
-        agg.device_ms += e->timing().device_ms;
-        agg.kernel_launches += e->timing().kernel_launches;
-        g.last_timing = e->timing();
-    }
-    agg.seconds = now_s() - t0;
-    agg.ier = first_rc;
-    g.last = agg;
-    return first_rc;
+    return flush_locked(g);
 }
 
 int mfixgpu_iter_tot(int vno)
@@ -530,6 +557,8 @@ void mfixgpu_finalize(void)
 {
     Global &g = G();
     std::lock_guard<std::mutex> lk(g.mu);
+    // calls still queued are dropped unsolved: their IER keeps MFIXGPU_ERR_INCOMPLETE
+    g.deferred.clear();
     g.engine.reset();
 }
 

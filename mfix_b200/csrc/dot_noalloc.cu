@@ -17,12 +17,15 @@
 // overlaps on the GPU, for example on two streams, race on the array.
 //
 // The first call on each device looks up the array's device address with
-// cudaGetSymbolAddress (that device current) and caches it; make that first call
-// before any stream capture.
+// cudaGetSymbolAddress (that device current) and caches it together with the
+// device's current context; make that first call before any stream capture.  A
+// call that finds another context current (the host reset the device, which
+// loads the library's module again at a new address) looks the address up anew.
 #include <cstdint>
 #include <mutex>
 #include <string>
 
+#include <cuda.h>  // CUcontext and the cuCtxGetCurrent signature only: the driver is reached through the runtime
 #include <cuda_runtime.h>
 
 #include "../../include/mfixgpu.h"
@@ -91,7 +94,30 @@ __global__ void __launch_bounds__(NOALLOC_THREADS) k_dot_noalloc(const double *_
 }
 
 std::mutex g_mu;
-void *g_scratch[64] = {};  // device address of noalloc_scratch, per device ordinal
+void *g_scratch[64] = {};      // device address of noalloc_scratch, per device ordinal
+CUcontext g_scratch_ctx[64] = {};  // the context that address belongs to
+
+// The current context (nullptr when the driver's entry point is unavailable, in
+// which case the cached address is trusted as it stands).
+CUcontext current_context()
+{
+    using Fn = CUresult (*)(CUcontext *);
+    static Fn fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void *p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<Fn>(p);
+        else
+            cudaGetLastError();
+    }
+    CUcontext c = nullptr;
+    if (fn && fn(&c) != CUDA_SUCCESS) c = nullptr;
+    return c;
+}
 
 int fail(const std::string &msg, int code)
 {
@@ -117,11 +143,12 @@ extern "C" int mfixgpu_dot_product_par_noalloc(const double *r1_dev, const doubl
         cudaGetLastError();
         return fail("no usable CUDA device", MFIXGPU_ERR_CUDA);
     }
-    if (!g_scratch[dev]) {
+    if (!g_scratch[dev] || current_context() != g_scratch_ctx[dev]) {
         void *p = nullptr;
-        const cudaError_t e = cudaGetSymbolAddress(&p, noalloc_scratch);
+        const cudaError_t e = cudaGetSymbolAddress(&p, noalloc_scratch);  // makes the device's context current
         if (e != cudaSuccess || !p) return fail(std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e), MFIXGPU_ERR_CUDA);
         g_scratch[dev] = p;
+        g_scratch_ctx[dev] = current_context();
     }
     cudaStream_t s = static_cast<cudaStream_t>(stream);
     cudaError_t e =

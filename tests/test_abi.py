@@ -163,3 +163,34 @@ def test_deferred_calls_without_gpu():
     assert leq.flush_lin_eq() == leq.IER_CUDA
     assert [c.value for c in cells] == [leq.IER_CUDA] * 3 and leq.pending_lin_eq() == 0
     assert leq.flush_lin_eq() == 0  # nothing queued
+
+
+@pytest.mark.skipif(_gpu_visible(), reason="checks the behaviour without a GPU")
+def test_deferred_queue_aliasing_geometry_finalize():
+    """A deferred call whose VAR or A_M(:,:,M) slice is already queued solves the
+    queue first (the earlier call's IER is written, the new call waits alone); a
+    geometry registered after a call was queued does not change that call; and
+    mfixgpu_finalize drops the queue, leaving its IERs at INCOMPLETE."""
+    n = 120
+    a = np.zeros((3, 7, n))
+    a[:, 3] = -1.0
+    b = np.ones((3, n))
+    xs = [np.zeros(n) for _ in range(3)]
+    assert leq.init_geometry(4, 5, 6, 1, n, 2) == 0
+    c0 = leq.defer_lin_eq("U_s", 3, xs[0], a, b, 0, 10, 2, "RSRS", 1e-8, "LINE")
+    c1 = leq.defer_lin_eq("U_s", 3, xs[1], a, b, 1, 10, 2, "RSRS", 1e-8, "LINE")
+    assert leq.pending_lin_eq() == 2
+    same_var = leq.defer_lin_eq("U_s", 3, xs[0], a, b, 2, 10, 2, "RSRS", 1e-8, "LINE")
+    assert (c0.value, c1.value) == (leq.IER_CUDA, leq.IER_CUDA)  # the queue was solved first
+    assert same_var.value == leq.IER_INCOMPLETE and leq.pending_lin_eq() == 1
+    same_slice = leq.defer_lin_eq("U_s", 3, xs[1], a, b, 2, 10, 2, "RSRS", 1e-8, "LINE")
+    assert same_var.value == leq.IER_CUDA and same_slice.value == leq.IER_INCOMPLETE
+    assert leq.pending_lin_eq() == 1
+    # a new geometry: the queued call keeps its own, the flush still runs it
+    assert leq.init_geometry(2, 5, 3, 1, 30, 0) == 0
+    assert leq.flush_lin_eq() == leq.IER_CUDA and same_slice.value == leq.IER_CUDA
+    assert leq.init_geometry(4, 5, 6, 1, n, 2) == 0
+    left = leq.defer_lin_eq("U_s", 3, xs[2], a, b, 2, 10, 2, "RSRS", 1e-8, "LINE")
+    assert leq.pending_lin_eq() == 1
+    leq.finalize()
+    assert leq.pending_lin_eq() == 0 and left.value == leq.IER_INCOMPLETE
