@@ -13,10 +13,13 @@ one complete solve.  Reported:
              mfixgpu_solve_lin_eq_ with pinned host arrays, copies inside the timing;
 * roofline   the J-line sweep kernel (the dominant kernel): algorithmic bytes per
              launch / average launch time from CUDA events over the timed steps;
-* cpu_baseline  the oracle (a C restatement of the reference's FP64 LEQ_BICGS with the
-             reference's OpenMP loops) on a bounded sample of the same system.
+* accuracy   each form's error against an FP64 solution refined to a true residual of
+             1e-14 (long-double residuals), and its difference from the oracle's solution;
+* cpu_baseline  one complete solve of the same system by the oracle (a C restatement of the
+             reference's FP64 LEQ_BICGS with the reference's OpenMP loops), timed.
 
-``--impl reference`` times that CPU implementation alone (rank 0), with all host cores.
+``--impl reference`` times that CPU implementation alone (rank 0), with all host cores:
+each step is one complete solve.
 Multi-GPU: every rank solves its own replica (the path shards by independent
 systems; a single system fits one GPU), value = systems solved by all ranks / max
 over ranks of the device time.
@@ -54,10 +57,6 @@ WORKLOADS = {
     "serve_poisson": dict(kind="serve", rate=2000.0, seconds=15.0, pool=64, seed=0, budget=150e9),
 }
 DEFAULT_WORKLOAD = "conv_diff_256"
-# Iterations the oracle (the reference's FP64 LEQ_BICGS restated in C) takes to
-# converge on each seeded workload, from complete oracle solves of them; the CPU
-# arm times a bounded sample of iterations and scales it by these counts.
-FP64_ITERATIONS = {"conv_diff_256": 66, "conv_diff_64": 65, "conv_diff_192": None, "pressure_192x384x192": None}
 
 BYTES_FP64_ITER = 576  # algorithmic bytes per cell per BiCGSTAB iteration, FP64 (72 words)
 BYTES_FP32_ITER = 288  # the same in the FP32 inner solve
@@ -226,30 +225,37 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def cpu_sample(sys0, iters_needed: int | None, sample_iters=(2, 5)) -> dict:
-    """Time the oracle (reference FP64 LEQ_BICGS restated in C, OpenMP) on a bounded
-    sample: two runs of m1 and m2 iterations give the per-iteration time and the
-    setup time; solves/s = 1 / (setup + iterations_needed * per_iteration)."""
+def cpu_solve(sys0) -> tuple:
+    """One complete solve of the system by the oracle (the reference's FP64
+    LEQ_BICGS restated in C, with the reference's OpenMP loops), timed; returns
+    (seconds, the solved copy with its unit-scaled A/B, the oracle's stats)."""
     import oracle as O
 
-    times = []
-    for m in sample_iters:
-        s = sys0.copy()
-        t0 = time.perf_counter()
-        O.leq_bicgs(s, max_exec=m)
-        times.append(time.perf_counter() - t0)
-    m1, m2 = sample_iters
-    t_iter = max((times[1] - times[0]) / (m2 - m1), 1e-9)
-    t_setup = max(times[0] - m1 * t_iter, 0.0)
-    n = sys0.n
-    out = {"cores": O.num_threads(), "kind": "port", "t_iter_s": t_iter, "t_setup_s": t_setup,
-           "sample": f"{m1} and {m2} BiCGSTAB iterations of the {sys0.imax2}x{sys0.jmax2}x{sys0.kmax2}-cell system "
-                     f"(setup + per-iteration time), scaled to the {iters_needed} iterations a full FP64 solve takes",
-           "gbs": BYTES_FP64_ITER * n / t_iter / 1e9}
-    if iters_needed:
-        t_solve = t_setup + iters_needed * t_iter
-        out["value"] = 1.0 / t_solve
-        out["unit"] = "solves/s"
+    s = sys0.copy()
+    t0 = time.perf_counter()
+    st = O.leq_bicgs(s)
+    return time.perf_counter() - t0, s, st
+
+
+def accuracy(ref, st_ref, xs: dict) -> dict:
+    """Errors of each solution in `xs` against the FP64 truth: the oracle's solution
+    refined until ||b - A x|| <= 1e-14 ||b|| (x0 = 0, so ||b|| is the initial
+    residual) with long-double residuals, on the unit-scaled system `ref`."""
+    import oracle as O
+
+    r0 = O.true_resid(ref, np.zeros(ref.n))
+    t0 = time.perf_counter()
+    x_truth, rel = O.truth_from(ref, ref.x, r0, rtol=1e-14)
+    t_truth = time.perf_counter() - t0
+    nt = float(np.linalg.norm(x_truth))
+    no = float(np.linalg.norm(ref.x))
+    out = {"truth_rel_resid": rel, "truth_s": t_truth,
+           "oracle": {"iterations": st_ref["iterations"], "true_rel_resid": O.true_resid(ref, ref.x) / r0,
+                      "err_vs_truth": float(np.linalg.norm(ref.x - x_truth)) / nt}}
+    for name, x in xs.items():
+        out[name] = {"err_vs_truth": float(np.linalg.norm(x - x_truth)) / nt,
+                     "rel_diff_vs_oracle": float(np.linalg.norm(x - ref.x)) / no,
+                     "true_rel_resid": O.true_resid(ref, x) / r0}
     return out
 
 
@@ -269,24 +275,30 @@ def run_reference(args) -> None:
         return run_reference_sample(args)
     if WORKLOADS[w]["kind"] == "cg":
         return run_reference_cg(args)
+    import oracle as O
+
     sys0 = make_system(w)
-    iters = FP64_ITERATIONS.get(w)
-    vals = []
     for _ in range(args.warmup):
-        cpu_sample(sys0, iters)
+        cpu_solve(sys0)
+    times, its = [], 0
     t0 = time.perf_counter()
     for _ in range(args.steps):
-        vals.append(cpu_sample(sys0, iters))
+        dt, _, st = cpu_solve(sys0)
+        times.append(dt)
+        its = st["iterations"]
     wall = time.perf_counter() - t0
-    v = float(np.mean([x.get("value", float("nan")) for x in vals]))
+    v = args.steps / sum(times)
+    sample = (f"{args.steps} complete oracle solves of the {sys0.imax2}x{sys0.jmax2}x{sys0.kmax2}-cell system "
+              f"({its} iterations each), one per step")
     line = {"impl": "reference", "metric": "solves/s", "value": v, "unit": "solves/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 / v if v > 0 else None,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * sum(times) / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": workload_config(w, sys0),
-            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": vals[0]["cores"], "kind": "port",
-                             "sample": vals[0]["sample"]},
+            "cpu_baseline": {"value": v, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
+                             "sample": sample},
             "e2e": {"value": v, "unit": "solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-            "wall_s": wall, "cpu_gbs": float(np.mean([x["gbs"] for x in vals]))}
+            "wall_s": wall, "iterations": its,
+            "cpu_gbs": BYTES_FP64_ITER * its * sys0.n / (sum(times) / args.steps) / 1e9}
     print(json.dumps(line), flush=True)
 
 
@@ -474,28 +486,35 @@ def run_ours(args) -> None:
     value = world * args.steps / (tot_mixed / 1e3)
     fp64_value = world * args.steps / (tot_64 / 1e3)
 
-    # ---- e2e through the Fortran-convention entry point, pinned host arrays
+    # ---- e2e through the Fortran-convention entry point, pinned host arrays:
+    # the copies of A_M, B_M, VAR in and of VAR and the scaled A_M/B_M out are
+    # inside the timing (mixed form: the headline; FP64 drop-in beside it)
     a_h = torch.empty((7, n), dtype=torch.float64).pin_memory().numpy()
     b_h = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
     x_h = torch.empty(n, dtype=torch.float64).pin_memory().numpy()
-    leq.set_option("precision", 1)
     leq.init_geometry(sys0.imax2, sys0.jmax2, sys0.kmax2, 1, n, 0)
-    e2e_t = []
-    for it in range(args.warmup + args.steps):
-        np.copyto(a_h, sys0.a)
-        np.copyto(b_h, sys0.b)
-        x_h[:] = 0.0
-        barrier()
-        t0 = time.perf_counter()
-        ier = leq.solve_lin_eq("Pp_g", 1, x_h, a_h, b_h, 0, sys0.itmax, 2, "RSRS", sys0.tol, "LINE")
-        t1 = time.perf_counter()
-        if ier != 0:
-            raise RuntimeError(f"e2e solve IER {ier}: {leq.last_error()}")
-        if it >= args.warmup:
-            e2e_t.append(t1 - t0)
-    leq.set_option("precision", 0)
-    e2e_tot = max_over_ranks(sum(e2e_t))
-    e2e_value = world * args.steps / e2e_tot
+
+    def e2e(precision: int, steps: int, warm: int) -> float:
+        leq.set_option("precision", precision)
+        e2e_t = []
+        for it in range(warm + steps):
+            np.copyto(a_h, sys0.a)
+            np.copyto(b_h, sys0.b)
+            x_h[:] = 0.0
+            barrier()
+            t0 = time.perf_counter()
+            ier = leq.solve_lin_eq("Pp_g", 1, x_h, a_h, b_h, 0, sys0.itmax, 2, "RSRS", sys0.tol, "LINE")
+            t1 = time.perf_counter()
+            if ier != 0:
+                raise RuntimeError(f"e2e solve IER {ier}: {leq.last_error()}")
+            if it >= warm:
+                e2e_t.append(t1 - t0)
+        leq.set_option("precision", 0)
+        return world * steps / max_over_ranks(sum(e2e_t))
+
+    e2e_value = e2e(1, args.steps, args.warmup)
+    e2e_fp64_steps = max(3, args.steps // 2)
+    e2e_fp64 = e2e(0, e2e_fp64_steps, 1)
 
     # ---- roofline of the J-line sweep kernel (FP32 in the mixed form)
     peak, peak_kind = measured_peak_hbm()
@@ -519,7 +538,9 @@ def run_ours(args) -> None:
         "config": workload_config(w, sys0),
         "roofline": roof,
         "e2e": {"value": e2e_value, "unit": "solves/s", "h2d_bytes_per_step": 9 * 8 * n,
-                "d2h_bytes_per_step": 9 * 8 * n, "entry": "mfixgpu_solve_lin_eq_ (pinned host A_M/B_M/VAR)"},
+                "d2h_bytes_per_step": 9 * 8 * n, "entry": "mfixgpu_solve_lin_eq_ (pinned host A_M/B_M/VAR)",
+                "fp64_drop_in": {"value": e2e_fp64, "unit": "solves/s", "steps": e2e_fp64_steps,
+                                 "h2d_bytes_per_step": 9 * 8 * n, "d2h_bytes_per_step": 9 * 8 * n}},
         "gpu_launches": int(launches),
         "clocks": sampler.summary(),
         "mixed": {"solves_per_s": value, "ms_per_solve": tot_mixed / args.steps, "inner_iterations": rm.iterations,
@@ -535,9 +556,20 @@ def run_ours(args) -> None:
         "wall_s_timed_mixed": wall,
     }
     if rank == 0 and world == 1 and not args.no_cpu:
-        cb = cpu_sample(sys0, fp64_iters)
-        line["cpu_baseline"] = {"value": cb.get("value"), "unit": "solves/s", "cores": cb["cores"], "kind": "port",
-                                "sample": cb["sample"], "gbs": cb["gbs"]}
+        import oracle as O
+
+        # one complete oracle solve (the CPU baseline), then the accuracy of both
+        # forms against the oracle's solution and against the 1e-14 truth
+        t_cpu, ref, st_ref = cpu_solve(sys0)
+        line["cpu_baseline"] = {"value": 1.0 / t_cpu, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
+                                "sample": f"one complete oracle solve of the same system ({st_ref['iterations']} "
+                                          f"iterations, {t_cpu:.1f} s)",
+                                "gbs": BYTES_FP64_ITER * st_ref["iterations"] * n / t_cpu / 1e9}
+        acc = accuracy(ref, st_ref, {"fp64": x64.cpu().numpy(), "mixed": xm.cpu().numpy()})
+        line["accuracy"] = acc
+        for form in ("fp64", "mixed"):
+            line[form]["err_vs_truth"] = acc[form]["err_vs_truth"]
+            line[form]["rel_diff_vs_oracle"] = acc[form]["rel_diff_vs_oracle"]
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -68,6 +68,8 @@ def lib() -> C.CDLL:
         L.orc_true_resid.restype = C.c_double
         L.orc_truth_solve.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_double, C.c_int, C.c_uint64, _dp]
         L.orc_truth_solve.restype = C.c_int
+        L.orc_truth_refine.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_double, C.c_double, C.c_int, C.c_uint64, _dp]
+        L.orc_truth_refine.restype = C.c_int
         L.orc_num_threads.restype = C.c_int
         _lib = L
     return _lib
@@ -179,6 +181,16 @@ def truth(s, rtol: float = 1e-14, max_steps: int = 60, seed: int = 0x7A7E) -> tu
     x = s.x.copy()
     rel = C.c_double(0.0)
     lib().orc_truth_solve(C.byref(geom(s)), _p(s.a), _p(s.b), _p(x), rtol, max_steps, seed, C.byref(rel))
+    return x, rel.value
+
+
+def truth_from(s, x0: np.ndarray, r0: float, rtol: float = 1e-14, max_steps: int = 60,
+               seed: int = 0x7A7E) -> tuple[np.ndarray, float]:
+    """Refines the guess x0 of the (already scaled) system until ||b - A x|| <= rtol * r0
+    (long-double residuals); returns x and ||b - A x|| / r0."""
+    x = np.array(x0, dtype=np.float64, copy=True)
+    rel = C.c_double(0.0)
+    lib().orc_truth_refine(C.byref(geom(s)), _p(s.a), _p(s.b), _p(x), float(r0), rtol, max_steps, seed, C.byref(rel))
     return x, rel.value
 
 

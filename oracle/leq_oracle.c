@@ -645,10 +645,15 @@ static void bicgs_inner(const orc_geom *g, const double *a, const double *r0, do
 int orc_truth_solve(const orc_geom *g, const double *a, const double *b, double *x, double rtol, int max_iter,
                     uint64_t rt_seed, double *final_rel)
 {
+    return orc_truth_refine(g, a, b, x, orc_true_resid(g, a, b, x), rtol, max_iter, rt_seed, final_rel);
+}
+
+int orc_truth_refine(const orc_geom *g, const double *a, const double *b, double *x, double r0, double rtol,
+                     int max_iter, uint64_t rt_seed, double *final_rel)
+{
     const int64_t n = g->n;
     double *work = (double *)calloc((size_t)(10 * n), sizeof(double));
     double *r = work + 8 * n, *d = work + 9 * n;
-    const double r0 = orc_true_resid(g, a, b, x);
     double rel = 1.0;
     int steps = 0;
     if (r0 == 0.0) {

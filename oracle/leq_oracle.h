@@ -88,6 +88,10 @@ double orc_true_resid(const orc_geom *g, const double *a, const double *b, const
  * ||b-Ax|| <= rtol * ||b-A x0|| (long-double residuals). Returns restarts used or -1. */
 int orc_truth_solve(const orc_geom *g, const double *a, const double *b, double *x, double rtol,
                     int max_iter, uint64_t rt_seed, double *final_rel);
+/* The same refinement from the guess in x, stopping at ||b-Ax|| <= rtol * r0 for a
+ * given r0 (e.g. ||b|| for the system's zero initial guess). */
+int orc_truth_refine(const orc_geom *g, const double *a, const double *b, double *x, double r0, double rtol,
+                     int max_iter, uint64_t rt_seed, double *final_rel);
 
 int orc_num_threads(void);
 
