@@ -111,7 +111,7 @@ typedef struct {
     int fp64_fallback;  /* mixed form: 1 when the FP32 iteration stalled and the FP64 drop-in re-solved */
     long long kernel_launches; /* kernels of this library launched by the solve */
     int mixed_iterations; /* mixed form: FP32 iterations spent before an FP64 re-solve */
-    int pad3;
+    int deflated;       /* mixed form: 1 when the near-null mode was deflated (option "deflate") */
 } mfixgpu_stats;
 
 int mfixgpu_last_stats(mfixgpu_stats *out);
@@ -134,8 +134,14 @@ const char *mfixgpu_last_error(void);
  *                    the best one seen (default 10)
  *   "mixed_stalls"   mixed form: hand over after this many reliable updates without a 10% gain (default 6)
  *   "mixed_min_margin" mixed form: a system whose smallest diagonal-dominance margin,
- *                    min over rows of |sum of A's row| / |A(0)|, is below this is solved by the
- *                    FP64 drop-in from the start (default 1e-4; 0 never)
+ *                    min over rows of |sum of A's row| / |A(0)|, is below this (pressure correction)
+ *                    is deflated, or with "deflate" 0 solved by the FP64 drop-in from the start
+ *                    (default 1e-4; 0 never)
+ *   "deflate"        mixed form, systems below mixed_min_margin: 1 (default) the FP32 inner iteration's
+ *                    preconditioner also solves the constant mode over the coupled rows exactly
+ *                    (Phat = M^{-1} P + c z, z = 1 on rows with a nonzero neighbour coefficient,
+ *                    c = z^T P / z^T A z), which keeps it converging on near-singular operators;
+ *                    0: such systems go to the FP64 drop-in
  *   "write_back_ab"  1 (default) copy the scaled A_M/B_M slices back
  *   "rtilde_seed"    seed of the Rtilde random stream (replaces RANDOM_NUMBER, model/leq_bicgs.f:298)
  *   "inner_tol"      mixed form: drop of the FP32 residual between FP64 reliable updates (default 1e-2)

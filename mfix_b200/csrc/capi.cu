@@ -34,6 +34,7 @@ struct Options {
     double mixed_growth = 10.0;
     int mixed_stalls = 6;
     double mixed_min_margin = 1e-4;
+    int deflate = 1;
     int check_every = 4;
     int use_graph = 1;
     int time_kernels = 0;
@@ -121,6 +122,7 @@ SolveOptions make_opts(const Options &o, int pc, const char sweep4[4])
     so.mixed_growth = o.mixed_growth;
     so.mixed_stalls = o.mixed_stalls;
     so.mixed_min_margin = o.mixed_min_margin;
+    so.deflate = o.deflate != 0;
     so.check_every = o.check_every;
     so.use_graph = o.use_graph != 0;
     so.time_kernels = o.time_kernels != 0;
@@ -209,6 +211,7 @@ void solve_impl(int vno, double *var, double *a_m, double *b_m, int m, int itmax
     g.last.kernel_launches = e->timing().kernel_launches;
     g.last.fp64_fallback = r.fp64_fallback;
     g.last.mixed_iterations = r.mixed_iterations;
+    g.last.deflated = r.deflated;
     g.last_timing = e->timing();
     finish(code);
 }
@@ -490,6 +493,8 @@ int mfixgpu_set_option(const char *name, double value)
     } else if (k == "mixed_growth") {
         if (!(value > 1)) return MFIXGPU_ERR_ARGS;
         g.opt.mixed_growth = value;
+    } else if (k == "deflate") {
+        g.opt.deflate = value != 0;
     } else if (k == "mixed_min_margin") {
         if (!(value >= 0)) return MFIXGPU_ERR_ARGS;
         g.opt.mixed_min_margin = value;
@@ -527,6 +532,7 @@ double mfixgpu_get_option(const char *name)
     if (k == "mixed_growth") return g.opt.mixed_growth;
     if (k == "mixed_stalls") return g.opt.mixed_stalls;
     if (k == "mixed_min_margin") return g.opt.mixed_min_margin;
+    if (k == "deflate") return g.opt.deflate;
     if (k == "check_every") return g.opt.check_every;
     if (k == "use_graph") return g.opt.use_graph;
     if (k == "time_kernels") return g.opt.time_kernels;

@@ -88,6 +88,8 @@ struct SysDev {
     double *x64[2];      // VAR; x64[1] keeps the initial guess in the mixed form (FP64 re-solve)
     float *a32;          // FP32 copy of the scaled diagonals (mixed form)
     float *defect;       // mixed form: row sums of the scaled A, formed in FP64 (A x = sum a_nb (x_nb - x) + defect x)
+    unsigned char *defl_z;  // mixed form: 1 on rows coupled to a neighbour, 0 on decoupled (wall) rows
+    float *defl_az;      // mixed form, deflated systems: A z, formed in FP64
     void *vec[NVEC];     // work vectors, double or float by precision
     void *fac[3];        // J-line LU factors per cell (l, 1/u, c/u), double or float by precision
     int *line_flag;      // per J-line (i-1)+(k-1)*imax2: 1 where DGTSV interchanges rows or meets a zero pivot
@@ -127,6 +129,10 @@ struct SysState {
     int method;           // LEQ_METHOD: 2 BiCGSTAB, 5 CG
     int line_skips;       // J-lines left unchanged because DGTSV reported INFO != 0
     int line_fallbacks;   // J-lines solved by the sequential pivoting path
+    int defl_allow;       // mixed form: a system below min_margin may be deflated instead of handed over
+    int defl;             // mixed form: the inner iteration deflates z (coupled-row indicator)
+    double defl_e;        // z^T A z
+    double defl_cp, defl_cs;  // z^T P / z^T A z and z^T S / z^T A z of the current iteration
     int err;
     unsigned int arrivals;  // tiles that finished the current reduction kernel
 };

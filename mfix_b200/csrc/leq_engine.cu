@@ -166,6 +166,7 @@ SolveResult result_of(const SysState &st, bool mixed)
     r.line_skips = st.line_skips;
     r.line_fallbacks = st.line_fallbacks;
     r.outer_steps = st.outer_steps;
+    r.deflated = mixed ? st.defl : 0;
     r.rnorm0 = mixed ? st.outer_rnorm0 : st.rnorm0;
     r.rnorm = mixed ? st.outer_rnorm : st.rnorm;
     if (st.status != ST_DONE) {
@@ -214,7 +215,8 @@ size_t vec_region_bytes(int64_t n, int64_t lines, int precision)
 {
     const size_t ew = precision == PREC_MIXED ? 4 : 8;
     size_t b = 0;
-    if (precision == PREC_MIXED) b += align_up(7 * (size_t)n * 4, 256) + align_up((size_t)n * 4, 256);
+    if (precision == PREC_MIXED)  // FP32 diagonals, row sums, deflation vector z and A z
+        b += align_up(7 * (size_t)n * 4, 256) + 2 * align_up((size_t)n * 4, 256) + align_up((size_t)n, 256);
     b += (NVEC + 3) * align_up((size_t)n * ew, 256) + align_up((size_t)lines * 4, 256);
     return b;
 }
@@ -245,10 +247,14 @@ void carve_work(SysDev &d, char *work, int64_t lines, int precision, char *x0)
     };
     d.a32 = nullptr;
     d.defect = nullptr;
+    d.defl_z = nullptr;
+    d.defl_az = nullptr;
     d.x64[1] = nullptr;
     if (precision == PREC_MIXED) {
         d.a32 = (float *)take(7 * n * 4);
         d.defect = (float *)take(n * 4);
+        d.defl_az = (float *)take(n * 4);
+        d.defl_z = (unsigned char *)take(n);
         d.x64[1] = (double *)x0;  // initial guess, kept for an FP64 re-solve
     }
     for (int v = 0; v < NVEC; ++v) d.vec[v] = take(n * ew);
@@ -314,6 +320,7 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         st.growth_limit = opt.mixed_growth;
         st.stall_limit = opt.mixed_stalls;
         st.min_margin = opt.mixed_min_margin;
+        st.defl_allow = opt.deflate ? 1 : 0;
         st.margin_bits = 0x7f800000u;
         st.i = 1;
         st.iter = 1;
@@ -1072,7 +1079,8 @@ int Engine::launch_setup(const SolveOptions &opt, bool scale)
     }
     if (mixed) {
         CK(launch_to_f32(view_, cfg_));
-        launches_ += 1;
+        CK(launch_defl_setup(view_, cfg_));
+        launches_ += 2;
     } else if (cg) {  // R = B - A Var and Rnorm0 (model/leq_cg.f:236-259)
         CK(launch_init_residual<double>(view_, cfg_));
         launches_ += 1;

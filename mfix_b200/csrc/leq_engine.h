@@ -44,6 +44,7 @@ struct SolveResult {
     int outer_steps = 0;
     int fp64_fallback = 0;     // mixed form handed the system to an FP64 re-solve
     int mixed_iterations = 0;  // FP32 iterations spent before that hand-over
+    int deflated = 0;          // mixed form: the near-null mode was deflated (near-singular operator)
     double rnorm0 = 0.0, rnorm = 0.0;
 };
 
@@ -59,7 +60,9 @@ struct SolveOptions {
     double inner_tol = 1e-2;     // mixed form: residual drop between reliable updates
     double mixed_growth = 10.0;  // mixed form: true-residual growth over the best that hands over to FP64
     int mixed_stalls = 6;        // mixed form: reliable updates without a 10% gain that hand over
-    double mixed_min_margin = 1e-4;  // mixed form: smaller diagonal-dominance margins go straight to FP64
+    double mixed_min_margin = 1e-4;  // mixed form: smaller diagonal-dominance margins are deflated (or go to FP64)
+    bool deflate = true;         // mixed form: deflate the near-null mode of systems below mixed_min_margin
+                                 // (false: they go straight to the FP64 drop-in)
     int check_every = 4;         // iterations between host checks of the state
     bool use_graph = true;       // capture the iteration body in a CUDA graph
     bool time_kernels = false;   // record events around every J-line launch (no graph replay)

@@ -293,9 +293,10 @@ __global__ void k_init_done(BatchView b)
         st.phase = PH_INNER;
         return;
     }
-    // a nearly singular operator (pressure correction) goes to the FP64 drop-in
-    // before any FP32 iteration: its FP32 Krylov process stagnates
-    if (st.mixed && __uint_as_float(st.margin_bits) < st.min_margin) {
+    // a nearly singular operator (pressure correction) is deflated (k_defl_setup);
+    // where that is off or impossible it goes to the FP64 drop-in before any FP32
+    // iteration: its undeflated FP32 Krylov process stagnates
+    if (st.mixed && __uint_as_float(st.margin_bits) < st.min_margin && !st.defl) {
         st.exit_kind = EX_FALLBACK;
         st.ier = -20;
         st.status = ST_DONE;
@@ -322,13 +323,18 @@ __global__ void k_to_f32(BatchView b)
         #pragma unroll 4
         for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
             double sum = 0.0;
+            bool coupled = false;
 #pragma unroll
             for (int q = 0; q < 7; ++q) {
                 const double v = d.a64[q * n + c];
                 d.a32[q * n + c] = (float)v;
-                if (d.do_k || (q != 0 && q != 6)) sum += v;
+                if (d.do_k || (q != 0 && q != 6)) {
+                    sum += v;
+                    if (q != 3 && v != 0.0) coupled = true;
+                }
             }
             d.defect[c] = (float)sum;  // the row sum, exact to FP32 rounding however small
+            d.defl_z[c] = coupled ? 1 : 0;
             const double a0 = fabs(d.a64[3 * n + c]);
             if (a0 > 0.0) margin = fminf(margin, (float)(fabs(sum) / a0));
         }
@@ -336,6 +342,43 @@ __global__ void k_to_f32(BatchView b)
         for (int o = 16; o > 0; o >>= 1) margin = fminf(margin, __shfl_xor_sync(0xffffffffu, margin, o));
         if ((threadIdx.x & 31) == 0) atomicMin(&b.st[tl.sys].margin_bits, __float_as_uint(margin));
     }
+}
+
+// Deflation of the near-null mode (mixed form, systems whose diagonal-dominance
+// margin is below min_margin: pressure correction, where the rows of coupled
+// cells sum to a millionth of their diagonal).  z is 1 on the rows coupled to a
+// neighbour and 0 on decoupled (wall) rows; the preconditioner becomes
+//   Phat = M^{-1} P + c z,  c = z^T P / z^T A z,
+// so that the constant mode over the coupled cells, which the line sweeps barely
+// reduce, is solved exactly in every application.  This kernel forms A z in FP64
+// (stored in FP32) and E = z^T A z.
+__global__ void k_defl_setup(BatchView b)
+{
+    TileRun run{-1, 0};
+    auto fin = [&](SysState &st, const double(&tot)[1]) {
+        st.defl_e = tot[0];
+        st.defl = (tot[0] != 0.0 && isfinite(tot[0])) ? 1 : 0;
+    };
+    for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
+        const Tile tl = b.tiles[t];
+        const SysDev &d = b.sys[tl.sys];
+        SysState &st = b.st[tl.sys];
+        if (!gate_ok(st, G_INIT) || !st.mixed || !st.defl_allow ||
+            !(__uint_as_float(st.margin_bits) < st.min_margin))
+            continue;
+        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
+        double v[1] = {0.0};
+        #pragma unroll 2
+        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+            const CellIdx q = cell_ijk(d, (uint32_t)c);
+            const double az = stencil_row<double, unsigned char>(d, d.a64, d.defl_z, (uint32_t)c, q);
+            d.defl_az[c] = (float)az;
+            if (d.defl_z[c]) v[0] += az;
+        }
+        tile_partial<1>(b, d, tl.idx, v);
+        run_add<1>(b, run, tl.sys, fin);
+    }
+    run_close<1>(b, run, fin);
 }
 
 // R = B - A*Var and ||R|| (model/leq_bicgs.f:283-291).
@@ -638,11 +681,22 @@ struct Batch {
     static constexpr int STREAM = sizeof(T) == 8 ? 4 : 8;
 };
 
+// z^T v over a cell pair (deflated mixed systems)
+template <typename T>
+__device__ __forceinline__ double zdot2(const unsigned char *z, int64_t c, const vec2_t<T> &v)
+{
+    const uchar2 zz = *reinterpret_cast<const uchar2 *>(z + c);
+    return (zz.x ? (double)v.x : 0.0) + (zz.y ? (double)v.y : 0.0);
+}
+
 // P = R (i = 1) or P = R + beta*(P - omega*V) (model/leq_bicgs.f:334-343).
+// Deflated mixed systems also form c_p = z^T P / z^T A z.
 template <typename T, bool MIXED>
 __global__ void __launch_bounds__(256, 4) k_p_update(BatchView b)
 {
     constexpr int U2 = Batch<T>::STREAM / 2;
+    TileRun run{-1, 0};
+    auto fin = [&](SysState &st, const double(&tot)[1]) { st.defl_cp = tot[0] / st.defl_e; };
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
@@ -653,6 +707,8 @@ __global__ void __launch_bounds__(256, 4) k_p_update(BatchView b)
         const T *__restrict__ r = vec<T>(d, V_R) + c0;
         T *__restrict__ p = vec<T>(d, V_P) + c0;
         const int np = cnt >> 1;  // cell pairs; an odd last cell is done by thread 0
+        const bool defl = MIXED && st.defl;
+        double zv[1] = {0.0};
         if (st.i == 1) {
             for (int base = threadIdx.x; base < np; base += U2 * blockDim.x) {
                 vec2_t<T> rv[U2];
@@ -664,10 +720,16 @@ __global__ void __launch_bounds__(256, 4) k_p_update(BatchView b)
 #pragma unroll
                 for (int u = 0; u < U2; ++u) {
                     const int q = base + u * blockDim.x;
-                    if (q < np) st2(p + 2 * q, rv[u]);
+                    if (q < np) {
+                        st2(p + 2 * q, rv[u]);
+                        if (defl) zv[0] += zdot2<T>(d.defl_z, c0 + 2 * q, rv[u]);
+                    }
                 }
             }
-            if ((cnt & 1) && threadIdx.x == 0) p[cnt - 1] = r[cnt - 1];
+            if ((cnt & 1) && threadIdx.x == 0) {
+                p[cnt - 1] = r[cnt - 1];
+                if (defl && d.defl_z[c0 + cnt - 1]) zv[0] += (double)r[cnt - 1];
+            }
         } else {
             const T beta = (T)st.beta, omega = (T)st.omega;
             const T *__restrict__ v = vec<T>(d, V_V) + c0;
@@ -685,17 +747,26 @@ __global__ void __launch_bounds__(256, 4) k_p_update(BatchView b)
 #pragma unroll
                 for (int u = 0; u < U2; ++u) {
                     const int q = base + u * blockDim.x;
-                    if (q < np)
-                        st2(p + 2 * q, mk2<T>(rv[u].x + beta * (pv[u].x - omega * vv[u].x),
-                                              rv[u].y + beta * (pv[u].y - omega * vv[u].y)));
+                    if (q < np) {
+                        const vec2_t<T> pn = mk2<T>(rv[u].x + beta * (pv[u].x - omega * vv[u].x),
+                                                    rv[u].y + beta * (pv[u].y - omega * vv[u].y));
+                        st2(p + 2 * q, pn);
+                        if (defl) zv[0] += zdot2<T>(d.defl_z, c0 + 2 * q, pn);
+                    }
                 }
             }
             if ((cnt & 1) && threadIdx.x == 0) {
                 const int c = cnt - 1;
                 p[c] = r[c] + beta * (p[c] - omega * v[c]);
+                if (defl && d.defl_z[c0 + c]) zv[0] += (double)p[c];
             }
         }
+        if (defl) {
+            tile_partial<1>(b, d, tl.idx, zv);
+            run_add<1>(b, run, tl.sys, fin);
+        }
     }
+    run_close<1>(b, run, fin);
 }
 
 // DIAG preconditioner, LEQ_MSOLVE1 (model/leqsol_mod.f:719-746): var = b / A(0).
@@ -779,6 +850,9 @@ __global__ void __launch_bounds__(256) k_matvec_alpha(BatchView b, int src)
         const T *__restrict__ rt = vec<T>(d, V_RT);
         T *__restrict__ y = vec<T>(d, V_V);
         double v[1] = {0.0};
+        // deflated mixed systems: V = A (Phat + c_p z) = A Phat + c_p A z
+        const bool defl = MIXED && st.defl;
+        const double cp = defl ? st.defl_cp : 0.0;
         if constexpr (PAIR) {
             const int np = cnt >> 1;
             for (int base = threadIdx.x; base < np; base += UP * blockDim.x) {
@@ -796,7 +870,12 @@ __global__ void __launch_bounds__(256) k_matvec_alpha(BatchView b, int src)
                 for (int u = 0; u < UP; ++u) {
                     const int q = base + u * blockDim.x;
                     if (q < np) {
-                        const vec2_t<T> yv = dot_pair7<T, MIXED>(rw[u], d.do_k);
+                        vec2_t<T> yv = dot_pair7<T, MIXED>(rw[u], d.do_k);
+                        if (defl) {
+                            const float2 az = ld2(d.defl_az + c0 + 2 * q);
+                            yv.x = yv.x + (T)(cp * (double)az.x);
+                            yv.y = yv.y + (T)(cp * (double)az.y);
+                        }
                         st2(y + c0 + 2 * q, yv);
                         v[0] += (double)rtv[u].x * (double)yv.x;
                         v[0] += (double)rtv[u].y * (double)yv.y;
@@ -819,7 +898,8 @@ __global__ void __launch_bounds__(256) k_matvec_alpha(BatchView b, int src)
             for (int u = 0; u < U; ++u) {
                 const int c = base + u * blockDim.x;
                 if (c < cnt) {
-                    const T yv = dot_row7<T, MIXED>(rw[u], d.do_k);
+                    T yv = dot_row7<T, MIXED>(rw[u], d.do_k);
+                    if (defl) yv = yv + (T)(cp * (double)d.defl_az[c0 + c]);
                     y[c0 + c] = yv;
                     v[0] += (double)rtv[u] * (double)yv;
                 }
@@ -832,18 +912,21 @@ __global__ void __launch_bounds__(256) k_matvec_alpha(BatchView b, int src)
     run_close<1>(b, run, fin);
 }
 
-// S = R - alpha*V and Snorm (model/leq_bicgs.f:365-375).
+// S = R - alpha*V and Snorm (model/leq_bicgs.f:365-375); deflated mixed systems
+// also form c_s = z^T S / z^T A z.
 template <typename T, bool MIXED>
 __global__ void __launch_bounds__(256, 4) k_s_update(BatchView b)
 {
     constexpr int U2 = Batch<T>::STREAM / 2;
+    constexpr int NV = MIXED ? 2 : 1;
     TileRun run{-1, 0};
-    auto fin = [&](SysState &st, const double(&tot)[1]) {
+    auto fin = [&](SysState &st, const double(&tot)[NV]) {
         st.snorm = sqrt(tot[0]);
         if (MIXED)
             st.snorm_exit = (st.snorm <= 0.1 * st.tol * st.outer_rnorm0) ? 1 : 0;
         else
             st.snorm_exit = (st.snorm <= DBL_EPSILON) ? 1 : 0;  // TOLMIN = EPSILON(ONE)
+        if (MIXED && st.defl) st.defl_cs = tot[NV - 1] / st.defl_e;
     };
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
@@ -856,7 +939,10 @@ __global__ void __launch_bounds__(256, 4) k_s_update(BatchView b)
         const T *__restrict__ r = vec<T>(d, V_R) + c0;
         const T *__restrict__ vv = vec<T>(d, V_V) + c0;
         T *__restrict__ s = vec<T>(d, V_S) + c0;
-        double v[1] = {0.0};
+        const bool defl = MIXED && st.defl;
+        double v[NV];
+#pragma unroll
+        for (int k = 0; k < NV; ++k) v[k] = 0.0;
         const int np = cnt >> 1;
         for (int base = threadIdx.x; base < np; base += U2 * blockDim.x) {
             vec2_t<T> rv[U2], wv[U2];
@@ -876,6 +962,7 @@ __global__ void __launch_bounds__(256, 4) k_s_update(BatchView b)
                     st2(s + 2 * q, mk2<T>(s0, s1));
                     v[0] += (double)s0 * (double)s0;
                     v[0] += (double)s1 * (double)s1;
+                    if (defl) v[NV - 1] += zdot2<T>(d.defl_z, c0 + 2 * q, mk2<T>(s0, s1));
                 }
             }
         }
@@ -884,11 +971,12 @@ __global__ void __launch_bounds__(256, 4) k_s_update(BatchView b)
             const T sv = r[c] - alpha * vv[c];
             s[c] = sv;
             v[0] += (double)sv * (double)sv;
+            if (defl && d.defl_z[c0 + c]) v[NV - 1] += (double)sv;
         }
-        tile_partial<1>(b, d, tl.idx, v);
-        run_add<1>(b, run, tl.sys, fin);
+        tile_partial<NV>(b, d, tl.idx, v);
+        run_add<NV>(b, run, tl.sys, fin);
     }
-    run_close<1>(b, run, fin);
+    run_close<NV>(b, run, fin);
 }
 
 // T = A*Shat, omega = (T,S)/(T,T) with (T,T) = 0 -> SMALL_NUMBER (model/leq_bicgs.f:409-427).
@@ -915,6 +1003,9 @@ __global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
         const T *__restrict__ s = vec<T>(d, V_S);
         T *__restrict__ y = vec<T>(d, V_T);
         double v[2] = {0.0, 0.0};
+        // deflated mixed systems: T = A (Shat + c_s z) = A Shat + c_s A z
+        const bool defl = MIXED && st.defl;
+        const double cs = defl ? st.defl_cs : 0.0;
         if constexpr (PAIR) {
             const int np = cnt >> 1;
             for (int base = threadIdx.x; base < np; base += UP * blockDim.x) {
@@ -932,7 +1023,12 @@ __global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
                 for (int u = 0; u < UP; ++u) {
                     const int q = base + u * blockDim.x;
                     if (q < np) {
-                        const vec2_t<T> yv = dot_pair7<T, MIXED>(rw[u], d.do_k);
+                        vec2_t<T> yv = dot_pair7<T, MIXED>(rw[u], d.do_k);
+                        if (defl) {
+                            const float2 az = ld2(d.defl_az + c0 + 2 * q);
+                            yv.x = yv.x + (T)(cs * (double)az.x);
+                            yv.y = yv.y + (T)(cs * (double)az.y);
+                        }
                         st2(y + c0 + 2 * q, yv);
                         v[0] += (double)yv.x * (double)sv[u].x;
                         v[1] += (double)yv.x * (double)yv.x;
@@ -957,7 +1053,8 @@ __global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
             for (int u = 0; u < U; ++u) {
                 const int c = base + u * blockDim.x;
                 if (c < cnt) {
-                    const T yv = dot_row7<T, MIXED>(rw[u], d.do_k);
+                    T yv = dot_row7<T, MIXED>(rw[u], d.do_k);
+                    if (defl) yv = yv + (T)(cs * (double)d.defl_az[c0 + c]);
                     y[c0 + c] = yv;
                     v[0] += (double)yv * (double)sv[u];
                     v[1] += (double)yv * (double)yv;
@@ -1067,7 +1164,12 @@ __global__ void __launch_bounds__(256) k_xr_update(BatchView b, int ph_id, int s
         const T *__restrict__ ph = vec<T>(d, ph_id) + c0;
         double v[2] = {0.0, 0.0};
         const int np = cnt >> 1;
+        // deflated mixed systems: Phat + c_p z and Shat + c_s z, so x also gains
+        // (alpha c_p + omega c_s) on the coupled rows
+        const bool defl = MIXED && st.defl;
+        const unsigned char *__restrict__ zr = defl ? d.defl_z + c0 : nullptr;
         if (st.snorm_exit) {
+            const X_T wz = defl ? (X_T)(st.alpha * st.defl_cp) : X_T(0);
             for (int base = threadIdx.x; base < np; base += U2 * blockDim.x) {
                 vec2_t<X_T> xv[U2];
                 vec2_t<T> pv[U2];
@@ -1082,13 +1184,24 @@ __global__ void __launch_bounds__(256) k_xr_update(BatchView b, int ph_id, int s
 #pragma unroll
                 for (int u = 0; u < U2; ++u) {
                     const int q = base + u * blockDim.x;
-                    if (q < np)
-                        st2(x + 2 * q, mk2<X_T>(xv[u].x + alpha * (X_T)pv[u].x, xv[u].y + alpha * (X_T)pv[u].y));
+                    if (q < np) {
+                        vec2_t<X_T> xn = mk2<X_T>(xv[u].x + alpha * (X_T)pv[u].x, xv[u].y + alpha * (X_T)pv[u].y);
+                        if (defl) {
+                            const uchar2 zz = *reinterpret_cast<const uchar2 *>(zr + 2 * q);
+                            if (zz.x) xn.x = xn.x + wz;
+                            if (zz.y) xn.y = xn.y + wz;
+                        }
+                        st2(x + 2 * q, xn);
+                    }
                 }
             }
-            if ((cnt & 1) && threadIdx.x == 0) x[cnt - 1] = x[cnt - 1] + alpha * (X_T)ph[cnt - 1];
+            if ((cnt & 1) && threadIdx.x == 0) {
+                x[cnt - 1] = x[cnt - 1] + alpha * (X_T)ph[cnt - 1];
+                if (defl && zr[cnt - 1]) x[cnt - 1] = x[cnt - 1] + wz;
+            }
         } else {
             const X_T omega = (X_T)st.omega;
+            const X_T wz = defl ? (X_T)(st.alpha * st.defl_cp + st.omega * st.defl_cs) : X_T(0);
             const T omega_t = (T)st.omega;
             const T *__restrict__ sh = vec<T>(d, sh_id) + c0;
             const T *__restrict__ s = vec<T>(d, V_S) + c0;
@@ -1114,8 +1227,14 @@ __global__ void __launch_bounds__(256) k_xr_update(BatchView b, int ph_id, int s
                 for (int u = 0; u < U2; ++u) {
                     const int q = base + u * blockDim.x;
                     if (q < np) {
-                        st2(x + 2 * q, mk2<X_T>(xv[u].x + alpha * (X_T)pv[u].x + omega * (X_T)hv[u].x,
-                                                xv[u].y + alpha * (X_T)pv[u].y + omega * (X_T)hv[u].y));
+                        vec2_t<X_T> xn = mk2<X_T>(xv[u].x + alpha * (X_T)pv[u].x + omega * (X_T)hv[u].x,
+                                                  xv[u].y + alpha * (X_T)pv[u].y + omega * (X_T)hv[u].y);
+                        if (defl) {
+                            const uchar2 zz = *reinterpret_cast<const uchar2 *>(zr + 2 * q);
+                            if (zz.x) xn.x = xn.x + wz;
+                            if (zz.y) xn.y = xn.y + wz;
+                        }
+                        st2(x + 2 * q, xn);
                         const T r0 = sv[u].x - omega_t * tw[u].x, r1 = sv[u].y - omega_t * tw[u].y;
                         st2(r + 2 * q, mk2<T>(r0, r1));
                         v[0] += (double)r0 * (double)r0;
@@ -1128,6 +1247,7 @@ __global__ void __launch_bounds__(256) k_xr_update(BatchView b, int ph_id, int s
             if ((cnt & 1) && threadIdx.x == 0) {
                 const int c = cnt - 1;
                 x[c] = x[c] + alpha * (X_T)ph[c] + omega * (X_T)sh[c];
+                if (defl && zr[c]) x[c] = x[c] + wz;
                 const T rv = s[c] - omega_t * tv[c];
                 r[c] = rv;
                 v[0] += (double)rv * (double)rv;
@@ -1327,6 +1447,36 @@ __device__ int dgtsv_rows(int L, T *sub, T *dg, T *sup, T *f)
     if (L > 1) f[L - 2] = (f[L - 2] - sup[L - 2] * f[L - 1]) / dg[L - 2];
     for (int i = L - 3; i >= 0; --i) f[i] = (f[i] - sup[i] * f[i + 1] - sub[i + 1] * f[i + 2]) / dg[i];
     return 0;
+}
+
+// DGTSV's INFO alone: the same interchanges and zero-pivot tests as dgtsv_rows on
+// the matrix rows, no right-hand side (INFO does not depend on it).
+template <typename T>
+__device__ int dgtsv_info(int L, T *sub, T *dg, T *sup)
+{
+    for (int i = 0; i < L - 1; ++i) {
+        T dli = sub[i + 1];
+        if (fabs(dg[i]) >= fabs(dli)) {
+            if (dg[i] != T(0)) {
+                const T fact = dli / dg[i];
+                dg[i + 1] = dg[i + 1] - fact * sup[i];
+            } else {
+                return i + 1;
+            }
+            if (i < L - 2) sub[i + 1] = T(0);
+        } else {
+            const T fact = dg[i] / dli;
+            dg[i] = dli;
+            const T temp = dg[i + 1];
+            dg[i + 1] = sup[i] - fact * temp;
+            if (i < L - 2) {
+                sub[i + 1] = sup[i + 1];
+                sup[i + 1] = -fact * sub[i + 1];
+            }
+            sup[i] = temp;
+        }
+    }
+    return dg[L - 1] == T(0) ? L : 0;
 }
 
 __device__ __forceinline__ int find_sys(const int *prefix, int nsys, int item)
@@ -1743,9 +1893,11 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
 // For short lines in large numbers (batches and serving) each lane runs the two
 // recurrences down its own line, keeping y in the destination (the line's own
 // cells, which no other line of the wave reads); no staging, few instructions
-// per row.  A flagged line runs DGTSV with interchanges in global scratch: the
-// line's factor cells (unused for a flagged line) and its cells of T (dead
-// during MSOLVE), so that a line left unchanged (INFO != 0) keeps VAR.
+// per row.  A flagged line runs DGTSV with interchanges: its matrix rows in the
+// line's factor cells (unused for a flagged line), first without the right-hand
+// side to find INFO (a line left unchanged on INFO != 0 keeps its old values),
+// then, when INFO = 0, again with the right-hand side in the line's own cells of
+// the destination.
 template <typename T>
 __global__ void __launch_bounds__(128) k_jline_thread(BatchView b, WaveArgs w)
 {
@@ -1792,21 +1944,27 @@ __global__ void __launch_bounds__(128) k_jline_thread(BatchView b, WaveArgs w)
                     dstp[r] = xv;
                 }
             } else {
-                // DGTSV with interchanges, in global scratch: the line's factor cells
-                // (unused for a flagged line) and its cells of T (dead during MSOLVE)
+                // DGTSV with interchanges: the matrix rows in the line's factor cells
+                // (unused for a flagged line); INFO first, from the matrix alone
                 T *sub = reinterpret_cast<T *>(d.fac[0]) + x.base;
                 T *dg = reinterpret_cast<T *>(d.fac[1]) + x.base;
                 T *sup = reinterpret_cast<T *>(d.fac[2]) + x.base;
-                T *rs = vec<T>(d, V_T) + x.base;
-                for (int r = 0; r < L; ++r) line_row<T>(x, r, sub[r], dg[r], sup[r], rs[r]);
-                const int skip = dgtsv_rows<T>(L, sub, dg, sup, rs) != 0;
+                T f_unused;
+                for (int r = 0; r < L; ++r) line_row<T>(x, r, sub[r], dg[r], sup[r], f_unused);
+                const int skip = dgtsv_info<T>(L, sub, dg, sup) != 0;
                 atomicAdd(&st.line_fallbacks, 1);
-                if (skip) atomicAdd(&st.line_skips, 1);
-                const T *oldl = vec<T>(d, w.old) + x.base;
-                if (!skip)
-                    for (int r = 0; r < L; ++r) dstp[r] = rs[r];
-                else if (w.write_old)
-                    for (int r = 0; r < L; ++r) dstp[r] = oldl[r];
+                if (skip) {
+                    atomicAdd(&st.line_skips, 1);
+                    const T *oldl = vec<T>(d, w.old) + x.base;
+                    if (w.write_old)
+                        for (int r = 0; r < L; ++r) dstp[r] = oldl[r];
+                } else {
+                    // the right-hand side of row r goes to the line's own cell r of the
+                    // destination; a later row reads only its own cell (a neighbour that
+                    // clamps onto itself), so the rows are formed before they are overwritten
+                    for (int r = 0; r < L; ++r) line_row<T>(x, r, sub[r], dg[r], sup[r], dstp[r]);
+                    dgtsv_rows<T>(L, sub, dg, sup, dstp);
+                }
             }
         }
     }
@@ -2354,6 +2512,11 @@ cudaError_t launch_init_done(const BatchView &b, const LaunchCfg &c)
 cudaError_t launch_to_f32(const BatchView &b, const LaunchCfg &c)
 {
     k_to_f32<<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b);
+    CHECK_LAUNCH();
+}
+cudaError_t launch_defl_setup(const BatchView &b, const LaunchCfg &c)
+{
+    k_defl_setup<<<c.cell_grid, CELL_THREADS, 0, c.stream>>>(b);
     CHECK_LAUNCH();
 }
 template <typename T>

@@ -37,6 +37,7 @@ struct LaunchCfg {
 cudaError_t launch_scale(const BatchView &b, const LaunchCfg &c);
 cudaError_t launch_after_scale(const BatchView &b, const LaunchCfg &c);
 cudaError_t launch_to_f32(const BatchView &b, const LaunchCfg &c);
+cudaError_t launch_defl_setup(const BatchView &b, const LaunchCfg &c);  // mixed form: A z and z^T A z
 cudaError_t launch_init_done(const BatchView &b, const LaunchCfg &c);
 cudaError_t launch_scale_diag(const BatchView &b, const LaunchCfg &c);  // LEQ_CG0's scaling by A(0)
 template <typename T>

@@ -34,7 +34,7 @@ class Stats(C.Structure):
                 ("line_skips", C.c_int), ("line_fallbacks", C.c_int), ("outer_steps", C.c_int), ("pad", C.c_int),
                 ("rnorm0", C.c_double), ("rnorm", C.c_double), ("seconds", C.c_double), ("device_ms", C.c_double),
                 ("jline_ms", C.c_double), ("jline_launches", C.c_int), ("fp64_fallback", C.c_int),
-                ("kernel_launches", C.c_longlong), ("mixed_iterations", C.c_int), ("pad3", C.c_int)]
+                ("kernel_launches", C.c_longlong), ("mixed_iterations", C.c_int), ("deflated", C.c_int)]
 
 
 class Geom(C.Structure):

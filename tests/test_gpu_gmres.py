@@ -90,3 +90,25 @@ def test_method4_hands_breakdown_to_gmres(cuda, case):
     assert leq.iter_tot(4) - before == st_b["iter_tot_add"]
     assert np.array_equal(got.a, ref.a) and np.array_equal(got.b, ref.b)  # BiCGSTAB's scaling came back
     assert _close(got.x, ref.x, 1e-6)
+
+
+@pytest.mark.parametrize("lanes", [1, 2, 32])
+def test_method4_singular_row_each_line_shape(cuda, lanes):
+    """The zero row's J-line meets a zero pivot in DGTSV (INFO != 0, the line is left
+    unchanged) inside the GMRES preconditioner, whose right-hand side is a work
+    vector of its own: every line-kernel shape (one lane per line included) gives
+    the oracle's VAR."""
+    s = S.conv_diff(10, 12, 9, seed=2)
+    s.itmax = 30
+    s.a[:, 5 * s.jmax2 + 3 + 4 * s.jmax2 * s.imax2] = 0.0
+    ref = s.copy()
+    assert O.leq_bicgs(ref, pc="LINE")["ier"] == -2
+    st_g = O.leq_gmres(ref)
+    assert leq.set_option("line_lanes", lanes) == 0
+    try:
+        got = s.copy()
+        ier = leq.solve_system(got, method=4, pc="LINE", vno=4)
+    finally:
+        leq.set_option("line_lanes", 0)
+    assert ier == st_g["ier"], leq.last_error()
+    assert _close(got.x, ref.x, 1e-9)

@@ -2,12 +2,15 @@
 
 Mixed form (FP32 BiCGSTAB, FP64 solution accumulation and reliable updates):
 IER 0, the FP64 true relative residual of the scaled system <= TOL, and a
-solution within 1e-6 of the FP64 drop-in's.  On the well-conditioned
-convection-diffusion systems it takes no more than 1.3x the FP64 iterations and
-never hands over to FP64; the near-singular pressure-like system (zero wall
-coupling, diagonal excess 1e-6, so a diagonal-dominance margin of 1e-6) goes
-to the FP64 drop-in before any FP32 iteration.  Batch: uneven systems solved together give results
-bit-identical to each system solved alone, in both precisions.
+solution within 1e-6 of the FP64 drop-in's, never handing over to FP64.  On the
+well-conditioned convection-diffusion systems it takes no more than 1.3x the
+FP64 iterations; the near-singular pressure-like systems (zero wall coupling,
+diagonal excess 1e-6, so a diagonal-dominance margin of 1e-6) are deflated
+(the constant mode over the coupled rows solved exactly in every
+preconditioner application) and take no more iterations than the FP64 drop-in.
+With deflation off they go to the FP64 drop-in before any FP32 iteration.
+Batch: uneven systems solved together give results bit-identical to each
+system solved alone, in both precisions.
 """
 import numpy as np
 import pytest
@@ -44,23 +47,37 @@ def test_mixed_converges_to_tol(make, near_singular):
     assert np.array_equal(m.a, ref.a) and np.array_equal(m.b, ref.b)
     assert _true_rel(ref, m.x) <= s.tol * 1.01
     assert np.linalg.norm(m.x - ref.x) <= 1e-6 * np.linalg.norm(ref.x)
+    assert st["fp64_fallback"] == 0
+    assert st["outer_steps"] >= 1
+    assert st["deflated"] == (1 if near_singular else 0)
     if not near_singular:
-        assert st["fp64_fallback"] == 0
-        assert st["outer_steps"] >= 1
         assert st["iterations"] <= 1.3 * st_ref["iterations"] + 2
-    else:  # diagonal-dominance margin 1e-6 < 1e-4: FP64 from the start, no FP32 iteration spent
-        assert st["fp64_fallback"] == 1 and st["mixed_iterations"] == 0
+    else:  # margin 1e-6 < 1e-4: deflated, and no slower than FP64 in iterations
+        assert st["iterations"] <= st_ref["iterations"] + 2
 
 
 def test_margin_routing_threshold():
-    """The routing follows the option: with mixed_min_margin = 0 the pressure-like
-    system is attempted in FP32 (and may still hand over later)."""
+    """The routing follows the options: below mixed_min_margin a system is
+    deflated (default) or, with deflate = 0, solved by the FP64 drop-in before any
+    FP32 iteration; with mixed_min_margin = 0 the pressure-like system is
+    attempted in FP32 without deflation (and may still hand over later)."""
     s = S.pressure_like(20, 22, 18, seed=5, nspheres=3, rmin=2, rmax=4, itmax=3000)
+    assert leq.get_option("deflate") == 1
+    assert leq.set_option("precision", 1) == 0 and leq.set_option("deflate", 0) == 0
+    try:
+        m = s.copy()
+        assert leq.solve_system(m) == 0
+        st = leq.last_stats()
+        assert st["fp64_fallback"] == 1 and st["mixed_iterations"] == 0 and st["deflated"] == 0
+    finally:
+        leq.set_option("deflate", 1)
+        leq.set_option("precision", 0)
     assert leq.set_option("precision", 1) == 0 and leq.set_option("mixed_min_margin", 0.0) == 0
     try:
         m = s.copy()
         assert leq.solve_system(m) == 0
         st = leq.last_stats()
+        assert st["deflated"] == 0
         assert st["fp64_fallback"] == 0 or st["mixed_iterations"] > 0
     finally:
         leq.set_option("mixed_min_margin", 1e-4)
