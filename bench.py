@@ -54,13 +54,17 @@ WORKLOADS = {
     "batch_64": dict(kind="batch", count=64, seed=0, itmax=500, tol=1e-8),
     # Poisson request stream: sizes log-uniform per axis on [24, 160], 20% pressure-like,
     # TOL from {1e-6, 1e-8}, 150 GB HBM admission budget
-    "serve_poisson": dict(kind="serve", rate=2000.0, seconds=15.0, pool=64, seed=0, budget=150e9),
+    "serve_poisson": dict(kind="serve", rate=2000.0, seconds=60.0, pool=1024, seed=0, budget=150e9),
 }
 DEFAULT_WORKLOAD = "conv_diff_256"
 
 BYTES_FP64_ITER = 576  # algorithmic bytes per cell per BiCGSTAB iteration, FP64 (72 words)
 BYTES_FP32_ITER = 288  # the same in the FP32 inner solve
 BYTES_OUTER = 104      # FP64 refinement step: r = b - A x (80) + x update (24)
+# a deflated FP32 iteration (near-singular systems) also reads z in the P, S and X
+# updates (1 B each) and A z in both matvecs (4 B each)
+BYTES_DEFL_ITER = 11
+BYTES_DEFL_SETUP = 61  # z (1) written; A z from the FP64 diagonals (56) and z, written (4)
 BYTES_SETUP = 128      # unit scaling (16 w) of FP64 A and B
 # Algorithmic bytes per cell of one launch of each kernel class (FP32 inner form,
 # FP64 drop-in): operands read + results written, reductions fused.
@@ -371,6 +375,124 @@ def workload_config(w: str, s) -> dict:
             "l2_policy": "inputs larger than L2 (A_M 7*8*cells bytes), no flush needed"}
 
 
+def pressure_measure(dev, steps: int, warmup: int) -> dict:
+    """The pressure-correction-like system (192x384x192 interior cells, symmetric
+    diffusion with void-fraction-weighted faces, diagonal excess 1e-6): the FP64
+    drop-in and the mixed form (deflated) on the device-resident arrays; solves/s,
+    iterations, FP64 true residual of the scaled system, and the measured
+    coefficient contrast."""
+    import torch
+
+    from mfix_b200 import leq
+    from mfix_b200 import systems as S
+
+    name = "pressure_192x384x192"
+    t0 = time.perf_counter()
+    s = make_system(name)
+    t_gen = time.perf_counter() - t0
+    n = s.n
+    A0 = torch.from_numpy(s.a).to(dev)
+    B0 = torch.from_numpy(s.b).to(dev)
+    A, B = torch.empty_like(A0), torch.empty_like(B0)
+    X = torch.zeros(n, dtype=torch.float64, device=dev)
+    geom = leq.geom(s.imax2, s.jmax2, s.kmax2, s.do_k)
+
+    def solve(precision):
+        A.copy_(A0)
+        B.copy_(B0)
+        X.zero_()
+        torch.cuda.synchronize()
+        rc, res = leq.batch_solve([s], precision=precision, on_device=True,
+                                  pointers=[(A.data_ptr(), B.data_ptr(), X.data_ptr())])
+        if rc != 0 or res[0].ier != 0:
+            raise RuntimeError(f"pressure solve rc={rc} ier={res[0].ier if res else None}: {leq.last_error()}")
+        return res[0], leq.last_stats()
+
+    def true_rel():
+        y = torch.empty_like(X)
+        leq.leq_matvec(geom, A.data_ptr(), X.data_ptr(), y.data_ptr())
+        return float(torch.linalg.vector_norm(B - y) / torch.linalg.vector_norm(B))
+
+    peak, peak_kind = measured_peak_hbm()
+    out = {"workload": name, "grid": list(WORKLOADS[name]["dims"]), "cells": n, "tol": s.tol,
+           "coefficient_contrast": S.coefficient_contrast(s), "generation_s": t_gen, "steps": steps}
+    xs = {}
+    for form, prec in (("fp64", 0), ("mixed", 1)):
+        for _ in range(warmup):
+            solve(prec)
+        ms = []
+        for _ in range(steps):
+            r, st = solve(prec)
+            ms.append(st["device_ms"])
+        t = float(np.mean(ms))
+        if prec == 0:
+            alg = n * (r.iterations * BYTES_FP64_ITER + BYTES_SETUP + 80)
+        else:
+            per = BYTES_FP32_ITER + (BYTES_DEFL_ITER if st["deflated"] else 0)
+            alg = n * (r.iterations * per + r.outer_steps * BYTES_OUTER + BYTES_SETUP + 7 * 12 +
+                       (BYTES_DEFL_SETUP if st["deflated"] else 0))
+        out[form] = {"solves_per_s": 1e3 / t, "ms_per_solve": t, "iterations": r.iterations,
+                     "outer_steps": r.outer_steps, "fp64_fallback": r.fp64_fallback, "deflated": st["deflated"],
+                     "true_rel_resid": true_rel(), "alg_gbs": alg / (t / 1e3) / 1e9,
+                     "frac_of_peak": alg / (t / 1e3) / 1e9 / peak, "gpu_launches": st["kernel_launches"]}
+        xs[form] = X.clone()
+    out["mixed_vs_fp64"] = out["mixed"]["solves_per_s"] / out["fp64"]["solves_per_s"]
+    out["mixed"]["rel_diff_vs_fp64"] = float(torch.linalg.vector_norm(xs["mixed"] - xs["fp64"]) /
+                                             torch.linalg.vector_norm(xs["fp64"]))
+    out["peak_gbs"], out["peak_kind"] = peak, peak_kind
+    return out
+
+
+def run_legs(args, dev) -> dict:
+    """The other benchmark configurations, measured in the default run: the
+    pressure-like system, the 512-system batch and a serving run; each with the
+    clocks seen during it, or the error that stopped it."""
+    import torch
+
+    legs = {}
+    want = [x for x in args.legs.split(",") if x]
+
+    def leg(name, fn):
+        sampler = ClockSampler(dev.index or 0)
+        t0 = time.perf_counter()
+        try:
+            with sampler:
+                r = fn()
+            r["clocks"] = sampler.summary()
+        except Exception as e:  # a failed leg is reported, the headline stands
+            r = {"error": f"{type(e).__name__}: {e}"}
+        r["wall_s"] = time.perf_counter() - t0
+        legs[name] = r
+        torch.cuda.empty_cache()
+
+    if "pressure" in want:
+        leg("pressure", lambda: pressure_measure(dev, 2, 1))
+    if "batch" in want:
+        def batch():
+            w = WORKLOADS["batch_512"]
+            t0 = time.perf_counter()
+            systems, _ = batch_systems(w["count"], w["seed"], w["tol"])
+            m = batch_measure(systems, dev, 3, 1)
+            m["generation_s"] = time.perf_counter() - t0
+            m["config"] = {"systems": w["count"], "sizes": "per axis U{16..96}", "tol": w["tol"], "itmax": w["itmax"]}
+            return m
+        leg("batch_512", batch)
+    if "serving" in want:
+        def serving():
+            w = WORKLOADS["serve_poisson"]
+            t0 = time.perf_counter()
+            pool = serve_pool(w["pool"], w["seed"])
+            m = serve_measure(pool, 10.0, w["budget"], fracs=(0.5,))
+            m["generation_s"] = time.perf_counter() - t0
+            m["config"] = {"sizes": "per axis log-uniform on [24, 160]", "pressure_share": 0.2, "tol": [1e-6, 1e-8],
+                           "hbm_budget_gb": w["budget"] / 1e9,
+                           "note": "10 s runs (the serve_poisson workload runs the 60 s of the spec)"}
+            del pool
+            return m
+        leg("serving", serving)
+    return legs
+
+
 def run_ours(args) -> None:
     import torch
 
@@ -555,6 +677,11 @@ def run_ours(args) -> None:
         "kernels_fp64": class_table(kt_fp64, n, False, peak, work_64),
         "wall_s_timed_mixed": wall,
     }
+    if world == 1 and args.legs:
+        # the other configurations (after the headline's own measurements)
+        del A0, B0, A, B, X, a_h, b_h, x_h
+        torch.cuda.empty_cache()
+        line["legs"] = run_legs(args, dev)
     if rank == 0 and world == 1 and not args.no_cpu:
         import oracle as O
 
@@ -722,42 +849,18 @@ def _alg_bytes(n: int, precision: int, iterations: int, outer: int, fallback_ite
     return n * (iterations * BYTES_FP64_ITER + BYTES_SETUP + 80)
 
 
-def run_batch_bench(args) -> None:
-    """512 uneven systems: one batched mixed-precision solve (every launch covers
-    all systems) vs a loop of plain FP64 single-system solves on the same arrays."""
+def batch_measure(systems, dev, steps: int, warmup: int, barrier=None, mx=None, sm=None) -> dict:
+    """The batched mixed form (every launch covers all systems) and the FP64 forms
+    on the same device arrays: `steps` timed mixed batches after `warmup`, one
+    FP64 batch, one loop of FP64 single-system solves.  mx / sm reduce a value
+    over ranks (max / sum); the defaults are the identity (one rank)."""
     import torch
 
     from mfix_b200 import leq
-    from mfix_b200 import systems as S
 
-    from mfix_b200 import shard
-
-    rank, world, local = dist_env()
-    w = WORKLOADS[args.workload]
-    sizes = S.batch_sizes(w["count"], w["seed"])
-    specs_all = [("conv_diff", d, w["tol"], q) for q, d in enumerate(sizes)]
-    # ranks share the independent systems (no collective on the data path)
-    mine = shard.assign([(i + 2) * (j + 2) * (k + 2) for i, j, k in sizes], world)[rank]
-    specs = [specs_all[q] for q in mine]
-    t0 = time.perf_counter()
-    systems = generate_systems(specs)
-    t_gen = time.perf_counter() - t0
-    cells = sum(x.n for x in systems)
-    dev = torch.device("cuda", local)
-    torch.cuda.set_device(dev)
-    if world > 1:
-        import datetime
-
-        import torch.distributed as dist
-
-        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300))
-
-    def barrier():
-        if world > 1:
-            import torch.distributed as dist
-
-            dist.barrier()
-        torch.cuda.synchronize()
+    barrier = barrier or (lambda: torch.cuda.synchronize())
+    mx = mx or (lambda v: v)
+    sm = sm or (lambda v: v)
     pristine = [(torch.from_numpy(x.a).to(dev), torch.from_numpy(x.b).to(dev)) for x in systems]
     work = [(torch.empty_like(a), torch.empty_like(b), torch.zeros(x.n, dtype=torch.float64, device=dev))
             for (a, b), x in zip(pristine, systems)]
@@ -794,84 +897,159 @@ def run_batch_bench(args) -> None:
             res.append(r[0])
         return res, dev_s, time.perf_counter() - t, launches
 
-    if args.only != "all":  # profiling runs: the batched solve of one form only
-        if args.line_lanes:
-            leq.set_option("line_lanes", args.line_lanes)
-        for _ in range(args.warmup + args.steps):
-            res, t_dev, t_wall, nl = batched(1 if args.only == "mixed" else 0)
-        print(f"{args.only} batch: {len(systems)} systems, {t_dev * 1e3:.1f} ms, {nl} launches, "
-              f"iterations max {max(r.iterations for r in res)} mean {np.mean([r.iterations for r in res]):.1f}")
-        leq.set_option("time_kernels", 1)  # fixed batch with events around every J-line launch
-        res, t_dev, t_wall, nl = batched(1 if args.only == "mixed" else 0)
-        st = leq.last_stats()
-        leq.set_option("time_kernels", 0)
-        print(f"  timed J-line launches: {st['jline_launches']} in {st['jline_ms']:.1f} ms of {t_dev * 1e3:.1f} ms; "
-              f"lanes {sorted(set(g for e, l, g in leq.autotune_table()))}")
-        for k, (ms, nl) in leq.last_kernel_times().items():
-            print(f"  {k:14s} {ms:9.2f} ms {nl:6d} launches")
-        return
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         batched(1)
     loop_fp64()  # warm: autotuning of every line length, graph paths
     barrier()
-    sampler = ClockSampler(local)
-    mixed = []
-    with sampler:
-        for _ in range(args.steps):
-            mixed.append(batched(1))
-        barrier()
-    fp64b = [batched(0) for _ in range(max(1, args.steps // 2))]
+    mixed = [batched(1) for _ in range(steps)]
+    barrier()
+    fp64b = [batched(0) for _ in range(max(1, steps // 2))]
     loop = loop_fp64()
     barrier()
     peak, peak_kind = measured_peak_hbm()
     rm = mixed[-1][0]
-    mx = lambda v: shard.max_over_ranks(v, dev)
-    sm = lambda v: shard.sum_over_ranks(v, dev)
     m_dev = mx(float(np.mean([m[1] for m in mixed])))
     m_wall = mx(float(np.mean([m[2] for m in mixed])))
     alg_m = sm(sum(_alg_bytes(x.n, 1, r.iterations, r.outer_steps) for x, r in zip(systems, rm)))
     alg_64 = sm(sum(_alg_bytes(x.n, 0, r.iterations, 0) for x, r in zip(systems, loop[0])))
     f_dev = mx(float(np.mean([m[1] for m in fp64b])))
-    loop = (loop[0], mx(loop[1]), mx(loop[2]), int(sm(loop[3])))
+    alg_f = sm(sum(_alg_bytes(x.n, 0, r.iterations, 0) for x, r in zip(systems, fp64b[-1][0])))
+    loop_dev, loop_wall, loop_launch = mx(loop[1]), mx(loop[2]), int(sm(loop[3]))
     nsys = int(sm(len(systems)))
-    cells = int(sm(cells))
+    return {
+        "systems": nsys, "cells": int(sm(sum(x.n for x in systems))), "steps": steps,
+        "mixed_batched": {"solves_per_s_device": nsys / m_dev, "solves_per_s_wall": nsys / m_wall,
+                          "ms_per_batch": m_dev * 1e3, "alg_gbs": alg_m / m_dev / 1e9,
+                          "frac_of_peak": alg_m / m_dev / 1e9 / peak, "peak_gbs": peak, "peak_kind": peak_kind,
+                          "fp64_fallbacks": sum(r.fp64_fallback for r in rm), "gpu_launches": int(mixed[-1][3]),
+                          "iterations_mean": float(np.mean([r.iterations for r in rm]))},
+        "fp64_batched": {"solves_per_s_device": nsys / f_dev, "alg_gbs": alg_f / f_dev / 1e9,
+                         "frac_of_peak": alg_f / f_dev / 1e9 / peak},
+        "fp64_loop": {"solves_per_s_device": nsys / loop_dev, "solves_per_s_wall": nsys / loop_wall,
+                      "alg_gbs": alg_64 / loop_dev / 1e9, "gpu_launches": loop_launch,
+                      "iterations_mean": float(np.mean([r.iterations for r in loop[0]]))},
+        "mixed_batched_vs_fp64_batched": f_dev / m_dev,
+        "mixed_batched_vs_fp64_loop_device": loop_dev / m_dev,
+        "mixed_batched_vs_fp64_loop_wall": loop_wall / m_wall,
+    }
+
+
+def batch_systems(count: int, seed: int, tol: float, indices=None):
+    """The batch workload's systems (per-axis sizes U{16..96}), generated in spawned
+    processes; `indices` selects a subset (a rank's share)."""
+    from mfix_b200 import systems as S
+
+    sizes = S.batch_sizes(count, seed)
+    specs = [("conv_diff", d, tol, q) for q, d in enumerate(sizes)]
+    if indices is not None:
+        specs = [specs[q] for q in indices]
+    return generate_systems(specs), sizes
+
+
+def run_batch_bench(args) -> None:
+    """512 uneven systems: one batched mixed-precision solve (every launch covers
+    all systems) vs a loop of plain FP64 single-system solves on the same arrays."""
+    import torch
+
+    from mfix_b200 import leq
+    from mfix_b200 import shard
+    from mfix_b200 import systems as S
+
+    rank, world, local = dist_env()
+    w = WORKLOADS[args.workload]
+    sizes = S.batch_sizes(w["count"], w["seed"])
+    # ranks share the independent systems (no collective on the data path)
+    mine = shard.assign([(i + 2) * (j + 2) * (k + 2) for i, j, k in sizes], world)[rank]
+    t0 = time.perf_counter()
+    systems, _ = batch_systems(w["count"], w["seed"], w["tol"], mine)
+    t_gen = time.perf_counter() - t0
+    dev = torch.device("cuda", local)
+    torch.cuda.set_device(dev)
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", init_method="env://", timeout=datetime.timedelta(seconds=300))
+
+    def barrier():
+        if world > 1:
+            import torch.distributed as dist
+
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    if args.only != "all":  # profiling runs: the batched solve of one form only
+        if args.line_lanes:
+            leq.set_option("line_lanes", args.line_lanes)
+        import torch as _t
+
+        pristine = [(_t.from_numpy(x.a).to(dev), _t.from_numpy(x.b).to(dev)) for x in systems]
+        ptrs = []
+        work = []
+        for (a0, b0), x in zip(pristine, systems):
+            a, b, xx = a0.clone(), b0.clone(), _t.zeros(x.n, dtype=_t.float64, device=dev)
+            work.append((a, b, xx))
+            ptrs.append((a.data_ptr(), b.data_ptr(), xx.data_ptr()))
+
+        def once(tk):
+            for (a0, b0), (a, b, xx) in zip(pristine, work):
+                a.copy_(a0)
+                b.copy_(b0)
+                xx.zero_()
+            _t.cuda.synchronize()
+            leq.set_option("time_kernels", tk)
+            rc, res = leq.batch_solve(systems, precision=1 if args.only == "mixed" else 0, on_device=True,
+                                      pointers=ptrs)
+            leq.set_option("time_kernels", 0)
+            if rc != 0:
+                raise RuntimeError(leq.last_error())
+            return res, leq.last_stats()
+
+        for _ in range(args.warmup + args.steps):
+            res, st = once(0)
+        print(f"{args.only} batch: {len(systems)} systems, {st['device_ms']:.1f} ms, {st['kernel_launches']} launches, "
+              f"iterations max {max(r.iterations for r in res)} mean {np.mean([r.iterations for r in res]):.1f}")
+        res, st = once(1)
+        print(f"  timed J-line launches: {st['jline_launches']} in {st['jline_ms']:.1f} ms of {st['device_ms']:.1f} ms; "
+              f"lanes {sorted(set(g for e, l, g in leq.autotune_table()))}")
+        for k, (ms, nl) in leq.last_kernel_times().items():
+            print(f"  {k:14s} {ms:9.2f} ms {nl:6d} launches")
+        return
+    sampler = ClockSampler(local)
+    with sampler:
+        m = batch_measure(systems, dev, args.steps, args.warmup, barrier,
+                          lambda v: shard.max_over_ranks(v, dev), lambda v: shard.sum_over_ranks(v, dev))
+    mb = m["mixed_batched"]
+    peak, peak_kind = measured_peak_hbm()
     line = {
-        "metric": "solves/s", "value": nsys / m_dev, "unit": "solves/s", "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": m_dev * 1e3, "higher_is_better": True, "scaling": "strong",
-        "vs_baseline": None, "dtype": "fp32-inner/fp64-refinement", "data": "synthetic",
-        "config": {"workload": args.workload, "systems": nsys, "cells": cells, "sizes": "per axis U{16..96}",
-                   "parallelism": f"systems sharded over {world} rank(s), longest first",
+        "metric": "solves/s", "value": mb["solves_per_s_device"], "unit": "solves/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": mb["ms_per_batch"], "higher_is_better": True,
+        "scaling": "strong", "vs_baseline": None, "dtype": "fp32-inner/fp64-refinement", "data": "synthetic",
+        "config": {"workload": args.workload, "systems": m["systems"], "cells": m["cells"],
+                   "sizes": "per axis U{16..96}", "parallelism": f"systems sharded over {world} rank(s), longest first",
                    "pc": "LINE", "sweep": "RSRS", "tol": w["tol"], "itmax": w["itmax"],
                    "l2_policy": "inputs larger than L2 (A_M of the batch 7*8*cells bytes)"},
-        "roofline": {"kernel": "whole batched solve (algorithmic bytes)", "bound": "hbm",
-                     "achieved": alg_m / m_dev / 1e9, "peak": peak, "unit": "GB/s",
-                     "frac": alg_m / m_dev / 1e9 / peak, "peak_kind": peak_kind, "traffic": None},
+        "roofline": {"kernel": "whole batched solve (algorithmic bytes)", "bound": "hbm", "achieved": mb["alg_gbs"],
+                     "peak": peak, "unit": "GB/s", "frac": mb["frac_of_peak"], "peak_kind": peak_kind, "traffic": None},
         "e2e": None,
-        "gpu_launches": int(mixed[-1][3]),
+        "gpu_launches": mb["gpu_launches"],
         "clocks": sampler.summary(),
-        "mixed_batched": {"solves_per_s_device": nsys / m_dev, "solves_per_s_wall": nsys / m_wall,
-                          "alg_gbs": alg_m / m_dev / 1e9, "fp64_fallbacks": sum(r.fp64_fallback for r in rm),
-                          "iterations_mean": float(np.mean([r.iterations for r in rm]))},
-        "fp64_batched": {"solves_per_s_device": nsys / f_dev},
-        "fp64_loop": {"solves_per_s_device": nsys / loop[1], "solves_per_s_wall": nsys / loop[2],
-                      "alg_gbs": alg_64 / loop[1] / 1e9, "gpu_launches": int(loop[3]),
-                      "iterations_mean": float(np.mean([r.iterations for r in loop[0]]))},
-        "mixed_batched_vs_fp64_loop_device": loop[1] / m_dev,
-        "mixed_batched_vs_fp64_loop_wall": loop[2] / m_wall,
         "generation_s": t_gen,
+        **{k: v for k, v in m.items() if k not in ("systems", "cells", "steps")},
     }
     if not args.no_cpu and rank == 0 and world == 1:
         import oracle as O
 
         t = time.perf_counter()
         k = 0
-        while k < nsys and (k < 4 or time.perf_counter() - t < 15.0):
+        while k < len(systems) and (k < 4 or time.perf_counter() - t < 15.0):
             c = systems[k].copy()
             O.leq_bicgs(c)
             k += 1
         dt = time.perf_counter() - t
         line["cpu_baseline"] = {"value": k / dt, "unit": "solves/s", "cores": O.num_threads(), "kind": "port",
-                                "sample": f"the first {k} of the {nsys} systems solved completely"}
+                                "sample": f"the first {k} of the {len(systems)} systems solved completely"}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:
@@ -898,8 +1076,10 @@ def _serve_run(leq, pool, precision, rate, seconds, seed, budget, check_every=8,
     nreq = int(rate * seconds * 1.2) + 16
     arrivals = np.cumsum(rng.exponential(1.0 / rate, nreq))
     arrivals = arrivals[arrivals < seconds]
-    which = rng.integers(0, len(pool), len(arrivals))
-    tols = np.where(rng.random(len(arrivals)) < 0.5, 1e-6, 1e-8)
+    # requests walk the pool of distinct systems in order (from a random start), so
+    # no system repeats before the pool is exhausted; each keeps its own TOL
+    which = (int(rng.integers(0, len(pool))) + np.arange(len(arrivals))) % len(pool)
+    tols = np.array([pool[q].tol for q in which])
     shared_x = [np.empty(p.n) for p in pool]  # outputs of unverified requests (never read)
     results, private = {}, {}
     srv = leq.Server(precision=precision, max_systems=max_systems, check_every=check_every, hbm_budget=budget)
@@ -984,10 +1164,12 @@ def _serve_closed(leq, pool, precision, inflight, seconds, seed, budget, check_e
     xs = [np.empty(p.n) for p in pool]  # outputs (never read)
     srv = leq.Server(precision=precision, max_systems=max_systems, check_every=check_every, hbm_budget=budget)
     which = {}
+    nxt = [int(rng.integers(0, len(pool)))]  # requests walk the pool of distinct systems in order
 
     def submit():
-        q = int(rng.integers(0, len(pool)))
-        t = srv.submit(_Req(pool[q], xs[q], float(1e-6 if rng.random() < 0.5 else 1e-8)), zero_guess=True)
+        q = nxt[0] % len(pool)
+        nxt[0] += 1
+        t = srv.submit(_Req(pool[q], xs[q], pool[q].tol), zero_guess=True)
         if t < 0:
             raise RuntimeError(f"submit failed: {t} {leq.last_error()}")
         which[t] = q
@@ -1035,46 +1217,42 @@ def _serve_closed(leq, pool, precision, inflight, seconds, seed, budget, check_e
             "nonzero_ier": sum(1 for _, r in done if r["ier"] != 0)}
 
 
-def run_serve_bench(args) -> None:
-    """The request server on a stream of mixed-size requests, mixed form vs FP64
-    form: capacity from closed-loop runs, p50/p99 latency from Poisson streams at
-    50% and 80% of the FP64 capacity (the same offered load for both forms), and
-    the workload's own offered rate (saturating) with served rate and backlog."""
+def serve_pool(count: int, seed: int):
+    """The serving workload's pool of distinct request systems (per-axis sizes
+    log-uniform on [24, 160], 20% pressure-like, TOL from {1e-6, 1e-8}), generated
+    in spawned processes, with pinned host copies of A_M and B_M (the server's
+    copies overlap the iterations)."""
     import torch
 
-    from mfix_b200 import leq
     from mfix_b200 import systems as S
 
-    w = WORKLOADS[args.workload]
-    rate = args.rate or w["rate"]
-    seconds = args.seconds or w["seconds"]
-    specs = S.serve_mix(w["pool"], w["seed"])
-    t0 = time.perf_counter()
-    pool = generate_systems(specs)
-    t_gen = time.perf_counter() - t0
-    torch.cuda.set_device(0)
-    # pinned host copies of the request arrays (the copies overlap the iterations)
+    pool = generate_systems(S.serve_mix(count, seed))
     for p in pool:
         a = torch.empty(p.a.shape, dtype=torch.float64).pin_memory().numpy()
         b = torch.empty(p.b.shape, dtype=torch.float64).pin_memory().numpy()
         np.copyto(a, p.a)
         np.copyto(b, p.b)
         p.a, p.b = a, b
-    peak, peak_kind = measured_peak_hbm()
-    sampler = ClockSampler(0)
-    with sampler:
-        cap_m = _serve_closed(leq, pool, 1, 256, seconds, 11, w["budget"])
-        cap_f = _serve_closed(leq, pool, 0, 256, seconds, 11, w["budget"])
-        if args.capacity_only:
-            print(json.dumps({"capacity": {"mixed": cap_m, "fp64": cap_f}}), flush=True)
-            return
-        loads = []
-        for frac in (0.5, 0.8):
-            lam = frac * cap_f["capacity"]
-            loads.append((frac, _serve_run(leq, pool, 1, lam, seconds, 2, w["budget"]),
-                          _serve_run(leq, pool, 0, lam, seconds, 2, w["budget"])))
-        sat = _serve_run(leq, pool, 1, rate, min(seconds, 10.0), 1, w["budget"])
+    return pool
 
+
+def serve_measure(pool, seconds: float, budget: float, fracs=(0.5,), offered=None) -> dict:
+    """Capacity of both forms from closed-loop runs (256 requests in flight), p50/p99
+    latency of both forms from Poisson streams at `fracs` of the FP64 capacity (the
+    same offered load for both), optionally the stream at `offered` req/s
+    (saturating: served rate and backlog); a sample of results checked against the
+    FP64 true residual."""
+    from mfix_b200 import leq
+
+    peak, peak_kind = measured_peak_hbm()
+    cap_m = _serve_closed(leq, pool, 1, 256, seconds, 11, budget)
+    cap_f = _serve_closed(leq, pool, 0, 256, seconds, 11, budget)
+    loads = []
+    for frac in fracs:
+        lam = frac * cap_f["capacity"]
+        loads.append((frac, _serve_run(leq, pool, 1, lam, seconds, 2, budget),
+                      _serve_run(leq, pool, 0, lam, seconds, 2, budget)))
+    sat = _serve_run(leq, pool, 1, offered, min(seconds, 10.0), 1, budget) if offered else None
     worst, checked = 0.0, 0
     for _, rm, rf in loads:
         for r in (rm, rf):
@@ -1086,32 +1264,64 @@ def run_serve_bench(args) -> None:
                 worst = max(worst, rel / float(r["_tols"][i]))
                 checked += 1
     strip = lambda r: {k: v for k, v in r.items() if not k.startswith("_")}
-    lat = {f"{int(100 * frac)}pct_of_fp64_capacity": {"offered_rate": rm["offered_rate"], "mixed": strip(rm),
-                                                       "fp64": strip(rf)} for frac, rm, rf in loads}
     half = loads[0]
+    out = {
+        "pool_systems": len(pool), "pool_cells_mean": float(np.mean([p.n for p in pool])), "seconds_per_run": seconds,
+        "capacity": {"mixed": cap_m, "fp64": cap_f, "mixed_vs_fp64": cap_m["capacity"] / cap_f["capacity"]},
+        "capacity_frac_of_peak": {"mixed": cap_m["alg_gbs"] / peak, "fp64": cap_f["alg_gbs"] / peak,
+                                  "peak_gbs": peak, "peak_kind": peak_kind},
+        "latency": {f"{int(100 * frac)}pct_of_fp64_capacity": {"offered_rate": rm["offered_rate"], "mixed": strip(rm),
+                                                               "fp64": strip(rf)} for frac, rm, rf in loads},
+        "p50_p99_ms": {"mixed": [half[1]["latency_ms"]["p50"], half[1]["latency_ms"]["p99"]],
+                       "fp64": [half[2]["latency_ms"]["p50"], half[2]["latency_ms"]["p99"]],
+                       "offered_rate": half[1]["offered_rate"]},
+        "verified_requests": checked, "worst_true_resid_over_tol": worst,
+        "gpu_launches": half[1]["gpu_launches"],
+    }
+    if sat is not None:
+        out["offered_stream"] = strip(sat)
+    return out
+
+
+def run_serve_bench(args) -> None:
+    """The request server on a stream of mixed-size requests, mixed form vs FP64
+    form: capacity from closed-loop runs, p50/p99 latency from Poisson streams at
+    50% and 80% of the FP64 capacity (the same offered load for both forms), and
+    the workload's own offered rate (saturating) with served rate and backlog."""
+    import torch
+
+    w = WORKLOADS[args.workload]
+    rate = args.rate or w["rate"]
+    seconds = args.seconds or w["seconds"]
+    torch.cuda.set_device(0)
+    t0 = time.perf_counter()
+    pool = serve_pool(w["pool"], w["seed"])
+    t_gen = time.perf_counter() - t0
+    sampler = ClockSampler(0)
+    with sampler:
+        m = serve_measure(pool, seconds, w["budget"], fracs=(0.5, 0.8), offered=rate)
+    peak, peak_kind = measured_peak_hbm()
+    cap_m = m["capacity"]["mixed"]
     line = {
         "metric": "solves/s & p50/p99 latency", "value": cap_m["capacity"], "unit": "solves/s", "n_gpus": 1,
         "steps": 1, "warmup": 1, "ms_per_step": seconds * 1e3, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "fp32-inner/fp64-refinement", "data": "synthetic",
         "config": {"workload": args.workload, "seconds_per_run": seconds, "pool_systems": len(pool),
-                   "pool_cells_mean": float(np.mean([p.n for p in pool])),
+                   "pool_cells_mean": m["pool_cells_mean"],
                    "sizes": "per axis log-uniform on [24, 160]", "pressure_share": 0.2, "tol": [1e-6, 1e-8],
-                   "hbm_budget_gb": w["budget"] / 1e9, "max_systems_per_batch": 512, "check_every": SERVE_CHECK_EVERY or 8,
+                   "hbm_budget_gb": w["budget"] / 1e9, "max_systems_per_batch": 512,
+                   "check_every": SERVE_CHECK_EVERY or 8,
                    "capacity": "closed loop, 256 requests in flight, completions after the first 20% of the run",
-                   "inputs": "pinned host A_M/B_M copied in per request, VAR copied out; zero initial guess"},
+                   "inputs": "pinned host A_M/B_M copied in per request, VAR copied out; zero initial guess; "
+                             "requests walk a pool of distinct systems"},
         "roofline": {"kernel": "served solves at capacity (algorithmic bytes of completed requests)", "bound": "hbm",
                      "achieved": cap_m["alg_gbs"], "peak": peak, "unit": "GB/s", "frac": cap_m["alg_gbs"] / peak,
                      "peak_kind": peak_kind, "traffic": None},
         "e2e": {"value": cap_m["capacity"], "unit": "solves/s", "note": "host arrays in and out per request"},
-        "gpu_launches": half[1]["gpu_launches"],
+        "gpu_launches": m["gpu_launches"],
         "clocks": sampler.summary(),
-        "capacity": {"mixed": cap_m, "fp64": cap_f, "mixed_vs_fp64": cap_m["capacity"] / cap_f["capacity"]},
-        "latency": lat,
-        "p50_p99_ms_at_half_fp64_capacity": {"mixed": [half[1]["latency_ms"]["p50"], half[1]["latency_ms"]["p99"]],
-                                             "fp64": [half[2]["latency_ms"]["p50"], half[2]["latency_ms"]["p99"]]},
-        "offered_stream": strip(sat),
-        "verified_requests": checked, "worst_true_resid_over_tol": worst,
         "generation_s": t_gen,
+        **{k: v for k, v in m.items() if k not in ("gpu_launches",)},
     }
     print(json.dumps(line), flush=True)
 
@@ -1124,6 +1334,9 @@ def main() -> None:
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline sample")
+    ap.add_argument("--legs", default="pressure,batch,serving",
+                    help="default workload: the other configurations measured in the same run (comma list of "
+                         "pressure, batch, serving; empty: none)")
     ap.add_argument("--line-lanes", type=int, default=0, help="force lanes per J-line (0: autotuned)")
     ap.add_argument("--rate", type=float, default=0.0, help="serving: offered requests/s (0: the workload's)")
     ap.add_argument("--serve-check", type=int, default=0, help="serving: iterations between state reads")

@@ -142,6 +142,9 @@ const char *mfixgpu_last_error(void);
  *                    (Phat = M^{-1} P + c z, z = 1 on rows with a nonzero neighbour coefficient,
  *                    c = z^T P / z^T A z), which keeps it converging on near-singular operators;
  *                    0: such systems go to the FP64 drop-in
+ *   "replace_every"  mixed form, deflated systems: the FP32 residual is replaced by the FP64 true
+ *                    residual at least every this many inner iterations (default 20; 0: only after
+ *                    the inner_tol drop)
  *   "write_back_ab"  1 (default) copy the scaled A_M/B_M slices back
  *   "rtilde_seed"    seed of the Rtilde random stream (replaces RANDOM_NUMBER, model/leq_bicgs.f:298)
  *   "inner_tol"      mixed form: drop of the FP32 residual between FP64 reliable updates (default 1e-2)

@@ -35,6 +35,7 @@ struct Options {
     int mixed_stalls = 6;
     double mixed_min_margin = 1e-4;
     int deflate = 1;
+    int replace_every = 20;
     int check_every = 4;
     int use_graph = 1;
     int time_kernels = 0;
@@ -123,6 +124,7 @@ SolveOptions make_opts(const Options &o, int pc, const char sweep4[4])
     so.mixed_stalls = o.mixed_stalls;
     so.mixed_min_margin = o.mixed_min_margin;
     so.deflate = o.deflate != 0;
+    so.replace_every = o.replace_every;
     so.check_every = o.check_every;
     so.use_graph = o.use_graph != 0;
     so.time_kernels = o.time_kernels != 0;
@@ -495,6 +497,9 @@ int mfixgpu_set_option(const char *name, double value)
         g.opt.mixed_growth = value;
     } else if (k == "deflate") {
         g.opt.deflate = value != 0;
+    } else if (k == "replace_every") {
+        if (value < 0) return MFIXGPU_ERR_ARGS;
+        g.opt.replace_every = (int)value;
     } else if (k == "mixed_min_margin") {
         if (!(value >= 0)) return MFIXGPU_ERR_ARGS;
         g.opt.mixed_min_margin = value;
@@ -533,6 +538,7 @@ double mfixgpu_get_option(const char *name)
     if (k == "mixed_stalls") return g.opt.mixed_stalls;
     if (k == "mixed_min_margin") return g.opt.mixed_min_margin;
     if (k == "deflate") return g.opt.deflate;
+    if (k == "replace_every") return g.opt.replace_every;
     if (k == "check_every") return g.opt.check_every;
     if (k == "use_graph") return g.opt.use_graph;
     if (k == "time_kernels") return g.opt.time_kernels;

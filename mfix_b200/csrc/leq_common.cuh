@@ -133,6 +133,8 @@ struct SysState {
     int defl;             // mixed form: the inner iteration deflates z (coupled-row indicator)
     double defl_e;        // z^T A z
     double defl_cp, defl_cs;  // z^T P / z^T A z and z^T S / z^T A z of the current iteration
+    int replace_every;    // mixed form, deflated systems: FP64 residual replacement at least every this many iterations
+    int since_outer;      // mixed form: inner iterations since the last FP64 update
     int err;
     unsigned int arrivals;  // tiles that finished the current reduction kernel
 };

@@ -321,6 +321,7 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         st.stall_limit = opt.mixed_stalls;
         st.min_margin = opt.mixed_min_margin;
         st.defl_allow = opt.deflate ? 1 : 0;
+        st.replace_every = opt.replace_every;
         st.margin_bits = 0x7f800000u;
         st.i = 1;
         st.iter = 1;

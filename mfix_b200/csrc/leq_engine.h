@@ -63,6 +63,7 @@ struct SolveOptions {
     double mixed_min_margin = 1e-4;  // mixed form: smaller diagonal-dominance margins are deflated (or go to FP64)
     bool deflate = true;         // mixed form: deflate the near-null mode of systems below mixed_min_margin
                                  // (false: they go straight to the FP64 drop-in)
+    int replace_every = 20;      // mixed form, deflated systems: FP64 residual replacement interval (0: off)
     int check_every = 4;         // iterations between host checks of the state
     bool use_graph = true;       // capture the iteration body in a CUDA graph
     bool time_kernels = false;   // record events around every J-line launch (no graph replay)

@@ -1123,7 +1123,12 @@ __device__ inline void fin_xr_inner(SysState &s, double rr, double rtr)
         return;
     }
     if (rn > s.maxr) s.maxr = rn;
-    if (rn <= s.inner_tol * s.maxr || rn <= s.tol * s.outer_rnorm0 || s.inner_total >= s.itmax) {
+    s.since_outer += 1;
+    // deflated (near-singular) systems also replace the residual at a fixed
+    // interval: their slow FP32 recurrence drifts from the true residual long
+    // before it has dropped by inner_tol
+    const bool due = s.defl && s.replace_every > 0 && s.since_outer >= s.replace_every;
+    if (rn <= s.inner_tol * s.maxr || rn <= s.tol * s.outer_rnorm0 || s.inner_total >= s.itmax || due) {
         s.phase = PH_OUTER;
         return;
     }
@@ -1285,14 +1290,23 @@ __device__ inline void fin_outer(SysState &s, double rr, double rtr32)
         return;
     }
     // guard: FP32 iterations that diverge or stall on a (near-)singular operator
-    // hand the system to an FP64 re-solve instead of returning a worse answer
+    // hand the system to an FP64 re-solve instead of returning a worse answer.
+    // A deflated system's residual plateaus for hundreds of iterations (as the
+    // FP64 drop-in's does on it) and is replaced at a fixed interval, so its
+    // stall window is 400 iterations and its growth limit 1e4.
     if (rn < 0.9 * s.best) {
         s.best = rn;
         s.stall = 0;
     } else {
         s.stall += 1;
     }
-    if (!(rn == rn) || rn > s.growth_limit * s.best || s.stall >= s.stall_limit) {
+    int stall_limit = s.stall_limit;
+    double growth_limit = s.growth_limit;
+    if (s.defl && s.replace_every > 0) {
+        stall_limit = max(stall_limit, (400 + s.replace_every - 1) / s.replace_every);
+        growth_limit = fmax(growth_limit, 1e4);
+    }
+    if (!(rn == rn) || rn > growth_limit * s.best || s.stall >= stall_limit) {
         s.exit_kind = EX_FALLBACK;
         s.ier = -20;
         s.status = ST_DONE;
@@ -1305,6 +1319,7 @@ __device__ inline void fin_outer(SysState &s, double rr, double rtr32)
     }
     s.maxr = rn;
     s.inner_first = 1;
+    s.since_outer = 0;
     s.snorm_exit = 0;
     s.phase = PH_INNER;
     if (fresh) {

@@ -175,6 +175,7 @@ int Engine::live_add(const LiveSystem &ls)
     st.stall_limit = live_opt_.mixed_stalls;
     st.min_margin = live_opt_.mixed_min_margin;
     st.defl_allow = live_opt_.deflate ? 1 : 0;
+    st.replace_every = live_opt_.replace_every;
     st.margin_bits = 0x7f800000u;
     st.i = 1;
     st.iter = 1;
