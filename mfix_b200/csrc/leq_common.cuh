@@ -73,6 +73,14 @@ enum LineKind : int { LK_WARP = 0, LK_THREAD = 1 };
 struct SysDev {
     int imax2, jmax2, kmax2, do_k;
     int64_t n;           // DIMENSION_3 (cells incl. the wall layer)
+    // Layout of the arrays in the form's working precision.  The FP64 drop-in
+    // works on the caller's arrays (line pitch JMAX2, n cells).  The mixed form's
+    // FP32 arrays (diagonals, factors, vectors) are its own: each J-line padded to
+    // a pitch that is a multiple of four cells, so every line starts on a 16-byte
+    // boundary; the pad cells hold zeros (diagonal A(0) = 1).
+    int jp;              // line pitch of those arrays
+    int64_t np;          // their cells: jp * imax2 * kmax2
+    FastDiv div_jp;      // division by jp
     FastDiv div_j;       // division by jmax2
     FastDiv div_i;       // division by imax2
     FastDiv div_h;       // division by half_lines

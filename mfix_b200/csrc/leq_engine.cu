@@ -211,13 +211,23 @@ cudaError_t Engine::stage_close() { return cudaEventRecord(stage_ev_[stage_cur_]
 // nine iteration vectors and the three J-line factor arrays (elements of the
 // form's precision), then the per-line flags; the mixed form's copy of the
 // initial guess follows that region.
+// Line pitch and cells of a system's arrays in the form's precision: the mixed
+// form's FP32 arrays pad each J-line to a multiple of four cells.
+int form_pitch(int jmax2, int precision) { return precision == PREC_MIXED ? (jmax2 + 3) / 4 * 4 : jmax2; }
+int64_t form_cells(int64_t n, int64_t lines, int precision)
+{
+    if (precision != PREC_MIXED || lines <= 0) return n;
+    return (int64_t)form_pitch((int)(n / lines), precision) * lines;
+}
+
 size_t vec_region_bytes(int64_t n, int64_t lines, int precision)
 {
     const size_t ew = precision == PREC_MIXED ? 4 : 8;
+    const size_t m = (size_t)form_cells(n, lines, precision);
     size_t b = 0;
     if (precision == PREC_MIXED)  // FP32 diagonals, row sums, deflation vector z and A z
-        b += align_up(7 * (size_t)n * 4, 256) + 2 * align_up((size_t)n * 4, 256) + align_up((size_t)n, 256);
-    b += (NVEC + 3) * align_up((size_t)n * ew, 256) + align_up((size_t)lines * 4, 256);
+        b += align_up(7 * m * 4, 256) + 2 * align_up(m * 4, 256) + align_up(m, 256);
+    b += (NVEC + 3) * align_up(m * ew, 256) + align_up((size_t)lines * 4, 256);
     return b;
 }
 
@@ -237,7 +247,7 @@ size_t live_work_bytes(int64_t n, int64_t lines, int precision)
 
 void carve_work(SysDev &d, char *work, int64_t lines, int precision, char *x0)
 {
-    const size_t n = (size_t)d.n;
+    const size_t n = (size_t)form_cells(d.n, lines, precision);
     const size_t ew = precision == PREC_MIXED ? 4 : 8;
     size_t off = 0;
     auto take = [&](size_t bytes) {
@@ -293,8 +303,11 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         d.n = sp.n;
         d.div_j = make_fastdiv((uint32_t)sp.jmax2);
         d.div_i = make_fastdiv((uint32_t)sp.imax2);
+        d.jp = form_pitch(sp.jmax2, opt.precision);
+        d.np = (int64_t)d.jp * sp.imax2 * sp.kmax2;
+        d.div_jp = make_fastdiv((uint32_t)d.jp);
         d.pc = opt.pc;
-        d.ntiles = (int)((sp.n + TILE_CELLS - 1) / TILE_CELLS);
+        d.ntiles = (int)((std::max(sp.n, d.np) + TILE_CELLS - 1) / TILE_CELLS);
         d.tile_base = tile_base;
         tile_base += d.ntiles;
         shape_for(sp.jmax2, mixed ? 4 : 8, opt.force_lanes, &d.lane_group, &d.rows_per_lane, &d.line_kind);
@@ -374,7 +387,7 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
     cfg_.g_mv_pair = grid(oc.matvec_pair);
     cfg_.rows_pair = cfg_.rows_single = 0;
     for (int q = 0; q < nsys_; ++q)
-        if (h_sys_[q].n > 0) ((h_sys_[q].jmax2 & 1) ? cfg_.rows_single : cfg_.rows_pair) = 1;
+        if (h_sys_[q].n > 0) ((h_sys_[q].jp & 1) ? cfg_.rows_single : cfg_.rows_pair) = 1;
     cfg_.g_copy = grid(oc.copy);
     cfg_.g_outer = grid(oc.outer);
     return configure_lines(mixed ? 4 : 8);
@@ -418,7 +431,11 @@ int Engine::configure_lines(int elem, int only_L)
     const int items = h_prefix_[nsys_];
     cfg_.line_grid = std::max(1, std::min((items + wpb - 1) / wpb, sms_ * bpsm));
     // which line kernels the batch needs (systems with no line work count for none)
+    // rows per access of the warp kernel: four when every system's lines start on
+    // 16-byte boundaries (the mixed form's padded FP32 arrays) and its lanes' spans
+    // are multiples of four, two when they start on 8- or 16-byte boundaries
     cfg_.line_thread = cfg_.line_warp = cfg_.line_single = 0;
+    cfg_.line_vw = elem == 4 ? 4 : 2;
     for (int s = 0; s < nsys_; ++s) {
         if (h_prefix_[s + 1] == h_prefix_[s]) continue;
         const SysDev &d = h_sys_[s];
@@ -426,9 +443,11 @@ int Engine::configure_lines(int elem, int only_L)
             cfg_.line_thread = 1;
         } else {
             cfg_.line_warp = 1;
-            if (d.jmax2 & 1) cfg_.line_single = 1;
+            if (d.jp & 1) cfg_.line_single = 1;
+            if ((d.jp & 3) || d.lane_group < 4) cfg_.line_vw = std::min(cfg_.line_vw, 2);
         }
     }
+    if (cfg_.line_single) cfg_.line_vw = 1;
     if (!cfg_.line_thread && !cfg_.line_warp) cfg_.line_warp = 1;  // empty batch: a no-op launch
     const int tocc = elem == 4 ? line_thread_occupancy<float>() : line_thread_occupancy<double>();
     cfg_.line_grid_thread = std::max(1, std::min((items + 3) / 4, sms_ * tocc));
@@ -938,6 +957,9 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
         d.n = n;
         d.div_j = make_fastdiv((uint32_t)d.jmax2);
         d.div_i = make_fastdiv((uint32_t)d.imax2);
+        d.jp = d.jmax2;
+        d.np = n;
+        d.div_jp = d.div_j;
         if (!d_one_sys_) CK(cudaMalloc((void **)&d_one_sys_, sizeof(SysDev)));
         CK(cudaMemcpyAsync(d_one_sys_, &d, sizeof(SysDev), cudaMemcpyHostToDevice, stream_));
         if ((size_t)n * 8 > gm_basis_bytes_) {  // VAR_tmp in the GMRES scratch
@@ -1476,6 +1498,9 @@ int Engine::matvec(const SystemSpec &g, const double *a, const double *x, double
     d.n = g.n;
     d.div_j = make_fastdiv((uint32_t)g.jmax2);
     d.div_i = make_fastdiv((uint32_t)g.imax2);
+    d.jp = g.jmax2;
+    d.np = g.n;
+    d.div_jp = d.div_j;
     if (!d_one_sys_) CK(cudaMalloc((void **)&d_one_sys_, sizeof(SysDev)));
     CK(cudaMemcpyAsync(d_one_sys_, &d, sizeof(SysDev), cudaMemcpyHostToDevice, stream_));
     const int grid = std::max(1, std::min((int)((g.n + CELL_THREADS - 1) / CELL_THREADS), sms_ * 8));

@@ -355,6 +355,10 @@ void line_shape(int L, int *G, int *c);
 // the mixed form (work_bytes); live_work_bytes also leaves room for an FP64
 // re-solve of a mixed attempt in the same block.
 size_t vec_region_bytes(int64_t n, int64_t lines, int precision);
+// Line pitch and cells of the arrays in a form's precision (the mixed form pads
+// each J-line of its FP32 arrays to a multiple of four cells).
+int form_pitch(int jmax2, int precision);
+int64_t form_cells(int64_t n, int64_t lines, int precision);
 size_t work_bytes(int64_t n, int64_t lines, int precision);
 size_t live_work_bytes(int64_t n, int64_t lines, int precision);
 // Points d's work arrays into `work` (d.n and d.x64[0] set); x0: where the

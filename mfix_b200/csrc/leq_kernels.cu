@@ -54,6 +54,46 @@ __device__ __forceinline__ CellIdx cell_ijk(const SysDev &d, uint32_t c)
     return r;
 }
 
+// Layout of the arrays a kernel of element type T works on (SysDev::jp): the
+// FP64 drop-in's are the caller's (pitch JMAX2, n cells), the mixed form's FP32
+// arrays are padded (pitch jp, np cells).  j >= jmax2 marks a pad cell.
+template <typename T>
+__device__ __forceinline__ int pitch(const SysDev &d)
+{
+    return sizeof(T) == 4 ? d.jp : d.jmax2;
+}
+template <typename T>
+__device__ __forceinline__ int64_t cells(const SysDev &d)
+{
+    return sizeof(T) == 4 ? d.np : d.n;
+}
+template <typename T>
+__device__ __forceinline__ CellIdx cell_ijk_t(const SysDev &d, uint32_t c)
+{
+    if (sizeof(T) == 8) return cell_ijk(d, c);
+    const uint32_t line = fdiv(c, d.div_jp);
+    CellIdx r;
+    r.j = (int)(c - line * (uint32_t)d.jp);
+    const uint32_t k = fdiv(line, d.div_i);
+    r.k = (int)k;
+    r.i = (int)(line - k * (uint32_t)d.imax2);
+    return r;
+}
+
+// Index in the mixed form's padded FP32 arrays of natural cell c.
+__device__ __forceinline__ int64_t padded(const SysDev &d, int64_t c)
+{
+    const uint32_t line = fdiv((uint32_t)c, d.div_j);
+    return c + (int64_t)line * (d.jp - d.jmax2);
+}
+// Natural cell of padded index p (-1 for a pad cell).
+__device__ __forceinline__ int64_t natural(const SysDev &d, int64_t p)
+{
+    const uint32_t line = fdiv((uint32_t)p, d.div_jp);
+    const int j = (int)(p - (int64_t)line * d.jp);
+    return j < d.jmax2 ? (int64_t)line * d.jmax2 + j : -1;
+}
+
 // 7-point product of row c with x, in the operand order of LEQ_MATVEC
 // (model/leqsol_mod.f:240-250), neighbours clamped at the array edge.
 template <typename T, typename TX>
@@ -317,24 +357,35 @@ __global__ void k_to_f32(BatchView b)
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
         if (!gate_ok(b.st[tl.sys], G_INIT)) continue;
-        const int64_t n = d.n;
-        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(n, c0 + TILE_CELLS);
+        const int64_t n = d.n, np = d.np;
+        const int64_t p0 = (int64_t)tl.idx * TILE_CELLS, p1 = min(np, p0 + TILE_CELLS);
         float margin = __int_as_float(0x7f800000);  // +inf
         #pragma unroll 4
-        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
+        for (int64_t p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+            const int64_t c = natural(d, p);
+            if (c < 0) {  // pad cell of the padded FP32 arrays: zeros, A(0) = 1
+#pragma unroll
+                for (int q = 0; q < 7; ++q) d.a32[q * np + p] = q == 3 ? 1.f : 0.f;
+                d.defect[p] = 0.f;
+                d.defl_z[p] = 0;
+                d.defl_az[p] = 0.f;
+#pragma unroll
+                for (int v = V_R; v < NVEC; ++v) reinterpret_cast<float *>(d.vec[v])[p] = 0.f;
+                continue;
+            }
             double sum = 0.0;
             bool coupled = false;
 #pragma unroll
             for (int q = 0; q < 7; ++q) {
                 const double v = d.a64[q * n + c];
-                d.a32[q * n + c] = (float)v;
+                d.a32[q * np + p] = (float)v;
                 if (d.do_k || (q != 0 && q != 6)) {
                     sum += v;
                     if (q != 3 && v != 0.0) coupled = true;
                 }
             }
-            d.defect[c] = (float)sum;  // the row sum, exact to FP32 rounding however small
-            d.defl_z[c] = coupled ? 1 : 0;
+            d.defect[p] = (float)sum;  // the row sum, exact to FP32 rounding however small
+            d.defl_z[p] = coupled ? 1 : 0;
             const double a0 = fabs(d.a64[3 * n + c]);
             if (a0 > 0.0) margin = fminf(margin, (float)(fabs(sum) / a0));
         }
@@ -366,14 +417,31 @@ __global__ void k_defl_setup(BatchView b)
         if (!gate_ok(st, G_INIT) || !st.mixed || !st.defl_allow ||
             !(__uint_as_float(st.margin_bits) < st.min_margin))
             continue;
-        const int64_t c0 = (int64_t)tl.idx * TILE_CELLS, c1 = min(d.n, c0 + TILE_CELLS);
+        const int64_t p0 = (int64_t)tl.idx * TILE_CELLS, p1 = min(d.np, p0 + TILE_CELLS);
+        const int64_t n = d.n, c1 = d.jp, c2 = (int64_t)d.jp * d.imax2;
         double v[1] = {0.0};
         #pragma unroll 2
-        for (int64_t c = c0 + threadIdx.x; c < c1; c += blockDim.x) {
-            const CellIdx q = cell_ijk(d, (uint32_t)c);
-            const double az = stencil_row<double, unsigned char>(d, d.a64, d.defl_z, (uint32_t)c, q);
-            d.defl_az[c] = (float)az;
-            if (d.defl_z[c]) v[0] += az;
+        for (int64_t p = p0 + threadIdx.x; p < p1; p += blockDim.x) {
+            const int64_t c = natural(d, p);
+            if (c < 0) continue;  // pad cell (A z = 0 there)
+            // A z in the operand order of LEQ_MATVEC: FP64 diagonals at the natural
+            // cell, z at the padded neighbours (clamped at the array edge)
+            const CellIdx q = cell_ijk_t<float>(d, (uint32_t)p);
+            const unsigned char *z = d.defl_z;
+            const int64_t jm = q.j > 0 ? -1 : 0, jq = q.j < d.jmax2 - 1 ? 1 : 0;
+            const int64_t im = q.i > 0 ? -c1 : 0, ip = q.i < d.imax2 - 1 ? c1 : 0;
+            double az = d.a64[1 * n + c] * (double)z[p + jm];
+            az = az + d.a64[2 * n + c] * (double)z[p + im];
+            az = az + d.a64[3 * n + c] * (double)z[p];
+            az = az + d.a64[4 * n + c] * (double)z[p + ip];
+            az = az + d.a64[5 * n + c] * (double)z[p + jq];
+            if (d.do_k) {
+                const int64_t km = q.k > 0 ? -c2 : 0, kp = q.k < d.kmax2 - 1 ? c2 : 0;
+                az = az + d.a64[0 * n + c] * (double)z[p + km];
+                az = az + d.a64[6 * n + c] * (double)z[p + kp];
+            }
+            d.defl_az[p] = (float)az;
+            if (z[p]) v[0] += az;
         }
         tile_partial<1>(b, d, tl.idx, v);
         run_add<1>(b, run, tl.sys, fin);
@@ -468,10 +536,12 @@ struct Offs {
     int64_t jm, jp, im, ip, km, kp;
 };
 
-__device__ __forceinline__ Offs cell_offs(const SysDev &d, uint32_t c)
+template <typename T = double>
+__device__ __forceinline__ Offs cell_offs(const SysDev &d, uint32_t c, int *jout = nullptr)
 {
-    const CellIdx q = cell_ijk(d, c);
-    const int64_t c1 = d.jmax2, c2 = (int64_t)d.jmax2 * d.imax2;
+    const CellIdx q = cell_ijk_t<T>(d, c);
+    if (jout) *jout = q.j;
+    const int64_t c1 = pitch<T>(d), c2 = (int64_t)pitch<T>(d) * d.imax2;
     Offs o;
     o.jm = q.j > 0 ? -1 : 0;
     o.jp = q.j < d.jmax2 - 1 ? 1 : 0;
@@ -489,12 +559,14 @@ struct Row7 {
     T a[7], x[7];
 };
 
+// T = float: the mixed form's padded FP32 arrays; *jout receives the row's j
+// (j >= JMAX2 marks a pad cell, whose product the caller discards).
 template <typename T, typename TX, bool DEFECT = false>
 __device__ __forceinline__ void load_row7(const SysDev &d, const T *__restrict__ A, const TX *__restrict__ X,
-                                          int64_t c, Row7<T> &r)
+                                          int64_t c, Row7<T> &r, int *jout = nullptr)
 {
-    const int64_t n = d.n;
-    const Offs o = cell_offs(d, (uint32_t)c);
+    const int64_t n = cells<T>(d);
+    const Offs o = cell_offs<T>(d, (uint32_t)c, jout);
     r.a[0] = A[1 * n + c];
     r.x[0] = (T)X[c + o.jm];
     r.a[1] = A[2 * n + c];
@@ -589,7 +661,8 @@ __device__ __forceinline__ vec2_t<T> mk2(T a, T b)
 // form for odd JMAX2, whose cells may straddle two lines, needs one-by-one loads
 // of the i and k neighbours; in the same kernel it slowed the even form by
 // 10-25%.)
-__device__ __forceinline__ bool pair_rows(const SysDev &d) { return (d.jmax2 & 1) == 0; }
+template <typename T>
+__device__ __forceinline__ bool pair_rows(const SysDev &d) { return (pitch<T>(d) & 1) == 0; }
 
 template <typename T>
 struct Pair7 {
@@ -598,11 +671,12 @@ struct Pair7 {
 
 template <typename T, bool DEFECT = false>
 __device__ __forceinline__ void load_pair7(const SysDev &d, const T *__restrict__ A, const T *__restrict__ X,
-                                           int64_t c, Pair7<T> &r)
+                                           int64_t c, Pair7<T> &r, int *jout = nullptr)
 {
-    const int64_t n = d.n;
-    const CellIdx q = cell_ijk(d, (uint32_t)c);
-    const int64_t c1 = d.jmax2, c2 = (int64_t)d.jmax2 * d.imax2;
+    const int64_t n = cells<T>(d);
+    const CellIdx q = cell_ijk_t<T>(d, (uint32_t)c);
+    if (jout) *jout = q.j;
+    const int64_t c1 = pitch<T>(d), c2 = (int64_t)pitch<T>(d) * d.imax2;
     const int64_t im = q.i > 0 ? -c1 : 0, ip = q.i < d.imax2 - 1 ? c1 : 0;
     const vec2_t<T> xc = ld2(X + c);
     const T xl = X[c + (q.j > 0 ? -1 : 0)];              // x(j-1) of cell c (clamped)
@@ -703,7 +777,7 @@ __global__ void __launch_bounds__(256, 4) k_p_update(BatchView b)
         const SysState &st = b.st[tl.sys];
         if (!gate_ok(st, G_INNER)) continue;
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
-        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
+        const int cnt = (int)min((int64_t)TILE_CELLS, cells<T>(d) - c0);
         const T *__restrict__ r = vec<T>(d, V_R) + c0;
         T *__restrict__ p = vec<T>(d, V_P) + c0;
         const int np = cnt >> 1;  // cell pairs; an odd last cell is done by thread 0
@@ -779,8 +853,8 @@ __global__ void __launch_bounds__(256, 4) k_diag(BatchView b, int src, int dst, 
         const SysDev &d = b.sys[tl.sys];
         if (!gate_ok(b.st[tl.sys], gate)) continue;
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
-        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
-        const T *__restrict__ a0 = diag_base<T>(d) + 3 * d.n + c0;
+        const int cnt = (int)min((int64_t)TILE_CELLS, cells<T>(d) - c0);
+        const T *__restrict__ a0 = diag_base<T>(d) + 3 * cells<T>(d) + c0;
         const T *__restrict__ x = vec<T>(d, src) + c0;
         T *__restrict__ y = vec<T>(d, dst) + c0;
         for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
@@ -811,7 +885,7 @@ __global__ void __launch_bounds__(256, 4) k_copy(BatchView b, int src, int dst, 
         const SysDev &d = b.sys[tl.sys];
         if (!gate_ok(b.st[tl.sys], gate)) continue;
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
-        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
+        const int cnt = (int)min((int64_t)TILE_CELLS, cells<T>(d) - c0);
         const T *__restrict__ x = vec<T>(d, src) + c0;
         T *__restrict__ y = vec<T>(d, dst) + c0;
         for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
@@ -842,9 +916,9 @@ __global__ void __launch_bounds__(256) k_matvec_alpha(BatchView b, int src)
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
         SysState &st = b.st[tl.sys];
-        if (!gate_ok(st, G_INNER) || pair_rows(d) != PAIR) continue;
+        if (!gate_ok(st, G_INNER) || pair_rows<T>(d) != PAIR) continue;
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
-        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
+        const int cnt = (int)min((int64_t)TILE_CELLS, cells<T>(d) - c0);
         const T *__restrict__ a = diag_base<T>(d);
         const T *__restrict__ x = vec<T>(d, src);
         const T *__restrict__ rt = vec<T>(d, V_RT);
@@ -857,12 +931,13 @@ __global__ void __launch_bounds__(256) k_matvec_alpha(BatchView b, int src)
             const int np = cnt >> 1;
             for (int base = threadIdx.x; base < np; base += UP * blockDim.x) {
                 Pair7<T> rw[UP];
+                int jr[UP];
                 vec2_t<T> rtv[UP];
 #pragma unroll
                 for (int u = 0; u < UP; ++u) {
                     const int q = base + u * blockDim.x;
                     if (q < np) {
-                        load_pair7<T, MIXED>(d, a, x, c0 + 2 * q, rw[u]);
+                        load_pair7<T, MIXED>(d, a, x, c0 + 2 * q, rw[u], &jr[u]);
                         rtv[u] = ld2(rt + c0 + 2 * q);
                     }
                 }
@@ -871,6 +946,8 @@ __global__ void __launch_bounds__(256) k_matvec_alpha(BatchView b, int src)
                     const int q = base + u * blockDim.x;
                     if (q < np) {
                         vec2_t<T> yv = dot_pair7<T, MIXED>(rw[u], d.do_k);
+                        if (jr[u] >= d.jmax2) yv.x = T(0);  // pad cells of the padded FP32 arrays
+                        if (jr[u] + 1 >= d.jmax2) yv.y = T(0);
                         if (defl) {
                             const float2 az = ld2(d.defl_az + c0 + 2 * q);
                             yv.x = yv.x + (T)(cp * (double)az.x);
@@ -885,12 +962,13 @@ __global__ void __launch_bounds__(256) k_matvec_alpha(BatchView b, int src)
         } else {
         for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
             Row7<T> rw[U];
+            int jr[U];
             T rtv[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int c = base + u * blockDim.x;
                 if (c < cnt) {
-                    load_row7<T, T, MIXED>(d, a, x, c0 + c, rw[u]);
+                    load_row7<T, T, MIXED>(d, a, x, c0 + c, rw[u], &jr[u]);
                     rtv[u] = rt[c0 + c];
                 }
             }
@@ -899,6 +977,7 @@ __global__ void __launch_bounds__(256) k_matvec_alpha(BatchView b, int src)
                 const int c = base + u * blockDim.x;
                 if (c < cnt) {
                     T yv = dot_row7<T, MIXED>(rw[u], d.do_k);
+                    if (jr[u] >= d.jmax2) yv = T(0);
                     if (defl) yv = yv + (T)(cp * (double)d.defl_az[c0 + c]);
                     y[c0 + c] = yv;
                     v[0] += (double)rtv[u] * (double)yv;
@@ -934,7 +1013,7 @@ __global__ void __launch_bounds__(256, 4) k_s_update(BatchView b)
         SysState &st = b.st[tl.sys];
         if (!gate_ok(st, G_INNER)) continue;
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
-        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
+        const int cnt = (int)min((int64_t)TILE_CELLS, cells<T>(d) - c0);
         const T alpha = (T)st.alpha;
         const T *__restrict__ r = vec<T>(d, V_R) + c0;
         const T *__restrict__ vv = vec<T>(d, V_V) + c0;
@@ -995,9 +1074,9 @@ __global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
         SysState &st = b.st[tl.sys];
-        if (!gate_ok(st, G_INNER_NOSNORM) || pair_rows(d) != PAIR) continue;
+        if (!gate_ok(st, G_INNER_NOSNORM) || pair_rows<T>(d) != PAIR) continue;
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
-        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
+        const int cnt = (int)min((int64_t)TILE_CELLS, cells<T>(d) - c0);
         const T *__restrict__ a = diag_base<T>(d);
         const T *__restrict__ x = vec<T>(d, src);
         const T *__restrict__ s = vec<T>(d, V_S);
@@ -1010,12 +1089,13 @@ __global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
             const int np = cnt >> 1;
             for (int base = threadIdx.x; base < np; base += UP * blockDim.x) {
                 Pair7<T> rw[UP];
+                int jr[UP];
                 vec2_t<T> sv[UP];
 #pragma unroll
                 for (int u = 0; u < UP; ++u) {
                     const int q = base + u * blockDim.x;
                     if (q < np) {
-                        load_pair7<T, MIXED>(d, a, x, c0 + 2 * q, rw[u]);
+                        load_pair7<T, MIXED>(d, a, x, c0 + 2 * q, rw[u], &jr[u]);
                         sv[u] = ld2(s + c0 + 2 * q);
                     }
                 }
@@ -1024,6 +1104,8 @@ __global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
                     const int q = base + u * blockDim.x;
                     if (q < np) {
                         vec2_t<T> yv = dot_pair7<T, MIXED>(rw[u], d.do_k);
+                        if (jr[u] >= d.jmax2) yv.x = T(0);  // pad cells of the padded FP32 arrays
+                        if (jr[u] + 1 >= d.jmax2) yv.y = T(0);
                         if (defl) {
                             const float2 az = ld2(d.defl_az + c0 + 2 * q);
                             yv.x = yv.x + (T)(cs * (double)az.x);
@@ -1040,12 +1122,13 @@ __global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
         } else {
         for (int base = threadIdx.x; base < cnt; base += U * blockDim.x) {
             Row7<T> rw[U];
+            int jr[U];
             T sv[U];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
                 const int c = base + u * blockDim.x;
                 if (c < cnt) {
-                    load_row7<T, T, MIXED>(d, a, x, c0 + c, rw[u]);
+                    load_row7<T, T, MIXED>(d, a, x, c0 + c, rw[u], &jr[u]);
                     sv[u] = s[c0 + c];
                 }
             }
@@ -1054,6 +1137,7 @@ __global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
                 const int c = base + u * blockDim.x;
                 if (c < cnt) {
                     T yv = dot_row7<T, MIXED>(rw[u], d.do_k);
+                    if (jr[u] >= d.jmax2) yv = T(0);
                     if (defl) yv = yv + (T)(cs * (double)d.defl_az[c0 + c]);
                     y[c0 + c] = yv;
                     v[0] += (double)yv * (double)sv[u];
@@ -1142,6 +1226,19 @@ __device__ inline void fin_xr_inner(SysState &s, double rr, double rtr)
     }
 }
 
+// The mixed form accumulates x in the caller's VAR (natural layout) while its
+// FP32 vectors are padded: the cells of padded pair p (p even) in VAR.
+struct NatPair {
+    int64_t c;     // natural cell of the pair's first element
+    bool r0, r1;   // which of the two elements are cells (not pads)
+};
+__device__ __forceinline__ NatPair nat_pair(const SysDev &d, int64_t p)
+{
+    const uint32_t line = fdiv((uint32_t)p, d.div_jp);
+    const int j = (int)(p - (int64_t)line * d.jp);
+    return NatPair{(int64_t)line * d.jmax2 + j, j < d.jmax2, j + 1 < d.jmax2};
+}
+
 template <typename T, bool MIXED>
 __global__ void __launch_bounds__(256) k_xr_update(BatchView b, int ph_id, int sh_id)
 {
@@ -1159,12 +1256,30 @@ __global__ void __launch_bounds__(256) k_xr_update(BatchView b, int ph_id, int s
         SysState &st = b.st[tl.sys];
         if (!gate_ok(st, G_INNER)) continue;
         const int64_t c0 = (int64_t)tl.idx * TILE_CELLS;
-        const int cnt = (int)min((int64_t)TILE_CELLS, d.n - c0);
+        const int cnt = (int)min((int64_t)TILE_CELLS, cells<T>(d) - c0);
         // FP64 drop-in: X is VAR.  Mixed form: the solution is accumulated in FP64
-        // every iteration (x64 += alpha*Phat + omega*Shat with FP64 scalars).
+        // every iteration (x64 += alpha*Phat + omega*Shat with FP64 scalars), in
+        // VAR's own layout (nat_pair maps the padded pairs onto it).
         using X_T = typename std::conditional<MIXED, double, T>::type;
         X_T *__restrict__ x =
-            (MIXED ? reinterpret_cast<X_T *>(d.x64[0]) : reinterpret_cast<X_T *>(vec<T>(d, V_X))) + c0;
+            MIXED ? reinterpret_cast<X_T *>(d.x64[0]) : reinterpret_cast<X_T *>(vec<T>(d, V_X)) + c0;
+        auto xload = [&](int q) -> vec2_t<X_T> {
+            if constexpr (MIXED) {
+                const NatPair np2 = nat_pair(d, c0 + 2 * q);
+                return mk2<X_T>(np2.r0 ? x[np2.c] : X_T(0), np2.r1 ? x[np2.c + 1] : X_T(0));
+            } else {
+                return ld2(x + 2 * q);
+            }
+        };
+        auto xstore = [&](int q, const vec2_t<X_T> &v) {
+            if constexpr (MIXED) {
+                const NatPair np2 = nat_pair(d, c0 + 2 * q);
+                if (np2.r0) x[np2.c] = v.x;
+                if (np2.r1) x[np2.c + 1] = v.y;
+            } else {
+                st2(x + 2 * q, v);
+            }
+        };
         const X_T alpha = (X_T)st.alpha;
         const T *__restrict__ ph = vec<T>(d, ph_id) + c0;
         double v[2] = {0.0, 0.0};
@@ -1182,7 +1297,7 @@ __global__ void __launch_bounds__(256) k_xr_update(BatchView b, int ph_id, int s
                 for (int u = 0; u < U2; ++u) {
                     const int q = base + u * blockDim.x;
                     if (q < np) {
-                        xv[u] = ld2(x + 2 * q);
+                        xv[u] = xload(q);
                         pv[u] = ld2(ph + 2 * q);
                     }
                 }
@@ -1196,14 +1311,11 @@ __global__ void __launch_bounds__(256) k_xr_update(BatchView b, int ph_id, int s
                             if (zz.x) xn.x = xn.x + wz;
                             if (zz.y) xn.y = xn.y + wz;
                         }
-                        st2(x + 2 * q, xn);
+                        xstore(q, xn);
                     }
                 }
             }
-            if ((cnt & 1) && threadIdx.x == 0) {
-                x[cnt - 1] = x[cnt - 1] + alpha * (X_T)ph[cnt - 1];
-                if (defl && zr[cnt - 1]) x[cnt - 1] = x[cnt - 1] + wz;
-            }
+            if (!MIXED && (cnt & 1) && threadIdx.x == 0) x[cnt - 1] = x[cnt - 1] + alpha * (X_T)ph[cnt - 1];
         } else {
             const X_T omega = (X_T)st.omega;
             const X_T wz = defl ? (X_T)(st.alpha * st.defl_cp + st.omega * st.defl_cs) : X_T(0);
@@ -1220,7 +1332,7 @@ __global__ void __launch_bounds__(256) k_xr_update(BatchView b, int ph_id, int s
                 for (int u = 0; u < U2; ++u) {
                     const int q = base + u * blockDim.x;
                     if (q < np) {
-                        xv[u] = ld2(x + 2 * q);
+                        xv[u] = xload(q);
                         pv[u] = ld2(ph + 2 * q);
                         hv[u] = ld2(sh + 2 * q);
                         sv[u] = ld2(s + 2 * q);
@@ -1239,7 +1351,7 @@ __global__ void __launch_bounds__(256) k_xr_update(BatchView b, int ph_id, int s
                             if (zz.x) xn.x = xn.x + wz;
                             if (zz.y) xn.y = xn.y + wz;
                         }
-                        st2(x + 2 * q, xn);
+                        xstore(q, xn);
                         const T r0 = sv[u].x - omega_t * tw[u].x, r1 = sv[u].y - omega_t * tw[u].y;
                         st2(r + 2 * q, mk2<T>(r0, r1));
                         v[0] += (double)r0 * (double)r0;
@@ -1249,10 +1361,9 @@ __global__ void __launch_bounds__(256) k_xr_update(BatchView b, int ph_id, int s
                     }
                 }
             }
-            if ((cnt & 1) && threadIdx.x == 0) {
+            if (!MIXED && (cnt & 1) && threadIdx.x == 0) {
                 const int c = cnt - 1;
                 x[c] = x[c] + alpha * (X_T)ph[c] + omega * (X_T)sh[c];
-                if (defl && zr[c]) x[c] = x[c] + wz;
                 const T rv = s[c] - omega_t * tv[c];
                 r[c] = rv;
                 v[0] += (double)rv * (double)rv;
@@ -1370,7 +1481,7 @@ __global__ void __launch_bounds__(256) k_outer_step(BatchView b)
                 if (c < cnt) {
                     load_row7<double, double>(d, d.a64, x, c0 + c, rw[u]);
                     bv[u] = d.b64[c0 + c];
-                    rtv[u] = fresh ? 0.f : rt32[c0 + c];
+                    rtv[u] = fresh ? 0.f : rt32[padded(d, c0 + c)];
                 }
             }
 #pragma unroll
@@ -1379,9 +1490,10 @@ __global__ void __launch_bounds__(256) k_outer_step(BatchView b)
                 if (c < cnt) {
                     const double rv = bv[u] - dot_row7<double>(rw[u], d.do_k);
                     const float rf = (float)rv;
-                    r32[c0 + c] = rf;
+                    const int64_t pc = padded(d, c0 + c);  // the FP32 vectors are padded
+                    r32[pc] = rf;
                     const float rtf = fresh ? rf : rtv[u];
-                    if (fresh) rt32[c0 + c] = rf;
+                    if (fresh) rt32[pc] = rf;
                     v[0] += rv * rv;
                     v[1] += (double)rtf * (double)rf;
                 }
@@ -1517,20 +1629,22 @@ struct LineJob {
 };
 
 // The next work item at or after `item` whose system takes part in the wave.
-// pair: the two-row instance, which takes systems with an even JMAX2 only (the
-// one-row instance takes every system).  kind: which line kernel asks
-// (SysDev::line_kind: warp-staged or one lane per line); each takes
-// its own systems.  pf: the system of `item` when the caller has already
-// loaded it, else -1.
+// vw: rows per access of the asking instance, which takes systems whose line
+// pitch is a multiple of vw only (the one-row instance takes every system).
+// padded: the arrays are the mixed form's padded FP32 ones (pitch SysDev::jp).
+// kind: which line kernel asks (SysDev::line_kind: warp-staged or one lane per
+// line); each takes its own systems.  pf: the system of `item` when the caller
+// has already loaded it, else -1.
 __device__ __forceinline__ bool next_line_job(const BatchView &b, const WaveArgs &w, int item, int step, int total,
-                                              int lane, bool pair, int kind, LineJob &j, int pf = -1)
+                                              int lane, int vw, bool padded, int kind, LineJob &j, int pf = -1)
 {
     for (; item < total; item += step, pf = -1) {
         const int sidx = (w.kind == 0) ? (pf >= 0 ? pf : __ldg(b.line_sys + item)) : 0;
         if (!gate_ok(b.st[sidx], w.gate)) continue;
         const SysDev &d = b.sys[sidx];
         if (d.line_kind != kind) continue;
-        if (pair && (d.jmax2 & 1)) continue;
+        const int lp = padded ? d.jp : d.jmax2;
+        if (lp % vw) continue;
         j.item = item;
         j.sidx = sidx;
         j.G = d.lane_group;
@@ -1562,7 +1676,7 @@ __device__ __forceinline__ bool next_line_job(const BatchView &b, const WaveArgs
             j.i = lk.x;
             j.k = lk.y;
         }
-        j.base = (int64_t)(j.i - 1) * d.jmax2 + (int64_t)(j.k - 1) * d.jmax2 * d.imax2;
+        j.base = (int64_t)(j.i - 1) * lp + (int64_t)(j.k - 1) * lp * d.imax2;
         return true;
     }
     j.item = -1;
@@ -1575,11 +1689,11 @@ template <typename T>
 __device__ __forceinline__ LineCtx<T> line_ctx(const BatchView &b, const WaveArgs &w, const LineJob &j)
 {
     const SysDev &d = b.sys[j.sidx];
-    const int64_t c1 = d.jmax2, c2 = (int64_t)d.jmax2 * d.imax2;
+    const int64_t c1 = pitch<T>(d), c2 = (int64_t)pitch<T>(d) * d.imax2;
     LineCtx<T> x;
     x.a = diag_base<T>(d);
     x.rhs = vec<T>(d, w.rhs);
-    x.n = d.n;
+    x.n = cells<T>(d);
     x.L = j.L;
     x.do_k = d.do_k;
     x.base = j.base;
@@ -1627,14 +1741,15 @@ __global__ void k_line_factor(BatchView b, const int *all_line_prefix)
         if (!gate_ok(b.st[s], G_INIT)) continue;
         const SysDev &d = b.sys[s];
         const int li = g - all_line_prefix[s];  // (i-1) + (k-1)*imax2
-        const int k0 = (int)fdiv((uint32_t)li, d.div_i), i0 = li - k0 * d.imax2;
-        const int64_t base = (int64_t)i0 * d.jmax2 + (int64_t)k0 * d.jmax2 * d.imax2;
+        const int64_t base = (int64_t)li * d.jmax2;       // the line in the FP64 diagonals
+        const int64_t fbase = (int64_t)li * pitch<T>(d);  // and in the factor arrays
         const int64_t n = d.n;
         const int L = d.jmax2;
         const double *A = d.a64;
-        T *fl = reinterpret_cast<T *>(d.fac[0]) + base;
-        T *fr = reinterpret_cast<T *>(d.fac[1]) + base;
-        T *fq = reinterpret_cast<T *>(d.fac[2]) + base;
+        T *fl = reinterpret_cast<T *>(d.fac[0]) + fbase;
+        T *fr = reinterpret_cast<T *>(d.fac[1]) + fbase;
+        T *fq = reinterpret_cast<T *>(d.fac[2]) + fbase;
+        for (int r = L; r < pitch<T>(d); ++r) fl[r] = fr[r] = fq[r] = T(0);  // pad rows
         int flag = 0;
         double u = A[3 * n + base];
         fl[0] = T(0);
@@ -1678,8 +1793,22 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // from a zero start, which yields the chunk's affine map (value at its end as a
 // function of the value entering it), a warp scan that composes the maps, and a
 // second pass from the entering value.  No division remains in the sweep.
-template <typename T, bool PAIR>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView b, WaveArgs w, int cmax)
+// VW rows per access: a lane reads VW consecutive rows of each operand with one
+// load (16 bytes for VW = 4 in FP32 and VW = 2 in FP64), which needs lines that
+// start on VW-row boundaries (the mixed form's padded FP32 arrays, pitch a
+// multiple of four; an even JMAX2 for two rows).
+template <typename T, int VW>
+struct alignas(VW * sizeof(T)) RowsV {
+    T v[VW];
+};
+template <typename T, int VW>
+__device__ __forceinline__ RowsV<T, VW> ldv(const T *p)
+{
+    return *reinterpret_cast<const RowsV<T, VW> *>(p);
+}
+
+template <typename T, int VW>
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? (VW == 4 ? 5 : 6) : 4) k_jline(BatchView b, WaveArgs w, int cmax)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nwarps = blockDim.x >> 5;
@@ -1692,7 +1821,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
     const int step = gridDim.x * nwarps;
     LineJob j;
     int pf = -1;
-    for (int item = blockIdx.x * nwarps + warp; next_line_job(b, w, item, step, total, lane, PAIR, LK_WARP, j, pf);
+    for (int item = blockIdx.x * nwarps + warp; next_line_job(b, w, item, step, total, lane, VW, sizeof(T) == 4, LK_WARP, j, pf);
          item = j.item + step) {
         // the next item's system, loaded while this one is processed
         pf = (w.kind == 0 && j.item + step < total) ? __ldg(b.line_sys + j.item + step) : -1;
@@ -1713,58 +1842,48 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
         // even JMAX2 every line starts on an even cell, so lanes read two rows per
         // access; otherwise U single rows at a time.  The loads do not wait for the
         // line's pivot flag (a flagged line ignores them).
-        if constexpr (PAIR) {  // L is even
-            constexpr int U2 = 1;  // one row pair per lane and pass: FP32 fits 80 registers
-            using V2 = vec2_t<T>;
-            const int span = G * c;
+        if constexpr (VW > 1) {  // lines start on VW-row boundaries
+            using V = RowsV<T, VW>;
+            const int span = G * c;  // a multiple of VW (G >= VW)
             const T *rhs_l = x.rhs + x.base, *am1_l = x.a + 2 * x.n + x.base, *ap1_l = x.a + 4 * x.n + x.base;
             const T *am3_l = x.a + x.base, *ap3_l = x.a + 6 * x.n + x.base;
-            for (int r0 = 2 * gl; r0 < span; r0 += 2 * U2 * G) {
-                V2 rhs[U2], am1[U2], ap1[U2], am3[U2], ap3[U2], nim[U2], nip[U2], nkm[U2], nkp[U2];
-#pragma unroll
-                for (int u = 0; u < U2; ++u) {
-                    const int r = r0 + u * 2 * G;
-                    if (r < span) {  // factors straight to shared memory, zeros past the line (span is even: G > 1)
-                        const bool ok = j.valid && r < L;
-                        const void *z = d.fac[0];
-                        cp_async<2 * sizeof(T)>(fl + r, ok ? (const void *)(gl_ + r) : z, ok ? 2 * sizeof(T) : 0);
-                        cp_async<2 * sizeof(T)>(fr + r, ok ? (const void *)(gr_ + r) : z, ok ? 2 * sizeof(T) : 0);
-                        cp_async<2 * sizeof(T)>(fq + r, ok ? (const void *)(gq_ + r) : z, ok ? 2 * sizeof(T) : 0);
+            for (int r = VW * gl; r < span; r += VW * G) {
+                // factors straight to shared memory; rows past the line read the
+                // zeros of the pad cells or are zero-filled by the copy
+                const bool ok = j.valid && r < L;
+                const void *z = d.fac[0];
+                cp_async<VW * sizeof(T)>(fl + r, ok ? (const void *)(gl_ + r) : z, ok ? VW * sizeof(T) : 0);
+                cp_async<VW * sizeof(T)>(fr + r, ok ? (const void *)(gr_ + r) : z, ok ? VW * sizeof(T) : 0);
+                cp_async<VW * sizeof(T)>(fq + r, ok ? (const void *)(gq_ + r) : z, ok ? VW * sizeof(T) : 0);
+                V rhs, am1, ap1, am3, ap3, nim, nip, nkm, nkp;
+                if (ok) {  // rows r .. r+VW-1 lie on the line or on its pad cells
+                    rhs = ldv<T, VW>(rhs_l + r);
+                    am1 = ldv<T, VW>(am1_l + r);
+                    ap1 = ldv<T, VW>(ap1_l + r);
+                    nim = ldv<T, VW>(x.nb_im + r);
+                    nip = ldv<T, VW>(x.nb_ip + r);
+                    if (x.do_k) {
+                        am3 = ldv<T, VW>(am3_l + r);
+                        ap3 = ldv<T, VW>(ap3_l + r);
+                        nkm = ldv<T, VW>(x.nb_km + r);
+                        nkp = ldv<T, VW>(x.nb_kp + r);
                     }
-                    if (j.valid && r < L) {  // r even and L even: rows r and r+1 both on the line
-                        rhs[u] = ld2(rhs_l + r);
-                        am1[u] = ld2(am1_l + r);
-                        ap1[u] = ld2(ap1_l + r);
-                        nim[u] = ld2(x.nb_im + r);
-                        nip[u] = ld2(x.nb_ip + r);
+                }
+                V fv;
+#pragma unroll
+                for (int k = 0; k < VW; ++k) {
+                    T f0 = T(0);
+                    if (fast && r + k < L) {
+                        f0 = rhs.v[k] - am1.v[k] * nim.v[k];
+                        f0 = f0 - ap1.v[k] * nip.v[k];
                         if (x.do_k) {
-                            am3[u] = ld2(am3_l + r);
-                            ap3[u] = ld2(ap3_l + r);
-                            nkm[u] = ld2(x.nb_km + r);
-                            nkp[u] = ld2(x.nb_kp + r);
+                            f0 = f0 - am3.v[k] * nkm.v[k];
+                            f0 = f0 - ap3.v[k] * nkp.v[k];
                         }
                     }
+                    fv.v[k] = f0;
                 }
-#pragma unroll
-                for (int u = 0; u < U2; ++u) {
-                    const int r = r0 + u * 2 * G;
-                    if (r < span) {
-                        T f0 = T(0), f1 = T(0);
-                        if (fast && r < L) {
-                            f0 = rhs[u].x - am1[u].x * nim[u].x;
-                            f1 = rhs[u].y - am1[u].y * nim[u].y;
-                            f0 = f0 - ap1[u].x * nip[u].x;
-                            f1 = f1 - ap1[u].y * nip[u].y;
-                            if (x.do_k) {
-                                f0 = f0 - am3[u].x * nkm[u].x;
-                                f1 = f1 - am3[u].y * nkm[u].y;
-                                f0 = f0 - ap3[u].x * nkp[u].x;
-                                f1 = f1 - ap3[u].y * nkp[u].y;
-                            }
-                        }
-                        st2(f + r, mk2<T>(f0, f1));
-                    }
-                }
+                *reinterpret_cast<V *>(f + r) = fv;
             }
         } else {
             constexpr int U = 2;
@@ -1816,7 +1935,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
                 }
             }
         }
-        if constexpr (PAIR) cp_async_wait_all();
+        if constexpr (VW > 1) cp_async_wait_all();
         __syncwarp();
 
         // ---- forward recurrence y_r = f_r - l_r y_{r-1}
@@ -1894,7 +2013,10 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? 6 : 4) k_jline(BatchView
         if (j.valid) {
             T *dstp = vec<T>(d, w.dst) + x.base;
             const T *oldl = vec<T>(d, w.old) + x.base;
-            if (!skip) {
+            if (!skip && VW > 1) {  // VW rows per store; rows past the line are the zeros of its pad cells
+                for (int r = VW * gl; r < L; r += VW * G)
+                    *reinterpret_cast<RowsV<T, VW> *>(dstp + r) = *reinterpret_cast<const RowsV<T, VW> *>(f + r);
+            } else if (!skip) {
                 for (int r = gl; r < L; r += G) dstp[r] = f[r];
             } else if (w.write_old) {
                 for (int r = gl; r < L; r += G) dstp[r] = oldl[r];
@@ -1921,7 +2043,7 @@ __global__ void __launch_bounds__(128) k_jline_thread(BatchView b, WaveArgs w)
     const int total = (w.kind == 0) ? b.line_prefix[b.nsys] : w.count;
     const int step = gridDim.x * nwarps;
     LineJob j;
-    for (int item = blockIdx.x * nwarps + warp; next_line_job(b, w, item, step, total, lane, false, LK_THREAD, j);
+    for (int item = blockIdx.x * nwarps + warp; next_line_job(b, w, item, step, total, lane, 1, sizeof(T) == 4, LK_THREAD, j);
          item = j.item + step) {
         const SysDev &d = b.sys[j.sidx];
         SysState &st = b.st[j.sidx];
@@ -1996,7 +2118,7 @@ __global__ void k_seq_lines(BatchView b, SeqLineArgs a)
     SysState &st = b.st[0];
     if (!gate_ok(st, a.gate)) return;
     const SysDev &d = b.sys[0];
-    const int64_t n = d.n, c1 = d.jmax2, c2 = (int64_t)d.jmax2 * d.imax2;
+    const int64_t n = cells<T>(d), c1 = pitch<T>(d), c2 = (int64_t)pitch<T>(d) * d.imax2;
     const T *A = diag_base<T>(d);
     const T *rhs = vec<T>(d, a.rhs);
     T *var = vec<T>(d, a.var);
@@ -2029,7 +2151,7 @@ __global__ void k_seq_lines(BatchView b, SeqLineArgs a)
         const int64_t p = base + r * step;
         int ii, jj, kk;
         {
-            const CellIdx q = cell_ijk(d, (uint32_t)p);
+            const CellIdx q = cell_ijk_t<T>(d, (uint32_t)p);
             ii = q.i; jj = q.j; kk = q.k;
         }
         auto nb = [&](int dd) -> T {
@@ -2572,22 +2694,26 @@ int prepare_line_kernel(int cmax, int *warps)
     // process (some on other threads): it only ever grows
     static std::mutex mu;
     static int granted = 0;
+    constexpr int VMAX = sizeof(T) == 4 ? 4 : 2;  // widest instance
     {
         std::lock_guard<std::mutex> lk(mu);
         if (smem > granted) {
-            if (cudaFuncSetAttribute(k_jline<T, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+            if (cudaFuncSetAttribute(k_jline<T, VMAX>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
                     cudaSuccess ||
-                cudaFuncSetAttribute(k_jline<T, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+                cudaFuncSetAttribute(k_jline<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+                    cudaSuccess ||
+                cudaFuncSetAttribute(k_jline<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
                     cudaSuccess)
                 return 0;
             granted = smem;
         }
     }
-    int nb = 0, nb1 = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_jline<T, true>, wpb * 32, smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb1, k_jline<T, false>, wpb * 32, smem) != cudaSuccess)
+    int nb = 0, nb1 = 0, nb2 = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_jline<T, VMAX>, wpb * 32, smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, k_jline<T, 2>, wpb * 32, smem) != cudaSuccess ||
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb1, k_jline<T, 1>, wpb * 32, smem) != cudaSuccess)
         return 0;
-    return std::min(nb, nb1);
+    return std::min(nb, std::min(nb1, nb2));
 }
 
 template <typename T>
@@ -2642,10 +2768,13 @@ cudaError_t launch_jline(const BatchView &b, const LaunchCfg &c, const WaveArgs 
     if (c.line_thread) k_jline_thread<T><<<c.line_grid_thread, 128, 0, c.stream>>>(b, w);
     if (c.line_warp) {
         const int smem = c.line_warps * kernel_smem_line_bytes(c.line_cmax, (int)sizeof(T));
-        if (c.line_single)
-            k_jline<T, false><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax);
+        constexpr int VMAX = sizeof(T) == 4 ? 4 : 2;
+        if (c.line_single || c.line_vw == 1)
+            k_jline<T, 1><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax);
+        else if (c.line_vw >= VMAX)
+            k_jline<T, VMAX><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax);
         else
-            k_jline<T, true><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax);
+            k_jline<T, 2><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax);
     }
     CHECK_LAUNCH();
 }

@@ -29,7 +29,8 @@ struct LaunchCfg {
     int line_grid_thread;  // blocks of the one-lane-per-line kernel (4 warps each)
     int line_thread;       // 1: some system has one lane per line
     int line_warp;         // 1: some system has several lanes per line
-    int line_single;       // 1: some system with several lanes per line has an odd line length
+    int line_single;       // 1: some system with several lanes per line has an odd line pitch
+    int line_vw;           // rows per access of the warp J-line kernel (1, 2 or 4)
     cudaStream_t stream;
 };
 

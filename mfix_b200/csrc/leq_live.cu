@@ -28,7 +28,9 @@ static SysDev idle_sys()
     d.imax2 = d.jmax2 = d.kmax2 = 1;
     d.do_k = 1;
     d.n = 0;
-    d.div_j = d.div_i = d.div_h = make_fastdiv(1);
+    d.jp = 1;
+    d.np = 0;
+    d.div_j = d.div_i = d.div_h = d.div_jp = make_fastdiv(1);
     d.pc = PC_NONE;
     d.lane_group = 32;
     d.line_kind = LK_WARP;
@@ -148,8 +150,11 @@ int Engine::live_add(const LiveSystem &ls)
     d.n = sp.n;
     d.div_j = make_fastdiv((uint32_t)sp.jmax2);
     d.div_i = make_fastdiv((uint32_t)sp.imax2);
+    d.jp = form_pitch(sp.jmax2, prec);
+    d.np = (int64_t)d.jp * sp.imax2 * sp.kmax2;
+    d.div_jp = make_fastdiv((uint32_t)d.jp);
     d.pc = live_opt_.pc;
-    d.ntiles = (int)((sp.n + TILE_CELLS - 1) / TILE_CELLS);
+    d.ntiles = (int)((std::max(sp.n, d.np) + TILE_CELLS - 1) / TILE_CELLS);
     shape_for(sp.jmax2, mixed ? 4 : 8, live_opt_.force_lanes, &d.lane_group, &d.rows_per_lane, &d.line_kind);
     d.half_lines = (sp.imax2 + 1) / 2;
     d.div_h = make_fastdiv((uint32_t)d.half_lines);
