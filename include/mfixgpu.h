@@ -203,6 +203,54 @@ int mfixgpu_dot_product_par(const double *r1_dev, const double *r2_dev, int64_t 
 int mfixgpu_dot_product_par_noalloc(const double *r1_dev, const double *r2_dev, int64_t n, double *out_dev,
                                     void *stream);
 
+/* ---------------------------------------------------------------- pressure correction on the device */
+
+/* The fields SOLVE_PP_G assembles the gas pressure-correction system from
+ * (CONV_PP_G, model/conv_pp_g.f:33-182; SOURCE_PP_G, model/source_pp_g.f:18-214),
+ * in MFIX's own layouts: cell arrays of DIMENSION_3; D_E/D_N/D_T(DIMENSION_3,
+ * 0:DIMENSION_M) with phase m at m*DIMENSION_3; the solids arrays (DIMENSION_3,
+ * DIMENSION_M) with phase m at (m-1)*DIMENSION_3.  Served: an incompressible run
+ * (RO_G0 defined, so COMPRESSIBLE_PP_G is not called) on a Cartesian grid without
+ * cut cells, shear, point sources or user sources.  With on_device set every
+ * array pointer except close_packed is device memory; otherwise host memory,
+ * copied in. */
+typedef struct {
+    const int *flag;                          /* FLAG: 1 fluid, 10/11 pressure inflow/outflow */
+    const double *rop_ge, *rop_gn, *rop_gt;   /* gas face densities (CONV_ROP_G) */
+    const double *ayz, *axz, *axy;            /* face areas */
+    const double *u_g, *v_g, *w_g;            /* gas velocities */
+    const double *rop_g, *rop_go, *vol, *sum_r_g;
+    const double *d_e, *d_n, *d_t;            /* pressure-correction coefficients, phases 0..MMAX */
+    int mmax;                                 /* solids phases */
+    int ro_g0_defined;                        /* 1: incompressible gas (RO_G0 defined); 0 is not served */
+    const int *close_packed;                  /* CLOSE_PACKED(1:MMAX), nonzero = .TRUE. (host memory) */
+    const double *rop_se, *rop_sn, *rop_st;   /* solids face densities, phases 1..MMAX */
+    const double *u_s, *v_s, *w_s, *rop_s, *rop_so, *sum_r_s;
+    double odt;                               /* ODT = 1/DT */
+    long long ijk_p_g;                        /* IJK_P_G (1-based), <= 0 when undefined */
+    int on_device;
+    int pad;
+} mfixgpu_pp_fields;
+
+/* CONV_PP_G followed by SOURCE_PP_G on the device: A_M(:,:,0) (7*DIMENSION_3),
+ * B_M(:,0) and B_MMAX(:,0), the largest term of each cell's continuity residual
+ * (zero outside the fluid), written to the given arrays (host memory unless
+ * on_device).  Bit for bit the reference's arithmetic without fused
+ * multiply-adds.  Returns 0, MFIXGPU_ERR_NOGEOM, MFIXGPU_ERR_ARGS,
+ * MFIXGPU_ERR_UNSUPPORTED (a compressible run) or MFIXGPU_ERR_CUDA. */
+int mfixgpu_conv_source_pp_g(const mfixgpu_pp_fields *f, double *a_m, double *b_m, double *b_mmax);
+
+/* SOLVE_PP_G(NORMG, RESG, IER) (model/solve_pp_g.f:10-118) with the LEQ settings
+ * of equation 1 passed in (LEQ_IT(1), LEQ_METHOD(1), LEQ_SWEEP(1), LEQ_TOL(1),
+ * LEQ_PC(1)), gfortran convention: PP_G = 0, the system assembled on the
+ * device, RESG from CALC_RESID_PP (normalized by RESID(B_MMAX)/10 when NORMG
+ * = 0, model/solve_pp_g.f:94-104), then SOLVE_LIN_EQ('Pp_g', 1, PP_G, A_M, B_M, 0,
+ * ...).  Only the fields and PP_G cross the host link (none when on_device);
+ * A_M and B_M exist on the device only. */
+void mfixgpu_solve_pp_g_(const mfixgpu_pp_fields *f, const double *normg, double *pp_g, double *resg,
+                         const int *itmax, const int *method, const char *sweep, const double *tol, const char *pc,
+                         int *ier, size_t sweep_len, size_t pc_len);
+
 /* ---------------------------------------------------------------- batches */
 
 typedef struct {

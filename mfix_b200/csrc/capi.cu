@@ -62,9 +62,152 @@ struct Global {
         Geometry geom;
     };
     std::vector<Deferred> deferred;
+    DeviceArena pp;  // device copies of the pressure-correction fields and the assembled system
 };
 
 int flush_locked(Global &g);
+
+// ---- the gas pressure-correction system on the device (pp_assembly.cu)
+// The fields' device copies (or the caller's device pointers) and the system's
+// device arrays, from the arena g.pp.  Returns 0 or an error code (g.err set).
+struct PPDevice {
+    PPFields f{};
+    double *a = nullptr, *b = nullptr, *bmmax = nullptr, *x = nullptr, *part = nullptr;
+    int grid = 0;
+};
+
+int pp_prepare(Global &g, Engine *e, const mfixgpu_pp_fields *hf, PPDevice &dv)
+{
+    if (!g.geom.set) {
+        g.err = "mfixgpu_init_geometry has not been called";
+        return MFIXGPU_ERR_NOGEOM;
+    }
+    if (!hf) {
+        g.err = "null field record";
+        return MFIXGPU_ERR_ARGS;
+    }
+    if (!hf->ro_g0_defined) {
+        g.err = "a compressible run (RO_G0 undefined, COMPRESSIBLE_PP_G) is not served by the device assembly";
+        return MFIXGPU_ERR_UNSUPPORTED;
+    }
+    const int mmax = hf->mmax;
+    if (mmax < 0 || mmax > g.geom.dimension_m || (mmax > 0 && !hf->close_packed)) {
+        g.err = "MMAX outside 0:DIMENSION_M, or CLOSE_PACKED missing";
+        return MFIXGPU_ERR_ARGS;
+    }
+    const bool do_k = g.geom.do_k != 0;
+    bool solids = false;
+    for (int m = 0; m < mmax; ++m) solids = solids || !hf->close_packed[m];
+    const void *need[] = {hf->flag, hf->rop_ge, hf->rop_gn, hf->ayz, hf->axz, hf->u_g, hf->v_g, hf->rop_g,
+                          hf->rop_go, hf->vol, hf->sum_r_g, hf->d_e, hf->d_n};
+    for (const void *q : need)
+        if (!q) {
+            g.err = "null field array";
+            return MFIXGPU_ERR_ARGS;
+        }
+    if (do_k && (!hf->rop_gt || !hf->axy || !hf->w_g || !hf->d_t)) {
+        g.err = "null K-direction field array of a 3-D run";
+        return MFIXGPU_ERR_ARGS;
+    }
+    if (solids && (!hf->rop_se || !hf->rop_sn || !hf->u_s || !hf->v_s || !hf->rop_s || !hf->rop_so ||
+                   !hf->sum_r_s || (do_k && (!hf->rop_st || !hf->w_s)))) {
+        g.err = "null solids field array";
+        return MFIXGPU_ERR_ARGS;
+    }
+    const size_t n = (size_t)g.geom.n;
+    const size_t cell = n * 8, dph = (size_t)(mmax + 1) * n * 8, sph = (size_t)mmax * n * 8;
+    size_t bytes = 10 * cell + 3 * 256 + 4096 + 64 * 16;  // A (7n), B, B_MMAX, PP_G + partials
+    if (!hf->on_device) bytes += n * 4 + 13 * cell + 3 * dph + 9 * sph + 64 * 256;
+    bytes += (size_t)(mmax + 1) * 4 + 256;
+    cudaError_t ce = g.pp.reserve(bytes);
+    if (ce != cudaSuccess) {
+        g.err = std::string("device memory for the pressure-correction system: ") + cudaGetErrorString(ce);
+        return MFIXGPU_ERR_NOMEM;
+    }
+    g.pp.reset();
+    cudaStream_t s = e->stream();
+    auto put = [&](const void *src, size_t nbytes) -> const void * {
+        if (!src) return nullptr;
+        if (hf->on_device) return src;
+        void *d = g.pp.take(nbytes);
+        if (!d || cudaMemcpyAsync(d, src, nbytes, cudaMemcpyHostToDevice, s) != cudaSuccess) return nullptr;
+        return d;
+    };
+    PPFields &f = dv.f;
+    f.flag = (const int *)put(hf->flag, n * 4);
+    f.rop_ge = (const double *)put(hf->rop_ge, cell);
+    f.rop_gn = (const double *)put(hf->rop_gn, cell);
+    f.rop_gt = (const double *)put(do_k ? hf->rop_gt : nullptr, cell);
+    f.ayz = (const double *)put(hf->ayz, cell);
+    f.axz = (const double *)put(hf->axz, cell);
+    f.axy = (const double *)put(do_k ? hf->axy : nullptr, cell);
+    f.u_g = (const double *)put(hf->u_g, cell);
+    f.v_g = (const double *)put(hf->v_g, cell);
+    f.w_g = (const double *)put(do_k ? hf->w_g : nullptr, cell);
+    f.rop_g = (const double *)put(hf->rop_g, cell);
+    f.rop_go = (const double *)put(hf->rop_go, cell);
+    f.vol = (const double *)put(hf->vol, cell);
+    f.sum_r_g = (const double *)put(hf->sum_r_g, cell);
+    f.d_e = (const double *)put(hf->d_e, dph);
+    f.d_n = (const double *)put(hf->d_n, dph);
+    f.d_t = (const double *)put(do_k ? hf->d_t : nullptr, dph);
+    f.mmax = mmax;
+    if (solids) {
+        f.rop_se = (const double *)put(hf->rop_se, sph);
+        f.rop_sn = (const double *)put(hf->rop_sn, sph);
+        f.rop_st = (const double *)put(do_k ? hf->rop_st : nullptr, sph);
+        f.u_s = (const double *)put(hf->u_s, sph);
+        f.v_s = (const double *)put(hf->v_s, sph);
+        f.w_s = (const double *)put(do_k ? hf->w_s : nullptr, sph);
+        f.rop_s = (const double *)put(hf->rop_s, sph);
+        f.rop_so = (const double *)put(hf->rop_so, sph);
+        f.sum_r_s = (const double *)put(hf->sum_r_s, sph);
+    }
+    // CLOSE_PACKED is host memory in every case; a close-packed phase is skipped
+    std::vector<int> cp(mmax + 1, 1);
+    for (int m = 0; m < mmax; ++m) cp[m] = hf->close_packed[m] ? 1 : 0;
+    int *cpd = (int *)g.pp.take(cp.size() * 4);
+    if (!cpd || cudaMemcpyAsync(cpd, cp.data(), cp.size() * 4, cudaMemcpyHostToDevice, s) != cudaSuccess) {
+        g.err = "copy of CLOSE_PACKED";
+        return MFIXGPU_ERR_CUDA;
+    }
+    // pageable host sources: the copies must have read them before the call returns
+    if (cudaStreamSynchronize(s) != cudaSuccess) {
+        g.err = std::string("copy of the fields: ") + cudaGetErrorString(cudaGetLastError());
+        return MFIXGPU_ERR_CUDA;
+    }
+    f.close_packed = cpd;
+    f.odt = hf->odt;
+    f.ijk_p_g = hf->ijk_p_g;
+    if (!f.flag || !f.rop_ge || !f.rop_gn || !f.ayz || !f.axz || !f.u_g || !f.v_g || !f.rop_g || !f.rop_go ||
+        !f.vol || !f.sum_r_g || !f.d_e || !f.d_n) {
+        g.err = "copy of the fields to the device";
+        return MFIXGPU_ERR_CUDA;
+    }
+    dv.a = (double *)g.pp.take(7 * cell);
+    dv.b = (double *)g.pp.take(cell);
+    dv.bmmax = (double *)g.pp.take(cell);
+    dv.x = (double *)g.pp.take(cell);
+    dv.grid = std::max(1, std::min((int)((n + 255) / 256), 64 * 16));
+    dv.part = (double *)g.pp.take((size_t)dv.grid * 2 * 8);
+    if (!dv.a || !dv.b || !dv.bmmax || !dv.x || !dv.part) {
+        g.err = "internal: pressure-correction arena too small";
+        return MFIXGPU_ERR_CUDA;
+    }
+    return 0;
+}
+
+int pp_assemble(Global &g, Engine *e, PPDevice &dv)
+{
+    PPGeom pg{g.geom.imax2, g.geom.jmax2, g.geom.kmax2, g.geom.do_k, g.geom.n};
+    const int grid = std::max(1, std::min((int)((g.geom.n + 255) / 256), e->sm_count() * 8));
+    cudaError_t ce = launch_conv_source_pp(dv.f, pg, dv.a, dv.b, dv.bmmax, grid, e->stream());
+    if (ce != cudaSuccess) {
+        g.err = std::string("pressure-correction assembly: ") + cudaGetErrorString(ce);
+        return MFIXGPU_ERR_CUDA;
+    }
+    return 0;
+}
 
 Global &G()
 {
@@ -571,7 +714,141 @@ void mfixgpu_finalize(void)
     std::lock_guard<std::mutex> lk(g.mu);
     // calls still queued are dropped unsolved: their IER keeps MFIXGPU_ERR_INCOMPLETE
     g.deferred.clear();
+    g.pp.release();
     g.engine.reset();
+}
+
+int mfixgpu_conv_source_pp_g(const mfixgpu_pp_fields *f, double *a_m, double *b_m, double *b_mmax)
+{
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    if (!f || !a_m || !b_m || !b_mmax) return MFIXGPU_ERR_ARGS;
+    Engine *e = engine_locked(g);
+    if (!e) return MFIXGPU_ERR_CUDA;
+    PPDevice dv;
+    int rc = pp_prepare(g, e, f, dv);
+    if (rc) return rc;
+    if (f->on_device) {  // assembled straight into the caller's device arrays
+        dv.a = a_m;
+        dv.b = b_m;
+        dv.bmmax = b_mmax;
+    }
+    if ((rc = pp_assemble(g, e, dv))) return rc;
+    const size_t cell = (size_t)g.geom.n * 8;
+    cudaStream_t s = e->stream();
+    cudaError_t ce = cudaSuccess;
+    if (!f->on_device) {
+        ce = cudaMemcpyAsync(a_m, dv.a, 7 * cell, cudaMemcpyDeviceToHost, s);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(b_m, dv.b, cell, cudaMemcpyDeviceToHost, s);
+        if (ce == cudaSuccess) ce = cudaMemcpyAsync(b_mmax, dv.bmmax, cell, cudaMemcpyDeviceToHost, s);
+    }
+    if (ce == cudaSuccess) ce = cudaStreamSynchronize(s);
+    if (ce != cudaSuccess) {
+        g.err = std::string("pressure-correction assembly: ") + cudaGetErrorString(ce);
+        return MFIXGPU_ERR_CUDA;
+    }
+    return 0;
+}
+
+void mfixgpu_solve_pp_g_(const mfixgpu_pp_fields *f, const double *normg, double *pp_g, double *resg,
+                         const int *itmax, const int *method, const char *sweep, const double *tol, const char *pc,
+                         int *ier, size_t sweep_len, size_t pc_len)
+{
+    if (!ier) return;
+    if (!normg || !pp_g || !resg || !itmax || !method || !tol || !f) {
+        *ier = MFIXGPU_ERR_ARGS;
+        return;
+    }
+    Global &g = G();
+    std::unique_lock<std::mutex> lk(g.mu);
+    const double t0 = now_s();
+    g.last = mfixgpu_stats{};
+    Engine *e = engine_locked(g);
+    if (!e) {
+        *ier = MFIXGPU_ERR_CUDA;
+        return;
+    }
+    if (*method < 1 || *method > 5) {
+        g.err = "LEQ_METHOD " + std::to_string(*method) + " is not served by the GPU path (1-5)";
+        *ier = MFIXGPU_ERR_UNSUPPORTED;
+        return;
+    }
+    char s4[4], p4[4];
+    fortran_char4(sweep, sweep_len, s4);
+    fortran_char4(pc, pc_len, p4);
+    const int pcode = (*method == 1 || *method == 3) ? PC_LINE : decode_pc(p4);
+    if (pcode < 0) {
+        g.err = "preconditioner option not found";
+        *ier = MFIXGPU_ERR_UNSUPPORTED;
+        return;
+    }
+    PPDevice dv;
+    int rc = pp_prepare(g, e, f, dv);
+    if (!rc) rc = pp_assemble(g, e, dv);
+    cudaStream_t s = e->stream();
+    const int64_t n = g.geom.n;
+    // PP_G(:) = ZERO (model/solve_pp_g.f:71)
+    if (!rc && cudaMemsetAsync(dv.x, 0, (size_t)n * 8, s) != cudaSuccess) rc = MFIXGPU_ERR_CUDA;
+    // NORMG = 0: normalization from the dominant terms (:94-101), then RESG (:102-104)
+    double norm = *normg, r = 0.0;
+    if (!rc && norm == 0.0) {
+        if (resid_pp(dv.f.flag, dv.bmmax, n, 1.0, dv.part, dv.grid, s, &r) != cudaSuccess) rc = MFIXGPU_ERR_CUDA;
+        norm = r / 10.0;  // DEN = 1.0D1
+    }
+    if (!rc && resid_pp(dv.f.flag, dv.b, n, norm, dv.part, dv.grid, s, resg) != cudaSuccess) rc = MFIXGPU_ERR_CUDA;
+    if (rc) {
+        if (rc == MFIXGPU_ERR_CUDA && g.err.empty()) g.err = "pressure-correction residual";
+        *ier = rc;
+        return;
+    }
+    // SOLVE_LIN_EQ('Pp_g', 1, PP_G, A_M, B_M, 0, LEQI, LEQM, ...) (:113-114) on the device arrays
+    SystemSpec sp;
+    sp.imax2 = g.geom.imax2;
+    sp.jmax2 = g.geom.jmax2;
+    sp.kmax2 = g.geom.kmax2;
+    sp.do_k = g.geom.do_k;
+    sp.n = n;
+    sp.a = dv.a;
+    sp.b = dv.b;
+    sp.x = dv.x;
+    sp.tol = *tol;
+    sp.itmax = *itmax;
+    SolveOptions so = make_opts(g.opt, pcode, s4);
+    so.method = *method;
+    so.on_device = true;
+    std::vector<SolveResult> out;
+    rc = e->solve({sp}, so, out);
+    if (rc) {
+        g.err = e->last_error();
+        *ier = rc;
+        return;
+    }
+    if (cudaMemcpyAsync(pp_g, dv.x, (size_t)n * 8, cudaMemcpyDeviceToHost, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        g.err = "copy of PP_G";
+        *ier = MFIXGPU_ERR_CUDA;
+        return;
+    }
+    const SolveResult &res = out[0];
+    const int code = *method == 1 ? *ier : res.ier;
+    if (*method == 1)
+        g.iter_tot[0] = res.iter_tot_add;
+    else
+        g.iter_tot[0] += res.iter_tot_add;  // ITER_TOT(1), VNO = 1 for 'Pp_g'
+    g.last.iterations = res.iterations;
+    g.last.iter_tot_add = res.iter_tot_add;
+    g.last.exit_kind = res.exit_kind;
+    g.last.outer_steps = res.outer_steps;
+    g.last.rnorm0 = res.rnorm0;
+    g.last.rnorm = res.rnorm;
+    g.last.fp64_fallback = res.fp64_fallback;
+    g.last.mixed_iterations = res.mixed_iterations;
+    g.last.deflated = res.deflated;
+    g.last.device_ms = e->timing().device_ms;
+    g.last.kernel_launches = e->timing().kernel_launches;
+    g.last.ier = code;
+    g.last.seconds = now_s() - t0;
+    *ier = code;
 }
 
 int mfixgpu_leq_matvec(const mfixgpu_geom *gm, const double *a_dev, const double *var_dev, double *avar_dev)

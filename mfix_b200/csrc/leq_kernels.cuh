@@ -123,4 +123,30 @@ struct CellOcc {
 };
 void cell_occupancy(bool fp32, CellOcc *o);
 
+// ---- the gas pressure-correction system assembled on the device
+// (CONV_PP_G + SOURCE_PP_G, pp_assembly.cu); every pointer is device memory in
+// the reference's layouts: cell arrays of DIMENSION_3, D_E(DIMENSION_3, 0:MMAX),
+// ROP_SE etc. (DIMENSION_3, 1:MMAX) with phase m at m*n and (m-1)*n.
+struct PPFields {
+    const int *flag;  // FLAG: 1 fluid (FLUID_AT), 10/11 pressure inflow/outflow (P_FLOW_AT)
+    const double *rop_ge, *rop_gn, *rop_gt, *ayz, *axz, *axy, *u_g, *v_g, *w_g;
+    const double *rop_g, *rop_go, *vol, *sum_r_g, *d_e, *d_n, *d_t;
+    int mmax;
+    const int *close_packed;  // device copy of CLOSE_PACKED(1:MMAX)
+    const double *rop_se, *rop_sn, *rop_st, *u_s, *v_s, *w_s, *rop_s, *rop_so, *sum_r_s;
+    double odt;
+    long long ijk_p_g;  // 1-based, <= 0: undefined
+};
+struct PPGeom {
+    int imax2, jmax2, kmax2, do_k;
+    int64_t n;
+};
+// A_M(:,:,0) (7n), B_M(:,0), B_MMAX(:,0) on the device
+cudaError_t launch_conv_source_pp(const PPFields &f, const PPGeom &g, double *a, double *b, double *bmmax, int grid,
+                                  cudaStream_t s);
+// CALC_RESID_PP's RESID of v over the fluid cells with normalization norm
+// (blocks' partial sums in part_dev, 2 * grid doubles); synchronizes the stream.
+cudaError_t resid_pp(const int *flag, const double *v, int64_t n, double norm, double *part_dev, int grid,
+                     cudaStream_t s, double *resid);
+
 }  // namespace mfixgpu

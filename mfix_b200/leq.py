@@ -71,6 +71,65 @@ class ServerCountersC(C.Structure):
                 ("budget_bytes", C.c_double), ("seconds", C.c_double), ("busy_ms", C.c_double * 2)]
 
 
+class PPFieldsC(C.Structure):
+    """mfixgpu_pp_fields: the fields SOLVE_PP_G assembles the pressure correction from."""
+    _fields_ = [("flag", C.c_void_p), ("rop_ge", C.c_void_p), ("rop_gn", C.c_void_p), ("rop_gt", C.c_void_p),
+                ("ayz", C.c_void_p), ("axz", C.c_void_p), ("axy", C.c_void_p), ("u_g", C.c_void_p),
+                ("v_g", C.c_void_p), ("w_g", C.c_void_p), ("rop_g", C.c_void_p), ("rop_go", C.c_void_p),
+                ("vol", C.c_void_p), ("sum_r_g", C.c_void_p), ("d_e", C.c_void_p), ("d_n", C.c_void_p),
+                ("d_t", C.c_void_p), ("mmax", C.c_int), ("ro_g0_defined", C.c_int), ("close_packed", C.c_void_p),
+                ("rop_se", C.c_void_p), ("rop_sn", C.c_void_p), ("rop_st", C.c_void_p), ("u_s", C.c_void_p),
+                ("v_s", C.c_void_p), ("w_s", C.c_void_p), ("rop_s", C.c_void_p), ("rop_so", C.c_void_p),
+                ("sum_r_s", C.c_void_p), ("odt", C.c_double), ("ijk_p_g", C.c_longlong), ("on_device", C.c_int),
+                ("pad", C.c_int)]
+
+
+PP_ARRAYS = ("flag", "rop_ge", "rop_gn", "rop_gt", "ayz", "axz", "axy", "u_g", "v_g", "w_g", "rop_g", "rop_go", "vol",
+             "sum_r_g", "d_e", "d_n", "d_t", "rop_se", "rop_sn", "rop_st", "u_s", "v_s", "w_s", "rop_s", "rop_so",
+             "sum_r_s")
+
+
+def pp_struct(f, device_ptrs: dict | None = None) -> PPFieldsC:
+    """The C record of a :class:`mfix_b200.systems.PPFields` (host arrays), or of
+    device pointers given by name in device_ptrs (on_device set)."""
+    c = PPFieldsC()
+    for name in PP_ARRAYS:
+        if device_ptrs is not None:
+            setattr(c, name, device_ptrs.get(name) or None)
+        else:
+            arr = getattr(f, name)
+            setattr(c, name, arr.ctypes.data if arr is not None else None)
+    c.mmax = f.mmax
+    c.ro_g0_defined = 1
+    c.close_packed = f.close_packed.ctypes.data if f.mmax > 0 else None
+    c.odt = f.odt
+    c.ijk_p_g = f.ijk_p_g
+    c.on_device = 1 if device_ptrs is not None else 0
+    return c
+
+
+def conv_source_pp_g(f, a_m, b_m, b_mmax, device_ptrs: dict | None = None) -> int:
+    """mfixgpu_conv_source_pp_g: A_M(:,:,0), B_M(:,0), B_MMAX(:,0) assembled on the device
+    (numpy arrays, or device addresses with device_ptrs)."""
+    c = pp_struct(f, device_ptrs)
+    if device_ptrs is not None:
+        return lib().mfixgpu_conv_source_pp_g(C.byref(c), a_m, b_m, b_mmax)
+    return lib().mfixgpu_conv_source_pp_g(C.byref(c), _ptr(a_m), _ptr(b_m), _ptr(b_mmax))
+
+
+def solve_pp_g(f, normg: float, pp_g: np.ndarray, itmax: int = 500, method: int = 2, sweep: str = "RSRS",
+               tol: float = 1e-8, pc: str = "LINE") -> tuple[int, float]:
+    """SOLVE_PP_G(NORMG, RESG, IER) through mfixgpu_solve_pp_g_ with equation 1's LEQ settings:
+    returns (IER, RESG); PP_G is written in place."""
+    c = pp_struct(f)
+    ier = C.c_int(0)
+    resg = C.c_double(0.0)
+    lib().mfixgpu_solve_pp_g_(C.byref(c), C.byref(C.c_double(normg)), _ptr(pp_g), C.byref(resg),
+                              C.byref(C.c_int(itmax)), C.byref(C.c_int(method)), sweep.encode(),
+                              C.byref(C.c_double(tol)), pc.encode(), C.byref(ier), len(sweep), len(pc))
+    return ier.value, resg.value
+
+
 REQ_ZERO_GUESS = 1
 REQ_WRITE_AB = 2
 REQ_ON_DEVICE = 4
@@ -133,6 +192,11 @@ def _declare(L: C.CDLL) -> None:
     L.mfixgpu_batch_solve.restype = C.c_int
     L.mfixgpu_dot_product_par_noalloc.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
     L.mfixgpu_dot_product_par_noalloc.restype = C.c_int
+    L.mfixgpu_conv_source_pp_g.argtypes = [C.POINTER(PPFieldsC), C.c_void_p, C.c_void_p, C.c_void_p]
+    L.mfixgpu_conv_source_pp_g.restype = C.c_int
+    L.mfixgpu_solve_pp_g_.argtypes = [C.POINTER(PPFieldsC), _dp, C.c_void_p, _dp, _ip, _ip, C.c_char_p, _dp,
+                                      C.c_char_p, _ip, C.c_size_t, C.c_size_t]
+    L.mfixgpu_solve_pp_g_.restype = None
     L.mfixgpu_autotune_cache.argtypes = [C.c_char_p]
     L.mfixgpu_autotune_cache.restype = C.c_int
     L.mfixgpu_autotune_table.argtypes = [C.POINTER(C.c_int), C.c_int]

@@ -313,3 +313,103 @@ def make_request_system(kind: str, dims, tol: float, seed: int) -> System:
     if kind == "pressure_like":
         return pressure_scaled(*dims, seed=seed, tol=tol)
     return conv_diff(*dims, seed=seed, tol=tol)
+
+
+@dataclass
+class PPFields:
+    """The fields SOLVE_PP_G assembles the gas pressure correction from, in MFIX's
+    layouts (cell arrays of DIMENSION_3; D_E/D_N/D_T with MMAX+1 phases, the
+    solids arrays with MMAX phases, phase-major)."""
+    imax2: int
+    jmax2: int
+    kmax2: int
+    do_k: int
+    flag: np.ndarray
+    rop_ge: np.ndarray
+    rop_gn: np.ndarray
+    rop_gt: np.ndarray | None
+    ayz: np.ndarray
+    axz: np.ndarray
+    axy: np.ndarray | None
+    u_g: np.ndarray
+    v_g: np.ndarray
+    w_g: np.ndarray | None
+    rop_g: np.ndarray
+    rop_go: np.ndarray
+    vol: np.ndarray
+    sum_r_g: np.ndarray
+    d_e: np.ndarray
+    d_n: np.ndarray
+    d_t: np.ndarray | None
+    mmax: int
+    close_packed: np.ndarray
+    rop_se: np.ndarray | None
+    rop_sn: np.ndarray | None
+    rop_st: np.ndarray | None
+    u_s: np.ndarray | None
+    v_s: np.ndarray | None
+    w_s: np.ndarray | None
+    rop_s: np.ndarray | None
+    rop_so: np.ndarray | None
+    sum_r_s: np.ndarray | None
+    odt: float
+    ijk_p_g: int
+
+    @property
+    def n(self) -> int:
+        return self.imax2 * self.jmax2 * self.kmax2
+
+
+FLAG_FLUID, FLAG_P_OUTFLOW, FLAG_WALL = 1, 11, 100  # MFIX FLAG values (FLUID_AT, P_FLOW_AT, a wall)
+
+
+def pp_fields(imax: int, jmax: int, kmax: int, seed: int = 0, do_k: bool = True, mmax: int = 1,
+              close_packed=(0,), outflow: bool = True, obstacle: bool = True, ijk_p_g: int = 0,
+              dt: float = 0.01) -> PPFields:
+    """Seeded pressure-correction fields on a box with its wall layer: face
+    densities and areas, velocities, bulk densities, volumes, mass sources and
+    D coefficients; a pressure-outflow patch (FLAG 11) on the north wall, an
+    internal obstacle (wall cells) and `mmax` solids phases, close packed as
+    `close_packed` says.  ijk_p_g: 1-based reference cell (0: none)."""
+    imax2, jmax2, kmax2 = imax + 2, jmax + 2, (kmax + 2 if do_k else 1)
+    n = imax2 * jmax2 * kmax2
+    idx = np.arange(n, dtype=np.uint64)
+    u = lambda tag, lo, hi, m=1: lo + (hi - lo) * uniform(seed, tag, np.arange(m * n, dtype=np.uint64))
+    j, i, k = np.meshgrid(np.arange(jmax2), np.arange(imax2), np.arange(kmax2), indexing="ij")
+    j = j.transpose(2, 1, 0).ravel()  # J fastest, then I, then K
+    i = i.transpose(2, 1, 0).ravel()
+    k = k.transpose(2, 1, 0).ravel()
+    flag = np.full(n, FLAG_FLUID, dtype=np.int32)
+    wall = (i == 0) | (i == imax2 - 1) | (j == 0) | (j == jmax2 - 1)
+    if do_k:
+        wall |= (k == 0) | (k == kmax2 - 1)
+    flag[wall] = FLAG_WALL
+    if outflow:  # a pressure-outflow patch on the north wall
+        patch = (j == jmax2 - 1) & (i >= imax2 // 3) & (i < 2 * imax2 // 3)
+        if do_k:
+            patch &= (k >= kmax2 // 3) & (k < 2 * kmax2 // 3)
+        flag[patch] = FLAG_P_OUTFLOW
+    if obstacle:  # a block of wall cells inside
+        ob = (i >= imax2 // 2 - 1) & (i <= imax2 // 2) & (j >= jmax2 // 3) & (j <= jmax2 // 3 + 1)
+        if do_k:
+            ob &= (k >= kmax2 // 2 - 1) & (k <= kmax2 // 2)
+        flag[ob] = FLAG_WALL
+    del idx
+    cp = np.array(list(close_packed)[:mmax] + [0] * max(0, mmax - len(close_packed)), dtype=np.int32)
+    sol = mmax > 0
+    return PPFields(
+        imax2, jmax2, kmax2, 1 if do_k else 0, flag,
+        rop_ge=u(300, 0.5, 1.5), rop_gn=u(301, 0.5, 1.5), rop_gt=u(302, 0.5, 1.5) if do_k else None,
+        ayz=u(303, 0.8, 1.2), axz=u(304, 0.8, 1.2), axy=u(305, 0.8, 1.2) if do_k else None,
+        u_g=u(306, -1.0, 1.0), v_g=u(307, -1.0, 1.0), w_g=u(308, -1.0, 1.0) if do_k else None,
+        rop_g=u(309, 0.9, 1.1), rop_go=u(310, 0.9, 1.1), vol=u(311, 0.9, 1.1), sum_r_g=u(312, -0.01, 0.01),
+        d_e=u(313, 0.1, 1.0, mmax + 1), d_n=u(314, 0.1, 1.0, mmax + 1),
+        d_t=u(315, 0.1, 1.0, mmax + 1) if do_k else None,
+        mmax=mmax, close_packed=cp,
+        rop_se=u(316, 0.1, 0.5, mmax) if sol else None, rop_sn=u(317, 0.1, 0.5, mmax) if sol else None,
+        rop_st=u(318, 0.1, 0.5, mmax) if sol and do_k else None,
+        u_s=u(319, -0.5, 0.5, mmax) if sol else None, v_s=u(320, -0.5, 0.5, mmax) if sol else None,
+        w_s=u(321, -0.5, 0.5, mmax) if sol and do_k else None,
+        rop_s=u(322, 0.1, 0.3, mmax) if sol else None, rop_so=u(323, 0.1, 0.3, mmax) if sol else None,
+        sum_r_s=u(324, -0.001, 0.001, mmax) if sol else None,
+        odt=1.0 / dt, ijk_p_g=int(ijk_p_g))

@@ -71,6 +71,9 @@ def lib() -> C.CDLL:
         L.orc_truth_refine.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_double, C.c_double, C.c_int, C.c_uint64, _dp]
         L.orc_truth_refine.restype = C.c_int
         L.orc_num_threads.restype = C.c_int
+        L.orc_conv_source_pp_g.argtypes = [C.POINTER(Geom), C.c_void_p, vp, vp, vp]
+        L.orc_calc_resid_pp.argtypes = [C.POINTER(Geom), vp, vp, C.c_double]
+        L.orc_calc_resid_pp.restype = C.c_double
         _lib = L
     return _lib
 
@@ -192,6 +195,40 @@ def truth_from(s, x0: np.ndarray, r0: float, rtol: float = 1e-14, max_steps: int
     rel = C.c_double(0.0)
     lib().orc_truth_refine(C.byref(geom(s)), _p(s.a), _p(s.b), _p(x), float(r0), rtol, max_steps, seed, C.byref(rel))
     return x, rel.value
+
+
+class PPFieldsC(C.Structure):
+    _fields_ = [("flag", C.c_void_p), ("rop_ge", C.c_void_p), ("rop_gn", C.c_void_p), ("rop_gt", C.c_void_p),
+                ("ayz", C.c_void_p), ("axz", C.c_void_p), ("axy", C.c_void_p), ("u_g", C.c_void_p),
+                ("v_g", C.c_void_p), ("w_g", C.c_void_p), ("rop_g", C.c_void_p), ("rop_go", C.c_void_p),
+                ("vol", C.c_void_p), ("sum_r_g", C.c_void_p), ("d_e", C.c_void_p), ("d_n", C.c_void_p),
+                ("d_t", C.c_void_p), ("mmax", C.c_int), ("close_packed", C.c_void_p), ("rop_se", C.c_void_p),
+                ("rop_sn", C.c_void_p), ("rop_st", C.c_void_p), ("u_s", C.c_void_p), ("v_s", C.c_void_p),
+                ("w_s", C.c_void_p), ("rop_s", C.c_void_p), ("rop_so", C.c_void_p), ("sum_r_s", C.c_void_p),
+                ("odt", C.c_double), ("ijk_p_g", C.c_longlong)]
+
+
+def conv_source_pp_g(f):
+    """CONV_PP_G + SOURCE_PP_G restated in C: (A_M(:,:,0) as (7, n), B_M(:,0), B_MMAX(:,0))."""
+    c = PPFieldsC()
+    for name, _ in PPFieldsC._fields_:
+        if name in ("mmax", "odt", "ijk_p_g"):
+            continue
+        arr = getattr(f, name)
+        setattr(c, name, arr.ctypes.data if arr is not None else None)
+    c.mmax, c.odt, c.ijk_p_g = f.mmax, f.odt, f.ijk_p_g
+    g = Geom(f.imax2, f.jmax2, f.kmax2, f.do_k, f.n)
+    a = np.zeros((7, f.n))
+    b = np.zeros(f.n)
+    bm = np.zeros(f.n)
+    lib().orc_conv_source_pp_g(C.byref(g), C.byref(c), _p(a), _p(b), _p(bm))
+    return a, b, bm
+
+
+def calc_resid_pp(f, b: np.ndarray, norm: float) -> float:
+    """CALC_RESID_PP's RESID of b over the fluid cells."""
+    g = Geom(f.imax2, f.jmax2, f.kmax2, f.do_k, f.n)
+    return lib().orc_calc_resid_pp(C.byref(g), f.flag.ctypes.data, _p(b), norm)
 
 
 def num_threads() -> int:

@@ -965,3 +965,140 @@ int orc_leq_sor(const orc_geom *g, double *var, double *a, double *b, int itmax,
     free(tmp);
     return 0;
 }
+
+/* ------------------------------------------------------------------ pressure-correction assembly */
+/* CONV_PP_G (model/conv_pp_g.f:33-182) followed by SOURCE_PP_G
+ * (model/source_pp_g.f:18-214), incompressible (COMPRESSIBLE_PP_G is not
+ * called), no Cartesian-grid factors, no shear.  CONV_PP_G writes each face
+ * coefficient from the cell below the face (ROP_GE(IJK)*AYZ(IJK) is A_M(IJK,east)
+ * and A_M(IP_OF(IJK),west)); restated as a gather per fluid cell, it is
+ * A(west) = ROP_GE(IMJK)*AYZ(IMJK) whether or not IMJK is fluid (:80-106).
+ * Every sum keeps the reference's left-to-right order. */
+static int fluid_at(const int *flag, int64_t p) { return flag[p] == 1; }
+static int p_flow_at(const int *flag, int64_t p) { return flag[p] == 10 || flag[p] == 11; }
+
+void orc_conv_source_pp_g(const orc_geom *g, const orc_pp_fields *f, double *a, double *b, double *bmmax)
+{
+    const int64_t n = g->n, c1 = g->jmax2, c2 = (int64_t)g->jmax2 * g->imax2;
+    double *am3 = a, *am2 = a + n, *am1 = a + 2 * n, *a0 = a + 3 * n, *ap1 = a + 4 * n, *ap2 = a + 5 * n,
+           *ap3 = a + 6 * n;
+#pragma omp parallel for collapse(2) schedule(static)
+    for (int k = 1; k <= g->kmax2; ++k)
+        for (int i = 1; i <= g->imax2; ++i)
+            for (int j = 1; j <= g->jmax2; ++j) {
+                const int64_t p = cell(g, i, j, k);
+                if (!fluid_at(f->flag, p)) {  /* :187-199 */
+                    am3[p] = am2[p] = am1[p] = ap1[p] = ap2[p] = ap3[p] = 0.0;
+                    a0[p] = -1.0;
+                    b[p] = 0.0;
+                    bmmax[p] = 0.0;
+                    continue;
+                }
+                /* clamped neighbours (model/set_increments.f:80-109) */
+                const int64_t im = p + (i > 1 ? -c1 : 0), ip = p + (i < g->imax2 ? c1 : 0);
+                const int64_t jm = p + (j > 1 ? -1 : 0), jp = p + (j < g->jmax2 ? 1 : 0);
+                const int64_t km = p + ((g->do_k && k > 1) ? -c2 : 0), kp = p + ((g->do_k && k < g->kmax2) ? c2 : 0);
+                /* CONV_PP_G, gas phase (:80-119) */
+                double ae = f->rop_ge[p] * f->ayz[p];
+                double aw = f->rop_ge[im] * f->ayz[im];
+                double an = f->rop_gn[p] * f->axz[p];
+                double as = f->rop_gn[jm] * f->axz[jm];
+                double at = 0.0, ab = 0.0;
+                if (g->do_k) {
+                    at = f->rop_gt[p] * f->axy[p];
+                    ab = f->rop_gt[km] * f->axy[km];
+                }
+                /* SOURCE_PP_G (:87-106) */
+                const double bma = (f->rop_g[p] - f->rop_go[p]) * f->vol[p] * f->odt;
+                const double bme = ae * f->u_g[p];
+                const double bmw = aw * f->u_g[im];
+                const double bmn = an * f->v_g[p];
+                const double bms = as * f->v_g[jm];
+                const double bmt = g->do_k ? at * f->w_g[p] : 0.0;
+                const double bmb = g->do_k ? ab * f->w_g[km] : 0.0;
+                const double bmr = f->sum_r_g[p] * f->vol[p];
+                double bv = -((-(bma + bme - bmw + bmn - bms + bmt - bmb)) + bmr);
+                double mx = fabs(bma);
+                const double terms[7] = {bme, bmw, bmn, bms, bmt, bmb, bmr};
+                for (int q = 0; q < 7; ++q)
+                    if (fabs(terms[q]) > mx) mx = fabs(terms[q]);
+                ae = ae * f->d_e[p];
+                aw = aw * f->d_e[im];
+                an = an * f->d_n[p];
+                as = as * f->d_n[jm];
+                if (g->do_k) {
+                    at = at * f->d_t[p];
+                    ab = ab * f->d_t[km];
+                }
+                /* solids phases that do not become close packed (:117-145; CONV_PP_G :125-178) */
+                for (int m = 1; m <= f->mmax; ++m) {
+                    if (f->close_packed[m - 1]) continue;
+                    const int64_t o = (int64_t)(m - 1) * n, od = (int64_t)m * n;
+                    const double se = f->rop_se[o + p] * f->ayz[p];
+                    const double sw = f->rop_se[o + im] * f->ayz[im];
+                    const double sn = f->rop_sn[o + p] * f->axz[p];
+                    const double ss = f->rop_sn[o + jm] * f->axz[jm];
+                    double st = 0.0, sb = 0.0;
+                    if (g->do_k) {
+                        st = f->rop_st[o + p] * f->axy[p];
+                        sb = f->rop_st[o + km] * f->axy[km];
+                    }
+                    const double wt = g->do_k ? st * f->w_s[o + p] : 0.0;
+                    const double wb = g->do_k ? sb * f->w_s[o + km] : 0.0;
+                    bv = bv - ((-((f->rop_s[o + p] - f->rop_so[o + p]) * f->vol[p] * f->odt + se * f->u_s[o + p] -
+                                   sw * f->u_s[o + im] + sn * f->v_s[o + p] - ss * f->v_s[o + jm] + wt - wb)) +
+                               f->sum_r_s[o + p] * f->vol[p]);
+                    ae = ae + se * f->d_e[od + p];
+                    aw = aw + sw * f->d_e[od + im];
+                    an = an + sn * f->d_n[od + p];
+                    as = as + ss * f->d_n[od + jm];
+                    if (g->do_k) {
+                        at = at + st * f->d_t[od + p];
+                        ab = ab + sb * f->d_t[od + km];
+                    }
+                }
+                double ac = -(ae + aw + an + as + at + ab); /* :147-149 */
+                if (fabs(ac) < 1.0e-15) {                    /* :151-162, SMALL_NUMBER */
+                    if (fabs(bv) < 1.0e-15) {
+                        ac = -1.0;
+                        bv = 0.0;
+                    }
+                }
+                /* links to pressure-flow cells cut (:224-243) */
+                if (p_flow_at(f->flag, im)) aw = 0.0;
+                if (p_flow_at(f->flag, ip)) ae = 0.0;
+                if (p_flow_at(f->flag, jm)) as = 0.0;
+                if (p_flow_at(f->flag, jp)) an = 0.0;
+                if (p_flow_at(f->flag, km)) ab = 0.0;
+                if (p_flow_at(f->flag, kp)) at = 0.0;
+                am3[p] = ab;
+                am2[p] = as;
+                am1[p] = aw;
+                a0[p] = ac;
+                ap1[p] = ae;
+                ap2[p] = an;
+                ap3[p] = at;
+                b[p] = bv;
+                bmmax[p] = mx;
+            }
+    /* the reference cell of an incompressible run (:247-251) */
+    if (f->ijk_p_g >= 1 && f->ijk_p_g <= n) {
+        const int64_t p = f->ijk_p_g - 1;
+        for (int q = 0; q < 7; ++q) a[q * n + p] = 0.0;
+        a0[p] = -1.0;
+        b[p] = 0.0;
+    }
+}
+
+double orc_calc_resid_pp(const orc_geom *g, const int *flag, const double *b, double norm)
+{
+    double num = 0.0, den = 0.0;
+    for (int64_t p = 0; p < g->n; ++p)
+        if (fluid_at(flag, p)) {
+            num = num + fabs(b[p]);
+            den = den + 1.0;
+        }
+    if (den * norm > 0.0) return num / (den * norm);
+    if (num == 0.0) return 0.0;
+    return 1.0e32; /* LARGE_NUMBER */
+}

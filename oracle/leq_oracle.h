@@ -93,6 +93,32 @@ int orc_truth_solve(const orc_geom *g, const double *a, const double *b, double 
 int orc_truth_refine(const orc_geom *g, const double *a, const double *b, double *x, double r0, double rtol,
                      int max_iter, uint64_t rt_seed, double *final_rel);
 
+/* Pressure-correction system of the gas phase, A_M(:,:,0) / B_M(:,0) / B_MMAX(:,0),
+ * as CONV_PP_G (model/conv_pp_g.f:33-182) and SOURCE_PP_G (model/source_pp_g.f:18-214)
+ * build it for an incompressible run (RO_G0 defined) on a Cartesian grid without
+ * shear: face coefficients from the face densities and areas, the continuity
+ * residual and its largest term, the D_E/D_N/D_T factors, the solids phases
+ * that are not close packed, the centre coefficient, identity rows outside the
+ * fluid, the links to pressure-flow cells cut, and the reference cell IJK_P_G.
+ * Phase arrays are column-major: D_E(DIMENSION_3, 0:MMAX) and ROP_SE(DIMENSION_3,
+ * 1:MMAX) with phase m at offset m*n and (m-1)*n.  ijk_p_g is 1-based, <= 0 when
+ * undefined.  a is A_M(DIMENSION_3,-3:3), b and bmmax have n entries. */
+typedef struct {
+    const int *flag;
+    const double *rop_ge, *rop_gn, *rop_gt, *ayz, *axz, *axy, *u_g, *v_g, *w_g;
+    const double *rop_g, *rop_go, *vol, *sum_r_g, *d_e, *d_n, *d_t;
+    int mmax;
+    const int *close_packed;
+    const double *rop_se, *rop_sn, *rop_st, *u_s, *v_s, *w_s, *rop_s, *rop_so, *sum_r_s;
+    double odt;
+    long long ijk_p_g;
+} orc_pp_fields;
+void orc_conv_source_pp_g(const orc_geom *g, const orc_pp_fields *f, double *a, double *b, double *bmmax);
+
+/* CALC_RESID_PP (model/calc_resid.f:391-534), serial: RESID of B over the fluid
+ * cells (|B| summed in cell order) with normalization `norm`. */
+double orc_calc_resid_pp(const orc_geom *g, const int *flag, const double *b, double norm);
+
 int orc_num_threads(void);
 
 #ifdef __cplusplus

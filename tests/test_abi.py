@@ -194,3 +194,25 @@ def test_deferred_queue_aliasing_geometry_finalize():
     assert leq.pending_lin_eq() == 1
     leq.finalize()
     assert leq.pending_lin_eq() == 0 and left.value == leq.IER_INCOMPLETE
+
+
+def test_pp_assembly_argument_checks():
+    """The pressure-correction entry points refuse a missing field record, a
+    compressible run and missing arrays before any device work."""
+    from mfix_b200 import systems as S
+
+    f = S.pp_fields(6, 7, 5, seed=1, mmax=1)
+    assert leq.init_geometry(f.imax2, f.jmax2, f.kmax2, f.do_k, f.n, 2) == 0
+    a, b, bm = np.zeros((7, f.n)), np.zeros(f.n), np.zeros(f.n)
+    L = mfix_b200.lib()
+    assert L.mfixgpu_conv_source_pp_g(None, a.ctypes.data, b.ctypes.data, bm.ctypes.data) == leq.IER_ARGS
+    c = leq.pp_struct(f)
+    if _gpu_visible():
+        c.ro_g0_defined = 0
+        assert L.mfixgpu_conv_source_pp_g(ctypes.byref(c), a.ctypes.data, b.ctypes.data,
+                                          bm.ctypes.data) == leq.IER_UNSUPPORTED
+    else:  # without a device every call ends in the no-device code
+        assert L.mfixgpu_conv_source_pp_g(ctypes.byref(c), a.ctypes.data, b.ctypes.data,
+                                          bm.ctypes.data) == leq.IER_CUDA
+        ier, _ = leq.solve_pp_g(f, 0.0, np.zeros(f.n))
+        assert ier == leq.IER_CUDA
