@@ -6,11 +6,30 @@
 !> Call MFIXGPU_SETUP once after SET_INCREMENTS (it registers the box geometry
 !> the library cannot read from the MFIX modules).
 module mfixgpu_mod
-   use iso_c_binding, only: c_int, c_int64_t, c_double, c_char, c_ptr, c_null_char
+   use iso_c_binding, only: c_int, c_int64_t, c_long_long, c_double, c_char, c_ptr, c_null_char, c_null_ptr, &
+                            c_loc, c_size_t
    implicit none
    private
    public :: mfixgpu_setup, mfixgpu_set_option, mfixgpu_iter_tot, mfixgpu_finalize, mfixgpu_flush, &
-             solve_lin_eq_defer
+             solve_lin_eq_defer, solve_pp_g_gpu
+
+   !> mfixgpu_pp_fields (include/mfixgpu.h): the fields SOLVE_PP_G assembles from
+   type, bind(C) :: pp_fields_t
+      type(c_ptr) :: flag = c_null_ptr
+      type(c_ptr) :: rop_ge = c_null_ptr, rop_gn = c_null_ptr, rop_gt = c_null_ptr
+      type(c_ptr) :: ayz = c_null_ptr, axz = c_null_ptr, axy = c_null_ptr
+      type(c_ptr) :: u_g = c_null_ptr, v_g = c_null_ptr, w_g = c_null_ptr
+      type(c_ptr) :: rop_g = c_null_ptr, rop_go = c_null_ptr, vol = c_null_ptr, sum_r_g = c_null_ptr
+      type(c_ptr) :: d_e = c_null_ptr, d_n = c_null_ptr, d_t = c_null_ptr
+      integer(c_int) :: mmax = 0, ro_g0_defined = 1
+      type(c_ptr) :: close_packed = c_null_ptr
+      type(c_ptr) :: rop_se = c_null_ptr, rop_sn = c_null_ptr, rop_st = c_null_ptr
+      type(c_ptr) :: u_s = c_null_ptr, v_s = c_null_ptr, w_s = c_null_ptr
+      type(c_ptr) :: rop_s = c_null_ptr, rop_so = c_null_ptr, sum_r_s = c_null_ptr
+      real(c_double) :: odt = 0
+      integer(c_long_long) :: ijk_p_g = 0
+      integer(c_int) :: on_device = 0, pad = 0
+   end type pp_fields_t
 
    interface
       integer(c_int) function c_init_geometry(imax2, jmax2, kmax2, do_k, dimension_3, dimension_m) &
@@ -49,6 +68,19 @@ module mfixgpu_mod
       integer(c_int) function c_flush() bind(C, name="mfixgpu_solve_lin_eq_flush")
          import :: c_int
       end function c_flush
+
+      subroutine c_solve_pp_g(f, normg, pp_g, resg, itmax, method, sweep, tol, pc, ier, sweep_len, pc_len) &
+            bind(C, name="mfixgpu_solve_pp_g_")
+         import :: pp_fields_t, c_int, c_double, c_char, c_size_t
+         type(pp_fields_t), intent(in) :: f
+         real(c_double), intent(in) :: normg, tol
+         real(c_double), dimension(*), intent(inout) :: pp_g
+         real(c_double), intent(out) :: resg
+         integer(c_int), intent(in) :: itmax, method
+         character(kind=c_char), dimension(*), intent(in) :: sweep, pc
+         integer(c_int), intent(inout) :: ier
+         integer(c_size_t), value :: sweep_len, pc_len
+      end subroutine c_solve_pp_g
    end interface
 
 contains
@@ -85,6 +117,76 @@ contains
    integer function mfixgpu_flush()
       mfixgpu_flush = c_flush()
    end function mfixgpu_flush
+
+   !> SOLVE_PP_G(NORMG, RESG, IER) (model/solve_pp_g.f:10-118) on the device: the
+   !> pressure-correction system is assembled there from the fields below and solved
+   !> there; only the fields and PP_G cross the host link, and A_M/B_M are not used.
+   !> For an incompressible run (RO_G0 defined) on a Cartesian grid without shear,
+   !> point sources or user sources; other runs keep the reference's SOLVE_PP_G.
+   !> The addresses of the module arrays are taken through TARGET dummies, so the
+   !> arrays must be contiguous (they are: MFIX allocates them whole).
+   subroutine solve_pp_g_gpu(normg, resg, ier)
+      use fldvar, only: rop_g, rop_go, u_g, v_g, w_g, rop_s, rop_so, u_s, v_s, w_s
+      use mflux, only: rop_ge, rop_gn, rop_gt, rop_se, rop_sn, rop_st
+      use geometry, only: flag, ayz, axz, axy, vol, do_k
+      use pgcor, only: pp_g, d_e, d_n, d_t
+      use physprop, only: mmax, close_packed, ro_g0
+      use rxns, only: sum_r_g, sum_r_s
+      use run, only: odt
+      use bc, only: ijk_p_g
+      use param1, only: undefined, undefined_i
+      use leqsol, only: leq_it, leq_method, leq_sweep, leq_tol, leq_pc
+      double precision, intent(in) :: normg
+      double precision, intent(out) :: resg
+      integer, intent(inout) :: ier
+      type(pp_fields_t) :: f
+      integer(c_int), allocatable, target :: cp(:)
+      integer(c_int) :: cier
+      real(c_double) :: cres
+      integer :: m
+      f%flag = iaddr(flag)
+      f%rop_ge = daddr(rop_ge); f%rop_gn = daddr(rop_gn)
+      f%ayz = daddr(ayz); f%axz = daddr(axz)
+      f%u_g = daddr(u_g); f%v_g = daddr(v_g)
+      f%rop_g = daddr(rop_g); f%rop_go = daddr(rop_go); f%vol = daddr(vol); f%sum_r_g = daddr(sum_r_g)
+      f%d_e = daddr(d_e); f%d_n = daddr(d_n)
+      if (do_k) then
+         f%rop_gt = daddr(rop_gt); f%axy = daddr(axy); f%w_g = daddr(w_g); f%d_t = daddr(d_t)
+      end if
+      f%mmax = int(mmax, c_int)
+      allocate(cp(max(mmax, 1)))
+      cp = 0
+      do m = 1, mmax
+         if (close_packed(m)) cp(m) = 1
+      end do
+      f%close_packed = c_loc(cp)
+      if (mmax > 0) then
+         f%rop_se = daddr(rop_se); f%rop_sn = daddr(rop_sn)
+         f%u_s = daddr(u_s); f%v_s = daddr(v_s)
+         f%rop_s = daddr(rop_s); f%rop_so = daddr(rop_so); f%sum_r_s = daddr(sum_r_s)
+         if (do_k) then
+            f%rop_st = daddr(rop_st); f%w_s = daddr(w_s)
+         end if
+      end if
+      f%ro_g0_defined = merge(1_c_int, 0_c_int, ro_g0 /= undefined)
+      f%odt = odt
+      f%ijk_p_g = merge(int(ijk_p_g, c_long_long), 0_c_long_long, ijk_p_g /= undefined_i)
+      cier = int(ier, c_int)
+      call c_solve_pp_g(f, real(normg, c_double), pp_g, cres, int(leq_it(1), c_int), int(leq_method(1), c_int), &
+                        leq_sweep(1), real(leq_tol(1), c_double), leq_pc(1), cier, 4_c_size_t, 4_c_size_t)
+      resg = cres
+      ier = int(cier)
+      deallocate(cp)
+   contains
+      type(c_ptr) function daddr(x)
+         double precision, target, intent(in) :: x(*)
+         daddr = c_loc(x)
+      end function daddr
+      type(c_ptr) function iaddr(x)
+         integer, target, intent(in) :: x(*)
+         iaddr = c_loc(x)
+      end function iaddr
+   end subroutine solve_pp_g_gpu
 
    !> SOLVE_LIN_EQ_DEFER: SOLVE_LIN_EQ's dummy list, the call queued for MFIXGPU_FLUSH
    !> (the per-phase calls of one equation, e.g. model/solve_vel_star.f:308-331, then

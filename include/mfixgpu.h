@@ -38,11 +38,21 @@ extern "C" {
 /* Registers the box geometry that SOLVE_LIN_EQ reads from modules: IMAX2,
  * JMAX2, KMAX2 (model/set_max2.f:48-135), DO_K, DIMENSION_3
  * (model/set_param.f:98) and DIMENSION_M.  Call once after SET_INCREMENTS.
- * Only the serial, non-cyclic, non-cut-cell box is served: neighbour offsets
- * clamp at the array edge as in model/set_increments.f:80-109.  Returns 0 or
- * MFIXGPU_ERR_ARGS. */
+ * Only the serial, non-cut-cell box is served: neighbour offsets clamp at the
+ * array edge as in model/set_increments.f:80-109, or wrap along the cyclic axes
+ * registered by mfixgpu_init_cyclic.  Returns 0 or MFIXGPU_ERR_ARGS. */
 int mfixgpu_init_geometry(const int *imax2, const int *jmax2, const int *kmax2, const int *do_k,
                           const int64_t *dimension_3, const int *dimension_m);
+
+/* CYCLIC_X, CYCLIC_Y, CYCLIC_Z (nonzero = .TRUE.) of a serial run, registered
+ * after mfixgpu_init_geometry (which resets them): the neighbour increments of
+ * the interior cells wrap along those axes as SET_INCREMENTS builds them
+ * (model/set_increments.f:73-113 with IMAP_C(IMAX2) = IMIN1, IMAP_C(IMIN2) = IMAX1,
+ * model/dmp_modules/gridmap_mod.f:496-503), in LEQ_MATVEC and in the
+ * right-hand sides of the line sweeps; the lines themselves stay open
+ * tridiagonals, as LEQ_IKSWEEP solves them (model/leqsol_mod.f:907-909).  CYCLIC_Z
+ * is ignored in 2-D.  Returns 0, MFIXGPU_ERR_ARGS or MFIXGPU_ERR_NOGEOM. */
+int mfixgpu_init_cyclic(const int *cyclic_x, const int *cyclic_y, const int *cyclic_z);
 
 /* SOLVE_LIN_EQ(VNAME, VNO, VAR, A_M, B_M, M, ITMAX, METHOD, SWEEP, TOL1, PC, IER),
  * model/solve_lin_eq.f:17-78, in gfortran's convention: every argument by
@@ -142,6 +152,11 @@ const char *mfixgpu_last_error(void);
  *                    (Phat = M^{-1} P + c z, z = 1 on rows with a nonzero neighbour coefficient,
  *                    c = z^T P / z^T A z), which keeps it converging on near-singular operators;
  *                    0: such systems go to the FP64 drop-in
+ *   "do_transpose"   0 (default) / 1: the reference's DO_TRANSPOSE keyword (model/solve_lin_eq.f:139-150):
+ *                    METHOD 2 runs LEQ_BICGSt (model/leq_bicgst.f), i.e. LEQ_BICGS0's iteration on a
+ *                    transposed copy of A_M: A_M comes back unscaled and B_M scaled, and LEQ_MSOLVEt's
+ *                    letters apply (2-D: I only; 3-D: R, I, K; an odd IMAX2 with R returns
+ *                    MFIXGPU_ERR_UNSUPPORTED)
  *   "replace_every"  mixed form, deflated systems: the FP32 residual is replaced by the FP64 true
  *                    residual at least every this many inner iterations (default 20; 0: only after
  *                    the inner_tol drop)
@@ -173,6 +188,8 @@ void mfixgpu_finalize(void);
 typedef struct {
     int imax2, jmax2, kmax2, do_k;
     int64_t dimension_3;
+    int cyclic;  /* 1 CYCLIC_X | 2 CYCLIC_Y | 4 CYCLIC_Z (0: the clamped box) */
+    int pad;
 } mfixgpu_geom;
 
 /* LEQ_MATVEC(VNAME, VAR, A_M, AVAR), model/leqsol_mod.f:103-265: avar = A*var. */

@@ -24,6 +24,7 @@ struct Geometry {
     int imax2 = 0, jmax2 = 0, kmax2 = 0, do_k = 1;
     int64_t n = 0;
     int dimension_m = 0;
+    int cyc = 0;  // cyclic axes: 1 CYCLIC_X, 2 CYCLIC_Y, 4 CYCLIC_Z
 };
 
 struct Options {
@@ -36,6 +37,7 @@ struct Options {
     double mixed_min_margin = 1e-4;
     int deflate = 1;
     int replace_every = 20;
+    int do_transpose = 0;
     int check_every = 4;
     int use_graph = 1;
     int time_kernels = 0;
@@ -85,6 +87,10 @@ int pp_prepare(Global &g, Engine *e, const mfixgpu_pp_fields *hf, PPDevice &dv)
     if (!hf) {
         g.err = "null field record";
         return MFIXGPU_ERR_ARGS;
+    }
+    if (g.geom.cyc) {
+        g.err = "the device assembly of the pressure correction serves non-cyclic boxes";
+        return MFIXGPU_ERR_UNSUPPORTED;
     }
     if (!hf->ro_g0_defined) {
         g.err = "a compressible run (RO_G0 undefined, COMPRESSIBLE_PP_G) is not served by the device assembly";
@@ -320,6 +326,7 @@ void solve_impl(int vno, double *var, double *a_m, double *b_m, int m, int itmax
     s.jmax2 = g.geom.jmax2;
     s.kmax2 = g.geom.kmax2;
     s.do_k = g.geom.do_k;
+    s.cyc = g.geom.cyc;
     s.n = n;
     s.a = a_m + (size_t)m * 7 * (size_t)n;  // A_M(:,:,M)
     s.b = b_m + (size_t)m * (size_t)n;      // B_M(:,M)
@@ -329,6 +336,7 @@ void solve_impl(int vno, double *var, double *a_m, double *b_m, int m, int itmax
     std::vector<SolveResult> out;
     SolveOptions so = make_opts(g.opt, pc, sweep4);
     so.method = method;
+    so.transposed = g.opt.do_transpose && method == 2;  // DO_TRANSPOSE applies to CASE (2) only (:139-150)
     const int rc = e->solve({s}, so, out);
     if (rc) {
         g.err = e->last_error();
@@ -434,7 +442,8 @@ int flush_locked(Global &g)
     std::vector<int> code(all.size(), MFIXGPU_ERR_INCOMPLETE);
     mfixgpu_stats agg{};
     auto same_geom = [](const Geometry &a, const Geometry &b) {
-        return a.imax2 == b.imax2 && a.jmax2 == b.jmax2 && a.kmax2 == b.kmax2 && a.do_k == b.do_k && a.n == b.n;
+        return a.imax2 == b.imax2 && a.jmax2 == b.jmax2 && a.kmax2 == b.kmax2 && a.do_k == b.do_k && a.n == b.n &&
+               a.cyc == b.cyc;
     };
     for (size_t q0 = 0; q0 < all.size(); ++q0) {
         if (done[q0]) continue;
@@ -455,6 +464,7 @@ int flush_locked(Global &g)
             s.jmax2 = d.geom.jmax2;
             s.kmax2 = d.geom.kmax2;
             s.do_k = d.geom.do_k;
+            s.cyc = d.geom.cyc;
             s.n = n;
             s.a = d.a_m + (size_t)d.m * 7 * (size_t)n;  // A_M(:,:,M)
             s.b = d.b_m + (size_t)d.m * (size_t)n;      // B_M(:,M)
@@ -463,7 +473,9 @@ int flush_locked(Global &g)
             s.itmax = d.itmax;
         }
         std::vector<SolveResult> out;
-        const int rc = e->solve(specs, make_opts(g.opt, decode_pc(all[q0].pc), all[q0].sweep), out);
+        SolveOptions so = make_opts(g.opt, decode_pc(all[q0].pc), all[q0].sweep);
+        so.transposed = g.opt.do_transpose != 0;  // queued calls are METHOD 2
+        const int rc = e->solve(specs, so, out);
         if (rc) {
             g.err = e->last_error();
             for (size_t q : grp) code[q] = rc;
@@ -515,8 +527,21 @@ int mfixgpu_init_geometry(const int *imax2, const int *jmax2, const int *kmax2, 
     g.geom.jmax2 = *jmax2;
     g.geom.kmax2 = *kmax2;
     g.geom.do_k = *do_k ? 1 : 0;
+    g.geom.cyc = 0;  // set by mfixgpu_init_cyclic
     g.geom.n = *dimension_3;
     g.geom.dimension_m = *dimension_m;
+    return 0;
+}
+
+int mfixgpu_init_cyclic(const int *cyclic_x, const int *cyclic_y, const int *cyclic_z)
+{
+    Global &g = G();
+    std::lock_guard<std::mutex> lk(g.mu);
+    if (!cyclic_x || !cyclic_y || !cyclic_z) return MFIXGPU_ERR_ARGS;
+    if (!g.geom.set) return MFIXGPU_ERR_NOGEOM;
+    int c = (*cyclic_x ? 1 : 0) | (*cyclic_y ? 2 : 0) | (*cyclic_z ? 4 : 0);
+    if (!g.geom.do_k) c &= 3;  // no K direction in 2-D
+    g.geom.cyc = c;
     return 0;
 }
 
@@ -640,6 +665,8 @@ int mfixgpu_set_option(const char *name, double value)
         g.opt.mixed_growth = value;
     } else if (k == "deflate") {
         g.opt.deflate = value != 0;
+    } else if (k == "do_transpose") {
+        g.opt.do_transpose = value != 0;
     } else if (k == "replace_every") {
         if (value < 0) return MFIXGPU_ERR_ARGS;
         g.opt.replace_every = (int)value;
@@ -682,6 +709,7 @@ double mfixgpu_get_option(const char *name)
     if (k == "mixed_min_margin") return g.opt.mixed_min_margin;
     if (k == "deflate") return g.opt.deflate;
     if (k == "replace_every") return g.opt.replace_every;
+    if (k == "do_transpose") return g.opt.do_transpose;
     if (k == "check_every") return g.opt.check_every;
     if (k == "use_graph") return g.opt.use_graph;
     if (k == "time_kernels") return g.opt.time_kernels;
@@ -816,6 +844,7 @@ void mfixgpu_solve_pp_g_(const mfixgpu_pp_fields *f, const double *normg, double
     SolveOptions so = make_opts(g.opt, pcode, s4);
     so.method = *method;
     so.on_device = true;
+    so.transposed = g.opt.do_transpose && *method == 2;
     std::vector<SolveResult> out;
     rc = e->solve({sp}, so, out);
     if (rc) {
@@ -866,6 +895,7 @@ int mfixgpu_leq_matvec(const mfixgpu_geom *gm, const double *a_dev, const double
     s.jmax2 = gm->jmax2;
     s.kmax2 = gm->kmax2;
     s.do_k = gm->do_k ? 1 : 0;
+    s.cyc = gm->cyclic & 7;
     s.n = gm->dimension_3;
     const int rc = e->matvec(s, a_dev, var_dev, avar_dev);
     if (rc) g.err = e->last_error();
@@ -893,6 +923,7 @@ int mfixgpu_leq_msolve(const mfixgpu_geom *gm, const double *b_dev, const double
     s.jmax2 = gm->jmax2;
     s.kmax2 = gm->kmax2;
     s.do_k = gm->do_k ? 1 : 0;
+    s.cyc = gm->cyclic & 7;
     s.n = gm->dimension_3;
     const int rc = e->msolve(s, a_dev, b_dev, var_dev, pcode, s4);
     if (rc) g.err = e->last_error();

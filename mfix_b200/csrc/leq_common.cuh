@@ -78,6 +78,7 @@ struct SysDev {
     // FP32 arrays (diagonals, factors, vectors) are its own: each J-line padded to
     // a pitch that is a multiple of four cells, so every line starts on a 16-byte
     // boundary; the pad cells hold zeros (diagonal A(0) = 1).
+    int cyc;             // cyclic axes (1 I, 2 J, 4 K): the interior cells' neighbours wrap
     int jp;              // line pitch of those arrays
     int64_t np;          // their cells: jp * imax2 * kmax2
     FastDiv div_jp;      // division by jp
@@ -157,6 +158,19 @@ constexpr int TILE_CELLS = 4096;
 constexpr int CELL_THREADS = 256;
 
 // Ordered parameters of one J-line half-sweep (a "wave").
+// Along a cyclic axis with an odd number of interior cells the first and last
+// interior lines wrap onto each other with the same red/black colour; in the
+// reference's loop order (k outer, i inner) the last one comes second and sees the
+// first one's new value.  A line's wrap level counts such late positions: a
+// colour's lines run level by level.
+__host__ __device__ __forceinline__ int wrap_level(const SysDev &d, int i, int k)
+{
+    int l = 0;
+    if ((d.cyc & 1) && ((d.imax2 - 2) & 1) && i == d.imax2 - 1) ++l;
+    if (d.do_k && (d.cyc & 4) && ((d.kmax2 - 2) & 1) && k == d.kmax2 - 1) ++l;
+    return l;
+}
+
 struct WaveArgs {
     int kind;        // 0: lines with ((i + k) & 1) == par, 1: lines with i + k == diag, 2: single line list
     int par;         // parity or diagonal index
@@ -166,6 +180,7 @@ struct WaveArgs {
     int count;       // kinds 1 and 2 (single system): work items in the wave
     int nlines;      // kind 2: lines in `list`
     const int2 *list;  // kind 2: (i, k) of each line, 1-based
+    int lvl;         // kind 0: 0 every line of the parity, else only lines of wrap level lvl - 1
 };
 
 enum Gate : int {

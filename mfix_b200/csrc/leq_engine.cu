@@ -300,6 +300,7 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         d.jmax2 = sp.jmax2;
         d.kmax2 = sp.kmax2;
         d.do_k = sp.do_k;
+        d.cyc = sp.cyc;
         d.n = sp.n;
         d.div_j = make_fastdiv((uint32_t)sp.jmax2);
         d.div_i = make_fastdiv((uint32_t)sp.imax2);
@@ -658,11 +659,23 @@ int Engine::plan_msolve(const SolveOptions &opt, int src, int dst, int gate, int
         if (ch == 'A' || ch == 'a') return 'A';
         return 0;
     };
+    // LEQ_MSOLVEt (DO_TRANSPOSE, model/leq_bicgst.f:978-1177) serves I in 2-D (its
+    // red/black branch is 3-D only) and R, I, K in 3-D (no A); with an odd number of
+    // I-lines its red/black loop wraps within a k row, so that lines of one pass
+    // neighbour each other and their order matters: not served.
+    auto noop = [&](int L) {
+        if (!d0.do_k && (L == 'A' || L == 'K')) return true;  // no-ops in the 2-D branch
+        if (opt.transposed && ((!d0.do_k && L == 'R') || L == 'A')) return true;
+        return false;
+    };
+    if (opt.transposed && d0.do_k && (d0.imax2 & 1))
+        for (int q = 0; q < 4; ++q)
+            if (letter(opt.sweep[q]) == 'R')
+                return fail("DO_TRANSPOSE red/black sweeps with an odd IMAX2 are not served", -10);
     int first = 0;
     for (int q = 0; q < 4 && !first; ++q) {
         const int L = letter(opt.sweep[q]);
-        if (!L) continue;
-        if (!d0.do_k && (L == 'A' || L == 'K')) continue;  // no-ops in the 2-D branch
+        if (!L || noop(L)) continue;
         first = L;
     }
     if (!first) {
@@ -674,7 +687,15 @@ int Engine::plan_msolve(const SolveOptions &opt, int src, int dst, int gate, int
         plan_[which].push_back(cp);
         return 0;
     }
-    bool fused_guess = (first == 'R');
+    // red/black lines that wrap onto a line of their own colour (odd cyclic
+    // periods) run in wrap levels, after a plain Var = B copy
+    int wrap_levels = 1;
+    for (int s = 0; s < nsys_; ++s) {
+        const SysDev &d = h_sys_[s];
+        if (d.n == 0) continue;
+        wrap_levels = std::max(wrap_levels, 1 + wrap_level(d, d.imax2 - 1, d.kmax2 - 1));
+    }
+    bool fused_guess = (first == 'R') && wrap_levels == 1;
     if (!fused_guess) {
         Step cp{};
         cp.type = 1;
@@ -684,12 +705,13 @@ int Engine::plan_msolve(const SolveOptions &opt, int src, int dst, int gate, int
         plan_[which].push_back(cp);
     }
     int waves_done = 0;
-    auto wave = [&](int kind, int par, int count, const int2 *list, int nlines) {
+    auto wave = [&](int kind, int par, int count, const int2 *list, int nlines, int lvl = 0) {
         Step st{};
         st.type = 0;
         WaveArgs &w = st.w;
         w.kind = kind;
         w.par = par;
+        w.lvl = lvl;
         w.rhs = src;
         w.dst = dst;
         w.gate = gate;
@@ -712,14 +734,22 @@ int Engine::plan_msolve(const SolveOptions &opt, int src, int dst, int gate, int
         ++waves_done;
         plan_[which].push_back(st);
     };
+    auto red_black = [&]() {
+        for (int par = 1; par >= 0; --par) {
+            if (wrap_levels == 1) {
+                wave(0, par, 0, nullptr, 0);
+            } else {
+                for (int l = 0; l < wrap_levels; ++l) wave(0, par, 0, nullptr, 0, l + 1);
+            }
+        }
+    };
     std::vector<std::pair<size_t, size_t>> list_refs;  // (plan index, offset into h_lines_) for kind 2 / seq
     for (int q = 0; q < 4; ++q) {
         const int L = letter(opt.sweep[q]);
-        if (!L) continue;
+        if (!L || noop(L)) continue;
         if (!d0.do_k) {
             if (L == 'R') {  // :382-391, i odd then i even (the kernel flips the 3-D parity)
-                wave(0, 1, 0, nullptr, 0);
-                wave(0, 0, 0, nullptr, 0);
+                red_black();
             } else if (L == 'I') {  // :374-379, i = 1..imax2 in order
                 if (!single) return fail("sweep letter 'I' is served for single-system solves only", -10);
                 for (int dgl = 2; dgl <= d0.imax2 + 1; ++dgl) wave(1, dgl, 1, nullptr, 0);
@@ -727,8 +757,7 @@ int Engine::plan_msolve(const SolveOptions &opt, int src, int dst, int gate, int
             continue;
         }
         if (L == 'R') {  // :497-522, (i+k) odd first
-            wave(0, 1, 0, nullptr, 0);
-            wave(0, 0, 0, nullptr, 0);
+            red_black();
         } else if (L == 'I' || L == 'K') {
             // :567-582: lexicographic line Gauss-Seidel; both orders give the same
             // result, and the lines of one anti-diagonal i+k = const are independent.
@@ -760,10 +789,22 @@ int Engine::plan_msolve(const SolveOptions &opt, int src, int dst, int gate, int
                 std::vector<int> level((size_t)n1 * n2, 0);
                 int maxlev = 0;
                 std::vector<int> lev_of(order.size());
+                // the line's neighbour lines along the two cross axes, wrapped along a
+                // cyclic axis as the increments are (model/set_increments.f:73-113)
+                const int cyc1 = part == 0 ? (d0.cyc & 2) : (d0.cyc & 1);
+                const int cyc2 = part == 1 ? (d0.cyc & 2) : (d0.cyc & 4);
+                auto step = [](int b, int s, int m, int cyc) {  // neighbour of 1-based b in direction s
+                    if (cyc && b >= 2 && b <= m - 1) {
+                        if (s < 0) return b == 2 ? m - 1 : b - 1;
+                        return b == m - 1 ? 2 : b + 1;
+                    }
+                    return b + s;  // out of range: no neighbour line (clamped onto itself)
+                };
                 for (size_t t = 0; t < order.size(); ++t) {
                     const int b1 = order[t].x, b2 = order[t].y;
                     int lv = 0;
-                    const int nb[4][2] = {{b1 - 1, b2}, {b1 + 1, b2}, {b1, b2 - 1}, {b1, b2 + 1}};
+                    const int nb[4][2] = {{step(b1, -1, n1, cyc1), b2}, {step(b1, 1, n1, cyc1), b2},
+                                          {b1, step(b2, -1, n2, cyc2)}, {b1, step(b2, 1, n2, cyc2)}};
                     for (auto &p : nb)
                         if (p[0] >= 1 && p[0] <= n1 && p[1] >= 1 && p[1] <= n2)
                             lv = std::max(lv, level[(size_t)(p[1] - 1) * n1 + (p[0] - 1)]);
@@ -909,8 +950,21 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
     }
     if (opt.pc != PC_LINE && opt.pc != PC_DIAG && opt.pc != PC_NONE) return fail("unknown preconditioner", -10);
 
-    // inputs on the device: the caller's arrays, or copies in the input arena
+    // inputs on the device: the caller's arrays, or copies in the input arena.
+    // DO_TRANSPOSE scales a transposed copy of A_M that SOLVE_LIN_EQ discards
+    // (model/solve_lin_eq.f:139-150): A is scaled in a copy even when it is on the device.
     std::vector<SystemSpec> dev = specs;
+    if (opt.transposed && opt.on_device) {
+        size_t bytes = 4096;
+        for (const auto &s : specs) bytes += align_up(7 * (size_t)s.n * 8, 256);
+        cudaError_t e = in_arena_.reserve(bytes);
+        if (e != cudaSuccess) return fail(std::string("device memory for the copy of A: ") + cudaGetErrorString(e), -11);
+        in_arena_.reset();
+        for (size_t q = 0; q < specs.size(); ++q) {
+            dev[q].a = (double *)in_arena_.take(7 * (size_t)specs[q].n * 8);
+            CK(cudaMemcpyAsync(dev[q].a, specs[q].a, 7 * (size_t)specs[q].n * 8, cudaMemcpyDeviceToDevice, stream_));
+        }
+    }
     if (!opt.on_device) {
         size_t bytes = 4096;
         for (const auto &s : specs) bytes += align_up(7 * (size_t)s.n * 8, 256) + 2 * align_up((size_t)s.n * 8, 256);
@@ -937,7 +991,7 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
     if (!opt.on_device && opt.write_back_ab && opt.method != 3)  // GMRES leaves A and B as they are
         for (size_t q = 0; q < specs.size(); ++q) {
             const size_t n = (size_t)specs[q].n;
-            writeback_.push_back({specs[q].a, dev[q].a, 7 * n * 8});
+            if (!opt.transposed) writeback_.push_back({specs[q].a, dev[q].a, 7 * n * 8});
             writeback_.push_back({specs[q].b, dev[q].b, n * 8});
         }
     // several systems with red/black sweeps: a live batch, which drops systems
@@ -954,6 +1008,7 @@ int Engine::solve(const std::vector<SystemSpec> &specs, const SolveOptions &opt,
         d.jmax2 = dev[0].jmax2;
         d.kmax2 = dev[0].kmax2;
         d.do_k = dev[0].do_k;
+        d.cyc = dev[0].cyc;
         d.n = n;
         d.div_j = make_fastdiv((uint32_t)d.jmax2);
         d.div_i = make_fastdiv((uint32_t)d.imax2);
@@ -1495,6 +1550,7 @@ int Engine::matvec(const SystemSpec &g, const double *a, const double *x, double
     d.jmax2 = g.jmax2;
     d.kmax2 = g.kmax2;
     d.do_k = g.do_k;
+    d.cyc = g.cyc;
     d.n = g.n;
     d.div_j = make_fastdiv((uint32_t)g.jmax2);
     d.div_i = make_fastdiv((uint32_t)g.imax2);

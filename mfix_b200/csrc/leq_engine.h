@@ -20,6 +20,7 @@ enum Precision : int { PREC_FP64 = 0, PREC_MIXED = 1 };
 // One system to solve.  Pointers are host or device memory as the call says.
 struct SystemSpec {
     int imax2 = 0, jmax2 = 0, kmax2 = 0, do_k = 1;
+    int cyc = 0;          // cyclic axes: 1 I (CYCLIC_X), 2 J (CYCLIC_Y), 4 K (CYCLIC_Z)
     int64_t n = 0;
     double *a = nullptr;  // 7*n, A_M(DIMENSION_3,-3:3) layout
     double *b = nullptr;  // n
@@ -64,6 +65,8 @@ struct SolveOptions {
     bool deflate = true;         // mixed form: deflate the near-null mode of systems below mixed_min_margin
                                  // (false: they go straight to the FP64 drop-in)
     int replace_every = 20;      // mixed form, deflated systems: FP64 residual replacement interval (0: off)
+    bool transposed = false;     // DO_TRANSPOSE (model/solve_lin_eq.f:139-150): LEQ_BICGSt's preconditioner
+                                 // letters, and A is scaled in a copy (only B comes back scaled)
     int check_every = 4;         // iterations between host checks of the state
     bool use_graph = true;       // capture the iteration body in a CUDA graph
     bool time_kernels = false;   // record events around every J-line launch (no graph replay)

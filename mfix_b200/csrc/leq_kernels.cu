@@ -94,6 +94,22 @@ __device__ __forceinline__ int64_t natural(const SysDev &d, int64_t p)
     return j < d.jmax2 ? (int64_t)line * d.jmax2 + j : -1;
 }
 
+// Neighbour increments of a serial box (model/set_increments.f:73-113), in cells
+// of one axis: clamped at the array edge, or, along a cyclic axis, wrapping the
+// interior cells 1..m-2 (0-based t, extent m with the wall layer): IP1(I) =
+// IMAP_C(IMAP_C(I)+1) with IMAP_C(IMAX2) = IMIN1 and IMAP_C(IMIN2) = IMAX1
+// (model/dmp_modules/gridmap_mod.f:496-503).
+__device__ __forceinline__ int inc_m(int t, int m, bool cyc)
+{
+    if (cyc && t >= 1 && t <= m - 2) return t == 1 ? m - 3 : -1;
+    return t > 0 ? -1 : 0;
+}
+__device__ __forceinline__ int inc_p(int t, int m, bool cyc)
+{
+    if (cyc && t >= 1 && t <= m - 2) return t == m - 2 ? -(m - 3) : 1;
+    return t < m - 1 ? 1 : 0;
+}
+
 // 7-point product of row c with x, in the operand order of LEQ_MATVEC
 // (model/leqsol_mod.f:240-250), neighbours clamped at the array edge.
 template <typename T, typename TX>
@@ -102,8 +118,8 @@ __device__ __forceinline__ double stencil_row(const SysDev &d, const T *__restri
 {
     const int64_t n = d.n;
     const int64_t c1 = d.jmax2, c2 = (int64_t)d.jmax2 * d.imax2;
-    const int64_t jm = q.j > 0 ? -1 : 0, jp = q.j < d.jmax2 - 1 ? 1 : 0;
-    const int64_t im = q.i > 0 ? -c1 : 0, ip = q.i < d.imax2 - 1 ? c1 : 0;
+    const int64_t jm = inc_m(q.j, d.jmax2, d.cyc & 2), jp = inc_p(q.j, d.jmax2, d.cyc & 2);
+    const int64_t im = inc_m(q.i, d.imax2, d.cyc & 1) * c1, ip = inc_p(q.i, d.imax2, d.cyc & 1) * c1;
     const int64_t p = c;
     using A = typename std::conditional<(sizeof(T) > sizeof(TX)), T, TX>::type;
     A v = (A)a[1 * n + p] * (A)x[p + jm];          // A(-2) * x(j-1)
@@ -112,7 +128,7 @@ __device__ __forceinline__ double stencil_row(const SysDev &d, const T *__restri
     v = v + (A)a[4 * n + p] * (A)x[p + ip];        // A( 1) * x(i+1)
     v = v + (A)a[5 * n + p] * (A)x[p + jp];        // A( 2) * x(j+1)
     if (d.do_k) {
-        const int64_t km = q.k > 0 ? -c2 : 0, kp = q.k < d.kmax2 - 1 ? c2 : 0;
+        const int64_t km = inc_m(q.k, d.kmax2, d.cyc & 4) * c2, kp = inc_p(q.k, d.kmax2, d.cyc & 4) * c2;
         v = v + (A)a[0 * n + p] * (A)x[p + km];    // A(-3) * x(k-1)
         v = v + (A)a[6 * n + p] * (A)x[p + kp];    // A( 3) * x(k+1)
     }
@@ -428,15 +444,15 @@ __global__ void k_defl_setup(BatchView b)
             // cell, z at the padded neighbours (clamped at the array edge)
             const CellIdx q = cell_ijk_t<float>(d, (uint32_t)p);
             const unsigned char *z = d.defl_z;
-            const int64_t jm = q.j > 0 ? -1 : 0, jq = q.j < d.jmax2 - 1 ? 1 : 0;
-            const int64_t im = q.i > 0 ? -c1 : 0, ip = q.i < d.imax2 - 1 ? c1 : 0;
+            const int64_t jm = inc_m(q.j, d.jmax2, d.cyc & 2), jq = inc_p(q.j, d.jmax2, d.cyc & 2);
+            const int64_t im = inc_m(q.i, d.imax2, d.cyc & 1) * c1, ip = inc_p(q.i, d.imax2, d.cyc & 1) * c1;
             double az = d.a64[1 * n + c] * (double)z[p + jm];
             az = az + d.a64[2 * n + c] * (double)z[p + im];
             az = az + d.a64[3 * n + c] * (double)z[p];
             az = az + d.a64[4 * n + c] * (double)z[p + ip];
             az = az + d.a64[5 * n + c] * (double)z[p + jq];
             if (d.do_k) {
-                const int64_t km = q.k > 0 ? -c2 : 0, kp = q.k < d.kmax2 - 1 ? c2 : 0;
+                const int64_t km = inc_m(q.k, d.kmax2, d.cyc & 4) * c2, kp = inc_p(q.k, d.kmax2, d.cyc & 4) * c2;
                 az = az + d.a64[0 * n + c] * (double)z[p + km];
                 az = az + d.a64[6 * n + c] * (double)z[p + kp];
             }
@@ -543,12 +559,12 @@ __device__ __forceinline__ Offs cell_offs(const SysDev &d, uint32_t c, int *jout
     if (jout) *jout = q.j;
     const int64_t c1 = pitch<T>(d), c2 = (int64_t)pitch<T>(d) * d.imax2;
     Offs o;
-    o.jm = q.j > 0 ? -1 : 0;
-    o.jp = q.j < d.jmax2 - 1 ? 1 : 0;
-    o.im = q.i > 0 ? -c1 : 0;
-    o.ip = q.i < d.imax2 - 1 ? c1 : 0;
-    o.km = (d.do_k && q.k > 0) ? -c2 : 0;
-    o.kp = (d.do_k && q.k < d.kmax2 - 1) ? c2 : 0;
+    o.jm = inc_m(q.j, d.jmax2, d.cyc & 2);
+    o.jp = inc_p(q.j, d.jmax2, d.cyc & 2);
+    o.im = inc_m(q.i, d.imax2, d.cyc & 1) * c1;
+    o.ip = inc_p(q.i, d.imax2, d.cyc & 1) * c1;
+    o.km = d.do_k ? inc_m(q.k, d.kmax2, d.cyc & 4) * c2 : 0;
+    o.kp = d.do_k ? inc_p(q.k, d.kmax2, d.cyc & 4) * c2 : 0;
     return o;
 }
 
@@ -677,12 +693,15 @@ __device__ __forceinline__ void load_pair7(const SysDev &d, const T *__restrict_
     const CellIdx q = cell_ijk_t<T>(d, (uint32_t)c);
     if (jout) *jout = q.j;
     const int64_t c1 = pitch<T>(d), c2 = (int64_t)pitch<T>(d) * d.imax2;
-    const int64_t im = q.i > 0 ? -c1 : 0, ip = q.i < d.imax2 - 1 ? c1 : 0;
+    const int64_t im = inc_m(q.i, d.imax2, d.cyc & 1) * c1, ip = inc_p(q.i, d.imax2, d.cyc & 1) * c1;
     const vec2_t<T> xc = ld2(X + c);
-    const T xl = X[c + (q.j > 0 ? -1 : 0)];              // x(j-1) of cell c (clamped)
-    const T xr = X[c + 1 + (q.j + 1 < d.jmax2 - 1 ? 1 : 0)];  // x(j+1) of cell c+1 (clamped)
+    // x(j-1) of cell c and x(j+1) of cell c+1 (the pair's own cells otherwise);
+    // along a cyclic J both cells' J neighbours may wrap
+    const bool cj = (d.cyc & 2) != 0;
+    const T xl = X[c + inc_m(q.j, d.jmax2, cj)];
+    const T xr = X[c + 1 + inc_p(q.j + 1, d.jmax2, cj)];
     r.a[0] = ld2(A + 1 * n + c);
-    r.x[0] = mk2<T>(xl, xc.x);
+    r.x[0] = mk2<T>(xl, cj ? X[c + 1 + inc_m(q.j + 1, d.jmax2, true)] : xc.x);
     r.a[1] = ld2(A + 2 * n + c);
     r.x[1] = ld2(X + c + im);
     if constexpr (DEFECT)
@@ -693,9 +712,9 @@ __device__ __forceinline__ void load_pair7(const SysDev &d, const T *__restrict_
     r.a[3] = ld2(A + 4 * n + c);
     r.x[3] = ld2(X + c + ip);
     r.a[4] = ld2(A + 5 * n + c);
-    r.x[4] = mk2<T>(xc.y, xr);
+    r.x[4] = mk2<T>(cj ? X[c + inc_p(q.j, d.jmax2, true)] : xc.y, xr);
     if (d.do_k) {
-        const int64_t km = q.k > 0 ? -c2 : 0, kp = q.k < d.kmax2 - 1 ? c2 : 0;
+        const int64_t km = inc_m(q.k, d.kmax2, d.cyc & 4) * c2, kp = inc_p(q.k, d.kmax2, d.cyc & 4) * c2;
         r.a[5] = ld2(A + 0 * n + c);
         r.x[5] = ld2(X + c + km);
         r.a[6] = ld2(A + 6 * n + c);
@@ -1665,6 +1684,7 @@ __device__ __forceinline__ bool next_line_job(const BatchView &b, const WaveArgs
             const int i0 = (((1 + j.k) & 1) == par) ? 1 : 2;
             j.i = i0 + 2 * slot;
             j.valid = (j.k <= d.kmax2) && (j.i <= d.imax2);
+            if (w.lvl > 0 && j.valid) j.valid = wrap_level(d, j.i, j.k) == w.lvl - 1;
         } else if (w.kind == 1) {
             const int ilo = max(1, w.par - d.kmax2), ihi = min(d.imax2, w.par - 1);
             j.i = ilo + q;
@@ -1698,10 +1718,14 @@ __device__ __forceinline__ LineCtx<T> line_ctx(const BatchView &b, const WaveArg
     x.do_k = d.do_k;
     x.base = j.base;
     const T *nbr = vec<T>(d, w.nbr), *old = vec<T>(d, w.old);
-    x.nb_im = (j.i > 1) ? nbr + x.base - c1 : old + x.base;
-    x.nb_ip = (j.i < d.imax2) ? nbr + x.base + c1 : old + x.base;
-    x.nb_km = (j.k > 1) ? nbr + x.base - c2 : old + x.base;
-    x.nb_kp = (j.k < d.kmax2) ? nbr + x.base + c2 : old + x.base;
+    // the I and K neighbour lines (clamped onto the line itself at the array
+    // edge, wrapped along a cyclic axis)
+    const int im = inc_m(j.i - 1, d.imax2, d.cyc & 1), ip = inc_p(j.i - 1, d.imax2, d.cyc & 1);
+    const int km = inc_m(j.k - 1, d.kmax2, d.cyc & 4), kp = inc_p(j.k - 1, d.kmax2, d.cyc & 4);
+    x.nb_im = im ? nbr + x.base + im * c1 : old + x.base;
+    x.nb_ip = ip ? nbr + x.base + ip * c1 : old + x.base;
+    x.nb_km = km ? nbr + x.base + km * c2 : old + x.base;
+    x.nb_kp = kp ? nbr + x.base + kp * c2 : old + x.base;
     return x;
 }
 
@@ -2157,12 +2181,12 @@ __global__ void k_seq_lines(BatchView b, SeqLineArgs a)
         auto nb = [&](int dd) -> T {
             int64_t o = 0;
             switch (dd) {
-            case 0: o = kk > 0 ? -c2 : 0; break;
-            case 1: o = jj > 0 ? -1 : 0; break;
-            case 2: o = ii > 0 ? -c1 : 0; break;
-            case 4: o = ii < d.imax2 - 1 ? c1 : 0; break;
-            case 5: o = jj < d.jmax2 - 1 ? 1 : 0; break;
-            case 6: o = kk < d.kmax2 - 1 ? c2 : 0; break;
+            case 0: o = inc_m(kk, d.kmax2, d.cyc & 4) * c2; break;
+            case 1: o = inc_m(jj, d.jmax2, d.cyc & 2); break;
+            case 2: o = inc_m(ii, d.imax2, d.cyc & 1) * c1; break;
+            case 4: o = inc_p(ii, d.imax2, d.cyc & 1) * c1; break;
+            case 5: o = inc_p(jj, d.jmax2, d.cyc & 2); break;
+            case 6: o = inc_p(kk, d.kmax2, d.cyc & 4) * c2; break;
             }
             return var[p + o];
         };

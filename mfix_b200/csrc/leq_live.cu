@@ -147,6 +147,7 @@ int Engine::live_add(const LiveSystem &ls)
     d.jmax2 = sp.jmax2;
     d.kmax2 = sp.kmax2;
     d.do_k = sp.do_k;
+    d.cyc = sp.cyc;
     d.n = sp.n;
     d.div_j = make_fastdiv((uint32_t)sp.jmax2);
     d.div_i = make_fastdiv((uint32_t)sp.imax2);

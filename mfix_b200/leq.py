@@ -39,7 +39,7 @@ class Stats(C.Structure):
 
 class Geom(C.Structure):
     _fields_ = [("imax2", C.c_int), ("jmax2", C.c_int), ("kmax2", C.c_int), ("do_k", C.c_int),
-                ("dimension_3", C.c_int64)]
+                ("dimension_3", C.c_int64), ("cyclic", C.c_int), ("pad", C.c_int)]
 
 
 class SystemC(C.Structure):
@@ -156,6 +156,8 @@ def _declare(L: C.CDLL) -> None:
     L.mfixgpu_server_destroy.restype = C.c_int
     L.mfixgpu_init_geometry.argtypes = [_ip, _ip, _ip, _ip, C.POINTER(C.c_int64), _ip]
     L.mfixgpu_init_geometry.restype = C.c_int
+    L.mfixgpu_init_cyclic.argtypes = [_ip, _ip, _ip]
+    L.mfixgpu_init_cyclic.restype = C.c_int
     L.mfixgpu_solve_lin_eq_.argtypes = [C.c_char_p, _ip, C.c_void_p, C.c_void_p, C.c_void_p, _ip, _ip, _ip,
                                         C.c_char_p, _dp, C.c_char_p, _ip, C.c_size_t, C.c_size_t, C.c_size_t]
     L.mfixgpu_solve_lin_eq_.restype = None
@@ -315,8 +317,14 @@ def autotune_table() -> list[tuple[int, int, int]]:
     return [(buf[3 * q], buf[3 * q + 1], buf[3 * q + 2]) for q in range(n)]
 
 
-def geom(imax2: int, jmax2: int, kmax2: int, do_k: int) -> Geom:
-    return Geom(imax2, jmax2, kmax2, do_k, imax2 * jmax2 * kmax2)
+def geom(imax2: int, jmax2: int, kmax2: int, do_k: int, cyclic: int = 0) -> Geom:
+    return Geom(imax2, jmax2, kmax2, do_k, imax2 * jmax2 * kmax2, cyclic, 0)
+
+
+def init_cyclic(cyclic_x: bool, cyclic_y: bool, cyclic_z: bool) -> int:
+    """mfixgpu_init_cyclic: CYCLIC_X/Y/Z of the registered geometry."""
+    return lib().mfixgpu_init_cyclic(C.byref(C.c_int(int(cyclic_x))), C.byref(C.c_int(int(cyclic_y))),
+                                     C.byref(C.c_int(int(cyclic_z))))
 
 
 def leq_matvec(g: Geom, a_dev: int, var_dev: int, avar_dev: int) -> int:
@@ -382,6 +390,9 @@ def batch_solve(systems, sweep: str = "RSRS", pc: str = "LINE", precision: int =
 def solve_system(s, method: int = 2, sweep: str = "RSRS", pc: str = "LINE", vno: int = 1) -> int:
     """Drop-in solve of one :class:`mfix_b200.systems.System` (in place)."""
     rc = init_geometry(s.imax2, s.jmax2, s.kmax2, s.do_k, s.n, 0)
+    cyc = getattr(s, "cyc", 0)
+    if not rc and cyc:
+        rc = init_cyclic(cyc & 1, cyc & 2, cyc & 4)
     if rc:
         return rc
     return solve_lin_eq("Test", vno, s.x, s.a, s.b, 0, s.itmax, method, sweep, s.tol, pc)

@@ -68,6 +68,7 @@ class System:
     tol: float = 1e-8
     itmax: int = 500
     kind: str = ""
+    cyc: int = 0  # cyclic axes: 1 X (I), 2 Y (J), 4 Z (K)
 
     @property
     def n(self) -> int:
@@ -75,7 +76,7 @@ class System:
 
     def copy(self) -> "System":
         return System(self.imax2, self.jmax2, self.kmax2, self.do_k, self.a.copy(), self.b.copy(),
-                      self.x.copy(), self.tol, self.itmax, self.kind)
+                      self.x.copy(), self.tol, self.itmax, self.kind, self.cyc)
 
 
 def _grid(imax: int, jmax: int, kmax: int, do_k: bool):
@@ -244,15 +245,29 @@ def known_answer(imax: int, jmax: int, kmax: int, seed: int = 0, do_k: bool = Tr
     return System(imax2, jmax2, kmax2, int(do_k), a, b, np.zeros(n), 1e-10, 500, "known_answer"), x_act
 
 
-def matvec_np(imax2, jmax2, kmax2, do_k, a, x):
-    """A*x with the clamped neighbours of LEQ_MATVEC (numpy, any size)."""
+def neighbour_index(m: int, s: int, cyclic: bool) -> np.ndarray:
+    """0-based index of each cell's neighbour s = -1 / +1 along an axis of extent m:
+    clamped at the array edge (model/set_increments.f:80-109), or, along a cyclic
+    axis, the interior cells 1..m-2 wrapping onto each other (IMAP_C(IMAX2) = IMIN1,
+    IMAP_C(IMIN2) = IMAX1, model/dmp_modules/gridmap_mod.f:496-503)."""
+    idx = np.arange(m)
+    src = np.clip(idx + s, 0, m - 1)
+    if cyclic and m >= 3:
+        inner = (idx >= 1) & (idx <= m - 2)
+        wrapped = 1 + (idx - 1 + s) % (m - 2)
+        src = np.where(inner, wrapped, src)
+    return src
+
+
+def matvec_np(imax2, jmax2, kmax2, do_k, a, x, cyc: int = 0):
+    """A*x with the neighbours of LEQ_MATVEC (numpy, any size); cyc: cyclic axes
+    (1 I, 2 J, 4 K)."""
     shape = (kmax2, imax2, jmax2)
     X = x.reshape(shape)
+    bit = {0: 4, 1: 1, 2: 2}  # numpy axis -> cyclic bit
 
     def shift(ax, s):
-        idx = np.arange(shape[ax])
-        src = np.clip(idx + s, 0, shape[ax] - 1)
-        return np.take(X, src, axis=ax)
+        return np.take(X, neighbour_index(shape[ax], s, bool(cyc & bit[ax])), axis=ax)
 
     A = a.reshape(7, *shape)
     y = A[1] * shift(2, -1) + A[2] * shift(1, -1) + A[3] * X + A[4] * shift(1, 1) + A[5] * shift(2, 1)
@@ -413,3 +428,42 @@ def pp_fields(imax: int, jmax: int, kmax: int, seed: int = 0, do_k: bool = True,
         rop_s=u(322, 0.1, 0.3, mmax) if sol else None, rop_so=u(323, 0.1, 0.3, mmax) if sol else None,
         sum_r_s=u(324, -0.001, 0.001, mmax) if sol else None,
         odt=1.0 / dt, ijk_p_g=int(ijk_p_g))
+
+
+def conv_diff_cyclic(imax: int, jmax: int, kmax: int, seed: int = 0, cyc: int = 1, do_k: bool = True,
+                     itmax: int = 500, tol: float = 1e-8) -> System:
+    """conv_diff with periodic faces along the cyclic axes `cyc` (1 I, 2 J, 4 K):
+    the face between the last and the first interior cell of each line along
+    such an axis gets the same upwind coefficients as any interior face (row of
+    the last cell: its + diagonal; row of the first: its - diagonal), as the
+    neighbour increments of a cyclic run (model/set_increments.f:73-113) couple
+    them.  The centre is recomputed with the (1 + 1e-3) excess."""
+    s = conv_diff(imax, jmax, kmax, seed=seed, do_k=do_k, itmax=itmax, tol=tol)
+    s.cyc = cyc
+    imax2, jmax2, kmax2 = s.imax2, s.jmax2, s.kmax2
+    shape = (kmax2, imax2, jmax2)
+    a = s.a
+    inter = _interior(imax2, jmax2, kmax2, do_k)
+    flat = np.arange(s.n, dtype=np.int64).reshape(shape)
+    axes = [(0, 1, 1, -1, 1), (1, 2, 2, -2, 2)]
+    if do_k:
+        axes.append((2, 0, 3, -3, 4))
+    for axis, npax, d_low, d_high, bit in axes:
+        if not (cyc & bit) or shape[npax] < 4:
+            continue
+        last = [slice(None)] * 3
+        first = [slice(None)] * 3
+        last[npax] = shape[npax] - 2
+        first[npax] = 1
+        m_last, m_first = inter[tuple(last)], inter[tuple(first)]
+        lo = flat[tuple(last)][m_last]
+        hi = flat[tuple(first)][m_first]
+        D = 0.5 + uniform(seed, 60 + 4 * axis, lo)
+        F = normal(seed, 61 + 4 * axis, lo, 0.5)
+        a[d_low + 3][lo] = D + np.maximum(-F, 0.0)
+        a[d_high + 3][hi] = D + np.maximum(F, 0.0)
+    wall = ~inter.reshape(-1)
+    off = a[[0, 1, 2, 4, 5, 6]].sum(axis=0)
+    a[3] = np.where(wall, -1.0, -off * (1.0 + 1e-3))
+    s.kind = "conv_diff_cyclic"
+    return s

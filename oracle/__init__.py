@@ -21,7 +21,8 @@ _dp = C.POINTER(C.c_double)
 
 
 class Geom(C.Structure):
-    _fields_ = [("imax2", C.c_int), ("jmax2", C.c_int), ("kmax2", C.c_int), ("do_k", C.c_int), ("n", C.c_int64)]
+    _fields_ = [("imax2", C.c_int), ("jmax2", C.c_int), ("kmax2", C.c_int), ("do_k", C.c_int), ("n", C.c_int64),
+                ("cyclic", C.c_int), ("pad", C.c_int)]
 
 
 class Stats(C.Structure):
@@ -71,6 +72,11 @@ def lib() -> C.CDLL:
         L.orc_truth_refine.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_double, C.c_double, C.c_int, C.c_uint64, _dp]
         L.orc_truth_refine.restype = C.c_int
         L.orc_num_threads.restype = C.c_int
+        L.orc_leq_bicgst.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_char_p, C.c_double, C.c_char_p, C.c_int,
+                                     C.c_uint64, C.POINTER(Stats)]
+        L.orc_leq_bicgst.restype = C.c_int
+        L.orc_msolve_t.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_char_p, C.POINTER(C.c_int)]
+        L.orc_msolve_t.restype = C.c_int
         L.orc_conv_source_pp_g.argtypes = [C.POINTER(Geom), C.c_void_p, vp, vp, vp]
         L.orc_calc_resid_pp.argtypes = [C.POINTER(Geom), vp, vp, C.c_double]
         L.orc_calc_resid_pp.restype = C.c_double
@@ -84,7 +90,7 @@ def _p(a: np.ndarray) -> int:
 
 
 def geom(s) -> Geom:
-    return Geom(s.imax2, s.jmax2, s.kmax2, s.do_k, s.n)
+    return Geom(s.imax2, s.jmax2, s.kmax2, s.do_k, s.n, getattr(s, "cyc", 0), 0)
 
 
 def matvec(s, x: np.ndarray, a: np.ndarray | None = None) -> np.ndarray:
@@ -144,6 +150,22 @@ def leq_bicgs(s, sweep: str = "RSRS", pc: str = "LINE", seed: int = 0x5EED, max_
         lib().orc_leq_bicgs_sample(C.byref(geom(s)), _p(s.x), _p(s.a), _p(s.b), sw, s.tol, pcs, s.itmax, seed,
                                    max_exec, C.byref(st))
     return {k: getattr(st, k) for k, _ in Stats._fields_}
+
+
+def leq_bicgst(s, sweep: str = "RSRS", pc: str = "LINE", seed: int = 0x5EED) -> dict:
+    """LEQ_BICGSt (DO_TRANSPOSE) on s: s.x solution, s.b scaled, s.a left as given."""
+    st = Stats()
+    lib().orc_leq_bicgst(C.byref(geom(s)), _p(s.x), _p(s.a), _p(s.b), sweep.ljust(4)[:4].encode(), s.tol,
+                         pc.ljust(4)[:4].encode(), s.itmax, seed, C.byref(st))
+    return {k: getattr(st, k) for k, _ in Stats._fields_}
+
+
+def msolve_t(s, b: np.ndarray, sweep: str = "RSRS", a: np.ndarray | None = None) -> np.ndarray:
+    """LEQ_MSOLVEt on s's (scaled) A: var = M^{-1} b."""
+    var = np.zeros(s.n)
+    lib().orc_msolve_t(C.byref(geom(s)), _p(b), _p(s.a if a is None else a), _p(var), sweep.ljust(4)[:4].encode(),
+                       None)
+    return var
 
 
 def leq_cg(s, sweep: str = "RSRS", pc: str = "LINE") -> dict:

@@ -29,6 +29,26 @@ static inline int64_t cell(const orc_geom *g, int i, int j, int k)
     return (int64_t)(j - 1) + (int64_t)(i - 1) * g->jmax2 + (int64_t)(k - 1) * g->jmax2 * g->imax2;
 }
 
+/* Neighbour increments of a serial box (model/set_increments.f:73-113): clamped at
+ * the array edge (IM1(I) = MAX(ISTART3, I-1)), or, along a cyclic axis, wrapping
+ * the interior cells 2..m-1 (IP1(I) = IMAP_C(IMAP_C(I)+1), with IMAP_C(IMAX2) =
+ * IMIN1 and IMAP_C(IMIN2) = IMAX1, model/dmp_modules/gridmap_mod.f:496-503).  t is
+ * 1-based, m the extent including the wall layer; the result is in cells of
+ * that axis. */
+static inline int64_t inc_m(int t, int m, int cyc)
+{
+    if (cyc && t >= 2 && t <= m - 1) return t == 2 ? (int64_t)(m - 3) : -1;
+    return t > 1 ? -1 : 0;
+}
+static inline int64_t inc_p(int t, int m, int cyc)
+{
+    if (cyc && t >= 2 && t <= m - 1) return t == m - 1 ? -(int64_t)(m - 3) : 1;
+    return t < m ? 1 : 0;
+}
+#define CYC_X(g) (((g)->cyclic & 1) != 0)
+#define CYC_Y(g) (((g)->cyclic & 2) != 0)
+#define CYC_Z(g) (((g)->cyclic & 4) != 0)
+
 int orc_num_threads(void)
 {
 #ifdef _OPENMP
@@ -69,12 +89,12 @@ void orc_matvec(const orc_geom *g, const double *a, const double *x, double *y)
 #pragma omp parallel for collapse(2) schedule(static)
     for (int k = 1; k <= kmax2; ++k) {
         for (int i = 1; i <= imax2; ++i) {
-            const int64_t im = i > 1 ? -c1 : 0, ip = i < imax2 ? c1 : 0;
-            const int64_t km = (do_k && k > 1) ? -c2 : 0, kp = (do_k && k < kmax2) ? c2 : 0;
+            const int64_t im = inc_m(i, imax2, CYC_X(g)) * c1, ip = inc_p(i, imax2, CYC_X(g)) * c1;
+            const int64_t km = do_k ? inc_m(k, kmax2, CYC_Z(g)) * c2 : 0, kp = do_k ? inc_p(k, kmax2, CYC_Z(g)) * c2 : 0;
             const int64_t base = cell(g, i, 1, k);
             for (int j = 1; j <= jmax2; ++j) {
                 const int64_t p = base + (j - 1);
-                const int64_t jm = j > 1 ? -1 : 0, jp = j < jmax2 ? 1 : 0;
+                const int64_t jm = inc_m(j, jmax2, CYC_Y(g)), jp = inc_p(j, jmax2, CYC_Y(g));
                 double s = am2[p] * x[p + jm] + am1[p] * x[p + im] + a0[p] * x[p] + ap1[p] * x[p + ip] +
                            ap2[p] * x[p + jp];
                 if (do_k) {
@@ -164,8 +184,8 @@ int orc_iksweep(const orc_geom *g, int i, int k, double *var, const double *a, c
 {
     const int L = g->jmax2;
     const int64_t c1 = g->jmax2, c2 = (int64_t)g->jmax2 * g->imax2;
-    const int64_t im = i > 1 ? -c1 : 0, ip = i < g->imax2 ? c1 : 0;
-    const int64_t km = k > 1 ? -c2 : 0, kp = k < g->kmax2 ? c2 : 0;
+    const int64_t im = inc_m(i, g->imax2, CYC_X(g)) * c1, ip = inc_p(i, g->imax2, CYC_X(g)) * c1;
+    const int64_t km = inc_m(k, g->kmax2, CYC_Z(g)) * c2, kp = inc_p(k, g->kmax2, CYC_Z(g)) * c2;
     const double *am3 = DIAG(a, g, -3), *am2 = DIAG(a, g, -2), *am1 = DIAG(a, g, -1);
     const double *a0 = DIAG(a, g, 0), *ap1 = DIAG(a, g, 1), *ap2 = DIAG(a, g, 2), *ap3 = DIAG(a, g, 3);
     double *buf = (double *)malloc(sizeof(double) * 4 * (size_t)(L + 1));
@@ -192,7 +212,7 @@ int orc_isweep(const orc_geom *g, int i, double *var, const double *a, const dou
 {
     const int L = g->jmax2;
     const int64_t c1 = g->jmax2;
-    const int64_t im = i > 1 ? -c1 : 0, ip = i < g->imax2 ? c1 : 0;
+    const int64_t im = inc_m(i, g->imax2, CYC_X(g)) * c1, ip = inc_p(i, g->imax2, CYC_X(g)) * c1;
     const double *am2 = DIAG(a, g, -2), *am1 = DIAG(a, g, -1);
     const double *a0 = DIAG(a, g, 0), *ap1 = DIAG(a, g, 1), *ap2 = DIAG(a, g, 2);
     double *buf = (double *)malloc(sizeof(double) * 4 * (size_t)(L + 1));
@@ -219,8 +239,8 @@ int orc_jksweep(const orc_geom *g, int j, int k, double *var, const double *a, c
 {
     const int L = g->imax2;
     const int64_t c1 = g->jmax2, c2 = (int64_t)g->jmax2 * g->imax2;
-    const int64_t jm = j > 1 ? -1 : 0, jp = j < g->jmax2 ? 1 : 0;
-    const int64_t km = k > 1 ? -c2 : 0, kp = k < g->kmax2 ? c2 : 0;
+    const int64_t jm = inc_m(j, g->jmax2, CYC_Y(g)), jp = inc_p(j, g->jmax2, CYC_Y(g));
+    const int64_t km = inc_m(k, g->kmax2, CYC_Z(g)) * c2, kp = inc_p(k, g->kmax2, CYC_Z(g)) * c2;
     const double *am3 = DIAG(a, g, -3), *am2 = DIAG(a, g, -2), *am1 = DIAG(a, g, -1);
     const double *a0 = DIAG(a, g, 0), *ap1 = DIAG(a, g, 1), *ap2 = DIAG(a, g, 2), *ap3 = DIAG(a, g, 3);
     double *buf = (double *)malloc(sizeof(double) * 4 * (size_t)(L + 1));
@@ -247,8 +267,8 @@ int orc_ijsweep(const orc_geom *g, int i, int j, double *var, const double *a, c
 {
     const int L = g->kmax2;
     const int64_t c1 = g->jmax2;
-    const int64_t jm = j > 1 ? -1 : 0, jp = j < g->jmax2 ? 1 : 0;
-    const int64_t im = i > 1 ? -c1 : 0, ip = i < g->imax2 ? c1 : 0;
+    const int64_t jm = inc_m(j, g->jmax2, CYC_Y(g)), jp = inc_p(j, g->jmax2, CYC_Y(g));
+    const int64_t im = inc_m(i, g->imax2, CYC_X(g)) * c1, ip = inc_p(i, g->imax2, CYC_X(g)) * c1;
     const double *am3 = DIAG(a, g, -3), *am2 = DIAG(a, g, -2), *am1 = DIAG(a, g, -1);
     const double *a0 = DIAG(a, g, 0), *ap1 = DIAG(a, g, 1), *ap2 = DIAG(a, g, 2), *ap3 = DIAG(a, g, 3);
     double *buf = (double *)malloc(sizeof(double) * 4 * (size_t)(L + 1));
@@ -290,10 +310,13 @@ int orc_msolve(const orc_geom *g, const double *b, const double *a, double *var,
             if (do_i)
                 for (int i = 1; i <= g->imax2; ++i) nskip += orc_isweep(g, i, var, a, b) != 0;
             if (do_rb) {
+                /* an odd number of cyclic interior cells puts the wrapped lines in one
+                 * colour: the serial loop order then decides what each one reads */
+                const int par_ok = !(CYC_X(g) && ((g->imax2 - 2) & 1));
                 int s1 = 0, s2 = 0;
-#pragma omp parallel for reduction(+ : s1) schedule(static)
+#pragma omp parallel for reduction(+ : s1) schedule(static) if (par_ok)
                 for (int i = 1; i <= g->imax2; i += 2) s1 += orc_isweep(g, i, var, a, b) != 0;
-#pragma omp parallel for reduction(+ : s2) schedule(static)
+#pragma omp parallel for reduction(+ : s2) schedule(static) if (par_ok)
                 for (int i = 2; i <= g->imax2; i += 2) s2 += orc_isweep(g, i, var, a, b) != 0;
                 nskip += s1 + s2;
             }
@@ -326,11 +349,14 @@ int orc_msolve(const orc_geom *g, const double *b, const double *a, double *var,
         }
         if (do_rb) {
             /* :497-522: first the lines with (i+k) odd, then (i+k) even */
+            /* the I wrap stays inside one k iteration; the K wrap of an odd number of
+             * cyclic interior cells joins two k iterations of one colour */
+            const int par_ok = !(CYC_Z(g) && ((g->kmax2 - 2) & 1));
             int s1 = 0, s2 = 0;
-#pragma omp parallel for reduction(+ : s1) schedule(static)
+#pragma omp parallel for reduction(+ : s1) schedule(static) if (par_ok)
             for (int k = 1; k <= g->kmax2; ++k)
                 for (int i = (k % 2 != 0) ? 2 : 1; i <= g->imax2; i += 2) s1 += orc_iksweep(g, i, k, var, a, b) != 0;
-#pragma omp parallel for reduction(+ : s2) schedule(static)
+#pragma omp parallel for reduction(+ : s2) schedule(static) if (par_ok)
             for (int k = 1; k <= g->kmax2; ++k)
                 for (int i = (k % 2 != 0) ? 1 : 2; i <= g->imax2; i += 2) s2 += orc_iksweep(g, i, k, var, a, b) != 0;
             nskip += s1 + s2;
@@ -408,8 +434,21 @@ static int pc_mode(const char *pc)
     return -1;
 }
 
+static int msolve_t(const orc_geom *g, const double *b, const double *a, double *var, const char *sweep, int *skips);
+
+/* transposed: LEQ_BICGS0t (model/leq_bicgst.f:102-627), whose scaling has no zero-row
+ * test (:214-229) and whose preconditioner is LEQ_MSOLVEt */
+static int bicgs_run_x(const orc_geom *g, double *var, double *a, double *b, const char *sweep, double tol,
+                       const char *pc, int itmax, uint64_t rt_seed, int max_exec, orc_stats *st, int transposed);
+
 static int bicgs_run(const orc_geom *g, double *var, double *a, double *b, const char *sweep, double tol,
                      const char *pc, int itmax, uint64_t rt_seed, int max_exec, orc_stats *st)
+{
+    return bicgs_run_x(g, var, a, b, sweep, tol, pc, itmax, rt_seed, max_exec, st, 0);
+}
+
+static int bicgs_run_x(const orc_geom *g, double *var, double *a, double *b, const char *sweep, double tol,
+                       const char *pc, int itmax, uint64_t rt_seed, int max_exec, orc_stats *st, int transposed)
 {
     memset(st, 0, sizeof(*st));
     st->exit_kind = -1;
@@ -419,7 +458,17 @@ static int bicgs_run(const orc_geom *g, double *var, double *a, double *b, const
         return -10;
     }
     const int64_t n = g->n;
-    if (orc_scale(g, a, b) != 0) {
+    if (transposed) {
+#pragma omp parallel for schedule(static)
+        for (int64_t p = 0; p < g->n; ++p) {
+            double m = 0.0;
+            for (int q = 0; q < 7; ++q)
+                if (fabs(a[q * g->n + p]) > m) m = fabs(a[q * g->n + p]);
+            const double oam = 1.0 / m;
+            for (int q = 0; q < 7; ++q) a[q * g->n + p] = a[q * g->n + p] * oam;
+            b[p] = b[p] * oam;
+        }
+    } else if (orc_scale(g, a, b) != 0) {
         st->ier = -2;
         st->exit_kind = 4;
         return -2;
@@ -463,7 +512,8 @@ static int bicgs_run(const orc_geom *g, double *var, double *a, double *b, const
         }
         const double *Ph = P;
         if (mode == 2) {
-            if (orc_msolve(g, P, a, Pp, sweep, &st->line_info_skips) != 0) { ier = -12; break; }
+            if ((transposed ? msolve_t(g, P, a, Pp, sweep, &st->line_info_skips)
+                            : orc_msolve(g, P, a, Pp, sweep, &st->line_info_skips)) != 0) { ier = -12; break; }
             Ph = Pp;
         } else if (mode == 1) {
             orc_msolve1(g, P, a, Pp);
@@ -484,7 +534,8 @@ static int bicgs_run(const orc_geom *g, double *var, double *a, double *b, const
         }
         const double *Sh = S;
         if (mode == 2) {
-            if (orc_msolve(g, S, a, Sp, sweep, &st->line_info_skips) != 0) { ier = -12; break; }
+            if ((transposed ? msolve_t(g, S, a, Sp, sweep, &st->line_info_skips)
+                            : orc_msolve(g, S, a, Sp, sweep, &st->line_info_skips)) != 0) { ier = -12; break; }
             Sh = Sp;
         } else if (mode == 1) {
             orc_msolve1(g, S, a, Sp);
@@ -558,12 +609,13 @@ double orc_true_resid(const orc_geom *g, const double *a, const double *b, const
 #pragma omp parallel for collapse(2) reduction(+ : tot) schedule(static)
     for (int k = 1; k <= g->kmax2; ++k)
         for (int i = 1; i <= g->imax2; ++i) {
-            const int64_t im = i > 1 ? -c1 : 0, ip = i < g->imax2 ? c1 : 0;
-            const int64_t km = (g->do_k && k > 1) ? -c2 : 0, kp = (g->do_k && k < g->kmax2) ? c2 : 0;
+            const int64_t im = inc_m(i, g->imax2, CYC_X(g)) * c1, ip = inc_p(i, g->imax2, CYC_X(g)) * c1;
+            const int64_t km = g->do_k ? inc_m(k, g->kmax2, CYC_Z(g)) * c2 : 0;
+            const int64_t kp = g->do_k ? inc_p(k, g->kmax2, CYC_Z(g)) * c2 : 0;
             const int64_t base = cell(g, i, 1, k);
             for (int j = 1; j <= g->jmax2; ++j) {
                 const int64_t p = base + j - 1;
-                const int64_t jm = j > 1 ? -1 : 0, jp = j < g->jmax2 ? 1 : 0;
+                const int64_t jm = inc_m(j, g->jmax2, CYC_Y(g)), jp = inc_p(j, g->jmax2, CYC_Y(g));
                 long double s = (long double)am2[p] * x[p + jm] + (long double)am1[p] * x[p + im] +
                                 (long double)a0[p] * x[p] + (long double)ap1[p] * x[p + ip] +
                                 (long double)ap2[p] * x[p + jp];
@@ -583,12 +635,13 @@ static void true_resid_vec(const orc_geom *g, const double *a, const double *b, 
 #pragma omp parallel for collapse(2) schedule(static)
     for (int k = 1; k <= g->kmax2; ++k)
         for (int i = 1; i <= g->imax2; ++i) {
-            const int64_t im = i > 1 ? -c1 : 0, ip = i < g->imax2 ? c1 : 0;
-            const int64_t km = (g->do_k && k > 1) ? -c2 : 0, kp = (g->do_k && k < g->kmax2) ? c2 : 0;
+            const int64_t im = inc_m(i, g->imax2, CYC_X(g)) * c1, ip = inc_p(i, g->imax2, CYC_X(g)) * c1;
+            const int64_t km = g->do_k ? inc_m(k, g->kmax2, CYC_Z(g)) * c2 : 0;
+            const int64_t kp = g->do_k ? inc_p(k, g->kmax2, CYC_Z(g)) * c2 : 0;
             const int64_t base = cell(g, i, 1, k);
             for (int j = 1; j <= g->jmax2; ++j) {
                 const int64_t p = base + j - 1;
-                const int64_t jm = j > 1 ? -1 : 0, jp = j < g->jmax2 ? 1 : 0;
+                const int64_t jm = inc_m(j, g->jmax2, CYC_Y(g)), jp = inc_p(j, g->jmax2, CYC_Y(g));
                 long double s = (long double)am2[p] * x[p + jm] + (long double)am1[p] * x[p + im] +
                                 (long double)a0[p] * x[p] + (long double)ap1[p] * x[p + ip] +
                                 (long double)ap2[p] * x[p + jp];
@@ -1101,4 +1154,60 @@ double orc_calc_resid_pp(const orc_geom *g, const int *flag, const double *b, do
     if (den * norm > 0.0) return num / (den * norm);
     if (num == 0.0) return 0.0;
     return 1.0e32; /* LARGE_NUMBER */
+}
+
+/* ------------------------------------------------------------------ DO_TRANSPOSE: LEQ_BICGSt */
+/* LEQ_MSOLVEt (model/leq_bicgst.f:978-1177): SETGUESS, then per letter: in 2-D
+ * only I (LEQ_ISWEEPt over i in order); in 3-D R in the loop order of
+ * :1040-1061 (two passes over ik = icase, icase+2, ...; i wraps within the row
+ * when the row length is odd), I (k outer, i inner) and K (i outer, k inner).
+ * A, J and S do nothing.  The line solves are LEQ_IKSWEEP's / LEQ_ISWEEP's on the
+ * transposed copy, the same values. */
+static int msolve_t(const orc_geom *g, const double *b, const double *a, double *var, const char *sweep, int *skips)
+{
+    int nskip = 0;
+    memcpy(var, b, sizeof(double) * (size_t)g->n);
+    for (int it = 0; it < 4; ++it) {
+        const char ch = sweep[it];
+        const int do_i = (ch == 'I' || ch == 'i'), do_kk = (ch == 'K' || ch == 'k'), do_rb = (ch == 'R' || ch == 'r');
+        if (!g->do_k) {
+            if (do_i)
+                for (int i = 1; i <= g->imax2; ++i) nskip += orc_isweep(g, i, var, a, b) != 0;
+            continue;
+        }
+        if (do_rb) {
+            const int i1 = 1, k1 = 1, i2 = g->imax2, k2 = g->kmax2, isize = i2 - i1 + 1, ksize = k2 - k1 + 1;
+            for (int icase = 1; icase <= 2; ++icase)
+                for (int ik = icase; ik <= ksize * isize; ik += 2) {
+                    const int k = (ik % isize != 0) ? ik / isize + k1 : ik / isize + k1 - 1;
+                    int i = (ik - 1 - (k - k1) * isize) + i1 + (k % 2);
+                    if (i > i2) i = i - i2 + i1 - 1;
+                    nskip += orc_iksweep(g, i, k, var, a, b) != 0;
+                }
+        }
+        if (do_i)
+            for (int k = 1; k <= g->kmax2; ++k)
+                for (int i = 1; i <= g->imax2; ++i) nskip += orc_iksweep(g, i, k, var, a, b) != 0;
+        if (do_kk)
+            for (int i = 1; i <= g->imax2; ++i)
+                for (int k = 1; k <= g->kmax2; ++k) nskip += orc_iksweep(g, i, k, var, a, b) != 0;
+    }
+    if (skips) *skips += nskip;
+    return 0;
+}
+
+int orc_msolve_t(const orc_geom *g, const double *b, const double *a, double *var, const char *sweep, int *skips)
+{
+    return msolve_t(g, b, a, var, sweep, skips);
+}
+
+int orc_leq_bicgst(const orc_geom *g, double *var, const double *a, double *b, const char *sweep, double tol,
+                   const char *pc, int itmax, uint64_t rt_seed, orc_stats *st)
+{
+    /* SOLVE_LIN_EQ's transposed copy A_mt (model/solve_lin_eq.f:139-150): scaled, then discarded */
+    double *at = (double *)malloc(sizeof(double) * 7 * (size_t)g->n);
+    memcpy(at, a, sizeof(double) * 7 * (size_t)g->n);
+    const int r = bicgs_run_x(g, var, at, b, sweep, tol, pc, itmax, rt_seed, -1, st, 1);
+    free(at);
+    return r;
 }

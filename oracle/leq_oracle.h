@@ -31,6 +31,8 @@ typedef struct {
     int imax2, jmax2, kmax2; /* cell extents including the wall layer */
     int do_k;                /* 0: two-dimensional (kmax2 == 1) */
     int64_t n;               /* DIMENSION_3 */
+    int cyclic;              /* 1 CYCLIC_X, 2 CYCLIC_Y, 4 CYCLIC_Z: the interior cells' neighbours wrap */
+    int pad;
 } orc_geom;
 
 typedef struct {
@@ -118,6 +120,13 @@ void orc_conv_source_pp_g(const orc_geom *g, const orc_pp_fields *f, double *a, 
 /* CALC_RESID_PP (model/calc_resid.f:391-534), serial: RESID of B over the fluid
  * cells (|B| summed in cell order) with normalization `norm`. */
 double orc_calc_resid_pp(const orc_geom *g, const int *flag, const double *b, double norm);
+
+/* DO_TRANSPOSE: LEQ_MSOLVEt (model/leq_bicgst.f:978-1177) on the same A_M values,
+ * and LEQ_BICGSt's solve: LEQ_BICGS0's iteration with LEQ_MSOLVEt, A scaled in a
+ * copy (a is left as given), B scaled in place. */
+int orc_msolve_t(const orc_geom *g, const double *b, const double *a, double *var, const char *sweep, int *skips);
+int orc_leq_bicgst(const orc_geom *g, double *var, const double *a, double *b, const char *sweep, double tol,
+                   const char *pc, int itmax, uint64_t rt_seed, orc_stats *st);
 
 int orc_num_threads(void);
 

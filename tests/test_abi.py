@@ -53,6 +53,10 @@ def test_options_roundtrip():
     assert leq.set_option("precision", 3) == leq.IER_ARGS
     assert leq.set_option("no_such_option", 1) == leq.IER_ARGS
     assert leq.get_option("write_back_ab") == 1
+    assert leq.get_option("do_transpose") == 0
+    assert leq.set_option("do_transpose", 1) == 0 and leq.get_option("do_transpose") == 1
+    assert leq.set_option("do_transpose", 0) == 0
+    assert leq.get_option("deflate") == 1 and leq.get_option("replace_every") == 20
     # lanes per J-line: 1..32
     assert leq.set_option("line_lanes", 32) == 0 and leq.get_option("line_lanes") == 32
     assert leq.set_option("line_lanes", 33) == leq.IER_ARGS

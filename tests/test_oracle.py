@@ -284,3 +284,68 @@ def test_sor_is_one_jacobi_step():
     xj = s.x + (b - S.matvec_np(s.imax2, s.jmax2, s.kmax2, s.do_k, a, s.x))
     assert np.max(np.abs(xj - t.x)) <= 1e-14 * np.max(np.abs(xj))
     assert np.array_equal(t.a[3], np.ones(s.n)) and st["iter_tot_add"] == 5
+
+
+@pytest.mark.parametrize("cyc,do_k", [(1, True), (2, True), (4, True), (7, True), (3, False)])
+def test_cyclic_matvec_and_known_answer(cyc, do_k):
+    """Cyclic axes: the oracle's LEQ_MATVEC equals an independent numpy restatement
+    of the wrapped increments, and a system built from a known x (b = A x) is solved
+    back to it."""
+    s = S.conv_diff_cyclic(9, 11, 7 if do_k else 1, seed=12, cyc=cyc, do_k=do_k)
+    rng = np.random.default_rng(cyc)
+    x = rng.standard_normal(s.n)
+    y_np = S.matvec_np(s.imax2, s.jmax2, s.kmax2, s.do_k, s.a, x, cyc=s.cyc)
+    assert np.allclose(O.matvec(s, x), y_np, rtol=1e-13, atol=1e-13)
+    assert not np.allclose(y_np, S.matvec_np(s.imax2, s.jmax2, s.kmax2, s.do_k, s.a, x))  # the wrap matters
+    t = s.copy()
+    wall = t.a[3] == -1.0
+    x_act = rng.uniform(0.5, 1.5, s.n)
+    x_act[wall] = 0.0
+    t.b = S.matvec_np(t.imax2, t.jmax2, t.kmax2, t.do_k, t.a, x_act, cyc=t.cyc)
+    t.x[:] = 0.0
+    t.tol = 1e-12
+    st = O.leq_bicgs(t)
+    assert st["ier"] == 0
+    assert np.linalg.norm(t.x - x_act) <= 1e-8 * np.linalg.norm(x_act)
+
+
+def _rb_serial(s, b):
+    """LEQ_MSOLVE's 'R' letter (model/leqsol_mod.f:382-391 in 2-D, :497-522 in 3-D)
+    in a serial build's loop order, in plain Python: Var = B, then the J-lines
+    (i + k) odd first in k-outer / i-inner order, each a tridiagonal solve whose
+    right-hand side takes the wrapped I and K neighbours."""
+    n = s.n
+    A = s.a.reshape(7, s.kmax2, s.imax2, s.jmax2)
+    B = b.reshape(s.kmax2, s.imax2, s.jmax2)
+    V = B.copy()
+    ni = S.neighbour_index
+    im, ip = ni(s.imax2, -1, bool(s.cyc & 1)), ni(s.imax2, 1, bool(s.cyc & 1))
+    km, kp = ni(s.kmax2, -1, bool(s.cyc & 4)), ni(s.kmax2, 1, bool(s.cyc & 4))
+    first = 1 if s.do_k else 0   # 2-D: i odd (1-based) first, i.e. i + k even with k = 1
+    for colour in (first, 1 - first):
+        for k in range(s.kmax2):
+            for i in range(s.imax2):
+                if ((i + 1) + (k + 1)) % 2 != colour:
+                    continue
+                r = B[k, i] - A[2, k, i] * V[k, im[i]] - A[4, k, i] * V[k, ip[i]]
+                if s.do_k:
+                    r = r - A[0, k, i] * V[km[k], i] - A[6, k, i] * V[kp[k], i]
+                dl, d, du = A[1, k, i][1:], A[3, k, i], A[5, k, i][:-1]
+                _, _, _, x, info = lapack.dgtsv(dl.copy(), d.copy(), du.copy(), r.copy())
+                assert info == 0
+                V[k, i] = x
+    assert V.size == n
+    return V.reshape(-1)
+
+
+@pytest.mark.parametrize("dims,cyc,do_k", [((11, 7, 9), 5, True), ((11, 6, 8), 7, True), ((13, 8, 1), 1, False)])
+def test_cyclic_red_black_serial_order(dims, cyc, do_k):
+    """With an odd number of interior cells along a cyclic axis the first and last
+    interior lines share a colour; the oracle sweeps them in the serial loop order."""
+    s = S.conv_diff_cyclic(*dims, seed=13, cyc=cyc, do_k=do_k)
+    O.scale(s)
+    x = np.random.default_rng(2).standard_normal(s.n)
+    rc, v, _ = O.msolve(s, x, "RRRR"[:1] + "   ")
+    assert rc == 0
+    ref = _rb_serial(s, x)
+    assert np.max(np.abs(v - ref)) <= 1e-12 * np.max(np.abs(ref))
