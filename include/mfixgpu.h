@@ -118,10 +118,12 @@ typedef struct {
     double device_ms;   /* device time of the solve (CUDA events), copies excluded */
     double jline_ms;    /* summed J-line sweep kernel time (option "time_kernels") */
     int jline_launches; /* J-line sweep launches timed */
-    int fp64_fallback;  /* mixed form: 1 when the FP32 iteration stalled and the FP64 drop-in re-solved */
+    int fp64_fallback;  /* mixed form: 1 when the FP32 iteration stalled and the FP64 drop-in re-solved;
+                           after mfixgpu_batch_solve, the number of such systems */
     long long kernel_launches; /* kernels of this library launched by the solve */
     int mixed_iterations; /* mixed form: FP32 iterations spent before an FP64 re-solve */
-    int deflated;       /* mixed form: 1 when the near-null mode was deflated (option "deflate") */
+    int deflated;       /* mixed form: 1 when the near-null mode was deflated (option "deflate");
+                           after mfixgpu_batch_solve, the number of deflated systems */
 } mfixgpu_stats;
 
 int mfixgpu_last_stats(mfixgpu_stats *out);

@@ -1007,6 +1007,8 @@ int mfixgpu_batch_solve(mfixgpu_system *systems, int nsys, const char *sweep, co
         systems[q].rnorm0 = out[q].rnorm0;
         systems[q].rnorm = out[q].rnorm;
         systems[q].fp64_fallback = out[q].fp64_fallback;
+        g.last.deflated += out[q].deflated;
+        g.last.fp64_fallback += out[q].fp64_fallback;
     }
     return 0;
 }
