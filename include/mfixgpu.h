@@ -162,6 +162,13 @@ const char *mfixgpu_last_error(void);
  *   "replace_every"  mixed form, deflated systems: the FP32 residual is replaced by the FP64 true
  *                    residual at least every this many inner iterations (default 20; 0: only after
  *                    the inner_tol drop)
+ *   "restart_growth" mixed form, deflated systems: when a true residual exceeds this multiple of the
+ *                    best one, the FP32 Krylov process restarts from the true residual (default 100;
+ *                    0: never)
+ *   "staged_matvec"  mixed form: 2 (default) the FP32 matvecs stream their operands into shared memory
+ *                    by bulk copies, x's i/k neighbours read through L2; 1: x's i/k neighbour lines
+ *                    staged too; 0: per-thread register loads (all three give the same products and
+ *                    sums)
  *   "write_back_ab"  1 (default) copy the scaled A_M/B_M slices back
  *   "rtilde_seed"    seed of the Rtilde random stream (replaces RANDOM_NUMBER, model/leq_bicgs.f:298)
  *   "inner_tol"      mixed form: drop of the FP32 residual between FP64 reliable updates (default 1e-2)

@@ -37,6 +37,8 @@ struct Options {
     double mixed_min_margin = 1e-4;
     int deflate = 1;
     int replace_every = 20;
+    double restart_growth = 100.0;
+    int staged_matvec = 2;
     int do_transpose = 0;
     int check_every = 4;
     int use_graph = 1;
@@ -274,6 +276,8 @@ SolveOptions make_opts(const Options &o, int pc, const char sweep4[4])
     so.mixed_min_margin = o.mixed_min_margin;
     so.deflate = o.deflate != 0;
     so.replace_every = o.replace_every;
+    so.restart_growth = o.restart_growth;
+    so.staged_matvec = o.staged_matvec;
     so.check_every = o.check_every;
     so.use_graph = o.use_graph != 0;
     so.time_kernels = o.time_kernels != 0;
@@ -670,6 +674,12 @@ int mfixgpu_set_option(const char *name, double value)
     } else if (k == "replace_every") {
         if (value < 0) return MFIXGPU_ERR_ARGS;
         g.opt.replace_every = (int)value;
+    } else if (k == "restart_growth") {
+        if (!(value == 0 || value > 1)) return MFIXGPU_ERR_ARGS;
+        g.opt.restart_growth = value;
+    } else if (k == "staged_matvec") {
+        if (!(value >= 0 && value <= 2)) return MFIXGPU_ERR_ARGS;
+        g.opt.staged_matvec = (int)value;
     } else if (k == "mixed_min_margin") {
         if (!(value >= 0)) return MFIXGPU_ERR_ARGS;
         g.opt.mixed_min_margin = value;
@@ -709,6 +719,8 @@ double mfixgpu_get_option(const char *name)
     if (k == "mixed_min_margin") return g.opt.mixed_min_margin;
     if (k == "deflate") return g.opt.deflate;
     if (k == "replace_every") return g.opt.replace_every;
+    if (k == "staged_matvec") return g.opt.staged_matvec;
+    if (k == "restart_growth") return g.opt.restart_growth;
     if (k == "do_transpose") return g.opt.do_transpose;
     if (k == "check_every") return g.opt.check_every;
     if (k == "use_graph") return g.opt.use_graph;

@@ -173,6 +173,10 @@ SolveResult result_of(const SysState &st, bool mixed)
         r.ier = -15;
         r.exit_kind = EX_ERROR;
     }
+    if (st.err & 4) {
+        r.ier = -15;  // a staged copy did not complete within its time limit
+        r.exit_kind = EX_ERROR;
+    }
     if (st.err & 2) {
         r.ier = -12;  // DGTSV INFO != 0 inside a JK/IJ sweep (the reference stops there)
         r.exit_kind = EX_ERROR;
@@ -336,6 +340,7 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         st.min_margin = opt.mixed_min_margin;
         st.defl_allow = opt.deflate ? 1 : 0;
         st.replace_every = opt.replace_every;
+        st.restart_growth = opt.restart_growth;
         st.margin_bits = 0x7f800000u;
         st.i = 1;
         st.iter = 1;
@@ -389,6 +394,15 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
     cfg_.rows_pair = cfg_.rows_single = 0;
     for (int q = 0; q < nsys_; ++q)
         if (h_sys_[q].n > 0) ((h_sys_[q].jp & 1) ? cfg_.rows_single : cfg_.rows_pair) = 1;
+    cfg_.mv_staged = 0;
+    cfg_.g_mv_staged = 1;
+    if (mixed && opt.staged_matvec == 1 && oc.matvec_staged > 0) {
+        cfg_.mv_staged = 1;
+        cfg_.g_mv_staged = grid(oc.matvec_staged);
+    } else if (mixed && opt.staged_matvec == 2 && oc.matvec_staged_nowin > 0) {
+        cfg_.mv_staged = 2;
+        cfg_.g_mv_staged = grid(oc.matvec_staged_nowin);
+    }
     cfg_.g_copy = grid(oc.copy);
     cfg_.g_outer = grid(oc.outer);
     return configure_lines(mixed ? 4 : 8);

@@ -65,6 +65,9 @@ struct SolveOptions {
     bool deflate = true;         // mixed form: deflate the near-null mode of systems below mixed_min_margin
                                  // (false: they go straight to the FP64 drop-in)
     int replace_every = 20;      // mixed form, deflated systems: FP64 residual replacement interval (0: off)
+    double restart_growth = 100.0;  // mixed form, deflated systems: Krylov restart on this true-residual growth (0: off)
+    int staged_matvec = 2;       // mixed form: matvecs with operands staged by bulk copies (1: with x's
+                                 // line / plane windows; 0: register loads)
     bool transposed = false;     // DO_TRANSPOSE (model/solve_lin_eq.f:139-150): LEQ_BICGSt's preconditioner
                                  // letters, and A is scaled in a copy (only B comes back scaled)
     int check_every = 4;         // iterations between host checks of the state

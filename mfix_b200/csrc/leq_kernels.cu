@@ -144,18 +144,30 @@ __device__ __forceinline__ void warp_sum(double (&v)[NV])
         for (int o = 16; o > 0; o >>= 1) v[q] += __shfl_xor_sync(0xffffffffu, v[q], o);
 }
 
-// Reduce v over the block; thread 0 receives the block total in v.
-template <int NV>
+// The barrier of a reduction: the whole block (BAR = 0), or named barrier BAR
+// over the first NT threads (kernels whose other warps do other work).
+template <int BAR, int NT>
+__device__ __forceinline__ void bsync()
+{
+    if constexpr (BAR == 0)
+        __syncthreads();
+    else
+        asm volatile("bar.sync %0, %1;\n" ::"n"(BAR), "n"(NT) : "memory");
+}
+
+// Reduce v over the block (or the first NT threads, BAR > 0); thread 0 receives
+// the total in v.
+template <int NV, int BAR = 0, int NT = 0>
 __device__ __forceinline__ void block_sum(double (&v)[NV])
 {
     __shared__ double red[NV][32];
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = BAR ? NT >> 5 : blockDim.x >> 5;
     warp_sum<NV>(v);
-    __syncthreads();
+    bsync<BAR, NT>();
     if (lane == 0)
 #pragma unroll
         for (int q = 0; q < NV; ++q) red[q][warp] = v[q];
-    __syncthreads();
+    bsync<BAR, NT>();
     if (warp == 0) {
 #pragma unroll
         for (int q = 0; q < NV; ++q) v[q] = lane < nw ? red[q][lane] : 0.0;
@@ -173,10 +185,10 @@ struct TileRun {
     int count;
 };
 
-template <int NV>
+template <int NV, int BAR = 0, int NT = 0>
 __device__ __forceinline__ void tile_partial(const BatchView &b, const SysDev &d, int tile_idx, double (&v)[NV])
 {
-    block_sum<NV>(v);
+    block_sum<NV, BAR, NT>(v);
     if (threadIdx.x == 0) {
         double *slot = b.partials + 2 * (int64_t)(d.tile_base + tile_idx);
 #pragma unroll
@@ -186,7 +198,7 @@ __device__ __forceinline__ void tile_partial(const BatchView &b, const SysDev &d
 
 // Reports the run's tiles; the block that completes the system's count forms
 // the totals and calls fin(state, totals) on thread 0.
-template <int NV, typename Fin>
+template <int NV, int BAR = 0, int NT = 0, typename Fin>
 __device__ __forceinline__ void run_close(const BatchView &b, TileRun &run, Fin &fin)
 {
     if (run.count == 0) return;
@@ -198,30 +210,30 @@ __device__ __forceinline__ void run_close(const BatchView &b, TileRun &run, Fin 
         const unsigned prev = atomicAdd(&st.arrivals, (unsigned)run.count);
         last = (prev + (unsigned)run.count == (unsigned)d.ntiles);
     }
-    __syncthreads();
+    bsync<BAR, NT>();
     run.count = 0;
     if (!last) return;
     __threadfence();
     double acc[NV];
 #pragma unroll
     for (int q = 0; q < NV; ++q) acc[q] = 0.0;
-    for (int t = threadIdx.x; t < d.ntiles; t += blockDim.x) {
+    for (int t = threadIdx.x; t < d.ntiles; t += (BAR ? NT : (int)blockDim.x)) {
         const double *slot = b.partials + 2 * (int64_t)(d.tile_base + t);
 #pragma unroll
         for (int q = 0; q < NV; ++q) acc[q] += __ldcg(slot + q);
     }
-    block_sum<NV>(acc);
+    block_sum<NV, BAR, NT>(acc);
     if (threadIdx.x == 0) {
         st.arrivals = 0;
         fin(st, acc);
     }
 }
 
-template <int NV, typename Fin>
+template <int NV, int BAR = 0, int NT = 0, typename Fin>
 __device__ __forceinline__ void run_add(const BatchView &b, TileRun &run, int sys, Fin &fin)
 {
     if (run.sys != sys) {
-        run_close<NV>(b, run, fin);
+        run_close<NV, BAR, NT>(b, run, fin);
         run.sys = sys;
     }
     run.count += 1;
@@ -607,19 +619,29 @@ __device__ __forceinline__ void load_row7(const SysDev &d, const T *__restrict__
     }
 }
 
+// The defect form's terms with every rounding stated (a fused multiply-add per
+// term), so that each kernel forming the product gets the same bits whatever
+// the compiler would contract.
+__device__ __forceinline__ float dterm0(float a, float xn, float xc) { return __fmul_rn(a, __fsub_rn(xn, xc)); }
+__device__ __forceinline__ float dterm(float acc, float a, float xn, float xc)
+{
+    return __fmaf_rn(a, __fsub_rn(xn, xc), acc);
+}
+__device__ __forceinline__ float dcentre(float acc, float rowsum, float xc) { return __fmaf_rn(rowsum, xc, acc); }
+
 template <typename T, bool DEFECT = false>
 __device__ __forceinline__ T dot_row7(const Row7<T> &r, bool do_k)
 {
-    if constexpr (DEFECT) {  // a[2] holds the row sum
+    if constexpr (DEFECT) {  // a[2] holds the row sum (mixed form: T = float)
         const T xc = r.x[2];
-        T v = r.a[0] * (r.x[0] - xc);
-        v = v + r.a[1] * (r.x[1] - xc);
-        v = v + r.a[2] * xc;
-        v = v + r.a[3] * (r.x[3] - xc);
-        v = v + r.a[4] * (r.x[4] - xc);
+        T v = dterm0(r.a[0], r.x[0], xc);
+        v = dterm(v, r.a[1], r.x[1], xc);
+        v = dcentre(v, r.a[2], xc);
+        v = dterm(v, r.a[3], r.x[3], xc);
+        v = dterm(v, r.a[4], r.x[4], xc);
         if (do_k) {
-            v = v + r.a[5] * (r.x[5] - xc);
-            v = v + r.a[6] * (r.x[6] - xc);
+            v = dterm(v, r.a[5], r.x[5], xc);
+            v = dterm(v, r.a[6], r.x[6], xc);
         }
         return v;
     }
@@ -729,23 +751,23 @@ __device__ __forceinline__ void load_pair7(const SysDev &d, const T *__restrict_
 template <typename T, bool DEFECT = false>
 __device__ __forceinline__ vec2_t<T> dot_pair7(const Pair7<T> &r, bool do_k)
 {
-    if constexpr (DEFECT) {  // a[2] holds the row sums
+    if constexpr (DEFECT) {  // a[2] holds the row sums (mixed form: T = float)
         const T cx = r.x[2].x, cy = r.x[2].y;
-        T u = r.a[0].x * (r.x[0].x - cx);
-        T w = r.a[0].y * (r.x[0].y - cy);
-        u = u + r.a[1].x * (r.x[1].x - cx);
-        w = w + r.a[1].y * (r.x[1].y - cy);
-        u = u + r.a[2].x * cx;
-        w = w + r.a[2].y * cy;
-        u = u + r.a[3].x * (r.x[3].x - cx);
-        w = w + r.a[3].y * (r.x[3].y - cy);
-        u = u + r.a[4].x * (r.x[4].x - cx);
-        w = w + r.a[4].y * (r.x[4].y - cy);
+        T u = dterm0(r.a[0].x, r.x[0].x, cx);
+        T w = dterm0(r.a[0].y, r.x[0].y, cy);
+        u = dterm(u, r.a[1].x, r.x[1].x, cx);
+        w = dterm(w, r.a[1].y, r.x[1].y, cy);
+        u = dcentre(u, r.a[2].x, cx);
+        w = dcentre(w, r.a[2].y, cy);
+        u = dterm(u, r.a[3].x, r.x[3].x, cx);
+        w = dterm(w, r.a[3].y, r.x[3].y, cy);
+        u = dterm(u, r.a[4].x, r.x[4].x, cx);
+        w = dterm(w, r.a[4].y, r.x[4].y, cy);
         if (do_k) {
-            u = u + r.a[5].x * (r.x[5].x - cx);
-            w = w + r.a[5].y * (r.x[5].y - cy);
-            u = u + r.a[6].x * (r.x[6].x - cx);
-            w = w + r.a[6].y * (r.x[6].y - cy);
+            u = dterm(u, r.a[5].x, r.x[5].x, cx);
+            w = dterm(w, r.a[5].y, r.x[5].y, cy);
+            u = dterm(u, r.a[6].x, r.x[6].x, cx);
+            w = dterm(w, r.a[6].y, r.x[6].y, cy);
         }
         return mk2<T>(u, w);
     }
@@ -1171,6 +1193,392 @@ __global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
     run_close<2>(b, run, fin);
 }
 
+// ------------------------------------------------------------------ staged FP32 matvec
+// The mixed form's V = A*Phat with alpha (KIND 0) and T = A*Shat with omega
+// (KIND 1), with the operands streamed into shared memory by bulk copies of the
+// Tensor Memory Accelerator (cp.async.bulk, completion counted on an mbarrier).
+// One producer warp fills a ring of MV_STAGES stages of MV_CELLS cells; the
+// MV_THREADS consumer threads compute the oldest stage and hand its slot back
+// through a second mbarrier, so the bytes in flight per SM no longer depend on
+// the registers each thread holds, and the producer's bookkeeping (tile, state
+// and system loads) overlaps the consumers' work.  A stage holds the six
+// off-diagonals, the row sums (defect form), x and the reduction's second vector
+// (Rtilde or S); with WIN also x one line (i-1, i+1) and one plane (k-1, k+1)
+// away.  Other neighbours come from global memory.  Consumer thread t owns cells
+// 2t and 2t+1 of every stage, the cells it owns in k_matvec_alpha /
+// k_matvec_omega's pair form, in the same order, with the same roundings: the
+// products and the partial sums are the same bits.
+constexpr int MV_CELLS = 512;
+constexpr int MV_THREADS = MV_CELLS / 2;  // consumer threads
+constexpr int MV_BLOCK = MV_THREADS + 32; // and one producer warp
+constexpr int MV_STAGES = 4;
+enum : int { MA_KM = 0, MA_JM, MA_IM, MA_DEF, MA_IP, MA_JP, MA_KP, MA_X, MA_W, MA_XIM, MA_XIP, MA_XKM, MA_XKP };
+
+template <bool WIN>
+__host__ __device__ constexpr int mv_arrays() { return WIN ? 13 : 9; }
+
+// One stage of the ring: its cells and, copied once per tile by the producer,
+// what the consumers need of the system (shared-memory reads instead of loads
+// through the system table).
+struct MvMeta {
+    int sys;   // -1: no more work
+    int tile;  // tile index within the system
+    int cnt;   // cells of this stage (0: a tile past the FP32 arrays' end)
+    int last;  // the tile's last stage: its partial sum follows
+    int64_t c; // first cell
+    const float *x;   // the product's input
+    float *y;         // its output
+    const float *az;  // deflated systems: A z (else null)
+    double cz;        // deflated systems: c_p (alpha) or c_s (omega)
+    int64_t np;       // cells of the padded arrays
+    FastDiv div_jp, div_i;
+    int jp, imax2, jmax2, kmax2, cyc, do_k;
+};
+
+template <bool WIN>
+constexpr size_t mv_smem()
+{
+    return (size_t)MV_STAGES * mv_arrays<WIN>() * MV_CELLS * sizeof(float) + 2 * MV_STAGES * sizeof(uint64_t) +
+           MV_STAGES * sizeof(MvMeta);
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint64_t *mb, unsigned count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(mb)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint64_t *mb, unsigned bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(smem_addr(mb)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(uint64_t *mb)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(smem_addr(mb)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *mb, unsigned parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+        : "=r"(ok)
+        : "r"(smem_addr(mb)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+// Waits for the phase of `parity` to complete; false after about two seconds.
+__device__ __forceinline__ bool mbar_wait(uint64_t *mb, unsigned parity)
+{
+    const long long t0 = clock64();
+    while (!mbar_try_wait(mb, parity))
+        if (clock64() - t0 > (1LL << 32)) return false;
+    return true;
+}
+// global -> shared bulk copy; addresses 16-byte aligned, bytes a multiple of 16
+__device__ __forceinline__ void bulk_g2s(void *dst, const void *src, unsigned bytes, uint64_t *mb)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(mb))
+                 : "memory");
+}
+// OR of v over the consumer threads (named barrier 1)
+__device__ __forceinline__ bool consumers_or(bool v)
+{
+    uint32_t r;
+    asm volatile("{\n .reg .pred p, q;\n setp.ne.u32 p, %1, 0;\n bar.red.or.pred q, 1, %2, p;\n selp.u32 %0, 1, 0, q;\n}\n"
+                 : "=r"(r)
+                 : "r"((uint32_t)v), "n"(MV_THREADS)
+                 : "memory");
+    return r != 0;
+}
+
+template <int KIND, bool WIN>
+__global__ void __launch_bounds__(MV_BLOCK, WIN ? 2 : 3) k_matvec_staged(BatchView b, int src)
+{
+    constexpr int NA = mv_arrays<WIN>();
+    constexpr int NV = KIND == 0 ? 1 : 2;
+    extern __shared__ __align__(128) unsigned char mv_smem[];
+    float *buf = reinterpret_cast<float *>(mv_smem);
+    uint64_t *full = reinterpret_cast<uint64_t *>(mv_smem + (size_t)MV_STAGES * NA * MV_CELLS * sizeof(float));
+    uint64_t *empty = full + MV_STAGES;
+    MvMeta *meta = reinterpret_cast<MvMeta *>(empty + MV_STAGES);
+    const int gate = KIND == 0 ? G_INNER : G_INNER_NOSNORM;
+    const int wid = KIND == 0 ? V_RT : V_S;
+    const int yid = KIND == 0 ? V_V : V_T;
+    if (threadIdx.x == 0) {
+        for (int q = 0; q < MV_STAGES; ++q) {
+            mbar_init(full + q, 1);
+            mbar_init(empty + q, MV_THREADS / 32);
+        }
+        mbar_fence_init();
+    }
+    __syncthreads();
+
+    if (threadIdx.x >= MV_THREADS) {
+        // ---- producer: the block's tiles t = blockIdx.x + m*gridDim.x of the systems
+        // in this reduction, MV_CELLS cells a stage
+        if (threadIdx.x != MV_THREADS) return;
+        int pt = blockIdx.x, psub = 0, cur = -1;
+        MvMeta tm;  // the current tile's system fields
+        tm.sys = -1;
+        int64_t t0 = 0, tend = 0, c2 = 0;
+        const float *a = nullptr, *def = nullptr, *w = nullptr;
+        int last_s[MV_STAGES];
+        for (int q = 0; q < MV_STAGES; ++q) last_s[q] = -1;
+        for (int s = 0;; ++s) {
+            const int slot = s % MV_STAGES;
+            if (s >= MV_STAGES && !mbar_wait(empty + slot, (unsigned)(s / MV_STAGES - 1) & 1u)) {
+                // the consumers gave up: the copies still in flight, again bounded
+                for (int q = 0; q < MV_STAGES; ++q)
+                    if (last_s[q] >= 0) mbar_wait(full + q, (unsigned)(last_s[q] / MV_STAGES) & 1u);
+                return;
+            }
+            MvMeta m = tm;
+            m.sys = -1;
+            m.tile = 0;
+            m.cnt = 0;
+            m.last = 0;
+            m.c = 0;
+            while (pt < b.ntiles) {
+                if (pt != cur) {
+                    const Tile tl = b.tiles[pt];
+                    const SysState &st = b.st[tl.sys];
+                    if (!gate_ok(st, gate)) {
+                        pt += gridDim.x;
+                        psub = 0;
+                        continue;
+                    }
+                    const SysDev &d = b.sys[tl.sys];
+                    cur = pt;
+                    tm.sys = tl.sys;
+                    tm.tile = tl.idx;
+                    tm.x = vec<float>(d, src);
+                    tm.y = vec<float>(d, yid);
+                    tm.az = st.defl ? d.defl_az : nullptr;
+                    tm.cz = st.defl ? (KIND == 0 ? st.defl_cp : st.defl_cs) : 0.0;
+                    tm.np = d.np;
+                    tm.div_jp = d.div_jp;
+                    tm.div_i = d.div_i;
+                    tm.jp = d.jp;
+                    tm.imax2 = d.imax2;
+                    tm.jmax2 = d.jmax2;
+                    tm.kmax2 = d.kmax2;
+                    tm.cyc = d.cyc;
+                    tm.do_k = d.do_k;
+                    a = d.a32;
+                    def = d.defect;
+                    w = vec<float>(d, wid);
+                    c2 = (int64_t)d.jp * d.imax2;
+                    t0 = (int64_t)tl.idx * TILE_CELLS;
+                    tend = min(t0 + TILE_CELLS, d.np);
+                }
+                m = tm;
+                m.c = t0 + (int64_t)psub * MV_CELLS;
+                m.cnt = (int)max((int64_t)0, min((int64_t)MV_CELLS, tend - m.c));
+                m.last = m.c + MV_CELLS >= tend;
+                if (m.last) {
+                    pt += gridDim.x;
+                    psub = 0;
+                } else {
+                    ++psub;
+                }
+                break;
+            }
+            meta[slot] = m;
+            if (m.cnt == 0) {
+                mbar_arrive(full + slot);
+                if (m.sys < 0) return;
+                continue;
+            }
+            // array q holds cells [c + shift, c + shift + cnt) of its source, clipped
+            // to the source's [0, np)
+            float *sb = buf + (size_t)slot * NA * MV_CELLS;
+            const int64_t c = m.c, cnt = m.cnt, np = m.np, c1 = m.jp;
+            const float *x = m.x;
+            const float *srcs[NA];
+            int64_t shift[NA];
+            for (int q = 0; q < NA; ++q) srcs[q] = nullptr, shift[q] = 0;
+            srcs[MA_JM] = a + 1 * np;
+            srcs[MA_IM] = a + 2 * np;
+            srcs[MA_DEF] = def;
+            srcs[MA_IP] = a + 4 * np;
+            srcs[MA_JP] = a + 5 * np;
+            srcs[MA_X] = x;
+            srcs[MA_W] = w;
+            if (m.do_k) {
+                srcs[MA_KM] = a + 0 * np;
+                srcs[MA_KP] = a + 6 * np;
+            }
+            if constexpr (WIN) {
+                srcs[MA_XIM] = x, shift[MA_XIM] = -c1;
+                srcs[MA_XIP] = x, shift[MA_XIP] = c1;
+                if (m.do_k) {
+                    srcs[MA_XKM] = x, shift[MA_XKM] = -c2;
+                    srcs[MA_XKP] = x, shift[MA_XKP] = c2;
+                }
+            }
+            unsigned bytes = 0;
+#pragma unroll
+            for (int q = 0; q < NA; ++q) {
+                const int64_t lo = max(c + shift[q], (int64_t)0), hi = min(c + shift[q] + cnt, np);
+                if (srcs[q] && hi > lo) bytes += (unsigned)((hi - lo) * sizeof(float));
+            }
+            mbar_expect_tx(full + slot, bytes);
+#pragma unroll
+            for (int q = 0; q < NA; ++q) {
+                const int64_t lo = max(c + shift[q], (int64_t)0), hi = min(c + shift[q] + cnt, np);
+                if (srcs[q] && hi > lo)
+                    bulk_g2s(sb + q * MV_CELLS + (lo - c - shift[q]), srcs[q] + lo, (unsigned)((hi - lo) * sizeof(float)),
+                             full + slot);
+            }
+            last_s[slot] = s;
+        }
+    }
+
+    // ---- consumers
+    auto fin = [&](SysState &st, const double(&tot)[NV]) {
+        if constexpr (KIND == 0) {
+            st.alpha = st.rho / tot[0];
+        } else {
+            double txt = tot[NV - 1];
+            if (txt == 0.0) txt = 1.0e-15;  // SMALL_NUMBER
+            st.omega = tot[0] / txt;
+        }
+    };
+    TileRun run{-1, 0};
+    double v[NV];
+#pragma unroll
+    for (int q = 0; q < NV; ++q) v[q] = 0.0;
+    const int l = 2 * threadIdx.x;
+    for (int s = 0;; ++s) {
+        const int slot = s % MV_STAGES;
+        const bool ok = mbar_wait(full + slot, (unsigned)(s / MV_STAGES) & 1u);
+        if (consumers_or(!ok)) {  // the same answer in every consumer thread
+            if (threadIdx.x == 0) {
+                const int sys = meta[slot].sys;
+                atomicOr(&b.st[sys >= 0 && sys < b.nsys ? sys : 0].err, 4);
+            }
+            return;
+        }
+        const MvMeta &m = meta[slot];
+        const int sys = m.sys;
+        if (sys < 0) break;
+        const int tile = m.tile, last = m.last;
+        if (l < m.cnt) {
+            const float *sb = buf + (size_t)slot * NA * MV_CELLS;
+            const float *x = m.x;
+            const int64_t p = m.c + l;
+            const int jp = m.jp, imax2 = m.imax2, jmax2 = m.jmax2;
+            const uint32_t line = fdiv((uint32_t)p, m.div_jp);
+            const int j = (int)((uint32_t)p - line * (uint32_t)jp);
+            const uint32_t kk = fdiv(line, m.div_i);
+            const int k = (int)kk, i = (int)(line - kk * (uint32_t)imax2);
+            const int64_t c1 = jp, c2 = (int64_t)jp * imax2;
+            const float2 xc = *reinterpret_cast<const float2 *>(sb + MA_X * MV_CELLS + l);
+            // x at an i or k neighbour (the pair shares i and k): the cells themselves,
+            // the staged window, or global memory (in bounds for every cell's offset)
+            auto nb2 = [&](int arr, int64_t off, int64_t win) -> float2 {
+                if (off == 0) return xc;
+                if constexpr (WIN)
+                    if (off == win) return *reinterpret_cast<const float2 *>(sb + arr * MV_CELLS + l);
+                return __ldg(reinterpret_cast<const float2 *>(x + p + off));
+            };
+            // x at cell p + off of the stage's own cells, or from global memory
+            auto xat = [&](int64_t off) -> float {
+                const int64_t t = l + off;
+                if (t >= 0 && t < m.cnt) return sb[MA_X * MV_CELLS + t];
+                const int64_t g = p + off;
+                return (g >= 0 && g < m.np) ? __ldg(x + g) : 0.0f;  // out of range only for pad cells
+            };
+            float xjm0, xjm1, xjp0, xjp1;
+            int64_t im, ip, km = 0, kp = 0;
+            if (m.cyc == 0) {  // clamped neighbours (model/set_increments.f:80-109)
+                xjm0 = j > 0 ? xat(-1) : xc.x;
+                xjm1 = xc.x;
+                xjp0 = j < jmax2 - 1 ? xc.y : xc.x;
+                xjp1 = j + 1 < jmax2 - 1 ? xat(2) : xc.y;
+                im = i > 0 ? -c1 : 0;
+                ip = i < imax2 - 1 ? c1 : 0;
+                if (m.do_k) {
+                    km = k > 0 ? -c2 : 0;
+                    kp = k < m.kmax2 - 1 ? c2 : 0;
+                }
+            } else {
+                const bool cj = (m.cyc & 2) != 0;
+                const int64_t o0 = inc_m(j, jmax2, cj), o1 = inc_m(j + 1, jmax2, cj);
+                const int64_t o2 = inc_p(j, jmax2, cj), o3 = inc_p(j + 1, jmax2, cj);
+                xjm0 = o0 == 0 ? xc.x : xat(o0);
+                xjm1 = o1 == 0 ? xc.y : xat(1 + o1);
+                xjp0 = o2 == 0 ? xc.x : xat(o2);
+                xjp1 = o3 == 0 ? xc.y : xat(1 + o3);
+                im = inc_m(i, imax2, m.cyc & 1) * c1;
+                ip = inc_p(i, imax2, m.cyc & 1) * c1;
+                if (m.do_k) {
+                    km = inc_m(k, m.kmax2, m.cyc & 4) * c2;
+                    kp = inc_p(k, m.kmax2, m.cyc & 4) * c2;
+                }
+            }
+            const float2 xim = nb2(MA_XIM, im, -c1);
+            const float2 xip = nb2(MA_XIP, ip, c1);
+            const float2 ajm = *reinterpret_cast<const float2 *>(sb + MA_JM * MV_CELLS + l);
+            const float2 aim = *reinterpret_cast<const float2 *>(sb + MA_IM * MV_CELLS + l);
+            const float2 rs = *reinterpret_cast<const float2 *>(sb + MA_DEF * MV_CELLS + l);
+            const float2 aip = *reinterpret_cast<const float2 *>(sb + MA_IP * MV_CELLS + l);
+            const float2 ajp = *reinterpret_cast<const float2 *>(sb + MA_JP * MV_CELLS + l);
+            // dot_pair7's defect form, operand for operand
+            float u = dterm0(ajm.x, xjm0, xc.x);
+            float t = dterm0(ajm.y, xjm1, xc.y);
+            u = dterm(u, aim.x, xim.x, xc.x);
+            t = dterm(t, aim.y, xim.y, xc.y);
+            u = dcentre(u, rs.x, xc.x);
+            t = dcentre(t, rs.y, xc.y);
+            u = dterm(u, aip.x, xip.x, xc.x);
+            t = dterm(t, aip.y, xip.y, xc.y);
+            u = dterm(u, ajp.x, xjp0, xc.x);
+            t = dterm(t, ajp.y, xjp1, xc.y);
+            if (m.do_k) {
+                const float2 xkm = nb2(MA_XKM, km, -c2);
+                const float2 xkp = nb2(MA_XKP, kp, c2);
+                const float2 akm = *reinterpret_cast<const float2 *>(sb + MA_KM * MV_CELLS + l);
+                const float2 akp = *reinterpret_cast<const float2 *>(sb + MA_KP * MV_CELLS + l);
+                u = dterm(u, akm.x, xkm.x, xc.x);
+                t = dterm(t, akm.y, xkm.y, xc.y);
+                u = dterm(u, akp.x, xkp.x, xc.x);
+                t = dterm(t, akp.y, xkp.y, xc.y);
+            }
+            if (j >= jmax2) u = 0.0f;  // pad cells of the padded FP32 arrays
+            if (j + 1 >= jmax2) t = 0.0f;
+            const float2 wv = *reinterpret_cast<const float2 *>(sb + MA_W * MV_CELLS + l);
+            if (m.az) {  // deflated systems: A (Phat + c z) = A Phat + c A z
+                const float2 az = ld2(m.az + p);
+                u = u + (float)(m.cz * (double)az.x);
+                t = t + (float)(m.cz * (double)az.y);
+            }
+            st2(m.y + p, mk2<float>(u, t));
+            if constexpr (KIND == 0) {
+                v[0] += (double)wv.x * (double)u;
+                v[0] += (double)wv.y * (double)t;
+            } else {
+                v[0] += (double)u * (double)wv.x;
+                v[NV - 1] += (double)u * (double)u;
+                v[0] += (double)t * (double)wv.y;
+                v[NV - 1] += (double)t * (double)t;
+            }
+        }
+        __syncwarp();
+        if ((threadIdx.x & 31) == 0) mbar_arrive(empty + slot);  // this warp is done with the slot
+        if (last) {
+            tile_partial<NV, 1, MV_THREADS>(b, b.sys[sys], tile, v);
+            run_add<NV, 1, MV_THREADS>(b, run, sys, fin);
+#pragma unroll
+            for (int q = 0; q < NV; ++q) v[q] = 0.0;
+        }
+    }
+    run_close<NV, 1, MV_THREADS>(b, run, fin);
+}
+
 // X += alpha*Phat + omega*Shat; R = S - omega*T; Rnorm; next rho
 // (model/leq_bicgs.f:432-460 and :318 of the following iteration).
 __device__ inline void fin_xr_ref(SysState &s, double rr, double rtr)
@@ -1445,6 +1853,15 @@ __device__ inline void fin_outer(SysState &s, double rr, double rtr32)
     if (s.inner_total >= s.itmax) {
         s.iter = s.inner_total;
         final_logic(s, false);
+        return;
+    }
+    // a deflated system whose true residual has risen restart_growth-fold above its
+    // best: the FP32 Krylov process has drifted away from the FP64 residual, so it
+    // restarts from the true residual (Rtilde = R, P = R) at the next update, the
+    // stall window still bounding the restarts
+    if (s.defl && !fresh && s.restart_growth > 0.0 && rn > s.restart_growth * s.best) {
+        s.restart = 1;
+        s.phase = PH_OUTER;
         return;
     }
     s.maxr = rn;
@@ -2751,6 +3168,26 @@ int line_thread_occupancy()
     return nb > 0 ? nb : 1;
 }
 
+// Resident blocks per SM of the staged matvec (shared memory above the default
+// limit is requested first); 0 when it cannot run.
+static int staged_occupancy(bool win)
+{
+    const int smem = (int)(win ? mv_smem<true>() : mv_smem<false>());
+    cudaError_t e0 = win ? cudaFuncSetAttribute(k_matvec_staged<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
+                         : cudaFuncSetAttribute(k_matvec_staged<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    cudaError_t e1 = win ? cudaFuncSetAttribute(k_matvec_staged<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
+                         : cudaFuncSetAttribute(k_matvec_staged<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    int nb = 0;
+    if (e0 == cudaSuccess && e1 == cudaSuccess) {
+        if ((win ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_matvec_staged<1, true>, MV_BLOCK, smem)
+                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_matvec_staged<1, false>, MV_BLOCK, smem)) !=
+            cudaSuccess)
+            nb = 0;
+    }
+    cudaGetLastError();
+    return nb;
+}
+
 template <typename K>
 static int occ(K kern)
 {
@@ -2771,6 +3208,9 @@ void cell_occupancy(bool fp32, CellOcc *o)
         o->xr_update = occ(k_xr_update<float, true>);
         o->matvec = occ(k_matvec_omega<float, true, false>);
         o->matvec_pair = occ(k_matvec_omega<float, true, true>);
+        o->matvec_staged = staged_occupancy(true);
+        o->matvec_staged_nowin = staged_occupancy(false);
+        cudaGetLastError();
         o->copy = occ(k_copy<float>);
         o->outer = occ(k_outer_step);
     } else {
@@ -2817,6 +3257,14 @@ cudaError_t launch_copy(const BatchView &b, const LaunchCfg &c, int src, int dst
 template <typename T, bool MIXED>
 cudaError_t launch_matvec_alpha(const BatchView &b, const LaunchCfg &c, int src)
 {
+    // the mixed form's padded FP32 arrays: operands staged by bulk copies
+    if (MIXED && sizeof(T) == 4 && c.mv_staged) {
+        if (c.mv_staged == 2)
+            k_matvec_staged<0, false><<<c.g_mv_staged, MV_BLOCK, mv_smem<false>(), c.stream>>>(b, src);
+        else
+            k_matvec_staged<0, true><<<c.g_mv_staged, MV_BLOCK, mv_smem<true>(), c.stream>>>(b, src);
+        CHECK_LAUNCH();
+    }
     // two-cell rows for systems with an even JMAX2, one-cell rows for the others
     if (c.rows_pair) k_matvec_alpha<T, MIXED, true><<<c.g_mv_pair, CELL_THREADS, 0, c.stream>>>(b, src);
     if (c.rows_single) k_matvec_alpha<T, MIXED, false><<<c.g_mv, CELL_THREADS, 0, c.stream>>>(b, src);
@@ -2831,6 +3279,13 @@ cudaError_t launch_s_update(const BatchView &b, const LaunchCfg &c)
 template <typename T, bool MIXED>
 cudaError_t launch_matvec_omega(const BatchView &b, const LaunchCfg &c, int src)
 {
+    if (MIXED && sizeof(T) == 4 && c.mv_staged) {
+        if (c.mv_staged == 2)
+            k_matvec_staged<1, false><<<c.g_mv_staged, MV_BLOCK, mv_smem<false>(), c.stream>>>(b, src);
+        else
+            k_matvec_staged<1, true><<<c.g_mv_staged, MV_BLOCK, mv_smem<true>(), c.stream>>>(b, src);
+        CHECK_LAUNCH();
+    }
     if (c.rows_pair) k_matvec_omega<T, MIXED, true><<<c.g_mv_pair, CELL_THREADS, 0, c.stream>>>(b, src);
     if (c.rows_single) k_matvec_omega<T, MIXED, false><<<c.g_mv, CELL_THREADS, 0, c.stream>>>(b, src);
     CHECK_LAUNCH();

@@ -23,6 +23,9 @@ struct LaunchCfg {
     int g_mv_pair;        // grid of the matvec kernels' two-cell form
     int rows_pair;        // 1: some system has an even JMAX2 (two-cell matvec rows)
     int rows_single;      // 1: some system has an odd JMAX2 (one-cell matvec rows)
+    int mv_staged;        // mixed form: the matvecs stage their operands by bulk copies (1), without x's
+                          // line / plane windows (2), or load them per thread (0)
+    int g_mv_staged;      // grid of the staged matvec
     int line_grid;   // blocks for J-line kernels
     int line_cmax;   // max rows per lane over the batch (smem sizing)
     int line_warps;  // warps per block of the J-line kernel
@@ -120,6 +123,8 @@ int line_thread_occupancy();  // resident blocks per SM of the one-lane-per-line
 //  // sets the smem attribute, returns resident blocks per SM
 struct CellOcc {
     int p_update, s_update, xr_update, matvec, matvec_pair, copy, outer;
+    int matvec_staged;        // the bulk-copy staged FP32 matvec with x's line / plane windows (0: it cannot run)
+    int matvec_staged_nowin;  // the same without the windows
 };
 void cell_occupancy(bool fp32, CellOcc *o);
 

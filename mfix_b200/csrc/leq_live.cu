@@ -182,6 +182,7 @@ int Engine::live_add(const LiveSystem &ls)
     st.min_margin = live_opt_.mixed_min_margin;
     st.defl_allow = live_opt_.deflate ? 1 : 0;
     st.replace_every = live_opt_.replace_every;
+    st.restart_growth = live_opt_.restart_growth;
     st.margin_bits = 0x7f800000u;
     st.i = 1;
     st.iter = 1;
@@ -278,7 +279,16 @@ int Engine::live_commit()
     cfg_.g_mv_pair = grid(oc.matvec_pair);
     cfg_.rows_pair = cfg_.rows_single = 0;
     for (int q = 0; q < nsys_; ++q)
-        if (h_sys_[q].n > 0) ((h_sys_[q].jmax2 & 1) ? cfg_.rows_single : cfg_.rows_pair) = 1;
+        if (h_sys_[q].n > 0) ((h_sys_[q].jp & 1) ? cfg_.rows_single : cfg_.rows_pair) = 1;
+    cfg_.mv_staged = 0;
+    cfg_.g_mv_staged = 1;
+    if (mixed && live_opt_.staged_matvec == 1 && oc.matvec_staged > 0) {
+        cfg_.mv_staged = 1;
+        cfg_.g_mv_staged = grid(oc.matvec_staged);
+    } else if (mixed && live_opt_.staged_matvec == 2 && oc.matvec_staged_nowin > 0) {
+        cfg_.mv_staged = 2;
+        cfg_.g_mv_staged = grid(oc.matvec_staged_nowin);
+    }
     cfg_.g_copy = grid(oc.copy);
     cfg_.g_outer = grid(oc.outer);
     int rc = configure_lines(mixed ? 4 : 8);

@@ -57,6 +57,13 @@ def test_options_roundtrip():
     assert leq.set_option("do_transpose", 1) == 0 and leq.get_option("do_transpose") == 1
     assert leq.set_option("do_transpose", 0) == 0
     assert leq.get_option("deflate") == 1 and leq.get_option("replace_every") == 20
+    assert leq.get_option("staged_matvec") == 2
+    assert leq.get_option("restart_growth") == 100
+    assert leq.set_option("restart_growth", 0.5) == leq.IER_ARGS
+    assert leq.set_option("restart_growth", 0) == 0 and leq.set_option("restart_growth", 100) == 0
+    assert leq.set_option("staged_matvec", 0) == 0 and leq.get_option("staged_matvec") == 0
+    assert leq.set_option("staged_matvec", 3) == leq.IER_ARGS
+    assert leq.set_option("staged_matvec", 2) == 0
     # lanes per J-line: 1..32
     assert leq.set_option("line_lanes", 32) == 0 and leq.get_option("line_lanes") == 32
     assert leq.set_option("line_lanes", 33) == leq.IER_ARGS
