@@ -40,6 +40,11 @@ module mfixgpu_mod
          integer(c_int), intent(in) :: dimension_m
       end function c_init_geometry
 
+      integer(c_int) function c_init_cyclic(cyclic_x, cyclic_y, cyclic_z) bind(C, name="mfixgpu_init_cyclic")
+         import :: c_int
+         integer(c_int), intent(in) :: cyclic_x, cyclic_y, cyclic_z
+      end function c_init_cyclic
+
       subroutine c_solve_lin_eq(vname, vname_len, vno, var, a_m, b_m, m, itmax, method, &
             sweep, sweep_len, tol1, pc, pc_len, ier) bind(C, name="mfixgpu_solve_lin_eq")
          import :: c_int, c_double, c_char
@@ -85,9 +90,11 @@ module mfixgpu_mod
 
 contains
 
-   !> Registers IMAX2, JMAX2, KMAX2, DO_K, DIMENSION_3 and DIMENSION_M.
+   !> Registers IMAX2, JMAX2, KMAX2, DO_K, DIMENSION_3, DIMENSION_M and the cyclic
+   !> axes (CYCLIC_X/Y/Z, model/geometry_mod.f; their increments wrap as
+   !> model/set_increments.f:73-113 builds them).
    subroutine mfixgpu_setup(ier)
-      use geometry, only: imax2, jmax2, kmax2, do_k
+      use geometry, only: imax2, jmax2, kmax2, do_k, cyclic_x, cyclic_y, cyclic_z
       use param, only: dimension_3, dimension_m
       integer, intent(out) :: ier
       integer(c_int) :: dk
@@ -95,6 +102,9 @@ contains
       if (do_k) dk = 1
       ier = c_init_geometry(int(imax2, c_int), int(jmax2, c_int), int(kmax2, c_int), dk, &
                             int(dimension_3, c_int64_t), int(dimension_m, c_int))
+      if (ier /= 0) return
+      ier = c_init_cyclic(merge(1_c_int, 0_c_int, cyclic_x), merge(1_c_int, 0_c_int, cyclic_y), &
+                          merge(1_c_int, 0_c_int, cyclic_z))
    end subroutine mfixgpu_setup
 
    integer function mfixgpu_set_option(name, value)
