@@ -162,6 +162,11 @@ const char *mfixgpu_last_error(void);
  *   "replace_every"  mixed form, deflated systems: the FP32 residual is replaced by the FP64 true
  *                    residual at least every this many inner iterations (default 20; 0: only after
  *                    the inner_tol drop)
+ *   "minimize_dotproducts" 0 (default) / 1: the reference's MINIMIZE_DOTPRODUCTS for METHOD 2 in
+ *                    FP64 (model/leq_bicgs.f:372,411,439): no Snorm exit, Rnorm formed and tested
+ *                    every "icheck_bicgs" iterations (every fifth with do_transpose); the mixed
+ *                    form decides convergence on its FP64 residual and ignores it
+ *   "icheck_bicgs"   ICHECK_BICGS, >= 1 (default 1)
  *   "restart_growth" mixed form, deflated systems: when a true residual exceeds this multiple of the
  *                    best one, the FP32 Krylov process restarts from the true residual (default 100;
  *                    0: never)

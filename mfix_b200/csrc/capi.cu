@@ -38,6 +38,8 @@ struct Options {
     int deflate = 1;
     int replace_every = 20;
     double restart_growth = 100.0;
+    int minimize_dotproducts = 0;
+    int icheck_bicgs = 1;
     int staged_matvec = 2;
     int do_transpose = 0;
     int check_every = 4;
@@ -277,6 +279,8 @@ SolveOptions make_opts(const Options &o, int pc, const char sweep4[4])
     so.deflate = o.deflate != 0;
     so.replace_every = o.replace_every;
     so.restart_growth = o.restart_growth;
+    so.minimize_dotproducts = o.minimize_dotproducts;
+    so.icheck_bicgs = o.icheck_bicgs;
     so.staged_matvec = o.staged_matvec;
     so.check_every = o.check_every;
     so.use_graph = o.use_graph != 0;
@@ -674,11 +678,16 @@ int mfixgpu_set_option(const char *name, double value)
     } else if (k == "replace_every") {
         if (value < 0) return MFIXGPU_ERR_ARGS;
         g.opt.replace_every = (int)value;
+    } else if (k == "minimize_dotproducts") {
+        g.opt.minimize_dotproducts = value != 0;
+    } else if (k == "icheck_bicgs") {
+        if (value < 1) return MFIXGPU_ERR_ARGS;
+        g.opt.icheck_bicgs = (int)value;
     } else if (k == "restart_growth") {
         if (!(value == 0 || value > 1)) return MFIXGPU_ERR_ARGS;
         g.opt.restart_growth = value;
     } else if (k == "staged_matvec") {
-        if (!(value >= 0 && value <= 2)) return MFIXGPU_ERR_ARGS;
+        if (!(value >= 0 && value <= MV_SHAPES)) return MFIXGPU_ERR_ARGS;
         g.opt.staged_matvec = (int)value;
     } else if (k == "mixed_min_margin") {
         if (!(value >= 0)) return MFIXGPU_ERR_ARGS;
@@ -721,6 +730,8 @@ double mfixgpu_get_option(const char *name)
     if (k == "replace_every") return g.opt.replace_every;
     if (k == "staged_matvec") return g.opt.staged_matvec;
     if (k == "restart_growth") return g.opt.restart_growth;
+    if (k == "minimize_dotproducts") return g.opt.minimize_dotproducts;
+    if (k == "icheck_bicgs") return g.opt.icheck_bicgs;
     if (k == "do_transpose") return g.opt.do_transpose;
     if (k == "check_every") return g.opt.check_every;
     if (k == "use_graph") return g.opt.use_graph;

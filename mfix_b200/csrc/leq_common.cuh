@@ -143,6 +143,7 @@ struct SysState {
     double defl_e;        // z^T A z
     double defl_cp, defl_cs;  // z^T P / z^T A z and z^T S / z^T A z of the current iteration
     int replace_every;    // mixed form, deflated systems: FP64 residual replacement at least every this many iterations
+    int icheck;           // FP64 BiCGSTAB: 0, or MINIMIZE_DOTPRODUCTS with the Rnorm test every icheck iterations
     double restart_growth;  // mixed form, deflated systems: restart the Krylov process when a true residual exceeds
                             // this multiple of the best (0: never)
     int since_outer;      // mixed form: inner iterations since the last FP64 update

@@ -340,6 +340,7 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         st.min_margin = opt.mixed_min_margin;
         st.defl_allow = opt.deflate ? 1 : 0;
         st.replace_every = opt.replace_every;
+        st.icheck = (opt.minimize_dotproducts && !mixed) ? (opt.transposed ? 5 : std::max(1, opt.icheck_bicgs)) : 0;
         st.restart_growth = opt.restart_growth;
         st.margin_bits = 0x7f800000u;
         st.i = 1;
@@ -396,12 +397,9 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         if (h_sys_[q].n > 0) ((h_sys_[q].jp & 1) ? cfg_.rows_single : cfg_.rows_pair) = 1;
     cfg_.mv_staged = 0;
     cfg_.g_mv_staged = 1;
-    if (mixed && opt.staged_matvec == 1 && oc.matvec_staged > 0) {
-        cfg_.mv_staged = 1;
-        cfg_.g_mv_staged = grid(oc.matvec_staged);
-    } else if (mixed && opt.staged_matvec == 2 && oc.matvec_staged_nowin > 0) {
-        cfg_.mv_staged = 2;
-        cfg_.g_mv_staged = grid(oc.matvec_staged_nowin);
+    if (mixed && opt.staged_matvec >= 1 && opt.staged_matvec <= MV_SHAPES && oc.matvec_staged[opt.staged_matvec] > 0) {
+        cfg_.mv_staged = opt.staged_matvec;
+        cfg_.g_mv_staged = grid(oc.matvec_staged[opt.staged_matvec]);
     }
     cfg_.g_copy = grid(oc.copy);
     cfg_.g_outer = grid(oc.outer);

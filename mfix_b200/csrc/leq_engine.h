@@ -66,6 +66,8 @@ struct SolveOptions {
                                  // (false: they go straight to the FP64 drop-in)
     int replace_every = 20;      // mixed form, deflated systems: FP64 residual replacement interval (0: off)
     double restart_growth = 100.0;  // mixed form, deflated systems: Krylov restart on this true-residual growth (0: off)
+    int minimize_dotproducts = 0;   // FP64 BiCGSTAB: MINIMIZE_DOTPRODUCTS (no Snorm exit, Rnorm every icheck_bicgs)
+    int icheck_bicgs = 1;           // ICHECK_BICGS
     int staged_matvec = 2;       // mixed form: matvecs with operands staged by bulk copies (1: with x's
                                  // line / plane windows; 0: register loads)
     bool transposed = false;     // DO_TRANSPOSE (model/solve_lin_eq.f:139-150): LEQ_BICGSt's preconditioner

@@ -1045,7 +1045,8 @@ __global__ void __launch_bounds__(256, 4) k_s_update(BatchView b)
         if (MIXED)
             st.snorm_exit = (st.snorm <= 0.1 * st.tol * st.outer_rnorm0) ? 1 : 0;
         else
-            st.snorm_exit = (st.snorm <= DBL_EPSILON) ? 1 : 0;  // TOLMIN = EPSILON(ONE)
+            st.snorm_exit = (!st.icheck && st.snorm <= DBL_EPSILON) ? 1 : 0;  // TOLMIN = EPSILON(ONE); none
+                                                                              // with MINIMIZE_DOTPRODUCTS
         if (MIXED && st.defl) st.defl_cs = tot[NV - 1] / st.defl_e;
     };
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
@@ -1208,10 +1209,25 @@ __global__ void __launch_bounds__(256) k_matvec_omega(BatchView b, int src)
 // 2t and 2t+1 of every stage, the cells it owns in k_matvec_alpha /
 // k_matvec_omega's pair form, in the same order, with the same roundings: the
 // products and the partial sums are the same bits.
-constexpr int MV_CELLS = 512;
-constexpr int MV_THREADS = MV_CELLS / 2;  // consumer threads
+constexpr int MV_THREADS = 256;           // consumer threads
 constexpr int MV_BLOCK = MV_THREADS + 32; // and one producer warp
-constexpr int MV_STAGES = 4;
+// Shapes of the ring (option staged_matvec): whether x's line / plane windows are
+// staged, cells per stage, stages, resident blocks per SM.  Larger stages (1024
+// cells x 3, 2048 x 3, 1024 x 6) ran slower on 256^3 (10.3, 15.6, 16.8 ms of
+// matvecs per solve against 9.2): resident consumer warps, not the number of
+// copies, bound the kernel, and three blocks per SM is the register limit.
+template <int CFG>
+struct MvCfg;
+template <>
+struct MvCfg<1> {
+    static constexpr bool WIN = true;
+    static constexpr int CELLS = 512, STAGES = 4, BPS = 2;
+};
+template <>
+struct MvCfg<2> {
+    static constexpr bool WIN = false;
+    static constexpr int CELLS = 512, STAGES = 4, BPS = 3;
+};
 enum : int { MA_KM = 0, MA_JM, MA_IM, MA_DEF, MA_IP, MA_JP, MA_KP, MA_X, MA_W, MA_XIM, MA_XIP, MA_XKM, MA_XKP };
 
 template <bool WIN>
@@ -1235,11 +1251,12 @@ struct MvMeta {
     int jp, imax2, jmax2, kmax2, cyc, do_k;
 };
 
-template <bool WIN>
+template <int CFG>
 constexpr size_t mv_smem()
 {
-    return (size_t)MV_STAGES * mv_arrays<WIN>() * MV_CELLS * sizeof(float) + 2 * MV_STAGES * sizeof(uint64_t) +
-           MV_STAGES * sizeof(MvMeta);
+    using C = MvCfg<CFG>;
+    return (size_t)C::STAGES * mv_arrays<C::WIN>() * C::CELLS * sizeof(float) + 2 * C::STAGES * sizeof(uint64_t) +
+           C::STAGES * sizeof(MvMeta);
 }
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -1294,9 +1311,12 @@ __device__ __forceinline__ bool consumers_or(bool v)
     return r != 0;
 }
 
-template <int KIND, bool WIN>
-__global__ void __launch_bounds__(MV_BLOCK, WIN ? 2 : 3) k_matvec_staged(BatchView b, int src)
+template <int KIND, int CFG>
+__global__ void __launch_bounds__(MV_BLOCK, MvCfg<CFG>::BPS) k_matvec_staged(BatchView b, int src)
 {
+    constexpr bool WIN = MvCfg<CFG>::WIN;
+    constexpr int MV_CELLS = MvCfg<CFG>::CELLS;
+    constexpr int MV_STAGES = MvCfg<CFG>::STAGES;
     constexpr int NA = mv_arrays<WIN>();
     constexpr int NV = KIND == 0 ? 1 : 2;
     extern __shared__ __align__(128) unsigned char mv_smem[];
@@ -1451,7 +1471,6 @@ __global__ void __launch_bounds__(MV_BLOCK, WIN ? 2 : 3) k_matvec_staged(BatchVi
     double v[NV];
 #pragma unroll
     for (int q = 0; q < NV; ++q) v[q] = 0.0;
-    const int l = 2 * threadIdx.x;
     for (int s = 0;; ++s) {
         const int slot = s % MV_STAGES;
         const bool ok = mbar_wait(full + slot, (unsigned)(s / MV_STAGES) & 1u);
@@ -1466,6 +1485,8 @@ __global__ void __launch_bounds__(MV_BLOCK, WIN ? 2 : 3) k_matvec_staged(BatchVi
         const int sys = m.sys;
         if (sys < 0) break;
         const int tile = m.tile, last = m.last;
+        for (int u = 0; u < MV_CELLS / (2 * MV_THREADS); ++u) {
+        const int l = 2 * (threadIdx.x + MV_THREADS * u);
         if (l < m.cnt) {
             const float *sb = buf + (size_t)slot * NA * MV_CELLS;
             const float *x = m.x;
@@ -1567,6 +1588,7 @@ __global__ void __launch_bounds__(MV_BLOCK, WIN ? 2 : 3) k_matvec_staged(BatchVi
                 v[NV - 1] += (double)t * (double)t;
             }
         }
+        }
         __syncwarp();
         if ((threadIdx.x & 31) == 0) mbar_arrive(empty + slot);  // this warp is done with the slot
         if (last) {
@@ -1589,13 +1611,17 @@ __device__ inline void fin_xr_ref(SysState &s, double rr, double rtr)
         s.status = ST_DONE;
         return;
     }
-    s.rnorm = sqrt(rr);
-    if (s.rnorm <= s.tol * s.rnorm0) {
-        s.iter_tot_add = s.iter + 1;
-        s.ier = 0;
-        s.exit_kind = EX_RNORM;
-        s.status = ST_DONE;
-        return;
+    // with MINIMIZE_DOTPRODUCTS Rnorm is formed and tested every icheck-th
+    // iteration only (model/leq_bicgs.f:439; LEQ_BICGSt: every fifth, leq_bicgst.f:514)
+    if (!s.icheck || s.iter % s.icheck == 0) {
+        s.rnorm = sqrt(rr);
+        if (s.rnorm <= s.tol * s.rnorm0) {
+            s.iter_tot_add = s.iter + 1;
+            s.ier = 0;
+            s.exit_kind = EX_RNORM;
+            s.status = ST_DONE;
+            return;
+        }
     }
     s.iter += 1;
     s.i += 1;
@@ -2055,6 +2081,23 @@ __device__ __forceinline__ int find_sys(const int *prefix, int nsys, int item)
     return lo;
 }
 
+// The line (i, k), 1-based, of slot q of a kind-0 wave (lines with (i+k) of the
+// wave's parity, 3-D sweeps (i+k) odd first (model/leqsol_mod.f:497-509), 2-D
+// sweeps i odd first (:382-391), i.e. (i+k) even with k = 1: the wave's parity is
+// stated for 3-D and flipped for a 2-D system); false when the slot is past the
+// system's lines or outside the wave's wrap level.
+__device__ __forceinline__ bool wave_line(const SysDev &d, const WaveArgs &w, int q, int &i, int &k)
+{
+    k = (int)fdiv((uint32_t)q, d.div_h) + 1;
+    const int slot = q - (k - 1) * d.half_lines;
+    const int par = d.do_k ? w.par : (w.par ^ 1);
+    const int i0 = (((1 + k) & 1) == par) ? 1 : 2;
+    i = i0 + 2 * slot;
+    bool valid = (k <= d.kmax2) && (i <= d.imax2);
+    if (w.lvl > 0 && valid) valid = wrap_level(d, i, k) == w.lvl - 1;
+    return valid;
+}
+
 struct LineJob {
     int item;
     int sidx;
@@ -2092,16 +2135,7 @@ __device__ __forceinline__ bool next_line_job(const BatchView &b, const WaveArgs
         const int item0 = (w.kind == 0) ? b.line_prefix[sidx] : 0;
         const int q = (item - item0) * lpw + j.seg;
         if (w.kind == 0) {
-            j.k = (int)fdiv((uint32_t)q, d.div_h) + 1;
-            const int slot = q - (j.k - 1) * d.half_lines;
-            // 3-D sweeps take (i+k) odd first (model/leqsol_mod.f:497-509), 2-D
-            // sweeps i odd first (:382-391), i.e. (i+k) even with k = 1: the wave's
-            // parity is stated for 3-D and flipped for a 2-D system
-            const int par = d.do_k ? w.par : (w.par ^ 1);
-            const int i0 = (((1 + j.k) & 1) == par) ? 1 : 2;
-            j.i = i0 + 2 * slot;
-            j.valid = (j.k <= d.kmax2) && (j.i <= d.imax2);
-            if (w.lvl > 0 && j.valid) j.valid = wrap_level(d, j.i, j.k) == w.lvl - 1;
+            j.valid = wave_line(d, w, q, j.i, j.k);
         } else if (w.kind == 1) {
             const int ilo = max(1, w.par - d.kmax2), ihi = min(d.imax2, w.par - 1);
             j.i = ilo + q;
@@ -2248,6 +2282,77 @@ __device__ __forceinline__ RowsV<T, VW> ldv(const T *p)
     return *reinterpret_cast<const RowsV<T, VW> *>(p);
 }
 
+// c - a*b, a*b + c and a*b for the J-line sweeps: in FP32 with every rounding
+// stated (so that the register-staged and the bulk-staged kernels give the same
+// bits), in FP64 as written.
+template <typename T>
+__device__ __forceinline__ T fnms(T a, T b, T c) { return c - a * b; }
+template <>
+__device__ __forceinline__ float fnms<float>(float a, float b, float c) { return __fmaf_rn(-a, b, c); }
+template <typename T>
+__device__ __forceinline__ T fma_t(T a, T b, T c) { return a * b + c; }
+template <>
+__device__ __forceinline__ float fma_t<float>(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+template <typename T>
+__device__ __forceinline__ T mul_t(T a, T b) { return a * b; }
+template <>
+__device__ __forceinline__ float mul_t<float>(float a, float b) { return __fmul_rn(a, b); }
+
+// The two recurrences of a factored line, y_r = f_r - l_r y_{r-1} and
+// x_r = r_r y_r - q_r x_{r+1}, on shared-memory rows: lane gl of the line's G
+// lanes owns rows [gl*c, gl*c + c); a pass over the chunk from a zero start gives
+// its affine map, a log2(G)-step shuffle scan composes the maps, a second pass
+// starts from the entering value.  x replaces f.
+template <typename T>
+__device__ __forceinline__ void line_recurrences(T *f, const T *fl, const T *fr, const T *fq, int c, int G, int gl)
+{
+    T *cf = f + gl * c;
+    const T *cl = fl + gl * c, *cr = fr + gl * c, *cq = fq + gl * c;
+    T mb = T(0), ma = T(1);
+#pragma unroll 4
+    for (int t = 0; t < c; ++t) {
+        const T lt = cl[t];
+        mb = fnms(lt, mb, cf[t]);
+        ma = -lt * ma;
+    }
+    for (int dl = 1; dl < G; dl <<= 1) {
+        const T pa = __shfl_up_sync(0xffffffffu, ma, dl, G), pb = __shfl_up_sync(0xffffffffu, mb, dl, G);
+        if (gl >= dl) {
+            mb = fma_t(ma, pb, mb);
+            ma = mul_t(ma, pa);
+        }
+    }
+    T y = __shfl_up_sync(0xffffffffu, mb, 1, G);
+    if (gl == 0) y = T(0);
+#pragma unroll 4
+    for (int t = 0; t < c; ++t) {
+        y = fnms(cl[t], y, cf[t]);
+        cf[t] = y;
+    }
+    mb = T(0);
+    ma = T(1);
+#pragma unroll 4
+    for (int t = c - 1; t >= 0; --t) {
+        const T qt = cq[t];
+        mb = fnms(qt, mb, mul_t(cr[t], cf[t]));
+        ma = -qt * ma;
+    }
+    for (int dl = 1; dl < G; dl <<= 1) {
+        const T na = __shfl_down_sync(0xffffffffu, ma, dl, G), nb = __shfl_down_sync(0xffffffffu, mb, dl, G);
+        if (gl + dl < G) {
+            mb = fma_t(ma, nb, mb);
+            ma = mul_t(ma, na);
+        }
+    }
+    T xv = __shfl_down_sync(0xffffffffu, mb, 1, G);
+    if (gl == G - 1) xv = T(0);
+#pragma unroll 4
+    for (int t = c - 1; t >= 0; --t) {
+        xv = fnms(cq[t], xv, mul_t(cr[t], cf[t]));
+        cf[t] = xv;
+    }
+}
+
 template <typename T, int VW>
 __global__ void __launch_bounds__(128, sizeof(T) == 4 ? (VW == 4 ? 5 : 6) : 4) k_jline(BatchView b, WaveArgs w, int cmax)
 {
@@ -2315,11 +2420,11 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? (VW == 4 ? 5 : 6) : 4) k
                 for (int k = 0; k < VW; ++k) {
                     T f0 = T(0);
                     if (fast && r + k < L) {
-                        f0 = rhs.v[k] - am1.v[k] * nim.v[k];
-                        f0 = f0 - ap1.v[k] * nip.v[k];
+                        f0 = fnms(am1.v[k], nim.v[k], rhs.v[k]);
+                        f0 = fnms(ap1.v[k], nip.v[k], f0);
                         if (x.do_k) {
-                            f0 = f0 - am3.v[k] * nkm.v[k];
-                            f0 = f0 - ap3.v[k] * nkp.v[k];
+                            f0 = fnms(am3.v[k], nkm.v[k], f0);
+                            f0 = fnms(ap3.v[k], nkp.v[k], f0);
                         }
                     }
                     fv.v[k] = f0;
@@ -2358,11 +2463,11 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? (VW == 4 ? 5 : 6) : 4) k
                     if (r < G * c) {
                         T fv = T(0), l_ = T(0), r_ = T(0), q_ = T(0);
                         if (fast && r < L) {
-                            fv = rhs[u] - am1[u] * nim[u];
-                            fv = fv - ap1[u] * nip[u];
+                            fv = fnms(am1[u], nim[u], rhs[u]);
+                            fv = fnms(ap1[u], nip[u], fv);
                             if (x.do_k) {
-                                fv = fv - am3[u] * nkm[u];
-                                fv = fv - ap3[u] * nkp[u];
+                                fv = fnms(am3[u], nkm[u], fv);
+                                fv = fnms(ap3[u], nkp[u], fv);
                             }
                             l_ = lv[u];
                             r_ = rv[u];
@@ -2379,52 +2484,7 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? (VW == 4 ? 5 : 6) : 4) k
         if constexpr (VW > 1) cp_async_wait_all();
         __syncwarp();
 
-        // ---- forward recurrence y_r = f_r - l_r y_{r-1}
-        T *cf = f + gl * c, *cl = fl + gl * c, *cr = fr + gl * c, *cq = fq + gl * c;
-        T mb = T(0), ma = T(1);
-#pragma unroll 4
-        for (int t = 0; t < c; ++t) {
-            const T lt = cl[t];
-            mb = cf[t] - lt * mb;
-            ma = -lt * ma;
-        }
-        for (int dl = 1; dl < G; dl <<= 1) {
-            const T pa = __shfl_up_sync(0xffffffffu, ma, dl, G), pb = __shfl_up_sync(0xffffffffu, mb, dl, G);
-            if (gl >= dl) {
-                mb = ma * pb + mb;
-                ma = ma * pa;
-            }
-        }
-        T y = __shfl_up_sync(0xffffffffu, mb, 1, G);
-        if (gl == 0) y = T(0);
-#pragma unroll 4
-        for (int t = 0; t < c; ++t) {
-            y = cf[t] - cl[t] * y;
-            cf[t] = y;
-        }
-        // ---- backward recurrence x_r = r_r y_r - q_r x_{r+1}
-        mb = T(0);
-        ma = T(1);
-#pragma unroll 4
-        for (int t = c - 1; t >= 0; --t) {
-            const T qt = cq[t];
-            mb = cr[t] * cf[t] - qt * mb;
-            ma = -qt * ma;
-        }
-        for (int dl = 1; dl < G; dl <<= 1) {
-            const T na = __shfl_down_sync(0xffffffffu, ma, dl, G), nb = __shfl_down_sync(0xffffffffu, mb, dl, G);
-            if (gl + dl < G) {
-                mb = ma * nb + mb;
-                ma = ma * na;
-            }
-        }
-        T xv = __shfl_down_sync(0xffffffffu, mb, 1, G);
-        if (gl == G - 1) xv = T(0);
-#pragma unroll 4
-        for (int t = c - 1; t >= 0; --t) {
-            xv = cr[t] * cf[t] - cq[t] * xv;
-            cf[t] = xv;
-        }
+        line_recurrences<T>(f, fl, fr, fq, c, G, gl);
         __syncwarp();
 
         // ---- lines on which DGTSV interchanges rows or meets a zero pivot
@@ -3170,22 +3230,41 @@ int line_thread_occupancy()
 
 // Resident blocks per SM of the staged matvec (shared memory above the default
 // limit is requested first); 0 when it cannot run.
-static int staged_occupancy(bool win)
+template <int CFG>
+static int staged_occupancy_cfg()
 {
-    const int smem = (int)(win ? mv_smem<true>() : mv_smem<false>());
-    cudaError_t e0 = win ? cudaFuncSetAttribute(k_matvec_staged<0, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
-                         : cudaFuncSetAttribute(k_matvec_staged<0, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
-    cudaError_t e1 = win ? cudaFuncSetAttribute(k_matvec_staged<1, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem)
-                         : cudaFuncSetAttribute(k_matvec_staged<1, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    const int smem = (int)mv_smem<CFG>();
     int nb = 0;
-    if (e0 == cudaSuccess && e1 == cudaSuccess) {
-        if ((win ? cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_matvec_staged<1, true>, MV_BLOCK, smem)
-                 : cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_matvec_staged<1, false>, MV_BLOCK, smem)) !=
-            cudaSuccess)
-            nb = 0;
+    if (cudaFuncSetAttribute(k_matvec_staged<0, CFG>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) ==
+            cudaSuccess &&
+        cudaFuncSetAttribute(k_matvec_staged<1, CFG>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) ==
+            cudaSuccess &&
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_matvec_staged<1, CFG>, MV_BLOCK, smem) == cudaSuccess) {
+        cudaGetLastError();
+        return nb;
     }
     cudaGetLastError();
-    return nb;
+    return 0;
+}
+
+// Resident blocks per SM of the staged matvec shape CFG (shared memory above the
+// default limit is requested first); 0 when it cannot run.
+static int staged_occupancy(int cfg)
+{
+    switch (cfg) {
+    case 1: return staged_occupancy_cfg<1>();
+    case 2: return staged_occupancy_cfg<2>();
+    default: return 0;
+    }
+}
+
+template <int KIND>
+static void launch_staged(const BatchView &b, const LaunchCfg &c, int src)
+{
+    switch (c.mv_staged) {
+    case 1: k_matvec_staged<KIND, 1><<<c.g_mv_staged, MV_BLOCK, mv_smem<1>(), c.stream>>>(b, src); break;
+    default: k_matvec_staged<KIND, 2><<<c.g_mv_staged, MV_BLOCK, mv_smem<2>(), c.stream>>>(b, src); break;
+    }
 }
 
 template <typename K>
@@ -3208,8 +3287,7 @@ void cell_occupancy(bool fp32, CellOcc *o)
         o->xr_update = occ(k_xr_update<float, true>);
         o->matvec = occ(k_matvec_omega<float, true, false>);
         o->matvec_pair = occ(k_matvec_omega<float, true, true>);
-        o->matvec_staged = staged_occupancy(true);
-        o->matvec_staged_nowin = staged_occupancy(false);
+        for (int q = 1; q <= MV_SHAPES; ++q) o->matvec_staged[q] = staged_occupancy(q);
         cudaGetLastError();
         o->copy = occ(k_copy<float>);
         o->outer = occ(k_outer_step);
@@ -3259,10 +3337,7 @@ cudaError_t launch_matvec_alpha(const BatchView &b, const LaunchCfg &c, int src)
 {
     // the mixed form's padded FP32 arrays: operands staged by bulk copies
     if (MIXED && sizeof(T) == 4 && c.mv_staged) {
-        if (c.mv_staged == 2)
-            k_matvec_staged<0, false><<<c.g_mv_staged, MV_BLOCK, mv_smem<false>(), c.stream>>>(b, src);
-        else
-            k_matvec_staged<0, true><<<c.g_mv_staged, MV_BLOCK, mv_smem<true>(), c.stream>>>(b, src);
+        launch_staged<0>(b, c, src);
         CHECK_LAUNCH();
     }
     // two-cell rows for systems with an even JMAX2, one-cell rows for the others
@@ -3280,10 +3355,7 @@ template <typename T, bool MIXED>
 cudaError_t launch_matvec_omega(const BatchView &b, const LaunchCfg &c, int src)
 {
     if (MIXED && sizeof(T) == 4 && c.mv_staged) {
-        if (c.mv_staged == 2)
-            k_matvec_staged<1, false><<<c.g_mv_staged, MV_BLOCK, mv_smem<false>(), c.stream>>>(b, src);
-        else
-            k_matvec_staged<1, true><<<c.g_mv_staged, MV_BLOCK, mv_smem<true>(), c.stream>>>(b, src);
+        launch_staged<1>(b, c, src);
         CHECK_LAUNCH();
     }
     if (c.rows_pair) k_matvec_omega<T, MIXED, true><<<c.g_mv_pair, CELL_THREADS, 0, c.stream>>>(b, src);

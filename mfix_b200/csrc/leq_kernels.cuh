@@ -121,10 +121,11 @@ int prepare_line_kernel(int cmax, int *warps);
 template <typename T>
 int line_thread_occupancy();  // resident blocks per SM of the one-lane-per-line kernel
 //  // sets the smem attribute, returns resident blocks per SM
+constexpr int MV_SHAPES = 2;  // ring shapes of the staged FP32 matvec (option staged_matvec 1..2)
+
 struct CellOcc {
     int p_update, s_update, xr_update, matvec, matvec_pair, copy, outer;
-    int matvec_staged;        // the bulk-copy staged FP32 matvec with x's line / plane windows (0: it cannot run)
-    int matvec_staged_nowin;  // the same without the windows
+    int matvec_staged[MV_SHAPES + 1];  // the bulk-copy staged FP32 matvec, per ring shape 1.. (0: it cannot run)
 };
 void cell_occupancy(bool fp32, CellOcc *o);
 

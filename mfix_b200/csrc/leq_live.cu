@@ -182,6 +182,9 @@ int Engine::live_add(const LiveSystem &ls)
     st.min_margin = live_opt_.mixed_min_margin;
     st.defl_allow = live_opt_.deflate ? 1 : 0;
     st.replace_every = live_opt_.replace_every;
+    st.icheck = (live_opt_.minimize_dotproducts && !st.mixed)
+                    ? (live_opt_.transposed ? 5 : std::max(1, live_opt_.icheck_bicgs))
+                    : 0;
     st.restart_growth = live_opt_.restart_growth;
     st.margin_bits = 0x7f800000u;
     st.i = 1;
@@ -282,12 +285,9 @@ int Engine::live_commit()
         if (h_sys_[q].n > 0) ((h_sys_[q].jp & 1) ? cfg_.rows_single : cfg_.rows_pair) = 1;
     cfg_.mv_staged = 0;
     cfg_.g_mv_staged = 1;
-    if (mixed && live_opt_.staged_matvec == 1 && oc.matvec_staged > 0) {
-        cfg_.mv_staged = 1;
-        cfg_.g_mv_staged = grid(oc.matvec_staged);
-    } else if (mixed && live_opt_.staged_matvec == 2 && oc.matvec_staged_nowin > 0) {
-        cfg_.mv_staged = 2;
-        cfg_.g_mv_staged = grid(oc.matvec_staged_nowin);
+    if (mixed && live_opt_.staged_matvec >= 1 && live_opt_.staged_matvec <= MV_SHAPES && oc.matvec_staged[live_opt_.staged_matvec] > 0) {
+        cfg_.mv_staged = live_opt_.staged_matvec;
+        cfg_.g_mv_staged = grid(oc.matvec_staged[live_opt_.staged_matvec]);
     }
     cfg_.g_copy = grid(oc.copy);
     cfg_.g_outer = grid(oc.outer);

@@ -54,6 +54,9 @@ def lib() -> C.CDLL:
         L.orc_leq_bicgs.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_char_p, C.c_double, C.c_char_p, C.c_int,
                                     C.c_uint64, C.POINTER(Stats)]
         L.orc_leq_bicgs.restype = C.c_int
+        L.orc_leq_bicgs_icheck.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_char_p, C.c_double, C.c_char_p,
+                                           C.c_int, C.c_uint64, C.c_int, C.POINTER(Stats)]
+        L.orc_leq_bicgs_icheck.restype = C.c_int
         L.orc_leq_bicgs_sample.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_char_p, C.c_double, C.c_char_p,
                                            C.c_int, C.c_uint64, C.c_int, C.POINTER(Stats)]
         L.orc_leq_bicgs_sample.restype = C.c_int
@@ -73,7 +76,7 @@ def lib() -> C.CDLL:
         L.orc_truth_refine.restype = C.c_int
         L.orc_num_threads.restype = C.c_int
         L.orc_leq_bicgst.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_char_p, C.c_double, C.c_char_p, C.c_int,
-                                     C.c_uint64, C.POINTER(Stats)]
+                                     C.c_uint64, C.c_int, C.POINTER(Stats)]
         L.orc_leq_bicgst.restype = C.c_int
         L.orc_msolve_t.argtypes = [C.POINTER(Geom), vp, vp, vp, C.c_char_p, C.POINTER(C.c_int)]
         L.orc_msolve_t.restype = C.c_int
@@ -138,12 +141,17 @@ def uniform(seed: int, tag: int, idx: int) -> float:
     return lib().orc_uniform(seed, tag, idx)
 
 
-def leq_bicgs(s, sweep: str = "RSRS", pc: str = "LINE", seed: int = 0x5EED, max_exec: int | None = None) -> dict:
-    """LEQ_BICGS on s (in place: s.x solution, s.a / s.b scaled).  Returns the stats."""
+def leq_bicgs(s, sweep: str = "RSRS", pc: str = "LINE", seed: int = 0x5EED, max_exec: int | None = None,
+              icheck: int = 0) -> dict:
+    """LEQ_BICGS on s (in place: s.x solution, s.a / s.b scaled).  Returns the stats.
+    icheck > 0: MINIMIZE_DOTPRODUCTS with ICHECK_BICGS = icheck."""
     st = Stats()
     sw = sweep.ljust(4)[:4].encode()
     pcs = pc.ljust(4)[:4].encode()
-    if max_exec is None:
+    if icheck > 0:
+        lib().orc_leq_bicgs_icheck(C.byref(geom(s)), _p(s.x), _p(s.a), _p(s.b), sw, s.tol, pcs, s.itmax, seed,
+                                   int(icheck), C.byref(st))
+    elif max_exec is None:
         lib().orc_leq_bicgs(C.byref(geom(s)), _p(s.x), _p(s.a), _p(s.b), sw, s.tol, pcs, s.itmax, seed,
                             C.byref(st))
     else:
@@ -152,11 +160,12 @@ def leq_bicgs(s, sweep: str = "RSRS", pc: str = "LINE", seed: int = 0x5EED, max_
     return {k: getattr(st, k) for k, _ in Stats._fields_}
 
 
-def leq_bicgst(s, sweep: str = "RSRS", pc: str = "LINE", seed: int = 0x5EED) -> dict:
-    """LEQ_BICGSt (DO_TRANSPOSE) on s: s.x solution, s.b scaled, s.a left as given."""
+def leq_bicgst(s, sweep: str = "RSRS", pc: str = "LINE", seed: int = 0x5EED, minimize: bool = False) -> dict:
+    """LEQ_BICGSt (DO_TRANSPOSE) on s: s.x solution, s.b scaled, s.a left as given.
+    minimize: MINIMIZE_DOTPRODUCTS (the Rnorm test every fifth iteration)."""
     st = Stats()
     lib().orc_leq_bicgst(C.byref(geom(s)), _p(s.x), _p(s.a), _p(s.b), sweep.ljust(4)[:4].encode(), s.tol,
-                         pc.ljust(4)[:4].encode(), s.itmax, seed, C.byref(st))
+                         pc.ljust(4)[:4].encode(), s.itmax, seed, int(bool(minimize)), C.byref(st))
     return {k: getattr(st, k) for k, _ in Stats._fields_}
 
 

@@ -438,17 +438,22 @@ static int msolve_t(const orc_geom *g, const double *b, const double *a, double 
 
 /* transposed: LEQ_BICGS0t (model/leq_bicgst.f:102-627), whose scaling has no zero-row
  * test (:214-229) and whose preconditioner is LEQ_MSOLVEt */
+/* icheck: 0, or MINIMIZE_DOTPRODUCTS with the convergence test every icheck
+ * iterations (ICHECK_BICGS, model/leq_bicgs.f:372,411,439; LEQ_BICGSt tests every
+ * fifth, model/leq_bicgst.f:514): no Snorm exit, Rnorm formed only when tested. */
 static int bicgs_run_x(const orc_geom *g, double *var, double *a, double *b, const char *sweep, double tol,
-                       const char *pc, int itmax, uint64_t rt_seed, int max_exec, orc_stats *st, int transposed);
+                       const char *pc, int itmax, uint64_t rt_seed, int max_exec, orc_stats *st, int transposed,
+                       int icheck);
 
 static int bicgs_run(const orc_geom *g, double *var, double *a, double *b, const char *sweep, double tol,
                      const char *pc, int itmax, uint64_t rt_seed, int max_exec, orc_stats *st)
 {
-    return bicgs_run_x(g, var, a, b, sweep, tol, pc, itmax, rt_seed, max_exec, st, 0);
+    return bicgs_run_x(g, var, a, b, sweep, tol, pc, itmax, rt_seed, max_exec, st, 0, 0);
 }
 
 static int bicgs_run_x(const orc_geom *g, double *var, double *a, double *b, const char *sweep, double tol,
-                       const char *pc, int itmax, uint64_t rt_seed, int max_exec, orc_stats *st, int transposed)
+                       const char *pc, int itmax, uint64_t rt_seed, int max_exec, orc_stats *st, int transposed,
+                       int icheck)
 {
     memset(st, 0, sizeof(*st));
     st->exit_kind = -1;
@@ -524,8 +529,8 @@ static int bicgs_run_x(const orc_geom *g, double *var, double *a, double *b, con
         const double alpha = rho_m1 / rtv;
 #pragma omp parallel for schedule(static)
         for (int64_t p = 0; p < n; ++p) S[p] = R[p] - alpha * V[p];
-        const double snorm = sqrt(orc_dot(S, S, n));
-        if (snorm <= tolmin) {
+        const double snorm = icheck ? 1.0 : sqrt(orc_dot(S, S, n));
+        if (!icheck && snorm <= tolmin) {
 #pragma omp parallel for schedule(static)
             for (int64_t p = 0; p < n; ++p) var[p] = var[p] + alpha * Ph[p];
             converged = 1;
@@ -551,12 +556,14 @@ static int bicgs_run_x(const orc_geom *g, double *var, double *a, double *b, con
             var[p] = var[p] + alpha * Ph[p] + omega * Sh[p];
             R[p] = S[p] - omega * T[p];
         }
-        rnorm = sqrt(orc_dot(R, R, n));
-        if (rnorm <= tol * rnorm0) {
-            iter_tot_add = iter + 1;
-            converged = 1;
-            exit_kind = 0;
-            break;
+        if (!icheck || iter % icheck == 0) {
+            rnorm = sqrt(orc_dot(R, R, n));
+            if (rnorm <= tol * rnorm0) {
+                iter_tot_add = iter + 1;
+                converged = 1;
+                exit_kind = 0;
+                break;
+            }
         }
         ++iter;
         rho_m2 = rho_m1;
@@ -591,6 +598,12 @@ int orc_leq_bicgs(const orc_geom *g, double *var, double *a, double *b, const ch
                   const char *pc, int itmax, uint64_t rt_seed, orc_stats *st)
 {
     return bicgs_run(g, var, a, b, sweep, tol, pc, itmax, rt_seed, -1, st);
+}
+
+int orc_leq_bicgs_icheck(const orc_geom *g, double *var, double *a, double *b, const char *sweep, double tol,
+                         const char *pc, int itmax, uint64_t rt_seed, int icheck, orc_stats *st)
+{
+    return bicgs_run_x(g, var, a, b, sweep, tol, pc, itmax, rt_seed, -1, st, 0, icheck);
 }
 
 int orc_leq_bicgs_sample(const orc_geom *g, double *var, double *a, double *b, const char *sweep, double tol,
@@ -1202,12 +1215,12 @@ int orc_msolve_t(const orc_geom *g, const double *b, const double *a, double *va
 }
 
 int orc_leq_bicgst(const orc_geom *g, double *var, const double *a, double *b, const char *sweep, double tol,
-                   const char *pc, int itmax, uint64_t rt_seed, orc_stats *st)
+                   const char *pc, int itmax, uint64_t rt_seed, int minimize, orc_stats *st)
 {
     /* SOLVE_LIN_EQ's transposed copy A_mt (model/solve_lin_eq.f:139-150): scaled, then discarded */
     double *at = (double *)malloc(sizeof(double) * 7 * (size_t)g->n);
     memcpy(at, a, sizeof(double) * 7 * (size_t)g->n);
-    const int r = bicgs_run_x(g, var, at, b, sweep, tol, pc, itmax, rt_seed, -1, st, 1);
+    const int r = bicgs_run_x(g, var, at, b, sweep, tol, pc, itmax, rt_seed, -1, st, 1, minimize ? 5 : 0);
     free(at);
     return r;
 }

@@ -65,6 +65,11 @@ double orc_uniform(uint64_t seed, uint64_t tag, uint64_t idx);
 int orc_leq_bicgs(const orc_geom *g, double *var, double *a, double *b, const char *sweep,
                   double tol, const char *pc, int itmax, uint64_t rt_seed, orc_stats *st);
 
+/* MINIMIZE_DOTPRODUCTS = .TRUE. with ICHECK_BICGS = icheck (model/leq_bicgs.f:372,411,439):
+ * no Snorm exit, the Rnorm test every icheck-th iteration. */
+int orc_leq_bicgs_icheck(const orc_geom *g, double *var, double *a, double *b, const char *sweep, double tol,
+                         const char *pc, int itmax, uint64_t rt_seed, int icheck, orc_stats *st);
+
 /* Same algorithm with a cap on the number of iterations actually executed (timing samples). */
 int orc_leq_bicgs_sample(const orc_geom *g, double *var, double *a, double *b, const char *sweep,
                          double tol, const char *pc, int itmax, uint64_t rt_seed, int max_exec,
@@ -126,7 +131,7 @@ double orc_calc_resid_pp(const orc_geom *g, const int *flag, const double *b, do
  * copy (a is left as given), B scaled in place. */
 int orc_msolve_t(const orc_geom *g, const double *b, const double *a, double *var, const char *sweep, int *skips);
 int orc_leq_bicgst(const orc_geom *g, double *var, const double *a, double *b, const char *sweep, double tol,
-                   const char *pc, int itmax, uint64_t rt_seed, orc_stats *st);
+                   const char *pc, int itmax, uint64_t rt_seed, int minimize, orc_stats *st);
 
 int orc_num_threads(void);
 

@@ -59,6 +59,8 @@ def test_options_roundtrip():
     assert leq.get_option("deflate") == 1 and leq.get_option("replace_every") == 20
     assert leq.get_option("staged_matvec") == 2
     assert leq.get_option("restart_growth") == 100
+    assert leq.get_option("minimize_dotproducts") == 0 and leq.get_option("icheck_bicgs") == 1
+    assert leq.set_option("icheck_bicgs", 0) == leq.IER_ARGS
     assert leq.set_option("restart_growth", 0.5) == leq.IER_ARGS
     assert leq.set_option("restart_growth", 0) == 0 and leq.set_option("restart_growth", 100) == 0
     assert leq.set_option("staged_matvec", 0) == 0 and leq.get_option("staged_matvec") == 0

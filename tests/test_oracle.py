@@ -349,3 +349,27 @@ def test_cyclic_red_black_serial_order(dims, cyc, do_k):
     assert rc == 0
     ref = _rb_serial(s, x)
     assert np.max(np.abs(v - ref)) <= 1e-12 * np.max(np.abs(ref))
+
+
+def test_minimize_dotproducts_mode():
+    """MINIMIZE_DOTPRODUCTS (model/leq_bicgs.f:372,411,439): no Snorm exit and the
+    Rnorm test every ICHECK_BICGS-th iteration, so a converged solve stops on a
+    multiple of ICHECK_BICGS; with ICHECK_BICGS = 1 it is the plain iteration."""
+    s = S.conv_diff(14, 17, 12, seed=21)
+    base = s.copy()
+    st0 = O.leq_bicgs(base)
+    one = s.copy()
+    st1 = O.leq_bicgs(one, icheck=1)
+    assert st1["ier"] == st0["ier"] == 0 and st1["iterations"] == st0["iterations"]
+    assert np.array_equal(one.x, base.x)
+    for k in (3, 7):
+        t = s.copy()
+        stk = O.leq_bicgs(t, icheck=k)
+        assert stk["ier"] == 0 and stk["iterations"] % k == 0
+        assert st0["iterations"] <= stk["iterations"] < st0["iterations"] + k
+        sc = s.copy()
+        O.scale(sc)
+        assert O.true_resid(sc, t.x) <= s.tol * O.true_resid(sc, np.zeros(s.n)) * 1.01
+    tr = s.copy()
+    stt = O.leq_bicgst(tr, minimize=True)
+    assert stt["ier"] == 0 and stt["iterations"] % 5 == 0
