@@ -148,6 +148,25 @@ Engine::~Engine()
     if (stream_) cudaStreamDestroy(stream_);
 }
 
+// The host buffers the state snapshots land in: pinned and mapped, written by
+// k_state_snapshot through their device address.  The stream is drained before
+// an old buffer is freed (a snapshot may still be writing into it).
+int Engine::reserve_snapshots(size_t entries)
+{
+    if (entries <= h_st_pinned_cap_) return 0;
+    if (h_st_pinned_) {
+        CK(cudaStreamSynchronize(stream_));
+        cudaFreeHost(h_st_pinned_);
+    }
+    h_st_pinned_ = nullptr;
+    d_st_mapped_ = nullptr;
+    h_st_pinned_cap_ = 0;
+    CK(cudaHostAlloc((void **)&h_st_pinned_, sizeof(SysState) * entries, cudaHostAllocMapped));
+    CK(cudaHostGetDevicePointer((void **)&d_st_mapped_, h_st_pinned_, 0));
+    h_st_pinned_cap_ = entries;
+    return 0;
+}
+
 int Engine::fail(const std::string &msg, int code)
 {
     err_ = msg;
@@ -366,12 +385,7 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
         CK(cudaMalloc((void **)&d_partials_, need_part * sizeof(double)));
         part_cap_ = need_part;
     }
-    if ((size_t)nsys_ * 2 > h_st_pinned_cap_) {
-        if (h_st_pinned_) cudaFreeHost(h_st_pinned_);
-        h_st_pinned_ = nullptr;
-        CK(cudaMallocHost((void **)&h_st_pinned_, sizeof(SysState) * 2 * (size_t)nsys_));
-        h_st_pinned_cap_ = 2 * (size_t)nsys_;
-    }
+    if (const int rs = reserve_snapshots(2 * (size_t)nsys_)) return rs;
 
     view_.st = d_st_;
     view_.tiles = d_tiles_;
@@ -1320,8 +1334,8 @@ int Engine::run_batch(const std::vector<SystemSpec> &specs, const SolveOptions &
                 if (gexec) cudaGraphExecDestroy(gexec);
                 return rc;
             }
-        SysState *buf = h_st_pinned_ + (size_t)(snap & 1) * nsys_;
-        CK(cudaMemcpyAsync(buf, d_st_, sizeof(SysState) * nsys_, cudaMemcpyDeviceToHost, stream_));
+        CK(launch_state_snapshot(d_st_, d_st_mapped_ + (size_t)(snap & 1) * nsys_, nsys_, stream_));
+        ++launches_;
         CK(cudaEventRecord((snap & 1) ? ev_b_ : ev_a_, stream_));
         if (have_prev) {
             const int prev = (snap - 1) & 1;

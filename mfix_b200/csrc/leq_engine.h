@@ -286,8 +286,10 @@ private:
     size_t line_sys_cap_ = 0;
     int *d_allprefix_ = nullptr;
     double *d_partials_ = nullptr;
-    SysState *h_st_pinned_ = nullptr;
+    SysState *h_st_pinned_ = nullptr;  // state snapshots: pinned, mapped host memory
+    SysState *d_st_mapped_ = nullptr;  // the same memory as the kernels address it
     size_t h_st_pinned_cap_ = 0;
+    int reserve_snapshots(size_t entries);  // (re)allocates h_st_pinned_ for `entries` states
     BatchView view_{};
     LaunchCfg cfg_{};
 

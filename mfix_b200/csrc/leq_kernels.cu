@@ -1876,9 +1876,12 @@ __device__ inline void fin_outer(SysState &s, double rr, double rtr32)
         s.status = ST_DONE;
         return;
     }
+    // ITMAX spent without reaching TOL: the FP64 drop-in re-solves from the initial
+    // guess and gives the verdict (the mixed form is never worse than FP64's)
     if (s.inner_total >= s.itmax) {
-        s.iter = s.inner_total;
-        final_logic(s, false);
+        s.exit_kind = EX_FALLBACK;
+        s.ier = -20;
+        s.status = ST_DONE;
         return;
     }
     // a deflated system whose true residual has risen restart_growth-fold above its
@@ -3375,6 +3378,29 @@ cudaError_t launch_line_factor(const BatchView &b, const LaunchCfg &c, const int
     k_line_factor<T><<<(total_lines + 127) / 128, 128, 0, c.stream>>>(b, all_line_prefix);
     CHECK_LAUNCH();
 }
+// The per-system states written straight into pinned host memory by the SMs
+// (posted writes over the host link), not by a copy engine: a state read the host
+// polls on never queues behind bulk copies in flight on other streams (the scaled
+// A_M / B_M going back during the iterations, serving requests' inputs and results).
+static_assert(sizeof(SysState) % 8 == 0, "SysState copied in 8-byte words");
+__global__ void __launch_bounds__(256) k_state_snapshot(const SysState *__restrict__ src, SysState *dst, int nsys)
+{
+    const int64_t words = (int64_t)nsys * (int64_t)(sizeof(SysState) / 8);
+    const unsigned long long *s = reinterpret_cast<const unsigned long long *>(src);
+    unsigned long long *d = reinterpret_cast<unsigned long long *>(dst);
+    for (int64_t q = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; q < words; q += (int64_t)gridDim.x * blockDim.x)
+        d[q] = __ldcg(s + q);
+}
+
+cudaError_t launch_state_snapshot(const SysState *src, SysState *dst_host, int nsys, cudaStream_t s)
+{
+    if (nsys <= 0) return cudaSuccess;
+    const int64_t words = (int64_t)nsys * (int64_t)(sizeof(SysState) / 8);
+    const int grid = (int)std::min<int64_t>(64, (words + 255) / 256);
+    k_state_snapshot<<<grid, 256, 0, s>>>(src, dst_host, nsys);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_outer_step(const BatchView &b, const LaunchCfg &c)
 {
     k_outer_step<<<c.g_outer, CELL_THREADS, 0, c.stream>>>(b);

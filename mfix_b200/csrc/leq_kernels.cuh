@@ -93,6 +93,8 @@ cudaError_t launch_xr_update(const BatchView &b, const LaunchCfg &c, int ph, int
 
 // Mixed form: FP64 refinement step (outer residual in FP64, x accumulated in FP64)
 cudaError_t launch_outer_step(const BatchView &b, const LaunchCfg &c);
+// The states of nsys systems copied by the SMs into pinned (device-accessible) host memory.
+cudaError_t launch_state_snapshot(const SysState *src, SysState *dst_host, int nsys, cudaStream_t s);
 
 // Standalone kernels behind the per-routine C entry points
 template <typename T>

@@ -92,11 +92,9 @@ int Engine::live_open(int capacity, const SolveOptions &opt)
         CK(cudaMalloc((void **)&d_partials_, 2 * 1024 * sizeof(double)));
         part_cap_ = 2 * 1024;
     }
-    if ((size_t)capacity * 2 > h_st_pinned_cap_) {
-        if (h_st_pinned_) cudaFreeHost(h_st_pinned_);
-        h_st_pinned_ = nullptr;
-        CK(cudaMallocHost((void **)&h_st_pinned_, sizeof(SysState) * 2 * (size_t)capacity));
-        h_st_pinned_cap_ = 2 * (size_t)capacity;
+    {
+        const int rs = reserve_snapshots(2 * (size_t)capacity);
+        if (rs) return rs;
     }
     if (!ev_fence_) CK(cudaEventCreateWithFlags(&ev_fence_, cudaEventDisableTiming));
     for (int q = 0; q < 2; ++q) {
@@ -351,8 +349,8 @@ int Engine::live_step(int iterations)
     body_total_ += iterations;
     const int cap = (int)slot_used_.size();
     CK(cudaEventRecord(ev_c1_[b], stream_));
-    CK(cudaMemcpyAsync(h_st_pinned_ + (size_t)b * cap, d_st_, sizeof(SysState) * cap, cudaMemcpyDeviceToHost,
-                       stream_));
+    CK(launch_state_snapshot(d_st_, d_st_mapped_ + (size_t)b * cap, cap, stream_));
+    ++launches_;
     CK(cudaEventRecord(b ? ev_b_ : ev_a_, stream_));
     snap_bodies_[b] = body_total_;
     ++snap_count_;

@@ -91,6 +91,26 @@ def test_margin_routing_threshold():
         leq.set_option("precision", 0)
 
 
+def test_mixed_itmax_hands_over_to_fp64():
+    """ITMAX spent in FP32 without reaching TOL: the FP64 drop-in re-solves from
+    the initial guess and its verdict is the result, bit for bit."""
+    s = S.conv_diff(20, 22, 18, seed=6, itmax=8)
+    f = s.copy()
+    ier_f = leq.solve_system(f)
+    st_f = leq.last_stats()
+    assert ier_f in (-1, -2)
+    m = s.copy()
+    assert leq.set_option("precision", 1) == 0
+    try:
+        ier_m = leq.solve_system(m)
+        st_m = leq.last_stats()
+    finally:
+        leq.set_option("precision", 0)
+    assert ier_m == ier_f, leq.last_error()
+    assert st_m["fp64_fallback"] == 1 and st_m["iterations"] == st_f["iterations"]
+    assert np.array_equal(m.x, f.x) and np.array_equal(m.a, f.a) and np.array_equal(m.b, f.b)
+
+
 @pytest.mark.parametrize("precision", [0, 1])
 def test_batch_equals_alone(precision):
     sizes = [(9, 12, 7), (20, 15, 11), (5, 40, 6), (16, 16, 16), (31, 9, 4), (7, 7, 33)]
