@@ -512,8 +512,6 @@ def run_ours(args) -> None:
     dev = torch.device("cuda", local)
     if args.line_lanes:
         leq.set_option("line_lanes", args.line_lanes)
-    if args.line_stage >= 0:
-        leq.set_option("line_stage", args.line_stage)
     A0 = torch.from_numpy(sys0.a).to(dev)
     B0 = torch.from_numpy(sys0.b).to(dev)
     A = torch.empty_like(A0)
@@ -986,8 +984,6 @@ def run_batch_bench(args) -> None:
     if args.only != "all":  # profiling runs: the batched solve of one form only
         if args.line_lanes:
             leq.set_option("line_lanes", args.line_lanes)
-        if args.line_stage >= 0:
-            leq.set_option("line_stage", args.line_stage)
         import torch as _t
 
         pristine = [(_t.from_numpy(x.a).to(dev), _t.from_numpy(x.b).to(dev)) for x in systems]
@@ -1344,9 +1340,6 @@ def main() -> None:
                     help="default workload: the other configurations measured in the same run (comma list of "
                          "pressure, batch, serving; empty: none)")
     ap.add_argument("--line-lanes", type=int, default=0, help="force lanes per J-line (0: autotuned)")
-    ap.add_argument("--line-stage", type=int, default=-1,
-                    help="J-line kernel: 1 stage the rows past a line's first register passes, 0 register passes "
-                         "only (default: the library's)")
     ap.add_argument("--rate", type=float, default=0.0, help="serving: offered requests/s (0: the workload's)")
     ap.add_argument("--serve-check", type=int, default=0, help="serving: iterations between state reads")
     ap.add_argument("--tune-cache", default="", help="JSON file of J-line lanes choices: loaded, and new choices "

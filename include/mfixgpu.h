@@ -174,9 +174,6 @@ const char *mfixgpu_last_error(void);
  *                    by bulk copies, x's i/k neighbours read through L2; 1: x's i/k neighbour lines
  *                    staged too; 0: per-thread register loads (all three give the same products and
  *                    sums)
- *   "line_stage"     1 (default) the J-line kernel stages the rows past a line's first register
- *                    passes by asynchronous copies issued before them (one memory round trip per
- *                    register pass); 0: register passes only (both give the same bits)
  *   "write_back_ab"  1 (default) copy the scaled A_M/B_M slices back
  *   "rtilde_seed"    seed of the Rtilde random stream (replaces RANDOM_NUMBER, model/leq_bicgs.f:298)
  *   "inner_tol"      mixed form: drop of the FP32 residual between FP64 reliable updates (default 1e-2)

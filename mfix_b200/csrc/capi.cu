@@ -41,7 +41,6 @@ struct Options {
     int minimize_dotproducts = 0;
     int icheck_bicgs = 1;
     int staged_matvec = 2;
-    int line_stage = 1;
     int do_transpose = 0;
     int check_every = 4;
     int use_graph = 1;
@@ -283,7 +282,6 @@ SolveOptions make_opts(const Options &o, int pc, const char sweep4[4])
     so.minimize_dotproducts = o.minimize_dotproducts;
     so.icheck_bicgs = o.icheck_bicgs;
     so.staged_matvec = o.staged_matvec;
-    so.line_stage = o.line_stage;
     so.check_every = o.check_every;
     so.use_graph = o.use_graph != 0;
     so.time_kernels = o.time_kernels != 0;
@@ -691,9 +689,6 @@ int mfixgpu_set_option(const char *name, double value)
     } else if (k == "staged_matvec") {
         if (!(value >= 0 && value <= MV_SHAPES)) return MFIXGPU_ERR_ARGS;
         g.opt.staged_matvec = (int)value;
-    } else if (k == "line_stage") {
-        if (value != 0 && value != 1) return MFIXGPU_ERR_ARGS;
-        g.opt.line_stage = (int)value;
     } else if (k == "mixed_min_margin") {
         if (!(value >= 0)) return MFIXGPU_ERR_ARGS;
         g.opt.mixed_min_margin = value;
@@ -734,7 +729,6 @@ double mfixgpu_get_option(const char *name)
     if (k == "deflate") return g.opt.deflate;
     if (k == "replace_every") return g.opt.replace_every;
     if (k == "staged_matvec") return g.opt.staged_matvec;
-    if (k == "line_stage") return g.opt.line_stage;
     if (k == "restart_growth") return g.opt.restart_growth;
     if (k == "minimize_dotproducts") return g.opt.minimize_dotproducts;
     if (k == "icheck_bicgs") return g.opt.icheck_bicgs;

@@ -24,10 +24,6 @@ namespace mfixgpu {
 
 static size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
 
-// Most staged rows per lane of the warp J-line kernel (its shared-memory budget
-// beyond the line rows; the engine takes the most that keep the occupancy).
-static constexpr int MAX_STAGED_ROWS = 5;
-
 // The autotuner's choices are shared by every engine of the process (one-shot
 // solves and live batches pick the same lanes per line for the same line length,
 // so a system gives the same bits in either).
@@ -421,7 +417,6 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
     }
     cfg_.g_copy = grid(oc.copy);
     cfg_.g_outer = grid(oc.outer);
-    cfg_.line_stage = opt.line_stage ? 1 : 0;
     return configure_lines(mixed ? 4 : 8);
     return 0;
 }
@@ -457,23 +452,8 @@ int Engine::configure_lines(int elem, int only_L)
         return fail("internal: batch tables missing on the device", -13);
     cfg_.line_cmax = cmax;
     int wpb = 1;
-    auto prepare = [&](int sc, int *w) {
-        return elem == 4 ? prepare_line_kernel<float>(cmax, sc, w) : prepare_line_kernel<double>(cmax, sc, w);
-    };
-    const int bpsm = prepare(0, &wpb);
+    const int bpsm = elem == 4 ? prepare_line_kernel<float>(cmax, &wpb) : prepare_line_kernel<double>(cmax, &wpb);
     if (bpsm <= 0) return fail("J-lines too long for the shared-memory staging of the line kernel", -10);
-    // staged rows per lane: the most (up to MAX_STAGED_ROWS) that keep the
-    // resident blocks and warps per block of the unstaged kernel
-    cfg_.line_sc = 0;
-    if (cfg_.line_stage) {
-        for (int sc = MAX_STAGED_ROWS; sc >= 1; --sc) {
-            int w2 = 1;
-            if (prepare(sc, &w2) >= bpsm && w2 == wpb) {
-                cfg_.line_sc = sc;
-                break;
-            }
-        }
-    }
     cfg_.line_warps = wpb;
     const int items = h_prefix_[nsys_];
     cfg_.line_grid = std::max(1, std::min((items + wpb - 1) / wpb, sms_ * bpsm));
@@ -582,7 +562,7 @@ int Engine::autotune_lines(const SolveOptions &opt, int elem)
         for (int g = 1; g <= 32; g *= 2) {
             int G = 1, c = 1, kind = LK_WARP;
             set_shape(L, g, &G, &c, &kind);
-            if (kind == LK_WARP && (c > MAX_TUNED_ROWS || (size_t)kernel_smem_line_bytes(c, 0, elem) > 48 * 1024))
+            if (kind == LK_WARP && (c > MAX_TUNED_ROWS || (size_t)kernel_smem_line_bytes(c, elem) > 48 * 1024))
                 continue;
             for (int s = 0; s < nsys_; ++s)
                 if (h_sys_[s].jmax2 == L && h_sys_[s].n > 0) {

@@ -70,8 +70,6 @@ struct SolveOptions {
     int icheck_bicgs = 1;           // ICHECK_BICGS
     int staged_matvec = 2;       // mixed form: matvecs with operands staged by bulk copies (1: with x's
                                  // line / plane windows; 0: register loads)
-    int line_stage = 1;          // J-line kernel: stage the rows past a line's first register passes by
-                                 // asynchronous copies (0: register passes only)
     bool transposed = false;     // DO_TRANSPOSE (model/solve_lin_eq.f:139-150): LEQ_BICGSt's preconditioner
                                  // letters, and A is scaled in a copy (only B comes back scaled)
     int check_every = 4;         // iterations between host checks of the state

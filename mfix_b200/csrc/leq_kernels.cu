@@ -1716,14 +1716,9 @@ __global__ void __launch_bounds__(256) k_xr_update(BatchView b, int ph_id, int s
         using X_T = typename std::conditional<MIXED, double, T>::type;
         X_T *__restrict__ x =
             MIXED ? reinterpret_cast<X_T *>(d.x64[0]) : reinterpret_cast<X_T *>(vec<T>(d, V_X)) + c0;
-        // With an even JMAX2 a padded pair (even index) is a pair of cells of one
-        // line starting on an even natural index, or a pair of pad cells: one
-        // 16-byte access.  With an odd JMAX2 the two cells are read one by one.
-        const bool xeven = MIXED && (d.jmax2 & 1) == 0;
         auto xload = [&](int q) -> vec2_t<X_T> {
             if constexpr (MIXED) {
                 const NatPair np2 = nat_pair(d, c0 + 2 * q);
-                if (xeven) return np2.r0 ? ld2(x + np2.c) : mk2<X_T>(X_T(0), X_T(0));
                 return mk2<X_T>(np2.r0 ? x[np2.c] : X_T(0), np2.r1 ? x[np2.c + 1] : X_T(0));
             } else {
                 return ld2(x + 2 * q);
@@ -1732,10 +1727,6 @@ __global__ void __launch_bounds__(256) k_xr_update(BatchView b, int ph_id, int s
         auto xstore = [&](int q, const vec2_t<X_T> &v) {
             if constexpr (MIXED) {
                 const NatPair np2 = nat_pair(d, c0 + 2 * q);
-                if (xeven) {
-                    if (np2.r0) st2(x + np2.c, v);
-                    return;
-                }
                 if (np2.r0) x[np2.c] = v.x;
                 if (np2.r1) x[np2.c + 1] = v.y;
             } else {
@@ -1928,11 +1919,24 @@ __device__ inline void fin_outer(SysState &s, double rr, double rtr32)
     }
 }
 
+// True when a tile this block visits belongs to a system that passes the gate.
+// Every thread checks different tiles of the block's share, so a launch with
+// nothing to do costs one round of loads instead of one per tile in turn.
+__device__ __forceinline__ bool block_has_work(const BatchView &b, int gate)
+{
+    bool any = false;
+    for (int t = blockIdx.x + threadIdx.x * gridDim.x; t < b.ntiles && !any; t += blockDim.x * gridDim.x)
+        any = gate_ok(b.st[b.tiles[t].sys], gate);
+    return __syncthreads_or(any) != 0;
+}
+
 __global__ void __launch_bounds__(256) k_outer_step(BatchView b)
 {
     constexpr int U = 2;
     TileRun run{-1, 0};
     auto fin = [&](SysState &st, const double(&tot)[2]) { fin_outer(st, tot[0], tot[1]); };
+    // most launches find no system due for a reliable update
+    if (!block_has_work(b, G_OUTER)) return;
     for (int t = blockIdx.x; t < b.ntiles; t += gridDim.x) {
         const Tile tl = b.tiles[t];
         const SysDev &d = b.sys[tl.sys];
@@ -2365,45 +2369,8 @@ __device__ __forceinline__ void line_recurrences(T *f, const T *fl, const T *fr,
     }
 }
 
-// Operand rows of a line staged by asynchronous copies (VW > 1 instances): the
-// right-hand side, the four off-line coefficients and the four neighbour lines.
-enum StagedOperand : int { SO_RHS = 0, SO_AM1, SO_AP1, SO_NIM, SO_NIP, SO_AM3, SO_AP3, SO_NKM, SO_NKP, SO_COUNT };
-
-// Right-hand side of VW rows starting at row r from the operand rows (LEQ_IKSWEEP's
-// operand order); rows past the line, and every row of a flagged line, give zero.
 template <typename T, int VW>
-__device__ __forceinline__ RowsV<T, VW> line_f(const RowsV<T, VW> &rhs, const RowsV<T, VW> &am1, const RowsV<T, VW> &ap1,
-                                               const RowsV<T, VW> &nim, const RowsV<T, VW> &nip, const RowsV<T, VW> &am3,
-                                               const RowsV<T, VW> &ap3, const RowsV<T, VW> &nkm, const RowsV<T, VW> &nkp,
-                                               bool fast, bool do_k, int r, int L)
-{
-    RowsV<T, VW> fv;
-#pragma unroll
-    for (int k = 0; k < VW; ++k) {
-        T f0 = T(0);
-        if (fast && r + k < L) {
-            f0 = fnms(am1.v[k], nim.v[k], rhs.v[k]);
-            f0 = fnms(ap1.v[k], nip.v[k], f0);
-            if (do_k) {
-                f0 = fnms(am3.v[k], nkm.v[k], f0);
-                f0 = fnms(ap3.v[k], nkp.v[k], f0);
-            }
-        }
-        fv.v[k] = f0;
-    }
-    return fv;
-}
-
-// sc: staged rows per lane (0: none).  In the VW > 1 instances a line's rows
-// beyond its first register passes, up to G*sc of them, are copied into the
-// warp's staging rows by cp.async before the register passes start, so a line
-// costs one memory round trip per register pass; MFIX's line lengths (interior
-// cells plus two ghost cells, 2^m + 2) otherwise end in a nearly empty pass
-// that costs a full round trip.  The staged rows give the same right-hand sides
-// as the register rows (line_f), so results do not depend on sc.
-template <typename T, int VW>
-__global__ void __launch_bounds__(128, sizeof(T) == 4 ? (VW == 4 ? 5 : 6) : 4)
-    k_jline(BatchView b, WaveArgs w, int cmax, int sc)
+__global__ void __launch_bounds__(128, sizeof(T) == 4 ? (VW == 4 ? 5 : 6) : 4) k_jline(BatchView b, WaveArgs w, int cmax)
 {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     const int nwarps = blockDim.x >> 5;
@@ -2411,9 +2378,6 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? (VW == 4 ? 5 : 6) : 4)
     const int rows_w = 32 * cmax;
     T *s_f = reinterpret_cast<T *>(smem_raw) + (size_t)warp * 4 * rows_w;
     T *s_l = s_f + rows_w, *s_r = s_l + rows_w, *s_q = s_r + rows_w;
-    // staging rows: SO_COUNT arrays of 32*sc rows per warp, after every warp's line rows
-    const int srows = 32 * sc;
-    T *s_stage = reinterpret_cast<T *>(smem_raw) + (size_t)nwarps * 4 * rows_w + (size_t)warp * SO_COUNT * srows;
 
     const int total = (w.kind == 0) ? b.line_prefix[b.nsys] : w.count;
     const int step = gridDim.x * nwarps;
@@ -2442,73 +2406,46 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? (VW == 4 ? 5 : 6) : 4)
         // line's pivot flag (a flagged line ignores them).
         if constexpr (VW > 1) {  // lines start on VW-row boundaries
             using V = RowsV<T, VW>;
-            constexpr int VB = VW * sizeof(T);
             const int span = G * c;  // a multiple of VW (G >= VW)
-            const int pass_rows = VW * G;
             const T *rhs_l = x.rhs + x.base, *am1_l = x.a + 2 * x.n + x.base, *ap1_l = x.a + 4 * x.n + x.base;
             const T *am3_l = x.a + x.base, *ap3_l = x.a + 6 * x.n + x.base;
-            // rows holding line data (the line and its pad cells, whole VW-row
-            // groups); rows [first, lim) are staged, rows [lim, span) are zeros
-            const int lim = j.valid ? min(span, ((L + VW - 1) / VW) * VW) : 0;
-            int first = span;
-            if (sc > 0) first = min(span, max(1, (lim - G * sc + pass_rows - 1) / pass_rows) * pass_rows);
-            // row r of staged operand o at s_stage[seg * G * sc + o * srows + r - first]
-            for (int r = first + VW * gl; r < lim; r += pass_rows) {
-                T *stg = s_stage + seg * G * sc + (r - first);
-                cp_async<VB>(fl + r, gl_ + r, VB);
-                cp_async<VB>(fr + r, gr_ + r, VB);
-                cp_async<VB>(fq + r, gq_ + r, VB);
-                cp_async<VB>(stg + SO_RHS * srows, rhs_l + r, VB);
-                cp_async<VB>(stg + SO_AM1 * srows, am1_l + r, VB);
-                cp_async<VB>(stg + SO_AP1 * srows, ap1_l + r, VB);
-                cp_async<VB>(stg + SO_NIM * srows, x.nb_im + r, VB);
-                cp_async<VB>(stg + SO_NIP * srows, x.nb_ip + r, VB);
-                if (x.do_k) {
-                    cp_async<VB>(stg + SO_AM3 * srows, am3_l + r, VB);
-                    cp_async<VB>(stg + SO_AP3 * srows, ap3_l + r, VB);
-                    cp_async<VB>(stg + SO_NKM * srows, x.nb_km + r, VB);
-                    cp_async<VB>(stg + SO_NKP * srows, x.nb_kp + r, VB);
+            for (int r = VW * gl; r < span; r += VW * G) {
+                // factors straight to shared memory; rows past the line read the
+                // zeros of the pad cells or are zero-filled by the copy
+                const bool ok = j.valid && r < L;
+                const void *z = d.fac[0];
+                cp_async<VW * sizeof(T)>(fl + r, ok ? (const void *)(gl_ + r) : z, ok ? VW * sizeof(T) : 0);
+                cp_async<VW * sizeof(T)>(fr + r, ok ? (const void *)(gr_ + r) : z, ok ? VW * sizeof(T) : 0);
+                cp_async<VW * sizeof(T)>(fq + r, ok ? (const void *)(gq_ + r) : z, ok ? VW * sizeof(T) : 0);
+                V rhs, am1, ap1, am3, ap3, nim, nip, nkm, nkp;
+                if (ok) {  // rows r .. r+VW-1 lie on the line or on its pad cells
+                    rhs = ldv<T, VW>(rhs_l + r);
+                    am1 = ldv<T, VW>(am1_l + r);
+                    ap1 = ldv<T, VW>(ap1_l + r);
+                    nim = ldv<T, VW>(x.nb_im + r);
+                    nip = ldv<T, VW>(x.nb_ip + r);
+                    if (x.do_k) {
+                        am3 = ldv<T, VW>(am3_l + r);
+                        ap3 = ldv<T, VW>(ap3_l + r);
+                        nkm = ldv<T, VW>(x.nb_km + r);
+                        nkp = ldv<T, VW>(x.nb_kp + r);
+                    }
                 }
-            }
-            // register passes: rows [0, min(first, lim)), every group on the line or its pad cells
-            const int rl = min(first, lim);
-            for (int r = VW * gl; r < rl; r += pass_rows) {
-                cp_async<VB>(fl + r, gl_ + r, VB);  // factors straight to shared memory
-                cp_async<VB>(fr + r, gr_ + r, VB);
-                cp_async<VB>(fq + r, gq_ + r, VB);
-                V rhs = ldv<T, VW>(rhs_l + r), am1 = ldv<T, VW>(am1_l + r), ap1 = ldv<T, VW>(ap1_l + r),
-                  nim = ldv<T, VW>(x.nb_im + r), nip = ldv<T, VW>(x.nb_ip + r), am3, ap3, nkm, nkp;
-                if (x.do_k) {
-                    am3 = ldv<T, VW>(am3_l + r);
-                    ap3 = ldv<T, VW>(ap3_l + r);
-                    nkm = ldv<T, VW>(x.nb_km + r);
-                    nkp = ldv<T, VW>(x.nb_kp + r);
-                }
-                *reinterpret_cast<V *>(f + r) = line_f<T, VW>(rhs, am1, ap1, nim, nip, am3, ap3, nkm, nkp, fast, x.do_k, r, L);
-            }
-            // staged rows: each lane reads back the rows it copied itself
-            cp_async_wait_all();
-            for (int r = first + VW * gl; r < lim; r += pass_rows) {
-                const T *sr = s_stage + seg * G * sc + (r - first);
-                V rhs = ldv<T, VW>(sr + SO_RHS * srows), am1 = ldv<T, VW>(sr + SO_AM1 * srows),
-                  ap1 = ldv<T, VW>(sr + SO_AP1 * srows), nim = ldv<T, VW>(sr + SO_NIM * srows),
-                  nip = ldv<T, VW>(sr + SO_NIP * srows), am3, ap3, nkm, nkp;
-                if (x.do_k) {
-                    am3 = ldv<T, VW>(sr + SO_AM3 * srows);
-                    ap3 = ldv<T, VW>(sr + SO_AP3 * srows);
-                    nkm = ldv<T, VW>(sr + SO_NKM * srows);
-                    nkp = ldv<T, VW>(sr + SO_NKP * srows);
-                }
-                *reinterpret_cast<V *>(f + r) = line_f<T, VW>(rhs, am1, ap1, nim, nip, am3, ap3, nkm, nkp, fast, x.do_k, r, L);
-            }
-            for (int r = lim + VW * gl; r < span; r += pass_rows) {
-                V zv;  // rows past the line's groups (every row of a slot past the system's lines)
+                V fv;
 #pragma unroll
-                for (int k = 0; k < VW; ++k) zv.v[k] = T(0);
-                *reinterpret_cast<V *>(f + r) = zv;
-                *reinterpret_cast<V *>(fl + r) = zv;
-                *reinterpret_cast<V *>(fr + r) = zv;
-                *reinterpret_cast<V *>(fq + r) = zv;
+                for (int k = 0; k < VW; ++k) {
+                    T f0 = T(0);
+                    if (fast && r + k < L) {
+                        f0 = fnms(am1.v[k], nim.v[k], rhs.v[k]);
+                        f0 = fnms(ap1.v[k], nip.v[k], f0);
+                        if (x.do_k) {
+                            f0 = fnms(am3.v[k], nkm.v[k], f0);
+                            f0 = fnms(ap3.v[k], nkp.v[k], f0);
+                        }
+                    }
+                    fv.v[k] = f0;
+                }
+                *reinterpret_cast<V *>(f + r) = fv;
             }
         } else {
             constexpr int U = 2;
@@ -2560,7 +2497,8 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? (VW == 4 ? 5 : 6) : 4)
                 }
             }
         }
-        __syncwarp();  // (the VW > 1 instances waited for their copies above)
+        if constexpr (VW > 1) cp_async_wait_all();
+        __syncwarp();
 
         line_recurrences<T>(f, fl, fr, fq, c, G, gl);
         __syncwarp();
@@ -3253,19 +3191,18 @@ cudaError_t launch_p_update(const BatchView &b, const LaunchCfg &c)
     k_p_update<T, MIXED><<<c.g_p, CELL_THREADS, 0, c.stream>>>(b);
     CHECK_LAUNCH();
 }
-// Shared memory of one warp of the J-line kernel: right-hand side and the three
-// factor rows, plus sc staged rows per lane of each staged operand.
-int kernel_smem_line_bytes(int cmax, int sc, int elem_bytes) { return (4 * 32 * cmax + SO_COUNT * 32 * sc) * elem_bytes; }
+// Shared memory of one warp of the J-line kernel: right-hand side and the three factor rows.
+int kernel_smem_line_bytes(int cmax, int elem_bytes) { return 4 * 32 * cmax * elem_bytes; }
 
 // Picks the warps per block that fit the staging buffers, sets the shared-memory
 // attribute and returns the resident blocks per SM (0 when a line cannot fit).
 template <typename T>
-int prepare_line_kernel(int cmax, int sc, int *warps)
+int prepare_line_kernel(int cmax, int *warps)
 {
     int dev = 0, optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-    const int per_warp = kernel_smem_line_bytes(cmax, sc, (int)sizeof(T));
+    const int per_warp = kernel_smem_line_bytes(cmax, (int)sizeof(T));
     int wpb = std::min(4, optin / std::max(per_warp, 1));
     if (wpb < 1) return 0;
     *warps = wpb;
@@ -3283,20 +3220,16 @@ int prepare_line_kernel(int cmax, int sc, int *warps)
                 cudaFuncSetAttribute(k_jline<T, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
                     cudaSuccess ||
                 cudaFuncSetAttribute(k_jline<T, 1>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
-                    cudaSuccess) {
-                cudaGetLastError();
+                    cudaSuccess)
                 return 0;
-            }
             granted = smem;
         }
     }
     int nb = 0, nb1 = 0, nb2 = 0;
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, k_jline<T, VMAX>, wpb * 32, smem) != cudaSuccess ||
         cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb2, k_jline<T, 2>, wpb * 32, smem) != cudaSuccess ||
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb1, k_jline<T, 1>, wpb * 32, smem) != cudaSuccess) {
-        cudaGetLastError();
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb1, k_jline<T, 1>, wpb * 32, smem) != cudaSuccess)
         return 0;
-    }
     return std::min(nb, std::min(nb1, nb2));
 }
 
@@ -3392,14 +3325,14 @@ cudaError_t launch_jline(const BatchView &b, const LaunchCfg &c, const WaveArgs 
     // launch, the two-row instance when all their lines have even length
     if (c.line_thread) k_jline_thread<T><<<c.line_grid_thread, 128, 0, c.stream>>>(b, w);
     if (c.line_warp) {
-        const int smem = c.line_warps * kernel_smem_line_bytes(c.line_cmax, c.line_sc, (int)sizeof(T));
+        const int smem = c.line_warps * kernel_smem_line_bytes(c.line_cmax, (int)sizeof(T));
         constexpr int VMAX = sizeof(T) == 4 ? 4 : 2;
         if (c.line_single || c.line_vw == 1)
-            k_jline<T, 1><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax, c.line_sc);
+            k_jline<T, 1><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax);
         else if (c.line_vw >= VMAX)
-            k_jline<T, VMAX><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax, c.line_sc);
+            k_jline<T, VMAX><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax);
         else
-            k_jline<T, 2><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax, c.line_sc);
+            k_jline<T, 2><<<c.line_grid, c.line_warps * 32, smem, c.stream>>>(b, w, c.line_cmax);
     }
     CHECK_LAUNCH();
 }
@@ -3518,7 +3451,7 @@ cudaError_t launch_seq_lines(const BatchView &b, const SeqLineArgs &a, cudaStrea
     template cudaError_t launch_matvec_plain<T>(const SysDev *, const SysDev &, const T *, const T *, T *, \
                                                 cudaStream_t, int);                                       \
     template cudaError_t launch_seq_lines<T>(const BatchView &, const SeqLineArgs &, cudaStream_t);        \
-    template int prepare_line_kernel<T>(int, int, int *);                                                     \
+    template int prepare_line_kernel<T>(int, int *);                                                     \
     template int line_thread_occupancy<T>();                                                             \
     template cudaError_t launch_line_factor<T>(const BatchView &, const LaunchCfg &, const int *, int);
 #define INST_TM(T, M)                                                                       \

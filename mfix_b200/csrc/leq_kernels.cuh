@@ -28,8 +28,6 @@ struct LaunchCfg {
     int g_mv_staged;      // grid of the staged matvec
     int line_grid;   // blocks for J-line kernels
     int line_cmax;   // max rows per lane over the batch (smem sizing)
-    int line_sc;     // staged rows per lane of the warp J-line kernel (0: none)
-    int line_stage;  // 1: stage the rows past a line's first register passes (line_sc chosen per batch)
     int line_warps;  // warps per block of the J-line kernel
     int line_grid_thread;  // blocks of the one-lane-per-line kernel (4 warps each)
     int line_thread;       // 1: some system has one lane per line
@@ -119,9 +117,9 @@ struct SeqLineArgs {
 template <typename T>
 cudaError_t launch_seq_lines(const BatchView &b, const SeqLineArgs &a, cudaStream_t s);
 
-int kernel_smem_line_bytes(int cmax, int sc, int elem_bytes);
+int kernel_smem_line_bytes(int cmax, int elem_bytes);
 template <typename T>
-int prepare_line_kernel(int cmax, int sc, int *warps);
+int prepare_line_kernel(int cmax, int *warps);
 template <typename T>
 int line_thread_occupancy();  // resident blocks per SM of the one-lane-per-line kernel
 //  // sets the smem attribute, returns resident blocks per SM

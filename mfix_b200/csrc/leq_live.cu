@@ -108,7 +108,6 @@ int Engine::live_open(int capacity, const SolveOptions &opt)
     view_.nsys = capacity;
     view_.partials = d_partials_;
     cfg_.stream = stream_;
-    cfg_.line_stage = live_opt_.line_stage ? 1 : 0;
     int rc = configure_lines(mixed ? 4 : 8);
     if (rc) return rc;
 
@@ -290,7 +289,6 @@ int Engine::live_commit()
     }
     cfg_.g_copy = grid(oc.copy);
     cfg_.g_outer = grid(oc.outer);
-    cfg_.line_stage = live_opt_.line_stage ? 1 : 0;
     int rc = configure_lines(mixed ? 4 : 8);
     if (rc) return rc;
 

@@ -71,11 +71,6 @@ def test_options_roundtrip():
     assert leq.set_option("line_lanes", 33) == leq.IER_ARGS
     assert leq.set_option("line_lanes", 64) == leq.IER_ARGS
     assert leq.set_option("line_lanes", 0) == 0
-    # J-line staging of the rows past the register passes: 0 or 1
-    assert leq.get_option("line_stage") == 1
-    assert leq.set_option("line_stage", 0) == 0 and leq.get_option("line_stage") == 0
-    assert leq.set_option("line_stage", 2) == leq.IER_ARGS
-    assert leq.set_option("line_stage", 1) == 0
 
 
 def test_argument_errors_before_device_work():
