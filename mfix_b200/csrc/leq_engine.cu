@@ -422,7 +422,9 @@ int Engine::setup_batch(const std::vector<SystemSpec> &specs, const SolveOptions
 }
 
 // Work items of the J-line kernel (parity waves) and its launch shape, from each
-// system's lanes per line; the system table goes to the device here.  only_L > 0
+// system's lanes per line; the system table goes to the device here.  only_L = -1
+// keeps the line work of the systems whose line length is in tune_lengths_ only
+// (autotuning); only_L > 0
 // keeps the line work of the systems with that line length only (autotuning).
 int Engine::configure_lines(int elem, int only_L)
 {
@@ -432,7 +434,9 @@ int Engine::configure_lines(int elem, int only_L)
         const SysDev &d = h_sys_[s];
         cmax = std::max(cmax, d.rows_per_lane);
         const int lpw = 32 / d.lane_group;
-        const bool keep = d.n > 0 && (only_L == 0 || d.jmax2 == only_L);  // n = 0: empty slot of a live batch
+        const bool tuned = only_L < 0 && std::find(tune_lengths_.begin(), tune_lengths_.end(), d.jmax2) !=
+                                                tune_lengths_.end();
+        const bool keep = d.n > 0 && (only_L == 0 || d.jmax2 == only_L || tuned);  // n = 0: empty slot of a live batch
         const int64_t slots = keep ? (int64_t)d.half_lines * d.kmax2 : 0;
         h_prefix_[s + 1] = h_prefix_[s] + (int)((slots + lpw - 1) / lpw);
     }
@@ -523,12 +527,16 @@ void Engine::shape_for(int L, int elem, int forced, int *G, int *c, int *kind)
     *kind = *G == 1 ? LK_THREAD : LK_WARP;
 }
 
-// The autotuner: for every line length of the batch without a recorded choice,
-// time a red/black pass of the J-line kernel over the lines of that length only
-// (the other systems' line work masked out) for each lanes-per-line candidate
-// with at most MAX_TUNED_ROWS rows per lane, and keep the fastest.  The row
-// bound keeps the kernel's shared-memory staging, sized by the batch's largest
-// rows per lane, small enough for full occupancy.
+// The autotuner: for the line lengths of the batch without a recorded choice, time
+// a red/black pass of the J-line kernel over all their lines at once (the other
+// systems' line work masked out) for each lanes-per-line value g, each length
+// taking the smallest power of two at or above g that leaves it at most
+// MAX_TUNED_ROWS rows per lane, and keep the fastest g for all of them.  Timing
+// the whole mix at once ranks the shapes as the batch runs them: timing each
+// length alone, on its few systems, left a 512-system FP64 batch 10% slower than
+// one shape for every line.  The row bound keeps the kernel's shared-memory
+// staging, sized by the batch's largest rows per lane, small enough for full
+// occupancy.
 int Engine::autotune_lines(const SolveOptions &opt, int elem)
 {
     std::vector<int> todo;
@@ -553,52 +561,63 @@ int Engine::autotune_lines(const SolveOptions &opt, int elem)
         w[q].write_old = 1;
         w[q].gate = G_ANY;
     }
+    // lanes of length L under the candidate g (0: no shape fits)
+    auto lanes_for = [&](int L, int g) {
+        for (; g <= 32; g *= 2) {
+            int G = 1, c = 1, kind = LK_WARP;
+            set_shape(L, g, &G, &c, &kind);
+            if (kind != LK_WARP || (c <= MAX_TUNED_ROWS && (size_t)kernel_smem_line_bytes(c, elem) <= 48 * 1024))
+                return g;
+        }
+        return 0;
+    };
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
     CK(cudaEventCreate(&e1));
-    for (int L : todo) {
-        int best_g = 0;
-        float best_ms = 1e30f;
-        for (int g = 1; g <= 32; g *= 2) {
-            int G = 1, c = 1, kind = LK_WARP;
-            set_shape(L, g, &G, &c, &kind);
-            if (kind == LK_WARP && (c > MAX_TUNED_ROWS || (size_t)kernel_smem_line_bytes(c, elem) > 48 * 1024))
-                continue;
-            for (int s = 0; s < nsys_; ++s)
-                if (h_sys_[s].jmax2 == L && h_sys_[s].n > 0) {
-                    h_sys_[s].lane_group = G;
-                    h_sys_[s].rows_per_lane = c;
-                    h_sys_[s].line_kind = kind;
-                }
-            int rc = configure_lines(elem, L);
-            if (rc) return rc;
-            float tot = 0.f;
-            for (int rep = 0; rep < 4; ++rep) {
-                if (rep == 1) CK(cudaEventRecord(e0, stream_));
-                for (int q = 0; q < 2; ++q) CK(elem == 4 ? launch_jline<float>(view_, cfg_, w[q]) : launch_jline<double>(view_, cfg_, w[q]));
-            }
-            CK(cudaEventRecord(e1, stream_));
-            CK(cudaEventSynchronize(e1));
-            cudaEventElapsedTime(&tot, e0, e1);
-            if (tot < best_ms) {
-                best_ms = tot;
-                best_g = g;
-            }
+    tune_lengths_ = todo;
+    int best_g = 0;
+    float best_ms = 1e30f;
+    for (int g = 1; g <= 32; g *= 2) {
+        bool fits = true;
+        for (int L : todo) fits = fits && lanes_for(L, g) > 0;
+        if (!fits) continue;
+        for (int s = 0; s < nsys_; ++s) {
+            const int L = h_sys_[s].jmax2;
+            if (h_sys_[s].n > 0 && std::find(todo.begin(), todo.end(), L) != todo.end())
+                set_shape(L, lanes_for(L, g), &h_sys_[s].lane_group, &h_sys_[s].rows_per_lane, &h_sys_[s].line_kind);
         }
-        if (best_g == 0) {
-            int c_unused = 0;
-            line_shape(L, &best_g, &c_unused);
+        int rc = configure_lines(elem, -1);
+        if (rc) return rc;
+        float tot = 0.f;
+        for (int rep = 0; rep < 4; ++rep) {
+            if (rep == 1) CK(cudaEventRecord(e0, stream_));
+            for (int q = 0; q < 2; ++q) CK(elem == 4 ? launch_jline<float>(view_, cfg_, w[q]) : launch_jline<double>(view_, cfg_, w[q]));
         }
-        {
-            std::lock_guard<std::mutex> lk(tunes().mu);
-            tunes().lanes[std::make_pair(elem, L)] = best_g;
+        CK(cudaEventRecord(e1, stream_));
+        CK(cudaEventSynchronize(e1));
+        cudaEventElapsedTime(&tot, e0, e1);
+        if (tot < best_ms) {
+            best_ms = tot;
+            best_g = g;
         }
-        for (int s = 0; s < nsys_; ++s)
-            if (h_sys_[s].jmax2 == L && h_sys_[s].n > 0)
-                set_shape(L, best_g, &h_sys_[s].lane_group, &h_sys_[s].rows_per_lane, &h_sys_[s].line_kind);
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
+    tune_lengths_.clear();
+    for (int L : todo) {
+        int g = best_g > 0 ? lanes_for(L, best_g) : 0;
+        if (g == 0) {
+            int c_unused = 0;
+            line_shape(L, &g, &c_unused);
+        }
+        {
+            std::lock_guard<std::mutex> lk(tunes().mu);
+            tunes().lanes[std::make_pair(elem, L)] = g;
+        }
+        for (int s = 0; s < nsys_; ++s)
+            if (h_sys_[s].jmax2 == L && h_sys_[s].n > 0)
+                set_shape(L, g, &h_sys_[s].lane_group, &h_sys_[s].rows_per_lane, &h_sys_[s].line_kind);
+    }
     (void)opt;
     save_tune_cache();
     return configure_lines(elem);

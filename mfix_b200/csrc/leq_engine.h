@@ -203,6 +203,7 @@ private:
     int run_msolve_plan(int which, int elem);
     int bind_lists();
     int configure_lines(int elem, int only_L = 0);
+    std::vector<int> tune_lengths_;  // configure_lines(elem, -1): the line lengths being tuned
     void shape_for(int L, int elem, int forced, int *G, int *c, int *kind);
     int autotune_lines(const SolveOptions &opt, int elem);
     void save_tune_cache();
