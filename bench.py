@@ -901,7 +901,8 @@ def batch_measure(systems, dev, steps: int, warmup: int, barrier=None, mx=None, 
 
     for _ in range(warmup):
         batched(1)
-    loop_fp64()  # warm: autotuning of every line length, graph paths
+    batched(0)  # warm: each form's line shapes tuned on the whole batch (single solves tune one length alone)
+    loop_fp64()  # warm: graph paths of the single solves
     barrier()
     mixed = [batched(1) for _ in range(steps)]
     barrier()
