@@ -2278,20 +2278,6 @@ __device__ __forceinline__ void cp_async(void *smem_dst, const void *gmem_src, i
 
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
-// cp_async for rows read once: 16-byte copies bypass L1 (.cg); smaller ones
-// cannot and are cached like cp_async's.
-template <int B>
-__device__ __forceinline__ void cp_async_once(void *smem_dst, const void *gmem_src, int src_bytes)
-{
-    if constexpr (B == 16) {
-        const unsigned dst = (unsigned)__cvta_generic_to_shared(smem_dst);
-        asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(dst), "l"(gmem_src), "r"(src_bytes)
-                     : "memory");
-    } else {
-        cp_async<B>(smem_dst, gmem_src, src_bytes);
-    }
-}
-
 // ------------------------------------------------------------------ J-line half-sweep
 // One warp handles 32/G lines, G lanes per line; lane g owns the c rows
 // g*c .. g*c+c-1.  Each recurrence is split in three: a pass over the lane's rows
@@ -2310,26 +2296,6 @@ template <typename T, int VW>
 __device__ __forceinline__ RowsV<T, VW> ldv(const T *p)
 {
     return *reinterpret_cast<const RowsV<T, VW> *>(p);
-}
-// The same load marked streaming (evict first): for rows a line reads once, so
-// that L1 keeps the neighbour lines' rows, which the next lines read again.
-template <typename T, int VW>
-__device__ __forceinline__ RowsV<T, VW> ldv_once(const T *p)
-{
-    RowsV<T, VW> r;
-    if constexpr (sizeof(T) == 4 && VW == 4) {
-        const float4 v = __ldcs(reinterpret_cast<const float4 *>(p));
-        r.v[0] = v.x, r.v[1] = v.y, r.v[2] = v.z, r.v[3] = v.w;
-    } else if constexpr (sizeof(T) == 4 && VW == 2) {
-        const float2 v = __ldcs(reinterpret_cast<const float2 *>(p));
-        r.v[0] = v.x, r.v[1] = v.y;
-    } else if constexpr (sizeof(T) == 8 && VW == 2) {
-        const double2 v = __ldcs(reinterpret_cast<const double2 *>(p));
-        r.v[0] = v.x, r.v[1] = v.y;
-    } else {
-        r = ldv<T, VW>(p);
-    }
-    return r;
 }
 
 // c - a*b, a*b + c and a*b for the J-line sweeps: in FP32 with every rounding
@@ -2448,19 +2414,19 @@ __global__ void __launch_bounds__(128, sizeof(T) == 4 ? (VW == 4 ? 5 : 6) : 4) k
                 // zeros of the pad cells or are zero-filled by the copy
                 const bool ok = j.valid && r < L;
                 const void *z = d.fac[0];
-                cp_async_once<VW * sizeof(T)>(fl + r, ok ? (const void *)(gl_ + r) : z, ok ? VW * sizeof(T) : 0);
-                cp_async_once<VW * sizeof(T)>(fr + r, ok ? (const void *)(gr_ + r) : z, ok ? VW * sizeof(T) : 0);
-                cp_async_once<VW * sizeof(T)>(fq + r, ok ? (const void *)(gq_ + r) : z, ok ? VW * sizeof(T) : 0);
+                cp_async<VW * sizeof(T)>(fl + r, ok ? (const void *)(gl_ + r) : z, ok ? VW * sizeof(T) : 0);
+                cp_async<VW * sizeof(T)>(fr + r, ok ? (const void *)(gr_ + r) : z, ok ? VW * sizeof(T) : 0);
+                cp_async<VW * sizeof(T)>(fq + r, ok ? (const void *)(gq_ + r) : z, ok ? VW * sizeof(T) : 0);
                 V rhs, am1, ap1, am3, ap3, nim, nip, nkm, nkp;
                 if (ok) {  // rows r .. r+VW-1 lie on the line or on its pad cells
-                    rhs = ldv_once<T, VW>(rhs_l + r);
-                    am1 = ldv_once<T, VW>(am1_l + r);
-                    ap1 = ldv_once<T, VW>(ap1_l + r);
+                    rhs = ldv<T, VW>(rhs_l + r);
+                    am1 = ldv<T, VW>(am1_l + r);
+                    ap1 = ldv<T, VW>(ap1_l + r);
                     nim = ldv<T, VW>(x.nb_im + r);
                     nip = ldv<T, VW>(x.nb_ip + r);
                     if (x.do_k) {
-                        am3 = ldv_once<T, VW>(am3_l + r);
-                        ap3 = ldv_once<T, VW>(ap3_l + r);
+                        am3 = ldv<T, VW>(am3_l + r);
+                        ap3 = ldv<T, VW>(ap3_l + r);
                         nkm = ldv<T, VW>(x.nb_km + r);
                         nkp = ldv<T, VW>(x.nb_kp + r);
                     }
