@@ -180,7 +180,8 @@ const char *mfixgpu_last_error(void);
  *   "check_every"    iterations between host polls of convergence (default 4)
  *   "use_graph"      1 (default) replay the iteration body as a CUDA graph
  *   "time_kernels"   1: time every J-line sweep launch with CUDA events (no graph replay)
- *   "autotune"       1 (default): lanes per J-line picked by measurement for each new line length
+ *   "autotune"       1 (default): lanes per J-line picked by measurement for the new line lengths of a
+ *                    solve or batch (one lanes-per-line value timed on all their lines at once)
  *   "line_lanes"     0 (default) automatic, else lanes per J-line (1..32, rounded down to a power of two)
  * Returns 0, or MFIXGPU_ERR_ARGS for an unknown name. */
 int mfixgpu_set_option(const char *name, double value);
