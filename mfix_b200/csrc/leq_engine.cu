@@ -561,15 +561,20 @@ int Engine::autotune_lines(const SolveOptions &opt, int elem)
         w[q].write_old = 1;
         w[q].gate = G_ANY;
     }
-    // lanes of length L under the candidate g (0: no shape fits)
+    // lanes of length L under the candidate g: the smallest power of two at or
+    // above g within the row bound; for a line too long for the bound at any
+    // width, 32 while its staging stays within 48 KB per warp, else none (0:
+    // the candidate is skipped; one lane per line always fits)
     auto lanes_for = [&](int L, int g) {
-        for (; g <= 32; g *= 2) {
+        for (int h = g; h <= 32; h *= 2) {
             int G = 1, c = 1, kind = LK_WARP;
-            set_shape(L, g, &G, &c, &kind);
+            set_shape(L, h, &G, &c, &kind);
             if (kind != LK_WARP || (c <= MAX_TUNED_ROWS && (size_t)kernel_smem_line_bytes(c, elem) <= 48 * 1024))
-                return g;
+                return h;
         }
-        return 0;
+        int G = 1, c = 1, kind = LK_WARP;
+        set_shape(L, 32, &G, &c, &kind);
+        return (size_t)kernel_smem_line_bytes(c, elem) <= 48 * 1024 ? 32 : 0;
     };
     cudaEvent_t e0, e1;
     CK(cudaEventCreate(&e0));
@@ -606,7 +611,7 @@ int Engine::autotune_lines(const SolveOptions &opt, int elem)
     tune_lengths_.clear();
     for (int L : todo) {
         int g = best_g > 0 ? lanes_for(L, best_g) : 0;
-        if (g == 0) {
+        if (g == 0) {  // no candidate timed
             int c_unused = 0;
             line_shape(L, &g, &c_unused);
         }

@@ -131,6 +131,27 @@ def test_batch_equals_alone(precision):
         assert _true_rel(ref, together[q].x) <= s.tol * 1.01
 
 
+@pytest.mark.parametrize("precision", [0, 1])
+def test_batch_with_a_long_line(precision):
+    # JMAX2 = 602: more than 17 rows per lane at every width, so the autotuner
+    # gives that length 32 lanes (or one lane per line for all) while it times
+    # the batch's other lengths; results as alone and within TOL
+    systems = [S.conv_diff(4, 600, 3, seed=50), S.conv_diff(9, 20, 8, seed=51), S.conv_diff(6, 41, 5, seed=52)]
+    together = [s.copy() for s in systems]
+    rc, res = leq.batch_solve(together, precision=precision)
+    assert rc == 0, leq.last_error()
+    for q, s in enumerate(systems):
+        alone = s.copy()
+        rc1, r1 = leq.batch_solve([alone], precision=precision)
+        assert rc1 == 0
+        assert res[q].ier == r1[0].ier == 0
+        assert res[q].iterations == r1[0].iterations
+        assert np.array_equal(together[q].x, alone.x)
+        ref = s.copy()
+        O.leq_bicgs(ref)
+        assert _true_rel(ref, together[q].x) <= s.tol * 1.01
+
+
 def test_batch_rejects_sequential_letters():
     systems = [S.conv_diff(6, 6, 6, seed=q) for q in range(2)]
     rc, _ = leq.batch_solve(systems, sweep="ISIS")

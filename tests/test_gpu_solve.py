@@ -54,6 +54,8 @@ SOLVES = [
     ("none", lambda: S.conv_diff(10, 12, 8, seed=6), "RSRS", "NONE"),
     ("isis", lambda: S.conv_diff(11, 13, 7, seed=7), "ISIS", "LINE"),
     ("asas", lambda: S.conv_diff(9, 10, 8, seed=8), "ASAS", "LINE"),
+    # JMAX2 = 602: lines longer than the autotuner's 17 rows per lane at 32 lanes
+    ("long_lines", lambda: S.conv_diff(4, 600, 3, seed=14), "RSRS", "LINE"),
 ]
 
 
