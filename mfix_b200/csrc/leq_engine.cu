@@ -576,9 +576,20 @@ int Engine::autotune_lines(const SolveOptions &opt, int elem)
         set_shape(L, 32, &G, &c, &kind);
         return (size_t)kernel_smem_line_bytes(c, elem) <= 48 * 1024 ? 32 : 0;
     };
-    cudaEvent_t e0, e1;
-    CK(cudaEventCreate(&e0));
-    CK(cudaEventCreate(&e1));
+    // the timing events and the tuning mask are released on every way out
+    struct TuneScope {
+        std::vector<int> &mask;
+        cudaEvent_t e0 = nullptr, e1 = nullptr;
+        ~TuneScope()
+        {
+            if (e0) cudaEventDestroy(e0);
+            if (e1) cudaEventDestroy(e1);
+            mask.clear();
+        }
+    } scope{tune_lengths_};
+    CK(cudaEventCreate(&scope.e0));
+    CK(cudaEventCreate(&scope.e1));
+    const cudaEvent_t e0 = scope.e0, e1 = scope.e1;
     tune_lengths_ = todo;
     int best_g = 0;
     float best_ms = 1e30f;
@@ -606,9 +617,6 @@ int Engine::autotune_lines(const SolveOptions &opt, int elem)
             best_g = g;
         }
     }
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    tune_lengths_.clear();
     for (int L : todo) {
         int g = best_g > 0 ? lanes_for(L, best_g) : 0;
         if (g == 0) {  // no candidate timed
